@@ -1,0 +1,166 @@
+"""Oracle loaders -- TEST INFRASTRUCTURE ONLY.
+
+`port()` loads liboracle.so, the CPU restatement of the reference's BVH and
+path-tracing algorithms (bvh_oracle.cpp, pt_oracle.cpp).  `ref()` loads
+_ref/libref_bvh.so, the reference renderer's own BVH template and
+ray/triangle test compiled from its sources (recipe: oracle/Makefile), or
+returns None where it was not built.
+
+Only tests/, `__graft_entry__.smoke()` and bench.py's CPU-baseline leg may
+import this package.  The product (rise_b200) never does.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_port = None
+_ref = None
+
+_f32p = ctypes.POINTER(ctypes.c_float)
+_f64p = ctypes.POINTER(ctypes.c_double)
+_i32p = ctypes.POINTER(ctypes.c_int32)
+_u32p = ctypes.POINTER(ctypes.c_uint32)
+_u8p = ctypes.POINTER(ctypes.c_uint8)
+_vp = ctypes.c_void_p
+_i64 = ctypes.c_int64
+
+NODE2_DTYPE = np.dtype([("bmin", "<f4", 3), ("bmax", "<f4", 3), ("first", "<u4"),
+                        ("count", "<u2"), ("axis", "u1"), ("pad", "u1")])
+NODE4_DTYPE = np.dtype([("minx", "<f4", 4), ("miny", "<f4", 4), ("minz", "<f4", 4),
+                        ("maxx", "<f4", 4), ("maxy", "<f4", 4), ("maxz", "<f4", 4),
+                        ("child", "<i4", 4), ("count", "<u2", 4), ("nchild", "u1"),
+                        ("axis", "u1"), ("pad", "u1", 6)])
+NODE4_FIELDS = [f for f in NODE4_DTYPE.names if f != "pad"]
+assert NODE2_DTYPE.itemsize == 32 and NODE4_DTYPE.itemsize == 128
+
+
+def build():
+    """Compile liboracle.so (and _ref when the reference tree is present)."""
+    import subprocess
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+
+
+def _p(a, t):
+    return a.ctypes.data_as(t)
+
+
+def _setup(lib, prefix):
+    b = getattr(lib, prefix + "bvh_build")
+    b.restype = _vp
+    b.argtypes = [_f32p, _i64]
+    getattr(lib, prefix + "bvh_destroy").argtypes = [_vp]
+    for nm in ("bvh_num_nodes2", "bvh_num_nodes4"):
+        f = getattr(lib, prefix + nm)
+        f.restype = _i64
+        f.argtypes = [_vp]
+    c = getattr(lib, prefix + "closest")
+    c.restype = None
+    a = getattr(lib, prefix + "any")
+    a.restype = None
+    a.argtypes = [_vp, _f32p, _i64, _u8p, ctypes.c_int]
+    rt = getattr(lib, prefix + "ray_triangle")
+    rt.restype = ctypes.c_int
+    rt.argtypes = [_f64p] * 5 + [_f64p, _f64p, _f64p]
+
+
+def port():
+    global _port
+    if _port is None:
+        path = os.path.join(_HERE, "liboracle.so")
+        if not os.path.exists(path):
+            build()
+        lib = ctypes.CDLL(path)
+        _setup(lib, "orc_")
+        lib.orc_closest.argtypes = [_vp, _f32p, _i64, _i32p, _f64p, _f64p, ctypes.c_int]
+        lib.orc_bvh_export.argtypes = [_vp, _vp, _u32p, _vp]
+        lib.orc_closest_brute.argtypes = [_f32p, _i64, _f32p, _i64, _i32p, _f64p]
+        _port = lib
+    return _port
+
+
+def ref():
+    global _ref
+    if _ref is None:
+        path = os.path.join(_HERE, "_ref", "libref_bvh.so")
+        if not os.path.exists(path):
+            return None
+        lib = ctypes.CDLL(path)
+        _setup(lib, "ref_")
+        lib.ref_closest.argtypes = [_vp, _f32p, _i64, _i32p, _f64p, ctypes.c_int]
+        lib.ref_bvh_export.argtypes = [_vp, _vp, _u32p]
+        lib.ref_bvh_export4.argtypes = [_vp, _vp]
+        _ref = lib
+    return _ref
+
+
+class BVH:
+    """A BVH built by either the port (`kind='port'`) or the reference ('ref')."""
+
+    def __init__(self, tri9, kind="port"):
+        self.kind = kind
+        self.lib = port() if kind == "port" else ref()
+        if self.lib is None:
+            raise RuntimeError("reference harness oracle/_ref/libref_bvh.so is not built")
+        self.pre = "orc_" if kind == "port" else "ref_"
+        self.tri9 = np.ascontiguousarray(tri9, dtype=np.float32).reshape(-1, 9)
+        self.h = getattr(self.lib, self.pre + "bvh_build")(_p(self.tri9, _f32p), len(self.tri9))
+
+    def __del__(self):
+        h = getattr(self, "h", None)
+        if h:
+            getattr(self.lib, self.pre + "bvh_destroy")(h)
+            self.h = None
+
+    def nodes(self):
+        n2 = getattr(self.lib, self.pre + "bvh_num_nodes2")(self.h)
+        n4 = getattr(self.lib, self.pre + "bvh_num_nodes4")(self.h)
+        nodes2 = np.zeros(n2, NODE2_DTYPE)
+        prims = np.zeros(len(self.tri9), np.uint32)
+        nodes4 = np.zeros(n4, NODE4_DTYPE)
+        if self.kind == "port":
+            self.lib.orc_bvh_export(self.h, nodes2.ctypes.data, _p(prims, _u32p), nodes4.ctypes.data)
+        else:
+            self.lib.ref_bvh_export(self.h, nodes2.ctypes.data, _p(prims, _u32p))
+            self.lib.ref_bvh_export4(self.h, nodes4.ctypes.data)
+        return nodes2, prims, nodes4
+
+    def closest(self, rays, threads=os.cpu_count(), edge=False):
+        rays = np.ascontiguousarray(rays, dtype=np.float32).reshape(-1, 8)
+        n = len(rays)
+        ids = np.empty(n, np.int32)
+        t = np.empty(n, np.float64)
+        if self.kind == "port":
+            e = np.empty(n, np.float64) if edge else None
+            self.lib.orc_closest(self.h, _p(rays, _f32p), n, _p(ids, _i32p), _p(t, _f64p),
+                                 _p(e, _f64p) if edge else None, threads)
+            return (ids, t, e) if edge else (ids, t)
+        self.lib.ref_closest(self.h, _p(rays, _f32p), n, _p(ids, _i32p), _p(t, _f64p), threads)
+        return ids, t
+
+    def any(self, rays, threads=os.cpu_count()):
+        rays = np.ascontiguousarray(rays, dtype=np.float32).reshape(-1, 8)
+        occ = np.empty(len(rays), np.uint8)
+        getattr(self.lib, self.pre + "any")(self.h, _p(rays, _f32p), len(rays), _p(occ, _u8p), threads)
+        return occ
+
+
+def closest_brute(tri9, rays):
+    lib = port()
+    tri9 = np.ascontiguousarray(tri9, dtype=np.float32).reshape(-1, 9)
+    rays = np.ascontiguousarray(rays, dtype=np.float32).reshape(-1, 8)
+    ids = np.empty(len(rays), np.int32)
+    t = np.empty(len(rays), np.float64)
+    lib.orc_closest_brute(_p(tri9, _f32p), len(tri9), _p(rays, _f32p), len(rays), _p(ids, _i32p), _p(t, _f64p))
+    return ids, t
+
+
+def ray_triangle(o, d, v0, ea, eb, kind="port"):
+    """The reference's double Moller-Trumbore on one triangle: (hit, t, alpha, beta)."""
+    lib = port() if kind == "port" else ref()
+    fn = lib.orc_ray_triangle if kind == "port" else lib.ref_ray_triangle
+    arrs = [np.ascontiguousarray(x, dtype=np.float64) for x in (o, d, v0, ea, eb)]
+    t, a, b = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+    hit = fn(*[_p(x, _f64p) for x in arrs], ctypes.byref(t), ctypes.byref(a), ctypes.byref(b))
+    return bool(hit), t.value, a.value, b.value

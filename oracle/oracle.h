@@ -1,0 +1,61 @@
+/* oracle.h -- TEST INFRASTRUCTURE ONLY.
+ *
+ * CPU restatement ("port") of the reference renderer's hot-path algorithms:
+ * the SAH-binned BVH builder, its BVH4 collapse and traversal, the
+ * double-precision Moller-Trumbore ray/triangle test, and (pt_oracle.cpp) the
+ * hero-wavelength spectral path tracer.  Every function cites the reference
+ * file:line it follows.  Only tests/, the smoke check and bench.py's CPU
+ * baseline leg load this library; the product never does.
+ */
+#ifndef RTB200_ORACLE_H
+#define RTB200_ORACLE_H
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Same 32-byte packing as the reference BVH2 node
+ * (src/Library/Acceleration/BVH.h:87-96). */
+typedef struct {
+    float    bmin[3];
+    float    bmax[3];
+    uint32_t first_or_left;
+    uint16_t count;
+    uint8_t  axis;
+    uint8_t  pad;
+} orc_node2;
+
+/* Same 128-byte packing as the reference BVH4 node (BVH.h:124-137). */
+typedef struct {
+    float    minx[4], miny[4], minz[4];
+    float    maxx[4], maxy[4], maxz[4];
+    int32_t  child[4];
+    uint16_t count[4];
+    uint8_t  nchild;
+    uint8_t  axis;
+    uint8_t  pad[6];   /* the reference node is alignas(16): 128 bytes */
+} orc_node4;
+
+typedef struct orc_bvh orc_bvh;
+
+orc_bvh* orc_bvh_build(const float* tri9, int64_t n_tri);
+void     orc_bvh_destroy(orc_bvh* b);
+int64_t  orc_bvh_num_nodes2(const orc_bvh* b);
+int64_t  orc_bvh_num_nodes4(const orc_bvh* b);
+void     orc_bvh_export(const orc_bvh* b, orc_node2* nodes2, uint32_t* prims, orc_node4* nodes4);
+
+/* rays: 8 floats each (ox,oy,oz,tmin, dx,dy,dz,tmax). */
+void orc_closest(const orc_bvh* b, const float* rays, int64_t n, int32_t* id, double* t,
+                 double* edge_dist, int threads);
+void orc_any(const orc_bvh* b, const float* rays, int64_t n, uint8_t* occ, int threads);
+/* Brute force over every triangle (small cases only). */
+void orc_closest_brute(const float* tri9, int64_t n_tri, const float* rays, int64_t n,
+                       int32_t* id, double* t);
+int  orc_ray_triangle(const double* o, const double* d, const double* v0, const double* ea,
+                      const double* eb, double* t, double* alpha, double* beta);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
