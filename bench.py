@@ -1,0 +1,306 @@
+"""Benchmark: batched BVH ray casting on one B200 (or N replicas).
+
+Workload (one "step"): one pass of 4,194,304 closest-hit rays over a
+1,000,000-triangle soup (centroids uniform in the unit cube, vertices offset
+by N(0, 0.01^2); rays from a radius-2 sphere towards uniform targets in the
+cube; seed 7), through the reference's BVH (SAH 32 bins, leaf 4, collapsed to
+4-wide nodes) in the FP32-node layout.  Metric: Mrays/s.
+
+  python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+
+Under torchrun each rank holds the scene and casts its own 4,194,304 rays
+(weak scaling, no collective on the data path).  `--impl reference` times
+the reference renderer's own CPU BVH (oracle/_ref, or the oracle port where
+the reference was not built) on the host cores instead.
+"""
+import argparse
+import json
+import os
+import re
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N_TRI = 1_000_000
+N_RAYS = 4_194_304
+SEED = 7
+BYTES_CLOSEST = 48  # ray in 32 B + hit out 16 B
+BYTES_ANY = 33      # ray in 32 B + occlusion flag 1 B
+WORKLOAD = ("raycast microbench: 1,000,000-triangle soup, 4,194,304 rays from a radius-2 sphere, "
+            "closest-hit, reference BVH (SAH 32 bins, leaf 4) collapsed to 4-wide FP32 nodes")
+METRIC = "Mrays/s"
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=200)
+    p.add_argument("--warmup", type=int, default=5)
+    p.add_argument("--impl", default="rtb200", choices=["rtb200", "reference"])
+    p.add_argument("--e2e-steps", type=int, default=5)
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    return p.parse_args()
+
+
+def dist_info():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def load_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def profiled_traffic(name):
+    """Per-launch DRAM bytes from a committed ncu summary (profiles/<name>.md)."""
+    path = os.path.join(ROOT, "profiles", name + ".md")
+    if not os.path.exists(path):
+        return None
+    m = re.search(r"traffic_bytes_per_launch:\s*([0-9.eE+]+)", open(path).read())
+    return float(m.group(1)) if m else None
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle sampling around a timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        self.proc.wait()
+        rows = [r.split(",") for r in open(self.path).read().strip().splitlines() if r.strip()]
+        os.unlink(self.path)
+        sm = [float(r[1]) for r in rows if len(r) >= 9 and r[1].strip().replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if len(r) >= 9 and r[2].strip().replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows if len(r) >= 9 for k in range(4) if r[5 + k].strip() == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def cpu_reference_time(tri, rays, seconds=12.0, threads=None):
+    """Time the reference CPU BVH (oracle/_ref, else the oracle port) on host
+    cores over a bounded sample of the rays.  Returns (Mrays/s, kind, cores, n)."""
+    import oracle
+    kind = "reference" if oracle.ref() is not None else "port"
+    threads = threads or os.cpu_count()
+    b = oracle.BVH(tri, "ref" if kind == "reference" else "port")
+    probe = rays[:32768]
+    t0 = time.perf_counter()
+    b.closest(probe, threads=threads)
+    rate = len(probe) / max(time.perf_counter() - t0, 1e-6)
+    n = int(min(len(rays), max(65536, rate * seconds)))
+    t0 = time.perf_counter()
+    b.closest(rays[:n], threads=threads)
+    dt = time.perf_counter() - t0
+    return n / dt / 1e6, kind, threads, n
+
+
+def run_reference(args):
+    rank, world, _ = dist_info()
+    if rank != 0:
+        return
+    import oracle
+    from rise_b200 import scenes
+    tri = scenes.soup_triangles(N_TRI, seed=SEED)
+    rays = scenes.sphere_rays(N_RAYS, seed=SEED)
+    kind = "reference" if oracle.ref() is not None else "port"
+    b = oracle.BVH(tri, "ref" if kind == "reference" else "port")
+    threads = os.cpu_count()
+    sample = 65536
+    for i in range(args.warmup):
+        b.closest(rays[(i * sample) % N_RAYS:][:sample], threads=threads)
+    t0 = time.perf_counter()
+    for i in range(args.steps):
+        s = (i * sample) % (N_RAYS - sample)
+        b.closest(rays[s:s + sample], threads=threads)
+    dt = time.perf_counter() - t0
+    v = args.steps * sample / dt / 1e6
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": v, "unit": "Mrays/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded)", "config": {"workload": WORKLOAD, "n_tri": N_TRI, "n_rays": N_RAYS},
+        "cpu_baseline": {"value": v, "unit": "Mrays/s", "cores": threads, "kind": kind,
+                         "sample": f"{sample} rays per step of the {N_RAYS}-ray set, BVH build excluded"},
+        "e2e": {"value": v, "unit": "Mrays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }))
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+        return
+    import torch
+    import torch.distributed as dist
+    from rise_b200 import raycaster, scenes
+
+    rank, world, local = dist_info()
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+
+    tri = scenes.soup_triangles(N_TRI, seed=SEED)
+    rays = scenes.sphere_rays(N_RAYS, seed=SEED + 1000 * rank)
+    srays = scenes.sphere_rays(N_RAYS, seed=SEED + 1000 * rank, shadow=True)
+
+    ctx = raycaster.Context(local)
+    sf = raycaster.Scene(ctx)
+    sf.add_triangles(tri)
+    sf.commit("f32")
+    sq = raycaster.Scene(ctx)
+    sq.add_triangles(tri)
+    sq.commit("q8")
+    rf, rq = raycaster.RayCaster(sf), raycaster.RayCaster(sq)
+
+    stream = torch.cuda.current_stream()
+    sh = stream.cuda_stream
+    d_rays = torch.from_numpy(rays).cuda()
+    d_srays = torch.from_numpy(srays).cuda()
+    d_hits = torch.empty((N_RAYS, 4), dtype=torch.float32, device="cuda")
+    d_occ = torch.empty(N_RAYS, dtype=torch.uint8, device="cuda")
+
+    def step_closest(rc):
+        rc.cast_rays_device(d_rays.data_ptr(), d_hits.data_ptr(), N_RAYS, sh)
+
+    def step_any(rc):
+        rc.cast_shadow_rays_device(d_srays.data_ptr(), d_occ.data_ptr(), N_RAYS, sh)
+
+    def barrier():
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    for _ in range(max(3, args.warmup)):
+        step_closest(rf)
+    barrier()
+    clocks = ClockSampler(local)
+    clocks.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        step_closest(rf)
+    e1.record(stream)
+    barrier()
+    clk = clocks.stop()
+    ms = e0.elapsed_time(e1)
+    if world > 1:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    ms_step = ms / args.steps
+    value = world * N_RAYS / (ms_step * 1e-3) / 1e6
+
+    # Variants (same device-resident protocol, shorter runs).
+    def timed(fn, rc, n=20):
+        for _ in range(3):
+            fn(rc)
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(n):
+            fn(rc)
+        b.record(stream)
+        torch.cuda.synchronize()
+        return a.elapsed_time(b) / n
+
+    variants = {}
+    for name, fn, rc in (("closest_q8", step_closest, rq), ("any_f32", step_any, rf), ("any_q8", step_any, rq)):
+        variants[name] = N_RAYS / (timed(fn, rc) * 1e-3) / 1e6
+    hit_rate = float((d_hits[:, 1].view(torch.int32) >= 0).float().mean())
+
+    # End to end through the public host-buffer API: pinned host rays in,
+    # host hits out, copies inside the timed region.
+    h_rays = torch.from_numpy(rays).pin_memory().numpy()
+    h_hits = torch.empty(N_RAYS * 16, dtype=torch.uint8).pin_memory().numpy().view(raycaster.HIT_DTYPE)
+    from rise_b200._native import check, lib
+    import ctypes
+    for _ in range(2):
+        check(lib().rtb200_cast_closest(sf.h, ctypes.c_void_p(h_rays.ctypes.data), N_RAYS,
+                                        ctypes.c_void_p(h_hits.ctypes.data)), ctx.h)
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.e2e_steps):
+        check(lib().rtb200_cast_closest(sf.h, ctypes.c_void_p(h_rays.ctypes.data), N_RAYS,
+                                        ctypes.c_void_p(h_hits.ctypes.data)), ctx.h)
+    e2e_s = (time.perf_counter() - t0) / args.e2e_steps
+    if world > 1:
+        t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e = world * N_RAYS / e2e_s / 1e6
+
+    peak, peak_kind = load_peaks()
+    achieved = BYTES_CLOSEST * N_RAYS / (ms_step * 1e-3) / 1e9
+    traffic = profiled_traffic("raycast_closest_f32_soup1M")
+    info = sf.info()
+
+    out = {
+        "metric": METRIC, "value": value, "unit": "Mrays/s", "n_gpus": world, "steps": args.steps,
+        "warmup": max(3, args.warmup), "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded: triangles seed 7, rays seed 7 + 1000*rank)",
+        "config": {"workload": WORKLOAD, "n_tri": N_TRI, "n_rays_per_gpu": N_RAYS, "layout": "f32",
+                   "parallelism": f"replicas x{world}",
+                   "l2_policy": "inputs larger than L2 (rays 134 MB per pass); scene (nodes + triangles) stays resident",
+                   "bvh_nodes": info["n_nodes"], "scene_device_bytes": info["device_bytes"],
+                   "bvh_build_s": round(info["build_seconds"], 3), "hit_rate": round(hit_rate, 6)},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
+                     "algorithmic_bytes_per_ray": BYTES_CLOSEST},
+        "variants_mrays_s": variants,
+        "e2e": {"value": e2e, "unit": "Mrays/s", "h2d_bytes_per_step": 32 * N_RAYS,
+                "d2h_bytes_per_step": 16 * N_RAYS},
+        "gpu_launches": args.steps,
+        "clocks": clk,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        v, kind, cores, n = cpu_reference_time(tri, rays)
+        out["cpu_baseline"] = {"value": v, "unit": "Mrays/s", "cores": cores, "kind": kind,
+                               "sample": f"first {n} rays of the {N_RAYS}-ray set, closest-hit, BVH build excluded"}
+    sf.close()
+    sq.close()
+    ctx.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(out))
+
+
+if __name__ == "__main__":
+    main()

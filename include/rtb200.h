@@ -1,0 +1,135 @@
+/* rtb200.h -- C ABI of the B200 spectral path tracer and BVH ray caster.
+ *
+ * A drop-in for one hot path of the RISE renderer: the unidirectional
+ * hero-wavelength spectral path tracer driven by PixelBasedRasterizerHelper
+ * and the BVH ray caster beneath it.  Plain pointers and sizes only; every
+ * call returns an RTB200_* status code and never throws.  Device memory is
+ * owned by the context.  A context is single-owner: calls on one context are
+ * serialised by an internal mutex.
+ *
+ * Entry point -> reference interface it replaces (paths relative to the
+ * reference source tree):
+ *
+ *   rtb200_ctx_create / _destroy
+ *       the Job/RuntimeContext ownership of a render (Job.cpp:9268-9318)
+ *   rtb200_scene_create / _add_mesh / _commit / _destroy
+ *       TriangleMeshGeometryIndexed::DoneIndexedTriangles + the BVH
+ *       constructor (Geometry/TriangleMeshGeometryIndexed.cpp:444-537,
+ *       Acceleration/BVH.h:162-192) and ObjectManager::PrepareForRendering
+ *       (Managers/ObjectManager.cpp:404)
+ *   rtb200_cast_closest[_device]
+ *       IRayCaster::CastRay's intersection step, i.e.
+ *       ObjectManager::IntersectRay (Managers/ObjectManager.cpp:270-318) ->
+ *       BVH::IntersectRay (Acceleration/BVH.h:1475-1560), batched
+ *   rtb200_cast_any[_device]
+ *       IRayCaster::CastShadowRay (Rendering/RayCaster.cpp:1958-1966) ->
+ *       ObjectManager::IntersectShadowRay (Managers/ObjectManager.cpp:320-374)
+ *       -> BVH::IntersectRay_IntersectionOnly (Acceleration/BVH.h:1639-1717),
+ *       batched
+ */
+#ifndef RTB200_H
+#define RTB200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes. */
+#define RTB200_OK          0
+#define RTB200_E_INVALID   1  /* bad argument or call order */
+#define RTB200_E_OOM       2  /* device allocation failed */
+#define RTB200_E_BUDGET    3  /* request exceeds the context's memory budget */
+#define RTB200_E_TIMEOUT   4  /* a bounded device wait gave up */
+#define RTB200_E_DEVICE    5  /* CUDA error or device-side error word set */
+#define RTB200_E_NOT_READY 6  /* asynchronous work still in flight */
+
+/* BVH device layouts for rtb200_scene_commit. */
+#define RTB200_BVH_F32     0  /* FP32 child boxes, 128-byte 4-wide nodes */
+#define RTB200_BVH_Q8      1  /* 8-bit conservative child boxes, 64-byte nodes */
+
+typedef struct rtb200_ctx rtb200_ctx;
+typedef struct rtb200_scene rtb200_scene;
+
+/* One ray, 32 bytes: origin, tmin, unit or non-unit direction, tmax.
+ * Hits are reported for tmin < t < tmax (tmax may be +inf). */
+typedef struct {
+    float ox, oy, oz, tmin;
+    float dx, dy, dz, tmax;
+} rtb200_ray;
+
+/* One closest-hit result, 16 bytes.  prim is the triangle index in the
+ * order triangles were added to the scene (-1 on a miss); t is the
+ * reference's double-precision distance rounded to FP32; (a, b) are the
+ * barycentric weights of the triangle's second and third vertex. */
+typedef struct {
+    float t;
+    int32_t prim;
+    float a, b;
+} rtb200_hit;
+
+/* ---- context ----------------------------------------------------------- */
+
+/* Create a context on CUDA device `device`.  budget_bytes caps the device
+ * memory the context may hold (0 = no cap). */
+int rtb200_ctx_create(int device, size_t budget_bytes, rtb200_ctx** out);
+int rtb200_ctx_destroy(rtb200_ctx* ctx);
+/* Message for the last failing call on this context ("" if none). */
+const char* rtb200_last_error(const rtb200_ctx* ctx);
+/* Device bytes currently held by the context. */
+size_t rtb200_ctx_bytes_in_use(const rtb200_ctx* ctx);
+
+/* ---- scenes ------------------------------------------------------------ */
+
+int rtb200_scene_create(rtb200_ctx* ctx, rtb200_scene** out);
+/* Add an indexed triangle mesh: xyz holds n_verts float triples, tri holds
+ * n_tri uint32 index triples.  Triangles are numbered scene-wide in the
+ * order they are added.  material is an index into the scene's material
+ * table (ignored by the ray caster).  double_sided follows the reference's
+ * bDoubleSided (normals face the incoming ray). */
+int rtb200_scene_add_mesh(rtb200_scene* scene, const float* xyz, int64_t n_verts,
+                          const uint32_t* tri, int64_t n_tri, int32_t material,
+                          int32_t double_sided);
+/* Build the BVH on the host (all cores) and upload it.  layout is one of
+ * RTB200_BVH_*.  Meshes cannot be added after commit. */
+int rtb200_scene_commit(rtb200_scene* scene, int32_t layout);
+/* Node / triangle counts and device bytes of a committed scene. */
+int rtb200_scene_info(const rtb200_scene* scene, int64_t* n_tri, int64_t* n_nodes,
+                      int64_t* device_bytes, double* build_seconds);
+int rtb200_scene_destroy(rtb200_scene* scene);
+
+/* ---- host BVH build and export ----------------------------------------- */
+
+/* Builds the reference BVH on the host (all cores) without a device and
+ * exposes its node arrays: BVH2 nodes in the reference's 32-byte packing,
+ * the leaf-order triangle indices, and the collapsed 128-byte BVH4 nodes.
+ * Replaces BVH::Serialize's node/index export
+ * (Acceleration/BVH.h:353-373) and the BVH4 collapse (BVH.h:477-642). */
+typedef struct rtb200_bvh_host rtb200_bvh_host;
+int rtb200_bvh_host_build(const float* tri9, int64_t n_tri, int32_t threads, rtb200_bvh_host** out);
+int rtb200_bvh_host_info(const rtb200_bvh_host* h, int64_t* n_nodes2, int64_t* n_nodes4);
+/* Any output pointer may be NULL.  nodes2: 32 * n_nodes2 bytes;
+ * prims: n_tri uint32; nodes4: 128 * n_nodes4 bytes. */
+int rtb200_bvh_host_export(const rtb200_bvh_host* h, void* nodes2, uint32_t* prims, void* nodes4);
+int rtb200_bvh_host_destroy(rtb200_bvh_host* h);
+
+/* ---- batched ray casting ----------------------------------------------- */
+
+/* Host buffers: copies rays to the device, casts, copies results back, and
+ * returns when the results are in `hits` / `occluded`. */
+int rtb200_cast_closest(rtb200_scene* scene, const rtb200_ray* rays, int64_t n, rtb200_hit* hits);
+int rtb200_cast_any(rtb200_scene* scene, const rtb200_ray* rays, int64_t n, uint8_t* occluded);
+
+/* Device buffers (device pointers), asynchronous on `stream` (a
+ * cudaStream_t; NULL = the context's stream).  The caller synchronises. */
+int rtb200_cast_closest_device(rtb200_scene* scene, const rtb200_ray* d_rays, int64_t n,
+                               rtb200_hit* d_hits, void* stream);
+int rtb200_cast_any_device(rtb200_scene* scene, const rtb200_ray* d_rays, int64_t n,
+                           uint8_t* d_occluded, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* RTB200_H */

@@ -1,0 +1,361 @@
+// api.cpp -- the C ABI (include/rtb200.h): contexts, scenes, batched casts.
+//
+// Ownership follows the reference's explicit create/release style
+// (src/Library/Interfaces/IReference.h) with opaque handles; failures return
+// a status code and leave a message in rtb200_last_error instead of logging.
+#include <chrono>
+#include <cstring>
+#include <new>
+
+#include "core.h"
+
+namespace rtb200 {
+
+int SetError(rtb200_ctx* ctx, int code, const std::string& msg)
+{
+    if (ctx) ctx->err = msg;
+    return code;
+}
+
+int CudaCheck(rtb200_ctx* ctx, cudaError_t e, const char* what)
+{
+    if (e == cudaSuccess) return RTB200_OK;
+    return SetError(ctx, e == cudaErrorMemoryAllocation ? RTB200_E_OOM : RTB200_E_DEVICE,
+                    std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+int DevAlloc(rtb200_ctx* ctx, void** p, size_t bytes)
+{
+    *p = nullptr;
+    if (bytes == 0) return RTB200_OK;
+    if (ctx->budget && ctx->in_use + bytes > ctx->budget)
+        return SetError(ctx, RTB200_E_BUDGET, "device memory budget exceeded");
+    cudaError_t e = cudaMalloc(p, bytes);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        *p = nullptr;
+        return SetError(ctx, RTB200_E_OOM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    }
+    ctx->in_use += bytes;
+    return RTB200_OK;
+}
+
+void DevFree(rtb200_ctx* ctx, void* p, size_t bytes)
+{
+    if (!p) return;
+    cudaFree(p);
+    ctx->in_use -= bytes;
+}
+
+namespace {
+
+int EnsureStage(rtb200_scene* s, size_t in_bytes, size_t out_bytes)
+{
+    rtb200_ctx* ctx = s->ctx;
+    if (in_bytes > s->stage_in) {
+        DevFree(ctx, s->d_in, s->stage_in);
+        s->d_in = nullptr;
+        s->stage_in = 0;
+        int rc = DevAlloc(ctx, &s->d_in, in_bytes);
+        if (rc) return rc;
+        s->stage_in = in_bytes;
+    }
+    if (out_bytes > s->stage_out) {
+        DevFree(ctx, s->d_out, s->stage_out);
+        s->d_out = nullptr;
+        s->stage_out = 0;
+        int rc = DevAlloc(ctx, &s->d_out, out_bytes);
+        if (rc) return rc;
+        s->stage_out = out_bytes;
+    }
+    return RTB200_OK;
+}
+
+int CheckErrWord(rtb200_scene* s, cudaStream_t st)
+{
+    unsigned err = 0;
+    cudaError_t e = cudaMemcpyAsync(&err, s->d_err, sizeof(err), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return CudaCheck(s->ctx, e, "error word readback");
+    if (err) {
+        cudaMemsetAsync(s->d_err, 0, sizeof(unsigned), st);
+        return SetError(s->ctx, RTB200_E_DEVICE, "device error word set (traversal stack overflow)");
+    }
+    return RTB200_OK;
+}
+
+bool Aligned16(const void* p) { return ((uintptr_t)p & 15u) == 0; }
+
+}  // namespace
+}  // namespace rtb200
+
+using namespace rtb200;
+
+extern "C" {
+
+int rtb200_ctx_create(int device, size_t budget_bytes, rtb200_ctx** out)
+{
+    if (!out) return RTB200_E_INVALID;
+    *out = nullptr;
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || device < 0 || device >= n) {
+        cudaGetLastError();
+        return RTB200_E_DEVICE;
+    }
+    rtb200_ctx* ctx = new (std::nothrow) rtb200_ctx();
+    if (!ctx) return RTB200_E_OOM;
+    ctx->device = device;
+    ctx->budget = budget_bytes;
+    if (cudaSetDevice(device) != cudaSuccess ||
+        cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        cudaGetLastError();
+        delete ctx;
+        return RTB200_E_DEVICE;
+    }
+    *out = ctx;
+    return RTB200_OK;
+}
+
+int rtb200_ctx_destroy(rtb200_ctx* ctx)
+{
+    if (!ctx) return RTB200_E_INVALID;
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+    cudaStreamDestroy(ctx->stream);
+    delete ctx;
+    return RTB200_OK;
+}
+
+const char* rtb200_last_error(const rtb200_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+size_t rtb200_ctx_bytes_in_use(const rtb200_ctx* ctx) { return ctx ? ctx->in_use : 0; }
+
+int rtb200_scene_create(rtb200_ctx* ctx, rtb200_scene** out)
+{
+    if (!ctx || !out) return RTB200_E_INVALID;
+    std::lock_guard<std::mutex> g(ctx->mu);
+    *out = nullptr;
+    rtb200_scene* s = new (std::nothrow) rtb200_scene();
+    if (!s) return SetError(ctx, RTB200_E_OOM, "host allocation failed");
+    s->ctx = ctx;
+    cudaSetDevice(ctx->device);
+    void* p = nullptr;
+    int rc = DevAlloc(ctx, &p, 256);
+    if (rc) { delete s; return rc; }
+    cudaMemset(p, 0, 256);
+    s->d_counter = (unsigned long long*)p;
+    s->d_err = (unsigned*)((char*)p + 64);
+    *out = s;
+    return RTB200_OK;
+}
+
+int rtb200_scene_add_mesh(rtb200_scene* s, const float* xyz, int64_t n_verts, const uint32_t* tri,
+                          int64_t n_tri, int32_t material, int32_t double_sided)
+{
+    if (!s) return RTB200_E_INVALID;
+    rtb200_ctx* ctx = s->ctx;
+    std::lock_guard<std::mutex> g(ctx->mu);
+    if (s->committed) return SetError(ctx, RTB200_E_INVALID, "scene already committed");
+    if (n_verts < 0 || n_tri < 0 || (n_tri > 0 && (!xyz || !tri)))
+        return SetError(ctx, RTB200_E_INVALID, "bad mesh arguments");
+    if ((int64_t)(s->tri_material.size()) + n_tri > (int64_t)INT32_MAX)
+        return SetError(ctx, RTB200_E_INVALID, "too many triangles");
+    for (int64_t i = 0; i < 3 * n_tri; ++i)
+        if ((int64_t)tri[i] >= n_verts) return SetError(ctx, RTB200_E_INVALID, "triangle index out of range");
+    const size_t base = s->tri9.size();
+    s->tri9.resize(base + 9 * (size_t)n_tri);
+    float* dst = s->tri9.data() + base;
+    for (int64_t i = 0; i < n_tri; ++i)
+        for (int j = 0; j < 3; ++j)
+            std::memcpy(dst + 9 * i + 3 * j, xyz + 3 * (size_t)tri[3 * i + j], 12);
+    s->tri_material.insert(s->tri_material.end(), (size_t)n_tri, material);
+    s->tri_double_sided.insert(s->tri_double_sided.end(), (size_t)n_tri, (uint8_t)(double_sided ? 1 : 0));
+    return RTB200_OK;
+}
+
+int rtb200_scene_commit(rtb200_scene* s, int32_t layout)
+{
+    if (!s) return RTB200_E_INVALID;
+    rtb200_ctx* ctx = s->ctx;
+    std::lock_guard<std::mutex> g(ctx->mu);
+    if (s->committed) return SetError(ctx, RTB200_E_INVALID, "scene already committed");
+    if (layout != RTB200_BVH_F32 && layout != RTB200_BVH_Q8) return SetError(ctx, RTB200_E_INVALID, "unknown BVH layout");
+    const int64_t n_tri = (int64_t)s->tri_material.size();
+    if (n_tri == 0) return SetError(ctx, RTB200_E_INVALID, "scene has no triangles");
+    cudaSetDevice(ctx->device);
+    const auto t0 = std::chrono::steady_clock::now();
+    BuildReferenceBVH(s->tri9.data(), n_tri, 0, s->bvh);
+    std::vector<GpuTri> tris;
+    EncodeTriangles(s->tri9.data(), s->bvh, tris);
+    std::vector<GpuNode4> nf;
+    std::vector<QNode4> nq;
+    const void* nodes_src;
+    size_t nodes_bytes;
+    if (layout == RTB200_BVH_Q8) {
+        EncodeQuantNodes(s->bvh, nq);
+        nodes_src = nq.data();
+        nodes_bytes = nq.size() * sizeof(QNode4);
+    } else {
+        EncodeGpuNodes(s->bvh, nf);
+        nodes_src = nf.data();
+        nodes_bytes = nf.size() * sizeof(GpuNode4);
+    }
+    s->build_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    void* dn = nullptr;
+    void* dt = nullptr;
+    int rc = DevAlloc(ctx, &dn, nodes_bytes);
+    if (rc) return rc;
+    rc = DevAlloc(ctx, &dt, tris.size() * sizeof(GpuTri));
+    if (rc) { DevFree(ctx, dn, nodes_bytes); return rc; }
+    cudaError_t e = cudaMemcpyAsync(dn, nodes_src, nodes_bytes, cudaMemcpyHostToDevice, ctx->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dt, tris.data(), tris.size() * sizeof(GpuTri), cudaMemcpyHostToDevice, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) {
+        DevFree(ctx, dn, nodes_bytes);
+        DevFree(ctx, dt, tris.size() * sizeof(GpuTri));
+        return CudaCheck(ctx, e, "scene upload");
+    }
+    s->d_nodes = dn;
+    s->nodes_bytes = nodes_bytes;
+    s->d_tris = (GpuTri*)dt;
+    s->tris_bytes = tris.size() * sizeof(GpuTri);
+    s->n_nodes = (int64_t)s->bvh.nodes4.size();
+    s->layout = layout;
+    s->committed = true;
+    return RTB200_OK;
+}
+
+int rtb200_scene_info(const rtb200_scene* s, int64_t* n_tri, int64_t* n_nodes, int64_t* device_bytes,
+                      double* build_seconds)
+{
+    if (!s) return RTB200_E_INVALID;
+    if (n_tri) *n_tri = (int64_t)s->tri_material.size();
+    if (n_nodes) *n_nodes = s->n_nodes;
+    if (device_bytes) *device_bytes = (int64_t)(s->nodes_bytes + s->tris_bytes);
+    if (build_seconds) *build_seconds = s->build_seconds;
+    return RTB200_OK;
+}
+
+int rtb200_scene_destroy(rtb200_scene* s)
+{
+    if (!s) return RTB200_E_INVALID;
+    rtb200_ctx* ctx = s->ctx;
+    std::lock_guard<std::mutex> g(ctx->mu);
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+    DevFree(ctx, s->d_nodes, s->nodes_bytes);
+    DevFree(ctx, s->d_tris, s->tris_bytes);
+    DevFree(ctx, s->d_in, s->stage_in);
+    DevFree(ctx, s->d_out, s->stage_out);
+    DevFree(ctx, s->d_counter, 256);
+    delete s;
+    return RTB200_OK;
+}
+
+struct rtb200_bvh_host {
+    BuiltBVH b;
+};
+
+int rtb200_bvh_host_build(const float* tri9, int64_t n_tri, int32_t threads, rtb200_bvh_host** out)
+{
+    if (!out || n_tri < 0 || (n_tri > 0 && !tri9) || n_tri > (int64_t)UINT32_MAX) return RTB200_E_INVALID;
+    rtb200_bvh_host* h = new (std::nothrow) rtb200_bvh_host();
+    if (!h) return RTB200_E_OOM;
+    BuildReferenceBVH(tri9, n_tri, threads, h->b);
+    *out = h;
+    return RTB200_OK;
+}
+
+int rtb200_bvh_host_info(const rtb200_bvh_host* h, int64_t* n2, int64_t* n4)
+{
+    if (!h) return RTB200_E_INVALID;
+    if (n2) *n2 = (int64_t)h->b.nodes2.size();
+    if (n4) *n4 = (int64_t)h->b.nodes4.size();
+    return RTB200_OK;
+}
+
+int rtb200_bvh_host_export(const rtb200_bvh_host* h, void* nodes2, uint32_t* prims, void* nodes4)
+{
+    if (!h) return RTB200_E_INVALID;
+    if (nodes2 && !h->b.nodes2.empty()) std::memcpy(nodes2, h->b.nodes2.data(), h->b.nodes2.size() * sizeof(Node2));
+    if (prims && !h->b.prims.empty()) std::memcpy(prims, h->b.prims.data(), h->b.prims.size() * 4);
+    if (nodes4 && !h->b.nodes4.empty()) std::memcpy(nodes4, h->b.nodes4.data(), h->b.nodes4.size() * sizeof(Node4));
+    return RTB200_OK;
+}
+
+int rtb200_bvh_host_destroy(rtb200_bvh_host* h)
+{
+    if (!h) return RTB200_E_INVALID;
+    delete h;
+    return RTB200_OK;
+}
+
+int rtb200_cast_closest_device(rtb200_scene* s, const rtb200_ray* d_rays, int64_t n, rtb200_hit* d_hits,
+                               void* stream)
+{
+    if (!s) return RTB200_E_INVALID;
+    rtb200_ctx* ctx = s->ctx;
+    std::lock_guard<std::mutex> g(ctx->mu);
+    if (!s->committed) return SetError(ctx, RTB200_E_INVALID, "scene not committed");
+    if (n < 0 || (n > 0 && (!d_rays || !d_hits))) return SetError(ctx, RTB200_E_INVALID, "bad ray buffers");
+    if (!Aligned16(d_rays) || !Aligned16(d_hits)) return SetError(ctx, RTB200_E_INVALID, "ray/hit buffers must be 16-byte aligned");
+    cudaSetDevice(ctx->device);
+    return CudaCheck(ctx, LaunchCastClosest(s, d_rays, n, d_hits, stream ? (cudaStream_t)stream : ctx->stream),
+                     "closest-hit launch");
+}
+
+int rtb200_cast_any_device(rtb200_scene* s, const rtb200_ray* d_rays, int64_t n, uint8_t* d_occ, void* stream)
+{
+    if (!s) return RTB200_E_INVALID;
+    rtb200_ctx* ctx = s->ctx;
+    std::lock_guard<std::mutex> g(ctx->mu);
+    if (!s->committed) return SetError(ctx, RTB200_E_INVALID, "scene not committed");
+    if (n < 0 || (n > 0 && (!d_rays || !d_occ))) return SetError(ctx, RTB200_E_INVALID, "bad ray buffers");
+    if (!Aligned16(d_rays)) return SetError(ctx, RTB200_E_INVALID, "ray buffer must be 16-byte aligned");
+    cudaSetDevice(ctx->device);
+    return CudaCheck(ctx, LaunchCastAny(s, d_rays, n, d_occ, stream ? (cudaStream_t)stream : ctx->stream),
+                     "any-hit launch");
+}
+
+int rtb200_cast_closest(rtb200_scene* s, const rtb200_ray* rays, int64_t n, rtb200_hit* hits)
+{
+    if (!s) return RTB200_E_INVALID;
+    rtb200_ctx* ctx = s->ctx;
+    std::lock_guard<std::mutex> g(ctx->mu);
+    if (!s->committed) return SetError(ctx, RTB200_E_INVALID, "scene not committed");
+    if (n < 0 || (n > 0 && (!rays || !hits))) return SetError(ctx, RTB200_E_INVALID, "bad ray buffers");
+    if (n == 0) return RTB200_OK;
+    cudaSetDevice(ctx->device);
+    int rc = EnsureStage(s, (size_t)n * sizeof(rtb200_ray), (size_t)n * sizeof(rtb200_hit));
+    if (rc) return rc;
+    cudaStream_t st = ctx->stream;
+    cudaError_t e = cudaMemcpyAsync(s->d_in, rays, (size_t)n * sizeof(rtb200_ray), cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = LaunchCastClosest(s, (const rtb200_ray*)s->d_in, n, (rtb200_hit*)s->d_out, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(hits, s->d_out, (size_t)n * sizeof(rtb200_hit), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return CudaCheck(ctx, e, "closest-hit cast");
+    return CheckErrWord(s, st);
+}
+
+int rtb200_cast_any(rtb200_scene* s, const rtb200_ray* rays, int64_t n, uint8_t* occ)
+{
+    if (!s) return RTB200_E_INVALID;
+    rtb200_ctx* ctx = s->ctx;
+    std::lock_guard<std::mutex> g(ctx->mu);
+    if (!s->committed) return SetError(ctx, RTB200_E_INVALID, "scene not committed");
+    if (n < 0 || (n > 0 && (!rays || !occ))) return SetError(ctx, RTB200_E_INVALID, "bad ray buffers");
+    if (n == 0) return RTB200_OK;
+    cudaSetDevice(ctx->device);
+    int rc = EnsureStage(s, (size_t)n * sizeof(rtb200_ray), (size_t)n);
+    if (rc) return rc;
+    cudaStream_t st = ctx->stream;
+    cudaError_t e = cudaMemcpyAsync(s->d_in, rays, (size_t)n * sizeof(rtb200_ray), cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = LaunchCastAny(s, (const rtb200_ray*)s->d_in, n, (uint8_t*)s->d_out, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(occ, s->d_out, (size_t)n, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return CudaCheck(ctx, e, "any-hit cast");
+    return CheckErrWord(s, st);
+}
+
+}  // extern "C"

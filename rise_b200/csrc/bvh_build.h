@@ -1,0 +1,92 @@
+// bvh_build.h -- host-side BVH construction for the B200 ray caster.
+//
+// Builds the reference renderer's BVH exactly (src/Library/Acceleration/BVH.h:
+// SAH-binned BVH2, 32 bins, leaf <= 4, Ctrav = Cint = 1, float boxes rounded
+// outward by one ulp, then the BVH4 collapse) so hit ids can be compared with
+// the reference bit for bit.  The build runs subtrees on all host cores and
+// then renumbers nodes into the reference's depth-first pair order, which
+// makes the node arrays byte-identical to a single-threaded reference build.
+//
+// The collapsed BVH4 is then re-encoded into one of two device layouts
+// (GpuNode4 with FP32 child boxes, or QNode4 with 8-bit child boxes quantised
+// conservatively against a per-node origin and power-of-two scale).
+#pragma once
+#include <cstdint>
+#include <vector>
+
+namespace rtb200 {
+
+// Reference BVH2 node, 32 bytes (BVH.h:87-96).
+struct Node2 {
+    float bmin[3];
+    float bmax[3];
+    uint32_t first_or_left;
+    uint16_t count;
+    uint8_t axis;
+    uint8_t pad;
+};
+static_assert(sizeof(Node2) == 32, "Node2 must be 32 bytes");
+
+// Reference BVH4 node, 128 bytes (BVH.h:124-137).
+struct alignas(16) Node4 {
+    float minx[4], miny[4], minz[4];
+    float maxx[4], maxy[4], maxz[4];
+    int32_t child[4];
+    uint16_t count[4];
+    uint8_t nchild;
+    uint8_t axis;
+    uint8_t pad[6];
+};
+static_assert(sizeof(Node4) == 128, "Node4 must be 128 bytes");
+
+struct BuiltBVH {
+    std::vector<Node2> nodes2;
+    std::vector<uint32_t> prims;   // leaf order -> input triangle index
+    std::vector<Node4> nodes4;
+};
+
+// tri9: n_tri triangles, 9 floats each (v0, v1, v2).  threads <= 0 uses all
+// host cores.
+void BuildReferenceBVH(const float* tri9, int64_t n_tri, int threads, BuiltBVH& out);
+
+// ---- device layouts -------------------------------------------------------
+
+// FP32 wide node: 4 child boxes as SoA float4 + child links, 128 bytes.
+// child[i] >= 0: internal node index when count[i] == 0, else first triangle
+// (in leaf order) of a leaf of count[i] triangles.  count[i] < 0: empty slot.
+struct alignas(16) GpuNode4 {
+    float lox[4], loy[4], loz[4];
+    float hix[4], hiy[4], hiz[4];
+    int32_t child[4];
+    int32_t count[4];
+};
+static_assert(sizeof(GpuNode4) == 128, "GpuNode4 must be 128 bytes");
+
+// Quantised wide node, 64 bytes.  Child box bounds are 8-bit integers q with
+// box = origin + q * 2^exp per axis; lower bounds are rounded down and upper
+// bounds up, and the encoder verifies the FP32 decode still contains the FP32
+// box, so culling is conservative.
+struct alignas(16) QNode4 {
+    float ox, oy, oz;              // origin (min corner of the union box)
+    int8_t ex, ey, ez;             // power-of-two scale exponents
+    uint8_t nchild;
+    uint8_t qlo[3][4];             // [axis][child]
+    uint8_t qhi[3][4];
+    int32_t child[4];
+    int16_t count[4];
+};
+static_assert(sizeof(QNode4) == 64, "QNode4 must be 64 bytes");
+
+// One triangle in leaf order: v0.w carries the input triangle index.
+struct alignas(16) GpuTri {
+    float v0[4];
+    float v1[4];
+    float v2[4];
+};
+static_assert(sizeof(GpuTri) == 48, "GpuTri must be 48 bytes");
+
+void EncodeGpuNodes(const BuiltBVH& b, std::vector<GpuNode4>& out);
+void EncodeQuantNodes(const BuiltBVH& b, std::vector<QNode4>& out);
+void EncodeTriangles(const float* tri9, const BuiltBVH& b, std::vector<GpuTri>& out);
+
+}  // namespace rtb200

@@ -1,0 +1,62 @@
+// core.h -- internal context and scene state behind the C ABI (rtb200.h).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/rtb200.h"
+#include "bvh_build.h"
+
+struct rtb200_ctx {
+    int device = 0;
+    int num_sms = 0;
+    size_t budget = 0;      // 0 = no cap
+    size_t in_use = 0;
+    cudaStream_t stream = nullptr;
+    std::mutex mu;
+    std::string err;
+};
+
+struct rtb200_scene {
+    rtb200_ctx* ctx = nullptr;
+    // host geometry, scene-wide triangle numbering
+    std::vector<float> tri9;
+    std::vector<int32_t> tri_material;
+    std::vector<uint8_t> tri_double_sided;
+    bool committed = false;
+    int32_t layout = RTB200_BVH_F32;
+    int64_t n_nodes = 0;
+    double build_seconds = 0.0;
+    rtb200::BuiltBVH bvh;            // kept for the path tracer's emitter tables
+    // device data
+    void* d_nodes = nullptr;
+    size_t nodes_bytes = 0;
+    rtb200::GpuTri* d_tris = nullptr;
+    size_t tris_bytes = 0;
+    // per-scene scratch: work counter (u64) and error word (u32)
+    unsigned long long* d_counter = nullptr;
+    unsigned* d_err = nullptr;
+    // staging for the host-buffer entry points
+    void* d_in = nullptr;
+    void* d_out = nullptr;
+    size_t stage_in = 0, stage_out = 0;
+};
+
+namespace rtb200 {
+
+// Device allocation against the context budget.
+int DevAlloc(rtb200_ctx* ctx, void** p, size_t bytes);
+void DevFree(rtb200_ctx* ctx, void* p, size_t bytes);
+int SetError(rtb200_ctx* ctx, int code, const std::string& msg);
+int CudaCheck(rtb200_ctx* ctx, cudaError_t e, const char* what);
+
+// Kernel launchers (raycast.cu).  Asynchronous on `stream`.
+cudaError_t LaunchCastClosest(const rtb200_scene* s, const rtb200_ray* d_rays, int64_t n,
+                              rtb200_hit* d_hits, cudaStream_t stream);
+cudaError_t LaunchCastAny(const rtb200_scene* s, const rtb200_ray* d_rays, int64_t n,
+                          uint8_t* d_occ, cudaStream_t stream);
+
+}  // namespace rtb200

@@ -1,0 +1,58 @@
+"""The product's host BVH builder (librtb200.so) reproduces the reference tree.
+
+Checked byte for byte against the reference's golden node arrays and, at
+larger sizes, against the oracle port (itself pinned to the reference).  No
+device is needed: rtb200_bvh_host_* run on the host only.
+"""
+import os
+
+import numpy as np
+import pytest
+
+import oracle
+from rise_b200 import raycaster, scenes
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def test_host_builder_matches_golden():
+    g = np.load(os.path.join(GOLDEN, "bvh_soup_2k.npz"))
+    n2, prims, n4 = raycaster.build_host_bvh(g["tri9"])
+    assert n2.view(np.uint8).tobytes() == g["nodes2"].tobytes()
+    assert (prims == g["prims"]).all()
+    r4 = g["nodes4"].view(raycaster.NODE4_DTYPE)
+    for f in oracle.NODE4_FIELDS:
+        assert (n4[f] == r4[f]).all(), f
+
+
+@pytest.mark.parametrize("n_tri,threads", [(1, 0), (4, 0), (5, 2), (300, 3), (70000, 0), (300000, 8)])
+def test_host_builder_matches_port(n_tri, threads):
+    tri = scenes.soup_triangles(n_tri, seed=100 + n_tri)
+    n2, prims, n4 = raycaster.build_host_bvh(tri, threads=threads)
+    p2, pp, p4 = oracle.BVH(tri, "port").nodes()
+    assert n2.tobytes() == p2.tobytes()
+    assert (prims == pp).all()
+    for f in oracle.NODE4_FIELDS:
+        assert (n4[f] == p4[f]).all(), f
+
+
+def test_host_builder_degenerate_inputs():
+    # All triangles share one centroid: the reference makes one big leaf.
+    tri = np.tile(np.array([[0, 0, 0, 1, 0, 0, 0, 1, 0]], np.float32), (40, 1))
+    n2, prims, n4 = raycaster.build_host_bvh(tri)
+    p2, pp, p4 = oracle.BVH(tri, "port").nodes()
+    assert n2.tobytes() == p2.tobytes() and len(n2) == 1 and n2[0]["count"] == 40
+    # Collinear centroids along one axis with duplicates.
+    x = np.repeat(np.arange(10, dtype=np.float32), 7)
+    tri = np.zeros((len(x), 9), np.float32)
+    tri[:, 0] = x
+    tri[:, 3] = x + 0.5
+    tri[:, 7] = 1.0
+    n2, prims, n4 = raycaster.build_host_bvh(tri)
+    p2, pp, p4 = oracle.BVH(tri, "port").nodes()
+    assert n2.tobytes() == p2.tobytes() and (prims == pp).all()
+
+
+def test_host_builder_empty():
+    n2, prims, n4 = raycaster.build_host_bvh(np.zeros((0, 9), np.float32))
+    assert len(n2) == 0 and len(prims) == 0 and len(n4) == 0

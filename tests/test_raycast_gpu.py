@@ -1,0 +1,146 @@
+"""GPU ray casting against the reference BVH (through the C ABI).
+
+Closest-hit ids must equal the reference's, hit distances must be within 4
+FP32 ulps of the reference's double distance, and shadow-ray occlusion must
+agree, except for the rays tests/parity.py explains (edge band 1e-6, equal
+distance ties, blockers at the shadow ray's end).  Both BVH layouts (FP32
+and 8-bit quantised child boxes) are held to the same bar.
+"""
+import os
+
+import numpy as np
+import pytest
+
+import oracle
+from rise_b200 import raycaster, scenes
+
+from parity import any_report, closest_report
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+LAYOUTS = ["f32", "q8"]
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    c = raycaster.Context(0)
+    yield c
+    c.close()
+
+
+def make_caster(ctx, tri9, layout):
+    s = raycaster.Scene(ctx)
+    s.add_triangles(tri9)
+    s.commit(layout)
+    return s, raycaster.RayCaster(s)
+
+
+@pytest.mark.parametrize("layout", LAYOUTS)
+def test_golden_closest_and_any(ctx, layout):
+    g = np.load(os.path.join(GOLDEN, "bvh_soup_2k.npz"))
+    s, rc = make_caster(ctx, g["tri9"], layout)
+    hits = rc.cast_rays(g["rays"])
+    rep = closest_report(g["tri9"], g["rays"], hits, g["ids"], g["t"])
+    assert rep["bad"] == [] and rep["t_over"] == 0, rep
+    occ = rc.cast_shadow_rays(g["shadow_rays"])
+    arep = any_report(g["tri9"], g["shadow_rays"], occ, g["occluded"])
+    assert arep["bad"] == [], arep
+    s.close()
+
+
+@pytest.mark.parametrize("layout", LAYOUTS)
+@pytest.mark.parametrize("n_tri,n_rays", [(1, 1000), (5, 1000), (50000, 100000), (300000, 100000)])
+def test_random_soup_parity(ctx, layout, n_tri, n_rays):
+    tri = scenes.soup_triangles(n_tri, seed=n_tri + 1)
+    rays = scenes.sphere_rays(n_rays, seed=n_tri + 1)
+    srays = scenes.sphere_rays(n_rays, seed=n_tri + 2, shadow=True)
+    s, rc = make_caster(ctx, tri, layout)
+    ob = oracle.BVH(tri, "port")
+    ids, t = ob.closest(rays)
+    hits = rc.cast_rays(rays)
+    rep = closest_report(tri, rays, hits, ids, t)
+    assert rep["bad"] == [] and rep["t_over"] == 0, {k: rep[k] for k in ("bad", "t_over", "max_ulp")}
+    assert len(rep["excluded"]) <= max(2, n_rays // 1000)
+    occ = rc.cast_shadow_rays(srays)
+    arep = any_report(tri, srays, occ, ob.any(srays))
+    assert arep["bad"] == [], arep
+    s.close()
+
+
+@pytest.mark.parametrize("layout", LAYOUTS)
+def test_edge_cases(ctx, layout):
+    # One unit triangle in z = 0 plus a far one; axis-aligned rays with zero
+    # direction components, rays clipped by tmax / tmin, rays from behind.
+    tri = np.array([[0, 0, 0, 1, 0, 0, 0, 1, 0],
+                    [0, 0, 5, 1, 0, 5, 0, 1, 5]], np.float32)
+    s, rc = make_caster(ctx, tri, layout)
+    inf = np.inf
+    rays = np.array([
+        [0.25, 0.25, 1, 0, 0, 0, -1, inf],      # straight down: hit tri 0 at t=1
+        [0.25, 0.25, 1, 0, 0, 0, -1, 0.5],      # clipped by tmax
+        [0.25, 0.25, 1, 1.5, 0, 0, -1, inf],    # tmin past tri 0 -> nothing below
+        [0.25, 0.25, 10, 0, 0, 0, -1, inf],     # hits tri 1 (z=5) first at t=5
+        [0.75, 0.75, 1, 0, 0, 0, -1, inf],      # outside the hypotenuse: miss
+        [0.25, 0.25, -1, 0, 0, 0, 1, inf],      # from below: back face, t=1
+        [0.25, 0.25, 1, 0, 1, 0, 0, inf],       # parallel to the plane: miss
+        [-5, 0.25, 0.0, 0, 1, 0, 0, inf],       # in the plane: degenerate, miss
+    ], np.float32)
+    hits = rc.cast_rays(rays)
+    assert list(hits["prim"]) == [0, -1, -1, 1, -1, 0, -1, -1]
+    assert hits["t"][0] == 1.0 and hits["t"][3] == 5.0 and hits["t"][5] == 1.0
+    assert abs(hits["a"][0] - 0.25) < 1e-6 and abs(hits["b"][0] - 0.25) < 1e-6
+    sr = rays.copy()
+    sr[:, 7] = [2, 0.5, inf, 4.9, 2, 2, 2, 2]
+    occ = rc.cast_shadow_rays(sr)
+    assert list(occ) == [1, 0, 0, 0, 0, 1, 0, 0]
+    assert len(rc.cast_rays(np.zeros((0, 8), np.float32))) == 0
+    s.close()
+
+
+def test_layouts_agree_and_are_deterministic(ctx):
+    tri = scenes.soup_triangles(200000, seed=5)
+    rays = scenes.sphere_rays(500000, seed=5)
+    sf, rf = make_caster(ctx, tri, "f32")
+    sq, rq = make_caster(ctx, tri, "q8")
+    a = rf.cast_rays(rays)
+    b = rq.cast_rays(rays)
+    c = rf.cast_rays(rays)
+    assert (a["prim"] == c["prim"]).all() and (a["t"] == c["t"]).all()
+    assert (a["prim"] == b["prim"]).mean() > 0.99999
+    sf.close()
+    sq.close()
+
+
+def test_device_api_matches_host_api(ctx):
+    torch = pytest.importorskip("torch")
+    tri = scenes.soup_triangles(20000, seed=9)
+    rays = scenes.sphere_rays(65536, seed=9)
+    s, rc = make_caster(ctx, tri, "f32")
+    host = rc.cast_rays(rays)
+    d_rays = torch.from_numpy(rays).cuda()
+    d_hits = torch.empty((len(rays), 4), dtype=torch.float32, device="cuda")
+    rc.cast_rays_device(d_rays.data_ptr(), d_hits.data_ptr(), len(rays), torch.cuda.current_stream().cuda_stream)
+    torch.cuda.synchronize()
+    dev = d_hits.cpu().numpy().view(raycaster.HIT_DTYPE).reshape(-1)
+    assert (dev["prim"] == host["prim"]).all() and (dev["t"] == host["t"]).all()
+    s.close()
+
+
+@pytest.mark.parametrize("layout", LAYOUTS)
+def test_full_size_microbench_sample(ctx, layout):
+    """1,000,000 triangles, 4,194,304 rays (the microbenchmark's full size):
+    every ray is cast; a seeded sample of 20,000 is checked against the
+    oracle, and the whole batch for hit rate and determinism."""
+    tri = scenes.soup_triangles(1_000_000, seed=7)
+    rays = scenes.sphere_rays(4_194_304, seed=7)
+    s, rc = make_caster(ctx, tri, layout)
+    hits = rc.cast_rays(rays)
+    again = rc.cast_rays(rays)
+    assert (hits["prim"] == again["prim"]).all()
+    assert (hits["prim"] >= 0).mean() > 0.999
+    idx = np.random.default_rng(0).choice(len(rays), 20000, replace=False)
+    ids, t = oracle.BVH(tri, "port").closest(rays[idx])
+    rep = closest_report(tri, rays[idx], hits[idx], ids, t)
+    assert rep["bad"] == [] and rep["t_over"] == 0, {k: rep[k] for k in ("bad", "t_over", "max_ulp")}
+    s.close()
