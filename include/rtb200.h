@@ -122,8 +122,9 @@ int rtb200_bvh_host_destroy(rtb200_bvh_host* h);
 int rtb200_cast_closest(rtb200_scene* scene, const rtb200_ray* rays, int64_t n, rtb200_hit* hits);
 int rtb200_cast_any(rtb200_scene* scene, const rtb200_ray* rays, int64_t n, uint8_t* occluded);
 
-/* Device buffers (device pointers), asynchronous on `stream` (a
- * cudaStream_t; NULL = the context's stream).  The caller synchronises. */
+/* Device buffers (device pointers), asynchronous on `stream`, a
+ * cudaStream_t taken as is (NULL is the CUDA default stream, as everywhere
+ * in CUDA).  The caller synchronises. */
 int rtb200_cast_closest_device(rtb200_scene* scene, const rtb200_ray* d_rays, int64_t n,
                                rtb200_hit* d_hits, void* stream);
 int rtb200_cast_any_device(rtb200_scene* scene, const rtb200_ray* d_rays, int64_t n,

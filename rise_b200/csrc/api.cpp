@@ -301,7 +301,7 @@ int rtb200_cast_closest_device(rtb200_scene* s, const rtb200_ray* d_rays, int64_
     if (n < 0 || (n > 0 && (!d_rays || !d_hits))) return SetError(ctx, RTB200_E_INVALID, "bad ray buffers");
     if (!Aligned16(d_rays) || !Aligned16(d_hits)) return SetError(ctx, RTB200_E_INVALID, "ray/hit buffers must be 16-byte aligned");
     cudaSetDevice(ctx->device);
-    return CudaCheck(ctx, LaunchCastClosest(s, d_rays, n, d_hits, stream ? (cudaStream_t)stream : ctx->stream),
+    return CudaCheck(ctx, LaunchCastClosest(s, d_rays, n, d_hits, (cudaStream_t)stream),
                      "closest-hit launch");
 }
 
@@ -314,7 +314,7 @@ int rtb200_cast_any_device(rtb200_scene* s, const rtb200_ray* d_rays, int64_t n,
     if (n < 0 || (n > 0 && (!d_rays || !d_occ))) return SetError(ctx, RTB200_E_INVALID, "bad ray buffers");
     if (!Aligned16(d_rays)) return SetError(ctx, RTB200_E_INVALID, "ray buffer must be 16-byte aligned");
     cudaSetDevice(ctx->device);
-    return CudaCheck(ctx, LaunchCastAny(s, d_rays, n, d_occ, stream ? (cudaStream_t)stream : ctx->stream),
+    return CudaCheck(ctx, LaunchCastAny(s, d_rays, n, d_occ, (cudaStream_t)stream),
                      "any-hit launch");
 }
 

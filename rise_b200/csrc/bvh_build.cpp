@@ -404,7 +404,7 @@ void EncodeGpuNodes(const BuiltBVH& b, std::vector<GpuNode4>& out)
             const bool valid = i < s.nchild;
             d.lox[i] = s.minx[i]; d.loy[i] = s.miny[i]; d.loz[i] = s.minz[i];
             d.hix[i] = s.maxx[i]; d.hiy[i] = s.maxy[i]; d.hiz[i] = s.maxz[i];
-            d.child[i] = valid ? s.child[i] : 0;
+            d.child[i] = !valid ? 0 : (s.count[i] > 0 ? ~s.child[i] : s.child[i]);
             d.count[i] = valid ? (int32_t)s.count[i] : -1;
         }
     }
@@ -451,7 +451,7 @@ void EncodeQuantNodes(const BuiltBVH& b, std::vector<QNode4>& out)
         d.ex = (int8_t)ex[0]; d.ey = (int8_t)ex[1]; d.ez = (int8_t)ex[2];
         for (int i = 0; i < 4; ++i) {
             const bool valid = i < s.nchild;
-            d.child[i] = valid ? s.child[i] : 0;
+            d.child[i] = !valid ? 0 : (s.count[i] > 0 ? ~s.child[i] : s.child[i]);
             d.count[i] = valid ? (int16_t)std::min<int>(s.count[i], 32767) : (int16_t)-1;
             for (int k = 0; k < 3; ++k) {
                 if (!valid) { d.qlo[k][i] = 255; d.qhi[k][i] = 0; continue; }
@@ -481,6 +481,11 @@ void EncodeTriangles(const float* tri9, const BuiltBVH& b, std::vector<GpuTri>& 
         t.v1[3] = 0.0f;
         t.v2[3] = 0.0f;
     }
+    // Mark the last triangle of every leaf (v1.w = 1) so the traversal can
+    // walk a leaf from its first slot without a separate count.
+    for (const Node4& n : b.nodes4)
+        for (int i = 0; i < n.nchild; ++i)
+            if (n.count[i] > 0) out[(size_t)n.child[i] + n.count[i] - 1].v1[3] = 1.0f;
 }
 
 }  // namespace rtb200

@@ -1,76 +1,62 @@
 // raycast.cu -- batched closest-hit and any-hit kernels for sm_100a.
 //
-// Persistent kernels: one grid of (SMs x resident blocks); each warp takes
-// 32 rays at a time from a per-scene work counter in global memory, so warps
-// whose rays finish early pick up more work instead of idling while the
-// slowest rays of a static partition finish.  Rays are read as two 16-byte
-// vector loads and hits written as one 16-byte store.
+// Persistent kernels: one grid of (SMs x resident blocks).  Each warp runs the
+// while-while traversal of raycast.cuh; lanes refill themselves with new rays
+// from a warp-local chunk as soon as their ray finishes, so SIMT lanes stay
+// busy on the long tail of incoherent rays.  Rays are read as two 16-byte
+// vector loads and hits written as one 16-byte store; the traversal stack
+// lives in shared memory ([depth][thread], conflict-free).
 #include "core.h"
 #include "raycast.cuh"
 
 namespace rtb200 {
 
-constexpr int kCastBlock = 256;
-
-template <class NodeT>
-__global__ void __launch_bounds__(kCastBlock)
-KCastClosest(const NodeT* __restrict__ nodes, const GpuTri* __restrict__ tris,
-             const rtb200_ray* __restrict__ rays, int64_t n, rtb200_hit* __restrict__ hits,
-             unsigned long long* counter, unsigned* err)
+__device__ __forceinline__ Ray LoadRay(const rtb200_ray* rays, long long i)
 {
-    const int lane = threadIdx.x & 31;
-    for (;;) {
-        unsigned long long base = 0;
-        if (lane == 0) base = atomicAdd(counter, 32ull);
-        base = __shfl_sync(0xffffffffu, base, 0);
-        if (base >= (unsigned long long)n) return;
-        const int64_t i = (int64_t)base + lane;
-        if (i < n) {
-            const float4 a = ldg4(rays + i);
-            const float4 b = ldg4(reinterpret_cast<const float*>(rays + i) + 4);
-            Ray r;
-            r.o[0] = a.x; r.o[1] = a.y; r.o[2] = a.z; r.tmin = a.w;
-            r.d[0] = b.x; r.d[1] = b.y; r.d[2] = b.z; r.tmax = b.w;
-            const HitRecord h = TraceClosest<NodeT>(nodes, tris, r, err);
-            float4 out;
-            if (h.prim >= 0) {
-                const float* tb = reinterpret_cast<const float*>(tris + h.prim);
-                const float4 A = ldg4(tb), B = ldg4(tb + 4), C = ldg4(tb + 8);
-                out.x = (float)RefineT(r.o, r.d, A, B, C);
-                out.y = A.w;  // input triangle index (bit pattern)
-                out.z = h.a;
-                out.w = h.b;
-            } else {
-                out.x = -1.0f;
-                out.y = __int_as_float(-1);
-                out.z = 0.0f;
-                out.w = 0.0f;
-            }
-            *reinterpret_cast<float4*>(hits + i) = out;
-        }
-    }
+    const float4 a = ldg4(rays + i);
+    const float4 b = ldg4(reinterpret_cast<const float*>(rays + i) + 4);
+    Ray r;
+    r.o[0] = a.x; r.o[1] = a.y; r.o[2] = a.z; r.tmin = a.w;
+    r.d[0] = b.x; r.d[1] = b.y; r.d[2] = b.z; r.tmax = b.w;
+    return r;
 }
 
-template <class NodeT>
-__global__ void __launch_bounds__(kCastBlock)
-KCastAny(const NodeT* __restrict__ nodes, const GpuTri* __restrict__ tris,
-         const rtb200_ray* __restrict__ rays, int64_t n, uint8_t* __restrict__ occ,
-         unsigned long long* counter, unsigned* err)
+template <class NodeT, bool ANY>
+__global__ void __launch_bounds__(kTraceBlock, 8)
+KTrace(const NodeT* __restrict__ nodes, const GpuTri* __restrict__ tris,
+       const rtb200_ray* __restrict__ rays, long long n, int ntri, rtb200_hit* __restrict__ hits,
+       uint8_t* __restrict__ occ, unsigned long long* counter, unsigned* err)
 {
-    const int lane = threadIdx.x & 31;
+    __shared__ int sstack[kTraceStack * kTraceBlock];
+    int* stk = sstack + threadIdx.x;
+    WarpFeed feed{0ull, 0ull, false};
+    TraceState s;
+    long long ray = -1;
     for (;;) {
-        unsigned long long base = 0;
-        if (lane == 0) base = atomicAdd(counter, 32ull);
-        base = __shfl_sync(0xffffffffu, base, 0);
-        if (base >= (unsigned long long)n) return;
-        const int64_t i = (int64_t)base + lane;
-        if (i < n) {
-            const float4 a = ldg4(rays + i);
-            const float4 b = ldg4(reinterpret_cast<const float*>(rays + i) + 4);
-            Ray r;
-            r.o[0] = a.x; r.o[1] = a.y; r.o[2] = a.z; r.tmin = a.w;
-            r.d[0] = b.x; r.d[1] = b.y; r.d[2] = b.z; r.tmax = b.w;
-            occ[i] = TraceAny<NodeT>(nodes, tris, r, err) ? 1 : 0;
+        const long long got = FeedTake(feed, ray < 0, (unsigned long long)n, counter);
+        if (got >= 0) {
+            ray = got;
+            StartRay(s, LoadRay(rays, ray));
+        }
+        if (__all_sync(kFull, ray < 0)) break;
+        if (ray >= 0 && TraceRound<NodeT, ANY>(s, nodes, tris, ntri, stk, err)) {
+            if (ANY) {
+                occ[ray] = s.bestSlot >= 0 ? 1 : 0;
+            } else {
+                float4 out;
+                if (s.bestSlot >= 0) {
+                    const float* tb = reinterpret_cast<const float*>(tris + s.bestSlot);
+                    const float4 A = ldg4(tb), B = ldg4(tb + 4), C = ldg4(tb + 8);
+                    out.x = (float)RefineT(s.p.o, s.d, A, B, C);
+                    out.y = A.w;  // input triangle index (bit pattern)
+                    out.z = s.ba;
+                    out.w = s.bb;
+                } else {
+                    out = make_float4(-1.0f, __int_as_float(-1), 0.0f, 0.0f);
+                }
+                *reinterpret_cast<float4*>(hits + ray) = out;
+            }
+            ray = -1;
         }
     }
 }
@@ -81,9 +67,23 @@ template <class K>
 int GridFor(K kernel, int num_sms)
 {
     int per_sm = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kCastBlock, 0) != cudaSuccess || per_sm < 1)
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kTraceBlock, 0) != cudaSuccess || per_sm < 1)
         per_sm = 1;
     return per_sm * num_sms;
+}
+
+template <class NodeT, bool ANY>
+cudaError_t LaunchTrace(const rtb200_scene* s, const rtb200_ray* d_rays, int64_t n, rtb200_hit* hits,
+                        uint8_t* occ, cudaStream_t stream)
+{
+    if (n <= 0) return cudaSuccess;
+    cudaError_t e = cudaMemsetAsync(s->d_counter, 0, sizeof(unsigned long long), stream);
+    if (e != cudaSuccess) return e;
+    static int grid = 0;
+    if (!grid) grid = GridFor(KTrace<NodeT, ANY>, s->ctx->num_sms);
+    KTrace<NodeT, ANY><<<grid, kTraceBlock, 0, stream>>>((const NodeT*)s->d_nodes, s->d_tris, d_rays, n,
+                                                         (int)s->tri_material.size(), hits, occ, s->d_counter, s->d_err);
+    return cudaGetLastError();
 }
 
 }  // namespace
@@ -91,41 +91,15 @@ int GridFor(K kernel, int num_sms)
 cudaError_t LaunchCastClosest(const rtb200_scene* s, const rtb200_ray* d_rays, int64_t n,
                               rtb200_hit* d_hits, cudaStream_t stream)
 {
-    if (n <= 0) return cudaSuccess;
-    cudaError_t e = cudaMemsetAsync(s->d_counter, 0, sizeof(unsigned long long), stream);
-    if (e != cudaSuccess) return e;
-    if (s->layout == RTB200_BVH_Q8) {
-        static int grid = 0;
-        if (!grid) grid = GridFor(KCastClosest<QNode4>, s->ctx->num_sms);
-        KCastClosest<QNode4><<<grid, kCastBlock, 0, stream>>>((const QNode4*)s->d_nodes, s->d_tris, d_rays, n,
-                                                              d_hits, s->d_counter, s->d_err);
-    } else {
-        static int grid = 0;
-        if (!grid) grid = GridFor(KCastClosest<GpuNode4>, s->ctx->num_sms);
-        KCastClosest<GpuNode4><<<grid, kCastBlock, 0, stream>>>((const GpuNode4*)s->d_nodes, s->d_tris, d_rays,
-                                                                n, d_hits, s->d_counter, s->d_err);
-    }
-    return cudaGetLastError();
+    if (s->layout == RTB200_BVH_Q8) return LaunchTrace<QNode4, false>(s, d_rays, n, d_hits, nullptr, stream);
+    return LaunchTrace<GpuNode4, false>(s, d_rays, n, d_hits, nullptr, stream);
 }
 
 cudaError_t LaunchCastAny(const rtb200_scene* s, const rtb200_ray* d_rays, int64_t n,
                           uint8_t* d_occ, cudaStream_t stream)
 {
-    if (n <= 0) return cudaSuccess;
-    cudaError_t e = cudaMemsetAsync(s->d_counter, 0, sizeof(unsigned long long), stream);
-    if (e != cudaSuccess) return e;
-    if (s->layout == RTB200_BVH_Q8) {
-        static int grid = 0;
-        if (!grid) grid = GridFor(KCastAny<QNode4>, s->ctx->num_sms);
-        KCastAny<QNode4><<<grid, kCastBlock, 0, stream>>>((const QNode4*)s->d_nodes, s->d_tris, d_rays, n, d_occ,
-                                                          s->d_counter, s->d_err);
-    } else {
-        static int grid = 0;
-        if (!grid) grid = GridFor(KCastAny<GpuNode4>, s->ctx->num_sms);
-        KCastAny<GpuNode4><<<grid, kCastBlock, 0, stream>>>((const GpuNode4*)s->d_nodes, s->d_tris, d_rays, n,
-                                                            d_occ, s->d_counter, s->d_err);
-    }
-    return cudaGetLastError();
+    if (s->layout == RTB200_BVH_Q8) return LaunchTrace<QNode4, true>(s, d_rays, n, nullptr, d_occ, stream);
+    return LaunchTrace<GpuNode4, true>(s, d_rays, n, nullptr, d_occ, stream);
 }
 
 }  // namespace rtb200

@@ -2,14 +2,17 @@
 //
 // Shared by the batch ray-cast kernels (raycast.cu) and the wavefront path
 // tracer (pathtrace.cu).  The traversal replaces the reference's single-ray
-// BVH4 walk (src/Library/Acceleration/BVH.h:1304-1471) with a per-thread
-// stack walk over the same collapsed tree, and the reference's
-// double-precision Moller-Trumbore leaf test
-// (src/Library/Intersection/RayTriangleIntersection.cpp:21-68) with the FP32
-// watertight test of Woop, Benthin and Wald (JCGT 2(1), 2013).  The closest hit
-// is re-measured in FP64 with the reference's formula, so the reported distance
-// is the reference's distance rounded once to FP32.
+// BVH4 walk (src/Library/Acceleration/BVH.h:1304-1471) over the same
+// collapsed tree with a warp-cooperative "while-while" walk: lanes first
+// descend internal nodes until every lane holds a postponed leaf, then test
+// leaves together, and a lane whose ray is finished takes the next ray from a
+// warp-local chunk of the batch.  The reference's double-precision
+// Moller-Trumbore leaf test (src/Library/Intersection/RayTriangleIntersection.cpp:21-68)
+// becomes the FP32 watertight test of Woop, Benthin and Wald (JCGT 2(1), 2013);
+// the closest hit is re-measured in FP64 with the reference's formula, so the
+// reported distance is the reference's distance rounded once to FP32.
 #pragma once
+#include <climits>
 #include <cstdint>
 #include <cuda_runtime.h>
 
@@ -17,8 +20,11 @@
 
 namespace rtb200 {
 
-constexpr int kStackSize = 96;
 constexpr unsigned kErrStackOverflow = 1u;
+constexpr int kEmpty = INT_MIN;      // no node / no leaf
+constexpr int kTraceBlock = 128;     // threads per block of the trace kernels
+constexpr int kTraceStack = 64;      // stack entries per thread (shared memory)
+constexpr unsigned kFull = 0xffffffffu;
 
 struct Ray {
     float o[3];
@@ -45,7 +51,7 @@ __device__ __forceinline__ void Prepare(const Ray& r, RayPre& p)
 {
     for (int k = 0; k < 3; ++k) {
         p.o[k] = r.o[k];
-        // Zero components map to +-FLT_MAX like the reference (BVH.h:1221-1224).
+        // Zero components map to FLT_MAX like the reference (BVH.h:1221-1224).
         p.inv[k] = (r.d[k] == 0.0f) ? 3.402823466e+38f : __frcp_rn(r.d[k]);
     }
     p.tmin = r.tmin;
@@ -117,21 +123,22 @@ __device__ __forceinline__ double RefineT(const float* o, const float* d, const 
 
 struct ChildHits {
     float t[4];
+    int c[4];
     unsigned mask;
 };
 
 // FP32 node: the reference slab arithmetic (BVH.h:738-763) per child.
-__device__ __forceinline__ void SlabF32(const GpuNode4* nodes, int ni, const RayPre& p, float best,
-                                        ChildHits& h, int4& child, int4& count)
+__device__ __forceinline__ void SlabF32(const GpuNode4* nodes, int ni, const RayPre& p, float best, ChildHits& h)
 {
     const float* base = reinterpret_cast<const float*>(nodes + ni);
     const float4 lx = ldg4(base + 0), ly = ldg4(base + 4), lz = ldg4(base + 8);
     const float4 hx = ldg4(base + 12), hy = ldg4(base + 16), hz = ldg4(base + 20);
-    child = ldg4i(base + 24);
-    count = ldg4i(base + 28);
+    const int4 child = ldg4i(base + 24);
+    const int4 count = ldg4i(base + 28);
     const float lxa[4] = {lx.x, lx.y, lx.z, lx.w}, lya[4] = {ly.x, ly.y, ly.z, ly.w}, lza[4] = {lz.x, lz.y, lz.z, lz.w};
     const float hxa[4] = {hx.x, hx.y, hx.z, hx.w}, hya[4] = {hy.x, hy.y, hy.z, hy.w}, hza[4] = {hz.x, hz.y, hz.z, hz.w};
     const int cnt[4] = {count.x, count.y, count.z, count.w};
+    h.c[0] = child.x; h.c[1] = child.y; h.c[2] = child.z; h.c[3] = child.w;
     h.mask = 0;
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
@@ -148,8 +155,7 @@ __device__ __forceinline__ void SlabF32(const GpuNode4* nodes, int ni, const Ray
 }
 
 // Quantised node: child slabs from 8-bit bounds, t = q * (2^e / d) + (origin - o) / d.
-__device__ __forceinline__ void SlabQ8(const QNode4* nodes, int ni, const RayPre& p, float best,
-                                       ChildHits& h, int4& child, int4& count)
+__device__ __forceinline__ void SlabQ8(const QNode4* nodes, int ni, const RayPre& p, float best, ChildHits& h)
 {
     const int4* base = reinterpret_cast<const int4*>(nodes + ni);
     const int4 w0 = __ldg(base + 0), w1 = __ldg(base + 1), w2 = __ldg(base + 2), w3 = __ldg(base + 3);
@@ -158,16 +164,15 @@ __device__ __forceinline__ void SlabQ8(const QNode4* nodes, int ni, const RayPre
     const int e[3] = {(int)(int8_t)(meta & 0xff), (int)(int8_t)((meta >> 8) & 0xff), (int)(int8_t)((meta >> 16) & 0xff)};
     const unsigned qlo[3] = {(unsigned)w1.x, (unsigned)w1.y, (unsigned)w1.z};
     const unsigned qhi[3] = {(unsigned)w1.w, (unsigned)w2.x, (unsigned)w2.y};
-    child = make_int4(w2.z, w2.w, w3.x, w3.y);
-    count = make_int4((int)(int16_t)(w3.z & 0xffff), (int)(int16_t)((unsigned)w3.z >> 16),
-                      (int)(int16_t)(w3.w & 0xffff), (int)(int16_t)((unsigned)w3.w >> 16));
+    h.c[0] = w2.z; h.c[1] = w2.w; h.c[2] = w3.x; h.c[3] = w3.y;
+    const int cnt[4] = {(int)(int16_t)(w3.z & 0xffff), (int)(int16_t)((unsigned)w3.z >> 16),
+                        (int)(int16_t)(w3.w & 0xffff), (int)(int16_t)((unsigned)w3.w >> 16)};
     float a[3], s[3];
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
         a[k] = (org[k] - p.o[k]) * p.inv[k];
         s[k] = __int_as_float((e[k] + 127) << 23) * p.inv[k];
     }
-    const int cnt[4] = {count.x, count.y, count.z, count.w};
     h.mask = 0;
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
@@ -181,8 +186,8 @@ __device__ __forceinline__ void SlabQ8(const QNode4* nodes, int ni, const RayPre
             tl[k] = fminf(t1, t2);
             th[k] = fmaxf(t1, t2);
         }
-        float tn = fmaxf(fmaxf(fmaxf(tl[0], tl[1]), tl[2]), p.tmin);
-        float tf = fminf(fminf(fminf(th[0], th[1]), th[2]), best);
+        const float tn = fmaxf(fmaxf(fmaxf(tl[0], tl[1]), tl[2]), p.tmin);
+        const float tf = fminf(fminf(fminf(th[0], th[1]), th[2]), best);
         h.t[i] = tn;
         if (tn <= tf && cnt[i] >= 0) h.mask |= 1u << i;
     }
@@ -192,145 +197,180 @@ template <class NodeT>
 struct Slab;
 template <>
 struct Slab<GpuNode4> {
-    __device__ __forceinline__ static void Run(const GpuNode4* n, int i, const RayPre& p, float b, ChildHits& h, int4& c, int4& k)
+    __device__ __forceinline__ static void Run(const GpuNode4* n, int i, const RayPre& p, float b, ChildHits& h)
     {
-        SlabF32(n, i, p, b, h, c, k);
+        SlabF32(n, i, p, b, h);
     }
 };
 template <>
 struct Slab<QNode4> {
-    __device__ __forceinline__ static void Run(const QNode4* n, int i, const RayPre& p, float b, ChildHits& h, int4& c, int4& k)
+    __device__ __forceinline__ static void Run(const QNode4* n, int i, const RayPre& p, float b, ChildHits& h)
     {
-        SlabQ8(n, i, p, b, h, c, k);
+        SlabQ8(n, i, p, b, h);
     }
 };
 
-__device__ __forceinline__ int Sel(const int4& v, int i) { return i == 0 ? v.x : (i == 1 ? v.y : (i == 2 ? v.z : v.w)); }
-
-struct HitRecord {
-    float t;
-    int prim;     // leaf-order triangle slot, -1 = miss
-    float a, b;
-};
-
-// Closest hit.  Returns the leaf-order slot of the closest triangle.
-template <class NodeT>
-__device__ __forceinline__ HitRecord TraceClosest(const NodeT* __restrict__ nodes, const GpuTri* __restrict__ tris,
-                                                  const Ray& r, unsigned* err)
+__device__ __forceinline__ void CSwap(float& ta, int& ca, float& tb, int& cb)
 {
-    RayPre p;
-    Prepare(r, p);
-    HitRecord hit;
-    hit.t = r.tmax;
-    hit.prim = -1;
-    hit.a = hit.b = 0.0f;
-    int stack[kStackSize];
-    int sp = 0;
-    int node = 0;
-    for (;;) {
-        ChildHits h;
-        int4 child, count;
-        Slab<NodeT>::Run(nodes, node, p, hit.t, h, child, count);
-        // Leaves first, in slot order.
-        unsigned inner = 0;
-        unsigned m = h.mask;
-        while (m) {
-            const int i = __ffs(m) - 1;
-            m &= m - 1;
-            const int c = Sel(count, i);
-            if (c > 0) {
-                const int first = Sel(child, i);
-                for (int s = first; s < first + c; ++s) {
-                    const float* tb = reinterpret_cast<const float*>(tris + s);
-                    const float4 A = ldg4(tb), B = ldg4(tb + 4), C = ldg4(tb + 8);
-                    float t, a, b;
-                    if (Watertight(p, A, B, C, hit.t, t, a, b)) {
-                        hit.t = t; hit.prim = s; hit.a = a; hit.b = b;
-                    }
-                }
-            } else {
-                inner |= 1u << i;
-            }
-        }
-        // Internal children: continue with the nearest, push the rest far-first.
-        int next = -1;
-        if (inner) {
-            int ord[4];
-            float key[4];
-            int n = 0;
-            while (inner) {
-                const int i = __ffs(inner) - 1;
-                inner &= inner - 1;
-                ord[n] = Sel(child, i);
-                key[n] = h.t[i];
-                ++n;
-            }
-            // Sort descending by entry distance (n <= 4).
-            for (int x = 1; x < n; ++x) {
-                const float kk = key[x];
-                const int oo = ord[x];
-                int y = x - 1;
-                while (y >= 0 && key[y] < kk) { key[y + 1] = key[y]; ord[y + 1] = ord[y]; --y; }
-                key[y + 1] = kk;
-                ord[y + 1] = oo;
-            }
-            for (int x = 0; x < n - 1; ++x) {
-                if (sp < kStackSize) stack[sp++] = ord[x];
-                else atomicOr(err, kErrStackOverflow);
-            }
-            next = ord[n - 1];
-        }
-        if (next < 0) {
-            if (sp == 0) break;
-            next = stack[--sp];
-        }
-        node = next;
-    }
-    return hit;
+    // After the call (ta, ca) holds the nearer entry.
+    const bool sw = tb < ta;
+    const float t = sw ? tb : ta;
+    const int c = sw ? cb : ca;
+    tb = sw ? ta : tb;
+    cb = sw ? ca : cb;
+    ta = t;
+    ca = c;
 }
 
-// Any hit within (tmin, tmax): returns true at the first accepted triangle.
-template <class NodeT>
-__device__ __forceinline__ bool TraceAny(const NodeT* __restrict__ nodes, const GpuTri* __restrict__ tris,
-                                         const Ray& r, unsigned* err)
-{
+// Per-lane traversal state of one ray.
+struct TraceState {
     RayPre p;
-    Prepare(r, p);
-    int stack[kStackSize];
-    int sp = 0;
-    int node = 0;
-    for (;;) {
+    float d[3];        // direction (for the FP64 distance refinement)
+    float best;        // current tmax
+    int bestSlot;      // leaf-order triangle slot of the closest hit
+    float ba, bb;      // its barycentrics
+    int node;          // next internal node, a leaf entry (~first), or kEmpty
+    int leaf;          // postponed leaf entry (~first) or kEmpty
+    int sp;            // stack depth
+};
+
+__device__ __forceinline__ void StartRay(TraceState& s, const Ray& r)
+{
+    Prepare(r, s.p);
+    s.d[0] = r.d[0]; s.d[1] = r.d[1]; s.d[2] = r.d[2];
+    s.best = r.tmax;
+    s.bestSlot = -1;
+    s.ba = s.bb = 0.0f;
+    s.node = 0;
+    s.leaf = kEmpty;
+    s.sp = 0;
+}
+
+__device__ __forceinline__ void Push(TraceState& s, int* stk, int v, unsigned* err)
+{
+    if (s.sp < kTraceStack) { stk[s.sp * kTraceBlock] = v; ++s.sp; }
+    else atomicOr(err, kErrStackOverflow);
+}
+
+__device__ __forceinline__ int Pop(TraceState& s, const int* stk)
+{
+    if (s.sp == 0) return kEmpty;
+    --s.sp;
+    return stk[s.sp * kTraceBlock];
+}
+
+// One round of while-while traversal for every active lane: descend internal
+// nodes until all active lanes hold a postponed leaf (or have run out of
+// nodes), then test postponed leaves.  ANY: stop at the first accepted hit.
+// Returns true when this lane's ray is finished.
+template <class NodeT, bool ANY>
+__device__ __forceinline__ bool TraceRound(TraceState& s, const NodeT* __restrict__ nodes,
+                                           const GpuTri* __restrict__ tris, int ntri, int* stk, unsigned* err)
+{
+    // Descend internal nodes.
+    while (s.node >= 0) {
         ChildHits h;
-        int4 child, count;
-        Slab<NodeT>::Run(nodes, node, p, r.tmax, h, child, count);
-        int next = -1;
-        unsigned m = h.mask;
-        while (m) {
-            const int i = __ffs(m) - 1;
-            m &= m - 1;
-            const int c = Sel(count, i);
-            const int first = Sel(child, i);
-            if (c > 0) {
-                for (int s = first; s < first + c; ++s) {
-                    const float* tb = reinterpret_cast<const float*>(tris + s);
-                    const float4 A = ldg4(tb), B = ldg4(tb + 4), C = ldg4(tb + 8);
-                    float t, a, b;
-                    if (Watertight(p, A, B, C, r.tmax, t, a, b)) return true;
-                }
-            } else if (next < 0) {
-                next = first;
-            } else if (sp < kStackSize) {
-                stack[sp++] = first;
-            } else {
-                atomicOr(err, kErrStackOverflow);
-            }
+        Slab<NodeT>::Run(nodes, s.node, s.p, s.best, h);
+        // Nearest-first ordering of the (up to 4) hit children.
+        float t0 = (h.mask & 1u) ? h.t[0] : __int_as_float(0x7f800000);
+        float t1 = (h.mask & 2u) ? h.t[1] : __int_as_float(0x7f800000);
+        float t2 = (h.mask & 4u) ? h.t[2] : __int_as_float(0x7f800000);
+        float t3 = (h.mask & 8u) ? h.t[3] : __int_as_float(0x7f800000);
+        int c0 = (h.mask & 1u) ? h.c[0] : kEmpty;
+        int c1 = (h.mask & 2u) ? h.c[1] : kEmpty;
+        int c2 = (h.mask & 4u) ? h.c[2] : kEmpty;
+        int c3 = (h.mask & 8u) ? h.c[3] : kEmpty;
+        CSwap(t0, c0, t1, c1);
+        CSwap(t2, c2, t3, c3);
+        CSwap(t0, c0, t2, c2);
+        CSwap(t1, c1, t3, c3);
+        CSwap(t1, c1, t2, c2);
+        // Push far to near; the nearest becomes the next node.
+        if (c3 != kEmpty) Push(s, stk, c3, err);
+        if (c2 != kEmpty) Push(s, stk, c2, err);
+        if (c1 != kEmpty) Push(s, stk, c1, err);
+        s.node = (c0 != kEmpty) ? c0 : Pop(s, stk);
+        // Postpone the first leaf met; keep descending until all lanes have one.
+        if (s.node < 0 && s.node != kEmpty && s.leaf == kEmpty) {
+            s.leaf = s.node;
+            s.node = Pop(s, stk);
         }
-        if (next < 0) {
-            if (sp == 0) return false;
-            next = stack[--sp];
-        }
-        node = next;
+        if (!__any_sync(__activemask(), s.leaf == kEmpty)) break;
     }
+    // Test leaves.
+    while (s.leaf != kEmpty) {
+        int slot = ~s.leaf;
+        for (;;) {
+            const float* tb = reinterpret_cast<const float*>(tris + slot);
+            const float4 A = ldg4(tb), B = ldg4(tb + 4), C = ldg4(tb + 8);
+            float t, a, b;
+            if (Watertight(s.p, A, B, C, s.best, t, a, b)) {
+                if (ANY) {
+                    s.bestSlot = slot;
+                    s.node = kEmpty;
+                    s.leaf = kEmpty;
+                    return true;
+                }
+                s.best = t;
+                s.bestSlot = slot;
+                s.ba = a;
+                s.bb = b;
+            }
+            // The last triangle of a leaf carries v1.w = 1; the array bound
+            // is a second stop so a leaf walk never leaves the buffer.
+            if (B.w != 0.0f || slot + 1 >= ntri) break;
+            ++slot;
+        }
+        s.leaf = kEmpty;
+        if (s.node < 0 && s.node != kEmpty) {
+            s.leaf = s.node;
+            s.node = Pop(s, stk);
+        }
+    }
+    return s.node == kEmpty;
+}
+
+// Warp-cooperative ray supply: a lane whose ray is finished takes the next
+// index from a warp-local chunk; the chunk is refilled from the global
+// counter kChunk rays at a time (one atomic per chunk per warp).
+struct WarpFeed {
+    unsigned long long next, end;
+    bool exhausted;
+};
+
+constexpr unsigned kChunk = 128;
+
+// Returns this lane's new ray index or -1.  `want` lanes ask for work.
+__device__ __forceinline__ long long FeedTake(WarpFeed& f, bool want, unsigned long long n,
+                                              unsigned long long* counter)
+{
+    const unsigned lane = threadIdx.x & 31u;
+    const unsigned wm = __ballot_sync(kFull, want);
+    if (!wm) return -1;
+    const unsigned need = __popc(wm);
+    const unsigned rank = __popc(wm & ((1u << lane) - 1u));
+    unsigned long long avail = f.end - f.next;
+    long long mine = -1;
+    if (rank < avail) mine = (long long)(f.next + rank);
+    if (avail < need && !f.exhausted) {
+        unsigned long long base = 0;
+        if (lane == 0) base = atomicAdd(counter, (unsigned long long)kChunk);
+        base = __shfl_sync(kFull, base, 0);
+        if (base >= n) {
+            f.exhausted = true;
+            f.next = f.end;
+        } else {
+            const unsigned long long end = (base + kChunk < n) ? base + kChunk : n;
+            const unsigned long long extra = need - avail;
+            if (rank >= avail && base + (rank - avail) < end) mine = (long long)(base + (rank - avail));
+            f.next = (base + extra < end) ? base + extra : end;
+            f.end = end;
+            if (end == n) f.exhausted = true;
+        }
+    } else {
+        f.next += (avail < need) ? avail : need;
+    }
+    return want ? mine : -1;
 }
 
 }  // namespace rtb200
