@@ -130,6 +130,25 @@ int rtb200_cast_closest_device(rtb200_scene* scene, const rtb200_ray* d_rays, in
 int rtb200_cast_any_device(rtb200_scene* scene, const rtb200_ray* d_rays, int64_t n,
                            uint8_t* d_occluded, void* stream);
 
+/* Closest hit that allocates no device memory (no counterpart in the
+ * reference: the reference renderer allocates on the host and never on a
+ * GPU).  For callers that must not call cudaMalloc/cudaFree when they cast
+ * rays -- e.g. a host application whose pool allocator owns all device
+ * memory, or a latency-critical thread that cannot afford the device-wide
+ * synchronisation cudaMalloc/cudaFree may cause.  Same kernel and results as
+ * rtb200_cast_closest_device; the kernel's scratch (work counter, error
+ * word) lives in a static RTB200_NOALLOC_SCRATCH_BYTES-byte device array,
+ * one per GPU, held until the process exits.  The first call on a device
+ * looks up that array's address (no allocation); make that first call
+ * before any stream capture.  Every call shares the array and clears it on
+ * its stream first, so calls whose work overlaps on the GPU race on it and
+ * must be serialised by the caller.  At most RTB200_NOALLOC_MAX_RAYS rays per
+ * call; larger n is rejected with RTB200_E_INVALID. */
+#define RTB200_NOALLOC_SCRATCH_BYTES 256
+#define RTB200_NOALLOC_MAX_RAYS 2147483647LL
+int rtb200_cast_closest_noalloc(rtb200_scene* scene, const rtb200_ray* d_rays, int64_t n,
+                                rtb200_hit* d_hits, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -42,7 +42,10 @@ SIGNATURES = {
     "rtb200_cast_any": (ctypes.c_int, [_vp, _vp, _i64, _vp]),
     "rtb200_cast_closest_device": (ctypes.c_int, [_vp, _vp, _i64, _vp, _vp]),
     "rtb200_cast_any_device": (ctypes.c_int, [_vp, _vp, _i64, _vp, _vp]),
+    "rtb200_cast_closest_noalloc": (ctypes.c_int, [_vp, _vp, _i64, _vp, _vp]),
 }
+NOALLOC_SCRATCH_BYTES = 256
+NOALLOC_MAX_RAYS = 2147483647
 
 _lib = None
 

@@ -58,5 +58,10 @@ cudaError_t LaunchCastClosest(const rtb200_scene* s, const rtb200_ray* d_rays, i
                               rtb200_hit* d_hits, cudaStream_t stream);
 cudaError_t LaunchCastAny(const rtb200_scene* s, const rtb200_ray* d_rays, int64_t n,
                           uint8_t* d_occ, cudaStream_t stream);
+// Closest-hit launch with caller-provided scratch (work counter and error
+// word); clears nothing itself.
+cudaError_t LaunchCastClosestScratch(const rtb200_scene* s, const rtb200_ray* d_rays, int64_t n,
+                                     rtb200_hit* d_hits, unsigned long long* counter, unsigned* err,
+                                     cudaStream_t stream);
 
 }  // namespace rtb200

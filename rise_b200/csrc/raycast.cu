@@ -95,6 +95,27 @@ cudaError_t LaunchCastClosest(const rtb200_scene* s, const rtb200_ray* d_rays, i
     return LaunchTrace<GpuNode4, false>(s, d_rays, n, d_hits, nullptr, stream);
 }
 
+cudaError_t LaunchCastClosestScratch(const rtb200_scene* s, const rtb200_ray* d_rays, int64_t n,
+                                     rtb200_hit* d_hits, unsigned long long* counter, unsigned* err,
+                                     cudaStream_t stream)
+{
+    if (n <= 0) return cudaSuccess;
+    if (s->layout == RTB200_BVH_Q8) {
+        static int grid = 0;
+        if (!grid) grid = GridFor(KTrace<QNode4, false>, s->ctx->num_sms);
+        KTrace<QNode4, false><<<grid, kTraceBlock, 0, stream>>>((const QNode4*)s->d_nodes, s->d_tris, d_rays, n,
+                                                                (int)s->tri_material.size(), d_hits, nullptr,
+                                                                counter, err);
+    } else {
+        static int grid = 0;
+        if (!grid) grid = GridFor(KTrace<GpuNode4, false>, s->ctx->num_sms);
+        KTrace<GpuNode4, false><<<grid, kTraceBlock, 0, stream>>>((const GpuNode4*)s->d_nodes, s->d_tris, d_rays,
+                                                                  n, (int)s->tri_material.size(), d_hits,
+                                                                  nullptr, counter, err);
+    }
+    return cudaGetLastError();
+}
+
 cudaError_t LaunchCastAny(const rtb200_scene* s, const rtb200_ray* d_rays, int64_t n,
                           uint8_t* d_occ, cudaStream_t stream)
 {
