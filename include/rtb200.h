@@ -100,6 +100,81 @@ int rtb200_scene_info(const rtb200_scene* scene, int64_t* n_tri, int64_t* n_node
                       int64_t* device_bytes, double* build_seconds);
 int rtb200_scene_destroy(rtb200_scene* scene);
 
+/* ---- spectral materials and lights ------------------------------------ */
+
+/* Spectra are tabulated at 81 samples, 380..780 nm in 5 nm steps, linearly
+ * interpolated (the reference's SPD interpolation, Utilities/Color/
+ * ColorUtils.cpp:270-300); they stand in for the reference's spectral
+ * painters (IPainter::GetColorNM, Interfaces/IPainter.h:67). */
+#define RTB200_SPECTRUM_SAMPLES 81
+
+/* Material models (reference classes under src/Library/Materials/). */
+#define RTB200_MAT_LAMBERTIAN 0   /* LambertianSPF + LambertianBRDF */
+#define RTB200_MAT_GGX        1   /* GGXSPF + GGXBRDF, conductor Fresnel */
+#define RTB200_MAT_DIELECTRIC 2   /* DielectricSPF, smooth, no BSDF */
+
+typedef struct {
+    int32_t type;         /* RTB200_MAT_* */
+    int32_t reflectance;  /* spectrum id: Lambertian albedo (-1 = black) */
+    int32_t emission;     /* spectrum id of emitted radiance (-1 = none);
+                             LambertianEmitter: one-sided, radiance = spectrum */
+    int32_t eta, kappa;   /* GGX conductor spectra (-1 = unused) */
+    float alpha;          /* GGX roughness */
+    float ior;            /* dielectric index of refraction */
+} rtb200_material;
+
+/* Returns the new spectrum / material id in *id_out.  Materials are
+ * referenced by rtb200_scene_add_mesh's `material`; a mesh whose material
+ * emits becomes one luminary (area light) at commit. */
+int rtb200_scene_add_spectrum(rtb200_scene* scene, const float* values, int32_t* id_out);
+int rtb200_scene_add_material(rtb200_scene* scene, const rtb200_material* m, int32_t* id_out);
+/* Uniform sky: radiance spectrum for rays that escape (-1 = none); visible
+ * selects whether camera rays see it directly. */
+int rtb200_scene_set_environment(rtb200_scene* scene, int32_t spectrum, int32_t visible);
+
+/* ---- render jobs (the rasterizer) -------------------------------------- */
+
+/* Settings of one progressive render.  Replaces the parameters of
+ * RISE_API_CreatePathTracingSpectralRasterizer (RISE_API.h:3112-3141) and the
+ * pinhole camera (Cameras/PinholeCamera.cpp:182-217) for this path. */
+typedef struct {
+    int32_t width, height;
+    float cam_pos[3], cam_look[3], cam_up[3];
+    float fov_deg;            /* vertical field of view */
+    float lambda_min, lambda_max;
+    int32_t max_depth;        /* path vertices, as the reference's max depth */
+    int32_t rr_min_depth;     /* Russian roulette from this depth (reference: 3) */
+    float rr_threshold;       /* reference: 0.05 */
+    int32_t nee_per_lambda;   /* 1: one light sample per wavelength, as the
+                                 reference; 0: one shared sample per vertex */
+    uint32_t seed;
+    int32_t max_paths;        /* path-pool capacity (0 = automatic) */
+} rtb200_render_settings;
+
+typedef struct rtb200_job rtb200_job;
+
+typedef struct {
+    int64_t spp;              /* samples per pixel rendered so far */
+    int64_t samples;          /* camera samples (paths) */
+    int64_t segments;         /* extended rays */
+    int64_t shadow_rays;
+    double seconds;           /* device time of all render calls */
+} rtb200_stats;
+
+/* A job holds the path pool, queues and film of one image on the device.
+ * rtb200_job_render adds spp samples per pixel and returns when they are in
+ * the film (PixelBasedRasterizerHelper::RasterizeScene's progressive passes,
+ * Rendering/PixelBasedRasterizerHelper.cpp:982-1440, with the per-pixel loop
+ * of PathTracingSpectralRasterizer::IntegratePixel,
+ * Rendering/PathTracingSpectralRasterizer.cpp:206-479).
+ * rtb200_job_read_film writes width*height*3 floats: the mean XYZ per pixel
+ * over all samples so far (rows top to bottom). */
+int rtb200_job_create(rtb200_scene* scene, const rtb200_render_settings* settings, rtb200_job** out);
+int rtb200_job_render(rtb200_job* job, int32_t spp);
+int rtb200_job_read_film(rtb200_job* job, float* xyz);
+int rtb200_job_stats(const rtb200_job* job, rtb200_stats* out);
+int rtb200_job_destroy(rtb200_job* job);
+
 /* ---- host BVH build and export ----------------------------------------- */
 
 /* Builds the reference BVH on the host (all cores) without a device and

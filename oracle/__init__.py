@@ -156,6 +156,48 @@ def closest_brute(tri9, rays):
     return ids, t
 
 
+def cie_table():
+    """The reference's CIE 1931 table (tests/golden/cie1931_5nm.json), 3 x 81."""
+    import json
+    path = os.path.join(os.path.dirname(_HERE), "tests", "golden", "cie1931_5nm.json")
+    d = json.load(open(path))
+    return np.array([d["x"], d["y"], d["z"]], np.float64)
+
+
+def pt_render(desc, spp, sample_begin=0, crop=None, threads=None, settings=None):
+    """Render a scenes.SceneDesc with the path-tracing oracle.
+
+    Returns the mean XYZ of samples sample_begin .. sample_begin+spp-1 per
+    pixel as float64 (h, w, 3) over `crop` = (x0, y0, x1, y1) (default: the
+    whole image)."""
+    lib = port()
+    st = settings or desc.settings
+    x0, y0, x1, y1 = crop or (0, 0, st.width, st.height)
+    tri9 = np.ascontiguousarray(desc.tri9, np.float32)
+    meshes = np.array(desc.meshes, np.int64).reshape(-1, 4)
+    spectra = np.ascontiguousarray(np.array(desc.spectra, np.float32).reshape(-1, 81))
+    mats_i = np.array([[m.type, m.reflectance, m.emission, m.eta, m.kappa] for m in desc.materials], np.int32)
+    mats_f = np.array([[m.alpha, m.ior] for m in desc.materials], np.float32)
+    envi = np.array([desc.env, desc.env_visible], np.int32)
+    cam = np.array(list(st.cam_pos) + list(st.cam_look) + list(st.cam_up) + [st.fov_deg], np.float64)
+    setd = np.array([st.lambda_min, st.lambda_max, st.rr_threshold], np.float64)
+    seti = np.array([st.width, st.height, st.max_depth, st.rr_min_depth, st.nee_per_lambda, st.seed], np.int32)
+    out = np.zeros((y1 - y0, x1 - x0, 3), np.float64)
+    cie = np.ascontiguousarray(cie_table())
+    f = lib.orc_pt_render
+    f.restype = ctypes.c_int
+    i32 = ctypes.c_int32
+    f.argtypes = [_f32p, _i64, _vp, i32, _f32p, i32, _vp, _f32p, i32, _vp, _f64p, _f64p, _vp, i32, i32,
+                  i32, i32, i32, i32, i32, _f64p, _f64p]
+    rc = f(_p(tri9, _f32p), len(tri9), meshes.ctypes.data, len(meshes), _p(spectra, _f32p), len(spectra),
+           mats_i.ctypes.data, _p(mats_f, _f32p), len(mats_i), envi.ctypes.data, _p(cam, _f64p), _p(setd, _f64p),
+           seti.ctypes.data, int(spp), int(sample_begin), x0, y0, x1, y1, threads or os.cpu_count(),
+           _p(out, _f64p), _p(cie, _f64p))
+    if rc != 0:
+        raise RuntimeError("oracle path tracer rejected the scene")
+    return out
+
+
 def ray_triangle(o, d, v0, ea, eb, kind="port"):
     """The reference's double Moller-Trumbore on one triangle: (hit, t, alpha, beta)."""
     lib = port() if kind == "port" else ref()

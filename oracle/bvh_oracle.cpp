@@ -436,6 +436,81 @@ bool Any(const Bvh& b, const float* r)
     return false;
 }
 
+// Double-precision ray variants for the path-tracing oracle: the reference
+// casts double rays; the traversal rounds them to float for the node tests
+// (BVH.h:1212-1225) and certifies leaves in double.
+int32_t ClosestD(const Bvh& b, const double od[3], const double dd[3], double* tOut)
+{
+    const float r[8] = {(float)od[0], (float)od[1], (float)od[2], 0.0f, (float)dd[0], (float)dd[1], (float)dd[2], 0.0f};
+    float o[3], d[3], inv[3];
+    PrepRay(r, o, d, inv);
+    double range = kInf;
+    int32_t best = -1;
+    if (b.nodes4.empty()) return -1;
+    std::vector<uint32_t> stack;
+    stack.push_back(0);
+    while (!stack.empty()) {
+        const uint32_t ni = stack.back();
+        stack.pop_back();
+        const orc_node4& n = b.nodes4[ni];
+        float te[4];
+        const uint32_t mask = RayBox4(o, inv, (float)range, n, te) & ((1u << n.nchild) - 1u);
+        if (!mask) continue;
+        for (int i = 0; i < 4; ++i) {
+            if (!(mask & (1u << i))) continue;
+            if (n.count[i] > 0) {
+                const uint32_t s = (uint32_t)n.child[i], e = s + n.count[i];
+                for (uint32_t p = s; p < e; ++p) {
+                    float ft;
+                    if (!FloatFilter(o, d, &b.filt[9ull * p], (float)range, &ft)) continue;
+                    double v0[3], ea[3], eb[3], t, al, be;
+                    TriEdges(b, b.prims[p], v0, ea, eb);
+                    if (RayTri(od, dd, v0, ea, eb, &t, &al, &be) && t < range) { range = t; best = (int32_t)b.prims[p]; }
+                }
+            } else {
+                stack.push_back((uint32_t)n.child[i]);
+            }
+        }
+    }
+    *tOut = range;
+    return best;
+}
+
+bool AnyD(const Bvh& b, const double od[3], const double dd[3], double howFar)
+{
+    float r[8] = {(float)od[0], (float)od[1], (float)od[2], 0.0f, (float)dd[0], (float)dd[1], (float)dd[2], (float)howFar};
+    float o[3], d[3], inv[3];
+    PrepRay(r, o, d, inv);
+    const float best = (float)howFar;
+    if (b.nodes4.empty()) return false;
+    std::vector<uint32_t> stack;
+    stack.push_back(0);
+    while (!stack.empty()) {
+        const uint32_t ni = stack.back();
+        stack.pop_back();
+        const orc_node4& n = b.nodes4[ni];
+        float te[4];
+        const uint32_t mask = RayBox4(o, inv, best, n, te) & ((1u << n.nchild) - 1u);
+        if (!mask) continue;
+        for (int i = 0; i < 4; ++i) {
+            if (!(mask & (1u << i))) continue;
+            if (n.count[i] > 0) {
+                const uint32_t s = (uint32_t)n.child[i], e = s + n.count[i];
+                for (uint32_t p = s; p < e; ++p) {
+                    float ft;
+                    if (!FloatFilter(o, d, &b.filt[9ull * p], best, &ft)) continue;
+                    double v0[3], ea[3], eb[3], t, al, be;
+                    TriEdges(b, b.prims[p], v0, ea, eb);
+                    if (RayTri(od, dd, v0, ea, eb, &t, &al, &be) && t > kNearZero && t < howFar) return true;
+                }
+            } else {
+                stack.push_back((uint32_t)n.child[i]);
+            }
+        }
+    }
+    return false;
+}
+
 template <class F>
 void Parallel(int64_t n, int threads, F fn)
 {
@@ -456,6 +531,16 @@ void Parallel(int64_t n, int threads, F fn)
 }  // namespace
 
 struct orc_bvh { Bvh b; };
+
+int32_t orc_closest_d(const orc_bvh* h, const double o[3], const double d[3], double* t)
+{
+    return ClosestD(h->b, o, d, t);
+}
+
+bool orc_any_d(const orc_bvh* h, const double o[3], const double d[3], double tmax)
+{
+    return AnyD(h->b, o, d, tmax);
+}
 
 extern "C" {
 

@@ -55,7 +55,28 @@ void orc_closest_brute(const float* tri9, int64_t n_tri, const float* rays, int6
 int  orc_ray_triangle(const double* o, const double* d, const double* v0, const double* ea,
                       const double* eb, double* t, double* alpha, double* beta);
 
+/* Spectral path tracer (pt_oracle.cpp): renders the mean XYZ of `spp`
+ * samples per pixel (samples sample_begin .. sample_begin + spp - 1) over the
+ * crop [x0, x1) x [y0, y1) into xyz (3 doubles per crop pixel, row-major).
+ *   meshes: n_mesh x 4 int64 (first triangle, count, material, double sided)
+ *   mats_i: n_mat x 5 int32 (type, reflectance, emission, eta, kappa)
+ *   mats_f: n_mat x 2 float (alpha, ior)
+ *   cam:    10 doubles (pos, look, up, vertical fov in degrees)
+ *   setd:   3 doubles (lambda_min, lambda_max, rr_threshold)
+ *   seti:   6 int32 (width, height, max_depth, rr_min_depth, nee_per_lambda, seed)
+ *   envi:   2 int32 (environment spectrum or -1, visible)
+ *   cie:    3 x 81 doubles, the reference's CIE 1931 table (x, y, z bars)
+ * Returns 0 on success. */
+int orc_pt_render(const float* tri9, int64_t n_tri, const int64_t* meshes, int32_t n_mesh,
+                  const float* spectra, int32_t n_spec, const int32_t* mats_i, const float* mats_f,
+                  int32_t n_mat, const int32_t* envi, const double* cam, const double* setd,
+                  const int32_t* seti, int32_t spp, int32_t sample_begin, int32_t x0, int32_t y0,
+                  int32_t x1, int32_t y1, int32_t threads, double* xyz, const double* cie);
+
 #ifdef __cplusplus
 }
+/* Double-precision ray queries used by the path-tracing oracle. */
+int32_t orc_closest_d(const orc_bvh* h, const double o[3], const double d[3], double* t);
+bool orc_any_d(const orc_bvh* h, const double o[3], const double d[3], double tmax);
 #endif
 #endif

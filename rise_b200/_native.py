@@ -43,6 +43,14 @@ SIGNATURES = {
     "rtb200_cast_closest_device": (ctypes.c_int, [_vp, _vp, _i64, _vp, _vp]),
     "rtb200_cast_any_device": (ctypes.c_int, [_vp, _vp, _i64, _vp, _vp]),
     "rtb200_cast_closest_noalloc": (ctypes.c_int, [_vp, _vp, _i64, _vp, _vp]),
+    "rtb200_scene_add_spectrum": (ctypes.c_int, [_vp, _vp, _vp]),
+    "rtb200_scene_add_material": (ctypes.c_int, [_vp, _vp, _vp]),
+    "rtb200_scene_set_environment": (ctypes.c_int, [_vp, _i32, _i32]),
+    "rtb200_job_create": (ctypes.c_int, [_vp, _vp, _vp]),
+    "rtb200_job_render": (ctypes.c_int, [_vp, _i32]),
+    "rtb200_job_read_film": (ctypes.c_int, [_vp, _vp]),
+    "rtb200_job_stats": (ctypes.c_int, [_vp, _vp]),
+    "rtb200_job_destroy": (ctypes.c_int, [_vp]),
 }
 NOALLOC_SCRATCH_BYTES = 256
 NOALLOC_MAX_RAYS = 2147483647

@@ -163,6 +163,7 @@ int rtb200_scene_add_mesh(rtb200_scene* s, const float* xyz, int64_t n_verts, co
         return SetError(ctx, RTB200_E_INVALID, "too many triangles");
     for (int64_t i = 0; i < 3 * n_tri; ++i)
         if ((int64_t)tri[i] >= n_verts) return SetError(ctx, RTB200_E_INVALID, "triangle index out of range");
+    s->meshes.push_back({(int64_t)s->tri_material.size(), n_tri, material, double_sided ? 1 : 0});
     const size_t base = s->tri9.size();
     s->tri9.resize(base + 9 * (size_t)n_tri);
     float* dst = s->tri9.data() + base;
@@ -222,6 +223,14 @@ int rtb200_scene_commit(rtb200_scene* s, int32_t layout)
     s->tris_bytes = tris.size() * sizeof(GpuTri);
     s->n_nodes = (int64_t)s->bvh.nodes4.size();
     s->layout = layout;
+    rc = UploadShading(s);
+    if (rc) {
+        DevFree(ctx, s->d_nodes, s->nodes_bytes);
+        DevFree(ctx, s->d_tris, s->tris_bytes);
+        s->d_nodes = nullptr;
+        s->d_tris = nullptr;
+        return rc;
+    }
     s->committed = true;
     return RTB200_OK;
 }
@@ -249,6 +258,7 @@ int rtb200_scene_destroy(rtb200_scene* s)
     DevFree(ctx, s->d_in, s->stage_in);
     DevFree(ctx, s->d_out, s->stage_out);
     DevFree(ctx, s->d_counter, 256);
+    FreeShading(s);
     delete s;
     return RTB200_OK;
 }

@@ -9,6 +9,7 @@
 
 #include "../../include/rtb200.h"
 #include "bvh_build.h"
+#include "pt_types.h"
 
 struct rtb200_ctx {
     int device = 0;
@@ -26,6 +27,25 @@ struct rtb200_scene {
     std::vector<float> tri9;
     std::vector<int32_t> tri_material;
     std::vector<uint8_t> tri_double_sided;
+    struct Mesh {
+        int64_t first, count;
+        int32_t material;
+        int32_t double_sided;
+    };
+    std::vector<Mesh> meshes;
+    // spectral shading data
+    std::vector<float> spectra;                 // 81 samples per spectrum
+    std::vector<rtb200::PtMaterial> materials;
+    int32_t env = -1, env_visible = 1;
+    std::vector<rtb200::PtLight> lights;        // built at commit
+    std::vector<rtb200::PtLightTri> light_tris;
+    // device copies (path tracer)
+    rtb200::PtTriAttr* d_attr = nullptr;
+    rtb200::PtMaterial* d_mats = nullptr;
+    float* d_spectra = nullptr;
+    rtb200::PtLight* d_lights = nullptr;
+    rtb200::PtLightTri* d_light_tris = nullptr;
+    size_t shade_bytes = 0;
     bool committed = false;
     int32_t layout = RTB200_BVH_F32;
     int64_t n_nodes = 0;
@@ -52,6 +72,11 @@ int DevAlloc(rtb200_ctx* ctx, void** p, size_t bytes);
 void DevFree(rtb200_ctx* ctx, void* p, size_t bytes);
 int SetError(rtb200_ctx* ctx, int code, const std::string& msg);
 int CudaCheck(rtb200_ctx* ctx, cudaError_t e, const char* what);
+
+// Shading tables of a committed scene (pt_api.cpp): per-triangle attributes
+// in leaf order, materials, spectra, luminaries.
+int UploadShading(rtb200_scene* s);
+void FreeShading(rtb200_scene* s);
 
 // Kernel launchers (raycast.cu).  Asynchronous on `stream`.
 cudaError_t LaunchCastClosest(const rtb200_scene* s, const rtb200_ray* d_rays, int64_t n,

@@ -1,0 +1,158 @@
+// pt_types.h -- device-side scene, job and queue descriptors of the spectral
+// path tracer (pathtrace.cu), shared with the host code that fills them.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "bvh_build.h"
+
+#define RTB_HD __host__ __device__ __forceinline__
+
+namespace rtb200 {
+
+// Material models on the path (reference classes in src/Library/Materials/).
+enum PtMatType : int {
+    kMatLambertian = 0,   // LambertianSPF/LambertianBRDF
+    kMatGGX = 1,          // GGXSPF/GGXBRDF, conductor Fresnel
+    kMatDielectric = 2,   // DielectricSPF (no BSDF: per-wavelength path)
+};
+
+struct PtMaterial {
+    int type;
+    int refl;        // reflectance spectrum (Lambertian albedo); -1 = black
+    int emit;        // emitted radiance spectrum; -1 = not an emitter
+    int eta;         // conductor eta spectrum (GGX) or -1
+    int kappa;       // conductor k spectrum (GGX) or -1
+    float alpha;     // GGX roughness (alpha)
+    float ior;       // dielectric index of refraction
+    int pad;
+};
+
+// One luminary: a mesh whose material emits.  Points are drawn uniformly by
+// area over its triangles (area CDF), like the reference's
+// TriangleMeshGeometryIndexed::UniformRandomPoint.
+struct PtLight {
+    int first;       // first entry in the light-triangle array
+    int count;
+    float area;      // total area of the luminary
+    float pdf;       // selection probability
+    int emit;        // emitted radiance spectrum
+    int pad[3];
+};
+
+struct PtLightTri {
+    float v0[3];
+    float e1[3];
+    float e2[3];
+    float cdf;       // cumulative area fraction up to and including this triangle
+    float pad[2];
+};
+
+struct PtCamera {
+    float pos[3];
+    float fwd[3];
+    float right[3];  // scaled by tan(fov/2) * aspect
+    float up[3];     // scaled by tan(fov/2)
+    int width, height;
+};
+
+struct PtSettings {
+    float lmin, lmax;        // wavelength range (nm)
+    float ynorm;             // (lmax - lmin) / integral of y-bar over the range
+    int max_depth;
+    int rr_min_depth;
+    float rr_threshold;
+    int nee_per_lambda;      // 1: one light sample per wavelength (reference); 0: shared
+    unsigned seed;
+    int env;                 // uniform-sky radiance spectrum, -1 = none
+    int env_visible;         // sky seen directly by camera rays
+    int n_lights;
+    int n_spectra;
+};
+
+// Per-triangle shading attributes in leaf order: material | double-sided
+// bit (bit 30), and luminary index (-1 = none).
+struct PtTriAttr {
+    int mat;
+    int light;
+};
+
+constexpr int kAttrDoubleSided = 1 << 30;
+constexpr int kAttrMatMask = (1 << 24) - 1;
+
+// Path flags (meta.z).
+constexpr unsigned kFlagDepthMask = 0xffu;
+constexpr unsigned kFlagConsiderEmission = 1u << 8;
+constexpr unsigned kFlagFinishing = 1u << 9;
+constexpr unsigned kFlagSpecular = 1u << 10;
+constexpr unsigned kTermShift = 12;        // 4 bits: terminated wavelengths
+
+// Shadow-ray queue entry, 48 bytes.
+struct ShadowEntry {
+    float4 o;        // origin, w = tmax
+    float4 d;        // direction, w = path slot (int bits)
+    float4 c;        // contribution per wavelength (added when unoccluded)
+};
+
+// Counters in device memory.
+enum PtCounter : int {
+    kCntActive = 0,     // paths to extend this iteration
+    kCntActiveNext = 1,
+    kCntFree = 2,       // finished / empty slots to regenerate
+    kCntFreeNext = 3,
+    kCntShadow = 4,
+    kCntSegments = 5,   // extended rays (statistics)
+    kCntShadowRays = 6,
+    kCntCount = 16,
+};
+
+struct PtScene {
+    const void* nodes;
+    int layout;
+    const GpuTri* tris;
+    int ntri;
+    const PtTriAttr* attr;
+    const PtMaterial* mats;
+    const float* spectra;      // n_spectra x 81 samples, 380..780 nm at 5 nm
+    const PtLight* lights;
+    const PtLightTri* light_tris;
+};
+
+struct PtPaths {
+    float4* ray_o;   // origin, tmin
+    float4* ray_d;   // direction, tmax
+    float4* hit;     // t, leaf slot (int bits, -1 miss), a, b
+    float4* thr;     // throughput per wavelength
+    float4* L;       // radiance per wavelength
+    float4* aux;     // x hero wavelength, y bsdf pdf
+    uint4* meta;     // x pixel, y sample, z flags, w rng key
+};
+
+struct PtQueues {
+    int* active;        // current
+    int* active_next;
+    int* free_;         // current
+    int* free_next;
+    ShadowEntry* shadow;
+    int* cnt;           // PtCounter
+    unsigned long long* sample_ctr;
+    unsigned long long* trace_ctr;   // [2]: extend, connect
+    unsigned* err;
+};
+
+struct PtFilm {
+    float* pass;        // 3 floats per pixel, atomically accumulated this call
+    float* sum;         // 3 floats per pixel, compensated running sum
+    float* comp;        // 3 floats per pixel, Kahan compensation
+};
+
+struct PtJobParams {
+    PtCamera cam;
+    PtSettings set;
+    int npix;
+    int capacity;                 // path slots
+    unsigned long long sample_begin;   // first sample index of this call (per pixel)
+    unsigned long long total;     // npix * samples in this call
+};
+
+}  // namespace rtb200

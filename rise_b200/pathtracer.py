@@ -1,0 +1,101 @@
+"""Host-side mirror of the reference's spectral path-tracing rasterizer.
+
+`SpectralRasterizer` plays the part of PathTracingSpectralRasterizer on top
+of PixelBasedRasterizerHelper (src/Library/Rendering/
+PathTracingSpectralRasterizer.cpp, PixelBasedRasterizerHelper.cpp): it owns
+a scene on the device and a render job, `rasterize_scene(spp)` adds spp
+samples per pixel (a progressive pass), and `film()` returns the mean XYZ
+per pixel.  Everything runs through the C ABI (include/rtb200.h).
+"""
+import ctypes
+
+import numpy as np
+
+from . import _native
+from ._native import check, lib
+from .raycaster import Scene
+
+
+class Material(ctypes.Structure):
+    _fields_ = [("type", ctypes.c_int32), ("reflectance", ctypes.c_int32), ("emission", ctypes.c_int32),
+                ("eta", ctypes.c_int32), ("kappa", ctypes.c_int32), ("alpha", ctypes.c_float),
+                ("ior", ctypes.c_float)]
+
+
+class RenderSettings(ctypes.Structure):
+    _fields_ = [("width", ctypes.c_int32), ("height", ctypes.c_int32),
+                ("cam_pos", ctypes.c_float * 3), ("cam_look", ctypes.c_float * 3), ("cam_up", ctypes.c_float * 3),
+                ("fov_deg", ctypes.c_float), ("lambda_min", ctypes.c_float), ("lambda_max", ctypes.c_float),
+                ("max_depth", ctypes.c_int32), ("rr_min_depth", ctypes.c_int32), ("rr_threshold", ctypes.c_float),
+                ("nee_per_lambda", ctypes.c_int32), ("seed", ctypes.c_uint32), ("max_paths", ctypes.c_int32)]
+
+
+class Stats(ctypes.Structure):
+    _fields_ = [("spp", ctypes.c_int64), ("samples", ctypes.c_int64), ("segments", ctypes.c_int64),
+                ("shadow_rays", ctypes.c_int64), ("seconds", ctypes.c_double)]
+
+
+def upload_scene(ctx, desc, layout="f32"):
+    """Create and commit a device scene from a scenes.SceneDesc."""
+    s = Scene(ctx)
+    L = lib()
+    for sp in desc.spectra:
+        sp = np.ascontiguousarray(sp, np.float32)
+        out = ctypes.c_int32()
+        check(L.rtb200_scene_add_spectrum(s.h, ctypes.c_void_p(sp.ctypes.data), ctypes.byref(out)), ctx.h)
+    for m in desc.materials:
+        cm = Material(m.type, m.reflectance, m.emission, m.eta, m.kappa, m.alpha, m.ior)
+        out = ctypes.c_int32()
+        check(L.rtb200_scene_add_material(s.h, ctypes.byref(cm), ctypes.byref(out)), ctx.h)
+    check(L.rtb200_scene_set_environment(s.h, desc.env, desc.env_visible), ctx.h)
+    for first, count, mat, ds in desc.meshes:
+        s.add_triangles(desc.tri9[first:first + count], material=mat, double_sided=ds)
+    s.commit(layout)
+    return s
+
+
+def settings_struct(st):
+    return RenderSettings(st.width, st.height, (ctypes.c_float * 3)(*st.cam_pos), (ctypes.c_float * 3)(*st.cam_look),
+                          (ctypes.c_float * 3)(*st.cam_up), st.fov_deg, st.lambda_min, st.lambda_max, st.max_depth,
+                          st.rr_min_depth, st.rr_threshold, st.nee_per_lambda, st.seed, st.max_paths)
+
+
+class SpectralRasterizer:
+    """One progressive spectral path-traced image of one scene."""
+
+    def __init__(self, ctx, desc, layout="f32", scene=None, settings=None):
+        self.ctx = ctx
+        self.desc = desc
+        self.owns_scene = scene is None
+        self.scene = scene if scene is not None else upload_scene(ctx, desc, layout)
+        self.settings = settings if settings is not None else desc.settings
+        h = ctypes.c_void_p()
+        cs = settings_struct(self.settings)
+        check(lib().rtb200_job_create(self.scene.h, ctypes.byref(cs), ctypes.byref(h)), ctx.h)
+        self.h = h
+
+    def rasterize_scene(self, spp):
+        """Add `spp` samples per pixel (blocking)."""
+        check(lib().rtb200_job_render(self.h, int(spp)), self.ctx.h)
+
+    def film(self):
+        """Mean XYZ per pixel, (height, width, 3) float32."""
+        st = self.settings
+        out = np.empty((st.height, st.width, 3), np.float32)
+        check(lib().rtb200_job_read_film(self.h, ctypes.c_void_p(out.ctypes.data)), self.ctx.h)
+        return out
+
+    def stats(self):
+        s = Stats()
+        check(lib().rtb200_job_stats(self.h, ctypes.byref(s)), self.ctx.h)
+        return {"spp": s.spp, "samples": s.samples, "segments": s.segments, "shadow_rays": s.shadow_rays,
+                "seconds": s.seconds}
+
+    def close(self):
+        if self.h:
+            lib().rtb200_job_destroy(self.h)
+            self.h = None
+        if self.owns_scene and self.scene is not None:
+            self.scene.close()
+            self.scene = None
+

@@ -7,14 +7,24 @@ start uniformly on a sphere of radius 2 around the cube centre (0.5, 0.5,
 0.5) and point at uniform targets inside the cube.  Closest-hit rays have an
 unbounded range; any-hit (shadow) rays end at their target.
 
-All arrays are float32.  Rays are packed 8 floats each:
+Path-tracing scenes are described by `SceneDesc` (triangle meshes with one
+material each, spectra tabulated at 81 samples over 380..780 nm in 5 nm
+steps, materials, optional uniform sky, pinhole camera and render
+settings); `cornell_box` builds the 32-triangle spectral Cornell box.
+
+All geometry is float32.  Rays are packed 8 floats each:
 (ox, oy, oz, tmin, dx, dy, dz, tmax) with a unit direction.
 """
+from dataclasses import dataclass, field
+
 import numpy as np
 
 CUBE_CENTRE = np.array([0.5, 0.5, 0.5], np.float64)
 SPHERE_RADIUS = 2.0
 VERTEX_SIGMA = 0.01
+
+WAVELENGTHS = np.arange(380.0, 781.0, 5.0)  # 81 spectrum samples
+MAT_LAMBERTIAN, MAT_GGX, MAT_DIELECTRIC = 0, 1, 2
 
 
 def soup_triangles(n_tri, seed=7):
@@ -47,3 +57,138 @@ def sphere_rays(n_rays, seed=7, shadow=False):
     rays[:, 4:7] = d
     rays[:, 7] = dist if shadow else np.inf
     return rays
+
+
+# ---- spectra -----------------------------------------------------------------
+
+def flat_spectrum(value, lo=380.0, hi=780.0, outside=0.0):
+    """`value` on [lo, hi] nm (inclusive grid points), `outside` elsewhere."""
+    s = np.full(81, outside, np.float32)
+    s[(WAVELENGTHS >= lo) & (WAVELENGTHS <= hi)] = value
+    return s
+
+
+# ---- path-tracing scene description ------------------------------------------
+
+@dataclass
+class Material:
+    type: int = MAT_LAMBERTIAN
+    reflectance: int = -1   # spectrum id
+    emission: int = -1      # spectrum id (radiance)
+    eta: int = -1
+    kappa: int = -1
+    alpha: float = 0.0
+    ior: float = 1.5
+
+
+@dataclass
+class RenderSettings:
+    width: int = 256
+    height: int = 256
+    cam_pos: tuple = (0.5, 0.5, -1.4)
+    cam_look: tuple = (0.5, 0.5, 0.0)
+    cam_up: tuple = (0.0, 1.0, 0.0)
+    fov_deg: float = 39.3
+    lambda_min: float = 400.0
+    lambda_max: float = 700.0
+    max_depth: int = 8
+    rr_min_depth: int = 3
+    rr_threshold: float = 0.05
+    nee_per_lambda: int = 1
+    seed: int = 1
+    max_paths: int = 0
+
+
+@dataclass
+class SceneDesc:
+    tri9: np.ndarray = None
+    meshes: list = field(default_factory=list)     # (first, count, material, double_sided)
+    spectra: list = field(default_factory=list)    # 81 floats each
+    materials: list = field(default_factory=list)  # Material
+    env: int = -1
+    env_visible: int = 1
+    settings: RenderSettings = field(default_factory=RenderSettings)
+    _tris: list = field(default_factory=list)
+
+    def add_spectrum(self, s):
+        self.spectra.append(np.asarray(s, np.float32).reshape(81))
+        return len(self.spectra) - 1
+
+    def add_material(self, m):
+        self.materials.append(m)
+        return len(self.materials) - 1
+
+    def add_mesh(self, tri9, material, double_sided=True):
+        tri9 = np.asarray(tri9, np.float32).reshape(-1, 9)
+        first = sum(len(t) for t in self._tris)
+        self._tris.append(tri9)
+        self.meshes.append((first, len(tri9), material, int(bool(double_sided))))
+        self.tri9 = np.concatenate(self._tris).astype(np.float32)
+
+    @property
+    def n_tri(self):
+        return 0 if self.tri9 is None else len(self.tri9)
+
+
+def _quad(p0, p1, p2, p3):
+    """Two triangles (p0, p1, p2), (p0, p2, p3); normal = (p1-p0) x (p2-p0)."""
+    return np.array([p0 + p1 + p2, p0 + p2 + p3], np.float32)
+
+
+def _box(cx, cz, sx, sy, sz, angle_deg):
+    """Five faces (no bottom) of a box on the floor, rotated about y."""
+    a = np.radians(angle_deg)
+    c, s = np.cos(a), np.sin(a)
+
+    def P(x, y, z):
+        x -= sx / 2
+        z -= sz / 2
+        return [cx + c * x + s * z, y, cz - s * x + c * z]
+    v = {k: P(*k) for k in [(0, 0, 0), (sx, 0, 0), (sx, 0, sz), (0, 0, sz),
+                            (0, sy, 0), (sx, sy, 0), (sx, sy, sz), (0, sy, sz)]}
+    q = [
+        ((0, sy, 0), (0, sy, sz), (sx, sy, sz), (sx, sy, 0)),   # top
+        ((0, 0, 0), (0, sy, 0), (sx, sy, 0), (sx, 0, 0)),       # front (z = 0 side)
+        ((sx, 0, sz), (sx, sy, sz), (0, sy, sz), (0, 0, sz)),   # back
+        ((0, 0, sz), (0, sy, sz), (0, sy, 0), (0, 0, 0)),       # left
+        ((sx, 0, 0), (sx, sy, 0), (sx, sy, sz), (sx, 0, sz)),   # right
+    ]
+    return np.concatenate([_quad(*(v[k] for k in f)) for f in q])
+
+
+def cornell_box(width=256, height=256, spp_seed=1, nee_per_lambda=1, max_depth=8):
+    """The 32-triangle spectral Cornell box.
+
+    Five unit-square walls (floor y=0, ceiling y=1, back z=1, red x=1, green
+    x=0; 10 triangles), two boxes of five faces rotated about the vertical
+    axis (20 triangles), and a 0.25 x 0.25 quad light just below the ceiling
+    facing down (2 triangles).  Lambertian reflectances: white 0.75 flat; red
+    0.6 on 600-700 nm, 0.05 elsewhere; green 0.6 on 500-570 nm, 0.05
+    elsewhere.  The light emits radiance 15 on 400-700 nm.  Pinhole camera,
+    max depth 8, Russian roulette from depth 3.
+    """
+    d = SceneDesc()
+    white = d.add_spectrum(flat_spectrum(0.75))
+    red = d.add_spectrum(flat_spectrum(0.6, 600, 700, 0.05))
+    green = d.add_spectrum(flat_spectrum(0.6, 500, 570, 0.05))
+    light = d.add_spectrum(flat_spectrum(15.0, 400, 700, 0.0))
+    m_white = d.add_material(Material(MAT_LAMBERTIAN, white))
+    m_red = d.add_material(Material(MAT_LAMBERTIAN, red))
+    m_green = d.add_material(Material(MAT_LAMBERTIAN, green))
+    m_light = d.add_material(Material(MAT_LAMBERTIAN, -1, light))
+    floor = _quad([0, 0, 0], [0, 0, 1], [1, 0, 1], [1, 0, 0])
+    ceil = _quad([0, 1, 0], [1, 1, 0], [1, 1, 1], [0, 1, 1])
+    back = _quad([0, 0, 1], [0, 1, 1], [1, 1, 1], [1, 0, 1])
+    d.add_mesh(np.concatenate([floor, ceil, back]), m_white)
+    d.add_mesh(_quad([1, 0, 0], [1, 0, 1], [1, 1, 1], [1, 1, 0]), m_red)
+    d.add_mesh(_quad([0, 0, 0], [0, 1, 0], [0, 1, 1], [0, 0, 1]), m_green)
+    d.add_mesh(np.concatenate([_box(0.67, 0.35, 0.3, 0.3, 0.3, -17.0),
+                               _box(0.33, 0.65, 0.3, 0.6, 0.3, 17.0)]), m_white)
+    y = 0.999
+    lo, hi = 0.375, 0.625
+    # Winding chosen so the face normal points down (-y): one-sided emitter.
+    d.add_mesh(_quad([lo, y, lo], [hi, y, lo], [hi, y, hi], [lo, y, hi]), m_light, double_sided=False)
+    d.settings = RenderSettings(width=width, height=height, seed=spp_seed, nee_per_lambda=nee_per_lambda,
+                                max_depth=max_depth)
+    assert d.n_tri == 32
+    return d
