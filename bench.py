@@ -46,6 +46,9 @@ def parse():
     p.add_argument("--impl", default="rtb200", choices=["rtb200", "reference"])
     p.add_argument("--e2e-steps", type=int, default=5)
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-path-tracer", action="store_true")
+    p.add_argument("--pt-only", action="store_true",
+                   help="run only the path-tracer measurement and print its JSON (for profiling)")
     return p.parse_args()
 
 
@@ -128,6 +131,66 @@ def cpu_reference_time(tri, rays, seconds=12.0, threads=None):
     return n / dt / 1e6, kind, threads, n
 
 
+def bench_path_tracer(ctx, rank, cpu_baseline=True):
+    """Spectral Cornell box (32 triangles, 256x256, 16 spp, 4 wavelengths per
+    sample, max depth 8, Russian roulette from depth 3): device throughput in
+    Msamples/s for both NEE modes, and relMSE against a 4096-spp render of an
+    independent seed at 16, 64 and 256 spp."""
+    from rise_b200 import pathtracer, scenes
+    out = {"workload": "spectral Cornell box: 32 triangles, 256x256, 16 spp, HWSS 4 wavelengths, "
+                       "max depth 8, RR from depth 3, seed 1"}
+    desc = scenes.cornell_box(256, 256)
+    scene = pathtracer.upload_scene(ctx, desc)
+    npix = 256 * 256
+    for nee, name in ((1, "nee_per_wavelength"), (0, "nee_shared")):
+        desc.settings.nee_per_lambda = nee
+        r = pathtracer.SpectralRasterizer(ctx, desc, scene=scene)
+        r.rasterize_scene(16)   # warm-up pass
+        t0 = r.stats()["seconds"]
+        reps = 4
+        for _ in range(reps):
+            r.rasterize_scene(16)
+        st = r.stats()
+        dt = (st["seconds"] - t0) / reps
+        out[name] = {"msamples_s": npix * 16 / dt / 1e6, "ms_per_16spp": dt * 1e3,
+                     "segments_per_sample": st["segments"] / st["samples"],
+                     "shadow_rays_per_sample": st["shadow_rays"] / st["samples"]}
+        r.close()
+    # Converged image: 4096 spp from another seed (per-wavelength NEE).
+    desc.settings.nee_per_lambda = 1
+    ref_settings = scenes.RenderSettings(**{**desc.settings.__dict__, "seed": 99991})
+    rref = pathtracer.SpectralRasterizer(ctx, desc, scene=scene, settings=ref_settings)
+    for _ in range(16):
+        rref.rasterize_scene(256)
+    ref = rref.film().astype(np.float64)
+    rref.close()
+    rel = {}
+    r = pathtracer.SpectralRasterizer(ctx, desc, scene=scene)
+    done = 0
+    for target in (16, 64, 256):
+        r.rasterize_scene(target - done)
+        done = target
+        img = r.film().astype(np.float64)
+        rel[str(target)] = float(np.mean((img - ref) ** 2 / (ref ** 2 + 1e-2)))
+    r.close()
+    out["relmse_vs_4096spp"] = rel
+    ms16 = out["nee_per_wavelength"]["ms_per_16spp"]
+    reach = [int(k) for k, v in rel.items() if v <= 1e-3]
+    if reach:
+        out["spp_to_relmse_1e-3"] = min(reach)
+        out["seconds_to_relmse_1e-3"] = min(reach) / 16 * ms16 * 1e-3
+    if cpu_baseline and rank == 0:
+        import oracle
+        t0 = time.perf_counter()
+        crop = (0, 96, 256, 160)   # 64 rows, 16 spp
+        oracle.pt_render(desc, 16, crop=crop)
+        dt = time.perf_counter() - t0
+        out["cpu_baseline"] = {"value": 256 * 64 * 16 / dt / 1e6, "unit": "Msamples/s", "cores": os.cpu_count(),
+                               "kind": "port", "sample": "rows 96-159 of the 256x256 image, 16 spp"}
+    scene.close()
+    return out
+
+
 def run_reference(args):
     rank, world, _ = dist_info()
     if rank != 0:
@@ -170,6 +233,11 @@ def main():
 
     rank, world, local = dist_info()
     torch.cuda.set_device(local)
+    if args.pt_only:
+        ctx = raycaster.Context(local)
+        print(json.dumps(bench_path_tracer(ctx, rank, cpu_baseline=False)))
+        ctx.close()
+        return
     if world > 1:
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=120))
@@ -294,6 +362,8 @@ def main():
                                "sample": f"first {n} rays of the {N_RAYS}-ray set, closest-hit, BVH build excluded"}
     sf.close()
     sq.close()
+    if not args.no_path_tracer:
+        out["path_tracer"] = bench_path_tracer(ctx, rank, cpu_baseline=world == 1 and not args.no_cpu_baseline)
     ctx.close()
     if world > 1:
         dist.barrier()
