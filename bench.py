@@ -47,6 +47,7 @@ def parse():
     p.add_argument("--e2e-steps", type=int, default=5)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-path-tracer", action="store_true")
+    p.add_argument("--no-large", action="store_true", help="skip the 3.4M-triangle scene")
     p.add_argument("--pt-only", action="store_true",
                    help="run only the path-tracer measurement and print its JSON (for profiling)")
     return p.parse_args()
@@ -187,6 +188,35 @@ def bench_path_tracer(ctx, rank, cpu_baseline=True):
         dt = time.perf_counter() - t0
         out["cpu_baseline"] = {"value": 256 * 64 * 16 / dt / 1e6, "unit": "Msamples/s", "cores": os.cpu_count(),
                                "kind": "port", "sample": "rows 96-159 of the 256x256 image, 16 spp"}
+    scene.close()
+    return out
+
+
+def bench_large_scene(ctx, layout="f32"):
+    """Large scene: 1024x1024 fBm heightfield (2,093,058 triangles) + 64 spheres
+    of 20,000 triangles (half GGX conductors, half glass), area light and sky;
+    1024x1024 pixels, 64 spp, 4 wavelengths, max depth 16."""
+    from rise_b200 import pathtracer, scenes
+    desc = scenes.spheres_scene()
+    t0 = time.perf_counter()
+    scene = pathtracer.upload_scene(ctx, desc, layout)
+    setup = time.perf_counter() - t0
+    info = scene.info()
+    r = pathtracer.SpectralRasterizer(ctx, desc, scene=scene)
+    r.rasterize_scene(4)      # warm-up
+    s0 = r.stats()
+    r.rasterize_scene(64)
+    s1 = r.stats()
+    dt = s1["seconds"] - s0["seconds"]
+    n = (s1["samples"] - s0["samples"])
+    out = {"workload": "1024^2 fBm heightfield + 64 x 20k-triangle spheres (GGX / glass), area light + sky, "
+                       "1024x1024, 64 spp, HWSS 4 wavelengths, max depth 16",
+           "n_tri": info["n_tri"], "layout": layout, "bvh_build_and_upload_s": round(setup, 3),
+           "msamples_s": n / dt / 1e6, "seconds_64spp": dt,
+           "segments_per_sample": (s1["segments"] - s0["segments"]) / n,
+           "shadow_rays_per_sample": (s1["shadow_rays"] - s0["shadow_rays"]) / n,
+           "mrays_s": ((s1["segments"] - s0["segments"]) + (s1["shadow_rays"] - s0["shadow_rays"])) / dt / 1e6}
+    r.close()
     scene.close()
     return out
 
@@ -364,6 +394,8 @@ def main():
     sq.close()
     if not args.no_path_tracer:
         out["path_tracer"] = bench_path_tracer(ctx, rank, cpu_baseline=world == 1 and not args.no_cpu_baseline)
+        if not args.no_large:
+            out["path_tracer_large"] = bench_large_scene(ctx)
     ctx.close()
     if world > 1:
         dist.barrier()

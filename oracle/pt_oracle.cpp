@@ -2,8 +2,8 @@
 //
 // Double-precision, one-sample-at-a-time restatement of the reference's
 // hero-wavelength spectral path tracer for the scenes of this project
-// (triangle meshes, Lambertian surfaces, Lambertian area emitters, uniform
-// sky):
+// (triangle meshes; Lambertian, GGX-conductor and smooth-dielectric
+// materials; Lambertian area emitters; uniform sky):
 //   * per-pixel sample loop, box pixel filter   PathTracingSpectralRasterizer.cpp:206-479
 //   * 4 equidistant wavelengths, XYZ, (b-a)/k_y  PathTracingSpectralRasterizer.cpp:121-198,
 //                                                SampledWavelengths.h:79-106,
@@ -12,9 +12,12 @@
 //       runaway guard :4099-4110, emission + MIS :4424-4518, NEE per
 //       wavelength :4523-4550, BSDF sample + companions :4597-4719,
 //       Russian roulette :4738-4769, update + Advance(1e-8) :4791-4816
-//   * area-light NEE                            LightSampler.cpp:2083-2271
-//   * cosine sampling, Lambertian value/pdf     LambertianSPF.cpp:90-172, LambertianBRDF.cpp:44-93,
+//   * area-light and sky NEE                    LightSampler.cpp:2083-2359
+//   * Lambertian                                LambertianSPF.cpp:90-172, LambertianBRDF.cpp:44-93,
 //                                                GeometricUtilities.cpp:85-98
+//   * GGX conductor                             GGXSPF.cpp:424-688, GGXBRDF.cpp:339-498,
+//                                                MicrofacetUtils.h, MicrofacetEnergyLUT.h, Optics.hpp
+//   * smooth dielectric                         DielectricSPF.cpp:120-300, Optics.cpp:101-160
 //   * point on a mesh luminary                  TriangleMeshGeometryIndexed.cpp:207-218,
 //                                                GeometricUtilities.cpp:543-569
 //   * power heuristic, Russian roulette         PathTransportUtilities.h:86-110, :251
@@ -25,6 +28,7 @@
 #include <algorithm>
 #include <atomic>
 #include <cmath>
+#include <mutex>
 #include <thread>
 #include <vector>
 
@@ -34,6 +38,7 @@ namespace {
 
 const double kPi = 3.14159265358979323846;
 const double kInvPi = 1.0 / kPi;
+const double kInv4Pi = 1.0 / (4.0 * kPi);
 const double kNearZero = 1e-12;
 
 inline uint32_t Mix32(uint32_t x)
@@ -62,14 +67,165 @@ inline double Dot(V a, V b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
 inline V Cross(V a, V b) { return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x}; }
 inline V Norm(V a) { return a * (1.0 / std::sqrt(Dot(a, a))); }
 
-struct Light {
-    int first, count, emit;
-    double area, pdf;
+// Frame around unit n (Duff et al., JCGT 6(1), 2017) -- the device's frame,
+// so that equal random numbers give equal directions.
+inline void Frame(V n, V& t, V& b)
+{
+    const double sg = std::copysign(1.0, n.z);
+    const double a = -1.0 / (sg + n.z);
+    const double c = n.x * n.y * a;
+    t = {1.0 + sg * n.x * n.x * a, sg * c, -sg * n.x};
+    b = {c, sg + n.y * n.y * a, -n.y};
+}
+
+// ---- GGX conductor ----------------------------------------------------------
+
+double Lambda(double alpha, double c)
+{
+    if (c >= 1.0 - 1e-10) return 0.0;
+    if (c < 1e-10) return 1e10;
+    const double c2 = c * c;
+    return (-1.0 + std::sqrt(1.0 + alpha * alpha * (1.0 - c2) / c2)) * 0.5;
+}
+double GgxD(double alpha, double ch)
+{
+    if (ch <= 0) return 0.0;
+    const double a2 = alpha * alpha;
+    const double d = ch * ch * (a2 - 1.0) + 1.0;
+    return a2 / (kPi * d * d);
+}
+// Spherical-cap visible-normal sample for view direction wl (local frame).
+V VndfLocal(V wl, double alpha, double u1, double u2)
+{
+    const V wh = Norm({alpha * wl.x, alpha * wl.y, wl.z});
+    const double phi = 2.0 * kPi * u1;
+    const double z = (1.0 - u2) * (1.0 + wh.z) - wh.z;
+    const double st = std::sqrt(std::max(0.0, 1.0 - z * z));
+    const V c = {st * std::cos(phi) + wh.x, st * std::sin(phi) + wh.y, z + wh.z};
+    return Norm({alpha * c.x, alpha * c.y, c.z});
+}
+double VndfPdf(V wi, V wo, V n, double alpha)
+{
+    const double ci = Dot(wi, n);
+    if (ci < 1e-10) return 0.0;
+    const V h = Norm(wi + wo);
+    const double ch = Dot(h, n), ih = Dot(wi, h), oh = Dot(wo, h);
+    if (ch <= 0 || ih <= 0 || oh < 1e-10) return 0.0;
+    const double g1 = 1.0 / (1.0 + Lambda(alpha, ci));
+    return g1 * ih * GgxD(alpha, ch) / ci / (4.0 * oh);
+}
+double ConductorF(double cosI, double ni, double nt, double kt)
+{
+    double c = std::fabs(cosI);
+    if (c < 1e-12) c = 1e-12;
+    const double c2 = c * c, s2 = std::max(0.0, 1.0 - c2), s = std::sqrt(s2), tn = s / c;
+    const double ni2 = ni * ni, nt2 = nt * nt, k2 = kt * kt, ns = ni2 * s2, nk = 4.0 * nt2 * k2;
+    double a2 = nt2 - k2 - ns;
+    const double sq = std::sqrt(a2 * a2 + nk);
+    double b2 = sq - nt2 + k2 + ns;
+    a2 = sq + nt2 - k2 - ns;
+    const double dni = 0.5 / ni2;
+    a2 = std::max(0.0, a2 * dni);
+    b2 = std::max(0.0, b2 * dni);
+    const double a = std::sqrt(a2), ab2 = a2 + b2, dcos = 2.0 * a * c, astan = 2.0 * a * s * tn, stan = s2 * tn * tn;
+    const double rs = (ab2 - dcos + c2) / (ab2 + dcos + c2);
+    const double rp = rs * (ab2 - astan + stan) / (ab2 + astan + stan);
+    return 0.5 * (rp + rs);
+}
+
+struct Tables {
+    double ess[32][32];
+    double eavg[32];
+    double glx[21], glw[21];
 };
-struct LTri {
-    V v0, e1, e2;
-    double cdf;
-};
+
+const Tables& GetTables()
+{
+    static Tables T;
+    static std::once_flag once;
+    std::call_once(once, []() {
+        // Gauss-Legendre nodes on [0, 1].
+        const int n = 21;
+        for (int i = 0; i < n; ++i) {
+            double z = std::cos(kPi * (i + 0.75) / (n + 0.5));
+            for (int it = 0; it < 100; ++it) {
+                double p0 = 1.0, p1 = z;
+                for (int k = 2; k <= n; ++k) { const double p2 = ((2.0 * k - 1.0) * z * p1 - (k - 1.0) * p0) / k; p0 = p1; p1 = p2; }
+                const double dp = n * (z * p1 - p0) / (z * z - 1.0);
+                const double dz = p1 / dp;
+                z -= dz;
+                if (std::fabs(dz) < 1e-15) break;
+            }
+            double p0 = 1.0, p1 = z;
+            for (int k = 2; k <= n; ++k) { const double p2 = ((2.0 * k - 1.0) * z * p1 - (k - 1.0) * p0) / k; p0 = p1; p1 = p2; }
+            const double dp = n * (z * p1 - p0) / (z * z - 1.0);
+            T.glx[i] = 0.5 * (z + 1.0);
+            T.glw[i] = 1.0 / ((1.0 - z * z) * dp * dp);
+        }
+        // E_ss(mu, alpha) by stratified visible-normal integration.
+        for (int a = 0; a < 32; ++a) {
+            const double alpha = 0.01 + 0.99 * a / 31.0;
+            double avg = 0.0;
+            for (int c = 0; c < 32; ++c) {
+                const double mu = (c + 0.5) / 32.0;
+                const V wo = {std::sqrt(std::max(0.0, 1.0 - mu * mu)), 0.0, mu};
+                const double g1o = 1.0 / (1.0 + Lambda(alpha, mu));
+                double sum = 0.0;
+                for (int i = 0; i < 64; ++i)
+                    for (int j = 0; j < 64; ++j) {
+                        const V m = VndfLocal(wo, alpha, (i + 0.5) / 64.0, (j + 0.5) / 64.0);
+                        const double d = Dot(wo, m);
+                        if (d <= 0) continue;
+                        const V wi = m * (2.0 * d) - wo;
+                        if (wi.z <= 0) continue;
+                        sum += (1.0 / (1.0 + Lambda(alpha, mu) + Lambda(alpha, wi.z))) / g1o;
+                    }
+                T.ess[a][c] = sum / 4096.0;
+                avg += T.ess[a][c] * mu;
+            }
+            T.eavg[a] = 2.0 * avg / 32.0;
+        }
+    });
+    return T;
+}
+
+double LookupEss(double cosT, double alpha)
+{
+    const Tables& T = GetTables();
+    const double a = std::max(0.0, std::min(1.0, (alpha - 0.01) / 0.99)) * 31.0;
+    const int a0 = (int)a, a1 = std::min(a0 + 1, 31);
+    const double af = a - a0;
+    double c = std::max(0.0, std::min(1.0, cosT)) * 32.0 - 0.5;
+    if (c < 0) c = 0;
+    const int c0 = (int)c, c1 = std::min(c0 + 1, 31);
+    const double cf = c - c0;
+    return (1 - af) * ((1 - cf) * T.ess[a0][c0] + cf * T.ess[a0][c1]) + af * ((1 - cf) * T.ess[a1][c0] + cf * T.ess[a1][c1]);
+}
+double LookupEavg(double alpha)
+{
+    const Tables& T = GetTables();
+    const double a = std::max(0.0, std::min(1.0, (alpha - 0.01) / 0.99)) * 31.0;
+    const int a0 = (int)a, a1 = std::min(a0 + 1, 31);
+    const double af = a - a0;
+    return (1 - af) * T.eavg[a0] + af * T.eavg[a1];
+}
+double FresnelAvg(double ni, double nt, double kt)
+{
+    const Tables& T = GetTables();
+    double s = 0.0;
+    for (int i = 0; i < 21; ++i) s += ConductorF(T.glx[i], ni, nt, kt) * 2.0 * T.glx[i] * T.glw[i];
+    return s;
+}
+double Fms(double favg, double eavg)
+{
+    const double den = 1.0 - favg * (1.0 - eavg);
+    return den < 1e-10 ? 0.0 : favg * favg * eavg / den;
+}
+
+struct Ggx { double alpha, spec, eta, k, favg; };
+
+struct Light { int first, count, emit; double area, pdf; };
+struct LTri { V v0, e1, e2; double cdf; };
 
 struct Scene {
     const float* tri9;
@@ -100,7 +256,6 @@ inline bool Interp(double nm, int& i, int& j, double& w)
     w = x - i;
     return true;
 }
-
 inline double Spec(const Scene& S, int id, double nm)
 {
     int i, j;
@@ -109,8 +264,71 @@ inline double Spec(const Scene& S, int id, double nm)
     const float* s = S.spectra + 81 * (size_t)id;
     return (double)s[i] + w * ((double)s[j] - (double)s[i]);
 }
-
 inline double PowerHeuristic(double a, double b) { return a * a / (a * a + b * b); }
+
+Ggx GgxAt(const Scene& S, int mat, double lam)
+{
+    Ggx g;
+    g.alpha = std::max((double)S.mf[2 * mat], 1e-4);
+    const int refl = S.mi[5 * mat + 1], eta = S.mi[5 * mat + 3], kap = S.mi[5 * mat + 4];
+    g.spec = refl >= 0 ? Spec(S, refl, lam) : 1.0;
+    g.eta = eta >= 0 ? Spec(S, eta, lam) : (double)S.mf[2 * mat + 1];
+    g.k = kap >= 0 ? Spec(S, kap, lam) : 0.0;
+    g.favg = FresnelAvg(1.0, g.eta, g.k);
+    return g;
+}
+
+// GGXBRDF::valueNM (r towards the viewer, v towards the light).
+double GgxValue(const Ggx& g, V n, V gn, V r, V v)
+{
+    const double nr = Dot(n, r), nv = Dot(n, v);
+    if (nr < kNearZero || nv < kNearZero) return 0.0;
+    if (Dot(v, gn) <= 0 || Dot(r, gn) <= 0) return 0.0;
+    const V h = Norm(v + r);
+    const double G2 = 1.0 / (1.0 + Lambda(g.alpha, nv) + Lambda(g.alpha, nr));
+    double f = 0.0;
+    const double sf = GgxD(g.alpha, Dot(h, n)) * G2 / (4.0 * nv * nr);
+    if (sf > 0) f = g.spec * ConductorF(Dot(r, h), 1.0, g.eta, g.k) * sf;
+    const double eavg = LookupEavg(g.alpha);
+    if (1.0 - eavg > 1e-10)
+        f += Fms(g.spec * g.favg, eavg) * (1.0 - LookupEss(nr, g.alpha)) * (1.0 - LookupEss(nv, g.alpha)) / (kPi * (1.0 - eavg));
+    return f;
+}
+double GgxPdf(const Ggx& g, V n, V gn, V r, V v)
+{
+    const double cv = Dot(v, n);
+    if (cv <= 0 || Dot(v, gn) <= 0) return 0.0;
+    const double ws = g.spec, wms = ws * (1.0 - LookupEss(Dot(r, n), g.alpha)), total = ws + wms;
+    if (total <= 1e-10) return 0.0;
+    return (wms * cv * kInvPi + ws * VndfPdf(r, v, n, g.alpha)) / total;
+}
+
+void EvalBsdf(const Scene& S, int mat, double lam, V ns, V gn, V r, V v, double& f, double& pdf)
+{
+    if (S.mi[5 * mat] == 1) {
+        const V n = Dot(r, ns) < 0 ? -ns : ns;
+        const Ggx g = GgxAt(S, mat, lam);
+        f = GgxValue(g, n, gn, r, v);
+        pdf = GgxPdf(g, n, gn, r, v);
+    } else {
+        const double nr = Dot(ns, r), nv = Dot(ns, v);
+        const bool same = (nr >= kNearZero && nv >= kNearZero) || (nr <= -kNearZero && nv <= -kNearZero);
+        const bool gate = Dot(v, gn) > 0 && Dot(r, gn) > 0;
+        f = (same && gate) ? Spec(S, S.mi[5 * mat + 1], lam) * kInvPi : 0.0;
+        pdf = (same && gate) ? std::fabs(nv) * kInvPi : 0.0;
+    }
+}
+
+double DielectricR(double cosI, double cosT, double ni, double nt)
+{
+    const double nn = ni * nt, cc = cosT * cosI, ni2 = ni * ni, nt2 = nt * nt;
+    const double ci2 = cosI * cosI, ct2 = cosT * cosT, nit = ni2 - nt2, cit = ci2 - ct2;
+    const double num = nit * nit * cc * cc + cit * cit * nn * nn;
+    double den = cc * (ni2 + nt2) + nn * (ci2 + ct2);
+    den *= den;
+    if (den < 1e-6 && num < 1e-6) return 1.0;
+    return std::min(1.0, num / den);
+}
 
 void Sample(const Scene& S, uint32_t pixel, uint32_t sample, double xyz[3])
 {
@@ -136,21 +354,24 @@ void Sample(const Scene& S, uint32_t pixel, uint32_t sample, double xyz[3])
         double t;
         const int prim = orc_closest_d(S.bvh, od, dd, &t);
         if (prim < 0) {
-            if (S.env >= 0 && (depth > 0 || S.envVisible))
-                for (int k = 0; k < 4; ++k) L[k] += thr[k] * Spec(S, S.env, lam[k]);
+            if (S.env >= 0 && (depth > 0 || S.envVisible)) {
+                const double w = bsdfPdf > 0 ? PowerHeuristic(bsdfPdf, kInv4Pi) : 1.0;
+                for (int k = 0; k < 4; ++k) L[k] += thr[k] * Spec(S, S.env, lam[k]) * w;
+            }
             break;
         }
         const V p = o + d * t;
         const float* tv = S.tri9 + 9 * (size_t)prim;
         const V a = {tv[0], tv[1], tv[2]}, b = {tv[3], tv[4], tv[5]}, c = {tv[6], tv[7], tv[8]};
-        V ng = Norm(Cross(b - a, c - a));
+        const V nface = Norm(Cross(b - a, c - a));
+        V ng = nface;
         const int mesh = S.triMesh[prim];
         const int mat = (int)S.meshes[4 * mesh + 2];
         const bool ds = S.meshes[4 * mesh + 3] != 0;
         const int light = S.meshLight[mesh];
         if (ds && Dot(ng, d) > 0) ng = -ng;
+        const V gnv = Dot(ng, d) < 0 ? ng : -ng;
         const int type = S.mi[5 * mat], refl = S.mi[5 * mat + 1], emit = S.mi[5 * mat + 2];
-        // Emission with MIS (:4424-4518).
         if (emit >= 0 && Dot(-d, ng) > 0) {
             double w = 1.0;
             if (bsdfPdf > 0 && light >= 0) {
@@ -160,66 +381,136 @@ void Sample(const Scene& S, uint32_t pixel, uint32_t sample, double xyz[3])
             }
             for (int k = 0; k < 4; ++k) L[k] += thr[k] * Spec(S, emit, lam[k]) * w;
         }
-        if (type != 0) break;
-        const V ns = ng;
-        const double viewCos = Dot(-d, ns);
-        // NEE (LightSampler.cpp:2083-2271), one light sample per wavelength
-        // (PathTracingIntegrator.cpp:4528-4549) or one shared sample.
-        if (!S.lights.empty() && viewCos > kNearZero) {
+        double kray[4] = {0, 0, 0, 0};
+        V nd;
+        double npdf = 0.0;
+        if (type == 2) {
+            // Smooth dielectric (DielectricSPF.cpp:120-300); constant index:
+            // the wavelength bundle continues together.
+            const double ior = S.mf[2 * mat + 1];
+            const bool entering = Dot(d, nface) < 0;
+            const V nn = entering ? nface : -nface;
+            const double n1 = entering ? 1.0 : ior, n2 = entering ? ior : 1.0;
+            const double cosI = -Dot(d, nn), eta = n1 / n2;
+            const double s2t = eta * eta * std::max(0.0, 1.0 - cosI * cosI);
+            double R = 1.0;
+            V tdir = {0, 0, 0};
+            if (s2t < 1.0) {
+                const double cosT = std::sqrt(1.0 - s2t);
+                tdir = Norm(d * eta + nn * (eta * cosI - cosT));
+                R = DielectricR(cosI, cosT, n1, n2);
+            }
+            nd = Rand(key, Dim(depth, 18)) < R ? Norm(d + nn * (2.0 * cosI)) : tdir;
+            for (double& k : kray) k = 1.0;
+        } else {
+            const V ns = ng, r = -d;
             const int nsamp = S.neePerLambda ? 4 : 1;
             for (int k = 0; k < nsamp; ++k) {
-                const double ul = Rand(key, Dim(depth, 4 * k));
-                int li = 0;
-                double acc = 0.0;
-                for (li = 0; li < (int)S.lights.size() - 1; ++li) {
-                    acc += S.lights[li].pdf;
-                    if (ul < acc) break;
+                if (!S.lights.empty()) {
+                    const double ul = Rand(key, Dim(depth, 4 * k));
+                    int li = 0;
+                    double acc = 0.0;
+                    for (li = 0; li < (int)S.lights.size() - 1; ++li) {
+                        acc += S.lights[li].pdf;
+                        if (ul < acc) break;
+                    }
+                    if (li != light) {
+                        const Light& lg = S.lights[li];
+                        const double ux = Rand(key, Dim(depth, 4 * k + 1)), uy = Rand(key, Dim(depth, 4 * k + 2)),
+                                     uz = Rand(key, Dim(depth, 4 * k + 3));
+                        int ts = lg.first + lg.count - 1;
+                        for (int q = lg.first; q < lg.first + lg.count; ++q)
+                            if (S.ltris[q].cdf >= uz) { ts = q; break; }
+                        const LTri& lt = S.ltris[ts];
+                        const double sa = std::sqrt(1.0 - ux);
+                        const V pl = lt.v0 + lt.e1 * (1.0 - sa) + lt.e2 * (sa * uy);
+                        const V nl = Norm(Cross(lt.e1, lt.e2));
+                        V toL = pl - p;
+                        const double dist = std::sqrt(Dot(toL, toL));
+                        toL = toL * (1.0 / dist);
+                        const double cosS = Dot(toL, ns), cosL = Dot(-toL, nl);
+                        const double pd[3] = {p.x, p.y, p.z}, ld[3] = {toL.x, toL.y, toL.z};
+                        if (cosL > 0 && cosS > 0 && !orc_any_d(S.bvh, pd, ld, dist - 0.001)) {
+                            const double geom = lg.area * cosL / (dist * dist);
+                            const double plight = lg.pdf * dist * dist / (lg.area * cosL);
+                            for (int j = 0; j < 4; ++j) {
+                                if (S.neePerLambda && j != k) continue;
+                                double f, pb;
+                                EvalBsdf(S, mat, lam[j], ns, gnv, r, toL, f, pb);
+                                const double w = (pb > 0 ? PowerHeuristic(plight, pb) : 1.0) / lg.pdf;
+                                L[j] += thr[j] * Spec(S, lg.emit, lam[j]) * cosS * geom * f * w;
+                            }
+                        }
+                    }
                 }
-                if (li == light) continue;
-                const Light& lg = S.lights[li];
-                const double ux = Rand(key, Dim(depth, 4 * k + 1)), uy = Rand(key, Dim(depth, 4 * k + 2)),
-                             uz = Rand(key, Dim(depth, 4 * k + 3));
-                int ts = lg.first + lg.count - 1;
-                for (int q = lg.first; q < lg.first + lg.count; ++q)
-                    if (S.ltris[q].cdf >= uz) { ts = q; break; }
-                const LTri& lt = S.ltris[ts];
-                const double sa = std::sqrt(1.0 - ux);
-                const double alpha = 1.0 - sa, beta = sa * uy;
-                const V pl = lt.v0 + lt.e1 * alpha + lt.e2 * beta;
-                const V nl = Norm(Cross(lt.e1, lt.e2));
-                V toL = pl - p;
-                const double dist = std::sqrt(Dot(toL, toL));
-                toL = toL * (1.0 / dist);
-                const double cosS = Dot(toL, ns), cosL = Dot(-toL, nl);
-                if (cosL <= 0 || cosS <= 0) continue;
-                const double pd[3] = {p.x, p.y, p.z}, ld[3] = {toL.x, toL.y, toL.z};
-                if (orc_any_d(S.bvh, pd, ld, dist - 0.001)) continue;
-                const double geom = lg.area * cosL / (dist * dist);
-                const double w = PowerHeuristic(lg.pdf * dist * dist / (lg.area * cosL), cosS * kInvPi) / lg.pdf;
-                for (int j = 0; j < 4; ++j) {
-                    if (S.neePerLambda && j != k) continue;
-                    L[j] += thr[j] * Spec(S, lg.emit, lam[j]) * cosS * geom * Spec(S, refl, lam[j]) * kInvPi * w;
+                if (S.env >= 0) {
+                    const double u1 = Rand(key, Dim(depth, 20 + 2 * k)), u2 = Rand(key, Dim(depth, 21 + 2 * k));
+                    const double z = 1.0 - 2.0 * u1, rr = std::sqrt(std::max(0.0, 1.0 - z * z));
+                    const V dir = {rr * std::cos(2.0 * kPi * u2), rr * std::sin(2.0 * kPi * u2), z};
+                    const double cosE = Dot(dir, ns);
+                    const double pd[3] = {p.x, p.y, p.z}, ed[3] = {dir.x, dir.y, dir.z};
+                    if (cosE > 0 && !orc_any_d(S.bvh, pd, ed, 1e300)) {
+                        for (int j = 0; j < 4; ++j) {
+                            if (S.neePerLambda && j != k) continue;
+                            double f, pb;
+                            EvalBsdf(S, mat, lam[j], ns, gnv, r, dir, f, pb);
+                            const double w = pb > 0 ? PowerHeuristic(kInv4Pi, pb) : 1.0;
+                            L[j] += thr[j] * Spec(S, S.env, lam[j]) * f * cosE / kInv4Pi * w;
+                        }
+                    }
                 }
             }
+            const V w = Dot(d, ns) > kNearZero ? -ns : ns;
+            const V gn = gnv;
+            V tx, ty;
+            Frame(w, tx, ty);
+            const double u1 = Rand(key, Dim(depth, 16)), u2 = Rand(key, Dim(depth, 17));
+            if (type == 1) {
+                const Ggx g0 = GgxAt(S, mat, lam[0]);
+                const double cosR = Dot(r, w);
+                const double ws = g0.spec, wms = ws * (1.0 - LookupEss(cosR, g0.alpha)), total = ws + wms;
+                if (!(total > 1e-10)) break;
+                const double pSpec = ws / total, pMS = wms / total;
+                double khero;
+                if (Rand(key, Dim(depth, 18)) < pSpec) {
+                    const V wl = {Dot(r, tx), Dot(r, ty), Dot(r, w)};
+                    const V ml = VndfLocal(wl, g0.alpha, u1, u2);
+                    const V mh = Norm(tx * ml.x + ty * ml.y + w * ml.z);
+                    const double rm = Dot(r, mh);
+                    if (!(rm > 0)) break;
+                    nd = Norm(mh * (2.0 * rm) - r);
+                    const double cosO = Dot(nd, w);
+                    if (!(cosO > 0 && Dot(nd, gn) > 0)) break;
+                    const double vpdf = VndfPdf(r, nd, w, g0.alpha);
+                    if (!(vpdf > 1e-10)) break;
+                    npdf = (wms * cosO * kInvPi + ws * vpdf) / total;
+                    const double G2 = 1.0 / (1.0 + Lambda(g0.alpha, cosR) + Lambda(g0.alpha, cosO));
+                    const double G1 = 1.0 / (1.0 + Lambda(g0.alpha, cosR));
+                    khero = g0.spec * ConductorF(rm, 1.0, g0.eta, g0.k) * G2 / (G1 * pSpec);
+                } else {
+                    const double phi = 2.0 * kPi * u1, sint = std::sqrt(u2), cost = std::sqrt(1.0 - u2);
+                    nd = Norm(tx * (std::cos(phi) * sint) + ty * (std::sin(phi) * sint) + w * cost);
+                    const double cosO = Dot(nd, w);
+                    if (!(cosO > 0 && Dot(nd, gn) > 0) || !(pMS > 1e-10)) break;
+                    npdf = (wms * cosO * kInvPi + ws * VndfPdf(r, nd, w, g0.alpha)) / total;
+                    const double eavg = LookupEavg(g0.alpha);
+                    if (!(1.0 - eavg > 1e-10)) break;
+                    const double fms = Fms(g0.spec * g0.favg, eavg) * (1.0 - LookupEss(cosO, g0.alpha)) *
+                                       (1.0 - LookupEss(cosR, g0.alpha)) / (kPi * (1.0 - eavg));
+                    khero = fms * kPi / pMS;
+                }
+                if (!(npdf > 0)) break;
+                kray[0] = khero;
+                const double cosV = std::fabs(Dot(nd, ns));
+                for (int k = 1; k < 4; ++k) kray[k] = GgxValue(GgxAt(S, mat, lam[k]), w, gnv, r, nd) * cosV / npdf;
+            } else {
+                const double phi = 2.0 * kPi * u1, sint = std::sqrt(u2), cost = std::sqrt(1.0 - u2);
+                nd = Norm(tx * (std::cos(phi) * sint) + ty * (std::sin(phi) * sint) + w * cost);
+                npdf = std::fabs(Dot(nd, w)) * kInvPi;
+                if (!(Dot(nd, gn) > 0)) break;
+                for (int k = 0; k < 4; ++k) kray[k] = Spec(S, refl, lam[k]);
+            }
         }
-        // Hero BSDF sample (:4597-4719).
-        const double u1 = Rand(key, Dim(depth, 16)), u2 = Rand(key, Dim(depth, 17));
-        const V w = Dot(d, ns) > kNearZero ? -ns : ns;
-        // The cosine lobe is symmetric about w, so any frame gives the same
-        // distribution; the device's frame (Duff et al., JCGT 6(1), 2017) is
-        // used so that equal random numbers give equal directions.
-        const double sg = std::copysign(1.0, w.z);
-        const double ia = -1.0 / (sg + w.z);
-        const double bb = w.x * w.y * ia;
-        const V tx = {1.0 + sg * w.x * w.x * ia, sg * bb, -sg * w.x};
-        const V ty = {bb, sg + w.y * w.y * ia, -w.y};
-        const double phi = 2.0 * kPi * u1, sint = std::sqrt(u2), cost = std::sqrt(1.0 - u2);
-        const V nd = Norm(tx * (std::cos(phi) * sint) + ty * (std::sin(phi) * sint) + w * cost);
-        const double pdf = std::fabs(Dot(nd, w)) * kInvPi;
-        const V gn = Dot(ng, d) < 0 ? ng : -ng;
-        if (!(Dot(nd, gn) > 0)) break;
-        double kray[4];
-        for (int k = 0; k < 4; ++k) kray[k] = Spec(S, refl, lam[k]);
         double prevMax = 0, currMax = 0;
         for (int k = 0; k < 4; ++k) {
             prevMax = std::max(prevMax, std::fabs(thr[k]));
@@ -234,7 +525,7 @@ void Sample(const Scene& S, uint32_t pixel, uint32_t sample, double xyz[3])
         }
         if (depth + 1 >= S.maxDepth) break;
         for (int k = 0; k < 4; ++k) thr[k] *= kray[k];
-        bsdfPdf = pdf;
+        bsdfPdf = npdf;
         o = p + nd * 1e-8;   // Ray::Advance(1e-8), PathTracingIntegrator.cpp:4812
         d = nd;
     }
@@ -263,7 +554,7 @@ extern "C" int orc_pt_render(const float* tri9, int64_t n_tri, const int64_t* me
                              int32_t x1, int32_t y1, int32_t threads, double* xyz, const double* cie)
 {
     (void)n_spec;
-    (void)mats_f;
+    GetTables();
     Scene S;
     S.tri9 = tri9;
     S.meshes = meshes;
@@ -282,8 +573,6 @@ extern "C" int orc_pt_render(const float* tri9, int64_t n_tri, const int64_t* me
     S.rrMinDepth = seti[3];
     S.neePerLambda = seti[4];
     S.seed = (uint32_t)seti[5];
-    // (b - a) / k_y with k_y the trapezoid integral over whole 5 nm cells
-    // (ColorUtils.cpp:327-348).
     {
         const double lo = std::max(S.lmin, 380.0), hi = std::min(S.lmax, 780.0);
         const int f = (int)((lo - 380.0) / 5.0), l = (int)((hi - 380.0) / 5.0);
@@ -291,7 +580,6 @@ extern "C" int orc_pt_render(const float* tri9, int64_t n_tri, const int64_t* me
         for (int i = f; i < l; ++i) ky += 0.5 * (cie[81 + i] + cie[81 + i + 1]) * 5.0;
         S.ynorm = ky > 0 ? (S.lmax - S.lmin) / ky : 0.0;
     }
-    // Camera frame: forward, right = forward x up, true up = right x forward.
     const V pos = {cam[0], cam[1], cam[2]}, look = {cam[3], cam[4], cam[5]}, upv = {cam[6], cam[7], cam[8]};
     const V f = Norm(look - pos);
     const V r = Norm(Cross(f, upv));

@@ -1,0 +1,20 @@
+// ggx_tables.h -- host-side GGX energy tables and conductor Fresnel.
+#pragma once
+
+namespace rtb200 {
+
+constexpr int kGgxLut = 32;
+
+struct GgxTables {
+    float ess[kGgxLut * kGgxLut];  // [alpha][mu]
+    float eavg[kGgxLut];
+};
+
+// Computed once per process (thread-safe).
+const GgxTables& GetGgxTables();
+// Unpolarised conductor Fresnel reflectance at |cos| of the incidence angle.
+double ConductorFresnel(double cosI, double ni, double nt, double kt);
+// 2 * integral over [0, 1] of ConductorFresnel(mu) mu dmu (21-point Gauss-Legendre).
+double ConductorFresnelAvg(double ni, double nt, double kt);
+
+}  // namespace rtb200

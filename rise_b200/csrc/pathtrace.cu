@@ -10,163 +10,25 @@
 // launches over device-side queues (no host round trip):
 //   KRegen   splat finished paths into the film, start new camera samples
 //   KExtend  closest hit for every active path (warp while-while traversal)
-//   KShade   emission + MIS, next-event estimation (shadow-ray queue),
-//            hero-wavelength BSDF sampling, Russian roulette
+//   KShade   emission + MIS, next-event estimation to area lights and the
+//            sky (shadow-ray queue), hero-wavelength BSDF sampling with
+//            companion-wavelength weights, Russian roulette
 //   KConnect any hit for the shadow-ray queue; unoccluded contributions are
 //            added to the path's per-wavelength radiance
 //   KSwap    rotate queue counters
 // Appends to queues are warp-aggregated (one atomic per warp).
 #include <cfloat>
 
-#include "cie1931.h"
+#include "bsdf.cuh"
 #include "core.h"
 #include "pathtrace.h"
+#include "pt_device.cuh"
 #include "raycast.cuh"
 
 namespace rtb200 {
 
-__constant__ float c_cie[3][RTB200_CIE_COUNT] = {{RTB200_CIE_XBAR}, {RTB200_CIE_YBAR}, {RTB200_CIE_ZBAR}};
-
-constexpr float kPi = 3.14159265358979323846f;
-constexpr float kInvPi = 0.31830988618379067154f;
-constexpr float kNearZero = 1e-12f;   // NEARZERO, Utilities/Math3D/Constants.h:33
 constexpr int kShadeBlock = 256;
-
-// ---- random numbers --------------------------------------------------------
-// Counter-based: every number is a hash of (seed, pixel, sample, dimension),
-// so the oracle draws the identical sequence on the CPU.
-
-__device__ __forceinline__ uint32_t Mix32(uint32_t x)
-{
-    x ^= x >> 16; x *= 0x7feb352du;
-    x ^= x >> 15; x *= 0x846ca68bu;
-    x ^= x >> 16;
-    return x;
-}
-
-__device__ __forceinline__ uint32_t PathKey(uint32_t seed, uint32_t pixel, uint32_t sample)
-{
-    return Mix32(Mix32(seed ^ 0x9e3779b9u ^ Mix32(pixel)) ^ sample);
-}
-
-__device__ __forceinline__ float Rand(uint32_t key, uint32_t dim)
-{
-    return (float)(Mix32(key ^ (dim * 0x9e3779b9u + 0x7f4a7c15u)) >> 8) * (1.0f / 16777216.0f);
-}
-
-// Dimension layout: camera jitter 0-1, hero wavelength 2; bounce `depth`
-// uses 8 + 32*depth + j: NEE sample i at j = 4i..4i+3 (light, x, y, triangle),
-// BSDF direction j = 16, 17, lobe selection 18, Russian roulette 19.
-__device__ __forceinline__ uint32_t Dim(int depth, int j) { return 8u + 32u * (uint32_t)depth + (uint32_t)j; }
-
-// ---- spectra ---------------------------------------------------------------
-
-// Linear interpolation on the 5 nm grid (InterpSPDIndices,
-// src/Library/Utilities/Color/ColorUtils.cpp:270-300); 0 outside 380..780 nm.
-__device__ __forceinline__ float Spec(const float* spectra, int id, float nm)
-{
-    if (id < 0 || !(nm >= 380.0f) || nm > 780.0f) return 0.0f;
-    const float x = (nm - 380.0f) * 0.2f;
-    const int i = (int)floorf(x);
-    const int j = i + 1 > 80 ? 80 : i + 1;
-    const float w = x - (float)i;
-    const float* s = spectra + id * RTB200_CIE_COUNT;
-    return s[i] + w * (s[j] - s[i]);
-}
-
-// ColorUtils::XYZFromNM (ColorUtils.cpp:313-325).
-__device__ __forceinline__ bool Cmf(float nm, float& X, float& Y, float& Z)
-{
-    if (!(nm >= 380.0f) || nm > 780.0f) return false;
-    const float x = (nm - 380.0f) * 0.2f;
-    const int i = (int)floorf(x);
-    const int j = i + 1 > 80 ? 80 : i + 1;
-    const float w = x - (float)i;
-    X = c_cie[0][i] + w * (c_cie[0][j] - c_cie[0][i]);
-    Y = c_cie[1][i] + w * (c_cie[1][j] - c_cie[1][i]);
-    Z = c_cie[2][i] + w * (c_cie[2][j] - c_cie[2][i]);
-    return true;
-}
-
-// SampledWavelengths::SampleEquidistant
-// (src/Library/Utilities/Color/SampledWavelengths.h:79-106).
-__device__ __forceinline__ void Wavelengths(float hero, float lmin, float lmax, float lam[4])
-{
-    const float range = lmax - lmin;
-    const float delta = range * 0.25f;
-    lam[0] = hero;
-#pragma unroll
-    for (int i = 1; i < 4; ++i) lam[i] = lmin + fmodf(hero - lmin + (float)i * delta, range);
-}
-
-__device__ __forceinline__ float Get(const float4& v, int i) { return i == 0 ? v.x : (i == 1 ? v.y : (i == 2 ? v.z : v.w)); }
-__device__ __forceinline__ void Set(float4& v, int i, float x)
-{
-    if (i == 0) v.x = x; else if (i == 1) v.y = x; else if (i == 2) v.z = x; else v.w = x;
-}
-
-// ---- small vector helpers --------------------------------------------------
-
-struct V3 { float x, y, z; };
-__device__ __forceinline__ V3 mk(float x, float y, float z) { return {x, y, z}; }
-__device__ __forceinline__ V3 operator+(V3 a, V3 b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
-__device__ __forceinline__ V3 operator-(V3 a, V3 b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
-__device__ __forceinline__ V3 operator*(V3 a, float s) { return {a.x * s, a.y * s, a.z * s}; }
-__device__ __forceinline__ V3 operator-(V3 a) { return {-a.x, -a.y, -a.z}; }
-__device__ __forceinline__ float dot(V3 a, V3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
-__device__ __forceinline__ V3 cross(V3 a, V3 b) { return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x}; }
-__device__ __forceinline__ V3 normalize(V3 a) { return a * rsqrtf(fmaxf(dot(a, a), 1e-30f)); }
-__device__ __forceinline__ V3 xyz(float4 v) { return {v.x, v.y, v.z}; }
-
-// Orthonormal basis around unit n (Duff et al., JCGT 6(1), 2017).
-__device__ __forceinline__ void Basis(V3 n, V3& t, V3& b)
-{
-    const float sign = copysignf(1.0f, n.z);
-    const float a = -1.0f / (sign + n.z);
-    const float c = n.x * n.y * a;
-    t = mk(1.0f + sign * n.x * n.x * a, sign * c, -sign * n.x);
-    b = mk(c, sign + n.y * n.y * a, -n.y);
-}
-
-// Ray origin pushed off the surface on the side of `dir` by a few float ulps
-// (Waechter and Binder, "A Fast and Robust Method for Avoiding
-// Self-Intersection", Ray Tracing Gems, 2019).  The reference advances the
-// origin by 1e-8 along the ray in double precision
-// (PathTracingIntegrator.cpp:4812); in FP32 that step is below one ulp.
-__device__ __forceinline__ V3 OffsetRay(V3 p, V3 ng, V3 dir)
-{
-    const V3 n = dot(dir, ng) >= 0.0f ? ng : -ng;
-    const float kOrigin = 1.0f / 32.0f, kFloat = 1.0f / 65536.0f, kInt = 256.0f;
-    const int ox = (int)(kInt * n.x), oy = (int)(kInt * n.y), oz = (int)(kInt * n.z);
-    const V3 pi = mk(__int_as_float(__float_as_int(p.x) + (p.x < 0 ? -ox : ox)),
-                     __int_as_float(__float_as_int(p.y) + (p.y < 0 ? -oy : oy)),
-                     __int_as_float(__float_as_int(p.z) + (p.z < 0 ? -oz : oz)));
-    return mk(fabsf(p.x) < kOrigin ? p.x + kFloat * n.x : pi.x,
-              fabsf(p.y) < kOrigin ? p.y + kFloat * n.y : pi.y,
-              fabsf(p.z) < kOrigin ? p.z + kFloat * n.z : pi.z);
-}
-
-// PathTransportUtilities::PowerHeuristic (Utilities/PathTransportUtilities.h:251).
-__device__ __forceinline__ float PowerHeuristic(float a, float b)
-{
-    const float a2 = a * a;
-    return a2 / (a2 + b * b);
-}
-
-// ---- warp-aggregated queue append -----------------------------------------
-
-__device__ __forceinline__ int WarpAppend(int* counter, bool pred)
-{
-    const unsigned act = __activemask();
-    const unsigned m = __ballot_sync(act, pred);
-    if (!m) return -1;
-    const int lane = threadIdx.x & 31;
-    const int leader = __ffs(m) - 1;
-    int base = 0;
-    if (lane == leader) base = atomicAdd(counter, __popc(m));
-    base = __shfl_sync(act, base, leader);
-    return pred ? base + __popc(m & ((1u << lane) - 1u)) : -1;
-}
+constexpr float kInv4Pi = 0.07957747154594767f;
 
 // ---- film ------------------------------------------------------------------
 
@@ -321,10 +183,34 @@ KConnect(const NodeT* __restrict__ nodes, PtScene S, PtPaths P, PtQueues Q)
     }
 }
 
-__device__ __forceinline__ void Finish(const PtPaths& P, const PtQueues& Q, int slot, uint4 m, bool& fin)
+__device__ __forceinline__ void PushShadow(const PtQueues& Q, V3 o, V3 d, float tmax, int slot, float4 c)
 {
-    P.meta[slot].z = m.z | kFlagFinishing;
-    fin = true;
+    const int at = WarpAppend(&Q.cnt[kCntShadow], true);
+    ShadowEntry e;
+    e.o = make_float4(o.x, o.y, o.z, tmax);
+    e.d = make_float4(d.x, d.y, d.z, __int_as_float(slot));
+    e.c = c;
+    Q.shadow[at] = e;
+}
+
+// BSDF value and sampling pdf at one wavelength for NEE (Lambertian or GGX).
+__device__ __forceinline__ void EvalBsdf(const PtMaterial& M, const float* spectra, float lam, V3 ns, V3 ng,
+                                         V3 r, V3 v, float& f, float& pdf)
+{
+    if (M.type == kMatGGX) {
+        const V3 n = dot(r, ns) < 0.0f ? -ns : ns;
+        const GgxParams g = GgxAt(M, spectra, lam);
+        f = GgxValue(g, n, ng, r, v);
+        pdf = GgxPdf(g, n, ng, r, v);
+    } else {
+        // LambertianBRDF::valueNM + LambertianSPF::Pdf: same side of the
+        // surface as the viewer (ShouldReflect, LambertianBRDF.cpp:44-75).
+        const float nr = dot(ns, r), nv = dot(ns, v);
+        const bool same = (nr >= kNearZero && nv >= kNearZero) || (nr <= -kNearZero && nv <= -kNearZero);
+        const bool gate = dot(v, ng) > 0.0f && dot(r, ng) > 0.0f;
+        f = (same && gate) ? Spec(spectra, M.refl, lam) * kInvPi : 0.0f;
+        pdf = (same && gate) ? fabsf(nv) * kInvPi : 0.0f;
+    }
 }
 
 __global__ void __launch_bounds__(kShadeBlock)
@@ -347,19 +233,18 @@ KShade(PtScene S, PtPaths P, PtQueues Q, PtJobParams J)
         float lam[4];
         Wavelengths(aux.x, set.lmin, set.lmax, lam);
         const V3 d = xyz(rd);
-        bool fin = false;
         bool cont = false;
-        int nsh = 0;
-        ShadowEntry sh[4];
         const int hslot = __float_as_int(h.y);
 
         do {
             if (hslot < 0) {
-                // Escaped: uniform sky radiance (IntegrateRayHWSS :5076-5120 for the
-                // camera ray, IntegrateFromHitHWSS :4235-4303 for continuations).
+                // Escaped: uniform sky (IntegrateRayHWSS :5076-5120 for camera
+                // rays; :4235-4303 with MIS against sky NEE for continuations).
                 if (set.env >= 0 && (depth > 0 || set.env_visible)) {
+                    const float w = bsdfPdf > 0.0f ? PowerHeuristic(bsdfPdf, kInv4Pi) : 1.0f;
                     for (int k = 0; k < 4; ++k)
-                        if (!(term & (1u << k))) Set(L, k, Get(L, k) + Get(thr, k) * Spec(S.spectra, set.env, lam[k]));
+                        if (!(term & (1u << k)))
+                            Set(L, k, Get(L, k) + Get(thr, k) * Spec(S.spectra, set.env, lam[k]) * w);
                 }
                 break;
             }
@@ -378,12 +263,14 @@ KShade(PtScene S, PtPaths P, PtQueues Q, PtJobParams J)
             const V3 p = xyz(ro) + d * t;
             const float* tb = reinterpret_cast<const float*>(S.tris + hslot);
             const float4 A = ldg4(tb), B = ldg4(tb + 4), C = ldg4(tb + 8);
-            V3 ng = normalize(cross(xyz(B) - xyz(A), xyz(C) - xyz(A)));
+            const V3 nface = normalize(cross(xyz(B) - xyz(A), xyz(C) - xyz(A)));
+            V3 ng = nface;
             const PtTriAttr at = S.attr[hslot];
             const int mi = at.mat & kAttrMatMask;
             // Double-sided meshes face the incoming ray
             // (TriangleMeshGeometryIndexed.cpp:170-188).
             if ((at.mat & kAttrDoubleSided) && dot(ng, d) > 0.0f) ng = -ng;
+            const V3 gnv = dot(ng, d) < 0.0f ? ng : -ng;   // geometric normal facing the ray
             const PtMaterial M = S.mats[mi];
 
             // PART 1: emission with MIS against light sampling (:4424-4518).
@@ -392,99 +279,194 @@ KShade(PtScene S, PtPaths P, PtQueues Q, PtJobParams J)
                 if (bsdfPdf > 0.0f && at.light >= 0) {
                     const PtLight lg = S.lights[at.light];
                     const float cosL = fabsf(dot(d, ng));
-                    if (cosL > 0.0f && lg.area > 0.0f) {
-                        const float pnee = lg.pdf * (t * t) / (lg.area * cosL);
-                        w = PowerHeuristic(bsdfPdf, pnee);
-                    }
+                    if (cosL > 0.0f && lg.area > 0.0f) w = PowerHeuristic(bsdfPdf, lg.pdf * (t * t) / (lg.area * cosL));
                 }
                 for (int k = 0; k < 4; ++k)
                     if (!(term & (1u << k))) Set(L, k, Get(L, k) + Get(thr, k) * Spec(S.spectra, M.emit, lam[k]) * w);
             }
-            if (M.type != kMatLambertian) break;  // other models: see KShade extensions
 
-            // Shading frame: flat triangles shade with the face normal; the
-            // Lambertian SPF samples around the normal on the viewer's side
-            // (LambertianSPF.cpp:90-160).
-            const V3 ns = ng;
-            const float viewCos = dot(-d, ns);
+            float4 kray = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            V3 nd;
+            float npdf = 0.0f;       // continuation pdf for the next emission MIS (0 = delta)
+            unsigned nflags = kFlagConsiderEmission;
 
-            // PART 2: next-event estimation to area lights
-            // (LightSampler::EvaluateDirectLightingNM, LightSampler.cpp:2083-2271).
-            if (set.n_lights > 0 && viewCos > kNearZero) {
+            if (M.type == kMatDielectric) {
+                // Smooth dielectric: Fresnel choice between reflection and
+                // refraction (DielectricSPF.cpp:120-300).  With a constant index
+                // every wavelength follows the hero's direction with the same
+                // weight, so the bundle continues together.
+                const bool entering = dot(d, nface) < 0.0f;
+                const V3 nn = entering ? nface : -nface;
+                const float n1 = entering ? 1.0f : M.ior, n2 = entering ? M.ior : 1.0f;
+                const float cosI = -dot(d, nn);
+                const float eta = n1 / n2;
+                const float s2t = eta * eta * fmaxf(0.0f, 1.0f - cosI * cosI);
+                float R = 1.0f;
+                V3 tdir = mk(0.0f, 0.0f, 0.0f);
+                if (s2t < 1.0f) {
+                    const float cosT = sqrtf(1.0f - s2t);
+                    tdir = normalize(d * eta + nn * (eta * cosI - cosT));
+                    R = DielectricR(cosI, cosT, n1, n2);
+                }
+                if (Rand(key, Dim(depth, 18)) < R) nd = normalize(d + nn * (2.0f * cosI));
+                else nd = tdir;
+                for (int k = 0; k < 4; ++k) Set(kray, k, (term & (1u << k)) ? 0.0f : 1.0f);
+                nflags |= kFlagSpecular;
+            } else {
+                const V3 ns = ng;
+                const V3 r = -d;
+                // PART 2: next-event estimation (LightSampler::EvaluateDirectLightingNM,
+                // LightSampler.cpp:1942-2361): one area-light sample and one sky
+                // sample per wavelength (reference) or one shared sample.
                 const int nsamp = set.nee_per_lambda ? 4 : 1;
                 for (int k = 0; k < nsamp; ++k) {
                     if (set.nee_per_lambda && (term & (1u << k))) continue;
-                    const float ul = Rand(key, Dim(depth, 4 * k + 0));
-                    int li = 0;
-                    {
-                        float acc = 0.0f;
-                        for (li = 0; li < set.n_lights - 1; ++li) {
-                            acc += S.lights[li].pdf;
-                            if (ul < acc) break;
+                    if (set.n_lights > 0) {
+                        const float ul = Rand(key, Dim(depth, 4 * k + 0));
+                        int li = 0;
+                        {
+                            float acc = 0.0f;
+                            for (li = 0; li < set.n_lights - 1; ++li) {
+                                acc += S.lights[li].pdf;
+                                if (ul < acc) break;
+                            }
+                        }
+                        if (li != at.light) {   // no self-illumination
+                            const PtLight lg = S.lights[li];
+                            const float ux = Rand(key, Dim(depth, 4 * k + 1));
+                            const float uy = Rand(key, Dim(depth, 4 * k + 2));
+                            const float uz = Rand(key, Dim(depth, 4 * k + 3));
+                            // First triangle whose area CDF reaches uz (std::lower_bound).
+                            int tsel = lg.first + lg.count - 1;
+                            for (int q = lg.first; q < lg.first + lg.count; ++q)
+                                if (S.light_tris[q].cdf >= uz) { tsel = q; break; }
+                            const PtLightTri lt = S.light_tris[tsel];
+                            // GeometricUtilities::PointOnTriangle (GeometricUtilities.cpp:543-569).
+                            const float sa = sqrtf(1.0f - ux);
+                            const float alpha = 1.0f - sa, beta = sa * uy;
+                            const V3 e1 = mk(lt.e1[0], lt.e1[1], lt.e1[2]), e2 = mk(lt.e2[0], lt.e2[1], lt.e2[2]);
+                            const V3 pl = mk(lt.v0[0], lt.v0[1], lt.v0[2]) + e1 * alpha + e2 * beta;
+                            const V3 nl = normalize(cross(e1, e2));
+                            V3 toL = pl - p;
+                            const float dist = sqrtf(dot(toL, toL));
+                            toL = toL * (1.0f / dist);
+                            const float cosS = dot(toL, ns);
+                            const float cosL = dot(-toL, nl);
+                            if (cosL > 0.0f && cosS > 0.0f) {
+                                const float geom = lg.area * cosL / (dist * dist);
+                                const float plight = lg.pdf * (dist * dist) / (lg.area * cosL);
+                                float4 c = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+                                bool any = false;
+                                for (int j = 0; j < 4; ++j) {
+                                    if (term & (1u << j)) continue;
+                                    if (set.nee_per_lambda && j != k) continue;
+                                    float f, pb;
+                                    EvalBsdf(M, S.spectra, lam[j], ns, gnv, r, toL, f, pb);
+                                    const float w = (pb > 0.0f ? PowerHeuristic(plight, pb) : 1.0f) / lg.pdf;
+                                    const float v = Get(thr, j) * Spec(S.spectra, lg.emit, lam[j]) * cosS * geom * f * w;
+                                    Set(c, j, v);
+                                    any |= v != 0.0f;
+                                }
+                                if (any) PushShadow(Q, OffsetRay(p, ng, toL), toL, dist - 0.001f, slot, c);
+                            }
                         }
                     }
-                    if (li == at.light) continue;   // no self-illumination
-                    const PtLight lg = S.lights[li];
-                    const float ux = Rand(key, Dim(depth, 4 * k + 1));
-                    const float uy = Rand(key, Dim(depth, 4 * k + 2));
-                    const float uz = Rand(key, Dim(depth, 4 * k + 3));
-                    // First triangle whose area CDF reaches uz (std::lower_bound).
-                    int tsel = lg.first + lg.count - 1;
-                    for (int q = lg.first; q < lg.first + lg.count; ++q)
-                        if (S.light_tris[q].cdf >= uz) { tsel = q; break; }
-                    const PtLightTri lt = S.light_tris[tsel];
-                    // GeometricUtilities::PointOnTriangle (GeometricUtilities.cpp:543-569).
-                    const float sa = sqrtf(1.0f - ux);
-                    const float alpha = 1.0f - sa, beta = sa * uy;
-                    const V3 e1 = mk(lt.e1[0], lt.e1[1], lt.e1[2]), e2 = mk(lt.e2[0], lt.e2[1], lt.e2[2]);
-                    const V3 pl = mk(lt.v0[0], lt.v0[1], lt.v0[2]) + e1 * alpha + e2 * beta;
-                    const V3 nl = normalize(cross(e1, e2));
-                    V3 toL = pl - p;
-                    const float dist = sqrtf(dot(toL, toL));
-                    toL = toL * (1.0f / dist);
-                    const float cosS = dot(toL, ns);
-                    const float cosL = dot(-toL, nl);
-                    if (cosL <= 0.0f || cosS <= 0.0f) continue;
-                    const float geom = lg.area * cosL / (dist * dist);
-                    // MIS: light pdf (solid angle) vs Lambertian pdf cos/pi.
-                    const float plight = lg.pdf * (dist * dist) / (lg.area * cosL);
-                    const float w = PowerHeuristic(plight, cosS * kInvPi) / lg.pdf;
-                    float4 c = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-                    bool any = false;
-                    for (int j = 0; j < 4; ++j) {
-                        if (term & (1u << j)) continue;
-                        if (set.nee_per_lambda && j != k) continue;
-                        const float f = Spec(S.spectra, M.refl, lam[j]) * kInvPi;
-                        const float v = Get(thr, j) * Spec(S.spectra, lg.emit, lam[j]) * cosS * geom * f * w;
-                        Set(c, j, v);
-                        any |= v != 0.0f;
+                    if (set.env >= 0) {
+                        // Uniform-sky NEE: uniform directions, pdf 1/(4 pi)
+                        // (LightSampler.cpp:2277-2359).
+                        const float u1 = Rand(key, Dim(depth, 20 + 2 * k)), u2 = Rand(key, Dim(depth, 21 + 2 * k));
+                        const float z = 1.0f - 2.0f * u1;
+                        const float rr = sqrtf(fmaxf(0.0f, 1.0f - z * z));
+                        float sp, cp;
+                        __sincosf(2.0f * kPi * u2, &sp, &cp);
+                        const V3 dir = mk(rr * cp, rr * sp, z);
+                        const float cosE = dot(dir, ns);
+                        if (cosE > 0.0f) {
+                            float4 c = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+                            bool any = false;
+                            for (int j = 0; j < 4; ++j) {
+                                if (term & (1u << j)) continue;
+                                if (set.nee_per_lambda && j != k) continue;
+                                float f, pb;
+                                EvalBsdf(M, S.spectra, lam[j], ns, gnv, r, dir, f, pb);
+                                const float w = pb > 0.0f ? PowerHeuristic(kInv4Pi, pb) : 1.0f;
+                                const float v = Get(thr, j) * Spec(S.spectra, set.env, lam[j]) * f * cosE / kInv4Pi * w;
+                                Set(c, j, v);
+                                any |= v != 0.0f;
+                            }
+                            if (any) PushShadow(Q, OffsetRay(p, ng, dir), dir, __int_as_float(0x7f800000), slot, c);
+                        }
                     }
-                    if (!any) continue;
-                    const V3 so = OffsetRay(p, ng, toL);
-                    ShadowEntry& e = sh[nsh++];
-                    e.o = make_float4(so.x, so.y, so.z, dist - 0.001f);
-                    e.d = make_float4(toL.x, toL.y, toL.z, __int_as_float(slot));
-                    e.c = c;
+                }
+
+                // PART 3: hero-wavelength BSDF sample (:4597-4719).
+                const V3 w = dot(d, ns) > kNearZero ? -ns : ns;   // viewer side
+                const V3 gn = gnv;
+                V3 tx, ty;
+                Basis(w, tx, ty);
+                const float u1 = Rand(key, Dim(depth, 16)), u2 = Rand(key, Dim(depth, 17));
+                if (M.type == kMatGGX) {
+                    const GgxParams g0 = GgxAt(M, S.spectra, lam[0]);
+                    const float cosR = dot(r, w);
+                    const float ws = g0.spec;
+                    const float wms = ws * (1.0f - LookupEss(cosR, g0.alpha));
+                    const float total = ws + wms;
+                    if (!(total > 1e-10f)) break;
+                    const float pSpec = ws / total, pMS = wms / total;
+                    float khero = 0.0f;
+                    if (Rand(key, Dim(depth, 18)) < pSpec) {
+                        const V3 mh = VndfSample(r, tx, ty, w, g0.alpha, u1, u2);
+                        const float rm = dot(r, mh);
+                        if (!(rm > 0.0f)) break;
+                        nd = normalize(mh * (2.0f * rm) - r);
+                        const float cosO = dot(nd, w);
+                        if (!(cosO > 0.0f && dot(nd, gn) > 0.0f)) break;
+                        const float vpdf = VndfPdf(r, nd, w, g0.alpha);
+                        if (!(vpdf > 1e-10f)) break;
+                        npdf = (wms * cosO * kInvPi + ws * vpdf) / total;
+                        const float G2 = 1.0f / (1.0f + GgxLambda(g0.alpha, cosR) + GgxLambda(g0.alpha, cosO));
+                        const float G1 = 1.0f / (1.0f + GgxLambda(g0.alpha, cosR));
+                        khero = g0.spec * ConductorF(rm, 1.0f, g0.eta, g0.k) * G2 / (G1 * pSpec);
+                    } else {
+                        // Multiple-scattering lobe, cosine-sampled.
+                        const float phi = 2.0f * kPi * u1;
+                        const float sint = sqrtf(u2), cost = sqrtf(1.0f - u2);
+                        float sp, cp;
+                        __sincosf(phi, &sp, &cp);
+                        nd = normalize(tx * (cp * sint) + ty * (sp * sint) + w * cost);
+                        const float cosO = dot(nd, w);
+                        if (!(cosO > 0.0f && dot(nd, gn) > 0.0f) || !(pMS > 1e-10f)) break;
+                        npdf = (wms * cosO * kInvPi + ws * VndfPdf(r, nd, w, g0.alpha)) / total;
+                        const float eavg = LookupEavg(g0.alpha);
+                        if (!(1.0f - eavg > 1e-10f)) break;
+                        const float fms = Fms(g0.spec * g0.favg, eavg) * (1.0f - LookupEss(cosO, g0.alpha)) *
+                                          (1.0f - LookupEss(cosR, g0.alpha)) / (kPi * (1.0f - eavg));
+                        khero = fms * kPi / pMS;   // f cos / (cos/pi) / pMS
+                    }
+                    if (!(npdf > 0.0f)) break;
+                    Set(kray, 0, (term & 1u) ? 0.0f : khero);
+                    const float cosV = fabsf(dot(nd, ns));
+                    // Companions evaluate the BSDF in the hero's direction and
+                    // divide by the hero's pdf (:4676-4714).
+                    for (int k = 1; k < 4; ++k) {
+                        if (term & (1u << k)) continue;
+                        const GgxParams gk = GgxAt(M, S.spectra, lam[k]);
+                        Set(kray, k, GgxValue(gk, w, gnv, r, nd) * cosV / npdf);
+                    }
+                } else {
+                    // Lambertian: cosine-weighted direction, kray = rho(lambda),
+                    // pdf = cos/pi (LambertianSPF.cpp:90-160).
+                    const float phi = 2.0f * kPi * u1;
+                    const float sint = sqrtf(u2), cost = sqrtf(1.0f - u2);
+                    float sp, cp;
+                    __sincosf(phi, &sp, &cp);
+                    nd = normalize(tx * (cp * sint) + ty * (sp * sint) + w * cost);
+                    npdf = fabsf(dot(nd, w)) * kInvPi;
+                    // Geometric-horizon gate (LambertianSPF.cpp:141-151).
+                    if (!(dot(nd, gn) > 0.0f)) break;
+                    for (int k = 0; k < 4; ++k) Set(kray, k, (term & (1u << k)) ? 0.0f : Spec(S.spectra, M.refl, lam[k]));
                 }
             }
-
-            // PART 3: hero-wavelength BSDF sample (:4597-4719): cosine-weighted
-            // direction, krayNM = reflectance(lambda), pdf = cos/pi.
-            const float u1 = Rand(key, Dim(depth, 16)), u2 = Rand(key, Dim(depth, 17));
-            const V3 w = dot(d, ns) > kNearZero ? -ns : ns;
-            V3 tx, ty;
-            Basis(w, tx, ty);
-            const float phi = 2.0f * kPi * u1;
-            const float sint = sqrtf(u2), cost = sqrtf(1.0f - u2);
-            float sp, cp;
-            __sincosf(phi, &sp, &cp);
-            const V3 nd = normalize(tx * (cp * sint) + ty * (sp * sint) + w * cost);
-            const float pdf = fabsf(dot(nd, w)) * kInvPi;
-            // Geometric-horizon gate (LambertianSPF.cpp:141-151).
-            const V3 gn = dot(ng, d) < 0.0f ? ng : -ng;
-            if (!(dot(nd, gn) > 0.0f)) break;
-            float4 kray;
-            for (int k = 0; k < 4; ++k) Set(kray, k, (term & (1u << k)) ? 0.0f : Spec(S.spectra, M.refl, lam[k]));
             // Russian roulette on the max over wavelengths (:4738-4769,
             // PathTransportUtilities.h:86-110).
             float prevMax = 0.0f, currMax = 0.0f;
@@ -504,39 +486,22 @@ KShade(PtScene S, PtPaths P, PtQueues Q, PtJobParams J)
             }
             if (depth + 1 >= set.max_depth) break;
             thr = make_float4(thr.x * kray.x, thr.y * kray.y, thr.z * kray.z, thr.w * kray.w);
-            const V3 no = OffsetRay(p, ng, nd);
+            const V3 no = OffsetRay(p, nface, nd);
             P.ray_o[slot] = make_float4(no.x, no.y, no.z, 0.0f);
             P.ray_d[slot] = make_float4(nd.x, nd.y, nd.z, __int_as_float(0x7f800000));
             P.thr[slot] = thr;
-            P.aux[slot] = make_float4(aux.x, pdf, 0.0f, 0.0f);
-            m.z = (m.z & ~kFlagDepthMask) | (unsigned)(depth + 1) | kFlagConsiderEmission;
+            P.aux[slot] = make_float4(aux.x, npdf, 0.0f, 0.0f);
+            m.z = (m.z & ~(kFlagDepthMask | kFlagSpecular)) | (unsigned)(depth + 1) | nflags;
             P.meta[slot].z = m.z;
             cont = true;
         } while (false);
 
         P.L[slot] = L;
-        if (!cont) Finish(P, Q, slot, m, fin);
+        if (!cont) P.meta[slot].z = m.z | kFlagFinishing;
         const int an = WarpAppend(&Q.cnt[kCntActiveNext], cont);
         if (cont) Q.active_next[an] = slot;
-        const int fn = WarpAppend(&Q.cnt[kCntFreeNext], fin);
-        if (fin) Q.free_next[fn] = slot;
-        // Shadow entries: lanes append their own count.
-        {
-            const unsigned act = __activemask();
-            const int lane = threadIdx.x & 31;
-            int incl = nsh;
-#pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                const int v = __shfl_up_sync(act, incl, o);
-                if (lane >= o && ((act >> (lane - o)) & 1u)) incl += v;
-            }
-            const int leader = 31 - __clz(act);
-            int base = 0;
-            if (lane == leader && incl > 0) base = atomicAdd(&Q.cnt[kCntShadow], incl);
-            base = __shfl_sync(act, base, leader);
-            const int at0 = base + incl - nsh;
-            for (int k = 0; k < nsh; ++k) Q.shadow[at0 + k] = sh[k];
-        }
+        const int fn = WarpAppend(&Q.cnt[kCntFreeNext], !cont);
+        if (!cont) Q.free_next[fn] = slot;
     }
 }
 
@@ -564,7 +529,7 @@ __global__ void KFold(PtFilm F, int n3)
     }
 }
 
-// ---- host launcher ---------------------------------------------------------
+// ---- host launchers ----------------------------------------------------------
 
 namespace {
 template <class K>
@@ -575,6 +540,13 @@ int TraceGrid(K kernel, int sms)
     return per * sms;
 }
 }  // namespace
+
+cudaError_t PtSetGgxTables(const float* ess, const float* eavg)
+{
+    cudaError_t e = cudaMemcpyToSymbol(c_ess, ess, sizeof(float) * kLut * kLut);
+    if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_eavg, eavg, sizeof(float) * kLut);
+    return e;
+}
 
 cudaError_t PtIteration(const PtLaunch& L, cudaStream_t st)
 {

@@ -19,6 +19,8 @@ struct PtLaunch {
 // asynchronous on `st`.  The caller swaps queues.active/active_next and
 // queues.free_/free_next after each call.
 cudaError_t PtIteration(const PtLaunch& L, cudaStream_t st);
+// Upload the GGX E_ss (32 x 32) and E_avg (32) tables to constant memory.
+cudaError_t PtSetGgxTables(const float* ess, const float* eavg);
 // Fold this call's film into the compensated running sums and clear it.
 cudaError_t PtFold(const PtFilm& F, int npix, int sms, cudaStream_t st);
 

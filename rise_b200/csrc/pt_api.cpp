@@ -9,6 +9,7 @@
 
 #include "cie1931.h"
 #include "core.h"
+#include "ggx_tables.h"
 #include "pathtrace.h"
 
 namespace rtb200 {
@@ -55,6 +56,24 @@ int UploadShading(rtb200_scene* s)
     rtb200_ctx* ctx = s->ctx;
     if (s->materials.empty()) return RTB200_OK;  // ray casting only
     const size_t nm = s->materials.size();
+    // GGX conductors: tabulate F_avg(lambda) on the 5 nm grid as an extra
+    // spectrum, and make sure the device holds the E_ss / E_avg tables.
+    for (PtMaterial& m : s->materials) {
+        if (m.type != kMatGGX) continue;
+        std::vector<float> favg(RTB200_CIE_COUNT);
+        for (int k = 0; k < RTB200_CIE_COUNT; ++k) {
+            const double eta = m.eta >= 0 ? s->spectra[(size_t)m.eta * RTB200_CIE_COUNT + k] : m.ior;
+            const double kap = m.kappa >= 0 ? s->spectra[(size_t)m.kappa * RTB200_CIE_COUNT + k] : 0.0;
+            favg[k] = (float)ConductorFresnelAvg(1.0, eta, kap);
+        }
+        m.pad = (int)(s->spectra.size() / RTB200_CIE_COUNT);
+        s->spectra.insert(s->spectra.end(), favg.begin(), favg.end());
+    }
+    {
+        const GgxTables& gt = GetGgxTables();
+        const cudaError_t e = PtSetGgxTables(gt.ess, gt.eavg);
+        if (e != cudaSuccess) return CudaCheck(ctx, e, "GGX tables");
+    }
     for (const auto& mesh : s->meshes)
         if (mesh.material < 0 || (size_t)mesh.material >= nm)
             return SetError(ctx, RTB200_E_INVALID, "mesh material id out of range");
@@ -198,6 +217,7 @@ int rtb200_scene_add_material(rtb200_scene* s, const rtb200_material* m, int32_t
     pm.kappa = m->kappa;
     pm.alpha = m->alpha;
     pm.ior = m->ior;
+    pm.pad = -1;   // conductor Fresnel average spectrum, built at commit
     *id_out = (int32_t)s->materials.size();
     s->materials.push_back(pm);
     return RTB200_OK;
@@ -243,7 +263,7 @@ int rtb200_job_create(rtb200_scene* s, const rtb200_render_settings* rs, rtb200_
     const size_t oRo = take(16 * c), oRd = take(16 * c), oHit = take(16 * c), oThr = take(16 * c), oL = take(16 * c),
                  oAux = take(16 * c), oMeta = take(16 * c);
     const size_t oQa = take(4 * c), oQan = take(4 * c), oQf = take(4 * c), oQfn = take(4 * c), oIota = take(4 * c);
-    const size_t oSh = take(sizeof(ShadowEntry) * 4 * c);
+    const size_t oSh = take(sizeof(ShadowEntry) * 8 * c);   // up to 4 light + 4 sky samples
     const size_t oPass = take(12 * np), oSum = take(12 * np), oComp = take(12 * np);
     const size_t oCnt = take(4 * kCntCount), oU64 = take(8 * 8), oErr = take(4);
     int rc = DevAlloc(ctx, &j->buf, off);

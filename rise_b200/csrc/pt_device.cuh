@@ -1,0 +1,158 @@
+// pt_device.cuh -- device helpers of the spectral path tracer: counter-based
+// random numbers, spectra and CIE lookups, HWSS wavelengths, small vector
+// algebra, ray-origin offsetting, MIS weights and warp-aggregated appends.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "cie1931.h"
+#include "pt_types.h"
+
+namespace rtb200 {
+
+constexpr float kPi = 3.14159265358979323846f;
+constexpr float kInvPi = 0.31830988618379067154f;
+constexpr float kNearZero = 1e-12f;   // NEARZERO, Utilities/Math3D/Constants.h:33
+
+// Defined here: this header is compiled into exactly one translation unit
+// (pathtrace.cu).
+__constant__ float c_cie[3][RTB200_CIE_COUNT] = {{RTB200_CIE_XBAR}, {RTB200_CIE_YBAR}, {RTB200_CIE_ZBAR}};
+
+// ---- random numbers ---------------------------------------------------------
+// Counter-based: every number is a hash of (seed, pixel, sample, dimension),
+// so the oracle draws the identical sequence on the CPU.
+
+__device__ __forceinline__ uint32_t Mix32(uint32_t x)
+{
+    x ^= x >> 16; x *= 0x7feb352du;
+    x ^= x >> 15; x *= 0x846ca68bu;
+    x ^= x >> 16;
+    return x;
+}
+
+__device__ __forceinline__ uint32_t PathKey(uint32_t seed, uint32_t pixel, uint32_t sample)
+{
+    return Mix32(Mix32(seed ^ 0x9e3779b9u ^ Mix32(pixel)) ^ sample);
+}
+
+__device__ __forceinline__ float Rand(uint32_t key, uint32_t dim)
+{
+    return (float)(Mix32(key ^ (dim * 0x9e3779b9u + 0x7f4a7c15u)) >> 8) * (1.0f / 16777216.0f);
+}
+
+// Dimension layout: camera jitter 0-1, hero wavelength 2; bounce `depth`
+// uses 8 + 32*depth + j: light sample i at j = 4i..4i+3 (light, x, y,
+// triangle), BSDF direction j = 16, 17, lobe / Fresnel choice 18, Russian
+// roulette 19, sky sample i at j = 20 + 2i, 21 + 2i.
+__device__ __forceinline__ uint32_t Dim(int depth, int j) { return 8u + 32u * (uint32_t)depth + (uint32_t)j; }
+
+// ---- spectra -----------------------------------------------------------------
+
+// Linear interpolation on the 5 nm grid (InterpSPDIndices,
+// src/Library/Utilities/Color/ColorUtils.cpp:270-300); 0 outside 380..780 nm.
+__device__ __forceinline__ float Spec(const float* spectra, int id, float nm)
+{
+    if (id < 0 || !(nm >= 380.0f) || nm > 780.0f) return 0.0f;
+    const float x = (nm - 380.0f) * 0.2f;
+    const int i = (int)floorf(x);
+    const int j = i + 1 > 80 ? 80 : i + 1;
+    const float w = x - (float)i;
+    const float* s = spectra + id * RTB200_CIE_COUNT;
+    return s[i] + w * (s[j] - s[i]);
+}
+
+// ColorUtils::XYZFromNM (ColorUtils.cpp:313-325).
+__device__ __forceinline__ bool Cmf(float nm, float& X, float& Y, float& Z)
+{
+    if (!(nm >= 380.0f) || nm > 780.0f) return false;
+    const float x = (nm - 380.0f) * 0.2f;
+    const int i = (int)floorf(x);
+    const int j = i + 1 > 80 ? 80 : i + 1;
+    const float w = x - (float)i;
+    X = c_cie[0][i] + w * (c_cie[0][j] - c_cie[0][i]);
+    Y = c_cie[1][i] + w * (c_cie[1][j] - c_cie[1][i]);
+    Z = c_cie[2][i] + w * (c_cie[2][j] - c_cie[2][i]);
+    return true;
+}
+
+// SampledWavelengths::SampleEquidistant
+// (src/Library/Utilities/Color/SampledWavelengths.h:79-106).
+__device__ __forceinline__ void Wavelengths(float hero, float lmin, float lmax, float lam[4])
+{
+    const float range = lmax - lmin;
+    const float delta = range * 0.25f;
+    lam[0] = hero;
+#pragma unroll
+    for (int i = 1; i < 4; ++i) lam[i] = lmin + fmodf(hero - lmin + (float)i * delta, range);
+}
+
+__device__ __forceinline__ float Get(const float4& v, int i) { return i == 0 ? v.x : (i == 1 ? v.y : (i == 2 ? v.z : v.w)); }
+__device__ __forceinline__ void Set(float4& v, int i, float x)
+{
+    if (i == 0) v.x = x; else if (i == 1) v.y = x; else if (i == 2) v.z = x; else v.w = x;
+}
+
+// ---- small vector helpers ---------------------------------------------------
+
+struct V3 { float x, y, z; };
+__device__ __forceinline__ V3 mk(float x, float y, float z) { return {x, y, z}; }
+__device__ __forceinline__ V3 operator+(V3 a, V3 b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
+__device__ __forceinline__ V3 operator-(V3 a, V3 b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+__device__ __forceinline__ V3 operator*(V3 a, float s) { return {a.x * s, a.y * s, a.z * s}; }
+__device__ __forceinline__ V3 operator-(V3 a) { return {-a.x, -a.y, -a.z}; }
+__device__ __forceinline__ float dot(V3 a, V3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+__device__ __forceinline__ V3 cross(V3 a, V3 b) { return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x}; }
+__device__ __forceinline__ V3 normalize(V3 a) { return a * rsqrtf(fmaxf(dot(a, a), 1e-30f)); }
+__device__ __forceinline__ V3 xyz(float4 v) { return {v.x, v.y, v.z}; }
+
+// Orthonormal basis around unit n (Duff et al., JCGT 6(1), 2017).
+__device__ __forceinline__ void Basis(V3 n, V3& t, V3& b)
+{
+    const float sign = copysignf(1.0f, n.z);
+    const float a = -1.0f / (sign + n.z);
+    const float c = n.x * n.y * a;
+    t = mk(1.0f + sign * n.x * n.x * a, sign * c, -sign * n.x);
+    b = mk(c, sign + n.y * n.y * a, -n.y);
+}
+
+// Ray origin pushed off the surface on the side of `dir` by a few float ulps
+// (Waechter and Binder, "A Fast and Robust Method for Avoiding
+// Self-Intersection", Ray Tracing Gems, 2019).  The reference advances the
+// origin by 1e-8 along the ray in double precision
+// (PathTracingIntegrator.cpp:4812); in FP32 that step is below one ulp.
+__device__ __forceinline__ V3 OffsetRay(V3 p, V3 ng, V3 dir)
+{
+    const V3 n = dot(dir, ng) >= 0.0f ? ng : -ng;
+    const float kOrigin = 1.0f / 32.0f, kFloat = 1.0f / 65536.0f, kInt = 256.0f;
+    const int ox = (int)(kInt * n.x), oy = (int)(kInt * n.y), oz = (int)(kInt * n.z);
+    const V3 pi = mk(__int_as_float(__float_as_int(p.x) + (p.x < 0 ? -ox : ox)),
+                     __int_as_float(__float_as_int(p.y) + (p.y < 0 ? -oy : oy)),
+                     __int_as_float(__float_as_int(p.z) + (p.z < 0 ? -oz : oz)));
+    return mk(fabsf(p.x) < kOrigin ? p.x + kFloat * n.x : pi.x,
+              fabsf(p.y) < kOrigin ? p.y + kFloat * n.y : pi.y,
+              fabsf(p.z) < kOrigin ? p.z + kFloat * n.z : pi.z);
+}
+
+// PathTransportUtilities::PowerHeuristic (Utilities/PathTransportUtilities.h:251).
+__device__ __forceinline__ float PowerHeuristic(float a, float b)
+{
+    const float a2 = a * a;
+    return a2 / (a2 + b * b);
+}
+
+// Warp-aggregated queue append: one atomic per warp; returns this lane's
+// index (or -1 when `pred` is false).
+__device__ __forceinline__ int WarpAppend(int* counter, bool pred)
+{
+    const unsigned act = __activemask();
+    const unsigned m = __ballot_sync(act, pred);
+    if (!m) return -1;
+    const int lane = threadIdx.x & 31;
+    const int leader = __ffs(m) - 1;
+    int base = 0;
+    if (lane == leader) base = atomicAdd(counter, __popc(m));
+    base = __shfl_sync(act, base, leader);
+    return pred ? base + __popc(m & ((1u << lane) - 1u)) : -1;
+}
+
+}  // namespace rtb200

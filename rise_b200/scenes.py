@@ -156,6 +156,119 @@ def _box(cx, cz, sx, sy, sz, angle_deg):
     return np.concatenate([_quad(*(v[k] for k in f)) for f in q])
 
 
+def fbm_heights(n, seed, octaves=6, amplitude=0.1):
+    """(n, n) heights: seeded value-noise fBm (lacunarity 2, gain 0.5), scaled
+    so the sum of octave amplitudes is `amplitude`."""
+    rng = np.random.default_rng(seed)
+    u = np.linspace(0.0, 1.0, n)
+    h = np.zeros((n, n))
+    amp, total = 1.0, 0.0
+    for o in range(octaves):
+        f = 4 * (2 ** o)
+        g = rng.random((f + 2, f + 2)) * 2.0 - 1.0
+        x = u * f
+        i = np.floor(x).astype(int)
+        t = x - i
+        t = t * t * (3 - 2 * t)
+        gx0, gx1 = i, i + 1
+        a = g[np.ix_(gx0, gx0)] * (1 - t)[None, :] + g[np.ix_(gx0, gx1)] * t[None, :]
+        b = g[np.ix_(gx1, gx0)] * (1 - t)[None, :] + g[np.ix_(gx1, gx1)] * t[None, :]
+        h += amp * (a * (1 - t)[:, None] + b * t[:, None])
+        total += amp
+        amp *= 0.5
+    return h * (amplitude / total)
+
+
+def heightfield(n, seed, amplitude=0.1, y0=0.0):
+    """(2 (n-1)^2, 9) triangles of an n x n vertex grid over x, z in [0, 1]."""
+    hgt = fbm_heights(n, seed, amplitude=amplitude) + y0
+    u = np.linspace(0.0, 1.0, n)
+    X, Z = np.meshgrid(u, u)
+    P = np.stack([X, hgt.T, Z], axis=-1).astype(np.float32)   # P[z, x]
+    a = P[:-1, :-1].reshape(-1, 3)
+    b = P[:-1, 1:].reshape(-1, 3)
+    c = P[1:, 1:].reshape(-1, 3)
+    d = P[1:, :-1].reshape(-1, 3)
+    t1 = np.concatenate([a, d, c], axis=1)   # normals up (+y)
+    t2 = np.concatenate([a, c, b], axis=1)
+    return np.concatenate([t1, t2]).astype(np.float32), hgt
+
+
+def uv_sphere(center, radius, n_tri):
+    """Closed UV sphere with about n_tri triangles, outward-facing winding."""
+    # nu segments around, nv rings: 2 nu (nv - 2) triangles (one per segment
+    # at each pole row).
+    nu = max(8, int(round(np.sqrt(n_tri / 2.0))))
+    nv = max(4, int(round(n_tri / (2.0 * nu))) + 2)
+    th = np.linspace(0.0, np.pi, nv)
+    ph = np.linspace(0.0, 2 * np.pi, nu + 1)
+    st, ct = np.sin(th), np.cos(th)
+    V = np.stack([st[:, None] * np.cos(ph)[None, :], np.broadcast_to(ct[:, None], (nv, nu + 1)),
+                  st[:, None] * np.sin(ph)[None, :]], axis=-1) * radius + np.asarray(center)
+    tris = []
+    for i in range(nv - 1):
+        a, b = V[i, :-1], V[i, 1:]
+        c, d = V[i + 1, :-1], V[i + 1, 1:]
+        if i > 0:
+            tris.append(np.concatenate([a, b, c], axis=1))
+        if i < nv - 2:
+            tris.append(np.concatenate([b, d, c], axis=1))
+    return np.concatenate(tris).astype(np.float32)
+
+
+def gold_like_spectra():
+    """Smooth conductor optical constants, eta and k over 380-780 nm."""
+    t = (WAVELENGTHS - 380.0) / 400.0
+    eta = (1.4 - 1.25 * t).astype(np.float32)
+    k = (1.8 + 2.6 * t).astype(np.float32)
+    return eta, k
+
+
+def spheres_scene(grid=1024, n_spheres=64, sphere_tris=20000, width=1024, height=1024, seed=3,
+                  max_depth=16, nee_per_lambda=1):
+    """Displaced heightfield plus tessellated spheres, one area light and a sky.
+
+    A grid x grid heightfield over the unit square with 6-octave fBm of
+    amplitude 0.1 (2 (grid-1)^2 triangles, Lambertian 0.5); n_spheres spheres
+    of sphere_tris triangles with radii U(0.02, 0.08) resting on it, half GGX
+    conductors with roughness U(0.05, 0.5), half dielectrics of index 1.5; a
+    0.3 x 0.3 area light of radiance 30 at height 1.2 and a uniform sky of
+    radiance 0.3 (both on 400-700 nm).  With the defaults this is the
+    large-scene configuration: 2,093,058 + 64 x 20,000 triangles, 1024 x 1024
+    pixels, max depth 16.
+    """
+    rng = np.random.default_rng(seed)
+    d = SceneDesc()
+    ground = d.add_spectrum(flat_spectrum(0.5))
+    sky = d.add_spectrum(flat_spectrum(0.3, 400, 700))
+    lightS = d.add_spectrum(flat_spectrum(30.0, 400, 700))
+    eta, k = gold_like_spectra()
+    s_eta, s_k = d.add_spectrum(eta), d.add_spectrum(k)
+    m_ground = d.add_material(Material(MAT_LAMBERTIAN, ground))
+    m_light = d.add_material(Material(MAT_LAMBERTIAN, -1, lightS))
+    hf, hgt = heightfield(grid, seed, 0.1)
+    d.add_mesh(hf, m_ground)
+    for i in range(n_spheres):
+        r = rng.uniform(0.02, 0.08)
+        x, z = rng.uniform(0.1, 0.9, 2)
+        gi, gj = int(round(x * (grid - 1))), int(round(z * (grid - 1)))
+        y = hgt[gi, gj] + r
+        if i % 2 == 0:
+            m = d.add_material(Material(MAT_GGX, -1, -1, s_eta, s_k, float(rng.uniform(0.05, 0.5)), 1.5))
+            d.add_mesh(uv_sphere((x, y, z), r, sphere_tris), m, double_sided=True)
+        else:
+            m = d.add_material(Material(MAT_DIELECTRIC, -1, -1, -1, -1, 0.0, 1.5))
+            d.add_mesh(uv_sphere((x, y, z), r, sphere_tris), m, double_sided=False)
+    lo, hi, ly = 0.35, 0.65, 1.2
+    d.add_mesh(_quad([lo, ly, lo], [hi, ly, lo], [hi, ly, hi], [lo, ly, hi]), m_light, double_sided=False)
+    d.env = sky
+    d.env_visible = 1
+    d.settings = RenderSettings(width=width, height=height, cam_pos=(0.5, 0.55, -0.45), cam_look=(0.5, 0.0, 0.55),
+                                cam_up=(0.0, 1.0, 0.0), fov_deg=45.0, max_depth=max_depth,
+                                nee_per_lambda=nee_per_lambda, seed=1)
+    return d
+
+
 def cornell_box(width=256, height=256, spp_seed=1, nee_per_lambda=1, max_depth=8):
     """The 32-triangle spectral Cornell box.
 

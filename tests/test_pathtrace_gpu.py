@@ -54,6 +54,38 @@ def test_same_seed_matches_oracle(ctx, nee_per_lambda, layout):
     assert abs(g[..., 1].mean() / o[..., 1].mean() - 1) < 2e-3
 
 
+def small_spheres(nee_per_lambda=1):
+    return scenes.spheres_scene(grid=64, n_spheres=8, sphere_tris=800, width=64, height=64,
+                                nee_per_lambda=nee_per_lambda)
+
+
+@pytest.mark.parametrize("nee_per_lambda", [1, 0])
+def test_materials_same_seed_matches_oracle(ctx, nee_per_lambda):
+    """GGX conductors, smooth dielectrics, heightfield, area light and sky."""
+    d = small_spheres(nee_per_lambda)
+    g, st = render_gpu(ctx, d, 16)
+    o = oracle.pt_render(d, 16)
+    assert np.isfinite(g).all()
+    close = (np.abs(g - o) <= 1e-3 * (np.abs(o) + 1e-3)).all(axis=2)
+    assert close.mean() > 0.90, close.mean()
+    assert rel_mse(g, o) < 2e-3
+    assert abs(g[..., 1].mean() / o[..., 1].mean() - 1) < 5e-3
+
+
+def test_materials_independent_seeds_z_test(ctx):
+    K, spp = 8, 16
+    d = small_spheres()
+    gs, os_ = [], []
+    for k in range(K):
+        d.settings.seed = 3000 + k
+        gs.append(render_gpu(ctx, d, spp)[0][..., 1])
+        d.settings.seed = 4000 + k
+        os_.append(oracle.pt_render(d, spp)[..., 1])
+    gs, os_ = np.array(gs), np.array(os_)
+    z = (gs.mean(0) - os_.mean(0)) / np.sqrt(gs.var(0, ddof=1) / K + os_.var(0, ddof=1) / K + 1e-12)
+    assert (np.abs(z) > 4).mean() < 0.005, (np.abs(z) > 4).mean()
+
+
 def test_independent_seeds_z_test(ctx):
     K, spp = 8, 16
     d = scenes.cornell_box(48, 48)
