@@ -175,6 +175,37 @@ int rtb200_job_read_film(rtb200_job* job, float* xyz);
 int rtb200_job_stats(const rtb200_job* job, rtb200_stats* out);
 int rtb200_job_destroy(rtb200_job* job);
 
+/* ---- engines: many jobs in one wavefront -------------------------------- */
+
+/* An engine owns a device pool of `capacity` path slots (0 = 2^21), the
+ * ray and shadow-ray queues, and a table of up to 1024 jobs.  Jobs of
+ * different scenes and resolutions (same BVH layout) share its wavefront:
+ * every iteration hands free path slots to whichever jobs still have samples
+ * to give, so their work overlaps on the device.  No counterpart in the
+ * reference, which renders one image at a time
+ * (PixelBasedRasterizerHelper::RasterizeScene,
+ * Rendering/PixelBasedRasterizerHelper.cpp:982-1440).
+ *
+ * rtb200_engine_render: render spp[i] more samples per pixel for each
+ *   jobs[i] in one shared wavefront and return when all are in the films;
+ *   use_graph replays the iterations from a captured CUDA graph.
+ * Continuous batching: rtb200_engine_submit adds a job with a request of
+ *   spp samples per pixel (allowed while other jobs are in flight);
+ *   rtb200_engine_step runs `iterations` wavefront iterations over all
+ *   submitted jobs; rtb200_engine_progress reports samples finished / total
+ *   of a job's request as of the last step; rtb200_engine_retire folds a
+ *   finished request into the job's film (RTB200_E_NOT_READY before that)
+ *   and removes the job from the engine. */
+typedef struct rtb200_engine rtb200_engine;
+int rtb200_engine_create(rtb200_ctx* ctx, int32_t capacity, rtb200_engine** out);
+int rtb200_engine_render(rtb200_engine* engine, rtb200_job* const* jobs, const int32_t* spp, int32_t n,
+                         int32_t use_graph);
+int rtb200_engine_submit(rtb200_engine* engine, rtb200_job* job, int32_t spp);
+int rtb200_engine_step(rtb200_engine* engine, int32_t iterations, int32_t use_graph);
+int rtb200_engine_progress(const rtb200_engine* engine, const rtb200_job* job, int64_t* done, int64_t* total);
+int rtb200_engine_retire(rtb200_engine* engine, rtb200_job* job);
+int rtb200_engine_destroy(rtb200_engine* engine);
+
 /* ---- host BVH build and export ----------------------------------------- */
 
 /* Builds the reference BVH on the host (all cores) without a device and

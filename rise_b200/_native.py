@@ -51,6 +51,13 @@ SIGNATURES = {
     "rtb200_job_read_film": (ctypes.c_int, [_vp, _vp]),
     "rtb200_job_stats": (ctypes.c_int, [_vp, _vp]),
     "rtb200_job_destroy": (ctypes.c_int, [_vp]),
+    "rtb200_engine_create": (ctypes.c_int, [_vp, _i32, _pvp]),
+    "rtb200_engine_render": (ctypes.c_int, [_vp, _vp, _vp, _i32, _i32]),
+    "rtb200_engine_submit": (ctypes.c_int, [_vp, _vp, _i32]),
+    "rtb200_engine_step": (ctypes.c_int, [_vp, _i32, _i32]),
+    "rtb200_engine_progress": (ctypes.c_int, [_vp, _vp, _pi64, _pi64]),
+    "rtb200_engine_retire": (ctypes.c_int, [_vp, _vp]),
+    "rtb200_engine_destroy": (ctypes.c_int, [_vp]),
 }
 NOALLOC_SCRATCH_BYTES = 256
 NOALLOC_MAX_RAYS = 2147483647

@@ -1,0 +1,573 @@
+// engine.cpp -- render jobs and the shared wavefront engine (include/rtb200.h).
+//
+// A job is one image: its scene, camera, settings and film (compensated
+// running sums plus this request's accumulator).  An engine owns a pool of
+// path slots, the ray / shadow-ray queues and a table of up to kMaxJobs job
+// descriptors.  Any number of jobs -- of different scenes and resolutions --
+// share one engine: every wavefront iteration regenerates free slots with
+// camera samples of whichever jobs still have samples to hand out, so the
+// jobs' work overlaps on the device (batched rendering, and continuous
+// batching when jobs are submitted while others are in flight).  A job
+// rendered alone (rtb200_job_render) uses a private engine.
+//
+// The reference renders one image at a time on a CPU thread pool
+// (PixelBasedRasterizerHelper::RasterizeScene, progressive passes at
+// Rendering/PixelBasedRasterizerHelper.cpp:1159-1293); a job's request of N
+// samples per pixel corresponds to one progressive pass of N samples.
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "cie1931.h"
+#include "core.h"
+#include "pathtrace.h"
+
+using namespace rtb200;
+
+namespace {
+
+constexpr int kMaxJobs = 1024;
+constexpr int kGraphIters = 2;   // iterations per captured graph (even: queue pointers return)
+
+const float kCieY[RTB200_CIE_COUNT] = {RTB200_CIE_YBAR};
+
+// ColorUtils::CIE_Y_Integral (src/Library/Utilities/Color/ColorUtils.cpp:327-348):
+// trapezoid sum of y-bar over whole 5 nm cells between the clamped bounds.
+double CieYIntegral(double a, double b)
+{
+    const double lo = a < 380.0 ? 380.0 : a;
+    const double hi = b > 780.0 ? 780.0 : b;
+    if (hi <= lo) return 0.0;
+    const int first = (int)((lo - 380.0) / 5.0);
+    const int last = (int)((hi - 380.0) / 5.0);
+    double sum = 0.0;
+    for (int i = first; i < last; ++i) sum += 0.5 * ((double)kCieY[i] + (double)kCieY[i + 1]) * 5.0;
+    return sum;
+}
+
+size_t Align(size_t x) { return (x + 255) & ~(size_t)255; }
+
+}  // namespace
+
+struct rtb200_job {
+    rtb200_scene* scene = nullptr;
+    rtb200_render_settings rs{};
+    PtCamera cam{};
+    PtSettings set{};
+    int npix = 0;
+    void* film_buf = nullptr;
+    size_t film_bytes = 0;
+    float* pass = nullptr;
+    float* sum = nullptr;
+    float* comp = nullptr;
+    long long spp_done = 0;
+    long long samples = 0;
+    double seconds = 0.0;
+    long long segments = 0, shadow_rays = 0;
+    rtb200_engine* engine = nullptr;   // engine the job is submitted to
+    int entry = -1;
+    long long pending_spp = 0;
+    rtb200_engine* own = nullptr;      // private engine of rtb200_job_render
+};
+
+struct rtb200_engine {
+    rtb200_ctx* ctx = nullptr;
+    int capacity = 0;
+    int layout = -1;
+    void* buf = nullptr;
+    size_t bytes = 0;
+    PtPaths paths{};
+    PtQueues queues{};
+    int* d_iota = nullptr;
+    PtJobDev* d_table = nullptr;
+    int* d_ids = nullptr;
+    unsigned long long* d_ctr = nullptr;   // [kMaxJobs] issued, [kMaxJobs] done
+    PtJobDev* h_table = nullptr;           // pinned
+    int* h_ids = nullptr;                  // pinned
+    int* h_cnt = nullptr;                  // pinned
+    unsigned long long* h_ctr = nullptr;   // pinned
+    rtb200_job* owner[kMaxJobs] = {};
+    unsigned long long total[kMaxJobs] = {};
+    std::vector<int> active;
+    bool dirty = true;
+    bool fresh = true;
+    int iter = 0;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    cudaGraphExec_t gexec = nullptr;
+    int gnjobs = -1;
+    long long seg_seen = 0, shadow_seen = 0;
+};
+
+namespace {
+
+PtLaunch MakeLaunch(const rtb200_engine* e)
+{
+    PtLaunch L;
+    L.jobs = e->d_table;
+    L.ids = e->d_ids;
+    L.njobs = (int)e->active.size();
+    L.layout = e->layout;
+    L.paths = e->paths;
+    L.queues = e->queues;
+    L.sms = e->ctx->num_sms;
+    return L;
+}
+
+void DropGraph(rtb200_engine* e)
+{
+    if (e->gexec) cudaGraphExecDestroy(e->gexec);
+    e->gexec = nullptr;
+    e->gnjobs = -1;
+}
+
+int EngineCreate(rtb200_ctx* ctx, int capacity, rtb200_engine** out)
+{
+    *out = nullptr;
+    if (capacity <= 0) capacity = 1 << 21;
+    capacity = (capacity + 31) & ~31;
+    rtb200_engine* e = new (std::nothrow) rtb200_engine();
+    if (!e) return SetError(ctx, RTB200_E_OOM, "host allocation failed");
+    e->ctx = ctx;
+    e->capacity = capacity;
+    const size_t c = (size_t)capacity;
+    size_t off = 0;
+    auto take = [&](size_t bytes) { const size_t at = off; off += Align(bytes); return at; };
+    const size_t oRo = take(16 * c), oRd = take(16 * c), oHit = take(16 * c), oThr = take(16 * c), oL = take(16 * c),
+                 oAux = take(16 * c), oMeta = take(16 * c);
+    const size_t oQa = take(4 * c), oQan = take(4 * c), oQf = take(4 * c), oQfn = take(4 * c), oIota = take(4 * c);
+    const size_t oSh = take(sizeof(ShadowEntry) * 8 * c);   // up to 4 light + 4 sky samples per path
+    const size_t oTab = take(sizeof(PtJobDev) * kMaxJobs), oIds = take(4 * kMaxJobs),
+                 oCtr = take(8 * 2 * kMaxJobs);
+    const size_t oCnt = take(4 * kCntCount), oTr = take(8 * 2), oSmp = take(8), oErr = take(4);
+    int rc = DevAlloc(ctx, &e->buf, off);
+    if (rc) { delete e; return rc; }
+    e->bytes = off;
+    char* b = (char*)e->buf;
+    cudaMemset(b, 0, off);
+    e->paths = PtPaths{(float4*)(b + oRo), (float4*)(b + oRd), (float4*)(b + oHit), (float4*)(b + oThr),
+                       (float4*)(b + oL), (float4*)(b + oAux), (uint4*)(b + oMeta)};
+    e->queues = PtQueues{(int*)(b + oQa), (int*)(b + oQan), (int*)(b + oQf), (int*)(b + oQfn),
+                         (ShadowEntry*)(b + oSh), (int*)(b + oCnt), (unsigned long long*)(b + oSmp),
+                         (unsigned long long*)(b + oTr), (unsigned*)(b + oErr)};
+    e->d_iota = (int*)(b + oIota);
+    e->d_table = (PtJobDev*)(b + oTab);
+    e->d_ids = (int*)(b + oIds);
+    e->d_ctr = (unsigned long long*)(b + oCtr);
+    {
+        std::vector<int> iota(c);
+        for (size_t i = 0; i < c; ++i) iota[i] = (int)i;
+        cudaMemcpy(e->d_iota, iota.data(), 4 * c, cudaMemcpyHostToDevice);
+    }
+    if (cudaMallocHost(&e->h_table, sizeof(PtJobDev) * kMaxJobs) != cudaSuccess ||
+        cudaMallocHost(&e->h_ids, 4 * kMaxJobs) != cudaSuccess ||
+        cudaMallocHost(&e->h_cnt, 4 * kCntCount) != cudaSuccess ||
+        cudaMallocHost(&e->h_ctr, 8 * 2 * kMaxJobs) != cudaSuccess || cudaEventCreate(&e->e0) != cudaSuccess ||
+        cudaEventCreate(&e->e1) != cudaSuccess) {
+        cudaGetLastError();
+        DevFree(ctx, e->buf, e->bytes);
+        if (e->h_table) cudaFreeHost(e->h_table);
+        if (e->h_ids) cudaFreeHost(e->h_ids);
+        if (e->h_cnt) cudaFreeHost(e->h_cnt);
+        if (e->h_ctr) cudaFreeHost(e->h_ctr);
+        delete e;
+        return SetError(ctx, RTB200_E_OOM, "pinned host allocation failed");
+    }
+    std::memset(e->h_table, 0, sizeof(PtJobDev) * kMaxJobs);
+    std::memset(e->h_ctr, 0, 8 * 2 * kMaxJobs);
+    *out = e;
+    return RTB200_OK;
+}
+
+void EngineDestroy(rtb200_engine* e)
+{
+    rtb200_ctx* ctx = e->ctx;
+    cudaStreamSynchronize(ctx->stream);
+    for (int i = 0; i < kMaxJobs; ++i)
+        if (e->owner[i]) { e->owner[i]->engine = nullptr; e->owner[i]->entry = -1; }
+    DropGraph(e);
+    DevFree(ctx, e->buf, e->bytes);
+    cudaFreeHost(e->h_table);
+    cudaFreeHost(e->h_ids);
+    cudaFreeHost(e->h_cnt);
+    cudaFreeHost(e->h_ctr);
+    cudaEventDestroy(e->e0);
+    cudaEventDestroy(e->e1);
+    delete e;
+}
+
+int EngineSubmit(rtb200_engine* e, rtb200_job* j, int spp)
+{
+    rtb200_ctx* ctx = e->ctx;
+    if (spp <= 0) return SetError(ctx, RTB200_E_INVALID, "spp must be positive");
+    if (j->engine) return SetError(ctx, RTB200_E_INVALID, "job is already submitted to an engine");
+    if (j->scene->ctx != ctx) return SetError(ctx, RTB200_E_INVALID, "job and engine belong to different contexts");
+    if (e->layout >= 0 && e->layout != j->scene->layout && !e->active.empty())
+        return SetError(ctx, RTB200_E_INVALID, "all jobs of an engine must use the same BVH layout");
+    int entry = -1;
+    for (int i = 0; i < kMaxJobs; ++i)
+        if (!e->owner[i]) { entry = i; break; }
+    if (entry < 0) return SetError(ctx, RTB200_E_BUDGET, "engine job table is full");
+    e->layout = j->scene->layout;
+    rtb200_scene* s = j->scene;
+    PtJobDev& d = e->h_table[entry];
+    d.scene = PtScene{s->d_nodes, s->layout, s->d_tris, (int)s->tri_material.size(), s->d_attr, s->d_mats,
+                      s->d_spectra, s->d_lights, s->d_light_tris};
+    d.cam = j->cam;
+    d.set = j->set;
+    d.npix = j->npix;
+    d.film = j->pass;
+    d.sample_begin = (unsigned long long)j->spp_done;
+    d.total = (unsigned long long)j->npix * (unsigned long long)spp;
+    d.sample_ctr = e->d_ctr + entry;
+    d.done_ctr = e->d_ctr + kMaxJobs + entry;
+    cudaMemsetAsync(e->d_ctr + entry, 0, 8, ctx->stream);
+    cudaMemsetAsync(e->d_ctr + kMaxJobs + entry, 0, 8, ctx->stream);
+    e->h_ctr[entry] = 0;
+    e->h_ctr[kMaxJobs + entry] = 0;
+    e->total[entry] = d.total;
+    e->owner[entry] = j;
+    e->active.push_back(entry);
+    e->dirty = true;
+    j->engine = e;
+    j->entry = entry;
+    j->pending_spp = spp;
+    return RTB200_OK;
+}
+
+int EngineStep(rtb200_engine* e, int iterations, bool graph)
+{
+    rtb200_ctx* ctx = e->ctx;
+    cudaStream_t st = ctx->stream;
+    if (e->active.empty()) return RTB200_OK;
+    if (e->dirty) {
+        for (size_t i = 0; i < e->active.size(); ++i) e->h_ids[i] = e->active[i];
+        cudaMemcpyAsync(e->d_table, e->h_table, sizeof(PtJobDev) * kMaxJobs, cudaMemcpyHostToDevice, st);
+        cudaMemcpyAsync(e->d_ids, e->h_ids, 4 * e->active.size(), cudaMemcpyHostToDevice, st);
+        e->dirty = false;
+    }
+    if (e->fresh) {
+        // Every slot starts free; statistics counters restart from zero.
+        cudaMemcpyAsync(e->queues.free_, e->d_iota, 4 * (size_t)e->capacity, cudaMemcpyDeviceToDevice, st);
+        int init[kCntCount] = {0};
+        init[kCntFree] = e->capacity;
+        std::memcpy(e->h_cnt, init, sizeof(init));
+        cudaMemcpyAsync(e->queues.cnt, e->h_cnt, 4 * kCntCount, cudaMemcpyHostToDevice, st);
+        e->fresh = false;
+        e->seg_seen = e->shadow_seen = 0;
+    }
+    PtLaunch L = MakeLaunch(e);
+    cudaError_t err = cudaSuccess;
+    if (graph) {
+        if (!e->gexec || e->gnjobs != L.njobs) {
+            DropGraph(e);
+            cudaGraph_t g = nullptr;
+            err = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
+            PtLaunch C = L;
+            for (int k = 0; k < kGraphIters && err == cudaSuccess; ++k) {
+                err = PtIteration(C, k, st);
+                std::swap(C.queues.active, C.queues.active_next);
+                std::swap(C.queues.free_, C.queues.free_next);
+            }
+            const cudaError_t e2 = cudaStreamEndCapture(st, &g);
+            if (err == cudaSuccess) err = e2;
+            if (err == cudaSuccess) err = cudaGraphInstantiate(&e->gexec, g, 0);
+            if (g) cudaGraphDestroy(g);
+            if (err != cudaSuccess) { DropGraph(e); return CudaCheck(ctx, err, "graph capture"); }
+            e->gnjobs = L.njobs;
+        }
+        const int reps = (iterations + kGraphIters - 1) / kGraphIters;
+        for (int r = 0; r < reps && err == cudaSuccess; ++r) err = cudaGraphLaunch(e->gexec, st);
+        e->iter += reps * kGraphIters;
+    } else {
+        // Direct launches; an even count keeps the queue buffers where the
+        // captured graph expects them.
+        const int n = ((iterations + 1) / 2) * 2;
+        for (int k = 0; k < n && err == cudaSuccess; ++k) {
+            err = PtIteration(L, e->iter++, st);
+            std::swap(L.queues.active, L.queues.active_next);
+            std::swap(L.queues.free_, L.queues.free_next);
+        }
+    }
+    if (err == cudaSuccess)
+        err = cudaMemcpyAsync(e->h_cnt, e->queues.cnt, 4 * kCntCount, cudaMemcpyDeviceToHost, st);
+    if (err == cudaSuccess) err = cudaMemcpyAsync(e->h_ctr, e->d_ctr, 8 * 2 * kMaxJobs, cudaMemcpyDeviceToHost, st);
+    if (err == cudaSuccess) err = cudaStreamSynchronize(st);
+    if (err != cudaSuccess) return CudaCheck(ctx, err, "wavefront step");
+    unsigned errw = 0;
+    cudaMemcpy(&errw, e->queues.err, 4, cudaMemcpyDeviceToHost);
+    if (errw) return SetError(ctx, RTB200_E_DEVICE, "device error word set (traversal stack overflow)");
+    // Per-job statistics: attribute this step's segments to the active jobs.
+    const long long seg = (unsigned)e->h_cnt[kCntSegments], sh = (unsigned)e->h_cnt[kCntShadowRays];
+    const long long dseg = seg - e->seg_seen, dsh = sh - e->shadow_seen;
+    e->seg_seen = seg;
+    e->shadow_seen = sh;
+    if (!e->active.empty()) {
+        for (int id : e->active) {
+            e->owner[id]->segments += dseg / (long long)e->active.size();
+            e->owner[id]->shadow_rays += dsh / (long long)e->active.size();
+        }
+    }
+    return RTB200_OK;
+}
+
+bool JobDone(const rtb200_engine* e, int entry) { return e->h_ctr[kMaxJobs + entry] >= e->total[entry]; }
+
+int EngineRetire(rtb200_engine* e, rtb200_job* j)
+{
+    rtb200_ctx* ctx = e->ctx;
+    if (j->engine != e) return SetError(ctx, RTB200_E_INVALID, "job is not submitted to this engine");
+    if (!JobDone(e, j->entry)) return SetError(ctx, RTB200_E_NOT_READY, "job still has samples in flight");
+    cudaError_t err = PtFold(j->pass, j->sum, j->comp, j->npix, ctx->num_sms, ctx->stream);
+    if (err != cudaSuccess) return CudaCheck(ctx, err, "film fold");
+    j->spp_done += j->pending_spp;
+    j->samples += (long long)j->npix * j->pending_spp;
+    j->pending_spp = 0;
+    const int entry = j->entry;
+    e->active.erase(std::find(e->active.begin(), e->active.end(), entry));
+    e->owner[entry] = nullptr;
+    e->total[entry] = 0;
+    e->h_table[entry].total = 0;
+    e->dirty = true;
+    j->engine = nullptr;
+    j->entry = -1;
+    return RTB200_OK;
+}
+
+// Submit all, step until every job is done, retire all.
+int EngineRender(rtb200_engine* e, rtb200_job* const* jobs, const int32_t* spp, int n, bool graph)
+{
+    rtb200_ctx* ctx = e->ctx;
+    for (int i = 0; i < n; ++i) {
+        const int rc = EngineSubmit(e, jobs[i], spp[i]);
+        if (rc) {
+            for (int k = 0; k < i; ++k) {
+                // Undo earlier submissions: nothing has run yet.
+                rtb200_job* j = jobs[k];
+                e->active.erase(std::find(e->active.begin(), e->active.end(), j->entry));
+                e->owner[j->entry] = nullptr;
+                e->total[j->entry] = 0;
+                j->engine = nullptr;
+                j->entry = -1;
+            }
+            e->dirty = true;
+            return rc;
+        }
+    }
+    cudaEventRecord(e->e0, ctx->stream);
+    const long long kMaxSteps = 1ll << 18;
+    for (long long step = 0;; ++step) {
+        const int rc = EngineStep(e, 4, graph);
+        if (rc) return rc;
+        bool all = true;
+        for (int i = 0; i < n; ++i) all = all && JobDone(e, jobs[i]->entry);
+        if (all) break;
+        if (step > kMaxSteps) return SetError(ctx, RTB200_E_TIMEOUT, "render did not finish its samples");
+    }
+    cudaEventRecord(e->e1, ctx->stream);
+    cudaEventSynchronize(e->e1);
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, e->e0, e->e1);
+    for (int i = 0; i < n; ++i) {
+        jobs[i]->seconds += ms * 1e-3;
+        const int rc = EngineRetire(e, jobs[i]);
+        if (rc) return rc;
+    }
+    return CudaCheck(ctx, cudaStreamSynchronize(ctx->stream), "film fold");
+}
+
+}  // namespace
+
+extern "C" {
+
+int rtb200_job_create(rtb200_scene* s, const rtb200_render_settings* rs, rtb200_job** out)
+{
+    if (!s || !rs || !out) return RTB200_E_INVALID;
+    rtb200_ctx* ctx = s->ctx;
+    std::lock_guard<std::mutex> g(ctx->mu);
+    *out = nullptr;
+    if (!s->committed || s->materials.empty())
+        return SetError(ctx, RTB200_E_INVALID, "scene must be committed with materials");
+    if (rs->width <= 0 || rs->height <= 0 || (int64_t)rs->width * rs->height > (1ll << 28) || rs->max_depth < 1 ||
+        rs->max_depth > 255 || !(rs->lambda_max > rs->lambda_min) || rs->lambda_min < 380.0f ||
+        rs->lambda_max > 780.0f || !(rs->fov_deg > 0.0f && rs->fov_deg < 180.0f))
+        return SetError(ctx, RTB200_E_INVALID, "bad render settings");
+    // Camera frame (pinhole; vertical field of view).
+    const float* P = rs->cam_pos;
+    double f[3] = {rs->cam_look[0] - P[0], rs->cam_look[1] - P[1], rs->cam_look[2] - P[2]};
+    const double fl = std::sqrt(f[0] * f[0] + f[1] * f[1] + f[2] * f[2]);
+    if (!(fl > 0.0)) return SetError(ctx, RTB200_E_INVALID, "degenerate camera frame");
+    for (double& x : f) x /= fl;
+    const double u[3] = {rs->cam_up[0], rs->cam_up[1], rs->cam_up[2]};
+    double r[3] = {f[1] * u[2] - f[2] * u[1], f[2] * u[0] - f[0] * u[2], f[0] * u[1] - f[1] * u[0]};
+    const double rl = std::sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
+    if (!(rl > 0.0)) return SetError(ctx, RTB200_E_INVALID, "degenerate camera frame");
+    for (double& x : r) x /= rl;
+    const double uu[3] = {r[1] * f[2] - r[2] * f[1], r[2] * f[0] - r[0] * f[2], r[0] * f[1] - r[1] * f[0]};
+    cudaSetDevice(ctx->device);
+    rtb200_job* j = new (std::nothrow) rtb200_job();
+    if (!j) return SetError(ctx, RTB200_E_OOM, "host allocation failed");
+    j->scene = s;
+    j->rs = *rs;
+    j->npix = rs->width * rs->height;
+    const double th = std::tan(0.5 * rs->fov_deg * 3.14159265358979323846 / 180.0);
+    const double aspect = (double)rs->width / (double)rs->height;
+    for (int k = 0; k < 3; ++k) {
+        j->cam.pos[k] = P[k];
+        j->cam.fwd[k] = (float)f[k];
+        j->cam.right[k] = (float)(r[k] * th * aspect);
+        j->cam.up[k] = (float)(uu[k] * th);
+    }
+    j->cam.width = rs->width;
+    j->cam.height = rs->height;
+    PtSettings& st = j->set;
+    st.lmin = rs->lambda_min;
+    st.lmax = rs->lambda_max;
+    const double ky = CieYIntegral(rs->lambda_min, rs->lambda_max);
+    st.ynorm = ky > 0.0 ? (float)((rs->lambda_max - rs->lambda_min) / ky) : 0.0f;
+    st.max_depth = rs->max_depth;
+    st.rr_min_depth = rs->rr_min_depth;
+    st.rr_threshold = rs->rr_threshold;
+    st.nee_per_lambda = rs->nee_per_lambda ? 1 : 0;
+    st.seed = rs->seed;
+    st.env = s->env;
+    st.env_visible = s->env_visible;
+    st.n_lights = (int)s->lights.size();
+    st.n_spectra = (int)(s->spectra.size() / RTB200_CIE_COUNT);
+    // Film: this request's accumulator, running sum, Kahan compensation.
+    const size_t plane = Align(12 * (size_t)j->npix);
+    int rc = DevAlloc(ctx, &j->film_buf, 3 * plane);
+    if (rc) { delete j; return rc; }
+    j->film_bytes = 3 * plane;
+    cudaMemset(j->film_buf, 0, 3 * plane);
+    j->pass = (float*)j->film_buf;
+    j->sum = (float*)((char*)j->film_buf + plane);
+    j->comp = (float*)((char*)j->film_buf + 2 * plane);
+    *out = j;
+    return RTB200_OK;
+}
+
+int rtb200_job_render(rtb200_job* j, int32_t spp)
+{
+    if (!j) return RTB200_E_INVALID;
+    rtb200_ctx* ctx = j->scene->ctx;
+    std::lock_guard<std::mutex> g(ctx->mu);
+    if (spp <= 0) return SetError(ctx, RTB200_E_INVALID, "spp must be positive");
+    if (j->engine) return SetError(ctx, RTB200_E_INVALID, "job is submitted to an engine");
+    cudaSetDevice(ctx->device);
+    if (!j->own) {
+        int cap = j->rs.max_paths > 0 ? j->rs.max_paths : std::min(std::max(j->npix * 8, 65536), 1 << 21);
+        const int rc = EngineCreate(ctx, cap, &j->own);
+        if (rc) return rc;
+    }
+    rtb200_job* list[1] = {j};
+    const int32_t s[1] = {spp};
+    return EngineRender(j->own, list, s, 1, false);
+}
+
+int rtb200_job_read_film(rtb200_job* j, float* xyz)
+{
+    if (!j || !xyz) return RTB200_E_INVALID;
+    rtb200_ctx* ctx = j->scene->ctx;
+    std::lock_guard<std::mutex> g(ctx->mu);
+    cudaSetDevice(ctx->device);
+    const size_t n3 = 3 * (size_t)j->npix;
+    std::vector<float> sum(n3), comp(n3);
+    cudaError_t e = cudaMemcpy(sum.data(), j->sum, 4 * n3, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(comp.data(), j->comp, 4 * n3, cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return CudaCheck(ctx, e, "film readback");
+    const double inv = j->spp_done > 0 ? 1.0 / (double)j->spp_done : 0.0;
+    for (size_t i = 0; i < n3; ++i) xyz[i] = (float)(((double)sum[i] - (double)comp[i]) * inv);
+    return RTB200_OK;
+}
+
+int rtb200_job_stats(const rtb200_job* j, rtb200_stats* out)
+{
+    if (!j || !out) return RTB200_E_INVALID;
+    out->spp = j->spp_done;
+    out->samples = j->samples;
+    out->segments = j->segments;
+    out->shadow_rays = j->shadow_rays;
+    out->seconds = j->seconds;
+    return RTB200_OK;
+}
+
+int rtb200_job_destroy(rtb200_job* j)
+{
+    if (!j) return RTB200_E_INVALID;
+    rtb200_ctx* ctx = j->scene->ctx;
+    std::lock_guard<std::mutex> g(ctx->mu);
+    if (j->engine) return SetError(ctx, RTB200_E_NOT_READY, "retire the job from its engine first");
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+    if (j->own) EngineDestroy(j->own);
+    DevFree(ctx, j->film_buf, j->film_bytes);
+    delete j;
+    return RTB200_OK;
+}
+
+int rtb200_engine_create(rtb200_ctx* ctx, int32_t capacity, rtb200_engine** out)
+{
+    if (!ctx || !out || capacity < 0) return RTB200_E_INVALID;
+    std::lock_guard<std::mutex> g(ctx->mu);
+    cudaSetDevice(ctx->device);
+    return EngineCreate(ctx, capacity, out);
+}
+
+int rtb200_engine_render(rtb200_engine* e, rtb200_job* const* jobs, const int32_t* spp, int32_t n, int32_t use_graph)
+{
+    if (!e || n < 0 || (n > 0 && (!jobs || !spp))) return RTB200_E_INVALID;
+    std::lock_guard<std::mutex> g(e->ctx->mu);
+    for (int i = 0; i < n; ++i)
+        if (!jobs[i]) return SetError(e->ctx, RTB200_E_INVALID, "null job");
+    cudaSetDevice(e->ctx->device);
+    return EngineRender(e, jobs, spp, n, use_graph != 0);
+}
+
+int rtb200_engine_submit(rtb200_engine* e, rtb200_job* job, int32_t spp)
+{
+    if (!e || !job) return RTB200_E_INVALID;
+    std::lock_guard<std::mutex> g(e->ctx->mu);
+    cudaSetDevice(e->ctx->device);
+    return EngineSubmit(e, job, spp);
+}
+
+int rtb200_engine_step(rtb200_engine* e, int32_t iterations, int32_t use_graph)
+{
+    if (!e || iterations <= 0) return RTB200_E_INVALID;
+    std::lock_guard<std::mutex> g(e->ctx->mu);
+    cudaSetDevice(e->ctx->device);
+    return EngineStep(e, iterations, use_graph != 0);
+}
+
+int rtb200_engine_progress(const rtb200_engine* e, const rtb200_job* job, int64_t* done, int64_t* total)
+{
+    if (!e || !job || job->engine != e) return RTB200_E_INVALID;
+    if (done) *done = (int64_t)e->h_ctr[kMaxJobs + job->entry];
+    if (total) *total = (int64_t)e->total[job->entry];
+    return RTB200_OK;
+}
+
+int rtb200_engine_retire(rtb200_engine* e, rtb200_job* job)
+{
+    if (!e || !job) return RTB200_E_INVALID;
+    std::lock_guard<std::mutex> g(e->ctx->mu);
+    cudaSetDevice(e->ctx->device);
+    const int rc = EngineRetire(e, job);
+    if (rc) return rc;
+    return CudaCheck(e->ctx, cudaStreamSynchronize(e->ctx->stream), "film fold");
+}
+
+int rtb200_engine_destroy(rtb200_engine* e)
+{
+    if (!e) return RTB200_E_INVALID;
+    rtb200_ctx* ctx = e->ctx;
+    std::lock_guard<std::mutex> g(ctx->mu);
+    cudaSetDevice(ctx->device);
+    EngineDestroy(e);
+    return RTB200_OK;
+}
+
+}  // extern "C"

@@ -35,8 +35,9 @@ constexpr float kInv4Pi = 0.07957747154594767f;
 // XYZ of one finished sample: sum over active wavelengths of
 // XYZ(lambda_i) * L_i, scaled by (lmax - lmin) / k_y / active
 // (PathTracingSpectralRasterizer.cpp:141-174).
-__device__ __forceinline__ void Splat(const PtPaths& P, const PtFilm& F, const PtSettings& S, int slot, uint4 m)
+__device__ __forceinline__ void Splat(const PtPaths& P, const PtJobDev& J, int slot, uint4 m)
 {
+    const PtSettings& S = J.set;
     const float4 L = P.L[slot];
     const float hero = P.aux[slot].x;
     float lam[4];
@@ -55,7 +56,7 @@ __device__ __forceinline__ void Splat(const PtPaths& P, const PtFilm& F, const P
     }
     if (active == 0) return;
     const float s = S.ynorm / (float)active;
-    float* px = F.pass + 3 * (size_t)m.x;
+    float* px = J.film + 3 * (size_t)m.x;
     if (X != 0.0f) atomicAdd(px + 0, X * s);
     if (Y != 0.0f) atomicAdd(px + 1, Y * s);
     if (Z != 0.0f) atomicAdd(px + 2, Z * s);
@@ -64,7 +65,8 @@ __device__ __forceinline__ void Splat(const PtPaths& P, const PtFilm& F, const P
 // ---- kernels ---------------------------------------------------------------
 
 __global__ void __launch_bounds__(kShadeBlock)
-KRegen(PtPaths P, PtQueues Q, PtFilm F, PtJobParams J)
+KRegen(const PtJobDev* __restrict__ jobs, const int* __restrict__ ids, int njobs, PtPaths P, PtQueues Q, int iter,
+       int assign)
 {
     const int n = Q.cnt[kCntFree];
     const int lane = threadIdx.x & 31;
@@ -77,39 +79,60 @@ KRegen(PtPaths P, PtQueues Q, PtFilm F, PtJobParams J)
         if (valid) {
             const uint4 m = P.meta[slot];
             if (m.z & kFlagFinishing) {
-                Splat(P, F, J.set, slot, m);
+                const PtJobDev& J = jobs[__float_as_int(P.aux[slot].z)];
+                Splat(P, J, slot, m);
+                atomicAdd(J.done_ctr, 1ull);
                 P.meta[slot].z = m.z & ~kFlagFinishing;
             }
         }
-        // Take new samples for the valid lanes (one atomic per warp).
-        const unsigned want = __ballot_sync(kFull, valid);
-        unsigned long long g0 = 0;
-        if (lane == 0 && want) g0 = atomicAdd(Q.sample_ctr, (unsigned long long)__popc(want));
-        g0 = __shfl_sync(kFull, g0, 0);
-        const unsigned long long g = g0 + __popc(want & ((1u << lane) - 1u));
-        const bool got = valid && g < J.total;
-        if (got) {
-            const uint32_t pixel = (uint32_t)(g % (unsigned long long)J.npix);
-            const uint32_t sample = (uint32_t)(J.sample_begin + g / (unsigned long long)J.npix);
-            const uint32_t key = PathKey(J.set.seed, pixel, sample);
-            const int px = (int)(pixel % (uint32_t)J.cam.width), py = (int)(pixel / (uint32_t)J.cam.width);
-            // Box pixel filter of width 1: uniform jitter inside the pixel.
-            const float fx = (float)px + Rand(key, 0), fy = (float)py + Rand(key, 1);
-            const float sx = 2.0f * fx / (float)J.cam.width - 1.0f;
-            const float sy = 1.0f - 2.0f * fy / (float)J.cam.height;
-            const V3 d = normalize(mk(J.cam.fwd[0] + sx * J.cam.right[0] + sy * J.cam.up[0],
-                                      J.cam.fwd[1] + sx * J.cam.right[1] + sy * J.cam.up[1],
-                                      J.cam.fwd[2] + sx * J.cam.right[2] + sy * J.cam.up[2]));
-            const float hero = J.set.lmin + Rand(key, 2) * (J.set.lmax - J.set.lmin);
-            P.ray_o[slot] = make_float4(J.cam.pos[0], J.cam.pos[1], J.cam.pos[2], 0.0f);
-            P.ray_d[slot] = make_float4(d.x, d.y, d.z, __int_as_float(0x7f800000));
-            P.thr[slot] = make_float4(1.0f, 1.0f, 1.0f, 1.0f);
-            P.L[slot] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-            P.aux[slot] = make_float4(hero, 0.0f, 0.0f, 0.0f);
-            P.meta[slot] = make_uint4(pixel, sample, kFlagConsiderEmission, key);
+        // Hand out new camera samples, one job at a time per warp (one
+        // atomic per warp and job), starting at a job that rotates with the
+        // warp and the iteration so every job receives slots.
+        bool need = valid && assign;
+        bool got = false;
+        const int start = njobs > 0 ? (warp + iter) % njobs : 0;
+        for (int k = 0; k < njobs && __any_sync(kFull, need); ++k) {
+            const int jid = ids[(start + k) % njobs];
+            const PtJobDev& J = jobs[jid];
+            unsigned long long issued = 0;
+            if (lane == 0) issued = *(volatile unsigned long long*)J.sample_ctr;
+            issued = __shfl_sync(kFull, issued, 0);
+            if (issued >= J.total) continue;
+            const unsigned want = __ballot_sync(kFull, need);
+            unsigned long long g0 = 0;
+            if (lane == 0) g0 = atomicAdd(J.sample_ctr, (unsigned long long)__popc(want));
+            g0 = __shfl_sync(kFull, g0, 0);
+            const unsigned long long g = g0 + __popc(want & ((1u << lane) - 1u));
+            if (need && g < J.total) {
+                const uint32_t pixel = (uint32_t)(g % (unsigned long long)J.npix);
+                const uint32_t sample = (uint32_t)(J.sample_begin + g / (unsigned long long)J.npix);
+                const uint32_t key = PathKey(J.set.seed, pixel, sample);
+                const int px = (int)(pixel % (uint32_t)J.cam.width), py = (int)(pixel / (uint32_t)J.cam.width);
+                // Box pixel filter of width 1: uniform jitter inside the pixel.
+                const float fx = (float)px + Rand(key, 0), fy = (float)py + Rand(key, 1);
+                const float sx = 2.0f * fx / (float)J.cam.width - 1.0f;
+                const float sy = 1.0f - 2.0f * fy / (float)J.cam.height;
+                const V3 d = normalize(mk(J.cam.fwd[0] + sx * J.cam.right[0] + sy * J.cam.up[0],
+                                          J.cam.fwd[1] + sx * J.cam.right[1] + sy * J.cam.up[1],
+                                          J.cam.fwd[2] + sx * J.cam.right[2] + sy * J.cam.up[2]));
+                const float hero = J.set.lmin + Rand(key, 2) * (J.set.lmax - J.set.lmin);
+                P.ray_o[slot] = make_float4(J.cam.pos[0], J.cam.pos[1], J.cam.pos[2], 0.0f);
+                P.ray_d[slot] = make_float4(d.x, d.y, d.z, __int_as_float(0x7f800000));
+                P.thr[slot] = make_float4(1.0f, 1.0f, 1.0f, 1.0f);
+                P.L[slot] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+                P.aux[slot] = make_float4(hero, 0.0f, __int_as_float(jid), 0.0f);
+                P.meta[slot] = make_uint4(pixel, sample, kFlagConsiderEmission, key);
+                got = true;
+                need = false;
+            }
         }
         const int at = WarpAppend(&Q.cnt[kCntActive], got);
         if (got) Q.active[at] = slot;
+        // Slots left without work stay queued for the next iteration, so
+        // jobs submitted later find them.
+        const bool idle = valid && !got;
+        const int fi = WarpAppend(&Q.cnt[kCntFreeNext], idle);
+        if (idle) Q.free_next[fi] = slot;
     }
 }
 
@@ -117,8 +140,11 @@ KRegen(PtPaths P, PtQueues Q, PtFilm F, PtJobParams J)
 // hit stores the leaf-order triangle slot for shading.
 template <class NodeT>
 __global__ void __launch_bounds__(kTraceBlock, 8)
-KExtend(const NodeT* __restrict__ nodes, PtScene S, PtPaths P, PtQueues Q)
+KExtend(const PtJobDev* __restrict__ jobs, PtPaths P, PtQueues Q)
 {
+    const NodeT* nodes = nullptr;
+    const GpuTri* tris = nullptr;
+    int ntri = 0;
     __shared__ int sstack[kTraceStack * kTraceBlock];
     int* stk = sstack + threadIdx.x;
     const long long n = Q.cnt[kCntActive];
@@ -131,6 +157,10 @@ KExtend(const NodeT* __restrict__ nodes, PtScene S, PtPaths P, PtQueues Q)
         if (got >= 0) {
             qi = got;
             slot = Q.active[qi];
+            const PtScene& S = jobs[__float_as_int(P.aux[slot].z)].scene;
+            nodes = (const NodeT*)S.nodes;
+            tris = S.tris;
+            ntri = S.ntri;
             const float4 o = P.ray_o[slot], d = P.ray_d[slot];
             Ray r;
             r.o[0] = o.x; r.o[1] = o.y; r.o[2] = o.z; r.tmin = o.w;
@@ -138,7 +168,7 @@ KExtend(const NodeT* __restrict__ nodes, PtScene S, PtPaths P, PtQueues Q)
             StartRay(s, r);
         }
         if (__all_sync(kFull, qi < 0)) break;
-        if (qi >= 0 && TraceRound<NodeT, false>(s, nodes, S.tris, S.ntri, stk, Q.err)) {
+        if (qi >= 0 && TraceRound<NodeT, false>(s, nodes, tris, ntri, stk, Q.err)) {
             P.hit[slot] = make_float4(s.best, __int_as_float(s.bestSlot), s.ba, s.bb);
             qi = -1;
         }
@@ -149,8 +179,11 @@ KExtend(const NodeT* __restrict__ nodes, PtScene S, PtPaths P, PtQueues Q)
 // contribution to the path's radiance.
 template <class NodeT>
 __global__ void __launch_bounds__(kTraceBlock, 8)
-KConnect(const NodeT* __restrict__ nodes, PtScene S, PtPaths P, PtQueues Q)
+KConnect(const PtJobDev* __restrict__ jobs, PtPaths P, PtQueues Q)
 {
+    const NodeT* nodes = nullptr;
+    const GpuTri* tris = nullptr;
+    int ntri = 0;
     __shared__ int sstack[kTraceStack * kTraceBlock];
     int* stk = sstack + threadIdx.x;
     const long long n = Q.cnt[kCntShadow];
@@ -162,13 +195,17 @@ KConnect(const NodeT* __restrict__ nodes, PtScene S, PtPaths P, PtQueues Q)
         if (got >= 0) {
             qi = got;
             const ShadowEntry e = Q.shadow[qi];
+            const PtScene& S = jobs[__float_as_int(P.aux[__float_as_int(e.d.w)].z)].scene;
+            nodes = (const NodeT*)S.nodes;
+            tris = S.tris;
+            ntri = S.ntri;
             Ray r;
             r.o[0] = e.o.x; r.o[1] = e.o.y; r.o[2] = e.o.z; r.tmin = 0.0f;
             r.d[0] = e.d.x; r.d[1] = e.d.y; r.d[2] = e.d.z; r.tmax = e.o.w;
             StartRay(s, r);
         }
         if (__all_sync(kFull, qi < 0)) break;
-        if (qi >= 0 && TraceRound<NodeT, true>(s, nodes, S.tris, S.ntri, stk, Q.err)) {
+        if (qi >= 0 && TraceRound<NodeT, true>(s, nodes, tris, ntri, stk, Q.err)) {
             if (s.bestSlot < 0) {
                 const ShadowEntry& e = Q.shadow[qi];
                 const int slot = __float_as_int(e.d.w);
@@ -214,18 +251,20 @@ __device__ __forceinline__ void EvalBsdf(const PtMaterial& M, const float* spect
 }
 
 __global__ void __launch_bounds__(kShadeBlock)
-KShade(PtScene S, PtPaths P, PtQueues Q, PtJobParams J)
+KShade(const PtJobDev* __restrict__ jobs, PtPaths P, PtQueues Q)
 {
     const int n = Q.cnt[kCntActive];
-    const PtSettings& set = J.set;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const int slot = Q.active[i];
+        const float4 aux = P.aux[slot];
+        const PtJobDev& J = jobs[__float_as_int(aux.z)];
+        const PtScene& S = J.scene;
+        const PtSettings& set = J.set;
         uint4 m = P.meta[slot];
         const float4 h = P.hit[slot];
         const float4 ro = P.ray_o[slot], rd = P.ray_d[slot];
         float4 thr = P.thr[slot];
         float4 L = P.L[slot];
-        const float4 aux = P.aux[slot];
         const int depth = (int)(m.z & kFlagDepthMask);
         const uint32_t key = m.w;
         const float bsdfPdf = aux.y;
@@ -490,7 +529,7 @@ KShade(PtScene S, PtPaths P, PtQueues Q, PtJobParams J)
             P.ray_o[slot] = make_float4(no.x, no.y, no.z, 0.0f);
             P.ray_d[slot] = make_float4(nd.x, nd.y, nd.z, __int_as_float(0x7f800000));
             P.thr[slot] = thr;
-            P.aux[slot] = make_float4(aux.x, npdf, 0.0f, 0.0f);
+            P.aux[slot] = make_float4(aux.x, npdf, aux.z, 0.0f);
             m.z = (m.z & ~(kFlagDepthMask | kFlagSpecular)) | (unsigned)(depth + 1) | nflags;
             P.meta[slot].z = m.z;
             cont = true;
@@ -517,15 +556,15 @@ __global__ void KSwap(int* cnt)
 }
 
 // Kahan-compensated fold of this call's film into the running sums.
-__global__ void KFold(PtFilm F, int n3)
+__global__ void KFold(float* pass, float* sum, float* comp, int n3)
 {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n3; i += gridDim.x * blockDim.x) {
-        const float y = F.pass[i] - F.comp[i];
-        const float s = F.sum[i];
+        const float y = pass[i] - comp[i];
+        const float s = sum[i];
         const float t = s + y;
-        F.comp[i] = (t - s) - y;
-        F.sum[i] = t;
-        F.pass[i] = 0.0f;
+        comp[i] = (t - s) - y;
+        sum[i] = t;
+        pass[i] = 0.0f;
     }
 }
 
@@ -548,37 +587,43 @@ cudaError_t PtSetGgxTables(const float* ess, const float* eavg)
     return e;
 }
 
-cudaError_t PtIteration(const PtLaunch& L, cudaStream_t st)
+cudaError_t PtIteration(const PtLaunch& L, int iter, cudaStream_t st)
 {
     const int shadeGrid = L.sms * 8;
-    KRegen<<<shadeGrid, kShadeBlock, 0, st>>>(L.paths, L.queues, L.film, L.params);
+    KRegen<<<shadeGrid, kShadeBlock, 0, st>>>(L.jobs, L.ids, L.njobs, L.paths, L.queues, iter, 1);
     cudaMemsetAsync(L.queues.trace_ctr, 0, 2 * sizeof(unsigned long long), st);
-    if (L.scene.layout == RTB200_BVH_Q8) {
+    if (L.layout == RTB200_BVH_Q8) {
         static int g = 0;
         if (!g) g = TraceGrid(KExtend<QNode4>, L.sms);
-        KExtend<QNode4><<<g, kTraceBlock, 0, st>>>((const QNode4*)L.scene.nodes, L.scene, L.paths, L.queues);
+        KExtend<QNode4><<<g, kTraceBlock, 0, st>>>(L.jobs, L.paths, L.queues);
     } else {
         static int g = 0;
         if (!g) g = TraceGrid(KExtend<GpuNode4>, L.sms);
-        KExtend<GpuNode4><<<g, kTraceBlock, 0, st>>>((const GpuNode4*)L.scene.nodes, L.scene, L.paths, L.queues);
+        KExtend<GpuNode4><<<g, kTraceBlock, 0, st>>>(L.jobs, L.paths, L.queues);
     }
-    KShade<<<shadeGrid, kShadeBlock, 0, st>>>(L.scene, L.paths, L.queues, L.params);
-    if (L.scene.layout == RTB200_BVH_Q8) {
+    KShade<<<shadeGrid, kShadeBlock, 0, st>>>(L.jobs, L.paths, L.queues);
+    if (L.layout == RTB200_BVH_Q8) {
         static int g = 0;
         if (!g) g = TraceGrid(KConnect<QNode4>, L.sms);
-        KConnect<QNode4><<<g, kTraceBlock, 0, st>>>((const QNode4*)L.scene.nodes, L.scene, L.paths, L.queues);
+        KConnect<QNode4><<<g, kTraceBlock, 0, st>>>(L.jobs, L.paths, L.queues);
     } else {
         static int g = 0;
         if (!g) g = TraceGrid(KConnect<GpuNode4>, L.sms);
-        KConnect<GpuNode4><<<g, kTraceBlock, 0, st>>>((const GpuNode4*)L.scene.nodes, L.scene, L.paths, L.queues);
+        KConnect<GpuNode4><<<g, kTraceBlock, 0, st>>>(L.jobs, L.paths, L.queues);
     }
     KSwap<<<1, 1, 0, st>>>(L.queues.cnt);
     return cudaGetLastError();
 }
 
-cudaError_t PtFold(const PtFilm& F, int npix, int sms, cudaStream_t st)
+cudaError_t PtDrain(const PtLaunch& L, cudaStream_t st)
 {
-    KFold<<<sms * 4, 256, 0, st>>>(F, 3 * npix);
+    KRegen<<<L.sms * 8, kShadeBlock, 0, st>>>(L.jobs, L.ids, L.njobs, L.paths, L.queues, 0, 0);
+    return cudaGetLastError();
+}
+
+cudaError_t PtFold(float* pass, float* sum, float* comp, int npix, int sms, cudaStream_t st)
+{
+    KFold<<<sms * 4, 256, 0, st>>>(pass, sum, comp, 3 * npix);
     return cudaGetLastError();
 }
 

@@ -6,22 +6,28 @@
 
 namespace rtb200 {
 
+// Everything one wavefront iteration needs.  `jobs` is the device job table;
+// `ids` (device) lists the `njobs` table entries that may receive new
+// samples.  Every job in one engine uses the same BVH layout.
 struct PtLaunch {
-    PtScene scene;
+    const PtJobDev* jobs;
+    const int* ids;
+    int njobs;
+    int layout;
     PtPaths paths;
     PtQueues queues;
-    PtFilm film;
-    PtJobParams params;
     int sms;
 };
 
 // One wavefront iteration (regenerate, extend, shade, connect, swap counters),
 // asynchronous on `st`.  The caller swaps queues.active/active_next and
 // queues.free_/free_next after each call.
-cudaError_t PtIteration(const PtLaunch& L, cudaStream_t st);
+cudaError_t PtIteration(const PtLaunch& L, int iter, cudaStream_t st);
+// Splat paths still marked finished into their films (end of a render).
+cudaError_t PtDrain(const PtLaunch& L, cudaStream_t st);
 // Upload the GGX E_ss (32 x 32) and E_avg (32) tables to constant memory.
 cudaError_t PtSetGgxTables(const float* ess, const float* eavg);
-// Fold this call's film into the compensated running sums and clear it.
-cudaError_t PtFold(const PtFilm& F, int npix, int sms, cudaStream_t st);
+// Fold a film of this request into the compensated running sums and clear it.
+cudaError_t PtFold(float* pass, float* sum, float* comp, int npix, int sms, cudaStream_t st);
 
 }  // namespace rtb200

@@ -146,13 +146,20 @@ struct PtFilm {
     float* comp;        // 3 floats per pixel, Kahan compensation
 };
 
-struct PtJobParams {
+// One image being rendered: its scene, camera, settings, film and sample
+// counters.  The engine's kernels read a table of these; every path slot
+// records which job it belongs to (aux.z).
+struct PtJobDev {
+    PtScene scene;
     PtCamera cam;
     PtSettings set;
     int npix;
-    int capacity;                 // path slots
-    unsigned long long sample_begin;   // first sample index of this call (per pixel)
-    unsigned long long total;     // npix * samples in this call
+    int pad;
+    float* film;                       // 3 floats per pixel, this request's samples
+    unsigned long long sample_begin;   // first sample index (per pixel) of the request
+    unsigned long long total;          // npix * spp of the request
+    unsigned long long* sample_ctr;    // samples handed out so far (device)
+    unsigned long long* done_ctr;      // samples finished and splatted (device)
 };
 
 }  // namespace rtb200

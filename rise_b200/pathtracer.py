@@ -99,3 +99,44 @@ class SpectralRasterizer:
             self.scene.close()
             self.scene = None
 
+
+class Engine:
+    """A shared wavefront (path pool + queues) for many jobs at once.
+
+    `render` batches whole requests; `submit` / `step` / `progress` /
+    `retire` drive continuous batching, where jobs join while others are in
+    flight (see rtb200_engine_* in include/rtb200.h).
+    """
+
+    def __init__(self, ctx, capacity=0):
+        self.ctx = ctx
+        h = ctypes.c_void_p()
+        check(lib().rtb200_engine_create(ctx.h, int(capacity), ctypes.byref(h)), ctx.h)
+        self.h = h
+
+    def render(self, rasterizers, spp, use_graph=True):
+        n = len(rasterizers)
+        jobs = (ctypes.c_void_p * n)(*[r.h.value for r in rasterizers])
+        counts = (ctypes.c_int32 * n)(*[int(s) for s in spp])
+        check(lib().rtb200_engine_render(self.h, jobs, counts, n, int(bool(use_graph))), self.ctx.h)
+
+    def submit(self, rasterizer, spp):
+        check(lib().rtb200_engine_submit(self.h, rasterizer.h, int(spp)), self.ctx.h)
+
+    def step(self, iterations=4, use_graph=True):
+        check(lib().rtb200_engine_step(self.h, int(iterations), int(bool(use_graph))), self.ctx.h)
+
+    def progress(self, rasterizer):
+        done, total = ctypes.c_int64(), ctypes.c_int64()
+        check(lib().rtb200_engine_progress(self.h, rasterizer.h, ctypes.byref(done), ctypes.byref(total)),
+              self.ctx.h)
+        return done.value, total.value
+
+    def retire(self, rasterizer):
+        check(lib().rtb200_engine_retire(self.h, rasterizer.h), self.ctx.h)
+
+    def close(self):
+        if self.h:
+            lib().rtb200_engine_destroy(self.h)
+            self.h = None
+
