@@ -48,6 +48,7 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-path-tracer", action="store_true")
     p.add_argument("--no-large", action="store_true", help="skip the 3.4M-triangle scene")
+    p.add_argument("--no-batch", action="store_true", help="skip the 48-scene batch and the serving run")
     p.add_argument("--pt-only", action="store_true",
                    help="run only the path-tracer measurement and print its JSON (for profiling)")
     return p.parse_args()
@@ -219,6 +220,82 @@ def bench_large_scene(ctx, layout="f32"):
            "mrays_s": ((s1["segments"] - s0["segments"]) + (s1["shadow_rays"] - s0["shadow_rays"])) / dt / 1e6}
     r.close()
     scene.close()
+    return out
+
+
+def bench_batch(ctx):
+    """48 uneven scenes (heightfield + 16 spheres; triangles log-uniform
+    10k-1M, resolutions 128^2..1024^2, spp log-uniform 4-256, max depth
+    8-16): one shared engine replaying a captured CUDA graph, against the
+    same jobs rendered one scene at a time on the same engine and kernels."""
+    from rise_b200 import pathtracer, scenes
+    params = scenes.batch_scene_params()
+    t0 = time.perf_counter()
+    descs = [scenes.batch_scene(p) for p in params]
+    devs = [pathtracer.upload_scene(ctx, d) for d in descs]
+    setup = time.perf_counter() - t0
+    spp = [p["spp"] for p in params]
+    total = sum(p["res"] ** 2 * p["spp"] for p in params)
+    eng = pathtracer.Engine(ctx, 1 << 21)
+    out = {"workload": "48 scenes, triangles log-uniform 10k-1M, resolutions {128,256,512,1024}^2, "
+                       "spp log-uniform 4-256, max depth 8-16, FP32 BVH", "samples": total,
+           "triangles": int(sum(p["n_tri"] for p in params)), "scene_setup_s": round(setup, 2)}
+    try:
+        # Warm-up (kernels, graph capture) on a small job.
+        w = pathtracer.SpectralRasterizer(ctx, descs[0], scene=devs[0])
+        eng.render([w], [1])
+        w.close()
+        one = [pathtracer.SpectralRasterizer(ctx, d, scene=s) for d, s in zip(descs, devs)]
+        t0 = time.perf_counter()
+        for r, s in zip(one, spp):
+            eng.render([r], [s], use_graph=False)
+        t_one = time.perf_counter() - t0
+        bat = [pathtracer.SpectralRasterizer(ctx, d, scene=s) for d, s in zip(descs, devs)]
+        t0 = time.perf_counter()
+        eng.render(bat, spp, use_graph=True)
+        t_bat = time.perf_counter() - t0
+        same = all(np.allclose(a.film(), b.film(), rtol=1e-4, atol=1e-6) for a, b in zip(one[:6], bat[:6]))
+        out.update({"one_by_one": {"seconds": t_one, "msamples_s": total / t_one / 1e6},
+                    "batched_graph": {"seconds": t_bat, "msamples_s": total / t_bat / 1e6},
+                    "speedup": t_one / t_bat, "films_equal_first6": bool(same)})
+        for r in one + bat:
+            r.close()
+    finally:
+        eng.close()
+        for s in devs:
+            s.close()
+    return out
+
+
+def bench_serving(ctx, rate=20.0, duration=8.0, resolutions=(128, 256)):
+    """Serving loop: Poisson arrivals, progressive 16 -> 64 -> 256 spp per
+    request, scenes drawn from a resident pool of the batched-scenes
+    distribution (resolutions limited to `resolutions` so a run fits in the
+    bench); continuous batching vs one request at a time."""
+    from rise_b200 import pathtracer, scenes, serving
+    params = scenes.batch_scene_params(n=12, seed=5, max_tri=300_000, resolutions=resolutions)
+    descs = [scenes.batch_scene(p) for p in params]
+    devs = [pathtracer.upload_scene(ctx, d) for d in descs]
+    pool = list(zip(descs, devs))
+    arrivals = serving.poisson_arrivals(rate, duration, seed=9)
+    rng = np.random.default_rng(10)
+
+    def make():
+        reqs = []
+        for i, t in enumerate(arrivals):
+            k = int(rng.integers(len(pool)))
+            st = scenes.RenderSettings(**{**descs[k].settings.__dict__, "seed": 1000 + i})
+            reqs.append(serving.Request(i, t, k, st))
+        return reqs
+    out = {"workload": f"Poisson {rate}/s for {duration}s, progressive 16/64/256 spp, 12 resident scenes "
+                       f"(triangles 10k-300k, resolutions {list(resolutions)}, depth 8-16)",
+           "requests": len(arrivals)}
+    try:
+        out["continuous"] = serving.serve(ctx, pool, make(), mode="continuous")
+        out["fifo"] = serving.serve(ctx, pool, make(), mode="fifo")
+    finally:
+        for s in devs:
+            s.close()
     return out
 
 
@@ -397,6 +474,9 @@ def main():
         out["path_tracer"] = bench_path_tracer(ctx, rank, cpu_baseline=world == 1 and not args.no_cpu_baseline)
         if not args.no_large:
             out["path_tracer_large"] = bench_large_scene(ctx)
+        if not args.no_batch:
+            out["batch"] = bench_batch(ctx)
+            out["serving"] = bench_serving(ctx)
     ctx.close()
     if world > 1:
         dist.barrier()

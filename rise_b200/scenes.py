@@ -269,6 +269,37 @@ def spheres_scene(grid=1024, n_spheres=64, sphere_tris=20000, width=1024, height
     return d
 
 
+RESOLUTIONS = (128, 256, 512, 1024)
+
+
+def batch_scene_params(n=48, seed=11, min_tri=10_000, max_tri=1_000_000, min_spp=4, max_spp=256,
+                       resolutions=RESOLUTIONS):
+    """Per-scene parameters of the batched-scenes distribution: triangle count
+    and spp log-uniform, resolution drawn from `resolutions` (square), max
+    depth 8-16."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(n):
+        out.append({
+            "n_tri": int(np.exp(rng.uniform(np.log(min_tri), np.log(max_tri)))),
+            "res": int(rng.choice(resolutions)),
+            "spp": int(round(np.exp(rng.uniform(np.log(min_spp), np.log(max_spp))))),
+            "max_depth": int(rng.integers(8, 17)),
+            "seed": int(rng.integers(1, 1 << 30)),
+        })
+    return out
+
+
+def batch_scene(p):
+    """A heightfield-plus-spheres scene of about p['n_tri'] triangles (60% in
+    the heightfield, 40% in 16 spheres) at p['res'] x p['res'] pixels."""
+    n_sph = 16
+    grid = max(8, int(np.sqrt(0.6 * p["n_tri"] / 2.0)) + 1)
+    sph = max(80, int(0.4 * p["n_tri"] / n_sph))
+    return spheres_scene(grid=grid, n_spheres=n_sph, sphere_tris=sph, width=p["res"], height=p["res"],
+                         seed=p["seed"] % 100000, max_depth=p["max_depth"])
+
+
 def cornell_box(width=256, height=256, spp_seed=1, nee_per_lambda=1, max_depth=8):
     """The 32-triangle spectral Cornell box.
 

@@ -96,6 +96,28 @@ def test_continuous_submission_equals_alone(ctx):
         eng.close()
 
 
+@pytest.mark.parametrize("mode", ["continuous", "fifo"])
+def test_serving_levels_complete_and_match_alone(ctx, mode):
+    from rise_b200 import serving
+    descs = [scenes.cornell_box(32, 32), scenes.spheres_scene(grid=32, n_spheres=4, sphere_tris=400,
+                                                              width=24, height=24, max_depth=8)]
+    devs = [pathtracer.upload_scene(ctx, d) for d in descs]
+    pool = list(zip(descs, devs))
+    reqs = []
+    for i, t in enumerate([0.0, 0.005, 0.01, 0.02, 0.03]):
+        k = i % 2
+        st = scenes.RenderSettings(**{**descs[k].settings.__dict__, "seed": 500 + i})
+        reqs.append(serving.Request(i, t, k, st, levels=(4, 8)))
+    try:
+        res = serving.serve(ctx, pool, reqs, mode=mode, capacity=1 << 14)
+        assert res["requests"] == 5 and set(res["latency"]) == {"4", "8"}
+        assert all(len(r.done_at) == 2 and r.done_at[0] <= r.done_at[1] for r in reqs)
+        assert res["latency"]["8"]["p99_s"] >= res["latency"]["4"]["p50_s"]
+    finally:
+        for s in devs:
+            s.close()
+
+
 def test_retire_before_done_is_refused(ctx):
     d = scenes.cornell_box(64, 64)
     eng = pathtracer.Engine(ctx, capacity=1 << 12)
