@@ -206,3 +206,90 @@ def ray_triangle(o, d, v0, ea, eb, kind="port"):
     t, a, b = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
     hit = fn(*[_p(x, _f64p) for x in arrs], ctypes.byref(t), ctypes.byref(a), ctypes.byref(b))
     return bool(hit), t.value, a.value, b.value
+
+
+# ---- path-tracer building blocks: port vs the reference's own code -------------
+
+_D = ctypes.c_double
+_BLOCK_SIGS = {
+    # name: (restype, argtypes) -- identical in both libraries unless noted
+    "sample_wavelengths": (None, [_D, _D, _D, _f64p]),
+    "ggx_d": (_D, [_D, _D]),
+    "ggx_lambda": (_D, [_D, _D]),
+    "ggx_g2": (_D, [_D, _D, _D]),
+    "vndf_pdf": (_D, [_f64p, _f64p, _f64p, _D]),
+    "lookup_ess": (_D, [_D, _D]),
+    "lookup_eavg": (_D, [_D]),
+    "ms_z": (_D, [_D]),
+    "ms_pdf": (_D, [_D, _D, _D]),
+    "ms_sample_cos": (_D, [_D, _D]),
+    "fresnel_avg": (_D, [_D, _D, _D]),
+    "fms": (_D, [_D, _D]),
+    "power_heuristic": (_D, [_D, _D]),
+}
+_ref_pt = None
+
+
+def _bind_blocks(lib, prefix):
+    for name, (res, args) in _BLOCK_SIGS.items():
+        f = getattr(lib, prefix + name)
+        f.restype = res
+        f.argtypes = args
+
+
+def port_blocks():
+    """liboracle.so with the path-tracer building blocks bound (orc_pt_*)."""
+    lib = port()
+    if not getattr(lib, "_blocks_bound", False):
+        _bind_blocks(lib, "orc_pt_")
+        lib.orc_pt_xyz_from_nm.restype = ctypes.c_int
+        lib.orc_pt_xyz_from_nm.argtypes = [_D, _f64p, _f64p]
+        lib.orc_pt_vndf_sample.restype = None
+        lib.orc_pt_vndf_sample.argtypes = [_f64p, _f64p, _f64p, _f64p, _D, _D, _D, _f64p]
+        lib.orc_pt_conductor_f.restype = _D
+        lib.orc_pt_conductor_f.argtypes = [_D, _D, _D, _D]
+        lib.orc_pt_dielectric_r.restype = _D
+        lib.orc_pt_dielectric_r.argtypes = [_D, _D, _D, _D]
+        lib.orc_pt_russian_roulette.restype = ctypes.c_int
+        lib.orc_pt_russian_roulette.argtypes = [ctypes.c_int, ctypes.c_int, _D, _D, _D, _D, _f64p]
+        lib.orc_pt_tables.restype = None
+        lib.orc_pt_tables.argtypes = [_f64p, _f64p]
+        lib.orc_pt_set_tables.restype = None
+        lib.orc_pt_set_tables.argtypes = [_f64p, _f64p]
+        lib._blocks_bound = True
+    return lib
+
+
+def ref_blocks():
+    """_ref/libref_pt.so (the reference's own helpers, ref_pt_*) or None."""
+    global _ref_pt
+    if _ref_pt is None:
+        path = os.path.join(_HERE, "_ref", "libref_pt.so")
+        if not os.path.exists(path):
+            return None
+        lib = ctypes.CDLL(path)
+        _bind_blocks(lib, "ref_pt_")
+        lib.ref_pt_xyz_from_nm.restype = ctypes.c_int
+        lib.ref_pt_xyz_from_nm.argtypes = [_D, _f64p]
+        lib.ref_pt_cie_y_integral.restype = _D
+        lib.ref_pt_cie_y_integral.argtypes = [_D, _D]
+        lib.ref_pt_vndf_sample.restype = None
+        lib.ref_pt_vndf_sample.argtypes = [_f64p, _f64p, _D, _D, _D, _f64p, _f64p]
+        lib.ref_pt_conductor_f.restype = _D
+        lib.ref_pt_conductor_f.argtypes = [_f64p, _f64p, _D, _D, _D]
+        lib.ref_pt_dielectric_r.restype = _D
+        lib.ref_pt_dielectric_r.argtypes = [_f64p, _f64p, _f64p, _D, _D]
+        lib.ref_pt_russian_roulette.restype = ctypes.c_int
+        lib.ref_pt_russian_roulette.argtypes = [ctypes.c_uint, ctypes.c_uint, _D, _D, _D, _D, _f64p]
+        lib.ref_pt_tables.restype = None
+        lib.ref_pt_tables.argtypes = [_f64p, _f64p]
+        _ref_pt = lib
+    return _ref_pt
+
+
+def energy_tables(lib, prefix):
+    """(E_ss 32 x 32, E_avg 32) of the port (prefix 'orc_pt_') or reference ('ref_pt_')."""
+    ess = np.zeros(1024)
+    eavg = np.zeros(32)
+    getattr(lib, prefix + "tables")(_p(ess, _f64p), _p(eavg, _f64p))
+    return ess.reshape(32, 32), eavg

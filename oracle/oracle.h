@@ -73,6 +73,31 @@ int orc_pt_render(const float* tri9, int64_t n_tri, const int64_t* meshes, int32
                   const int32_t* seti, int32_t spp, int32_t sample_begin, int32_t x0, int32_t y0,
                   int32_t x1, int32_t y1, int32_t threads, double* xyz, const double* cie);
 
+/* Building blocks of the path-tracing oracle, exported so tests can hold each
+ * against the reference's own code (oracle/_ref/libref_pt.so). */
+void   orc_pt_sample_wavelengths(double u, double lmin, double lmax, double* lam4);
+int    orc_pt_xyz_from_nm(double nm, const double* cie, double* xyz3);
+double orc_pt_ggx_d(double alpha, double cos_h);
+double orc_pt_ggx_lambda(double alpha, double cos_t);
+double orc_pt_ggx_g2(double alpha, double cos_i, double cos_o);
+void   orc_pt_vndf_sample(const double* wi, const double* t, const double* b, const double* n, double alpha,
+                          double u1, double u2, double* m);
+double orc_pt_vndf_pdf(const double* wi, const double* wo, const double* n, double alpha);
+double orc_pt_conductor_f(double cos_i, double ni, double nt, double k);
+double orc_pt_dielectric_r(double cos_i, double cos_t, double ni, double nt);
+double orc_pt_lookup_ess(double c, double alpha);
+double orc_pt_lookup_eavg(double alpha);
+double orc_pt_ms_z(double alpha);
+double orc_pt_ms_pdf(double c, double alpha, double z);
+double orc_pt_ms_sample_cos(double alpha, double u);
+double orc_pt_fresnel_avg(double ni, double nt, double k);
+double orc_pt_fms(double favg, double eavg);
+double orc_pt_power_heuristic(double a, double b);
+int    orc_pt_russian_roulette(int depth, int min_depth, double threshold, double cur, double prev, double u,
+                               double* survival);
+void   orc_pt_tables(double* ess, double* eavg);
+void   orc_pt_set_tables(const double* ess, const double* eavg);
+
 #ifdef __cplusplus
 }
 /* Double-precision ray queries used by the path-tracing oracle. */

@@ -136,10 +136,14 @@ double ConductorF(double cosI, double ni, double nt, double kt)
 struct Tables {
     double ess[32][32];
     double eavg[32];
+    double msz[32];   // multiple-scattering lobe normalisation per alpha row
     double glx[21], glw[21];
 };
 
-const Tables& GetTables()
+void ComputeMsZ(Tables& T);
+int kEssStrata = 128;   // strata per axis of each E_ss cell
+
+Tables& MutableTables()
 {
     static Tables T;
     static std::once_flag once;
@@ -162,32 +166,38 @@ const Tables& GetTables()
             T.glx[i] = 0.5 * (z + 1.0);
             T.glw[i] = 1.0 / ((1.0 - z * z) * dp * dp);
         }
-        // E_ss(mu, alpha) by stratified visible-normal integration.
+        // E_ss(mu, alpha) by stratified visible-normal integration of the
+        // reference table's estimator (tools/GenerateMicrofacetEnergyLUT.cpp:
+        // reflect the view direction about a visible normal, weight by the
+        // masking G1 of the reflected direction), and E_avg by its midpoint
+        // sum 2 * sum(E_ss mu) / 32.
         for (int a = 0; a < 32; ++a) {
             const double alpha = 0.01 + 0.99 * a / 31.0;
             double avg = 0.0;
             for (int c = 0; c < 32; ++c) {
                 const double mu = (c + 0.5) / 32.0;
                 const V wo = {std::sqrt(std::max(0.0, 1.0 - mu * mu)), 0.0, mu};
-                const double g1o = 1.0 / (1.0 + Lambda(alpha, mu));
+                const int ns = kEssStrata;
                 double sum = 0.0;
-                for (int i = 0; i < 64; ++i)
-                    for (int j = 0; j < 64; ++j) {
-                        const V m = VndfLocal(wo, alpha, (i + 0.5) / 64.0, (j + 0.5) / 64.0);
+                for (int i = 0; i < ns; ++i)
+                    for (int j = 0; j < ns; ++j) {
+                        const V m = VndfLocal(wo, alpha, (i + 0.5) / ns, (j + 0.5) / ns);
                         const double d = Dot(wo, m);
                         if (d <= 0) continue;
-                        const V wi = m * (2.0 * d) - wo;
+                        const V wi = Norm(m * (2.0 * d) - wo);
                         if (wi.z <= 0) continue;
-                        sum += (1.0 / (1.0 + Lambda(alpha, mu) + Lambda(alpha, wi.z))) / g1o;
+                        sum += 1.0 / (1.0 + Lambda(alpha, wi.z));
                     }
-                T.ess[a][c] = sum / 4096.0;
+                T.ess[a][c] = sum / ((double)ns * ns);
                 avg += T.ess[a][c] * mu;
             }
             T.eavg[a] = 2.0 * avg / 32.0;
         }
+        ComputeMsZ(T);
     });
     return T;
 }
+const Tables& GetTables() { return MutableTables(); }
 
 double LookupEss(double cosT, double alpha)
 {
@@ -209,6 +219,94 @@ double LookupEavg(double alpha)
     const double af = a - a0;
     return (1 - af) * T.eavg[a0] + af * T.eavg[a1];
 }
+// ---- multiple-scattering lobe sampler (MicrofacetEnergyLUT.h:122-333) --------
+// E_ss is piecewise linear in mu between bin centres (flat outside the first
+// and last centre), so the lobe shape (1 - E_ss(mu)) mu is piecewise quadratic:
+// 33 segments with a closed-form cubic CDF, inverted by Newton steps kept
+// inside a bisection bracket.
+struct MsSeg { double lo, hi, e0, slope; };
+
+void MsSegments(const double row[32], MsSeg seg[33])
+{
+    seg[0] = {0.0, 0.5 / 32.0, row[0], 0.0};
+    for (int k = 0; k < 31; ++k) {
+        const double a = (k + 0.5) / 32.0, b = (k + 1.5) / 32.0;
+        seg[k + 1] = {a, b, row[k], (row[k + 1] - row[k]) / (b - a)};
+    }
+    seg[32] = {31.5 / 32.0, 1.0, row[31], 0.0};
+}
+double MsShape(const MsSeg& s, double y) { return std::max(0.0, (1.0 - (s.e0 + s.slope * y)) * (s.lo + y)); }
+double MsCdf(const MsSeg& s, double y)
+{
+    const double P = (1.0 - s.e0) * s.lo, Q = (1.0 - s.e0) - s.slope * s.lo, R = -s.slope;
+    return P * y + Q * y * y * 0.5 + R * y * y * y * (1.0 / 3.0);
+}
+double MsInvert(const MsSeg& s, double target, double w)
+{
+    double lo = 0.0, hi = w, y = 0.5 * w;
+    for (int it = 0; it < 30; ++it) {
+        const double diff = MsCdf(s, y) - target;
+        if (std::fabs(diff) < 1e-13) break;
+        if (diff > 0) hi = y; else lo = y;
+        const double dv = MsShape(s, y);
+        double nx = dv > 1e-12 ? y - diff / dv : 0.5 * (lo + hi);
+        if (!(nx > lo && nx < hi)) nx = 0.5 * (lo + hi);
+        y = nx;
+    }
+    return y;
+}
+void AlphaRow(double alpha, int& a0, int& a1, double& af)
+{
+    const double a = std::max(0.0, std::min(1.0, (alpha - 0.01) / 0.99)) * 31.0;
+    a0 = (int)a;
+    a1 = std::min(a0 + 1, 31);
+    af = a - a0;
+}
+void ComputeMsZ(Tables& T)
+{
+    for (int r = 0; r < 32; ++r) {
+        MsSeg seg[33];
+        MsSegments(T.ess[r], seg);
+        double I = 0.0;
+        for (const MsSeg& s : seg) I += MsCdf(s, s.hi - s.lo);
+        T.msz[r] = 2.0 * I;
+    }
+}
+double MsZ(double alpha)
+{
+    const Tables& T = GetTables();
+    int a0, a1;
+    double af;
+    AlphaRow(alpha, a0, a1, af);
+    return (1.0 - af) * T.msz[a0] + af * T.msz[a1];
+}
+double MsPdf(double c, double alpha, double z)
+{
+    if (z <= 1e-15) return 0.0;
+    c = std::max(0.0, std::min(1.0, c));
+    return std::max(0.0, (1.0 - LookupEss(c, alpha)) * c / (kPi * z));
+}
+double MsSampleCos(double alpha, double u)
+{
+    const Tables& T = GetTables();
+    int a0, a1;
+    double af;
+    AlphaRow(alpha, a0, a1, af);
+    double row[32];
+    for (int k = 0; k < 32; ++k) row[k] = (1.0 - af) * T.ess[a0][k] + af * T.ess[a1][k];
+    MsSeg seg[33];
+    MsSegments(row, seg);
+    double tot[33], I = 0.0;
+    for (int k = 0; k < 33; ++k) { tot[k] = MsCdf(seg[k], seg[k].hi - seg[k].lo); I += tot[k]; }
+    if (I <= 1e-15) return std::max(0.0, std::min(1.0, u));
+    const double target = std::max(0.0, std::min(I, u * I));
+    int k = 0;
+    double run = 0.0;
+    while (k < 32 && run + tot[k] < target) { run += tot[k]; ++k; }
+    const double y = MsInvert(seg[k], std::max(0.0, std::min(tot[k], target - run)), seg[k].hi - seg[k].lo);
+    return std::max(0.0, std::min(1.0, seg[k].lo + y));
+}
+
 double FresnelAvg(double ni, double nt, double kt)
 {
     const Tables& T = GetTables();
@@ -266,6 +364,28 @@ inline double Spec(const Scene& S, int id, double nm)
 }
 inline double PowerHeuristic(double a, double b) { return a * a / (a * a + b * b); }
 
+// SampledWavelengths::SampleEquidistant (SampledWavelengths.h:79-106): hero
+// uniform in [lmin, lmax], companions a quarter range apart with wrap-around.
+inline void Wavelengths(double u, double lmin, double lmax, double lam[4])
+{
+    const double range = lmax - lmin;
+    lam[0] = lmin + u * range;
+    for (int i = 1; i < 4; ++i) lam[i] = lmin + std::fmod(lam[0] - lmin + i * (range / 4.0), range);
+}
+
+// EvaluateRussianRoulette (PathTransportUtilities.h:86-110): returns true to
+// terminate; `survival` is the probability to divide by (1 when not applied).
+inline bool RussianRoulette(int depth, int minDepth, double threshold, double cur, double prev, double u,
+                            double& survival)
+{
+    survival = 1.0;
+    if (depth < minDepth) return false;
+    const double prob = std::min(1.0, cur / std::max(prev, threshold));
+    if (u >= prob) return true;
+    if (prob > 0 && prob < 1) survival = prob;
+    return false;
+}
+
 Ggx GgxAt(const Scene& S, int mat, double lam)
 {
     Ggx g;
@@ -299,8 +419,8 @@ double GgxPdf(const Ggx& g, V n, V gn, V r, V v)
     const double cv = Dot(v, n);
     if (cv <= 0 || Dot(v, gn) <= 0) return 0.0;
     const double ws = g.spec, wms = ws * (1.0 - LookupEss(Dot(r, n), g.alpha)), total = ws + wms;
-    if (total <= 1e-10) return 0.0;
-    return (wms * cv * kInvPi + ws * VndfPdf(r, v, n, g.alpha)) / total;
+    if (total < 1e-10) return cv * kInvPi;
+    return (wms * MsPdf(cv, g.alpha, MsZ(g.alpha)) + ws * VndfPdf(r, v, n, g.alpha)) / total;
 }
 
 void EvalBsdf(const Scene& S, int mat, double lam, V ns, V gn, V r, V v, double& f, double& pdf)
@@ -338,11 +458,8 @@ void Sample(const Scene& S, uint32_t pixel, uint32_t sample, double xyz[3])
     const double sx = 2.0 * fx / S.width - 1.0, sy = 1.0 - 2.0 * fy / S.height;
     V d = Norm(S.fwd + S.right * sx + S.up * sy);
     V o = S.pos;
-    const double hero = S.lmin + Rand(key, 2) * (S.lmax - S.lmin);
     double lam[4];
-    const double range = S.lmax - S.lmin;
-    lam[0] = hero;
-    for (int i = 1; i < 4; ++i) lam[i] = S.lmin + std::fmod(hero - S.lmin + i * range / 4.0, range);
+    Wavelengths(Rand(key, 2), S.lmin, S.lmax, lam);
     double thr[4] = {1, 1, 1, 1}, L[4] = {0, 0, 0, 0};
     double bsdfPdf = 0.0;
     for (int depth = 0; depth < S.maxDepth; ++depth) {
@@ -471,6 +588,7 @@ void Sample(const Scene& S, uint32_t pixel, uint32_t sample, double xyz[3])
                 const double ws = g0.spec, wms = ws * (1.0 - LookupEss(cosR, g0.alpha)), total = ws + wms;
                 if (!(total > 1e-10)) break;
                 const double pSpec = ws / total, pMS = wms / total;
+                const double msz = MsZ(g0.alpha);
                 double khero;
                 if (Rand(key, Dim(depth, 18)) < pSpec) {
                     const V wl = {Dot(r, tx), Dot(r, ty), Dot(r, w)};
@@ -483,21 +601,25 @@ void Sample(const Scene& S, uint32_t pixel, uint32_t sample, double xyz[3])
                     if (!(cosO > 0 && Dot(nd, gn) > 0)) break;
                     const double vpdf = VndfPdf(r, nd, w, g0.alpha);
                     if (!(vpdf > 1e-10)) break;
-                    npdf = (wms * cosO * kInvPi + ws * vpdf) / total;
+                    npdf = (wms * MsPdf(cosO, g0.alpha, msz) + ws * vpdf) / total;
                     const double G2 = 1.0 / (1.0 + Lambda(g0.alpha, cosR) + Lambda(g0.alpha, cosO));
                     const double G1 = 1.0 / (1.0 + Lambda(g0.alpha, cosR));
                     khero = g0.spec * ConductorF(rm, 1.0, g0.eta, g0.k) * G2 / (G1 * pSpec);
                 } else {
-                    const double phi = 2.0 * kPi * u1, sint = std::sqrt(u2), cost = std::sqrt(1.0 - u2);
+                    // Multiple-scattering lobe: mu from (1 - E_ss(mu)) mu, uniform azimuth.
+                    const double eavg = LookupEavg(g0.alpha);
+                    if (!(pMS > 1e-10 && 1.0 - eavg > 1e-10)) break;
+                    const double cost = MsSampleCos(g0.alpha, u1), sint = std::sqrt(std::max(0.0, 1.0 - cost * cost));
+                    const double phi = 2.0 * kPi * u2;
                     nd = Norm(tx * (std::cos(phi) * sint) + ty * (std::sin(phi) * sint) + w * cost);
                     const double cosO = Dot(nd, w);
-                    if (!(cosO > 0 && Dot(nd, gn) > 0) || !(pMS > 1e-10)) break;
-                    npdf = (wms * cosO * kInvPi + ws * VndfPdf(r, nd, w, g0.alpha)) / total;
-                    const double eavg = LookupEavg(g0.alpha);
-                    if (!(1.0 - eavg > 1e-10)) break;
+                    if (!(cosO > 0 && Dot(nd, gn) > 0)) break;
+                    const double mpdf = MsPdf(cosO, g0.alpha, msz);
+                    npdf = (wms * mpdf + ws * VndfPdf(r, nd, w, g0.alpha)) / total;
                     const double fms = Fms(g0.spec * g0.favg, eavg) * (1.0 - LookupEss(cosO, g0.alpha)) *
                                        (1.0 - LookupEss(cosR, g0.alpha)) / (kPi * (1.0 - eavg));
-                    khero = fms * kPi / pMS;
+                    if (!(mpdf > 1e-14)) break;
+                    khero = fms * cosO / (mpdf * pMS);
                 }
                 if (!(npdf > 0)) break;
                 kray[0] = khero;
@@ -517,12 +639,11 @@ void Sample(const Scene& S, uint32_t pixel, uint32_t sample, double xyz[3])
             currMax = std::max(currMax, std::fabs(thr[k] * kray[k]));
         }
         if (currMax <= kNearZero) break;
-        if (depth >= S.rrMinDepth) {
-            const double prob = std::min(1.0, currMax / std::max(prevMax, S.rrThreshold));
-            if (Rand(key, Dim(depth, 19)) >= prob) break;
-            if (prob > 0 && prob < 1)
-                for (double& k : kray) k /= prob;
-        }
+        double survival;
+        if (RussianRoulette(depth, S.rrMinDepth, S.rrThreshold, currMax, prevMax, Rand(key, Dim(depth, 19)), survival))
+            break;
+        if (survival != 1.0)
+            for (double& k : kray) k /= survival;
         if (depth + 1 >= S.maxDepth) break;
         for (int k = 0; k < 4; ++k) thr[k] *= kray[k];
         bsdfPdf = npdf;
@@ -656,3 +777,81 @@ extern "C" int orc_pt_render(const float* tri9, int64_t n_tri, const int64_t* me
     orc_bvh_destroy(S.bvh);
     return 0;
 }
+
+// ---- building blocks, exported for the component checks against the
+// reference's own code (tests only) ------------------------------------------
+
+extern "C" {
+
+void orc_pt_sample_wavelengths(double u, double lmin, double lmax, double* lam4) { Wavelengths(u, lmin, lmax, lam4); }
+
+int orc_pt_xyz_from_nm(double nm, const double* cie, double* xyz3)
+{
+    int i, j;
+    double w;
+    xyz3[0] = xyz3[1] = xyz3[2] = 0.0;
+    if (!Interp(nm, i, j, w)) return 0;
+    for (int c = 0; c < 3; ++c) xyz3[c] = cie[81 * c + i] + w * (cie[81 * c + j] - cie[81 * c + i]);
+    return 1;
+}
+
+double orc_pt_ggx_d(double alpha, double cosH) { return GgxD(alpha, cosH); }
+double orc_pt_ggx_lambda(double alpha, double cosT) { return Lambda(alpha, cosT); }
+double orc_pt_ggx_g2(double alpha, double ci, double co) { return 1.0 / (1.0 + Lambda(alpha, ci) + Lambda(alpha, co)); }
+
+// Visible-normal sample in the frame (t, b, n), as the path sampler draws it.
+void orc_pt_vndf_sample(const double* wi, const double* t, const double* b, const double* n, double alpha, double u1,
+                        double u2, double* m)
+{
+    const V r = {wi[0], wi[1], wi[2]}, tx = {t[0], t[1], t[2]}, ty = {b[0], b[1], b[2]}, w = {n[0], n[1], n[2]};
+    const V wl = {Dot(r, tx), Dot(r, ty), Dot(r, w)};
+    const V ml = VndfLocal(wl, alpha, u1, u2);
+    const V mh = Norm(tx * ml.x + ty * ml.y + w * ml.z);
+    m[0] = mh.x; m[1] = mh.y; m[2] = mh.z;
+}
+
+double orc_pt_vndf_pdf(const double* wi, const double* wo, const double* n, double alpha)
+{
+    return VndfPdf({wi[0], wi[1], wi[2]}, {wo[0], wo[1], wo[2]}, {n[0], n[1], n[2]}, alpha);
+}
+
+double orc_pt_conductor_f(double cosI, double ni, double nt, double k) { return ConductorF(cosI, ni, nt, k); }
+double orc_pt_dielectric_r(double cosI, double cosT, double ni, double nt) { return DielectricR(cosI, cosT, ni, nt); }
+double orc_pt_lookup_ess(double c, double alpha) { return LookupEss(c, alpha); }
+double orc_pt_lookup_eavg(double alpha) { return LookupEavg(alpha); }
+double orc_pt_ms_z(double alpha) { return MsZ(alpha); }
+double orc_pt_ms_pdf(double c, double alpha, double z) { return MsPdf(c, alpha, z); }
+double orc_pt_ms_sample_cos(double alpha, double u) { return MsSampleCos(alpha, u); }
+double orc_pt_fresnel_avg(double ni, double nt, double k) { return FresnelAvg(ni, nt, k); }
+double orc_pt_fms(double favg, double eavg) { return Fms(favg, eavg); }
+double orc_pt_power_heuristic(double a, double b) { return PowerHeuristic(a, b); }
+
+int orc_pt_russian_roulette(int depth, int min_depth, double threshold, double cur, double prev, double u,
+                            double* survival)
+{
+    return RussianRoulette(depth, min_depth, threshold, cur, prev, u, *survival) ? 1 : 0;
+}
+
+// Read the energy tables (E_ss 32 x 32 row-major by alpha, E_avg 32).
+void orc_pt_tables(double* ess, double* eavg)
+{
+    const Tables& T = GetTables();
+    for (int a = 0; a < 32; ++a) {
+        for (int c = 0; c < 32; ++c) ess[32 * a + c] = T.ess[a][c];
+        eavg[a] = T.eavg[a];
+    }
+}
+
+// Replace the energy tables (to check the lookups and the sampler on the
+// reference's own table values).  Not thread-safe: call with no render running.
+void orc_pt_set_tables(const double* ess, const double* eavg)
+{
+    Tables& T = MutableTables();
+    for (int a = 0; a < 32; ++a) {
+        for (int c = 0; c < 32; ++c) T.ess[a][c] = ess[32 * a + c];
+        T.eavg[a] = eavg[a];
+    }
+    ComputeMsZ(T);
+}
+
+}  // extern "C"

@@ -1,0 +1,137 @@
+// ref_pt_harness.cpp -- TEST INFRASTRUCTURE ONLY (oracle).
+//
+// A thin C-ABI harness around the reference renderer's own building blocks of
+// the spectral path tracer, so the oracle's restatement of each can be checked
+// against the reference's code on the same inputs:
+//   * hero + companion wavelengths     Utilities/Color/SampledWavelengths.h:79-106
+//   * CIE 1931 lookup, Y integral      Utilities/Color/ColorUtils.cpp:270-348
+//   * GGX D, Lambda, G2, VNDF          Utilities/MicrofacetUtils.h:66-371
+//   * energy tables, multiple-scattering lobe sampler and pdf, Fresnel average,
+//     F_ms                             Utilities/MicrofacetEnergyLUT.h
+//   * conductor / dielectric Fresnel   Utilities/Optics.hpp, Utilities/Optics.cpp:101-160
+//   * Russian roulette, power heuristic  Utilities/PathTransportUtilities.h:86-110, :251
+// The recipe in oracle/Makefile compiles this file with the reference headers
+// and ColorUtils.cpp / Color.cpp where they lie (never copied into this
+// repository) into oracle/_ref/libref_pt.so.  Only tests load it.
+
+// The reference headers are order-dependent: ColorUtils.h comes last.
+#include "Utilities/Color/SampledWavelengths.h"
+#include "Utilities/MicrofacetUtils.h"
+#include "Utilities/MicrofacetEnergyLUT.h"
+#include "Utilities/Optics.h"
+#include "Utilities/OrthonormalBasis3D.h"
+#include "Utilities/PathTransportUtilities.h"
+#include "Utilities/Color/ColorUtils.h"
+#include "Interfaces/ILog.h"
+
+namespace RISE
+{
+	// Optics.cpp reports total internal reflection through GlobalLog(); the
+	// harness does not link the reference's log subsystem.
+	class QuietPtLog : public ILog
+	{
+	public:
+		void Print( LOG_ENUM, const char* ) const override {}
+		void PrintEx( LOG_ENUM, const char*, ... ) const override {}
+		void PrintNew( const void*, const char*, const int, const char* ) const override {}
+		void PrintNew( const IReference*, const char*, const int, const char* ) const override {}
+		void PrintDelete( const void*, const char*, const int ) const override {}
+		void PrintDelete( const IReference*, const char*, const int ) const override {}
+		void FlushPrinters() override {}
+	};
+	ILog* GlobalLog() { static QuietPtLog log; return &log; }
+}
+
+using namespace RISE;
+
+namespace {
+inline Vector3 V(const double* p) { return Vector3(p[0], p[1], p[2]); }
+inline void Put(const Vector3& v, double* p) { p[0] = v.x; p[1] = v.y; p[2] = v.z; }
+}  // namespace
+
+extern "C" {
+
+void ref_pt_sample_wavelengths(double u, double lmin, double lmax, double* lam4)
+{
+    const SampledWavelengths s = SampledWavelengths::SampleEquidistant(u, lmin, lmax);
+    for (int i = 0; i < 4; ++i) lam4[i] = s.lambda[i];
+}
+
+int ref_pt_xyz_from_nm(double nm, double* xyz3)
+{
+    XYZPel p(0, 0, 0);
+    const bool ok = ColorUtils::XYZFromNM(p, nm);
+    xyz3[0] = p.X; xyz3[1] = p.Y; xyz3[2] = p.Z;
+    return ok ? 1 : 0;
+}
+
+double ref_pt_cie_y_integral(double a, double b) { return ColorUtils::CIE_Y_Integral(a, b); }
+
+double ref_pt_ggx_d(double alpha, double cosH) { return MicrofacetUtils::GGX_D<Scalar>(alpha, cosH); }
+double ref_pt_ggx_lambda(double alpha, double cosT) { return MicrofacetUtils::GGX_Lambda(alpha, cosT); }
+double ref_pt_ggx_g2(double alpha, double ci, double co) { return MicrofacetUtils::GGX_G2(alpha, ci, co); }
+
+// Visible-normal sample in the reference frame built from n (CreateFromW);
+// the frame is returned so the restatement can sample in the same frame.
+void ref_pt_vndf_sample(const double* wi, const double* n, double alpha, double u1, double u2, double* m,
+                        double* onb9)
+{
+    OrthonormalBasis3D onb;
+    onb.CreateFromW(V(n));
+    Put(MicrofacetUtils::VNDF_Sample_Aniso(V(wi), onb, alpha, alpha, u1, u2), m);
+    Put(onb.u(), onb9);
+    Put(onb.v(), onb9 + 3);
+    Put(onb.w(), onb9 + 6);
+}
+
+double ref_pt_vndf_pdf(const double* wi, const double* wo, const double* n, double alpha)
+{
+    OrthonormalBasis3D onb;
+    onb.CreateFromW(V(n));
+    return MicrofacetUtils::VNDF_Pdf_Aniso(V(wi), V(wo), onb, alpha, alpha);
+}
+
+double ref_pt_conductor_f(const double* v, const double* n, double ni, double nt, double k)
+{
+    return Optics::CalculateConductorReflectance<Scalar>(V(v), V(n), ni, nt, k);
+}
+
+double ref_pt_dielectric_r(const double* v, const double* tv, const double* n, double ni, double nt)
+{
+    return Optics::CalculateDielectricReflectance(V(v), V(tv), V(n), ni, nt);
+}
+
+double ref_pt_lookup_ess(double c, double alpha) { return MicrofacetEnergyLUT::LookupEss(c, alpha); }
+double ref_pt_lookup_eavg(double alpha) { return MicrofacetEnergyLUT::LookupEavg(alpha); }
+double ref_pt_ms_z(double alpha) { return MicrofacetEnergyLUT::MSLobeZ(alpha); }
+double ref_pt_ms_pdf(double c, double alpha, double z) { return MicrofacetEnergyLUT::MSPdf(c, alpha, z); }
+double ref_pt_ms_sample_cos(double alpha, double u) { return MicrofacetEnergyLUT::SampleMSCosTheta(alpha, u); }
+
+double ref_pt_fresnel_avg(double ni, double nt, double k)
+{
+    return MicrofacetEnergyLUT::ComputeFresnelAvg<Scalar>(Vector3(0, 0, 1), ni, nt, k);
+}
+
+double ref_pt_fms(double favg, double eavg) { return MicrofacetEnergyLUT::ComputeFms<Scalar>(favg, eavg); }
+
+void ref_pt_tables(double* ess, double* eavg)
+{
+    for (int a = 0; a < MicrofacetEnergyLUT::LUT_SIZE; ++a) {
+        for (int c = 0; c < MicrofacetEnergyLUT::LUT_SIZE; ++c)
+            ess[a * MicrofacetEnergyLUT::LUT_SIZE + c] = MicrofacetEnergyLUT::E_ss_TABLE[a][c];
+        eavg[a] = MicrofacetEnergyLUT::E_avg_TABLE[a];
+    }
+}
+
+double ref_pt_power_heuristic(double a, double b) { return PathTransportUtilities::PowerHeuristic(a, b); }
+
+int ref_pt_russian_roulette(unsigned depth, unsigned min_depth, double threshold, double cur, double prev, double u,
+                            double* survival)
+{
+    const PathTransportUtilities::RussianRouletteResult r =
+        PathTransportUtilities::EvaluateRussianRoulette(depth, min_depth, threshold, cur, prev, u);
+    *survival = r.survivalProb;
+    return r.terminate ? 1 : 0;
+}
+
+}  // extern "C"

@@ -187,6 +187,10 @@ int rtb200_scene_commit(rtb200_scene* s, int32_t layout)
     cudaSetDevice(ctx->device);
     const auto t0 = std::chrono::steady_clock::now();
     BuildReferenceBVH(s->tri9.data(), n_tri, 0, s->bvh);
+    s->stack_bound = TraceStackBound(s->bvh);
+    if (s->stack_bound > kTraceStackMax)
+        return SetError(ctx, RTB200_E_INVALID, "BVH deeper than the traversal stack (" +
+                        std::to_string(s->stack_bound) + " > " + std::to_string(kTraceStackMax) + " entries)");
     std::vector<GpuTri> tris;
     EncodeTriangles(s->tri9.data(), s->bvh, tris);
     std::vector<GpuNode4> nf;

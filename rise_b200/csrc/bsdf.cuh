@@ -9,7 +9,9 @@
 //                Kulla-Conty multiple-scattering lobe F_ms (1-E(mu_o))(1-E(mu_i)) /
 //                (pi (1-E_avg)) (Utilities/MicrofacetEnergyLUT.h).  Lobes are picked
 //                with the reference's weights w_s = specular colour, w_ms = w_s (1 -
-//                E(mu_i)); the multiple-scattering lobe is sampled cosine-weighted.
+//                E(mu_i)); the multiple-scattering lobe samples mu_o from its own
+//                shape (1 - E(mu_o)) mu_o by exact inversion of the piecewise-cubic
+//                CDF, with the matching density (MicrofacetEnergyLUT.h:122-333).
 //   Dielectric   DielectricSPF (Materials/DielectricSPF.cpp:120-451): smooth
 //                interface, Fresnel-weighted choice between mirror reflection and
 //                Snell refraction (delta lobes, no BSDF).
@@ -19,10 +21,15 @@
 namespace rtb200 {
 
 constexpr int kLut = 32;
-// E_ss / E_avg tables, uploaded at scene commit (defined here: this header is
-// compiled into exactly one translation unit, pathtrace.cu).
-__constant__ float c_ess[kLut * kLut];
-__constant__ float c_eavg[kLut];
+// Energy tables, uploaded at the first scene commit (defined here: this header
+// is compiled into exactly one translation unit, pathtrace.cu).  They live in
+// global memory and are read through the read-only cache: lanes of a warp
+// shade different materials and roughnesses, and divergent indices would
+// serialise constant-memory reads.
+__device__ float g_ess[kLut * kLut];          // E_ss[alpha row][mu cell]
+__device__ float g_eavg[kLut];
+__device__ float g_msz[kLut];                 // per row: 2 * integral of (1 - E_ss(mu)) mu dmu
+__device__ float g_mscum[kLut * (kLut + 2)];  // per row: integral of the lobe shape up to each segment
 
 // MicrofacetEnergyLUT::LookupEss / LookupEavg (MicrofacetEnergyLUT.h:90-120):
 // bilinear in (alpha, mu) with mu at cell centres.
@@ -37,8 +44,8 @@ __device__ __forceinline__ float LookupEss(float cosT, float alpha)
     const int c0 = (int)c;
     const int c1 = min(c0 + 1, kLut - 1);
     const float cf = c - (float)c0;
-    const float v00 = c_ess[a0 * kLut + c0], v01 = c_ess[a0 * kLut + c1];
-    const float v10 = c_ess[a1 * kLut + c0], v11 = c_ess[a1 * kLut + c1];
+    const float v00 = __ldg(g_ess + a0 * kLut + c0), v01 = __ldg(g_ess + a0 * kLut + c1);
+    const float v10 = __ldg(g_ess + a1 * kLut + c0), v11 = __ldg(g_ess + a1 * kLut + c1);
     return (1 - af) * ((1 - cf) * v00 + cf * v01) + af * ((1 - cf) * v10 + cf * v11);
 }
 
@@ -48,7 +55,103 @@ __device__ __forceinline__ float LookupEavg(float alpha)
     const int a0 = (int)a;
     const int a1 = min(a0 + 1, kLut - 1);
     const float af = a - (float)a0;
-    return (1 - af) * c_eavg[a0] + af * c_eavg[a1];
+    return (1 - af) * __ldg(g_eavg + a0) + af * __ldg(g_eavg + a1);
+}
+
+__device__ __forceinline__ void AlphaRow(float alpha, int& a0, int& a1, float& af)
+{
+    const float a = fmaxf(0.0f, fminf(1.0f, (alpha - 0.01f) / 0.99f)) * (kLut - 1);
+    a0 = (int)a;
+    a1 = min(a0 + 1, kLut - 1);
+    af = a - (float)a0;
+}
+
+// Normalisation Z(alpha) of the multiple-scattering lobe shape (1 - E(mu)) mu
+// (MSLobeZ): exact per table row, linear in the row blend.
+__device__ __forceinline__ float MsZ(float alpha)
+{
+    int a0, a1;
+    float af;
+    AlphaRow(alpha, a0, a1, af);
+    return (1.0f - af) * __ldg(g_msz + a0) + af * __ldg(g_msz + a1);
+}
+
+// Solid-angle density of the multiple-scattering lobe sampler (MSPdf).
+__device__ __forceinline__ float MsPdf(float c, float alpha, float z)
+{
+    if (z <= 1e-15f) return 0.0f;
+    c = fmaxf(0.0f, fminf(1.0f, c));
+    return fmaxf(0.0f, (1.0f - LookupEss(c, alpha)) * c / (kPi * z));
+}
+
+// Segment k (0 .. kLut) of the alpha-blended piecewise-linear E(mu): flat caps
+// below the first and above the last cell centre, linear spans between.
+struct MsSeg {
+    float lo, w, e0, slope;
+};
+
+__device__ __forceinline__ MsSeg MsSegment(int a0, int a1, float af, int k)
+{
+    MsSeg s;
+    const int j0 = max(k - 1, 0), j1 = min(k, kLut - 1);
+    const float r0 = (1.0f - af) * __ldg(g_ess + a0 * kLut + j0) + af * __ldg(g_ess + a1 * kLut + j0);
+    const float r1 = (1.0f - af) * __ldg(g_ess + a0 * kLut + j1) + af * __ldg(g_ess + a1 * kLut + j1);
+    s.lo = k == 0 ? 0.0f : (k - 0.5f) / kLut;
+    s.w = (k == 0 || k == kLut) ? 0.5f / kLut : 1.0f / kLut;
+    s.e0 = k == 0 ? r1 : r0;
+    s.slope = (k == 0 || k == kLut) ? 0.0f : (r1 - r0) * kLut;
+    return s;
+}
+
+// Integral of the lobe shape over the first y of a segment.
+__device__ __forceinline__ float MsCdf(const MsSeg& s, float y)
+{
+    const float P = (1.0f - s.e0) * s.lo, Q = (1.0f - s.e0) - s.slope * s.lo, R = -s.slope;
+    return y * (P + y * (0.5f * Q + y * (R * (1.0f / 3.0f))));
+}
+
+// Integral of the lobe shape over segments 0 .. k-1 of the blended row.  The
+// segment integrals are linear in the row values, hence in the row blend, so
+// the per-row cumulative tables blend exactly like E_ss itself.
+__device__ __forceinline__ float MsCum(int a0, int a1, float af, int k)
+{
+    return (1.0f - af) * __ldg(g_mscum + a0 * (kLut + 2) + k) + af * __ldg(g_mscum + a1 * (kLut + 2) + k);
+}
+
+// mu_o for the multiple-scattering lobe from one uniform number
+// (SampleMSCosTheta): find the segment whose cumulative integral brackets
+// u * I (binary search over the 33 segments), then invert its cubic CDF by
+// Newton steps kept inside a bisection bracket.
+__device__ __forceinline__ float MsSampleCos(float alpha, float u)
+{
+    int a0, a1;
+    float af;
+    AlphaRow(alpha, a0, a1, af);
+    const float I = MsCum(a0, a1, af, kLut + 1);
+    if (!(I > 1e-15f)) return fmaxf(0.0f, fminf(1.0f, u));
+    const float target = fmaxf(0.0f, fminf(I, u * I));
+    // Largest k in [0, kLut] with cum(k) < target (segment k holds the target).
+    int lo_k = 0, hi_k = kLut;
+    while (lo_k < hi_k) {
+        const int mid = (lo_k + hi_k + 1) >> 1;
+        if (MsCum(a0, a1, af, mid) < target) lo_k = mid; else hi_k = mid - 1;
+    }
+    const int k = lo_k;
+    const MsSeg s = MsSegment(a0, a1, af, k);
+    const float run = MsCum(a0, a1, af, k);
+    const float tot = MsCdf(s, s.w);
+    const float goal = fmaxf(0.0f, fminf(tot, target - run));
+    float lo = 0.0f, hi = s.w, y = 0.5f * s.w;
+    for (int it = 0; it < 30; ++it) {
+        const float diff = MsCdf(s, y) - goal;
+        if (fabsf(diff) <= 1e-7f * tot) break;
+        if (diff > 0.0f) hi = y; else lo = y;
+        const float dv = fmaxf(0.0f, (1.0f - (s.e0 + s.slope * y)) * (s.lo + y));
+        float nx = dv > 1e-12f ? y - diff / dv : 0.5f * (lo + hi);
+        if (!(nx > lo && nx < hi)) nx = 0.5f * (lo + hi);
+        y = nx;
+    }
+    return fmaxf(0.0f, fminf(1.0f, s.lo + y));
 }
 
 __device__ __forceinline__ float GgxLambda(float alpha, float cosT)
@@ -133,39 +236,70 @@ __device__ __forceinline__ GgxParams GgxAt(const PtMaterial& M, const float* spe
     return g;
 }
 
-// GGXBRDF::valueNM: r = towards the viewer, v = towards the light, n the
-// shading normal on the viewer's side, gn the geometric normal facing the
-// incoming ray.
-__device__ __forceinline__ float GgxValue(const GgxParams& g, V3 n, V3 gn, V3 r, V3 v)
+// ---- evaluation split by what depends on the wavelength ----------------------
+// Roughness is the same at every wavelength, so the microfacet terms, the
+// energy-table lookups and the sampling density are computed once per shading
+// point or direction pair; only the Fresnel terms and the specular colour are
+// evaluated per wavelength.
+
+// Per shading point: E_ss at the viewer direction, E_avg and the
+// multiple-scattering lobe normalisation.
+struct GgxPoint {
+    float alpha, essR, eavg, msz;
+};
+
+__device__ __forceinline__ GgxPoint GgxPointAt(float alpha, float cosR)
 {
-    const float nr = dot(n, r), nv = dot(n, v);
-    if (nr < kNearZero || nv < kNearZero) return 0.0f;
-    if (dot(v, gn) <= 0.0f || dot(r, gn) <= 0.0f) return 0.0f;
-    const V3 h = normalize(v + r);
-    const float D = GgxD(g.alpha, dot(h, n));
-    const float G2 = 1.0f / (1.0f + GgxLambda(g.alpha, nv) + GgxLambda(g.alpha, nr));
-    float f = 0.0f;
-    const float sf = D * G2 / (4.0f * nv * nr);
-    if (sf > 0.0f) f = g.spec * ConductorF(dot(r, h), 1.0f, g.eta, g.k) * sf;
-    const float eavg = LookupEavg(g.alpha);
-    if (1.0f - eavg > 1e-10f) {
-        const float fm = (1.0f - LookupEss(nr, g.alpha)) * (1.0f - LookupEss(nv, g.alpha)) / (kPi * (1.0f - eavg));
-        f += Fms(g.spec * g.favg, eavg) * fm;
-    }
-    return f;
+    GgxPoint g;
+    g.alpha = fmaxf(alpha, 1e-4f);
+    g.essR = LookupEss(cosR, g.alpha);
+    g.eavg = LookupEavg(g.alpha);
+    g.msz = MsZ(g.alpha);
+    return g;
 }
 
-// Mixture pdf of the GGX sampler at one wavelength (GGXSPF::Pdf); r towards
-// the viewer, v the sampled direction.
-__device__ __forceinline__ float GgxPdf(const GgxParams& g, V3 n, V3 gn, V3 r, V3 v)
+// Per (viewer r, light v) pair: the single-scattering factor D G2 / (4 nv nr)
+// and Fresnel cosine, the multiple-scattering factor (1-E(nr))(1-E(nv)) /
+// (pi (1-E_avg)), and the sampling density, which does not depend on the
+// specular colour (the lobe weights w_s and w_s (1 - E(nr)) share it).
+struct GgxPair {
+    float sf, rh, ms, pdf;
+    bool ok;
+};
+
+__device__ __forceinline__ GgxPair GgxPairAt(const GgxPoint& g, V3 n, V3 gn, V3 r, V3 v)
 {
-    const float cosV = dot(v, n);
-    if (cosV <= 0.0f || dot(v, gn) <= 0.0f) return 0.0f;
-    const float ws = g.spec;
-    const float wms = ws * (1.0f - LookupEss(dot(r, n), g.alpha));
-    const float total = ws + wms;
-    if (total <= 1e-10f) return 0.0f;
-    return (wms * cosV * kInvPi + ws * VndfPdf(r, v, n, g.alpha)) / total;
+    GgxPair q;
+    q.sf = q.rh = q.ms = q.pdf = 0.0f;
+    const float nr = dot(n, r), nv = dot(n, v);
+    q.ok = nr >= kNearZero && nv >= kNearZero && dot(v, gn) > 0.0f && dot(r, gn) > 0.0f;
+    if (!q.ok) return q;
+    const V3 h = normalize(v + r);
+    const float ch = dot(h, n);
+    const float D = GgxD(g.alpha, ch);
+    const float lr = GgxLambda(g.alpha, nr);
+    const float G2 = 1.0f / (1.0f + GgxLambda(g.alpha, nv) + lr);
+    q.sf = D * G2 / (4.0f * nv * nr);
+    q.rh = dot(r, h);
+    const float essV = LookupEss(nv, g.alpha);
+    if (1.0f - g.eavg > 1e-10f) q.ms = (1.0f - g.essR) * (1.0f - essV) / (kPi * (1.0f - g.eavg));
+    // VNDF pdf of reflecting r into v (MicrofacetUtils VNDF_Pdf).
+    const float oh = dot(v, h);
+    float vndf = 0.0f;
+    if (nr >= 1e-10f && ch > 0.0f && q.rh > 0.0f && oh >= 1e-10f)
+        vndf = (1.0f / (1.0f + lr)) * q.rh * D / nr / (4.0f * oh);
+    const float mspdf = g.msz <= 1e-15f ? 0.0f : fmaxf(0.0f, (1.0f - essV) * fminf(nv, 1.0f) / (kPi * g.msz));
+    q.pdf = ((1.0f - g.essR) * mspdf + vndf) / (2.0f - g.essR);
+    return q;
+}
+
+// The BSDF at one wavelength for a pair (GGXBRDF::valueNM).
+__device__ __forceinline__ float GgxValueAt(const GgxPair& q, const GgxParams& p, float eavg)
+{
+    if (!q.ok) return 0.0f;
+    float f = 0.0f;
+    if (q.sf > 0.0f) f = p.spec * ConductorF(q.rh, 1.0f, p.eta, p.k) * q.sf;
+    return f + Fms(p.spec * p.favg, eavg) * q.ms;
 }
 
 // Visible-normal sample around n for the view direction r (local frame

@@ -469,6 +469,23 @@ void EncodeQuantNodes(const BuiltBVH& b, std::vector<QNode4>& out)
     }
 }
 
+int TraceStackBound(const BuiltBVH& b)
+{
+    if (b.nodes4.empty()) return 0;
+    int bound = 0;
+    std::vector<std::pair<int32_t, int>> todo{{0, 0}};   // (node, entries deferred above it)
+    while (!todo.empty()) {
+        const auto [ni, above] = todo.back();
+        todo.pop_back();
+        const Node4& n = b.nodes4[ni];
+        const int here = above + (n.nchild > 0 ? n.nchild - 1 : 0);
+        bound = std::max(bound, here);
+        for (int i = 0; i < n.nchild; ++i)
+            if (n.count[i] == 0) todo.push_back({n.child[i], here});
+    }
+    return bound;
+}
+
 void EncodeTriangles(const float* tri9, const BuiltBVH& b, std::vector<GpuTri>& out)
 {
     out.resize(b.prims.size());

@@ -90,4 +90,17 @@ void EncodeGpuNodes(const BuiltBVH& b, std::vector<GpuNode4>& out);
 void EncodeQuantNodes(const BuiltBVH& b, std::vector<QNode4>& out);
 void EncodeTriangles(const float* tri9, const BuiltBVH& b, std::vector<GpuTri>& out);
 
+// Upper bound on the traversal stack depth of the BVH4: the largest sum of
+// (children - 1) over the internal nodes of one root-to-node path.  A
+// depth-first walk that continues into one child and pushes the others holds
+// at most this many deferred entries.
+int TraceStackBound(const BuiltBVH& b);
+
+// Traversal stack of the device kernels: kTraceStackShared entries per thread
+// in shared memory; scenes whose bound is larger run kernels that continue the
+// stack in local memory up to kTraceStackMax entries.  A scene whose bound
+// exceeds kTraceStackMax is refused at commit.
+constexpr int kTraceStackShared = 40;
+constexpr int kTraceStackMax = 128;
+
 }  // namespace rtb200

@@ -49,6 +49,7 @@ struct rtb200_scene {
     bool committed = false;
     int32_t layout = RTB200_BVH_F32;
     int64_t n_nodes = 0;
+    int32_t stack_bound = 0;         // TraceStackBound of the committed BVH
     double build_seconds = 0.0;
     rtb200::BuiltBVH bvh;            // kept for the path tracer's emitter tables
     // device data

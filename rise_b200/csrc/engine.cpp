@@ -97,7 +97,9 @@ struct rtb200_engine {
     int iter = 0;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     cudaGraphExec_t gexec = nullptr;
-    int gnjobs = -1;
+    int gnjobs = -1;                       // launch shape the graph was captured for
+    int glayout = -1;
+    bool gspill = false;
     long long seg_seen = 0, shadow_seen = 0;
 };
 
@@ -110,6 +112,8 @@ PtLaunch MakeLaunch(const rtb200_engine* e)
     L.ids = e->d_ids;
     L.njobs = (int)e->active.size();
     L.layout = e->layout;
+    L.spill = false;
+    for (int k : e->active) L.spill |= e->owner[k]->scene->stack_bound > kTraceStackShared;
     L.paths = e->paths;
     L.queues = e->queues;
     L.sms = e->ctx->num_sms;
@@ -261,7 +265,7 @@ int EngineStep(rtb200_engine* e, int iterations, bool graph)
     PtLaunch L = MakeLaunch(e);
     cudaError_t err = cudaSuccess;
     if (graph) {
-        if (!e->gexec || e->gnjobs != L.njobs) {
+        if (!e->gexec || e->gnjobs != L.njobs || e->glayout != L.layout || e->gspill != L.spill) {
             DropGraph(e);
             cudaGraph_t g = nullptr;
             err = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
@@ -277,6 +281,8 @@ int EngineStep(rtb200_engine* e, int iterations, bool graph)
             if (g) cudaGraphDestroy(g);
             if (err != cudaSuccess) { DropGraph(e); return CudaCheck(ctx, err, "graph capture"); }
             e->gnjobs = L.njobs;
+            e->glayout = L.layout;
+            e->gspill = L.spill;
         }
         const int reps = (iterations + kGraphIters - 1) / kGraphIters;
         for (int r = 0; r < reps && err == cudaSuccess; ++r) err = cudaGraphLaunch(e->gexec, st);

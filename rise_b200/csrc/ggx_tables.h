@@ -8,6 +8,10 @@ constexpr int kGgxLut = 32;
 struct GgxTables {
     float ess[kGgxLut * kGgxLut];  // [alpha][mu]
     float eavg[kGgxLut];
+    float msz[kGgxLut];            // per alpha row: 2 * integral of (1 - E_ss(mu)) mu dmu
+    // per alpha row: integral of (1 - E_ss(mu)) mu over the segments before
+    // segment k, k = 0 .. kGgxLut + 1 (the last entry is the whole integral)
+    float mscum[kGgxLut * (kGgxLut + 2)];
 };
 
 // Computed once per process (thread-safe).

@@ -138,7 +138,7 @@ KRegen(const PtJobDev* __restrict__ jobs, const int* __restrict__ ids, int njobs
 
 // Closest hit for every active path.  Same while-while walk as KTrace; the
 // hit stores the leaf-order triangle slot for shading.
-template <class NodeT>
+template <class NodeT, bool SPILL>
 __global__ void __launch_bounds__(kTraceBlock, 8)
 KExtend(const PtJobDev* __restrict__ jobs, PtPaths P, PtQueues Q)
 {
@@ -146,7 +146,8 @@ KExtend(const PtJobDev* __restrict__ jobs, PtPaths P, PtQueues Q)
     const GpuTri* tris = nullptr;
     int ntri = 0;
     __shared__ int sstack[kTraceStack * kTraceBlock];
-    int* stk = sstack + threadIdx.x;
+    int spill[SPILL ? kTraceSpill : 1];
+    const TraceStack stk{sstack + threadIdx.x, spill};
     const long long n = Q.cnt[kCntActive];
     WarpFeed feed{0ull, 0ull, false};
     TraceState s;
@@ -168,7 +169,7 @@ KExtend(const PtJobDev* __restrict__ jobs, PtPaths P, PtQueues Q)
             StartRay(s, r);
         }
         if (__all_sync(kFull, qi < 0)) break;
-        if (qi >= 0 && TraceRound<NodeT, false>(s, nodes, tris, ntri, stk, Q.err)) {
+        if (qi >= 0 && TraceRound<NodeT, false, SPILL>(s, nodes, tris, ntri, stk, Q.err)) {
             P.hit[slot] = make_float4(s.best, __int_as_float(s.bestSlot), s.ba, s.bb);
             qi = -1;
         }
@@ -177,7 +178,7 @@ KExtend(const PtJobDev* __restrict__ jobs, PtPaths P, PtQueues Q)
 
 // Any hit for the shadow-ray queue; unoccluded entries add their
 // contribution to the path's radiance.
-template <class NodeT>
+template <class NodeT, bool SPILL>
 __global__ void __launch_bounds__(kTraceBlock, 8)
 KConnect(const PtJobDev* __restrict__ jobs, PtPaths P, PtQueues Q)
 {
@@ -185,7 +186,8 @@ KConnect(const PtJobDev* __restrict__ jobs, PtPaths P, PtQueues Q)
     const GpuTri* tris = nullptr;
     int ntri = 0;
     __shared__ int sstack[kTraceStack * kTraceBlock];
-    int* stk = sstack + threadIdx.x;
+    int spill[SPILL ? kTraceSpill : 1];
+    const TraceStack stk{sstack + threadIdx.x, spill};
     const long long n = Q.cnt[kCntShadow];
     WarpFeed feed{0ull, 0ull, false};
     TraceState s;
@@ -205,7 +207,7 @@ KConnect(const PtJobDev* __restrict__ jobs, PtPaths P, PtQueues Q)
             StartRay(s, r);
         }
         if (__all_sync(kFull, qi < 0)) break;
-        if (qi >= 0 && TraceRound<NodeT, true>(s, nodes, tris, ntri, stk, Q.err)) {
+        if (qi >= 0 && TraceRound<NodeT, true, SPILL>(s, nodes, tris, ntri, stk, Q.err)) {
             if (s.bestSlot < 0) {
                 const ShadowEntry& e = Q.shadow[qi];
                 const int slot = __float_as_int(e.d.w);
@@ -230,24 +232,29 @@ __device__ __forceinline__ void PushShadow(const PtQueues& Q, V3 o, V3 d, float 
     Q.shadow[at] = e;
 }
 
-// BSDF value and sampling pdf at one wavelength for NEE (Lambertian or GGX).
-__device__ __forceinline__ void EvalBsdf(const PtMaterial& M, const float* spectra, float lam, V3 ns, V3 ng,
-                                         V3 r, V3 v, float& f, float& pdf)
+// Wavelength-independent BSDF data of a next-event direction v seen from r:
+// the GGX pair, or for Lambertian the same-side gate and pdf |nv|/pi
+// (LambertianBRDF::valueNM + LambertianSPF::Pdf, ShouldReflect at
+// LambertianBRDF.cpp:44-75).  The sampling pdf is wavelength-independent.
+__device__ __forceinline__ GgxPair NeePair(const PtMaterial& M, const GgxPoint& gp, V3 ns, V3 ng, V3 r, V3 v)
 {
-    if (M.type == kMatGGX) {
-        const V3 n = dot(r, ns) < 0.0f ? -ns : ns;
-        const GgxParams g = GgxAt(M, spectra, lam);
-        f = GgxValue(g, n, ng, r, v);
-        pdf = GgxPdf(g, n, ng, r, v);
-    } else {
-        // LambertianBRDF::valueNM + LambertianSPF::Pdf: same side of the
-        // surface as the viewer (ShouldReflect, LambertianBRDF.cpp:44-75).
-        const float nr = dot(ns, r), nv = dot(ns, v);
-        const bool same = (nr >= kNearZero && nv >= kNearZero) || (nr <= -kNearZero && nv <= -kNearZero);
-        const bool gate = dot(v, ng) > 0.0f && dot(r, ng) > 0.0f;
-        f = (same && gate) ? Spec(spectra, M.refl, lam) * kInvPi : 0.0f;
-        pdf = (same && gate) ? fabsf(nv) * kInvPi : 0.0f;
-    }
+    if (M.type == kMatGGX) return GgxPairAt(gp, dot(r, ns) < 0.0f ? -ns : ns, ng, r, v);
+    GgxPair q;
+    const float nr = dot(ns, r), nv = dot(ns, v);
+    const bool same = (nr >= kNearZero && nv >= kNearZero) || (nr <= -kNearZero && nv <= -kNearZero);
+    q.ok = same && dot(v, ng) > 0.0f && dot(r, ng) > 0.0f;
+    q.sf = q.rh = q.ms = 0.0f;
+    q.pdf = q.ok ? fabsf(nv) * kInvPi : 0.0f;
+    return q;
+}
+
+// The BSDF value at one wavelength for a next-event pair.
+__device__ __forceinline__ float NeeValue(const PtMaterial& M, const float* spectra, float lam, const GgxPair& q,
+                                          float eavg)
+{
+    if (!q.ok) return 0.0f;
+    if (M.type == kMatGGX) return GgxValueAt(q, GgxAt(M, spectra, lam), eavg);
+    return Spec(spectra, M.refl, lam) * kInvPi;
 }
 
 __global__ void __launch_bounds__(kShadeBlock)
@@ -354,6 +361,8 @@ KShade(const PtJobDev* __restrict__ jobs, PtPaths P, PtQueues Q)
             } else {
                 const V3 ns = ng;
                 const V3 r = -d;
+                GgxPoint gp{1.0f, 0.0f, 0.0f, 0.0f};
+                if (M.type == kMatGGX) gp = GgxPointAt(M.alpha, fabsf(dot(r, ns)));
                 // PART 2: next-event estimation (LightSampler::EvaluateDirectLightingNM,
                 // LightSampler.cpp:1942-2361): one area-light sample and one sky
                 // sample per wavelength (reference) or one shared sample.
@@ -396,11 +405,12 @@ KShade(const PtJobDev* __restrict__ jobs, PtPaths P, PtQueues Q)
                                 const float plight = lg.pdf * (dist * dist) / (lg.area * cosL);
                                 float4 c = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
                                 bool any = false;
+                                const GgxPair bq = NeePair(M, gp, ns, gnv, r, toL);
+                                const float pb = bq.pdf;
                                 for (int j = 0; j < 4; ++j) {
                                     if (term & (1u << j)) continue;
                                     if (set.nee_per_lambda && j != k) continue;
-                                    float f, pb;
-                                    EvalBsdf(M, S.spectra, lam[j], ns, gnv, r, toL, f, pb);
+                                    const float f = NeeValue(M, S.spectra, lam[j], bq, gp.eavg);
                                     const float w = (pb > 0.0f ? PowerHeuristic(plight, pb) : 1.0f) / lg.pdf;
                                     const float v = Get(thr, j) * Spec(S.spectra, lg.emit, lam[j]) * cosS * geom * f * w;
                                     Set(c, j, v);
@@ -423,11 +433,12 @@ KShade(const PtJobDev* __restrict__ jobs, PtPaths P, PtQueues Q)
                         if (cosE > 0.0f) {
                             float4 c = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
                             bool any = false;
+                            const GgxPair bq = NeePair(M, gp, ns, gnv, r, dir);
+                            const float pb = bq.pdf;
                             for (int j = 0; j < 4; ++j) {
                                 if (term & (1u << j)) continue;
                                 if (set.nee_per_lambda && j != k) continue;
-                                float f, pb;
-                                EvalBsdf(M, S.spectra, lam[j], ns, gnv, r, dir, f, pb);
+                                const float f = NeeValue(M, S.spectra, lam[j], bq, gp.eavg);
                                 const float w = pb > 0.0f ? PowerHeuristic(kInv4Pi, pb) : 1.0f;
                                 const float v = Get(thr, j) * Spec(S.spectra, set.env, lam[j]) * f * cosE / kInv4Pi * w;
                                 Set(c, j, v);
@@ -448,10 +459,11 @@ KShade(const PtJobDev* __restrict__ jobs, PtPaths P, PtQueues Q)
                     const GgxParams g0 = GgxAt(M, S.spectra, lam[0]);
                     const float cosR = dot(r, w);
                     const float ws = g0.spec;
-                    const float wms = ws * (1.0f - LookupEss(cosR, g0.alpha));
+                    const float wms = ws * (1.0f - gp.essR);
                     const float total = ws + wms;
                     if (!(total > 1e-10f)) break;
                     const float pSpec = ws / total, pMS = wms / total;
+                    const float msz = gp.msz;
                     float khero = 0.0f;
                     if (Rand(key, Dim(depth, 18)) < pSpec) {
                         const V3 mh = VndfSample(r, tx, ty, w, g0.alpha, u1, u2);
@@ -462,35 +474,38 @@ KShade(const PtJobDev* __restrict__ jobs, PtPaths P, PtQueues Q)
                         if (!(cosO > 0.0f && dot(nd, gn) > 0.0f)) break;
                         const float vpdf = VndfPdf(r, nd, w, g0.alpha);
                         if (!(vpdf > 1e-10f)) break;
-                        npdf = (wms * cosO * kInvPi + ws * vpdf) / total;
+                        npdf = (wms * MsPdf(cosO, g0.alpha, msz) + ws * vpdf) / total;
                         const float G2 = 1.0f / (1.0f + GgxLambda(g0.alpha, cosR) + GgxLambda(g0.alpha, cosO));
                         const float G1 = 1.0f / (1.0f + GgxLambda(g0.alpha, cosR));
                         khero = g0.spec * ConductorF(rm, 1.0f, g0.eta, g0.k) * G2 / (G1 * pSpec);
                     } else {
-                        // Multiple-scattering lobe, cosine-sampled.
-                        const float phi = 2.0f * kPi * u1;
-                        const float sint = sqrtf(u2), cost = sqrtf(1.0f - u2);
+                        // Multiple-scattering lobe: mu_o from (1 - E(mu_o)) mu_o,
+                        // uniform azimuth (GGXSPF.cpp:604-675).
+                        const float eavg = gp.eavg;
+                        if (!(pMS > 1e-10f && 1.0f - eavg > 1e-10f)) break;
+                        const float cost = MsSampleCos(g0.alpha, u1);
+                        const float sint = sqrtf(fmaxf(0.0f, 1.0f - cost * cost));
                         float sp, cp;
-                        __sincosf(phi, &sp, &cp);
+                        __sincosf(2.0f * kPi * u2, &sp, &cp);
                         nd = normalize(tx * (cp * sint) + ty * (sp * sint) + w * cost);
                         const float cosO = dot(nd, w);
-                        if (!(cosO > 0.0f && dot(nd, gn) > 0.0f) || !(pMS > 1e-10f)) break;
-                        npdf = (wms * cosO * kInvPi + ws * VndfPdf(r, nd, w, g0.alpha)) / total;
-                        const float eavg = LookupEavg(g0.alpha);
-                        if (!(1.0f - eavg > 1e-10f)) break;
+                        if (!(cosO > 0.0f && dot(nd, gn) > 0.0f)) break;
+                        const float mpdf = MsPdf(cosO, g0.alpha, msz);
+                        if (!(mpdf > 1e-14f)) break;
+                        npdf = (wms * mpdf + ws * VndfPdf(r, nd, w, g0.alpha)) / total;
                         const float fms = Fms(g0.spec * g0.favg, eavg) * (1.0f - LookupEss(cosO, g0.alpha)) *
-                                          (1.0f - LookupEss(cosR, g0.alpha)) / (kPi * (1.0f - eavg));
-                        khero = fms * kPi / pMS;   // f cos / (cos/pi) / pMS
+                                          (1.0f - gp.essR) / (kPi * (1.0f - eavg));
+                        khero = fms * cosO / (mpdf * pMS);
                     }
                     if (!(npdf > 0.0f)) break;
                     Set(kray, 0, (term & 1u) ? 0.0f : khero);
                     const float cosV = fabsf(dot(nd, ns));
                     // Companions evaluate the BSDF in the hero's direction and
                     // divide by the hero's pdf (:4676-4714).
+                    const GgxPair cq = GgxPairAt(gp, w, gnv, r, nd);
                     for (int k = 1; k < 4; ++k) {
                         if (term & (1u << k)) continue;
-                        const GgxParams gk = GgxAt(M, S.spectra, lam[k]);
-                        Set(kray, k, GgxValue(gk, w, gnv, r, nd) * cosV / npdf);
+                        Set(kray, k, GgxValueAt(cq, GgxAt(M, S.spectra, lam[k]), gp.eavg) * cosV / npdf);
                     }
                 } else {
                     // Lambertian: cosine-weighted direction, kray = rho(lambda),
@@ -580,10 +595,28 @@ int TraceGrid(K kernel, int sms)
 }
 }  // namespace
 
-cudaError_t PtSetGgxTables(const float* ess, const float* eavg)
+// Extension kernel (closest hits of the path queue) when `extend`, else the
+// connection kernel (shadow rays); grids cached per instantiation.
+template <class NodeT, bool SPILL>
+void LaunchTraceKernels(const PtLaunch& L, cudaStream_t st, bool extend)
 {
-    cudaError_t e = cudaMemcpyToSymbol(c_ess, ess, sizeof(float) * kLut * kLut);
-    if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_eavg, eavg, sizeof(float) * kLut);
+    if (extend) {
+        static int g = 0;
+        if (!g) g = TraceGrid(KExtend<NodeT, SPILL>, L.sms);
+        KExtend<NodeT, SPILL><<<g, kTraceBlock, 0, st>>>(L.jobs, L.paths, L.queues);
+    } else {
+        static int g = 0;
+        if (!g) g = TraceGrid(KConnect<NodeT, SPILL>, L.sms);
+        KConnect<NodeT, SPILL><<<g, kTraceBlock, 0, st>>>(L.jobs, L.paths, L.queues);
+    }
+}
+
+cudaError_t PtSetGgxTables(const float* ess, const float* eavg, const float* msz, const float* mscum)
+{
+    cudaError_t e = cudaMemcpyToSymbol(g_ess, ess, sizeof(float) * kLut * kLut);
+    if (e == cudaSuccess) e = cudaMemcpyToSymbol(g_eavg, eavg, sizeof(float) * kLut);
+    if (e == cudaSuccess) e = cudaMemcpyToSymbol(g_msz, msz, sizeof(float) * kLut);
+    if (e == cudaSuccess) e = cudaMemcpyToSymbol(g_mscum, mscum, sizeof(float) * kLut * (kLut + 2));
     return e;
 }
 
@@ -593,23 +626,19 @@ cudaError_t PtIteration(const PtLaunch& L, int iter, cudaStream_t st)
     KRegen<<<shadeGrid, kShadeBlock, 0, st>>>(L.jobs, L.ids, L.njobs, L.paths, L.queues, iter, 1);
     cudaMemsetAsync(L.queues.trace_ctr, 0, 2 * sizeof(unsigned long long), st);
     if (L.layout == RTB200_BVH_Q8) {
-        static int g = 0;
-        if (!g) g = TraceGrid(KExtend<QNode4>, L.sms);
-        KExtend<QNode4><<<g, kTraceBlock, 0, st>>>(L.jobs, L.paths, L.queues);
+        if (L.spill) LaunchTraceKernels<QNode4, true>(L, st, true);
+        else LaunchTraceKernels<QNode4, false>(L, st, true);
     } else {
-        static int g = 0;
-        if (!g) g = TraceGrid(KExtend<GpuNode4>, L.sms);
-        KExtend<GpuNode4><<<g, kTraceBlock, 0, st>>>(L.jobs, L.paths, L.queues);
+        if (L.spill) LaunchTraceKernels<GpuNode4, true>(L, st, true);
+        else LaunchTraceKernels<GpuNode4, false>(L, st, true);
     }
     KShade<<<shadeGrid, kShadeBlock, 0, st>>>(L.jobs, L.paths, L.queues);
     if (L.layout == RTB200_BVH_Q8) {
-        static int g = 0;
-        if (!g) g = TraceGrid(KConnect<QNode4>, L.sms);
-        KConnect<QNode4><<<g, kTraceBlock, 0, st>>>(L.jobs, L.paths, L.queues);
+        if (L.spill) LaunchTraceKernels<QNode4, true>(L, st, false);
+        else LaunchTraceKernels<QNode4, false>(L, st, false);
     } else {
-        static int g = 0;
-        if (!g) g = TraceGrid(KConnect<GpuNode4>, L.sms);
-        KConnect<GpuNode4><<<g, kTraceBlock, 0, st>>>(L.jobs, L.paths, L.queues);
+        if (L.spill) LaunchTraceKernels<GpuNode4, true>(L, st, false);
+        else LaunchTraceKernels<GpuNode4, false>(L, st, false);
     }
     KSwap<<<1, 1, 0, st>>>(L.queues.cnt);
     return cudaGetLastError();

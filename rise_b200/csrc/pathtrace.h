@@ -14,6 +14,7 @@ struct PtLaunch {
     const int* ids;
     int njobs;
     int layout;
+    bool spill;        // some job's BVH needs the local-memory stack continuation
     PtPaths paths;
     PtQueues queues;
     int sms;
@@ -25,8 +26,9 @@ struct PtLaunch {
 cudaError_t PtIteration(const PtLaunch& L, int iter, cudaStream_t st);
 // Splat paths still marked finished into their films (end of a render).
 cudaError_t PtDrain(const PtLaunch& L, cudaStream_t st);
-// Upload the GGX E_ss (32 x 32) and E_avg (32) tables to constant memory.
-cudaError_t PtSetGgxTables(const float* ess, const float* eavg);
+// Upload the GGX E_ss (32 x 32), E_avg (32), multiple-scattering lobe
+// normalisation (32) and cumulative segment integral (32 x 34) tables.
+cudaError_t PtSetGgxTables(const float* ess, const float* eavg, const float* msz, const float* mscum);
 // Fold a film of this request into the compensated running sums and clear it.
 cudaError_t PtFold(float* pass, float* sum, float* comp, int npix, int sms, cudaStream_t st);
 

@@ -56,7 +56,7 @@ int UploadShading(rtb200_scene* s)
     }
     {
         const GgxTables& gt = GetGgxTables();
-        const cudaError_t e = PtSetGgxTables(gt.ess, gt.eavg);
+        const cudaError_t e = PtSetGgxTables(gt.ess, gt.eavg, gt.msz, gt.mscum);
         if (e != cudaSuccess) return CudaCheck(ctx, e, "GGX tables");
     }
     for (const auto& mesh : s->meshes)

@@ -21,14 +21,15 @@ __device__ __forceinline__ Ray LoadRay(const rtb200_ray* rays, long long i)
     return r;
 }
 
-template <class NodeT, bool ANY>
+template <class NodeT, bool ANY, bool SPILL>
 __global__ void __launch_bounds__(kTraceBlock, 8)
 KTrace(const NodeT* __restrict__ nodes, const GpuTri* __restrict__ tris,
        const rtb200_ray* __restrict__ rays, long long n, int ntri, rtb200_hit* __restrict__ hits,
        uint8_t* __restrict__ occ, unsigned long long* counter, unsigned* err)
 {
     __shared__ int sstack[kTraceStack * kTraceBlock];
-    int* stk = sstack + threadIdx.x;
+    int spill[SPILL ? kTraceSpill : 1];
+    const TraceStack stk{sstack + threadIdx.x, spill};
     WarpFeed feed{0ull, 0ull, false};
     TraceState s;
     long long ray = -1;
@@ -39,7 +40,7 @@ KTrace(const NodeT* __restrict__ nodes, const GpuTri* __restrict__ tris,
             StartRay(s, LoadRay(rays, ray));
         }
         if (__all_sync(kFull, ray < 0)) break;
-        if (ray >= 0 && TraceRound<NodeT, ANY>(s, nodes, tris, ntri, stk, err)) {
+        if (ray >= 0 && TraceRound<NodeT, ANY, SPILL>(s, nodes, tris, ntri, stk, err)) {
             if (ANY) {
                 occ[ray] = s.bestSlot >= 0 ? 1 : 0;
             } else {
@@ -72,17 +73,31 @@ int GridFor(K kernel, int num_sms)
     return per_sm * num_sms;
 }
 
-template <class NodeT, bool ANY>
-cudaError_t LaunchTrace(const rtb200_scene* s, const rtb200_ray* d_rays, int64_t n, rtb200_hit* hits,
-                        uint8_t* occ, cudaStream_t stream)
+// One launch over `n` rays with the work counter and error word given.  The
+// grid is the kernel's occupancy times the SM count, cached per instantiation.
+template <class NodeT, bool ANY, bool SPILL>
+void Launch(const rtb200_scene* s, const rtb200_ray* d_rays, int64_t n, rtb200_hit* hits, uint8_t* occ,
+            unsigned long long* counter, unsigned* err, cudaStream_t stream)
+{
+    static int grid = 0;
+    if (!grid) grid = GridFor(KTrace<NodeT, ANY, SPILL>, s->ctx->num_sms);
+    KTrace<NodeT, ANY, SPILL><<<grid, kTraceBlock, 0, stream>>>((const NodeT*)s->d_nodes, s->d_tris, d_rays, n,
+                                                                (int)s->tri_material.size(), hits, occ, counter, err);
+}
+
+template <bool ANY>
+cudaError_t Dispatch(const rtb200_scene* s, const rtb200_ray* d_rays, int64_t n, rtb200_hit* hits, uint8_t* occ,
+                     unsigned long long* counter, unsigned* err, cudaStream_t stream)
 {
     if (n <= 0) return cudaSuccess;
-    cudaError_t e = cudaMemsetAsync(s->d_counter, 0, sizeof(unsigned long long), stream);
-    if (e != cudaSuccess) return e;
-    static int grid = 0;
-    if (!grid) grid = GridFor(KTrace<NodeT, ANY>, s->ctx->num_sms);
-    KTrace<NodeT, ANY><<<grid, kTraceBlock, 0, stream>>>((const NodeT*)s->d_nodes, s->d_tris, d_rays, n,
-                                                         (int)s->tri_material.size(), hits, occ, s->d_counter, s->d_err);
+    const bool spill = s->stack_bound > kTraceStack;
+    if (s->layout == RTB200_BVH_Q8) {
+        if (spill) Launch<QNode4, ANY, true>(s, d_rays, n, hits, occ, counter, err, stream);
+        else Launch<QNode4, ANY, false>(s, d_rays, n, hits, occ, counter, err, stream);
+    } else {
+        if (spill) Launch<GpuNode4, ANY, true>(s, d_rays, n, hits, occ, counter, err, stream);
+        else Launch<GpuNode4, ANY, false>(s, d_rays, n, hits, occ, counter, err, stream);
+    }
     return cudaGetLastError();
 }
 
@@ -91,36 +106,26 @@ cudaError_t LaunchTrace(const rtb200_scene* s, const rtb200_ray* d_rays, int64_t
 cudaError_t LaunchCastClosest(const rtb200_scene* s, const rtb200_ray* d_rays, int64_t n,
                               rtb200_hit* d_hits, cudaStream_t stream)
 {
-    if (s->layout == RTB200_BVH_Q8) return LaunchTrace<QNode4, false>(s, d_rays, n, d_hits, nullptr, stream);
-    return LaunchTrace<GpuNode4, false>(s, d_rays, n, d_hits, nullptr, stream);
+    if (n <= 0) return cudaSuccess;
+    const cudaError_t e = cudaMemsetAsync(s->d_counter, 0, sizeof(unsigned long long), stream);
+    if (e != cudaSuccess) return e;
+    return Dispatch<false>(s, d_rays, n, d_hits, nullptr, s->d_counter, s->d_err, stream);
 }
 
 cudaError_t LaunchCastClosestScratch(const rtb200_scene* s, const rtb200_ray* d_rays, int64_t n,
                                      rtb200_hit* d_hits, unsigned long long* counter, unsigned* err,
                                      cudaStream_t stream)
 {
-    if (n <= 0) return cudaSuccess;
-    if (s->layout == RTB200_BVH_Q8) {
-        static int grid = 0;
-        if (!grid) grid = GridFor(KTrace<QNode4, false>, s->ctx->num_sms);
-        KTrace<QNode4, false><<<grid, kTraceBlock, 0, stream>>>((const QNode4*)s->d_nodes, s->d_tris, d_rays, n,
-                                                                (int)s->tri_material.size(), d_hits, nullptr,
-                                                                counter, err);
-    } else {
-        static int grid = 0;
-        if (!grid) grid = GridFor(KTrace<GpuNode4, false>, s->ctx->num_sms);
-        KTrace<GpuNode4, false><<<grid, kTraceBlock, 0, stream>>>((const GpuNode4*)s->d_nodes, s->d_tris, d_rays,
-                                                                  n, (int)s->tri_material.size(), d_hits,
-                                                                  nullptr, counter, err);
-    }
-    return cudaGetLastError();
+    return Dispatch<false>(s, d_rays, n, d_hits, nullptr, counter, err, stream);
 }
 
 cudaError_t LaunchCastAny(const rtb200_scene* s, const rtb200_ray* d_rays, int64_t n,
                           uint8_t* d_occ, cudaStream_t stream)
 {
-    if (s->layout == RTB200_BVH_Q8) return LaunchTrace<QNode4, true>(s, d_rays, n, nullptr, d_occ, stream);
-    return LaunchTrace<GpuNode4, true>(s, d_rays, n, nullptr, d_occ, stream);
+    if (n <= 0) return cudaSuccess;
+    const cudaError_t e = cudaMemsetAsync(s->d_counter, 0, sizeof(unsigned long long), stream);
+    if (e != cudaSuccess) return e;
+    return Dispatch<true>(s, d_rays, n, nullptr, d_occ, s->d_counter, s->d_err, stream);
 }
 
 }  // namespace rtb200

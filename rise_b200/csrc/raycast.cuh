@@ -23,7 +23,13 @@ namespace rtb200 {
 constexpr unsigned kErrStackOverflow = 1u;
 constexpr int kEmpty = INT_MIN;      // no node / no leaf
 constexpr int kTraceBlock = 128;     // threads per block of the trace kernels
-constexpr int kTraceStack = 64;      // stack entries per thread (shared memory)
+// Traversal stack per thread: the first kTraceStack entries in shared memory
+// (20 KB per block: 8 blocks of 128 threads stay resident per SM next to 64
+// registers).  Kernels instantiated with SPILL continue it in local memory for
+// scenes whose TraceStackBound exceeds kTraceStack; the others carry no local
+// array at all.
+constexpr int kTraceStack = kTraceStackShared;
+constexpr int kTraceSpill = kTraceStackMax - kTraceStackShared;
 constexpr unsigned kFull = 0xffffffffu;
 
 struct Ray {
@@ -92,9 +98,13 @@ __device__ __forceinline__ bool Watertight(const RayPre& p, const float4& A4, co
     }
     if ((U < 0.0f || V < 0.0f || W < 0.0f) && (U > 0.0f || V > 0.0f || W > 0.0f)) return false;
     const float det = U + V + W;
-    if (det == 0.0f) return false;
-    const float T = U * (p.sz * Az) + V * (p.sz * Bz) + W * (p.sz * Cz);
     const float adet = fabsf(det);
+    // det is the Moller-Trumbore determinant e1 . (d x e2) divided by the
+    // dominant direction component, |det_MT| = adet / |sz|: the reference
+    // rejects |det_MT| < 1e-12 (RayTriangleIntersection.cpp:40-42), which
+    // also drops triangles with edges below ~1e-6.
+    if (!(adet >= 1e-12f * fabsf(p.sz))) return false;
+    const float T = U * (p.sz * Az) + V * (p.sz * Bz) + W * (p.sz * Cz);
     const float sT = copysignf(1.0f, det) * T;
     if (sT <= p.tmin * adet || sT >= tmax * adet) return false;
     const float rcp = 1.0f / det;
@@ -246,26 +256,39 @@ __device__ __forceinline__ void StartRay(TraceState& s, const Ray& r)
     s.sp = 0;
 }
 
-__device__ __forceinline__ void Push(TraceState& s, int* stk, int v, unsigned* err)
+// The stack: `stk` points at this thread's column of the shared-memory part
+// ([depth][thread]); `spill` is the thread's local-memory continuation.
+struct TraceStack {
+    int* stk;
+    int* spill;
+};
+
+// Overflow (a bound computed wrongly) drops the entry and raises the error
+// flag, which the host turns into an error status.
+template <bool SPILL>
+__device__ __forceinline__ void Push(TraceState& s, const TraceStack& st, int v, unsigned* err)
 {
-    if (s.sp < kTraceStack) { stk[s.sp * kTraceBlock] = v; ++s.sp; }
+    if (s.sp < kTraceStack) { st.stk[s.sp * kTraceBlock] = v; ++s.sp; }
+    else if (SPILL && s.sp < kTraceStack + kTraceSpill) { st.spill[s.sp - kTraceStack] = v; ++s.sp; }
     else atomicOr(err, kErrStackOverflow);
 }
 
-__device__ __forceinline__ int Pop(TraceState& s, const int* stk)
+template <bool SPILL>
+__device__ __forceinline__ int Pop(TraceState& s, const TraceStack& st)
 {
     if (s.sp == 0) return kEmpty;
     --s.sp;
-    return stk[s.sp * kTraceBlock];
+    if (!SPILL || s.sp < kTraceStack) return st.stk[s.sp * kTraceBlock];
+    return st.spill[s.sp - kTraceStack];
 }
 
 // One round of while-while traversal for every active lane: descend internal
 // nodes until all active lanes hold a postponed leaf (or have run out of
 // nodes), then test postponed leaves.  ANY: stop at the first accepted hit.
 // Returns true when this lane's ray is finished.
-template <class NodeT, bool ANY>
+template <class NodeT, bool ANY, bool SPILL>
 __device__ __forceinline__ bool TraceRound(TraceState& s, const NodeT* __restrict__ nodes,
-                                           const GpuTri* __restrict__ tris, int ntri, int* stk, unsigned* err)
+                                           const GpuTri* __restrict__ tris, int ntri, const TraceStack& stk, unsigned* err)
 {
     // Descend internal nodes.
     while (s.node >= 0) {
@@ -286,14 +309,14 @@ __device__ __forceinline__ bool TraceRound(TraceState& s, const NodeT* __restric
         CSwap(t1, c1, t3, c3);
         CSwap(t1, c1, t2, c2);
         // Push far to near; the nearest becomes the next node.
-        if (c3 != kEmpty) Push(s, stk, c3, err);
-        if (c2 != kEmpty) Push(s, stk, c2, err);
-        if (c1 != kEmpty) Push(s, stk, c1, err);
-        s.node = (c0 != kEmpty) ? c0 : Pop(s, stk);
+        if (c3 != kEmpty) Push<SPILL>(s, stk, c3, err);
+        if (c2 != kEmpty) Push<SPILL>(s, stk, c2, err);
+        if (c1 != kEmpty) Push<SPILL>(s, stk, c1, err);
+        s.node = (c0 != kEmpty) ? c0 : Pop<SPILL>(s, stk);
         // Postpone the first leaf met; keep descending until all lanes have one.
         if (s.node < 0 && s.node != kEmpty && s.leaf == kEmpty) {
             s.leaf = s.node;
-            s.node = Pop(s, stk);
+            s.node = Pop<SPILL>(s, stk);
         }
         if (!__any_sync(__activemask(), s.leaf == kEmpty)) break;
     }
@@ -324,7 +347,7 @@ __device__ __forceinline__ bool TraceRound(TraceState& s, const NodeT* __restric
         s.leaf = kEmpty;
         if (s.node < 0 && s.node != kEmpty) {
             s.leaf = s.node;
-            s.node = Pop(s, stk);
+            s.node = Pop<SPILL>(s, stk);
         }
     }
     return s.node == kEmpty;

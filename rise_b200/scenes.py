@@ -59,6 +59,51 @@ def sphere_rays(n_rays, seed=7, shadow=False):
     return rays
 
 
+def nested_clusters(levels=30, ratio=0.3, per=5, scale=1e3, seed=1):
+    """Self-similar clusters whose BVH is deep: level k holds three clusters of
+    `per` small triangles near the corners (0.9,0.1,0.1), (0.1,0.9,0.1),
+    (0.1,0.1,0.9) of a cube of side scale * ratio**k at the origin, and the
+    next level nests inside it.  Every BVH4 node on the path down the levels
+    has siblings to defer, so the traversal stack grows with the level count
+    (46 deferred entries for the defaults)."""
+    rng = np.random.default_rng(seed)
+    corners = np.array([(0.9, 0.1, 0.1), (0.1, 0.9, 0.1), (0.1, 0.1, 0.9)])
+    rows = []
+    for k in range(levels):
+        s = scale * ratio ** k
+        for cc in corners:
+            c = (cc + rng.uniform(-0.05, 0.05, (per, 3))) * s
+            e = 0.03 * s
+            rows.append(np.concatenate([c + [e, 0, 0], c + [0, e, 0], c + [0, 0, e]], axis=1))
+    return np.concatenate(rows).astype(np.float32)
+
+
+def cluster_rays(tri9, n_rays, seed=7, shadow=False):
+    """Rays aimed at random triangles of `tri9` from 20 triangle sizes away,
+    so rays reach every scale of a `nested_clusters` scene.  Shadow rays stop
+    0.1 % short of the aim point, as a renderer's shadow ray stops short of the
+    surface point it connects to (ending exactly on the aimed triangle would
+    leave its occlusion to FP32 rounding)."""
+    rng = np.random.default_rng(seed)
+    t = tri9.reshape(-1, 3, 3).astype(np.float64)
+    pick = rng.integers(0, len(t), n_rays)
+    w = rng.dirichlet((1.0, 1.0, 1.0), n_rays)
+    tgt = np.einsum("nk,nkj->nj", w, t[pick])
+    size = np.linalg.norm(t[pick, 1] - t[pick, 0], axis=1)
+    z = rng.normal(size=(n_rays, 3))
+    z /= np.linalg.norm(z, axis=1, keepdims=True)
+    o = tgt + 20.0 * size[:, None] * z
+    d = tgt - o
+    dist = np.linalg.norm(d, axis=1)
+    d /= dist[:, None]
+    rays = np.empty((n_rays, 8), np.float32)
+    rays[:, 0:3] = o
+    rays[:, 3] = 0.0
+    rays[:, 4:7] = d
+    rays[:, 7] = dist * 0.999 if shadow else np.inf
+    return rays
+
+
 # ---- spectra -----------------------------------------------------------------
 
 def flat_spectrum(value, lo=380.0, hi=780.0, outside=0.0):

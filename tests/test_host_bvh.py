@@ -56,3 +56,26 @@ def test_host_builder_degenerate_inputs():
 def test_host_builder_empty():
     n2, prims, n4 = raycaster.build_host_bvh(np.zeros((0, 9), np.float32))
     assert len(n2) == 0 and len(prims) == 0 and len(n4) == 0
+
+
+def stack_bound(nodes4):
+    """Largest sum of (children - 1) over the internal nodes of one
+    root-to-node path: the deferred entries a depth-first BVH4 walk can hold."""
+    best, todo = 0, [(0, 0)]
+    while todo:
+        ni, above = todo.pop()
+        n = nodes4[ni]
+        here = above + max(int(n["nchild"]) - 1, 0)
+        best = max(best, here)
+        todo.extend((int(n["child"][i]), here) for i in range(int(n["nchild"])) if n["count"][i] == 0)
+    return best
+
+
+def test_traversal_stack_bounds():
+    # The shared-memory stack holds 40 entries; these scenes stay within it
+    # (the path-tracer scenes up to 3.4M triangles included) ...
+    assert stack_bound(raycaster.build_host_bvh(scenes.soup_triangles(100_000, 7))[2]) <= 40
+    assert stack_bound(raycaster.build_host_bvh(scenes.cornell_box(8, 8).tri9)[2]) <= 40
+    # ... and the nested-cluster scene needs the local-memory continuation.
+    b = stack_bound(raycaster.build_host_bvh(scenes.nested_clusters())[2])
+    assert 40 < b <= 128

@@ -98,6 +98,26 @@ def test_edge_cases(ctx, layout):
     s.close()
 
 
+@pytest.mark.parametrize("layout", LAYOUTS)
+def test_deep_bvh_local_stack_parity(ctx, layout):
+    # A BVH whose traversal stack bound (46) exceeds the shared-memory part
+    # (40) runs the kernels that continue the stack in local memory.
+    tri = scenes.nested_clusters()
+    rays = scenes.cluster_rays(tri, 20000, seed=3)
+    srays = scenes.cluster_rays(tri, 20000, seed=4, shadow=True)
+    s, rc = make_caster(ctx, tri, layout)
+    ob = oracle.BVH(tri, "port")
+    ids, t = ob.closest(rays)
+    hits = rc.cast_rays(rays)
+    rep = closest_report(tri, rays, hits, ids, t)
+    assert rep["bad"] == [] and rep["t_over"] == 0, {k: rep[k] for k in ("bad", "t_over", "max_ulp")}
+    assert (ids >= 0).mean() > 0.3   # rays at triangles below the 1e-12 determinant miss
+    occ = rc.cast_shadow_rays(srays)
+    arep = any_report(tri, srays, occ, ob.any(srays))
+    assert arep["bad"] == [], arep
+    s.close()
+
+
 def test_layouts_agree_and_are_deterministic(ctx):
     tri = scenes.soup_triangles(200000, seed=5)
     rays = scenes.sphere_rays(500000, seed=5)
