@@ -29,7 +29,7 @@ using namespace rtb200;
 
 namespace {
 
-constexpr int kMaxJobs = 1024;
+constexpr int kMaxJobs = kPtMaxJobs;
 constexpr int kGraphIters = 2;   // iterations per captured graph (even: queue pointers return)
 
 const float kCieY[RTB200_CIE_COUNT] = {RTB200_CIE_YBAR};
@@ -145,7 +145,8 @@ int EngineCreate(rtb200_ctx* ctx, int capacity, rtb200_engine** out)
     const size_t oSh = take(sizeof(ShadowEntry) * 8 * c);   // up to 4 light + 4 sky samples per path
     const size_t oTab = take(sizeof(PtJobDev) * kMaxJobs), oIds = take(4 * kMaxJobs),
                  oCtr = take(8 * 2 * kMaxJobs);
-    const size_t oCnt = take(4 * kCntCount), oTr = take(8 * 2), oSmp = take(8), oErr = take(4);
+    const size_t oCnt = take(4 * kCntCount), oTr = take(8 * 2), oSmp = take(8), oErr = take(4),
+                 oAsg = take(sizeof(PtAssign) * kMaxJobs);
     int rc = DevAlloc(ctx, &e->buf, off);
     if (rc) { delete e; return rc; }
     e->bytes = off;
@@ -155,7 +156,7 @@ int EngineCreate(rtb200_ctx* ctx, int capacity, rtb200_engine** out)
                        (float4*)(b + oL), (float4*)(b + oAux), (uint4*)(b + oMeta)};
     e->queues = PtQueues{(int*)(b + oQa), (int*)(b + oQan), (int*)(b + oQf), (int*)(b + oQfn),
                          (ShadowEntry*)(b + oSh), (int*)(b + oCnt), (unsigned long long*)(b + oSmp),
-                         (unsigned long long*)(b + oTr), (unsigned*)(b + oErr)};
+                         (unsigned long long*)(b + oTr), (unsigned*)(b + oErr), (PtAssign*)(b + oAsg)};
     e->d_iota = (int*)(b + oIota);
     e->d_table = (PtJobDev*)(b + oTab);
     e->d_ids = (int*)(b + oIds);

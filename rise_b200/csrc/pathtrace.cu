@@ -6,8 +6,9 @@
 // PathTracingSpectralRasterizer::IntegratePixelSpectral
 // (src/Library/Rendering/PathTracingSpectralRasterizer.cpp:121-198).
 //
-// A fixed pool of path slots lives in HBM as SoA.  One iteration is five
+// A fixed pool of path slots lives in HBM as SoA.  One iteration is six
 // launches over device-side queues (no host round trip):
+//   KAssign  split the free slots among the jobs that have samples left
 //   KRegen   splat finished paths into the film, start new camera samples
 //   KExtend  closest hit for every active path (warp while-while traversal)
 //   KShade   emission + MIS, next-event estimation to area lights and the
@@ -64,11 +65,81 @@ __device__ __forceinline__ void Splat(const PtPaths& P, const PtJobDev& J, int s
 
 // ---- kernels ---------------------------------------------------------------
 
+// Inclusive prefix sum over a block of up to 1024 threads.
+__device__ __forceinline__ int BlockScan(int v, int* warp_sums)
+{
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    for (int o = 1; o < 32; o <<= 1) {
+        const int u = __shfl_up_sync(kFull, v, o);
+        if (lane >= o) v += u;
+    }
+    if (lane == 31) warp_sums[w] = v;
+    __syncthreads();
+    if (w == 0) {
+        int s = lane < (int)(blockDim.x >> 5) ? warp_sums[lane] : 0;
+        for (int o = 1; o < 32; o <<= 1) {
+            const int u = __shfl_up_sync(kFull, s, o);
+            if (lane >= o) s += u;
+        }
+        warp_sums[lane] = s;
+    }
+    __syncthreads();
+    const int r = v + (w > 0 ? warp_sums[w - 1] : 0);
+    __syncthreads();
+    return r;
+}
+
+// Split this iteration's free slots among the jobs that still have camera
+// samples (one block, one thread per job): every such job first gets an equal
+// share (capped by what it has left), the remainder goes to jobs in an order
+// that rotates with the iteration.  Each job's range of free-queue entries and
+// first sample index go to Q.assign; the job's issued counter advances by its
+// share.  Prefix sums replace per-warp atomics on one counter per job.
+__global__ void __launch_bounds__(kPtMaxJobs)
+KAssign(const PtJobDev* __restrict__ jobs, const int* __restrict__ ids, int njobs, PtQueues Q, int iter)
+{
+    __shared__ int sums[32];
+    const int t = threadIdx.x;
+    const int n = Q.cnt[kCntFree];
+    int jid = -1, rem = 0;
+    unsigned long long issued = 0;
+    if (t < njobs) {
+        jid = ids[(t + iter) % njobs];
+        const PtJobDev& J = jobs[jid];
+        issued = *J.sample_ctr;
+        if (issued < J.total) rem = (int)min(J.total - issued, (unsigned long long)n);
+    }
+    const int live = BlockScan(rem > 0 ? 1 : 0, sums);
+    __shared__ int s_live, s_first;
+    if (t == blockDim.x - 1) s_live = live;
+    __syncthreads();
+    const int share = s_live > 0 ? n / s_live : 0;
+    const int first = min(rem, share);
+    const int firstIncl = BlockScan(first, sums);
+    if (t == blockDim.x - 1) s_first = firstIncl;
+    __syncthreads();
+    const int left = n - s_first;
+    const int more = rem - first;
+    const int moreIncl = BlockScan(more, sums);
+    const int extra = max(0, min(more, left - (moreIncl - more)));
+    const int take = first + extra;
+    const int takeIncl = BlockScan(take, sums);
+    if (t < njobs) {
+        PtAssign a;
+        a.base = issued;
+        a.off = takeIncl - take;
+        a.jid = jid;
+        Q.assign[t] = a;
+        if (take > 0) *jobs[jid].sample_ctr = issued + (unsigned long long)take;
+    }
+    if (t == blockDim.x - 1) Q.cnt[kCntAssigned] = takeIncl;
+}
+
 __global__ void __launch_bounds__(kShadeBlock)
-KRegen(const PtJobDev* __restrict__ jobs, const int* __restrict__ ids, int njobs, PtPaths P, PtQueues Q, int iter,
-       int assign)
+KRegen(const PtJobDev* __restrict__ jobs, int njobs, PtPaths P, PtQueues Q, int assign)
 {
     const int n = Q.cnt[kCntFree];
+    const int nassigned = assign ? Q.cnt[kCntAssigned] : 0;
     const int lane = threadIdx.x & 31;
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int nwarps = (gridDim.x * blockDim.x) >> 5;
@@ -76,34 +147,32 @@ KRegen(const PtJobDev* __restrict__ jobs, const int* __restrict__ ids, int njobs
         const int i = base + lane;
         const bool valid = i < n;
         const int slot = valid ? Q.free_[i] : -1;
+        int fin_job = -1;
         if (valid) {
             const uint4 m = P.meta[slot];
             if (m.z & kFlagFinishing) {
-                const PtJobDev& J = jobs[__float_as_int(P.aux[slot].z)];
-                Splat(P, J, slot, m);
-                atomicAdd(J.done_ctr, 1ull);
+                fin_job = __float_as_int(P.aux[slot].z);
+                Splat(P, jobs[fin_job], slot, m);
                 P.meta[slot].z = m.z & ~kFlagFinishing;
             }
         }
-        // Hand out new camera samples, one job at a time per warp (one
-        // atomic per warp and job), starting at a job that rotates with the
-        // warp and the iteration so every job receives slots.
-        bool need = valid && assign;
+        // Finished samples, one atomic per job present in the warp.
+        const unsigned grp = __match_any_sync(kFull, fin_job);
+        if (fin_job >= 0 && lane == __ffs(grp) - 1) atomicAdd(jobs[fin_job].done_ctr, (unsigned long long)__popc(grp));
+        // New camera samples: free entry i < nassigned belongs to the job
+        // whose assigned range holds it (KAssign).
         bool got = false;
-        const int start = njobs > 0 ? (warp + iter) % njobs : 0;
-        for (int k = 0; k < njobs && __any_sync(kFull, need); ++k) {
-            const int jid = ids[(start + k) % njobs];
+        if (valid && i < nassigned) {
+            int lo = 0, hi = njobs - 1;   // largest k with assign[k].off <= i
+            while (lo < hi) {
+                const int mid = (lo + hi + 1) >> 1;
+                if (Q.assign[mid].off <= i) lo = mid; else hi = mid - 1;
+            }
+            const PtAssign a = Q.assign[lo];
+            const int jid = a.jid;
             const PtJobDev& J = jobs[jid];
-            unsigned long long issued = 0;
-            if (lane == 0) issued = *(volatile unsigned long long*)J.sample_ctr;
-            issued = __shfl_sync(kFull, issued, 0);
-            if (issued >= J.total) continue;
-            const unsigned want = __ballot_sync(kFull, need);
-            unsigned long long g0 = 0;
-            if (lane == 0) g0 = atomicAdd(J.sample_ctr, (unsigned long long)__popc(want));
-            g0 = __shfl_sync(kFull, g0, 0);
-            const unsigned long long g = g0 + __popc(want & ((1u << lane) - 1u));
-            if (need && g < J.total) {
+            const unsigned long long g = a.base + (unsigned long long)(i - a.off);
+            {   // PinholeCamera::GenerateRay (Cameras/PinholeCamera.cpp:182-210)
                 const uint32_t pixel = (uint32_t)(g % (unsigned long long)J.npix);
                 const uint32_t sample = (uint32_t)(J.sample_begin + g / (unsigned long long)J.npix);
                 const uint32_t key = PathKey(J.set.seed, pixel, sample);
@@ -123,7 +192,6 @@ KRegen(const PtJobDev* __restrict__ jobs, const int* __restrict__ ids, int njobs
                 P.aux[slot] = make_float4(hero, 0.0f, __int_as_float(jid), 0.0f);
                 P.meta[slot] = make_uint4(pixel, sample, kFlagConsiderEmission, key);
                 got = true;
-                need = false;
             }
         }
         const int at = WarpAppend(&Q.cnt[kCntActive], got);
@@ -623,7 +691,8 @@ cudaError_t PtSetGgxTables(const float* ess, const float* eavg, const float* msz
 cudaError_t PtIteration(const PtLaunch& L, int iter, cudaStream_t st)
 {
     const int shadeGrid = L.sms * 8;
-    KRegen<<<shadeGrid, kShadeBlock, 0, st>>>(L.jobs, L.ids, L.njobs, L.paths, L.queues, iter, 1);
+    KAssign<<<1, kPtMaxJobs, 0, st>>>(L.jobs, L.ids, L.njobs, L.queues, iter);
+    KRegen<<<shadeGrid, kShadeBlock, 0, st>>>(L.jobs, L.njobs, L.paths, L.queues, 1);
     cudaMemsetAsync(L.queues.trace_ctr, 0, 2 * sizeof(unsigned long long), st);
     if (L.layout == RTB200_BVH_Q8) {
         if (L.spill) LaunchTraceKernels<QNode4, true>(L, st, true);
@@ -646,7 +715,7 @@ cudaError_t PtIteration(const PtLaunch& L, int iter, cudaStream_t st)
 
 cudaError_t PtDrain(const PtLaunch& L, cudaStream_t st)
 {
-    KRegen<<<L.sms * 8, kShadeBlock, 0, st>>>(L.jobs, L.ids, L.njobs, L.paths, L.queues, 0, 0);
+    KRegen<<<L.sms * 8, kShadeBlock, 0, st>>>(L.jobs, L.njobs, L.paths, L.queues, 0);
     return cudaGetLastError();
 }
 

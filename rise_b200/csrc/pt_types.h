@@ -103,6 +103,7 @@ enum PtCounter : int {
     kCntShadow = 4,
     kCntSegments = 5,   // extended rays (statistics)
     kCntShadowRays = 6,
+    kCntAssigned = 7,   // free slots given camera samples this iteration
     kCntCount = 16,
 };
 
@@ -128,6 +129,16 @@ struct PtPaths {
     uint4* meta;     // x pixel, y sample, z flags, w rng key
 };
 
+constexpr int kPtMaxJobs = 1024;   // jobs per engine (one KAssign thread each)
+
+// Camera samples handed to one job in one iteration: free-queue entries
+// [off, next job's off) take the job's samples base, base + 1, ...
+struct PtAssign {
+    unsigned long long base;
+    int off;
+    int jid;
+};
+
 struct PtQueues {
     int* active;        // current
     int* active_next;
@@ -138,6 +149,7 @@ struct PtQueues {
     unsigned long long* sample_ctr;
     unsigned long long* trace_ctr;   // [2]: extend, connect
     unsigned* err;
+    PtAssign* assign;                // [max jobs], written by KAssign
 };
 
 struct PtFilm {
