@@ -93,7 +93,11 @@ int rtb200_scene_add_mesh(rtb200_scene* scene, const float* xyz, int64_t n_verts
                           const uint32_t* tri, int64_t n_tri, int32_t material,
                           int32_t double_sided);
 /* Build the BVH on the host (all cores) and upload it.  layout is one of
- * RTB200_BVH_*.  Meshes cannot be added after commit. */
+ * RTB200_BVH_*.  Meshes cannot be added after commit.  The device traversal
+ * stack holds at most 128 deferred nodes; a BVH whose worst root-to-node path
+ * defers more (only deeply nested geometry does) is refused with
+ * RTB200_E_INVALID, where the reference's unbounded stack
+ * (Acceleration/BVH.h:1311-1320) would go on. */
 int rtb200_scene_commit(rtb200_scene* scene, int32_t layout);
 /* Node / triangle counts and device bytes of a committed scene. */
 int rtb200_scene_info(const rtb200_scene* scene, int64_t* n_tri, int64_t* n_nodes,

@@ -394,17 +394,43 @@ void BuildReferenceBVH(const float* tri9, int64_t n_tri, int threads, BuiltBVH& 
     Collapse(out.nodes2, out.nodes4);
 }
 
+std::vector<int32_t> BreadthFirstPositions(const BuiltBVH& b)
+{
+    const size_t n = b.nodes4.size();
+    std::vector<int32_t> pos(n, -1);
+    if (n == 0) return pos;
+    std::vector<int32_t> q;
+    q.reserve(n);
+    q.push_back(0);
+    for (size_t h = 0; h < q.size(); ++h) {
+        const int32_t ni = q[h];
+        pos[ni] = (int32_t)h;
+        const Node4& s = b.nodes4[ni];
+        for (int i = 0; i < s.nchild; ++i)
+            if (s.count[i] == 0) q.push_back(s.child[i]);
+    }
+    return pos;
+}
+
+// Child link of slot i: the breadth-first position of an internal child, or
+// ~first triangle of a leaf.
+inline int32_t Link(const Node4& s, int i, const std::vector<int32_t>& pos)
+{
+    return s.count[i] > 0 ? ~s.child[i] : pos[s.child[i]];
+}
+
 void EncodeGpuNodes(const BuiltBVH& b, std::vector<GpuNode4>& out)
 {
     out.resize(b.nodes4.size());
+    const std::vector<int32_t> pos = BreadthFirstPositions(b);
     for (size_t n = 0; n < b.nodes4.size(); ++n) {
         const Node4& s = b.nodes4[n];
-        GpuNode4& d = out[n];
+        GpuNode4& d = out[pos[n]];
         for (int i = 0; i < 4; ++i) {
             const bool valid = i < s.nchild;
             d.lox[i] = s.minx[i]; d.loy[i] = s.miny[i]; d.loz[i] = s.minz[i];
             d.hix[i] = s.maxx[i]; d.hiy[i] = s.maxy[i]; d.hiz[i] = s.maxz[i];
-            d.child[i] = !valid ? 0 : (s.count[i] > 0 ? ~s.child[i] : s.child[i]);
+            d.child[i] = !valid ? 0 : Link(s, i, pos);
             d.count[i] = valid ? (int32_t)s.count[i] : -1;
         }
     }
@@ -423,9 +449,10 @@ inline float Decode(float o, int e, int q)
 void EncodeQuantNodes(const BuiltBVH& b, std::vector<QNode4>& out)
 {
     out.resize(b.nodes4.size());
+    const std::vector<int32_t> pos = BreadthFirstPositions(b);
     for (size_t n = 0; n < b.nodes4.size(); ++n) {
         const Node4& s = b.nodes4[n];
-        QNode4& d = out[n];
+        QNode4& d = out[pos[n]];
         std::memset(&d, 0, sizeof(d));
         d.nchild = s.nchild;
         const float* lo[3] = {s.minx, s.miny, s.minz};
@@ -451,7 +478,7 @@ void EncodeQuantNodes(const BuiltBVH& b, std::vector<QNode4>& out)
         d.ex = (int8_t)ex[0]; d.ey = (int8_t)ex[1]; d.ez = (int8_t)ex[2];
         for (int i = 0; i < 4; ++i) {
             const bool valid = i < s.nchild;
-            d.child[i] = !valid ? 0 : (s.count[i] > 0 ? ~s.child[i] : s.child[i]);
+            d.child[i] = !valid ? 0 : Link(s, i, pos);
             d.count[i] = valid ? (int16_t)std::min<int>(s.count[i], 32767) : (int16_t)-1;
             for (int k = 0; k < 3; ++k) {
                 if (!valid) { d.qlo[k][i] = 255; d.qhi[k][i] = 0; continue; }

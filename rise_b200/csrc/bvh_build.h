@@ -86,6 +86,8 @@ struct alignas(16) GpuTri {
 };
 static_assert(sizeof(GpuTri) == 48, "GpuTri must be 48 bytes");
 
+// Both device layouts store the nodes in breadth-first order (root first), so
+// the top levels, which every ray visits, share cache lines and pages.
 void EncodeGpuNodes(const BuiltBVH& b, std::vector<GpuNode4>& out);
 void EncodeQuantNodes(const BuiltBVH& b, std::vector<QNode4>& out);
 void EncodeTriangles(const float* tri9, const BuiltBVH& b, std::vector<GpuTri>& out);

@@ -100,6 +100,7 @@ struct rtb200_engine {
     int gnjobs = -1;                       // launch shape the graph was captured for
     int glayout = -1;
     bool gspill = false;
+    const rtb200_scene* gscene = nullptr;  // the shared scene, or null when jobs differ
     long long seg_seen = 0, shadow_seen = 0;
 };
 
@@ -113,7 +114,12 @@ PtLaunch MakeLaunch(const rtb200_engine* e)
     L.njobs = (int)e->active.size();
     L.layout = e->layout;
     L.spill = false;
-    for (int k : e->active) L.spill |= e->owner[k]->scene->stack_bound > kTraceStackShared;
+    L.uniform = !e->active.empty();
+    for (int k : e->active) {
+        L.spill |= e->owner[k]->scene->stack_bound > kTraceStackShared;
+        L.uniform &= e->owner[k]->scene == e->owner[e->active[0]]->scene;
+    }
+    L.scene = L.uniform ? e->h_table[e->active[0]].scene : PtScene{};
     L.paths = e->paths;
     L.queues = e->queues;
     L.sms = e->ctx->num_sms;
@@ -218,7 +224,7 @@ int EngineSubmit(rtb200_engine* e, rtb200_job* j, int spp)
     e->layout = j->scene->layout;
     rtb200_scene* s = j->scene;
     PtJobDev& d = e->h_table[entry];
-    d.scene = PtScene{s->d_nodes, s->layout, s->d_tris, (int)s->tri_material.size(), s->d_attr, s->d_mats,
+    d.scene = PtScene{s->d_nodes, s->layout, (int)s->n_nodes, s->d_tris, (int)s->tri_material.size(), s->d_attr, s->d_mats,
                       s->d_spectra, s->d_lights, s->d_light_tris};
     d.cam = j->cam;
     d.set = j->set;
@@ -266,7 +272,9 @@ int EngineStep(rtb200_engine* e, int iterations, bool graph)
     PtLaunch L = MakeLaunch(e);
     cudaError_t err = cudaSuccess;
     if (graph) {
-        if (!e->gexec || e->gnjobs != L.njobs || e->glayout != L.layout || e->gspill != L.spill) {
+        const rtb200_scene* us = L.uniform ? e->owner[e->active[0]]->scene : nullptr;
+        if (!e->gexec || e->gnjobs != L.njobs || e->glayout != L.layout || e->gspill != L.spill ||
+            e->gscene != us) {
             DropGraph(e);
             cudaGraph_t g = nullptr;
             err = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
@@ -284,6 +292,7 @@ int EngineStep(rtb200_engine* e, int iterations, bool graph)
             e->gnjobs = L.njobs;
             e->glayout = L.layout;
             e->gspill = L.spill;
+            e->gscene = us;
         }
         const int reps = (iterations + kGraphIters - 1) / kGraphIters;
         for (int r = 0; r < reps && err == cudaSuccess; ++r) err = cudaGraphLaunch(e->gexec, st);

@@ -206,13 +206,15 @@ KRegen(const PtJobDev* __restrict__ jobs, int njobs, PtPaths P, PtQueues Q, int 
 
 // Closest hit for every active path.  Same while-while walk as KTrace; the
 // hit stores the leaf-order triangle slot for shading.
-template <class NodeT, bool SPILL>
+// UNIFORM: every job shares the scene `us` (kernel argument, no per-path
+// lookup of the job's scene).
+template <class NodeT, bool SPILL, bool UNIFORM>
 __global__ void __launch_bounds__(kTraceBlock, 8)
-KExtend(const PtJobDev* __restrict__ jobs, PtPaths P, PtQueues Q)
+KExtend(const PtJobDev* __restrict__ jobs, PtPaths P, PtQueues Q, PtScene us)
 {
-    const NodeT* nodes = nullptr;
-    const GpuTri* tris = nullptr;
-    int ntri = 0;
+    const NodeT* nodes = UNIFORM ? (const NodeT*)us.nodes : nullptr;
+    const GpuTri* tris = UNIFORM ? us.tris : nullptr;
+    int ntri = UNIFORM ? us.ntri : 0;
     __shared__ int sstack[kTraceStack * kTraceBlock];
     int spill[SPILL ? kTraceSpill : 1];
     const TraceStack stk{sstack + threadIdx.x, spill};
@@ -226,10 +228,12 @@ KExtend(const PtJobDev* __restrict__ jobs, PtPaths P, PtQueues Q)
         if (got >= 0) {
             qi = got;
             slot = Q.active[qi];
-            const PtScene& S = jobs[__float_as_int(P.aux[slot].z)].scene;
-            nodes = (const NodeT*)S.nodes;
-            tris = S.tris;
-            ntri = S.ntri;
+            if (!UNIFORM) {
+                const PtScene& S = jobs[__float_as_int(P.aux[slot].z)].scene;
+                nodes = (const NodeT*)S.nodes;
+                tris = S.tris;
+                ntri = S.ntri;
+            }
             const float4 o = P.ray_o[slot], d = P.ray_d[slot];
             Ray r;
             r.o[0] = o.x; r.o[1] = o.y; r.o[2] = o.z; r.tmin = o.w;
@@ -246,13 +250,13 @@ KExtend(const PtJobDev* __restrict__ jobs, PtPaths P, PtQueues Q)
 
 // Any hit for the shadow-ray queue; unoccluded entries add their
 // contribution to the path's radiance.
-template <class NodeT, bool SPILL>
+template <class NodeT, bool SPILL, bool UNIFORM>
 __global__ void __launch_bounds__(kTraceBlock, 8)
-KConnect(const PtJobDev* __restrict__ jobs, PtPaths P, PtQueues Q)
+KConnect(const PtJobDev* __restrict__ jobs, PtPaths P, PtQueues Q, PtScene us)
 {
-    const NodeT* nodes = nullptr;
-    const GpuTri* tris = nullptr;
-    int ntri = 0;
+    const NodeT* nodes = UNIFORM ? (const NodeT*)us.nodes : nullptr;
+    const GpuTri* tris = UNIFORM ? us.tris : nullptr;
+    int ntri = UNIFORM ? us.ntri : 0;
     __shared__ int sstack[kTraceStack * kTraceBlock];
     int spill[SPILL ? kTraceSpill : 1];
     const TraceStack stk{sstack + threadIdx.x, spill};
@@ -265,10 +269,12 @@ KConnect(const PtJobDev* __restrict__ jobs, PtPaths P, PtQueues Q)
         if (got >= 0) {
             qi = got;
             const ShadowEntry e = Q.shadow[qi];
-            const PtScene& S = jobs[__float_as_int(P.aux[__float_as_int(e.d.w)].z)].scene;
-            nodes = (const NodeT*)S.nodes;
-            tris = S.tris;
-            ntri = S.ntri;
+            if (!UNIFORM) {
+                const PtScene& S = jobs[__float_as_int(P.aux[__float_as_int(e.d.w)].z)].scene;
+                nodes = (const NodeT*)S.nodes;
+                tris = S.tris;
+                ntri = S.ntri;
+            }
             Ray r;
             r.o[0] = e.o.x; r.o[1] = e.o.y; r.o[2] = e.o.z; r.tmin = 0.0f;
             r.d[0] = e.d.x; r.d[1] = e.d.y; r.d[2] = e.d.z; r.tmax = e.o.w;
@@ -665,17 +671,29 @@ int TraceGrid(K kernel, int sms)
 
 // Extension kernel (closest hits of the path queue) when `extend`, else the
 // connection kernel (shadow rays); grids cached per instantiation.
-template <class NodeT, bool SPILL>
+template <class NodeT, bool SPILL, bool UNIFORM>
 void LaunchTraceKernels(const PtLaunch& L, cudaStream_t st, bool extend)
 {
     if (extend) {
         static int g = 0;
-        if (!g) g = TraceGrid(KExtend<NodeT, SPILL>, L.sms);
-        KExtend<NodeT, SPILL><<<g, kTraceBlock, 0, st>>>(L.jobs, L.paths, L.queues);
+        if (!g) g = TraceGrid(KExtend<NodeT, SPILL, UNIFORM>, L.sms);
+        KExtend<NodeT, SPILL, UNIFORM><<<g, kTraceBlock, 0, st>>>(L.jobs, L.paths, L.queues, L.scene);
     } else {
         static int g = 0;
-        if (!g) g = TraceGrid(KConnect<NodeT, SPILL>, L.sms);
-        KConnect<NodeT, SPILL><<<g, kTraceBlock, 0, st>>>(L.jobs, L.paths, L.queues);
+        if (!g) g = TraceGrid(KConnect<NodeT, SPILL, UNIFORM>, L.sms);
+        KConnect<NodeT, SPILL, UNIFORM><<<g, kTraceBlock, 0, st>>>(L.jobs, L.paths, L.queues, L.scene);
+    }
+}
+
+template <class NodeT>
+void LaunchTrace(const PtLaunch& L, cudaStream_t st, bool extend)
+{
+    if (L.spill) {
+        if (L.uniform) LaunchTraceKernels<NodeT, true, true>(L, st, extend);
+        else LaunchTraceKernels<NodeT, true, false>(L, st, extend);
+    } else {
+        if (L.uniform) LaunchTraceKernels<NodeT, false, true>(L, st, extend);
+        else LaunchTraceKernels<NodeT, false, false>(L, st, extend);
     }
 }
 
@@ -694,21 +712,11 @@ cudaError_t PtIteration(const PtLaunch& L, int iter, cudaStream_t st)
     KAssign<<<1, kPtMaxJobs, 0, st>>>(L.jobs, L.ids, L.njobs, L.queues, iter);
     KRegen<<<shadeGrid, kShadeBlock, 0, st>>>(L.jobs, L.njobs, L.paths, L.queues, 1);
     cudaMemsetAsync(L.queues.trace_ctr, 0, 2 * sizeof(unsigned long long), st);
-    if (L.layout == RTB200_BVH_Q8) {
-        if (L.spill) LaunchTraceKernels<QNode4, true>(L, st, true);
-        else LaunchTraceKernels<QNode4, false>(L, st, true);
-    } else {
-        if (L.spill) LaunchTraceKernels<GpuNode4, true>(L, st, true);
-        else LaunchTraceKernels<GpuNode4, false>(L, st, true);
-    }
+    if (L.layout == RTB200_BVH_Q8) LaunchTrace<QNode4>(L, st, true);
+    else LaunchTrace<GpuNode4>(L, st, true);
     KShade<<<shadeGrid, kShadeBlock, 0, st>>>(L.jobs, L.paths, L.queues);
-    if (L.layout == RTB200_BVH_Q8) {
-        if (L.spill) LaunchTraceKernels<QNode4, true>(L, st, false);
-        else LaunchTraceKernels<QNode4, false>(L, st, false);
-    } else {
-        if (L.spill) LaunchTraceKernels<GpuNode4, true>(L, st, false);
-        else LaunchTraceKernels<GpuNode4, false>(L, st, false);
-    }
+    if (L.layout == RTB200_BVH_Q8) LaunchTrace<QNode4>(L, st, false);
+    else LaunchTrace<GpuNode4>(L, st, false);
     KSwap<<<1, 1, 0, st>>>(L.queues.cnt);
     return cudaGetLastError();
 }

@@ -15,6 +15,8 @@ struct PtLaunch {
     int njobs;
     int layout;
     bool spill;        // some job's BVH needs the local-memory stack continuation
+    bool uniform;      // every job renders `scene`
+    PtScene scene;
     PtPaths paths;
     PtQueues queues;
     int sms;

@@ -110,6 +110,7 @@ enum PtCounter : int {
 struct PtScene {
     const void* nodes;
     int layout;
+    int n_nodes;
     const GpuTri* tris;
     int ntri;
     const PtTriAttr* attr;
