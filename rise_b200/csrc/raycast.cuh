@@ -137,28 +137,46 @@ struct ChildHits {
     unsigned mask;
 };
 
-// FP32 node: the reference slab arithmetic (BVH.h:738-763) per child.
+// Three-input minimum / maximum (one instruction on sm_100a).
+__device__ __forceinline__ float Max3(float a, float b, float c)
+{
+    float d;
+    asm("max.f32 %0, %1, %2, %3;" : "=f"(d) : "f"(a), "f"(b), "f"(c));
+    return d;
+}
+__device__ __forceinline__ float Min3(float a, float b, float c)
+{
+    float d;
+    asm("min.f32 %0, %1, %2, %3;" : "=f"(d) : "f"(a), "f"(b), "f"(c));
+    return d;
+}
+
+// FP32 node: the reference slab arithmetic (BVH.h:738-763) per child.  The
+// reference takes min / max of the two plane distances per axis; with a
+// finite reciprocal (zero components map to FLT_MAX) the near plane is the
+// low one for a positive reciprocal and the high one otherwise, so loading
+// the near and far planes by the ray's direction signs gives bit-identical
+// entry / exit distances without the per-axis min / max.
 __device__ __forceinline__ void SlabF32(const GpuNode4* nodes, int ni, const RayPre& p, float best, ChildHits& h)
 {
     const float* base = reinterpret_cast<const float*>(nodes + ni);
-    const float4 lx = ldg4(base + 0), ly = ldg4(base + 4), lz = ldg4(base + 8);
-    const float4 hx = ldg4(base + 12), hy = ldg4(base + 16), hz = ldg4(base + 20);
+    // Float offsets of lox, loy, loz, hix, hiy, hiz: 0, 4, 8, 12, 16, 20.
+    const int nx = p.inv[0] < 0.0f ? 12 : 0, ny = p.inv[1] < 0.0f ? 16 : 4, nz = p.inv[2] < 0.0f ? 20 : 8;
+    const float4 Nx = ldg4(base + nx), Ny = ldg4(base + ny), Nz = ldg4(base + nz);
+    const float4 Fx = ldg4(base + (12 - nx)), Fy = ldg4(base + (20 - ny)), Fz = ldg4(base + (28 - nz));
     const int4 child = ldg4i(base + 24);
     const int4 count = ldg4i(base + 28);
-    const float lxa[4] = {lx.x, lx.y, lx.z, lx.w}, lya[4] = {ly.x, ly.y, ly.z, ly.w}, lza[4] = {lz.x, lz.y, lz.z, lz.w};
-    const float hxa[4] = {hx.x, hx.y, hx.z, hx.w}, hya[4] = {hy.x, hy.y, hy.z, hy.w}, hza[4] = {hz.x, hz.y, hz.z, hz.w};
+    const float nxa[4] = {Nx.x, Nx.y, Nx.z, Nx.w}, nya[4] = {Ny.x, Ny.y, Ny.z, Ny.w}, nza[4] = {Nz.x, Nz.y, Nz.z, Nz.w};
+    const float fxa[4] = {Fx.x, Fx.y, Fx.z, Fx.w}, fya[4] = {Fy.x, Fy.y, Fy.z, Fy.w}, fza[4] = {Fz.x, Fz.y, Fz.z, Fz.w};
     const int cnt[4] = {count.x, count.y, count.z, count.w};
     h.c[0] = child.x; h.c[1] = child.y; h.c[2] = child.z; h.c[3] = child.w;
     h.mask = 0;
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
-        const float t1x = (lxa[i] - p.o[0]) * p.inv[0], t2x = (hxa[i] - p.o[0]) * p.inv[0];
-        const float t1y = (lya[i] - p.o[1]) * p.inv[1], t2y = (hya[i] - p.o[1]) * p.inv[1];
-        const float t1z = (lza[i] - p.o[2]) * p.inv[2], t2z = (hza[i] - p.o[2]) * p.inv[2];
-        float tn = fmaxf(fmaxf(fminf(t1x, t2x), fminf(t1y, t2y)), fminf(t1z, t2z));
-        float tf = fminf(fminf(fmaxf(t1x, t2x), fmaxf(t1y, t2y)), fmaxf(t1z, t2z));
-        tn = fmaxf(tn, p.tmin);
-        tf = fminf(tf, best);
+        const float tn = Max3((nxa[i] - p.o[0]) * p.inv[0], (nya[i] - p.o[1]) * p.inv[1],
+                              fmaxf((nza[i] - p.o[2]) * p.inv[2], p.tmin));
+        const float tf = Min3((fxa[i] - p.o[0]) * p.inv[0], (fya[i] - p.o[1]) * p.inv[1],
+                              fminf((fza[i] - p.o[2]) * p.inv[2], best));
         h.t[i] = tn;
         if (tn <= tf && cnt[i] >= 0) h.mask |= 1u << i;
     }
@@ -172,8 +190,16 @@ __device__ __forceinline__ void SlabQ8(const QNode4* nodes, int ni, const RayPre
     const float org[3] = {__int_as_float(w0.x), __int_as_float(w0.y), __int_as_float(w0.z)};
     const unsigned meta = (unsigned)w0.w;
     const int e[3] = {(int)(int8_t)(meta & 0xff), (int)(int8_t)((meta >> 8) & 0xff), (int)(int8_t)((meta >> 16) & 0xff)};
+    // Near / far quantised planes per axis by the direction's sign (see SlabF32).
     const unsigned qlo[3] = {(unsigned)w1.x, (unsigned)w1.y, (unsigned)w1.z};
     const unsigned qhi[3] = {(unsigned)w1.w, (unsigned)w2.x, (unsigned)w2.y};
+    unsigned qn[3], qf[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const bool neg = p.inv[k] < 0.0f;
+        qn[k] = neg ? qhi[k] : qlo[k];
+        qf[k] = neg ? qlo[k] : qhi[k];
+    }
     h.c[0] = w2.z; h.c[1] = w2.w; h.c[2] = w3.x; h.c[3] = w3.y;
     const int cnt[4] = {(int)(int16_t)(w3.z & 0xffff), (int)(int16_t)((unsigned)w3.z >> 16),
                         (int)(int16_t)(w3.w & 0xffff), (int)(int16_t)((unsigned)w3.w >> 16)};
@@ -189,15 +215,11 @@ __device__ __forceinline__ void SlabQ8(const QNode4* nodes, int ni, const RayPre
         float tl[3], th[3];
 #pragma unroll
         for (int k = 0; k < 3; ++k) {
-            const float ql = (float)((qlo[k] >> (8 * i)) & 0xff);
-            const float qh = (float)((qhi[k] >> (8 * i)) & 0xff);
-            const float t1 = fmaf(ql, s[k], a[k]);
-            const float t2 = fmaf(qh, s[k], a[k]);
-            tl[k] = fminf(t1, t2);
-            th[k] = fmaxf(t1, t2);
+            tl[k] = fmaf((float)((qn[k] >> (8 * i)) & 0xff), s[k], a[k]);
+            th[k] = fmaf((float)((qf[k] >> (8 * i)) & 0xff), s[k], a[k]);
         }
-        const float tn = fmaxf(fmaxf(fmaxf(tl[0], tl[1]), tl[2]), p.tmin);
-        const float tf = fminf(fminf(fminf(th[0], th[1]), th[2]), best);
+        const float tn = Max3(tl[0], tl[1], fmaxf(tl[2], p.tmin));
+        const float tf = Min3(th[0], th[1], fminf(th[2], best));
         h.t[i] = tn;
         if (tn <= tf && cnt[i] >= 0) h.mask |= 1u << i;
     }
