@@ -136,8 +136,9 @@ def cpu_reference_time(tri, rays, seconds=12.0, threads=None):
 def bench_path_tracer(ctx, rank, cpu_baseline=True):
     """Spectral Cornell box (32 triangles, 256x256, 16 spp, 4 wavelengths per
     sample, max depth 8, Russian roulette from depth 3): device throughput in
-    Msamples/s for both NEE modes, and relMSE against a 4096-spp render of an
-    independent seed at 16, 64 and 256 spp."""
+    Msamples/s for both NEE modes, and relMSE at 16 .. 1024 spp against the
+    FP64 oracle's 16384-spp image (tests/golden/cornell_fp64_16384spp.npz,
+    independent seed), with the spp and device time to reach relMSE <= 1e-3."""
     from rise_b200 import pathtracer, scenes
     out = {"workload": "spectral Cornell box: 32 triangles, 256x256, 16 spp, HWSS 4 wavelengths, "
                        "max depth 8, RR from depth 3, seed 1"}
@@ -158,29 +159,25 @@ def bench_path_tracer(ctx, rank, cpu_baseline=True):
                      "segments_per_sample": st["segments"] / st["samples"],
                      "shadow_rays_per_sample": st["shadow_rays"] / st["samples"]}
         r.close()
-    # Converged image: 4096 spp from another seed (per-wavelength NEE).
+    # relMSE against the FP64 oracle's converged image (per-wavelength NEE).
     desc.settings.nee_per_lambda = 1
-    ref_settings = scenes.RenderSettings(**{**desc.settings.__dict__, "seed": 99991})
-    rref = pathtracer.SpectralRasterizer(ctx, desc, scene=scene, settings=ref_settings)
-    for _ in range(16):
-        rref.rasterize_scene(256)
-    ref = rref.film().astype(np.float64)
-    rref.close()
-    rel = {}
+    ref = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "tests", "golden",
+                               "cornell_fp64_16384spp.npz"))["xyz"].astype(np.float64)
+    rel, secs = {}, {}
     r = pathtracer.SpectralRasterizer(ctx, desc, scene=scene)
     done = 0
-    for target in (16, 64, 256):
+    for target in (16, 64, 256, 512, 1024):
         r.rasterize_scene(target - done)
         done = target
         img = r.film().astype(np.float64)
         rel[str(target)] = float(np.mean((img - ref) ** 2 / (ref ** 2 + 1e-2)))
+        secs[str(target)] = r.stats()["seconds"]
     r.close()
-    out["relmse_vs_4096spp"] = rel
-    ms16 = out["nee_per_wavelength"]["ms_per_16spp"]
+    out["relmse_vs_fp64_oracle_16384spp"] = rel
     reach = [int(k) for k, v in rel.items() if v <= 1e-3]
     if reach:
         out["spp_to_relmse_1e-3"] = min(reach)
-        out["seconds_to_relmse_1e-3"] = min(reach) / 16 * ms16 * 1e-3
+        out["device_seconds_to_relmse_1e-3"] = secs[str(min(reach))]
     if cpu_baseline and rank == 0:
         import oracle
         oracle.pt_render(desc, 1, crop=(0, 0, 8, 8))   # one-time table setup outside the timing
@@ -197,7 +194,9 @@ def bench_path_tracer(ctx, rank, cpu_baseline=True):
 def bench_large_scene(ctx, layout="f32"):
     """Large scene: 1024x1024 fBm heightfield (2,093,058 triangles) + 64 spheres
     of 20,000 triangles (half GGX conductors, half glass), area light and sky;
-    1024x1024 pixels, 64 spp, 4 wavelengths, max depth 16."""
+    1024x1024 pixels, 64 spp, 4 wavelengths, max depth 16.  relMSE at 64 and
+    256 spp over the 128x128 image centre against the FP64 oracle's 2048-spp
+    render of that crop (tests/golden/spheres_fp64_crop.npz, independent seed)."""
     from rise_b200 import pathtracer, scenes
     desc = scenes.spheres_scene()
     t0 = time.perf_counter()
@@ -219,6 +218,20 @@ def bench_large_scene(ctx, layout="f32"):
            "shadow_rays_per_sample": (s1["shadow_rays"] - s0["shadow_rays"]) / n,
            "mrays_s": ((s1["segments"] - s0["segments"]) + (s1["shadow_rays"] - s0["shadow_rays"])) / dt / 1e6}
     r.close()
+    ref_path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "tests", "golden", "spheres_fp64_crop.npz")
+    if os.path.exists(ref_path):
+        z = np.load(ref_path)
+        ref = z["xyz"].astype(np.float64)
+        x0, y0, x1, y1 = (int(v) for v in z["crop"])
+        r = pathtracer.SpectralRasterizer(ctx, desc, scene=scene)
+        rel, done = {}, 0
+        for target in (64, 256):
+            r.rasterize_scene(target - done)
+            done = target
+            img = r.film()[y0:y1, x0:x1].astype(np.float64)
+            rel[str(target)] = float(np.mean((img - ref) ** 2 / (ref ** 2 + 1e-2)))
+        r.close()
+        out["relmse_vs_fp64_oracle_crop"] = {"crop": [x0, y0, x1, y1], "oracle_spp": int(z["spp"]), **rel}
     scene.close()
     return out
 
@@ -226,9 +239,12 @@ def bench_large_scene(ctx, layout="f32"):
 def bench_batch(ctx):
     """48 uneven scenes (heightfield + 16 spheres; triangles log-uniform
     10k-1M, resolutions 128^2..1024^2, spp log-uniform 4-256, max depth
-    8-16): one shared engine replaying a captured CUDA graph, against the
-    same jobs rendered one scene at a time on the same engine and kernels."""
-    from rise_b200 import pathtracer, scenes
+    8-16): one shared engine replaying a captured CUDA graph, with pool
+    capacity and poll interval from the autotuner (tuned on every 4th scene
+    at 1/8 of its spp), against the same jobs rendered one scene at a time on
+    the same engine and kernels, and against the plain path (rtb200_job_render
+    per scene: its own default-sized engine, no graph)."""
+    from rise_b200 import autotune, pathtracer, scenes
     params = scenes.batch_scene_params()
     t0 = time.perf_counter()
     descs = [scenes.batch_scene(p) for p in params]
@@ -236,10 +252,16 @@ def bench_batch(ctx):
     setup = time.perf_counter() - t0
     spp = [p["spp"] for p in params]
     total = sum(p["res"] ** 2 * p["spp"] for p in params)
-    eng = pathtracer.Engine(ctx, 1 << 21)
+    t0 = time.perf_counter()
+    best, tried = autotune.tune(ctx, descs[::4], devs[::4], [max(1, s // 8) for s in spp[::4]], use_cache=False)
+    tune_s = time.perf_counter() - t0
+    eng = pathtracer.Engine(ctx, best.capacity)
+    eng.set_poll(best.poll)
     out = {"workload": "48 scenes, triangles log-uniform 10k-1M, resolutions {128,256,512,1024}^2, "
                        "spp log-uniform 4-256, max depth 8-16, FP32 BVH", "samples": total,
-           "triangles": int(sum(p["n_tri"] for p in params)), "scene_setup_s": round(setup, 2)}
+           "triangles": int(sum(p["n_tri"] for p in params)), "scene_setup_s": round(setup, 2),
+           "autotune": {"capacity": best.capacity, "poll": best.poll, "seconds": round(tune_s, 2),
+                        "tried": [[c.capacity, c.poll, round(c.msamples_s, 1)] for c in tried]}}
     try:
         # Warm-up (kernels, graph capture) on a small job.
         w = pathtracer.SpectralRasterizer(ctx, descs[0], scene=devs[0])
@@ -255,10 +277,17 @@ def bench_batch(ctx):
         eng.render(bat, spp, use_graph=True)
         t_bat = time.perf_counter() - t0
         same = all(np.allclose(a.film(), b.film(), rtol=1e-4, atol=1e-6) for a, b in zip(one[:6], bat[:6]))
-        out.update({"one_by_one": {"seconds": t_one, "msamples_s": total / t_one / 1e6},
+        plain = [pathtracer.SpectralRasterizer(ctx, d, scene=s) for d, s in zip(descs, devs)]
+        t0 = time.perf_counter()
+        for r, s in zip(plain, spp):
+            r.rasterize_scene(s)
+        t_plain = time.perf_counter() - t0
+        out.update({"plain_job_render": {"seconds": t_plain, "msamples_s": total / t_plain / 1e6},
+                    "one_by_one": {"seconds": t_one, "msamples_s": total / t_one / 1e6},
                     "batched_graph": {"seconds": t_bat, "msamples_s": total / t_bat / 1e6},
-                    "speedup": t_one / t_bat, "films_equal_first6": bool(same)})
-        for r in one + bat:
+                    "speedup": t_one / t_bat, "speedup_vs_plain": t_plain / t_bat,
+                    "films_equal_first6": bool(same)})
+        for r in one + bat + plain:
             r.close()
     finally:
         eng.close()

@@ -209,6 +209,11 @@ int rtb200_engine_step(rtb200_engine* engine, int32_t iterations, int32_t use_gr
 int rtb200_engine_progress(const rtb200_engine* engine, const rtb200_job* job, int64_t* done, int64_t* total);
 int rtb200_engine_retire(rtb200_engine* engine, rtb200_job* job);
 int rtb200_engine_destroy(rtb200_engine* engine);
+/* Wavefront iterations rtb200_engine_render runs between host polls of the
+ * jobs' progress (default 4; rounded up to even, 2 .. 1024).  Fewer polls
+ * save host round trips, more let a finished batch stop sooner; the project's
+ * autotuner (rise_b200/autotune.py) picks it with the pool capacity. */
+int rtb200_engine_set_poll(rtb200_engine* engine, int32_t iterations);
 
 /* ---- host BVH build and export ----------------------------------------- */
 

@@ -58,6 +58,7 @@ SIGNATURES = {
     "rtb200_engine_progress": (ctypes.c_int, [_vp, _vp, _pi64, _pi64]),
     "rtb200_engine_retire": (ctypes.c_int, [_vp, _vp]),
     "rtb200_engine_destroy": (ctypes.c_int, [_vp]),
+    "rtb200_engine_set_poll": (ctypes.c_int, [_vp, ctypes.c_int32]),
 }
 NOALLOC_SCRATCH_BYTES = 256
 NOALLOC_MAX_RAYS = 2147483647

@@ -76,6 +76,7 @@ struct rtb200_job {
 struct rtb200_engine {
     rtb200_ctx* ctx = nullptr;
     int capacity = 0;
+    int poll = 4;                          // iterations between host polls in EngineRender
     int layout = -1;
     void* buf = nullptr;
     size_t bytes = 0;
@@ -375,7 +376,7 @@ int EngineRender(rtb200_engine* e, rtb200_job* const* jobs, const int32_t* spp, 
     cudaEventRecord(e->e0, ctx->stream);
     const long long kMaxSteps = 1ll << 18;
     for (long long step = 0;; ++step) {
-        const int rc = EngineStep(e, 4, graph);
+        const int rc = EngineStep(e, e->poll, graph);
         if (rc) return rc;
         bool all = true;
         for (int i = 0; i < n; ++i) all = all && JobDone(e, jobs[i]->entry);
@@ -574,6 +575,15 @@ int rtb200_engine_retire(rtb200_engine* e, rtb200_job* job)
     const int rc = EngineRetire(e, job);
     if (rc) return rc;
     return CudaCheck(e->ctx, cudaStreamSynchronize(e->ctx->stream), "film fold");
+}
+
+int rtb200_engine_set_poll(rtb200_engine* e, int32_t iterations)
+{
+    if (!e) return RTB200_E_INVALID;
+    std::lock_guard<std::mutex> g(e->ctx->mu);
+    if (iterations < 1 || iterations > 1024) return SetError(e->ctx, RTB200_E_INVALID, "poll interval out of range");
+    e->poll = (iterations + 1) & ~1;
+    return RTB200_OK;
 }
 
 int rtb200_engine_destroy(rtb200_engine* e)

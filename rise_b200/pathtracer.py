@@ -120,6 +120,10 @@ class Engine:
         counts = (ctypes.c_int32 * n)(*[int(s) for s in spp])
         check(lib().rtb200_engine_render(self.h, jobs, counts, n, int(bool(use_graph))), self.ctx.h)
 
+    def set_poll(self, iterations):
+        """Wavefront iterations between host progress polls in `render`."""
+        check(lib().rtb200_engine_set_poll(self.h, int(iterations)), self.ctx.h)
+
     def submit(self, rasterizer, spp):
         check(lib().rtb200_engine_submit(self.h, rasterizer.h, int(spp)), self.ctx.h)
 

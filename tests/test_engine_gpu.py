@@ -137,3 +137,29 @@ def test_retire_before_done_is_refused(ctx):
     finally:
         r.close()
         eng.close()
+
+
+def test_autotune_picks_a_config_and_poll_does_not_change_images(ctx):
+    from rise_b200 import autotune
+    descs = mixed_descs()
+    devs = [pathtracer.upload_scene(ctx, d) for d in descs]
+    spp = [4, 2, 4]
+    try:
+        best, tried = autotune.tune(ctx, descs, devs, spp, capacities=(1 << 14, 1 << 16), polls=(2, 8),
+                                    use_cache=False)
+        assert len(tried) == 4 and best in tried and best.msamples_s > 0
+        films = []
+        for poll in (2, 8):
+            eng = pathtracer.Engine(ctx, best.capacity)
+            eng.set_poll(poll)
+            rs = [pathtracer.SpectralRasterizer(ctx, d, scene=s) for d, s in zip(descs, devs)]
+            eng.render(rs, spp)
+            films.append([r.film() for r in rs])
+            for r in rs:
+                r.close()
+            eng.close()
+        for a, b in zip(*films):
+            assert np.allclose(a, b, rtol=1e-5, atol=1e-7)
+    finally:
+        for s in devs:
+            s.close()
