@@ -51,6 +51,8 @@ def parse():
     p.add_argument("--no-batch", action="store_true", help="skip the 48-scene batch and the serving run")
     p.add_argument("--pt-only", action="store_true",
                    help="run only the path-tracer measurement and print its JSON (for profiling)")
+    p.add_argument("--large-only", action="store_true",
+                   help="run only the large-scene path-tracer measurement and print its JSON (for profiling)")
     return p.parse_args()
 
 
@@ -370,9 +372,9 @@ def main():
 
     rank, world, local = dist_info()
     torch.cuda.set_device(local)
-    if args.pt_only:
+    if args.pt_only or args.large_only:
         ctx = raycaster.Context(local)
-        print(json.dumps(bench_path_tracer(ctx, rank, cpu_baseline=False)))
+        print(json.dumps(bench_large_scene(ctx) if args.large_only else bench_path_tracer(ctx, rank, cpu_baseline=False)))
         ctx.close()
         return
     if world > 1:

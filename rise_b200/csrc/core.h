@@ -36,6 +36,7 @@ struct rtb200_scene {
     // spectral shading data
     std::vector<float> spectra;                 // 81 samples per spectrum
     std::vector<rtb200::PtMaterial> materials;
+    bool mixed_shading = false;      // materials of more than one shading class
     int32_t env = -1, env_visible = 1;
     std::vector<rtb200::PtLight> lights;        // built at commit
     std::vector<rtb200::PtLightTri> light_tris;

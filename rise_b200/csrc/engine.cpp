@@ -102,6 +102,7 @@ struct rtb200_engine {
     int glayout = -1;
     bool gspill = false;
     const rtb200_scene* gscene = nullptr;  // the shared scene, or null when jobs differ
+    bool gclassify = false;
     long long seg_seen = 0, shadow_seen = 0;
 };
 
@@ -116,8 +117,10 @@ PtLaunch MakeLaunch(const rtb200_engine* e)
     L.layout = e->layout;
     L.spill = false;
     L.uniform = !e->active.empty();
+    L.classify = false;
     for (int k : e->active) {
         L.spill |= e->owner[k]->scene->stack_bound > kTraceStackShared;
+        L.classify |= e->owner[k]->scene->mixed_shading;
         L.uniform &= e->owner[k]->scene == e->owner[e->active[0]]->scene;
     }
     L.scene = L.uniform ? e->h_table[e->active[0]].scene : PtScene{};
@@ -153,7 +156,7 @@ int EngineCreate(rtb200_ctx* ctx, int capacity, rtb200_engine** out)
     const size_t oTab = take(sizeof(PtJobDev) * kMaxJobs), oIds = take(4 * kMaxJobs),
                  oCtr = take(8 * 2 * kMaxJobs);
     const size_t oCnt = take(4 * kCntCount), oTr = take(8 * 2), oSmp = take(8), oErr = take(4),
-                 oAsg = take(sizeof(PtAssign) * kMaxJobs);
+                 oAsg = take(sizeof(PtAssign) * kMaxJobs), oShd = take(4 * c * kShadeClasses);
     int rc = DevAlloc(ctx, &e->buf, off);
     if (rc) { delete e; return rc; }
     e->bytes = off;
@@ -163,7 +166,8 @@ int EngineCreate(rtb200_ctx* ctx, int capacity, rtb200_engine** out)
                        (float4*)(b + oL), (float4*)(b + oAux), (uint4*)(b + oMeta)};
     e->queues = PtQueues{(int*)(b + oQa), (int*)(b + oQan), (int*)(b + oQf), (int*)(b + oQfn),
                          (ShadowEntry*)(b + oSh), (int*)(b + oCnt), (unsigned long long*)(b + oSmp),
-                         (unsigned long long*)(b + oTr), (unsigned*)(b + oErr), (PtAssign*)(b + oAsg)};
+                         (unsigned long long*)(b + oTr), (unsigned*)(b + oErr), (PtAssign*)(b + oAsg),
+                         (int*)(b + oShd), capacity};
     e->d_iota = (int*)(b + oIota);
     e->d_table = (PtJobDev*)(b + oTab);
     e->d_ids = (int*)(b + oIds);
@@ -275,7 +279,7 @@ int EngineStep(rtb200_engine* e, int iterations, bool graph)
     if (graph) {
         const rtb200_scene* us = L.uniform ? e->owner[e->active[0]]->scene : nullptr;
         if (!e->gexec || e->gnjobs != L.njobs || e->glayout != L.layout || e->gspill != L.spill ||
-            e->gscene != us) {
+            e->gscene != us || e->gclassify != L.classify) {
             DropGraph(e);
             cudaGraph_t g = nullptr;
             err = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
@@ -294,6 +298,7 @@ int EngineStep(rtb200_engine* e, int iterations, bool graph)
             e->glayout = L.layout;
             e->gspill = L.spill;
             e->gscene = us;
+            e->gclassify = L.classify;
         }
         const int reps = (iterations + kGraphIters - 1) / kGraphIters;
         for (int r = 0; r < reps && err == cudaSuccess; ++r) err = cudaGraphLaunch(e->gexec, st);

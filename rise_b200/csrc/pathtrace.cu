@@ -6,11 +6,12 @@
 // PathTracingSpectralRasterizer::IntegratePixelSpectral
 // (src/Library/Rendering/PathTracingSpectralRasterizer.cpp:121-198).
 //
-// A fixed pool of path slots lives in HBM as SoA.  One iteration is six
+// A fixed pool of path slots lives in HBM as SoA.  One iteration is seven
 // launches over device-side queues (no host round trip):
 //   KAssign  split the free slots among the jobs that have samples left
 //   KRegen   splat finished paths into the film, start new camera samples
 //   KExtend  closest hit for every active path (warp while-while traversal)
+//   KClassify sort the active paths by the material they hit
 //   KShade   emission + MIS, next-event estimation to area lights and the
 //            sky (shadow-ray queue), hero-wavelength BSDF sampling with
 //            companion-wavelength weights, Russian roulette
@@ -331,12 +332,45 @@ __device__ __forceinline__ float NeeValue(const PtMaterial& M, const float* spec
     return Spec(spectra, M.refl, lam) * kInvPi;
 }
 
+// Sort the active paths into shading classes (escaped or Lambertian, GGX,
+// dielectric) so KShade's warps each run one material model.
 __global__ void __launch_bounds__(kShadeBlock)
-KShade(const PtJobDev* __restrict__ jobs, PtPaths P, PtQueues Q)
+KClassify(const PtJobDev* __restrict__ jobs, PtPaths P, PtQueues Q)
 {
     const int n = Q.cnt[kCntActive];
+    const int stride = gridDim.x * blockDim.x;
+    for (int base = blockIdx.x * blockDim.x; base < n; base += stride) {
+        const int i = base + threadIdx.x;
+        int cls = -1, slot = -1;
+        if (i < n) {
+            slot = Q.active[i];
+            const int hslot = __float_as_int(P.hit[slot].y);
+            cls = 0;
+            if (hslot >= 0) {
+                const PtScene& S = jobs[__float_as_int(P.aux[slot].z)].scene;
+                const int type = S.mats[S.attr[hslot].mat & kAttrMatMask].type;
+                cls = type == kMatGGX ? 1 : (type == kMatDielectric ? 2 : 0);
+            }
+        }
+#pragma unroll
+        for (int c = 0; c < kShadeClasses; ++c) {
+            const int at = WarpAppend(&Q.cnt[kCntClass + c], cls == c);
+            if (cls == c) Q.shade[c * Q.capacity + at] = slot;
+        }
+    }
+}
+
+// classified: the paths come from KClassify's class ranges, else straight from
+// the active queue (scenes with one shading class skip the sort).
+__global__ void __launch_bounds__(kShadeBlock)
+KShade(const PtJobDev* __restrict__ jobs, PtPaths P, PtQueues Q, int classified)
+{
+    const int c0 = Q.cnt[kCntClass], c1 = Q.cnt[kCntClass + 1];
+    const int n = classified ? c0 + c1 + Q.cnt[kCntClass + 2] : Q.cnt[kCntActive];
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const int slot = Q.active[i];
+        const int slot = !classified ? Q.active[i]
+                       : i < c0 ? Q.shade[i]
+                       : (i < c0 + c1 ? Q.shade[Q.capacity + (i - c0)] : Q.shade[2 * Q.capacity + (i - c0 - c1)]);
         const float4 aux = P.aux[slot];
         const PtJobDev& J = jobs[__float_as_int(aux.z)];
         const PtScene& S = J.scene;
@@ -441,6 +475,7 @@ KShade(const PtJobDev* __restrict__ jobs, PtPaths P, PtQueues Q)
                 // LightSampler.cpp:1942-2361): one area-light sample and one sky
                 // sample per wavelength (reference) or one shared sample.
                 const int nsamp = set.nee_per_lambda ? 4 : 1;
+                #pragma unroll 1
                 for (int k = 0; k < nsamp; ++k) {
                     if (set.nee_per_lambda && (term & (1u << k))) continue;
                     if (set.n_lights > 0) {
@@ -481,6 +516,7 @@ KShade(const PtJobDev* __restrict__ jobs, PtPaths P, PtQueues Q)
                                 bool any = false;
                                 const GgxPair bq = NeePair(M, gp, ns, gnv, r, toL);
                                 const float pb = bq.pdf;
+                                #pragma unroll 1
                                 for (int j = 0; j < 4; ++j) {
                                     if (term & (1u << j)) continue;
                                     if (set.nee_per_lambda && j != k) continue;
@@ -509,6 +545,7 @@ KShade(const PtJobDev* __restrict__ jobs, PtPaths P, PtQueues Q)
                             bool any = false;
                             const GgxPair bq = NeePair(M, gp, ns, gnv, r, dir);
                             const float pb = bq.pdf;
+                            #pragma unroll 1
                             for (int j = 0; j < 4; ++j) {
                                 if (term & (1u << j)) continue;
                                 if (set.nee_per_lambda && j != k) continue;
@@ -577,6 +614,7 @@ KShade(const PtJobDev* __restrict__ jobs, PtPaths P, PtQueues Q)
                     // Companions evaluate the BSDF in the hero's direction and
                     // divide by the hero's pdf (:4676-4714).
                     const GgxPair cq = GgxPairAt(gp, w, gnv, r, nd);
+                    #pragma unroll 1
                     for (int k = 1; k < 4; ++k) {
                         if (term & (1u << k)) continue;
                         Set(kray, k, GgxValueAt(cq, GgxAt(M, S.spectra, lam[k]), gp.eavg) * cosV / npdf);
@@ -635,6 +673,7 @@ KShade(const PtJobDev* __restrict__ jobs, PtPaths P, PtQueues Q)
 
 __global__ void KSwap(int* cnt)
 {
+    for (int c = 0; c < kShadeClasses; ++c) cnt[kCntClass + c] = 0;
     cnt[kCntSegments] += cnt[kCntActive];
     cnt[kCntShadowRays] += cnt[kCntShadow];
     cnt[kCntActive] = cnt[kCntActiveNext];
@@ -714,7 +753,8 @@ cudaError_t PtIteration(const PtLaunch& L, int iter, cudaStream_t st)
     cudaMemsetAsync(L.queues.trace_ctr, 0, 2 * sizeof(unsigned long long), st);
     if (L.layout == RTB200_BVH_Q8) LaunchTrace<QNode4>(L, st, true);
     else LaunchTrace<GpuNode4>(L, st, true);
-    KShade<<<shadeGrid, kShadeBlock, 0, st>>>(L.jobs, L.paths, L.queues);
+    if (L.classify) KClassify<<<shadeGrid, kShadeBlock, 0, st>>>(L.jobs, L.paths, L.queues);
+    KShade<<<shadeGrid, kShadeBlock, 0, st>>>(L.jobs, L.paths, L.queues, L.classify ? 1 : 0);
     if (L.layout == RTB200_BVH_Q8) LaunchTrace<QNode4>(L, st, false);
     else LaunchTrace<GpuNode4>(L, st, false);
     KSwap<<<1, 1, 0, st>>>(L.queues.cnt);

@@ -16,6 +16,7 @@ struct PtLaunch {
     int layout;
     bool spill;        // some job's BVH needs the local-memory stack continuation
     bool uniform;      // every job renders `scene`
+    bool classify;     // some job's scene mixes shading classes: sort paths before shading
     PtScene scene;
     PtPaths paths;
     PtQueues queues;

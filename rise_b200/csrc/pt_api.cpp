@@ -41,6 +41,7 @@ int UploadShading(rtb200_scene* s)
     rtb200_ctx* ctx = s->ctx;
     if (s->materials.empty()) return RTB200_OK;  // ray casting only
     const size_t nm = s->materials.size();
+    for (const PtMaterial& m : s->materials) s->mixed_shading |= m.type != s->materials[0].type;
     // GGX conductors: tabulate F_avg(lambda) on the 5 nm grid as an extra
     // spectrum, and make sure the device holds the E_ss / E_avg tables.
     for (PtMaterial& m : s->materials) {

@@ -104,6 +104,7 @@ enum PtCounter : int {
     kCntSegments = 5,   // extended rays (statistics)
     kCntShadowRays = 6,
     kCntAssigned = 7,   // free slots given camera samples this iteration
+    kCntClass = 8,      // kCntClass + c: active paths of shading class c (KClassify)
     kCntCount = 16,
 };
 
@@ -151,7 +152,14 @@ struct PtQueues {
     unsigned long long* trace_ctr;   // [2]: extend, connect
     unsigned* err;
     PtAssign* assign;                // [max jobs], written by KAssign
+    int* shade;                      // [kShadeClasses][capacity]: active slots by shading class
+    int capacity;
 };
+
+// Shading classes: paths that escaped or hit Lambertian surfaces, GGX
+// conductors, smooth dielectrics.  KShade runs them as contiguous ranges so a
+// warp shades one material model.
+constexpr int kShadeClasses = 3;
 
 struct PtFilm {
     float* pass;        // 3 floats per pixel, atomically accumulated this call
