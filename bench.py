@@ -291,6 +291,28 @@ def bench_batch(ctx):
                     "films_equal_first6": bool(same)})
         for r in one + bat + plain:
             r.close()
+        # Small requests (the same 48 scenes at 128x128, 16 spp): the plain
+        # path pays its per-job tail and host polls 48 times, the engine once.
+        small = [scenes.RenderSettings(**{**d.settings.__dict__, "width": 128, "height": 128}) for d in descs]
+        n_small = 48 * 128 * 128 * 16
+        warm = pathtracer.SpectralRasterizer(ctx, descs[0], scene=devs[0], settings=small[0])
+        warm.rasterize_scene(1)
+        warm.close()
+        plain = [pathtracer.SpectralRasterizer(ctx, d, scene=s, settings=st) for d, s, st in zip(descs, devs, small)]
+        t0 = time.perf_counter()
+        for r in plain:
+            r.rasterize_scene(16)
+        t_plain_s = time.perf_counter() - t0
+        bat = [pathtracer.SpectralRasterizer(ctx, d, scene=s, settings=st) for d, s, st in zip(descs, devs, small)]
+        t0 = time.perf_counter()
+        eng.render(bat, [16] * 48, use_graph=True)
+        t_bat_s = time.perf_counter() - t0
+        out["small_requests"] = {"workload": "the 48 scenes at 128x128, 16 spp each",
+                                 "plain_job_render": {"seconds": t_plain_s, "msamples_s": n_small / t_plain_s / 1e6},
+                                 "batched_graph": {"seconds": t_bat_s, "msamples_s": n_small / t_bat_s / 1e6},
+                                 "speedup_vs_plain": t_plain_s / t_bat_s}
+        for r in plain + bat:
+            r.close()
     finally:
         eng.close()
         for s in devs:

@@ -172,11 +172,18 @@ typedef struct {
  * of PathTracingSpectralRasterizer::IntegratePixel,
  * Rendering/PathTracingSpectralRasterizer.cpp:206-479).
  * rtb200_job_read_film writes width*height*3 floats: the mean XYZ per pixel
- * over all samples so far (rows top to bottom). */
+ * over all samples so far (rows top to bottom); RTB200_E_NOT_READY while a
+ * request of the job is in flight on an engine. */
 int rtb200_job_create(rtb200_scene* scene, const rtb200_render_settings* settings, rtb200_job** out);
 int rtb200_job_render(rtb200_job* job, int32_t spp);
 int rtb200_job_read_film(rtb200_job* job, float* xyz);
 int rtb200_job_stats(const rtb200_job* job, rtb200_stats* out);
+/* relMSE of the job's film against a reference image (width*height*3 host
+ * floats, XYZ): the mean over pixels and channels of (x - r)^2 / (r^2 + 1e-2),
+ * reduced on the device in FP64.  Films keep a Kahan-compensated FP32 running
+ * sum up to 4096 samples per pixel and an FP64 one beyond.  No counterpart in
+ * the reference (its convergence tests compare images on the host). */
+int rtb200_job_relmse(rtb200_job* job, const float* ref_xyz, double* relmse);
 int rtb200_job_destroy(rtb200_job* job);
 
 /* ---- engines: many jobs in one wavefront -------------------------------- */

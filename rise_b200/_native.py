@@ -59,6 +59,7 @@ SIGNATURES = {
     "rtb200_engine_retire": (ctypes.c_int, [_vp, _vp]),
     "rtb200_engine_destroy": (ctypes.c_int, [_vp]),
     "rtb200_engine_set_poll": (ctypes.c_int, [_vp, ctypes.c_int32]),
+    "rtb200_job_relmse": (ctypes.c_int, [_vp, _vp, ctypes.POINTER(ctypes.c_double)]),
 }
 NOALLOC_SCRATCH_BYTES = 256
 NOALLOC_MAX_RAYS = 2147483647

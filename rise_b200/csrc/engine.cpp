@@ -30,6 +30,11 @@ using namespace rtb200;
 namespace {
 
 constexpr int kMaxJobs = kPtMaxJobs;
+constexpr long long kWideSpp = 4096;   // samples per pixel kept in the compensated FP32 film
+// Requests of at least this many samples per pixel fold their FP32 pass film
+// into the running sum after every engine step, so no FP32 atomic sum spans
+// more than one step's worth of samples.
+constexpr long long kFoldEverySpp = 64;
 constexpr int kGraphIters = 2;   // iterations per captured graph (even: queue pointers return)
 
 const float kCieY[RTB200_CIE_COUNT] = {RTB200_CIE_YBAR};
@@ -63,6 +68,7 @@ struct rtb200_job {
     float* pass = nullptr;
     float* sum = nullptr;
     float* comp = nullptr;
+    double* wide = nullptr;            // FP64 running sum once past kWideSpp samples per pixel
     long long spp_done = 0;
     long long samples = 0;
     double seconds = 0.0;
@@ -313,6 +319,12 @@ int EngineStep(rtb200_engine* e, int iterations, bool graph)
             std::swap(L.queues.free_, L.queues.free_next);
         }
     }
+    for (size_t a = 0; a < e->active.size() && err == cudaSuccess; ++a) {
+        rtb200_job* j = e->owner[e->active[a]];
+        if (j->pending_spp < kFoldEverySpp) continue;
+        err = j->wide ? PtFoldWide(j->pass, j->sum, j->comp, j->wide, j->npix, false, ctx->num_sms, st)
+                      : PtFold(j->pass, j->sum, j->comp, j->npix, ctx->num_sms, st);
+    }
     if (err == cudaSuccess)
         err = cudaMemcpyAsync(e->h_cnt, e->queues.cnt, 4 * kCntCount, cudaMemcpyDeviceToHost, st);
     if (err == cudaSuccess) err = cudaMemcpyAsync(e->h_ctr, e->d_ctr, 8 * 2 * kMaxJobs, cudaMemcpyDeviceToHost, st);
@@ -342,7 +354,19 @@ int EngineRetire(rtb200_engine* e, rtb200_job* j)
     rtb200_ctx* ctx = e->ctx;
     if (j->engine != e) return SetError(ctx, RTB200_E_INVALID, "job is not submitted to this engine");
     if (!JobDone(e, j->entry)) return SetError(ctx, RTB200_E_NOT_READY, "job still has samples in flight");
-    cudaError_t err = PtFold(j->pass, j->sum, j->comp, j->npix, ctx->num_sms, ctx->stream);
+    // Past kWideSpp samples per pixel the running sum moves to FP64.
+    cudaError_t err;
+    if (!j->wide && j->spp_done + j->pending_spp > kWideSpp) {
+        void* w = nullptr;
+        const int rc = DevAlloc(ctx, &w, 8 * 3 * (size_t)j->npix);
+        if (rc) return rc;
+        j->wide = (double*)w;
+        err = PtFoldWide(j->pass, j->sum, j->comp, j->wide, j->npix, true, ctx->num_sms, ctx->stream);
+    } else if (j->wide) {
+        err = PtFoldWide(j->pass, j->sum, j->comp, j->wide, j->npix, false, ctx->num_sms, ctx->stream);
+    } else {
+        err = PtFold(j->pass, j->sum, j->comp, j->npix, ctx->num_sms, ctx->stream);
+    }
     if (err != cudaSuccess) return CudaCheck(ctx, err, "film fold");
     j->spp_done += j->pending_spp;
     j->samples += (long long)j->npix * j->pending_spp;
@@ -494,14 +518,47 @@ int rtb200_job_read_film(rtb200_job* j, float* xyz)
     if (!j || !xyz) return RTB200_E_INVALID;
     rtb200_ctx* ctx = j->scene->ctx;
     std::lock_guard<std::mutex> g(ctx->mu);
+    if (j->engine) return SetError(ctx, RTB200_E_NOT_READY, "job has a request in flight");
     cudaSetDevice(ctx->device);
     const size_t n3 = 3 * (size_t)j->npix;
+    const double inv = j->spp_done > 0 ? 1.0 / (double)j->spp_done : 0.0;
+    if (j->wide) {
+        std::vector<double> wide(n3);
+        const cudaError_t e = cudaMemcpy(wide.data(), j->wide, 8 * n3, cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess) return CudaCheck(ctx, e, "film readback");
+        for (size_t i = 0; i < n3; ++i) xyz[i] = (float)(wide[i] * inv);
+        return RTB200_OK;
+    }
     std::vector<float> sum(n3), comp(n3);
     cudaError_t e = cudaMemcpy(sum.data(), j->sum, 4 * n3, cudaMemcpyDeviceToHost);
     if (e == cudaSuccess) e = cudaMemcpy(comp.data(), j->comp, 4 * n3, cudaMemcpyDeviceToHost);
     if (e != cudaSuccess) return CudaCheck(ctx, e, "film readback");
-    const double inv = j->spp_done > 0 ? 1.0 / (double)j->spp_done : 0.0;
     for (size_t i = 0; i < n3; ++i) xyz[i] = (float)(((double)sum[i] - (double)comp[i]) * inv);
+    return RTB200_OK;
+}
+
+int rtb200_job_relmse(rtb200_job* j, const float* ref_xyz, double* relmse)
+{
+    if (!j || !ref_xyz || !relmse) return RTB200_E_INVALID;
+    rtb200_ctx* ctx = j->scene->ctx;
+    std::lock_guard<std::mutex> g(ctx->mu);
+    if (j->engine) return SetError(ctx, RTB200_E_NOT_READY, "job has a request in flight");
+    cudaSetDevice(ctx->device);
+    const size_t n3 = 3 * (size_t)j->npix;
+    void* buf = nullptr;
+    int rc = DevAlloc(ctx, &buf, Align(4 * n3) + 8);
+    if (rc) return rc;
+    float* d_ref = (float*)buf;
+    double* d_out = (double*)((char*)buf + Align(4 * n3));
+    double sum = 0.0;
+    cudaError_t e = cudaMemcpyAsync(d_ref, ref_xyz, 4 * n3, cudaMemcpyHostToDevice, ctx->stream);
+    const double inv = j->spp_done > 0 ? 1.0 / (double)j->spp_done : 0.0;
+    if (e == cudaSuccess) e = PtRelMse(j->sum, j->comp, j->wide, d_ref, j->npix, inv, d_out, ctx->num_sms, ctx->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&sum, d_out, 8, cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    DevFree(ctx, buf, Align(4 * n3) + 8);
+    if (e != cudaSuccess) return CudaCheck(ctx, e, "relMSE");
+    *relmse = sum / (double)n3;
     return RTB200_OK;
 }
 
@@ -526,6 +583,7 @@ int rtb200_job_destroy(rtb200_job* j)
     cudaStreamSynchronize(ctx->stream);
     if (j->own) EngineDestroy(j->own);
     DevFree(ctx, j->film_buf, j->film_bytes);
+    if (j->wide) DevFree(ctx, j->wide, 8 * 3 * (size_t)j->npix);
     delete j;
     return RTB200_OK;
 }

@@ -696,6 +696,40 @@ __global__ void KFold(float* pass, float* sum, float* comp, int n3)
     }
 }
 
+// Fold into the FP64 running sum used past 4096 spp; `first` moves the
+// compensated FP32 sum over.
+__global__ void KFoldWide(float* pass, float* sum, float* comp, double* wide, int n3, int first)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n3; i += gridDim.x * blockDim.x) {
+        double w = first ? (double)sum[i] - (double)comp[i] : wide[i];
+        wide[i] = w + (double)pass[i];
+        pass[i] = 0.0f;
+        if (first) sum[i] = comp[i] = 0.0f;
+    }
+}
+
+// relMSE of the film mean (sum / spp, FP32 compensated or FP64) against
+// `ref`: sum over pixels and channels of (x - r)^2 / (r^2 + 1e-2), in FP64.
+__global__ void KRelMse(const float* __restrict__ sum, const float* __restrict__ comp, const double* __restrict__ wide,
+                        const float* __restrict__ ref, int n3, double inv_spp, double* out)
+{
+    double acc = 0.0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n3; i += gridDim.x * blockDim.x) {
+        const double x = (wide ? wide[i] : (double)sum[i] - (double)comp[i]) * inv_spp;
+        const double r = ref[i];
+        acc += (x - r) * (x - r) / (r * r + 1e-2);
+    }
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(kFull, acc, o);
+    __shared__ double part[32];
+    if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        acc = threadIdx.x < (blockDim.x >> 5) ? part[threadIdx.x] : 0.0;
+        for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(kFull, acc, o);
+        if (threadIdx.x == 0) atomicAdd(out, acc);
+    }
+}
+
 // ---- host launchers ----------------------------------------------------------
 
 namespace {
@@ -764,6 +798,22 @@ cudaError_t PtIteration(const PtLaunch& L, int iter, cudaStream_t st)
 cudaError_t PtDrain(const PtLaunch& L, cudaStream_t st)
 {
     KRegen<<<L.sms * 8, kShadeBlock, 0, st>>>(L.jobs, L.njobs, L.paths, L.queues, 0);
+    return cudaGetLastError();
+}
+
+cudaError_t PtFoldWide(float* pass, float* sum, float* comp, double* wide, int npix, bool first, int sms,
+                       cudaStream_t st)
+{
+    KFoldWide<<<sms * 4, 256, 0, st>>>(pass, sum, comp, wide, 3 * npix, first ? 1 : 0);
+    return cudaGetLastError();
+}
+
+cudaError_t PtRelMse(const float* sum, const float* comp, const double* wide, const float* ref, int npix,
+                     double inv_spp, double* out, int sms, cudaStream_t st)
+{
+    cudaError_t e = cudaMemsetAsync(out, 0, sizeof(double), st);
+    if (e != cudaSuccess) return e;
+    KRelMse<<<sms * 2, 256, 0, st>>>(sum, comp, wide, ref, 3 * npix, inv_spp, out);
     return cudaGetLastError();
 }
 

@@ -34,5 +34,12 @@ cudaError_t PtDrain(const PtLaunch& L, cudaStream_t st);
 cudaError_t PtSetGgxTables(const float* ess, const float* eavg, const float* msz, const float* mscum);
 // Fold a film of this request into the compensated running sums and clear it.
 cudaError_t PtFold(float* pass, float* sum, float* comp, int npix, int sms, cudaStream_t st);
+// The same into an FP64 running sum (first: move the FP32 sums over first).
+cudaError_t PtFoldWide(float* pass, float* sum, float* comp, double* wide, int npix, bool first, int sms,
+                       cudaStream_t st);
+// *out = sum over pixels and channels of (x - r)^2 / (r^2 + 1e-2), x the film
+// mean, r the device reference; FP64 accumulation.
+cudaError_t PtRelMse(const float* sum, const float* comp, const double* wide, const float* ref, int npix,
+                     double inv_spp, double* out, int sms, cudaStream_t st);
 
 }  // namespace rtb200

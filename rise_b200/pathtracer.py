@@ -78,6 +78,17 @@ class SpectralRasterizer:
         """Add `spp` samples per pixel (blocking)."""
         check(lib().rtb200_job_render(self.h, int(spp)), self.ctx.h)
 
+    def relmse(self, ref_xyz):
+        """relMSE of the film against `ref_xyz` ((height, width, 3) XYZ),
+        reduced on the device in FP64."""
+        ref = np.ascontiguousarray(ref_xyz, np.float32)
+        st = self.settings
+        if ref.shape != (st.height, st.width, 3):
+            raise ValueError("reference image has the wrong shape")
+        out = ctypes.c_double()
+        check(lib().rtb200_job_relmse(self.h, ctypes.c_void_p(ref.ctypes.data), ctypes.byref(out)), self.ctx.h)
+        return out.value
+
     def film(self):
         """Mean XYZ per pixel, (height, width, 3) float32."""
         st = self.settings

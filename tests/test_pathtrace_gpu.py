@@ -158,3 +158,33 @@ def test_large_scene_against_fp64_oracle_crop(ctx):
     for a in (0, 64):
         for b in (0, 64):
             assert abs(crop[a:a + 64, b:b + 64].mean() / ref[a:a + 64, b:b + 64].mean() - 1.0) < 2e-2, (a, b)
+
+
+def test_device_relmse_matches_host_and_fp64_film_past_4096_spp(ctx):
+    """rtb200_job_relmse (FP64 device reduction) equals the host formula on
+    the read-back film; a job rendered past 4096 spp switches to the FP64
+    running sum at a different point depending on its passes, and the films
+    agree to FP32 rounding."""
+    d = scenes.cornell_box(16, 16)
+    ref = oracle.pt_render(d, 64)
+    r = pathtracer.SpectralRasterizer(ctx, d)
+    try:
+        r.rasterize_scene(64)
+        f = r.film().astype(np.float64)
+        assert abs(r.relmse(ref) / rel_mse(f, ref) - 1.0) < 1e-5
+    finally:
+        r.close()
+    films = []
+    for passes in ([4096, 8], [2048, 2048, 8], [4100, 4]):
+        r = pathtracer.SpectralRasterizer(ctx, d)
+        try:
+            for s in passes:
+                r.rasterize_scene(s)
+            assert r.stats()["spp"] == sum(passes)
+            films.append(r.film().astype(np.float64))
+            if sum(passes) == 4104:
+                assert abs(r.relmse(films[0]) - rel_mse(r.film().astype(np.float64), films[0])) < 1e-12
+        finally:
+            r.close()
+    assert np.allclose(films[0], films[1], rtol=2e-6, atol=1e-9)
+    assert np.isfinite(films[2]).all() and films[2].max() > 0
