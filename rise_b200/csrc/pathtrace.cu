@@ -30,6 +30,9 @@
 namespace rtb200 {
 
 constexpr int kShadeBlock = 256;
+// Leaves tested per lane per traversal round in KExtend / KConnect (measured
+// best for the path tracer's mixed secondary and shadow rays).
+constexpr int kPathLeaves = 1;
 constexpr float kInv4Pi = 0.07957747154594767f;
 
 // ---- film ------------------------------------------------------------------
@@ -242,7 +245,7 @@ KExtend(const PtJobDev* __restrict__ jobs, PtPaths P, PtQueues Q, PtScene us)
             StartRay(s, r);
         }
         if (__all_sync(kFull, qi < 0)) break;
-        if (qi >= 0 && TraceRound<NodeT, false, SPILL>(s, nodes, tris, ntri, stk, Q.err)) {
+        if (qi >= 0 && TraceRound<NodeT, false, SPILL, kPathLeaves>(s, nodes, tris, ntri, stk, Q.err)) {
             P.hit[slot] = make_float4(s.best, __int_as_float(s.bestSlot), s.ba, s.bb);
             qi = -1;
         }
@@ -282,7 +285,7 @@ KConnect(const PtJobDev* __restrict__ jobs, PtPaths P, PtQueues Q, PtScene us)
             StartRay(s, r);
         }
         if (__all_sync(kFull, qi < 0)) break;
-        if (qi >= 0 && TraceRound<NodeT, true, SPILL>(s, nodes, tris, ntri, stk, Q.err)) {
+        if (qi >= 0 && TraceRound<NodeT, true, SPILL, kPathLeaves>(s, nodes, tris, ntri, stk, Q.err)) {
             if (s.bestSlot < 0) {
                 const ShadowEntry& e = Q.shadow[qi];
                 const int slot = __float_as_int(e.d.w);
