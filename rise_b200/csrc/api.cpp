@@ -28,9 +28,15 @@ int DevAlloc(rtb200_ctx* ctx, void** p, size_t bytes)
 {
     *p = nullptr;
     if (bytes == 0) return RTB200_OK;
+    if (ctx->budget && ctx->in_use + ctx->cached + bytes > ctx->budget) DevReleaseCache(ctx);
     if (ctx->budget && ctx->in_use + bytes > ctx->budget)
         return SetError(ctx, RTB200_E_BUDGET, "device memory budget exceeded");
     cudaError_t e = cudaMalloc(p, bytes);
+    if (e == cudaErrorMemoryAllocation && ctx->cached) {
+        cudaGetLastError();
+        DevReleaseCache(ctx);
+        e = cudaMalloc(p, bytes);
+    }
     if (e != cudaSuccess) {
         cudaGetLastError();
         *p = nullptr;
@@ -45,6 +51,43 @@ void DevFree(rtb200_ctx* ctx, void* p, size_t bytes)
     if (!p) return;
     cudaFree(p);
     ctx->in_use -= bytes;
+}
+
+int DevAllocCached(rtb200_ctx* ctx, void** p, size_t bytes)
+{
+    auto it = ctx->cache.find(bytes);
+    if (it != ctx->cache.end() && !it->second.empty()) {
+        if (ctx->budget && ctx->in_use + bytes > ctx->budget)
+            return SetError(ctx, RTB200_E_BUDGET, "device memory budget exceeded");
+        *p = it->second.back();
+        it->second.pop_back();
+        ctx->cached -= bytes;
+        ctx->in_use += bytes;
+        return RTB200_OK;
+    }
+    return DevAlloc(ctx, p, bytes);
+}
+
+void DevFreeCached(rtb200_ctx* ctx, void* p, size_t bytes)
+{
+    if (!p) return;
+    if (ctx->cached + bytes > kDevCacheBytes) {
+        DevFree(ctx, p, bytes);
+        return;
+    }
+    ctx->cache[bytes].push_back(p);
+    ctx->cached += bytes;
+    ctx->in_use -= bytes;
+}
+
+void DevReleaseCache(rtb200_ctx* ctx)
+{
+    if (!ctx->cached) return;
+    cudaStreamSynchronize(ctx->stream);
+    for (auto& kv : ctx->cache)
+        for (void* q : kv.second) cudaFree(q);
+    ctx->cache.clear();
+    ctx->cached = 0;
 }
 
 namespace {
@@ -122,6 +165,7 @@ int rtb200_ctx_destroy(rtb200_ctx* ctx)
     if (!ctx) return RTB200_E_INVALID;
     cudaSetDevice(ctx->device);
     cudaStreamSynchronize(ctx->stream);
+    DevReleaseCache(ctx);
     cudaStreamDestroy(ctx->stream);
     delete ctx;
     return RTB200_OK;

@@ -4,6 +4,7 @@
 
 #include <cstdint>
 #include <mutex>
+#include <unordered_map>
 #include <string>
 #include <vector>
 
@@ -19,6 +20,11 @@ struct rtb200_ctx {
     cudaStream_t stream = nullptr;
     std::mutex mu;
     std::string err;
+    // Freed blocks of DevFreeCached by size, for reuse in stream order on
+    // `stream` (films come and go with every served request; cudaFree would
+    // synchronise the device each time).  Not counted in in_use.
+    std::unordered_map<size_t, std::vector<void*>> cache;
+    size_t cached = 0;
 };
 
 struct rtb200_scene {
@@ -72,6 +78,13 @@ namespace rtb200 {
 // Device allocation against the context budget.
 int DevAlloc(rtb200_ctx* ctx, void** p, size_t bytes);
 void DevFree(rtb200_ctx* ctx, void* p, size_t bytes);
+// The same for blocks used only by work on ctx->stream: a freed block is kept
+// (up to kDevCacheBytes in all) and handed to the next request of the same
+// size, which stream order makes safe.  DevReleaseCache returns them all.
+constexpr size_t kDevCacheBytes = size_t(4) << 30;
+int DevAllocCached(rtb200_ctx* ctx, void** p, size_t bytes);
+void DevFreeCached(rtb200_ctx* ctx, void* p, size_t bytes);
+void DevReleaseCache(rtb200_ctx* ctx);
 int SetError(rtb200_ctx* ctx, int code, const std::string& msg);
 int CudaCheck(rtb200_ctx* ctx, cudaError_t e, const char* what);
 

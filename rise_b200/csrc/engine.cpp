@@ -99,12 +99,13 @@ struct rtb200_engine {
     rtb200_job* owner[kMaxJobs] = {};
     unsigned long long total[kMaxJobs] = {};
     std::vector<int> active;
+    std::vector<int> changed;              // table entries to upload before the next step
     bool dirty = true;
     bool fresh = true;
     int iter = 0;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     cudaGraphExec_t gexec = nullptr;
-    int gnjobs = -1;                       // launch shape the graph was captured for
+    bool ggraph = false;                   // gexec holds a capture for the fields below
     int glayout = -1;
     bool gspill = false;
     const rtb200_scene* gscene = nullptr;  // the shared scene, or null when jobs differ
@@ -119,7 +120,6 @@ PtLaunch MakeLaunch(const rtb200_engine* e)
     PtLaunch L;
     L.jobs = e->d_table;
     L.ids = e->d_ids;
-    L.njobs = (int)e->active.size();
     L.layout = e->layout;
     L.spill = false;
     L.uniform = !e->active.empty();
@@ -140,7 +140,7 @@ void DropGraph(rtb200_engine* e)
 {
     if (e->gexec) cudaGraphExecDestroy(e->gexec);
     e->gexec = nullptr;
-    e->gnjobs = -1;
+    e->ggraph = false;
 }
 
 int EngineCreate(rtb200_ctx* ctx, int capacity, rtb200_engine** out)
@@ -184,7 +184,7 @@ int EngineCreate(rtb200_ctx* ctx, int capacity, rtb200_engine** out)
         cudaMemcpy(e->d_iota, iota.data(), 4 * c, cudaMemcpyHostToDevice);
     }
     if (cudaMallocHost(&e->h_table, sizeof(PtJobDev) * kMaxJobs) != cudaSuccess ||
-        cudaMallocHost(&e->h_ids, 4 * kMaxJobs) != cudaSuccess ||
+        cudaMallocHost(&e->h_ids, 4 * (kMaxJobs + 1)) != cudaSuccess ||
         cudaMallocHost(&e->h_cnt, 4 * kCntCount) != cudaSuccess ||
         cudaMallocHost(&e->h_ctr, 8 * 2 * kMaxJobs) != cudaSuccess || cudaEventCreate(&e->e0) != cudaSuccess ||
         cudaEventCreate(&e->e1) != cudaSuccess) {
@@ -252,6 +252,7 @@ int EngineSubmit(rtb200_engine* e, rtb200_job* j, int spp)
     e->total[entry] = d.total;
     e->owner[entry] = j;
     e->active.push_back(entry);
+    e->changed.push_back(entry);
     e->dirty = true;
     j->engine = e;
     j->entry = entry;
@@ -264,12 +265,6 @@ int EngineStep(rtb200_engine* e, int iterations, bool graph)
     rtb200_ctx* ctx = e->ctx;
     cudaStream_t st = ctx->stream;
     if (e->active.empty()) return RTB200_OK;
-    if (e->dirty) {
-        for (size_t i = 0; i < e->active.size(); ++i) e->h_ids[i] = e->active[i];
-        cudaMemcpyAsync(e->d_table, e->h_table, sizeof(PtJobDev) * kMaxJobs, cudaMemcpyHostToDevice, st);
-        cudaMemcpyAsync(e->d_ids, e->h_ids, 4 * e->active.size(), cudaMemcpyHostToDevice, st);
-        e->dirty = false;
-    }
     if (e->fresh) {
         // Every slot starts free; statistics counters restart from zero.
         cudaMemcpyAsync(e->queues.free_, e->d_iota, 4 * (size_t)e->capacity, cudaMemcpyDeviceToDevice, st);
@@ -280,11 +275,22 @@ int EngineStep(rtb200_engine* e, int iterations, bool graph)
         e->fresh = false;
         e->seg_seen = e->shadow_seen = 0;
     }
+    if (e->dirty) {
+        // Upload the table entries that changed, the id list and its length.
+        for (int k : e->changed)
+            cudaMemcpyAsync(e->d_table + k, e->h_table + k, sizeof(PtJobDev), cudaMemcpyHostToDevice, st);
+        e->changed.clear();
+        for (size_t i = 0; i < e->active.size(); ++i) e->h_ids[i] = e->active[i];
+        e->h_ids[kMaxJobs] = (int)e->active.size();
+        cudaMemcpyAsync(e->d_ids, e->h_ids, 4 * e->active.size(), cudaMemcpyHostToDevice, st);
+        cudaMemcpyAsync(e->queues.cnt + kCntJobs, e->h_ids + kMaxJobs, 4, cudaMemcpyHostToDevice, st);
+        e->dirty = false;
+    }
     PtLaunch L = MakeLaunch(e);
     cudaError_t err = cudaSuccess;
     if (graph) {
         const rtb200_scene* us = L.uniform ? e->owner[e->active[0]]->scene : nullptr;
-        if (!e->gexec || e->gnjobs != L.njobs || e->glayout != L.layout || e->gspill != L.spill ||
+        if (!e->ggraph || e->glayout != L.layout || e->gspill != L.spill ||
             e->gscene != us || e->gclassify != L.classify) {
             DropGraph(e);
             cudaGraph_t g = nullptr;
@@ -300,7 +306,7 @@ int EngineStep(rtb200_engine* e, int iterations, bool graph)
             if (err == cudaSuccess) err = cudaGraphInstantiate(&e->gexec, g, 0);
             if (g) cudaGraphDestroy(g);
             if (err != cudaSuccess) { DropGraph(e); return CudaCheck(ctx, err, "graph capture"); }
-            e->gnjobs = L.njobs;
+            e->ggraph = true;
             e->glayout = L.layout;
             e->gspill = L.spill;
             e->gscene = us;
@@ -358,7 +364,7 @@ int EngineRetire(rtb200_engine* e, rtb200_job* j)
     cudaError_t err;
     if (!j->wide && j->spp_done + j->pending_spp > kWideSpp) {
         void* w = nullptr;
-        const int rc = DevAlloc(ctx, &w, 8 * 3 * (size_t)j->npix);
+        const int rc = DevAllocCached(ctx, &w, 8 * 3 * (size_t)j->npix);
         if (rc) return rc;
         j->wide = (double*)w;
         err = PtFoldWide(j->pass, j->sum, j->comp, j->wide, j->npix, true, ctx->num_sms, ctx->stream);
@@ -376,6 +382,7 @@ int EngineRetire(rtb200_engine* e, rtb200_job* j)
     e->owner[entry] = nullptr;
     e->total[entry] = 0;
     e->h_table[entry].total = 0;
+    e->changed.push_back(entry);
     e->dirty = true;
     j->engine = nullptr;
     j->entry = -1;
@@ -484,10 +491,11 @@ int rtb200_job_create(rtb200_scene* s, const rtb200_render_settings* rs, rtb200_
     st.n_spectra = (int)(s->spectra.size() / RTB200_CIE_COUNT);
     // Film: this request's accumulator, running sum, Kahan compensation.
     const size_t plane = Align(12 * (size_t)j->npix);
-    int rc = DevAlloc(ctx, &j->film_buf, 3 * plane);
+    int rc = DevAllocCached(ctx, &j->film_buf, 3 * plane);
     if (rc) { delete j; return rc; }
     j->film_bytes = 3 * plane;
-    cudaMemset(j->film_buf, 0, 3 * plane);
+    // Stream-ordered: a reused block may still be read by earlier work.
+    cudaMemsetAsync(j->film_buf, 0, 3 * plane, ctx->stream);
     j->pass = (float*)j->film_buf;
     j->sum = (float*)((char*)j->film_buf + plane);
     j->comp = (float*)((char*)j->film_buf + 2 * plane);
@@ -546,7 +554,7 @@ int rtb200_job_relmse(rtb200_job* j, const float* ref_xyz, double* relmse)
     cudaSetDevice(ctx->device);
     const size_t n3 = 3 * (size_t)j->npix;
     void* buf = nullptr;
-    int rc = DevAlloc(ctx, &buf, Align(4 * n3) + 8);
+    int rc = DevAllocCached(ctx, &buf, Align(4 * n3) + 8);
     if (rc) return rc;
     float* d_ref = (float*)buf;
     double* d_out = (double*)((char*)buf + Align(4 * n3));
@@ -556,7 +564,7 @@ int rtb200_job_relmse(rtb200_job* j, const float* ref_xyz, double* relmse)
     if (e == cudaSuccess) e = PtRelMse(j->sum, j->comp, j->wide, d_ref, j->npix, inv, d_out, ctx->num_sms, ctx->stream);
     if (e == cudaSuccess) e = cudaMemcpyAsync(&sum, d_out, 8, cudaMemcpyDeviceToHost, ctx->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
-    DevFree(ctx, buf, Align(4 * n3) + 8);
+    DevFreeCached(ctx, buf, Align(4 * n3) + 8);
     if (e != cudaSuccess) return CudaCheck(ctx, e, "relMSE");
     *relmse = sum / (double)n3;
     return RTB200_OK;
@@ -580,10 +588,11 @@ int rtb200_job_destroy(rtb200_job* j)
     std::lock_guard<std::mutex> g(ctx->mu);
     if (j->engine) return SetError(ctx, RTB200_E_NOT_READY, "retire the job from its engine first");
     cudaSetDevice(ctx->device);
-    cudaStreamSynchronize(ctx->stream);
-    if (j->own) EngineDestroy(j->own);
-    DevFree(ctx, j->film_buf, j->film_bytes);
-    if (j->wide) DevFree(ctx, j->wide, 8 * 3 * (size_t)j->npix);
+    if (j->own) EngineDestroy(j->own);   // synchronises the stream
+    // The film goes back to the context's cache; work still queued on the
+    // stream finishes before any later user of the block runs.
+    DevFreeCached(ctx, j->film_buf, j->film_bytes);
+    if (j->wide) DevFreeCached(ctx, j->wide, 8 * 3 * (size_t)j->npix);
     delete j;
     return RTB200_OK;
 }

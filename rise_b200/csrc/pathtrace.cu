@@ -94,38 +94,58 @@ __device__ __forceinline__ int BlockScan(int v, int* warp_sums)
 }
 
 // Split this iteration's free slots among the jobs that still have camera
-// samples (one block, one thread per job): every such job first gets an equal
-// share (capped by what it has left), the remainder goes to jobs in an order
-// that rotates with the iteration.  Each job's range of free-queue entries and
-// first sample index go to Q.assign; the job's issued counter advances by its
-// share.  Prefix sums replace per-warp atomics on one counter per job.
+// samples (one block, one thread per job).  Every such job first gets a
+// quarter of an equal share (capped by what it has left), so none starves;
+// the rest goes to jobs in order of fewest samples left (shortest remaining
+// first: in a serving mix the first progressive levels of new requests finish
+// before long high-spp levels).  Each job's range of free-queue entries and
+// first sample index go to Q.assign and its issued counter advances by its
+// share.  Block prefix sums replace per-warp atomics on one counter per job.
+// Images do not depend on this schedule: a sample's random numbers depend
+// only on its job, pixel and sample index.
 __global__ void __launch_bounds__(kPtMaxJobs)
-KAssign(const PtJobDev* __restrict__ jobs, const int* __restrict__ ids, int njobs, PtQueues Q, int iter)
+KAssign(const PtJobDev* __restrict__ jobs, const int* __restrict__ ids, PtQueues Q, int iter)
 {
+    const int njobs = Q.cnt[kCntJobs];
     __shared__ int sums[32];
+    __shared__ unsigned long long s_left[kPtMaxJobs];   // samples left per job (for the order)
+    __shared__ int s_sorted[kPtMaxJobs];
+    __shared__ int s_live, s_first;
     const int t = threadIdx.x;
     const int n = Q.cnt[kCntFree];
     int jid = -1, rem = 0;
-    unsigned long long issued = 0;
+    unsigned long long issued = 0, left_all = 0;
     if (t < njobs) {
         jid = ids[(t + iter) % njobs];
         const PtJobDev& J = jobs[jid];
         issued = *J.sample_ctr;
-        if (issued < J.total) rem = (int)min(J.total - issued, (unsigned long long)n);
+        if (issued < J.total) {
+            left_all = J.total - issued;
+            rem = (int)min(left_all, (unsigned long long)n);
+        }
     }
     const int live = BlockScan(rem > 0 ? 1 : 0, sums);
-    __shared__ int s_live, s_first;
     if (t == blockDim.x - 1) s_live = live;
     __syncthreads();
-    const int share = s_live > 0 ? n / s_live : 0;
+    const int share = s_live > 0 ? n / s_live / 4 : 0;
     const int first = min(rem, share);
     const int firstIncl = BlockScan(first, sums);
     if (t == blockDim.x - 1) s_first = firstIncl;
+    s_left[t] = left_all;
     __syncthreads();
     const int left = n - s_first;
     const int more = rem - first;
-    const int moreIncl = BlockScan(more, sums);
-    const int extra = max(0, min(more, left - (moreIncl - more)));
+    // Rank by samples left (ties by position), then a prefix sum in that order.
+    int rank = 0;
+    if (t < njobs)
+        for (int k = 0; k < njobs; ++k) rank += (s_left[k] < left_all) || (s_left[k] == left_all && k < t);
+    if (t < njobs) s_sorted[rank] = more;
+    __syncthreads();
+    const int v = t < njobs ? s_sorted[t] : 0;
+    const int inclSorted = BlockScan(v, sums);
+    s_sorted[t] = inclSorted - v;   // exclusive prefix in rank order
+    __syncthreads();
+    const int extra = t < njobs ? max(0, min(more, left - s_sorted[rank])) : 0;
     const int take = first + extra;
     const int takeIncl = BlockScan(take, sums);
     if (t < njobs) {
@@ -140,8 +160,9 @@ KAssign(const PtJobDev* __restrict__ jobs, const int* __restrict__ ids, int njob
 }
 
 __global__ void __launch_bounds__(kShadeBlock)
-KRegen(const PtJobDev* __restrict__ jobs, int njobs, PtPaths P, PtQueues Q, int assign)
+KRegen(const PtJobDev* __restrict__ jobs, PtPaths P, PtQueues Q, int assign)
 {
+    const int njobs = Q.cnt[kCntJobs];
     const int n = Q.cnt[kCntFree];
     const int nassigned = assign ? Q.cnt[kCntAssigned] : 0;
     const int lane = threadIdx.x & 31;
@@ -785,8 +806,8 @@ cudaError_t PtSetGgxTables(const float* ess, const float* eavg, const float* msz
 cudaError_t PtIteration(const PtLaunch& L, int iter, cudaStream_t st)
 {
     const int shadeGrid = L.sms * 8;
-    KAssign<<<1, kPtMaxJobs, 0, st>>>(L.jobs, L.ids, L.njobs, L.queues, iter);
-    KRegen<<<shadeGrid, kShadeBlock, 0, st>>>(L.jobs, L.njobs, L.paths, L.queues, 1);
+    KAssign<<<1, kPtMaxJobs, 0, st>>>(L.jobs, L.ids, L.queues, iter);
+    KRegen<<<shadeGrid, kShadeBlock, 0, st>>>(L.jobs, L.paths, L.queues, 1);
     cudaMemsetAsync(L.queues.trace_ctr, 0, 2 * sizeof(unsigned long long), st);
     if (L.layout == RTB200_BVH_Q8) LaunchTrace<QNode4>(L, st, true);
     else LaunchTrace<GpuNode4>(L, st, true);
@@ -800,7 +821,7 @@ cudaError_t PtIteration(const PtLaunch& L, int iter, cudaStream_t st)
 
 cudaError_t PtDrain(const PtLaunch& L, cudaStream_t st)
 {
-    KRegen<<<L.sms * 8, kShadeBlock, 0, st>>>(L.jobs, L.njobs, L.paths, L.queues, 0);
+    KRegen<<<L.sms * 8, kShadeBlock, 0, st>>>(L.jobs, L.paths, L.queues, 0);
     return cudaGetLastError();
 }
 

@@ -7,12 +7,12 @@
 namespace rtb200 {
 
 // Everything one wavefront iteration needs.  `jobs` is the device job table;
-// `ids` (device) lists the `njobs` table entries that may receive new
-// samples.  Every job in one engine uses the same BVH layout.
+// `ids` (device) lists the table entries that may receive new samples, and
+// queues.cnt[kCntJobs] (device) how many there are, so a captured iteration
+// serves any number of jobs.  Every job in one engine uses the same BVH layout.
 struct PtLaunch {
     const PtJobDev* jobs;
     const int* ids;
-    int njobs;
     int layout;
     bool spill;        // some job's BVH needs the local-memory stack continuation
     bool uniform;      // every job renders `scene`

@@ -105,6 +105,7 @@ enum PtCounter : int {
     kCntShadowRays = 6,
     kCntAssigned = 7,   // free slots given camera samples this iteration
     kCntClass = 8,      // kCntClass + c: active paths of shading class c (KClassify)
+    kCntJobs = 11,      // entries of the job id list (written by the host)
     kCntCount = 16,
 };
 
