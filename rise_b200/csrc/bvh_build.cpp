@@ -430,7 +430,7 @@ void EncodeGpuNodes(const BuiltBVH& b, std::vector<GpuNode4>& out)
             const bool valid = i < s.nchild;
             d.lox[i] = s.minx[i]; d.loy[i] = s.miny[i]; d.loz[i] = s.minz[i];
             d.hix[i] = s.maxx[i]; d.hiy[i] = s.maxy[i]; d.hiz[i] = s.maxz[i];
-            d.child[i] = !valid ? 0 : Link(s, i, pos);
+            d.child[i] = !valid ? INT32_MIN : Link(s, i, pos);
             d.count[i] = valid ? (int32_t)s.count[i] : -1;
         }
     }

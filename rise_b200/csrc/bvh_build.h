@@ -52,9 +52,12 @@ void BuildReferenceBVH(const float* tri9, int64_t n_tri, int threads, BuiltBVH& 
 // ---- device layouts -------------------------------------------------------
 
 // FP32 wide node: 4 child boxes as SoA float4 + child links, 128 bytes.
-// child[i] >= 0: internal node index; child[i] < 0: a leaf whose first
-// triangle (in leaf order) is ~child[i], holding count[i] triangles (the last
-// one carries GpuTri::v1[3] == 1).  count[i] < 0: empty slot.
+// child[i] >= 0: internal node index; child[i] == INT32_MIN: empty slot;
+// other child[i] < 0: a leaf whose first triangle (in leaf order) is
+// ~child[i], holding count[i] triangles (the last one carries
+// GpuTri::v1[3] == 1).  The traversal reads the first 112 bytes only (empty
+// slots are known from the link); count[i] (-1 for an empty slot) is kept
+// for the host's view of the node.
 struct alignas(16) GpuNode4 {
     float lox[4], loy[4], loz[4];
     float hix[4], hiy[4], hiz[4];

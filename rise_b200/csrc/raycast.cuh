@@ -164,11 +164,9 @@ __device__ __forceinline__ void SlabF32(const GpuNode4* nodes, int ni, const Ray
     const int nx = p.inv[0] < 0.0f ? 12 : 0, ny = p.inv[1] < 0.0f ? 16 : 4, nz = p.inv[2] < 0.0f ? 20 : 8;
     const float4 Nx = ldg4(base + nx), Ny = ldg4(base + ny), Nz = ldg4(base + nz);
     const float4 Fx = ldg4(base + (12 - nx)), Fy = ldg4(base + (20 - ny)), Fz = ldg4(base + (28 - nz));
-    const int4 child = ldg4i(base + 24);
-    const int4 count = ldg4i(base + 28);
+    const int4 child = ldg4i(base + 24);   // empty slots hold kEmpty; counts are not read
     const float nxa[4] = {Nx.x, Nx.y, Nx.z, Nx.w}, nya[4] = {Ny.x, Ny.y, Ny.z, Ny.w}, nza[4] = {Nz.x, Nz.y, Nz.z, Nz.w};
     const float fxa[4] = {Fx.x, Fx.y, Fx.z, Fx.w}, fya[4] = {Fy.x, Fy.y, Fy.z, Fy.w}, fza[4] = {Fz.x, Fz.y, Fz.z, Fz.w};
-    const int cnt[4] = {count.x, count.y, count.z, count.w};
     h.c[0] = child.x; h.c[1] = child.y; h.c[2] = child.z; h.c[3] = child.w;
     h.mask = 0;
 #pragma unroll
@@ -178,7 +176,7 @@ __device__ __forceinline__ void SlabF32(const GpuNode4* nodes, int ni, const Ray
         const float tf = Min3((fxa[i] - p.o[0]) * p.inv[0], (fya[i] - p.o[1]) * p.inv[1],
                               fminf((fza[i] - p.o[2]) * p.inv[2], best));
         h.t[i] = tn;
-        if (tn <= tf && cnt[i] >= 0) h.mask |= 1u << i;
+        if (tn <= tf && h.c[i] != kEmpty) h.mask |= 1u << i;
     }
 }
 
