@@ -3,6 +3,7 @@
 // Ownership follows the reference's explicit create/release style
 // (src/Library/Interfaces/IReference.h) with opaque handles; failures return
 // a status code and leave a message in rtb200_last_error instead of logging.
+#include <algorithm>
 #include <chrono>
 #include <cstring>
 #include <new>
@@ -114,6 +115,60 @@ int EnsureStage(rtb200_scene* s, size_t in_bytes, size_t out_bytes)
     return RTB200_OK;
 }
 
+// Host-buffer casts in chunks: the upload of chunk k+1 (copy_in stream) and
+// the download of chunk k-1 (copy_out stream) overlap the trace of chunk k,
+// with two staging buffers each way and events ordering their reuse.  Chunks
+// alternate between two trace streams (ctx->stream, ctx->trace2), each launch
+// with its own work counter, so one chunk's blocks start while the previous
+// chunk's last rays finish instead of the device idling in every launch's tail.
+// `trace(d_in, m, d_out, counter, stream)` launches the kernel on m staged rays.
+template <class Trace>
+cudaError_t PipelinedCast(rtb200_scene* s, const rtb200_ray* rays, int64_t n, void* out, size_t out_bytes_per_ray,
+                          int& rc, Trace trace)
+{
+    rtb200_ctx* ctx = s->ctx;
+    const int64_t chunk = std::max<int64_t>(std::min<int64_t>(n, int64_t(1) << 18), (n + 7) / 8);
+    const int nbuf = n > chunk ? 2 : 1;
+    rc = EnsureStage(s, (size_t)nbuf * chunk * sizeof(rtb200_ray), (size_t)nbuf * chunk * out_bytes_per_ray);
+    if (rc) return cudaSuccess;
+    cudaStream_t ts[2] = {ctx->stream, ctx->trace2};
+    // Work counters of the two trace streams (scene scratch bytes 128 and 192).
+    unsigned long long* counter[2] = {(unsigned long long*)((char*)s->d_counter + 128),
+                                      (unsigned long long*)((char*)s->d_counter + 192)};
+    // Everything after the work already queued on ctx->stream.
+    cudaError_t e = cudaEventRecord(ctx->ev_trace[0], ts[0]);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(ctx->copy_in, ctx->ev_trace[0], 0);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(ts[1], ctx->ev_trace[0], 0);
+    const int64_t nchunks = (n + chunk - 1) / chunk;
+    for (int64_t k = 0; k < nchunks && e == cudaSuccess; ++k) {
+        const int b = (int)(k & 1);
+        const int64_t off = k * chunk, m = std::min(chunk, n - off);
+        rtb200_ray* d_in = (rtb200_ray*)s->d_in + b * chunk;
+        char* d_out = (char*)s->d_out + (size_t)b * chunk * out_bytes_per_ray;
+        if (k >= 2) e = cudaStreamWaitEvent(ctx->copy_in, ctx->ev_trace[b], 0);   // chunk k-2 traced
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(d_in, rays + off, (size_t)m * sizeof(rtb200_ray), cudaMemcpyHostToDevice, ctx->copy_in);
+        if (e == cudaSuccess) e = cudaEventRecord(ctx->ev_up[b], ctx->copy_in);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(ts[b], ctx->ev_up[b], 0);
+        if (e == cudaSuccess && k >= 2) e = cudaStreamWaitEvent(ts[b], ctx->ev_down[b], 0);   // chunk k-2 downloaded
+        if (e == cudaSuccess) e = cudaMemsetAsync(counter[b], 0, sizeof(unsigned long long), ts[b]);
+        if (e == cudaSuccess) e = trace(d_in, m, d_out, counter[b], ts[b]);
+        if (e == cudaSuccess) e = cudaEventRecord(ctx->ev_trace[b], ts[b]);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(ctx->copy_out, ctx->ev_trace[b], 0);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync((char*)out + (size_t)off * out_bytes_per_ray, d_out, (size_t)m * out_bytes_per_ray,
+                                cudaMemcpyDeviceToHost, ctx->copy_out);
+        if (e == cudaSuccess) e = cudaEventRecord(ctx->ev_down[b], ctx->copy_out);
+    }
+    // Later work on ctx->stream waits for both trace streams and the downloads.
+    if (e == cudaSuccess) e = cudaEventRecord(ctx->ev_trace[1], ts[1]);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(ts[0], ctx->ev_trace[1], 0);
+    if (e == cudaSuccess) e = cudaEventRecord(ctx->ev_down[0], ctx->copy_out);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(ts[0], ctx->ev_down[0], 0);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ts[0]);
+    return e;
+}
+
 int CheckErrWord(rtb200_scene* s, cudaStream_t st)
 {
     unsigned err = 0;
@@ -149,9 +204,17 @@ int rtb200_ctx_create(int device, size_t budget_bytes, rtb200_ctx** out)
     if (!ctx) return RTB200_E_OOM;
     ctx->device = device;
     ctx->budget = budget_bytes;
-    if (cudaSetDevice(device) != cudaSuccess ||
-        cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess ||
-        cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    bool ok = cudaSetDevice(device) == cudaSuccess &&
+              cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, device) == cudaSuccess &&
+              cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) == cudaSuccess &&
+              cudaStreamCreateWithFlags(&ctx->copy_in, cudaStreamNonBlocking) == cudaSuccess &&
+              cudaStreamCreateWithFlags(&ctx->copy_out, cudaStreamNonBlocking) == cudaSuccess &&
+              cudaStreamCreateWithFlags(&ctx->trace2, cudaStreamNonBlocking) == cudaSuccess;
+    for (int b = 0; b < 2 && ok; ++b)
+        ok = cudaEventCreateWithFlags(&ctx->ev_up[b], cudaEventDisableTiming) == cudaSuccess &&
+             cudaEventCreateWithFlags(&ctx->ev_trace[b], cudaEventDisableTiming) == cudaSuccess &&
+             cudaEventCreateWithFlags(&ctx->ev_down[b], cudaEventDisableTiming) == cudaSuccess;
+    if (!ok) {
         cudaGetLastError();
         delete ctx;
         return RTB200_E_DEVICE;
@@ -166,6 +229,14 @@ int rtb200_ctx_destroy(rtb200_ctx* ctx)
     cudaSetDevice(ctx->device);
     cudaStreamSynchronize(ctx->stream);
     DevReleaseCache(ctx);
+    for (int b = 0; b < 2; ++b) {
+        cudaEventDestroy(ctx->ev_up[b]);
+        cudaEventDestroy(ctx->ev_trace[b]);
+        cudaEventDestroy(ctx->ev_down[b]);
+    }
+    cudaStreamDestroy(ctx->copy_in);
+    cudaStreamDestroy(ctx->copy_out);
+    cudaStreamDestroy(ctx->trace2);
     cudaStreamDestroy(ctx->stream);
     delete ctx;
     return RTB200_OK;
@@ -385,15 +456,14 @@ int rtb200_cast_closest(rtb200_scene* s, const rtb200_ray* rays, int64_t n, rtb2
     if (n < 0 || (n > 0 && (!rays || !hits))) return SetError(ctx, RTB200_E_INVALID, "bad ray buffers");
     if (n == 0) return RTB200_OK;
     cudaSetDevice(ctx->device);
-    int rc = EnsureStage(s, (size_t)n * sizeof(rtb200_ray), (size_t)n * sizeof(rtb200_hit));
+    int rc = RTB200_OK;
+    const cudaError_t e = PipelinedCast(s, rays, n, hits, sizeof(rtb200_hit), rc,
+        [s](const rtb200_ray* in, int64_t m, char* out, unsigned long long* counter, cudaStream_t st) {
+            return LaunchCastClosestScratch(s, in, m, (rtb200_hit*)out, counter, s->d_err, st);
+        });
     if (rc) return rc;
-    cudaStream_t st = ctx->stream;
-    cudaError_t e = cudaMemcpyAsync(s->d_in, rays, (size_t)n * sizeof(rtb200_ray), cudaMemcpyHostToDevice, st);
-    if (e == cudaSuccess) e = LaunchCastClosest(s, (const rtb200_ray*)s->d_in, n, (rtb200_hit*)s->d_out, st);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(hits, s->d_out, (size_t)n * sizeof(rtb200_hit), cudaMemcpyDeviceToHost, st);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) return CudaCheck(ctx, e, "closest-hit cast");
-    return CheckErrWord(s, st);
+    return CheckErrWord(s, ctx->stream);
 }
 
 int rtb200_cast_any(rtb200_scene* s, const rtb200_ray* rays, int64_t n, uint8_t* occ)
@@ -405,15 +475,14 @@ int rtb200_cast_any(rtb200_scene* s, const rtb200_ray* rays, int64_t n, uint8_t*
     if (n < 0 || (n > 0 && (!rays || !occ))) return SetError(ctx, RTB200_E_INVALID, "bad ray buffers");
     if (n == 0) return RTB200_OK;
     cudaSetDevice(ctx->device);
-    int rc = EnsureStage(s, (size_t)n * sizeof(rtb200_ray), (size_t)n);
+    int rc = RTB200_OK;
+    const cudaError_t e = PipelinedCast(s, rays, n, occ, 1, rc,
+        [s](const rtb200_ray* in, int64_t m, char* out, unsigned long long* counter, cudaStream_t st) {
+            return LaunchCastAnyScratch(s, in, m, (uint8_t*)out, counter, s->d_err, st);
+        });
     if (rc) return rc;
-    cudaStream_t st = ctx->stream;
-    cudaError_t e = cudaMemcpyAsync(s->d_in, rays, (size_t)n * sizeof(rtb200_ray), cudaMemcpyHostToDevice, st);
-    if (e == cudaSuccess) e = LaunchCastAny(s, (const rtb200_ray*)s->d_in, n, (uint8_t*)s->d_out, st);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(occ, s->d_out, (size_t)n, cudaMemcpyDeviceToHost, st);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) return CudaCheck(ctx, e, "any-hit cast");
-    return CheckErrWord(s, st);
+    return CheckErrWord(s, ctx->stream);
 }
 
 }  // extern "C"

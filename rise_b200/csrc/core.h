@@ -18,6 +18,10 @@ struct rtb200_ctx {
     size_t budget = 0;      // 0 = no cap
     size_t in_use = 0;
     cudaStream_t stream = nullptr;
+    // Copy streams, a second trace stream and events of the pipelined
+    // host-buffer casts.
+    cudaStream_t copy_in = nullptr, copy_out = nullptr, trace2 = nullptr;
+    cudaEvent_t ev_up[2] = {}, ev_trace[2] = {}, ev_down[2] = {};
     std::mutex mu;
     std::string err;
     // Freed blocks of DevFreeCached by size, for reuse in stream order on
@@ -100,6 +104,8 @@ cudaError_t LaunchCastAny(const rtb200_scene* s, const rtb200_ray* d_rays, int64
                           uint8_t* d_occ, cudaStream_t stream);
 // Closest-hit launch with caller-provided scratch (work counter and error
 // word); clears nothing itself.
+cudaError_t LaunchCastAnyScratch(const rtb200_scene* s, const rtb200_ray* d_rays, int64_t n, uint8_t* d_occ,
+                                 unsigned long long* counter, unsigned* err, cudaStream_t stream);
 cudaError_t LaunchCastClosestScratch(const rtb200_scene* s, const rtb200_ray* d_rays, int64_t n,
                                      rtb200_hit* d_hits, unsigned long long* counter, unsigned* err,
                                      cudaStream_t stream);

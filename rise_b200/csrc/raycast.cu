@@ -123,6 +123,12 @@ cudaError_t LaunchCastClosestScratch(const rtb200_scene* s, const rtb200_ray* d_
     return Dispatch<false>(s, d_rays, n, d_hits, nullptr, counter, err, stream);
 }
 
+cudaError_t LaunchCastAnyScratch(const rtb200_scene* s, const rtb200_ray* d_rays, int64_t n, uint8_t* d_occ,
+                                 unsigned long long* counter, unsigned* err, cudaStream_t stream)
+{
+    return Dispatch<true>(s, d_rays, n, nullptr, d_occ, counter, err, stream);
+}
+
 cudaError_t LaunchCastAny(const rtb200_scene* s, const rtb200_ray* d_rays, int64_t n,
                           uint8_t* d_occ, cudaStream_t stream)
 {
