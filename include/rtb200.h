@@ -153,7 +153,22 @@ typedef struct {
                                  reference; 0: one shared sample per vertex */
     uint32_t seed;
     int32_t max_paths;        /* path-pool capacity (0 = automatic) */
+    int32_t filter;           /* RTB200_FILTER_* */
+    float filter_size;        /* Gaussian: kernel width in pixels (support = size / 2), 0 < size <= 16 */
+    float filter_sigma;       /* Gaussian: standard deviation in pixels, > 0 */
 } rtb200_render_settings;
+
+/* Pixel filters.  BOX: uniform jitter in the pixel, the pixel is the mean of
+ * its own samples.  GAUSSIAN: the reference's GaussianPixelFilter
+ * (Sampling/GaussianPixelFilter.h:40-127).  With a half-width above 0.501
+ * pixel every sample is splatted into the pixels within the support and a
+ * pixel resolves to sum(w XYZ) / sum(w), 0 where sum(w) <= 1e-10
+ * (PixelBasedRasterizerHelper.cpp:143-149, FilteredFilm.cpp:42-132); a
+ * narrower kernel instead moves each camera sample by the truncated
+ * Gaussian about the pixel centre and averages the pixel's own samples
+ * (PathTracingSpectralRasterizer.cpp:321-331). */
+#define RTB200_FILTER_BOX 0
+#define RTB200_FILTER_GAUSSIAN 1
 
 typedef struct rtb200_job rtb200_job;
 

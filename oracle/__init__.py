@@ -180,8 +180,10 @@ def pt_render(desc, spp, sample_begin=0, crop=None, threads=None, settings=None)
     mats_f = np.array([[m.alpha, m.ior] for m in desc.materials], np.float32)
     envi = np.array([desc.env, desc.env_visible], np.int32)
     cam = np.array(list(st.cam_pos) + list(st.cam_look) + list(st.cam_up) + [st.fov_deg], np.float64)
-    setd = np.array([st.lambda_min, st.lambda_max, st.rr_threshold], np.float64)
-    seti = np.array([st.width, st.height, st.max_depth, st.rr_min_depth, st.nee_per_lambda, st.seed], np.int32)
+    setd = np.array([st.lambda_min, st.lambda_max, st.rr_threshold, getattr(st, "filter_size", 2.0),
+                     getattr(st, "filter_sigma", 0.5)], np.float64)
+    seti = np.array([st.width, st.height, st.max_depth, st.rr_min_depth, st.nee_per_lambda, st.seed,
+                     getattr(st, "filter", 0)], np.int32)
     out = np.zeros((y1 - y0, x1 - x0, 3), np.float64)
     cie = np.ascontiguousarray(cie_table())
     f = lib.orc_pt_render
@@ -226,6 +228,7 @@ _BLOCK_SIGS = {
     "fresnel_avg": (_D, [_D, _D, _D]),
     "fms": (_D, [_D, _D]),
     "power_heuristic": (_D, [_D, _D]),
+    "gaussian_weight": (_D, [_D, _D, _D, _D]),
 }
 _ref_pt = None
 

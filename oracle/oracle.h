@@ -62,8 +62,12 @@ int  orc_ray_triangle(const double* o, const double* d, const double* v0, const 
  *   mats_i: n_mat x 5 int32 (type, reflectance, emission, eta, kappa)
  *   mats_f: n_mat x 2 float (alpha, ior)
  *   cam:    10 doubles (pos, look, up, vertical fov in degrees)
- *   setd:   3 doubles (lambda_min, lambda_max, rr_threshold)
- *   seti:   6 int32 (width, height, max_depth, rr_min_depth, nee_per_lambda, seed)
+ *   setd:   5 doubles (lambda_min, lambda_max, rr_threshold, filter size, filter sigma)
+ *   seti:   7 int32 (width, height, max_depth, rr_min_depth, nee_per_lambda, seed, filter)
+ * filter 0 is the box film (mean of the pixel's own samples); filter 1 is the
+ * Gaussian pixel filter: with size / 2 > 0.501 the samples of every pixel
+ * within the support are splatted and a pixel is sum(w XYZ) / sum(w); a
+ * narrower kernel warps each camera sample about the pixel centre instead.
  *   envi:   2 int32 (environment spectrum or -1, visible)
  *   cie:    3 x 81 doubles, the reference's CIE 1931 table (x, y, z bars)
  * Returns 0 on success. */
@@ -75,6 +79,7 @@ int orc_pt_render(const float* tri9, int64_t n_tri, const int64_t* meshes, int32
 
 /* Building blocks of the path-tracing oracle, exported so tests can hold each
  * against the reference's own code (oracle/_ref/libref_pt.so). */
+double orc_pt_gaussian_weight(double size, double sigma, double dx, double dy);
 void   orc_pt_sample_wavelengths(double u, double lmin, double lmax, double* lam4);
 int    orc_pt_xyz_from_nm(double nm, const double* cie, double* xyz3);
 double orc_pt_ggx_d(double alpha, double cos_h);

@@ -342,6 +342,9 @@ struct Scene {
     int width, height, maxDepth, rrMinDepth, neePerLambda;
     uint32_t seed;
     V pos, fwd, right, up;
+    // Gaussian pixel filter too narrow for the filtered film: the camera
+    // sample is warped about the pixel centre (warpSigma > 0), else 0.
+    double warpSigma = 0.0, warpTrunc = 1.0;
 };
 
 // InterpSPDIndices + linear interpolation (ColorUtils.cpp:270-300).
@@ -454,7 +457,17 @@ void Sample(const Scene& S, uint32_t pixel, uint32_t sample, double xyz[3])
 {
     const uint32_t key = PathKey(S.seed, pixel, sample);
     const int px = (int)(pixel % (uint32_t)S.width), py = (int)(pixel / (uint32_t)S.width);
-    const double fx = px + Rand(key, 0), fy = py + Rand(key, 1);
+    double ox = Rand(key, 0), oy = Rand(key, 1);
+    if (S.warpSigma > 0.0) {
+        // GaussianPixelFilter::warp (Sampling/GaussianPixelFilter.h:109-127),
+        // about the pixel centre (PathTracingSpectralRasterizer.cpp:327-328).
+        const double v = std::max(S.warpTrunc + (1.0 - S.warpTrunc) * ox, 1e-30);
+        const double r = S.warpSigma * std::sqrt(-2.0 * std::log(v));
+        const double th = 2.0 * kPi * oy;
+        ox = 0.5 + r * std::cos(th);
+        oy = 0.5 + r * std::sin(th);
+    }
+    const double fx = px + ox, fy = py + oy;
     const double sx = 2.0 * fx / S.width - 1.0, sy = 1.0 - 2.0 * fy / S.height;
     V d = Norm(S.fwd + S.right * sx + S.up * sy);
     V o = S.pos;
@@ -668,6 +681,17 @@ void Sample(const Scene& S, uint32_t pixel, uint32_t sample, double xyz[3])
 
 }  // namespace
 
+/* GaussianPixelFilter::EvaluateFilter (Sampling/GaussianPixelFilter.h:67-78):
+ * exp(-r^2 / (2 sigma^2)) / (2 pi sigma^2) inside the size x size box centred
+ * on the pixel centre, 0 outside it. */
+extern "C" double orc_pt_gaussian_weight(double size, double sigma, double dx, double dy)
+{
+    const double h = 0.5 * size;
+    if (std::fabs(dx) > h || std::fabs(dy) > h) return 0.0;
+    const double two_s2 = 2.0 * sigma * sigma;
+    return 1.0 / (kPi * two_s2) * std::exp(-(dx * dx + dy * dy) / two_s2);
+}
+
 extern "C" int orc_pt_render(const float* tri9, int64_t n_tri, const int64_t* meshes, int32_t n_mesh,
                              const float* spectra, int32_t n_spec, const int32_t* mats_i, const float* mats_f,
                              int32_t n_mat, const int32_t* envi, const double* cam, const double* setd,
@@ -754,6 +778,62 @@ extern "C" int orc_pt_render(const float* tri9, int64_t n_tri, const int64_t* me
     for (size_t i = 0; i < S.lights.size(); ++i) S.lights[i].pdf = weight[i] / wsum;
     S.bvh = orc_bvh_build(tri9, n_tri);
     const int cw = x1 - x0, ch = y1 - y0;
+    if (seti[6] == 1 && 0.5 * setd[3] <= 0.501) {
+        // Too narrow for the filtered film (PixelBasedRasterizerHelper.cpp:143-149).
+        const double k = 0.5 * setd[3] / setd[4];
+        S.warpSigma = setd[4];
+        S.warpTrunc = std::exp(-0.5 * k * k);
+    } else if (seti[6] == 1) {
+        // GaussianPixelFilter + FilteredFilm (Rendering/FilteredFilm.cpp:42-132):
+        // every sample of the pixels within the support of the crop is
+        // splatted at its screen position (uniform in its pixel, pixel centres
+        // on integer coordinates); a crop pixel resolves to sum(w XYZ) / sum(w).
+        const double size = setd[3], hw = 0.5 * setd[3], sigma = setd[4];
+        const int m = (int)std::ceil(hw) + 1;
+        const int ex0 = std::max(0, x0 - m), ex1 = std::min(S.width, x1 + m);
+        const int ey0 = std::max(0, y0 - m), ey1 = std::min(S.height, y1 + m);
+        const int nt = std::max(1, threads);
+        std::vector<std::vector<double>> films(nt, std::vector<double>(4 * (size_t)cw * ch, 0.0));
+        std::atomic<int> row(ey0);
+        auto fwork = [&](int tid) {
+            std::vector<double>& film = films[tid];
+            for (int py; (py = row.fetch_add(1)) < ey1;) {
+                for (int px = ex0; px < ex1; ++px) {
+                    const uint32_t pixel = (uint32_t)(py * S.width + px);
+                    for (int s = 0; s < spp; ++s) {
+                        const uint32_t sample = (uint32_t)(sample_begin + s);
+                        double v[3];
+                        Sample(S, pixel, sample, v);
+                        const uint32_t key = PathKey(S.seed, pixel, sample);
+                        const double sx = px + Rand(key, 0) - 0.5, sy = py + Rand(key, 1) - 0.5;
+                        const int qx0 = std::max(x0, (int)std::floor(sx - hw));
+                        const int qx1 = std::min(x1 - 1, (int)std::floor(sx + hw));
+                        const int qy0 = std::max(y0, (int)std::floor(sy - hw));
+                        const int qy1 = std::min(y1 - 1, (int)std::floor(sy + hw));
+                        for (int qy = qy0; qy <= qy1; ++qy)
+                            for (int qx = qx0; qx <= qx1; ++qx) {
+                                const double w = orc_pt_gaussian_weight(size, sigma, sx - qx, sy - qy);
+                                if (w == 0.0) continue;
+                                double* f = &film[4 * ((size_t)(qy - y0) * cw + (qx - x0))];
+                                for (int c = 0; c < 3; ++c) f[c] += w * v[c];
+                                f[3] += w;
+                            }
+                    }
+                }
+            }
+        };
+        std::vector<std::thread> fpool;
+        for (int t = 0; t < nt; ++t) fpool.emplace_back(fwork, t);
+        for (auto& t : fpool) t.join();
+        for (size_t p = 0; p < (size_t)cw * ch; ++p) {
+            double a[4] = {0, 0, 0, 0};
+            for (const auto& film : films)
+                for (int c = 0; c < 4; ++c) a[c] += film[4 * p + c];
+            for (int c = 0; c < 3; ++c) xyz[3 * p + c] = std::fabs(a[3]) > 1e-10 ? a[c] / a[3] : 0.0;
+        }
+        orc_bvh_destroy(S.bvh);
+        return 0;
+    }
     std::atomic<int> next(0);
     auto work = [&]() {
         for (;;) {

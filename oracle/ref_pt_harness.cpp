@@ -23,6 +23,8 @@
 #include "Utilities/PathTransportUtilities.h"
 #include "Utilities/Color/ColorUtils.h"
 #include "Interfaces/ILog.h"
+#include "Interfaces/IOptions.h"
+#include "Sampling/GaussianPixelFilter.h"
 
 namespace RISE
 {
@@ -40,6 +42,22 @@ namespace RISE
 		void FlushPrinters() override {}
 	};
 	ILog* GlobalLog() { static QuietPtLog log; return &log; }
+
+	// Default-valued options: the reference-counting base of the pixel
+	// filter links the reference's thread wrapper, which reads one
+	// scheduling option; the harness does not link the options-file parser.
+	class DefaultPtOptions : public IOptions
+	{
+	public:
+		void addref() const override {}
+		bool release() const override { return false; }
+		unsigned int refcount() const override { return 1; }
+		int ReadInt( const char*, int d ) override { return d; }
+		double ReadDouble( const char*, double d ) override { return d; }
+		bool ReadBool( const char*, bool d ) override { return d; }
+		String ReadString( const char*, String d ) override { return d; }
+	};
+	IOptions& GlobalOptions() { static DefaultPtOptions o; return o; }
 }
 
 using namespace RISE;
@@ -132,6 +150,14 @@ int ref_pt_russian_roulette(unsigned depth, unsigned min_depth, double threshold
         PathTransportUtilities::EvaluateRussianRoulette(depth, min_depth, threshold, cur, prev, u);
     *survival = r.survivalProb;
     return r.terminate ? 1 : 0;
+}
+
+double ref_pt_gaussian_weight(double size, double sigma, double dx, double dy)
+{
+    Implementation::GaussianPixelFilter* f = new Implementation::GaussianPixelFilter(size, sigma);
+    const double w = f->EvaluateFilter(dx, dy);
+    f->release();
+    return w;
 }
 
 }  // extern "C"

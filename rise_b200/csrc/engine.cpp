@@ -63,6 +63,8 @@ struct rtb200_job {
     PtCamera cam{};
     PtSettings set{};
     int npix = 0;
+    int channels = 3;                  // floats per film pixel: XYZ (+ weight when splatted)
+    int film_n = 0;                    // channels * npix
     void* film_buf = nullptr;
     size_t film_bytes = 0;
     float* pass = nullptr;
@@ -328,8 +330,8 @@ int EngineStep(rtb200_engine* e, int iterations, bool graph)
     for (size_t a = 0; a < e->active.size() && err == cudaSuccess; ++a) {
         rtb200_job* j = e->owner[e->active[a]];
         if (j->pending_spp < kFoldEverySpp) continue;
-        err = j->wide ? PtFoldWide(j->pass, j->sum, j->comp, j->wide, j->npix, false, ctx->num_sms, st)
-                      : PtFold(j->pass, j->sum, j->comp, j->npix, ctx->num_sms, st);
+        err = j->wide ? PtFoldWide(j->pass, j->sum, j->comp, j->wide, j->film_n, false, ctx->num_sms, st)
+                      : PtFold(j->pass, j->sum, j->comp, j->film_n, ctx->num_sms, st);
     }
     if (err == cudaSuccess)
         err = cudaMemcpyAsync(e->h_cnt, e->queues.cnt, 4 * kCntCount, cudaMemcpyDeviceToHost, st);
@@ -364,14 +366,14 @@ int EngineRetire(rtb200_engine* e, rtb200_job* j)
     cudaError_t err;
     if (!j->wide && j->spp_done + j->pending_spp > kWideSpp) {
         void* w = nullptr;
-        const int rc = DevAllocCached(ctx, &w, 8 * 3 * (size_t)j->npix);
+        const int rc = DevAllocCached(ctx, &w, 8 * (size_t)j->film_n);
         if (rc) return rc;
         j->wide = (double*)w;
-        err = PtFoldWide(j->pass, j->sum, j->comp, j->wide, j->npix, true, ctx->num_sms, ctx->stream);
+        err = PtFoldWide(j->pass, j->sum, j->comp, j->wide, j->film_n, true, ctx->num_sms, ctx->stream);
     } else if (j->wide) {
-        err = PtFoldWide(j->pass, j->sum, j->comp, j->wide, j->npix, false, ctx->num_sms, ctx->stream);
+        err = PtFoldWide(j->pass, j->sum, j->comp, j->wide, j->film_n, false, ctx->num_sms, ctx->stream);
     } else {
-        err = PtFold(j->pass, j->sum, j->comp, j->npix, ctx->num_sms, ctx->stream);
+        err = PtFold(j->pass, j->sum, j->comp, j->film_n, ctx->num_sms, ctx->stream);
     }
     if (err != cudaSuccess) return CudaCheck(ctx, err, "film fold");
     j->spp_done += j->pending_spp;
@@ -447,6 +449,10 @@ int rtb200_job_create(rtb200_scene* s, const rtb200_render_settings* rs, rtb200_
         rs->max_depth > 255 || !(rs->lambda_max > rs->lambda_min) || rs->lambda_min < 380.0f ||
         rs->lambda_max > 780.0f || !(rs->fov_deg > 0.0f && rs->fov_deg < 180.0f))
         return SetError(ctx, RTB200_E_INVALID, "bad render settings");
+    if (rs->filter != RTB200_FILTER_BOX &&
+        !(rs->filter == RTB200_FILTER_GAUSSIAN && rs->filter_size > 0.0f && rs->filter_size <= 16.0f &&
+          rs->filter_sigma > 0.0f))
+        return SetError(ctx, RTB200_E_INVALID, "bad pixel filter settings");
     // Camera frame (pinhole; vertical field of view).
     const float* P = rs->cam_pos;
     double f[3] = {rs->cam_look[0] - P[0], rs->cam_look[1] - P[1], rs->cam_look[2] - P[2]};
@@ -489,8 +495,21 @@ int rtb200_job_create(rtb200_scene* s, const rtb200_render_settings* rs, rtb200_
     st.env_visible = s->env_visible;
     st.n_lights = (int)s->lights.size();
     st.n_spectra = (int)(s->spectra.size() / RTB200_CIE_COUNT);
-    // Film: this request's accumulator, running sum, Kahan compensation.
-    const size_t plane = Align(12 * (size_t)j->npix);
+    const bool gauss = rs->filter == RTB200_FILTER_GAUSSIAN;
+    st.filter = !gauss ? kFilterBox : (0.5 * rs->filter_size > 0.501 ? kFilterSplat : kFilterWarp);
+    st.filt_half = gauss ? 0.5f * rs->filter_size : 0.5f;
+    st.filt_inv2s2 = gauss ? 1.0f / (2.0f * rs->filter_sigma * rs->filter_sigma) : 0.0f;
+    st.filt_norm = gauss ? (float)(1.0 / (3.14159265358979323846 * 2.0 * rs->filter_sigma * rs->filter_sigma)) : 1.0f;
+    st.filt_sigma = gauss ? rs->filter_sigma : 0.0f;
+    {
+        const double k = gauss ? 0.5 * rs->filter_size / rs->filter_sigma : 0.0;
+        st.filt_trunc = (float)std::exp(-0.5 * k * k);
+    }
+    // Film: this request's accumulator, running sum, Kahan compensation; XYZ
+    // per pixel, plus the weight sum for splatted films.
+    j->channels = st.filter == kFilterSplat ? 4 : 3;
+    j->film_n = j->channels * j->npix;
+    const size_t plane = Align(4 * (size_t)j->film_n);
     int rc = DevAllocCached(ctx, &j->film_buf, 3 * plane);
     if (rc) { delete j; return rc; }
     j->film_bytes = 3 * plane;
@@ -528,20 +547,29 @@ int rtb200_job_read_film(rtb200_job* j, float* xyz)
     std::lock_guard<std::mutex> g(ctx->mu);
     if (j->engine) return SetError(ctx, RTB200_E_NOT_READY, "job has a request in flight");
     cudaSetDevice(ctx->device);
-    const size_t n3 = 3 * (size_t)j->npix;
-    const double inv = j->spp_done > 0 ? 1.0 / (double)j->spp_done : 0.0;
+    const size_t n = (size_t)j->film_n;
+    std::vector<double> acc(n);
     if (j->wide) {
-        std::vector<double> wide(n3);
-        const cudaError_t e = cudaMemcpy(wide.data(), j->wide, 8 * n3, cudaMemcpyDeviceToHost);
+        const cudaError_t e = cudaMemcpy(acc.data(), j->wide, 8 * n, cudaMemcpyDeviceToHost);
         if (e != cudaSuccess) return CudaCheck(ctx, e, "film readback");
-        for (size_t i = 0; i < n3; ++i) xyz[i] = (float)(wide[i] * inv);
-        return RTB200_OK;
+    } else {
+        std::vector<float> sum(n), comp(n);
+        cudaError_t e = cudaMemcpy(sum.data(), j->sum, 4 * n, cudaMemcpyDeviceToHost);
+        if (e == cudaSuccess) e = cudaMemcpy(comp.data(), j->comp, 4 * n, cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess) return CudaCheck(ctx, e, "film readback");
+        for (size_t i = 0; i < n; ++i) acc[i] = (double)sum[i] - (double)comp[i];
     }
-    std::vector<float> sum(n3), comp(n3);
-    cudaError_t e = cudaMemcpy(sum.data(), j->sum, 4 * n3, cudaMemcpyDeviceToHost);
-    if (e == cudaSuccess) e = cudaMemcpy(comp.data(), j->comp, 4 * n3, cudaMemcpyDeviceToHost);
-    if (e != cudaSuccess) return CudaCheck(ctx, e, "film readback");
-    for (size_t i = 0; i < n3; ++i) xyz[i] = (float)(((double)sum[i] - (double)comp[i]) * inv);
+    if (j->channels == 3) {
+        const double inv = j->spp_done > 0 ? 1.0 / (double)j->spp_done : 0.0;
+        for (size_t i = 0; i < n; ++i) xyz[i] = (float)(acc[i] * inv);
+    } else {
+        // FilteredFilm resolve (Rendering/FilteredFilm.cpp:100-132): weighted
+        // sum over the weight; pixels no sample reached stay 0.
+        for (size_t p = 0; p < (size_t)j->npix; ++p) {
+            const double w = acc[4 * p + 3];
+            for (int c = 0; c < 3; ++c) xyz[3 * p + c] = std::fabs(w) > 1e-10 ? (float)(acc[4 * p + c] / w) : 0.0f;
+        }
+    }
     return RTB200_OK;
 }
 
@@ -561,7 +589,8 @@ int rtb200_job_relmse(rtb200_job* j, const float* ref_xyz, double* relmse)
     double sum = 0.0;
     cudaError_t e = cudaMemcpyAsync(d_ref, ref_xyz, 4 * n3, cudaMemcpyHostToDevice, ctx->stream);
     const double inv = j->spp_done > 0 ? 1.0 / (double)j->spp_done : 0.0;
-    if (e == cudaSuccess) e = PtRelMse(j->sum, j->comp, j->wide, d_ref, j->npix, inv, d_out, ctx->num_sms, ctx->stream);
+    if (e == cudaSuccess)
+        e = PtRelMse(j->sum, j->comp, j->wide, d_ref, j->npix, j->channels, inv, d_out, ctx->num_sms, ctx->stream);
     if (e == cudaSuccess) e = cudaMemcpyAsync(&sum, d_out, 8, cudaMemcpyDeviceToHost, ctx->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
     DevFreeCached(ctx, buf, Align(4 * n3) + 8);
@@ -592,7 +621,7 @@ int rtb200_job_destroy(rtb200_job* j)
     // The film goes back to the context's cache; work still queued on the
     // stream finishes before any later user of the block runs.
     DevFreeCached(ctx, j->film_buf, j->film_bytes);
-    if (j->wide) DevFreeCached(ctx, j->wide, 8 * 3 * (size_t)j->npix);
+    if (j->wide) DevFreeCached(ctx, j->wide, 8 * (size_t)j->film_n);
     delete j;
     return RTB200_OK;
 }

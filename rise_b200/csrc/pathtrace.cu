@@ -61,10 +61,39 @@ __device__ __forceinline__ void Splat(const PtPaths& P, const PtJobDev& J, int s
     }
     if (active == 0) return;
     const float s = S.ynorm / (float)active;
-    float* px = J.film + 3 * (size_t)m.x;
-    if (X != 0.0f) atomicAdd(px + 0, X * s);
-    if (Y != 0.0f) atomicAdd(px + 1, Y * s);
-    if (Z != 0.0f) atomicAdd(px + 2, Z * s);
+    if (S.filter != kFilterSplat) {
+        float* px = J.film + 3 * (size_t)m.x;
+        if (X != 0.0f) atomicAdd(px + 0, X * s);
+        if (Y != 0.0f) atomicAdd(px + 1, Y * s);
+        if (Z != 0.0f) atomicAdd(px + 2, Z * s);
+        return;
+    }
+    // FilteredFilm::Splat (Rendering/FilteredFilm.cpp:42-98): the sample's
+    // screen position (uniform in its pixel, pixel centres on integer
+    // coordinates) adds w XYZ and w to every pixel within the Gaussian's
+    // support, w = exp(-r^2 / 2 sigma^2) / (2 pi sigma^2)
+    // (GaussianPixelFilter.h:67-78).
+    const int W = J.cam.width, H = J.cam.height;
+    const int px = (int)(m.x % (uint32_t)W), py = (int)(m.x / (uint32_t)W);
+    const float sx = (float)px + Rand(m.w, 0) - 0.5f, sy = (float)py + Rand(m.w, 1) - 0.5f;
+    const float hw = S.filt_half;
+    const int x0 = max(0, (int)floorf(sx - hw)), x1 = min(W - 1, (int)floorf(sx + hw));
+    const int y0 = max(0, (int)floorf(sy - hw)), y1 = min(H - 1, (int)floorf(sy + hw));
+    X *= s; Y *= s; Z *= s;
+    for (int qy = y0; qy <= y1; ++qy) {
+        const float dy = sy - (float)qy;
+        if (fabsf(dy) > hw) continue;
+        for (int qx = x0; qx <= x1; ++qx) {
+            const float dx = sx - (float)qx;
+            if (fabsf(dx) > hw) continue;
+            const float w = S.filt_norm * expf(-(dx * dx + dy * dy) * S.filt_inv2s2);
+            float* f = J.film + 4 * ((size_t)qy * W + qx);
+            if (X != 0.0f) atomicAdd(f + 0, X * w);
+            if (Y != 0.0f) atomicAdd(f + 1, Y * w);
+            if (Z != 0.0f) atomicAdd(f + 2, Z * w);
+            atomicAdd(f + 3, w);
+        }
+    }
 }
 
 // ---- kernels ---------------------------------------------------------------
@@ -202,8 +231,20 @@ KRegen(const PtJobDev* __restrict__ jobs, PtPaths P, PtQueues Q, int assign)
                 const uint32_t sample = (uint32_t)(J.sample_begin + g / (unsigned long long)J.npix);
                 const uint32_t key = PathKey(J.set.seed, pixel, sample);
                 const int px = (int)(pixel % (uint32_t)J.cam.width), py = (int)(pixel / (uint32_t)J.cam.width);
-                // Box pixel filter of width 1: uniform jitter inside the pixel.
-                const float fx = (float)px + Rand(key, 0), fy = (float)py + Rand(key, 1);
+                // Box pixel filter of width 1 (and the splatted Gaussian):
+                // uniform jitter inside the pixel.  A Gaussian too narrow for
+                // the filtered film moves the sample about the pixel centre by
+                // the truncated kernel's inverse CDF (GaussianPixelFilter.h:109-127).
+                float ox = Rand(key, 0), oy = Rand(key, 1);
+                if (J.set.filter == kFilterWarp) {
+                    const float v = fmaxf(J.set.filt_trunc + (1.0f - J.set.filt_trunc) * ox, 1e-30f);
+                    const float r = J.set.filt_sigma * sqrtf(-2.0f * logf(v));
+                    float sn, cs;
+                    sincospif(2.0f * oy, &sn, &cs);
+                    ox = 0.5f + r * cs;
+                    oy = 0.5f + r * sn;
+                }
+                const float fx = (float)px + ox, fy = (float)py + oy;
                 const float sx = 2.0f * fx / (float)J.cam.width - 1.0f;
                 const float sy = 1.0f - 2.0f * fy / (float)J.cam.height;
                 const V3 d = normalize(mk(J.cam.fwd[0] + sx * J.cam.right[0] + sy * J.cam.up[0],
@@ -708,9 +749,9 @@ __global__ void KSwap(int* cnt)
 }
 
 // Kahan-compensated fold of this call's film into the running sums.
-__global__ void KFold(float* pass, float* sum, float* comp, int n3)
+__global__ void KFold(float* pass, float* sum, float* comp, int n)
 {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n3; i += gridDim.x * blockDim.x) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const float y = pass[i] - comp[i];
         const float s = sum[i];
         const float t = s + y;
@@ -722,9 +763,9 @@ __global__ void KFold(float* pass, float* sum, float* comp, int n3)
 
 // Fold into the FP64 running sum used past 4096 spp; `first` moves the
 // compensated FP32 sum over.
-__global__ void KFoldWide(float* pass, float* sum, float* comp, double* wide, int n3, int first)
+__global__ void KFoldWide(float* pass, float* sum, float* comp, double* wide, int n, int first)
 {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n3; i += gridDim.x * blockDim.x) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         double w = first ? (double)sum[i] - (double)comp[i] : wide[i];
         wide[i] = w + (double)pass[i];
         pass[i] = 0.0f;
@@ -732,14 +773,30 @@ __global__ void KFoldWide(float* pass, float* sum, float* comp, double* wide, in
     }
 }
 
-// relMSE of the film mean (sum / spp, FP32 compensated or FP64) against
-// `ref`: sum over pixels and channels of (x - r)^2 / (r^2 + 1e-2), in FP64.
+__device__ __forceinline__ double FilmValue(const float* __restrict__ sum, const float* __restrict__ comp,
+                                            const double* __restrict__ wide, int k)
+{
+    return wide ? wide[k] : (double)sum[k] - (double)comp[k];
+}
+
+// relMSE of the resolved film (FP32 compensated or FP64 sums; 3 channels:
+// sum / spp, 4 channels: weighted sum / weight, 0 where the weight is at most
+// 1e-10) against `ref` (XYZ per pixel): sum over pixels and channels of
+// (x - r)^2 / (r^2 + 1e-2), in FP64.
 __global__ void KRelMse(const float* __restrict__ sum, const float* __restrict__ comp, const double* __restrict__ wide,
-                        const float* __restrict__ ref, int n3, double inv_spp, double* out)
+                        const float* __restrict__ ref, int npix, int channels, double inv_spp, double* out)
 {
     double acc = 0.0;
+    const int n3 = 3 * npix;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n3; i += gridDim.x * blockDim.x) {
-        const double x = (wide ? wide[i] : (double)sum[i] - (double)comp[i]) * inv_spp;
+        double x;
+        if (channels == 3) {
+            x = FilmValue(sum, comp, wide, i) * inv_spp;
+        } else {
+            const int p = i / 3;
+            const double w = FilmValue(sum, comp, wide, 4 * p + 3);
+            x = fabs(w) > 1e-10 ? FilmValue(sum, comp, wide, 4 * p + i - 3 * p) / w : 0.0;
+        }
         const double r = ref[i];
         acc += (x - r) * (x - r) / (r * r + 1e-2);
     }
@@ -825,25 +882,25 @@ cudaError_t PtDrain(const PtLaunch& L, cudaStream_t st)
     return cudaGetLastError();
 }
 
-cudaError_t PtFoldWide(float* pass, float* sum, float* comp, double* wide, int npix, bool first, int sms,
+cudaError_t PtFoldWide(float* pass, float* sum, float* comp, double* wide, int n, bool first, int sms,
                        cudaStream_t st)
 {
-    KFoldWide<<<sms * 4, 256, 0, st>>>(pass, sum, comp, wide, 3 * npix, first ? 1 : 0);
+    KFoldWide<<<sms * 4, 256, 0, st>>>(pass, sum, comp, wide, n, first ? 1 : 0);
     return cudaGetLastError();
 }
 
 cudaError_t PtRelMse(const float* sum, const float* comp, const double* wide, const float* ref, int npix,
-                     double inv_spp, double* out, int sms, cudaStream_t st)
+                     int channels, double inv_spp, double* out, int sms, cudaStream_t st)
 {
     cudaError_t e = cudaMemsetAsync(out, 0, sizeof(double), st);
     if (e != cudaSuccess) return e;
-    KRelMse<<<sms * 2, 256, 0, st>>>(sum, comp, wide, ref, 3 * npix, inv_spp, out);
+    KRelMse<<<sms * 2, 256, 0, st>>>(sum, comp, wide, ref, npix, channels, inv_spp, out);
     return cudaGetLastError();
 }
 
-cudaError_t PtFold(float* pass, float* sum, float* comp, int npix, int sms, cudaStream_t st)
+cudaError_t PtFold(float* pass, float* sum, float* comp, int n, int sms, cudaStream_t st)
 {
-    KFold<<<sms * 4, 256, 0, st>>>(pass, sum, comp, 3 * npix);
+    KFold<<<sms * 4, 256, 0, st>>>(pass, sum, comp, n);
     return cudaGetLastError();
 }
 

@@ -32,14 +32,16 @@ cudaError_t PtDrain(const PtLaunch& L, cudaStream_t st);
 // Upload the GGX E_ss (32 x 32), E_avg (32), multiple-scattering lobe
 // normalisation (32) and cumulative segment integral (32 x 34) tables.
 cudaError_t PtSetGgxTables(const float* ess, const float* eavg, const float* msz, const float* mscum);
-// Fold a film of this request into the compensated running sums and clear it.
-cudaError_t PtFold(float* pass, float* sum, float* comp, int npix, int sms, cudaStream_t st);
+// Fold a film of this request (n floats) into the compensated running sums
+// and clear it.
+cudaError_t PtFold(float* pass, float* sum, float* comp, int n, int sms, cudaStream_t st);
 // The same into an FP64 running sum (first: move the FP32 sums over first).
-cudaError_t PtFoldWide(float* pass, float* sum, float* comp, double* wide, int npix, bool first, int sms,
+cudaError_t PtFoldWide(float* pass, float* sum, float* comp, double* wide, int n, bool first, int sms,
                        cudaStream_t st);
-// *out = sum over pixels and channels of (x - r)^2 / (r^2 + 1e-2), x the film
-// mean, r the device reference; FP64 accumulation.
+// *out = sum over pixels and XYZ channels of (x - r)^2 / (r^2 + 1e-2), x the
+// resolved film (channels 3: sum * inv_spp; 4: weighted sum / weight), r the
+// device reference; FP64 accumulation.
 cudaError_t PtRelMse(const float* sum, const float* comp, const double* wide, const float* ref, int npix,
-                     double inv_spp, double* out, int sms, cudaStream_t st);
+                     int channels, double inv_spp, double* out, int sms, cudaStream_t st);
 
 }  // namespace rtb200

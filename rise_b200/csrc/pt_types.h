@@ -68,7 +68,22 @@ struct PtSettings {
     int env_visible;         // sky seen directly by camera rays
     int n_lights;
     int n_spectra;
+    int filter;              // kFilterBox / kFilterSplat / kFilterWarp
+    float filt_half;         // support half-width in pixels
+    float filt_inv2s2;       // 1 / (2 sigma^2)
+    float filt_norm;         // 1 / (2 pi sigma^2)
+    float filt_sigma;        // Gaussian sigma in pixels (warp mode)
+    float filt_trunc;        // exp(-K^2 / 2), K = half-width / sigma (warp mode)
 };
+
+// Film modes of PtSettings::filter.  The reference splats into a filtered
+// film only when the filter's half-support exceeds 0.501 pixel
+// (PixelBasedRasterizerHelper.cpp:143-149); a narrower Gaussian instead warps
+// the camera sample by the truncated kernel and averages with weight 1
+// (PathTracingSpectralRasterizer.cpp:321-331, GaussianPixelFilter.h:109-127).
+constexpr int kFilterBox = 0;     // uniform jitter in the pixel, 3-channel mean
+constexpr int kFilterSplat = 1;   // Gaussian splat, 4 channels (XYZ and weight)
+constexpr int kFilterWarp = 2;    // Gaussian-warped position, 3-channel mean
 
 // Per-triangle shading attributes in leaf order: material | double-sided
 // bit (bit 30), and luminary index (-1 = none).

@@ -27,7 +27,8 @@ class RenderSettings(ctypes.Structure):
                 ("cam_pos", ctypes.c_float * 3), ("cam_look", ctypes.c_float * 3), ("cam_up", ctypes.c_float * 3),
                 ("fov_deg", ctypes.c_float), ("lambda_min", ctypes.c_float), ("lambda_max", ctypes.c_float),
                 ("max_depth", ctypes.c_int32), ("rr_min_depth", ctypes.c_int32), ("rr_threshold", ctypes.c_float),
-                ("nee_per_lambda", ctypes.c_int32), ("seed", ctypes.c_uint32), ("max_paths", ctypes.c_int32)]
+                ("nee_per_lambda", ctypes.c_int32), ("seed", ctypes.c_uint32), ("max_paths", ctypes.c_int32),
+                ("filter", ctypes.c_int32), ("filter_size", ctypes.c_float), ("filter_sigma", ctypes.c_float)]
 
 
 class Stats(ctypes.Structure):
@@ -57,7 +58,8 @@ def upload_scene(ctx, desc, layout="f32"):
 def settings_struct(st):
     return RenderSettings(st.width, st.height, (ctypes.c_float * 3)(*st.cam_pos), (ctypes.c_float * 3)(*st.cam_look),
                           (ctypes.c_float * 3)(*st.cam_up), st.fov_deg, st.lambda_min, st.lambda_max, st.max_depth,
-                          st.rr_min_depth, st.rr_threshold, st.nee_per_lambda, st.seed, st.max_paths)
+                          st.rr_min_depth, st.rr_threshold, st.nee_per_lambda, st.seed, st.max_paths,
+                          getattr(st, "filter", 0), getattr(st, "filter_size", 2.0), getattr(st, "filter_sigma", 0.5))
 
 
 class SpectralRasterizer:

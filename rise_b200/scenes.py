@@ -142,6 +142,9 @@ class RenderSettings:
     nee_per_lambda: int = 1
     seed: int = 1
     max_paths: int = 0
+    filter: int = 0           # 0 box; 1 Gaussian (GaussianPixelFilter; splatted when size / 2 > 0.501)
+    filter_size: float = 2.0  # Gaussian kernel width in pixels
+    filter_sigma: float = 0.5 # Gaussian standard deviation in pixels
 
 
 @dataclass

@@ -120,6 +120,9 @@ def main():
     out["fresnel_avg"] = [[ni, nt, k, r.ref_pt_fresnel_avg(ni, nt, k)] for ni, nt, k in [(1, 0.2, 3.0), (1, 1.5, 0.0), (1, 2.9, 3.1)]]
     out["fms"] = [[f, e, r.ref_pt_fms(f, e)] for f, e in [(0.9, 0.6), (0.3, 0.99), (1.0, 0.3)]]
     out["power_heuristic"] = [[a, b, r.ref_pt_power_heuristic(a, b)] for a, b in [(1, 1), (0.2, 5), (3, 0.01)]]
+    out["gaussian_filter"] = [[s, g, dx, dy, r.ref_pt_gaussian_weight(s, g, dx, dy)]
+                              for s, g in [(2.0, 0.5), (3.0, 1.0), (1.0, 0.3)]
+                              for dx, dy in [(0, 0), (0.3, -0.2), (0.99, 0.5), (1.0, 0.0), (-1.01, 0.1), (1.4, 1.4)]]
     rows = []
     for depth, mind, thr, cur, prev, u in [(2, 3, 0.05, 0.1, 1.0, 0.9), (3, 3, 0.05, 0.1, 1.0, 0.05), (3, 3, 0.05, 0.1, 1.0, 0.5),
                                            (5, 3, 0.05, 0.01, 0.02, 0.3), (4, 3, 0.05, 2.0, 1.0, 0.99), (6, 3, 0.05, 0.0, 0.5, 0.0)]:

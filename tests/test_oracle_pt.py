@@ -121,6 +121,11 @@ def test_golden_mis_and_roulette(port):
             assert s.value == surv
 
 
+def test_golden_gaussian_filter(port):
+    for size, sigma, dx, dy, want in GOLDEN["gaussian_filter"]:
+        assert close(port.orc_pt_gaussian_weight(size, sigma, dx, dy), want, 1e-14), (size, sigma, dx, dy)
+
+
 def test_energy_tables_match_reference_within_its_noise(port):
     ess, eavg = oracle.energy_tables(port, "orc_pt_")
     ref = np.array(GOLDEN["energy_tables"]["ess"])
@@ -257,3 +262,46 @@ def test_random_roulette_and_mis(port, ref):
         assert t1 == t2 and (t1 or s1.value == s2.value)
         a, b = rng.exponential(1, 2)
         assert port.orc_pt_power_heuristic(a, b) == ref.ref_pt_power_heuristic(a, b)
+
+
+def test_random_gaussian_filter(port, ref):
+    rng = np.random.default_rng(8)
+    for _ in range(2000):
+        size, sigma = rng.uniform(0.5, 6.0), rng.uniform(0.1, 2.0)
+        dx, dy = rng.uniform(-0.6, 0.6, 2) * size
+        a = port.orc_pt_gaussian_weight(size, sigma, dx, dy)
+        b = ref.ref_pt_gaussian_weight(size, sigma, dx, dy)
+        assert close(a, b, 1e-14), (size, sigma, dx, dy, a, b)
+
+
+def _gaussian(desc, size, sigma):
+    from rise_b200 import scenes
+    desc.settings = scenes.RenderSettings(**{**desc.settings.__dict__, "filter": 1, "filter_size": size,
+                                             "filter_sigma": sigma})
+    return desc
+
+
+def test_filtered_render_crop_equals_full_image():
+    """The splatting oracle renders the samples of the pixels around a crop,
+    so a crop equals the same pixels of the full image."""
+    from rise_b200 import scenes
+    d = _gaussian(scenes.cornell_box(32, 32), 3.0, 0.8)
+    full = oracle.pt_render(d, 4)
+    crop = oracle.pt_render(d, 4, crop=(0, 8, 12, 20))
+    assert np.allclose(crop, full[8:20, 0:12], rtol=1e-12, atol=1e-300)
+    box = oracle.pt_render(scenes.cornell_box(32, 32), 4)
+    assert np.isfinite(full).all() and not np.allclose(full, box)
+
+
+def test_narrow_gaussian_warps_camera_samples():
+    """A Gaussian of half-width <= 0.501 pixel moves the camera samples (a
+    different image from the box film's) and keeps a per-pixel mean (a crop
+    equals the full image exactly)."""
+    from rise_b200 import scenes
+    d = _gaussian(scenes.cornell_box(32, 32), 1.0, 0.3)
+    full = oracle.pt_render(d, 4)
+    crop = oracle.pt_render(d, 4, crop=(4, 4, 20, 12))
+    assert np.array_equal(crop, full[4:12, 4:20])
+    box = oracle.pt_render(scenes.cornell_box(32, 32), 4)
+    assert np.isfinite(full).all() and not np.allclose(full, box)
+    assert abs(full[..., 1].mean() / box[..., 1].mean() - 1) < 0.1

@@ -54,6 +54,65 @@ def test_same_seed_matches_oracle(ctx, nee_per_lambda, layout):
     assert abs(g[..., 1].mean() / o[..., 1].mean() - 1) < 2e-3
 
 
+def filtered(desc, size=2.0, sigma=0.5):
+    desc.settings = scenes.RenderSettings(**{**desc.settings.__dict__, "filter": 1,
+                                              "filter_size": size, "filter_sigma": sigma})
+    return desc
+
+
+@pytest.mark.parametrize("size,sigma", [(2.0, 0.5), (3.0, 1.0), (1.0, 0.3)])
+def test_gaussian_filter_same_seed_matches_oracle(ctx, size, sigma):
+    """GaussianPixelFilter + FilteredFilm: every sample splats into the pixels
+    within the kernel's support; a pixel resolves to sum(w XYZ) / sum(w).  A
+    kernel of half-width <= 0.501 (size 1.0) instead moves each camera sample
+    by the truncated Gaussian and averages the pixel's own samples."""
+    d = filtered(scenes.cornell_box(64, 64), size, sigma)
+    g, _ = render_gpu(ctx, d, 16, chunks=[4, 12])
+    o = oracle.pt_render(d, 16)
+    b = oracle.pt_render(scenes.cornell_box(64, 64), 16)
+    assert np.isfinite(g).all() and (g[..., 1] > 0).mean() > 0.9
+    close = (np.abs(g - o) <= 1e-3 * (np.abs(o) + 1e-3)).all(axis=2)
+    assert close.mean() > 0.9, close.mean()
+    assert rel_mse(g, o) < 1e-3
+    assert abs(g[..., 1].mean() / o[..., 1].mean() - 1) < 2e-3
+    # The filtered film differs from the box film far more than the device
+    # differs from the oracle.
+    assert rel_mse(o, b) > 10 * rel_mse(g, o)
+
+
+def test_gaussian_filter_relmse_and_wide_sums(ctx):
+    """Four-channel films (weighted XYZ + weight): device relMSE equals the
+    host formula, and the FP64 running sum past 4096 spp matches however the
+    passes were split."""
+    d = filtered(scenes.cornell_box(16, 16))
+    ref = oracle.pt_render(d, 64)
+    films = []
+    for passes in ([64], [4096, 8], [2048, 2048, 8]):
+        r = pathtracer.SpectralRasterizer(ctx, d)
+        try:
+            for s in passes:
+                r.rasterize_scene(s)
+            f = r.film().astype(np.float64)
+            films.append(f)
+            assert abs(r.relmse(ref) / rel_mse(f, ref) - 1.0) < 1e-3
+        finally:
+            r.close()
+    assert rel_mse(films[0], ref) < 1e-3
+    assert np.allclose(films[1], films[2], rtol=2e-6, atol=1e-9)
+
+
+def test_gaussian_filter_rejects_bad_kernels(ctx):
+    d = scenes.cornell_box(16, 16)
+    scene = pathtracer.upload_scene(ctx, d)
+    try:
+        for size, sigma in [(0.0, 0.5), (17.0, 1.0), (2.0, 0.0), (-1.0, 1.0)]:
+            with pytest.raises(Exception):
+                pathtracer.SpectralRasterizer(ctx, d, scene=scene,
+                                              settings=filtered(scenes.cornell_box(16, 16), size, sigma).settings)
+    finally:
+        scene.close()
+
+
 def small_spheres(nee_per_lambda=1):
     return scenes.spheres_scene(grid=64, n_spheres=8, sphere_tris=800, width=64, height=64,
                                 nee_per_lambda=nee_per_lambda)
