@@ -156,6 +156,8 @@ typedef struct {
     int32_t filter;           /* RTB200_FILTER_* */
     float filter_size;        /* Gaussian: kernel width in pixels (support = size / 2), 0 < size <= 16 */
     float filter_sigma;       /* Gaussian: standard deviation in pixels, > 0 */
+    int32_t adaptive_max_spp; /* adaptive sampling: maximum samples per pixel (0 = off) */
+    float adaptive_threshold; /* adaptive sampling: relative standard error to converge (reference: 0.01) */
 } rtb200_render_settings;
 
 /* Pixel filters.  BOX: uniform jitter in the pixel, the pixel is the mean of
@@ -178,6 +180,7 @@ typedef struct {
     int64_t segments;         /* extended rays */
     int64_t shadow_rays;
     double seconds;           /* device time of all render calls */
+    int64_t active_pixels;    /* pixels still sampled (adaptive: not yet converged nor at the maximum) */
 } rtb200_stats;
 
 /* A job holds the path pool, queues and film of one image on the device.
@@ -188,10 +191,26 @@ typedef struct {
  * Rendering/PathTracingSpectralRasterizer.cpp:206-479).
  * rtb200_job_read_film writes width*height*3 floats: the mean XYZ per pixel
  * over all samples so far (rows top to bottom); RTB200_E_NOT_READY while a
- * request of the job is in flight on an engine. */
+ * request of the job is in flight on an engine.
+ *
+ * Adaptive sampling (adaptive_max_spp > 0; AdaptiveSamplingConfig,
+ * Utilities/AdaptiveSamplingConfig.h, and the per-pixel loop of
+ * PathTracingSpectralRasterizer.cpp:256-410): each render call is one batch
+ * of spp samples for every pixel that has not converged, capped at
+ * adaptive_max_spp samples per pixel.  After the batch, a pixel with at least
+ * 32 samples converges when the standard error of its luminance (XYZ.Y) over
+ * its mean is below adaptive_threshold * (1 - 4 / N), or, for a black pixel,
+ * when the sum of squared deviations is below 1e-12 after 64 samples.  A
+ * pixel's value is the mean of its own samples (box filter) or the splat of
+ * all samples taken (Gaussian).  rtb200_stats.active_pixels says how many
+ * pixels the next call samples; a call with none left returns RTB200_OK and
+ * renders nothing.  rtb200_job_read_sample_counts writes the samples each
+ * pixel took (width*height uint32; the reference's sample map is counts /
+ * adaptive_max_spp). */
 int rtb200_job_create(rtb200_scene* scene, const rtb200_render_settings* settings, rtb200_job** out);
 int rtb200_job_render(rtb200_job* job, int32_t spp);
 int rtb200_job_read_film(rtb200_job* job, float* xyz);
+int rtb200_job_read_sample_counts(rtb200_job* job, uint32_t* counts);
 int rtb200_job_stats(const rtb200_job* job, rtb200_stats* out);
 /* relMSE of the job's film against a reference image (width*height*3 host
  * floats, XYZ): the mean over pixels and channels of (x - r)^2 / (r^2 + 1e-2),

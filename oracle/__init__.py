@@ -164,12 +164,15 @@ def cie_table():
     return np.array([d["x"], d["y"], d["z"]], np.float64)
 
 
-def pt_render(desc, spp, sample_begin=0, crop=None, threads=None, settings=None):
+def pt_render(desc, spp, sample_begin=0, crop=None, threads=None, settings=None, return_counts=False):
     """Render a scenes.SceneDesc with the path-tracing oracle.
 
     Returns the mean XYZ of samples sample_begin .. sample_begin+spp-1 per
     pixel as float64 (h, w, 3) over `crop` = (x0, y0, x1, y1) (default: the
-    whole image)."""
+    whole image); with the Gaussian filter, the resolved splat film.  With
+    adaptive sampling (settings.adaptive_max_spp > 0) every pixel takes
+    batches of `spp` samples until it converges or reaches the maximum;
+    return_counts adds the (h, w) int32 samples per pixel."""
     lib = port()
     st = settings or desc.settings
     x0, y0, x1, y1 = crop or (0, 0, st.width, st.height)
@@ -181,23 +184,24 @@ def pt_render(desc, spp, sample_begin=0, crop=None, threads=None, settings=None)
     envi = np.array([desc.env, desc.env_visible], np.int32)
     cam = np.array(list(st.cam_pos) + list(st.cam_look) + list(st.cam_up) + [st.fov_deg], np.float64)
     setd = np.array([st.lambda_min, st.lambda_max, st.rr_threshold, getattr(st, "filter_size", 2.0),
-                     getattr(st, "filter_sigma", 0.5)], np.float64)
+                     getattr(st, "filter_sigma", 0.5), getattr(st, "adaptive_threshold", 0.01)], np.float64)
     seti = np.array([st.width, st.height, st.max_depth, st.rr_min_depth, st.nee_per_lambda, st.seed,
-                     getattr(st, "filter", 0)], np.int32)
+                     getattr(st, "filter", 0), getattr(st, "adaptive_max_spp", 0)], np.int32)
     out = np.zeros((y1 - y0, x1 - x0, 3), np.float64)
+    counts = np.zeros((y1 - y0, x1 - x0), np.int32)
     cie = np.ascontiguousarray(cie_table())
     f = lib.orc_pt_render
     f.restype = ctypes.c_int
     i32 = ctypes.c_int32
     f.argtypes = [_f32p, _i64, _vp, i32, _f32p, i32, _vp, _f32p, i32, _vp, _f64p, _f64p, _vp, i32, i32,
-                  i32, i32, i32, i32, i32, _f64p, _f64p]
+                  i32, i32, i32, i32, i32, _f64p, _f64p, _vp]
     rc = f(_p(tri9, _f32p), len(tri9), meshes.ctypes.data, len(meshes), _p(spectra, _f32p), len(spectra),
            mats_i.ctypes.data, _p(mats_f, _f32p), len(mats_i), envi.ctypes.data, _p(cam, _f64p), _p(setd, _f64p),
            seti.ctypes.data, int(spp), int(sample_begin), x0, y0, x1, y1, threads or os.cpu_count(),
-           _p(out, _f64p), _p(cie, _f64p))
+           _p(out, _f64p), _p(cie, _f64p), counts.ctypes.data)
     if rc != 0:
         raise RuntimeError("oracle path tracer rejected the scene")
-    return out
+    return (out, counts) if return_counts else out
 
 
 def ray_triangle(o, d, v0, ea, eb, kind="port"):

@@ -62,12 +62,20 @@ int  orc_ray_triangle(const double* o, const double* d, const double* v0, const 
  *   mats_i: n_mat x 5 int32 (type, reflectance, emission, eta, kappa)
  *   mats_f: n_mat x 2 float (alpha, ior)
  *   cam:    10 doubles (pos, look, up, vertical fov in degrees)
- *   setd:   5 doubles (lambda_min, lambda_max, rr_threshold, filter size, filter sigma)
- *   seti:   7 int32 (width, height, max_depth, rr_min_depth, nee_per_lambda, seed, filter)
+ *   setd:   6 doubles (lambda_min, lambda_max, rr_threshold, filter size, filter sigma,
+ *           adaptive threshold)
+ *   seti:   8 int32 (width, height, max_depth, rr_min_depth, nee_per_lambda, seed, filter,
+ *           adaptive maximum samples per pixel or 0)
  * filter 0 is the box film (mean of the pixel's own samples); filter 1 is the
  * Gaussian pixel filter: with size / 2 > 0.501 the samples of every pixel
  * within the support are splatted and a pixel is sum(w XYZ) / sum(w); a
  * narrower kernel warps each camera sample about the pixel centre instead.
+ * Adaptive sampling (seti[7] = maximum samples per pixel > 0, setd[5] = its
+ * threshold): every pixel takes batches of `spp` samples from sample 0 until
+ * its luminance estimate converges or the maximum is reached (sample_begin
+ * must be 0); a pixel is the mean of its own samples (box, warped) or the
+ * splat of every sample taken (Gaussian).  counts (nullable) receives the
+ * samples each crop pixel took.
  *   envi:   2 int32 (environment spectrum or -1, visible)
  *   cie:    3 x 81 doubles, the reference's CIE 1931 table (x, y, z bars)
  * Returns 0 on success. */
@@ -75,7 +83,8 @@ int orc_pt_render(const float* tri9, int64_t n_tri, const int64_t* meshes, int32
                   const float* spectra, int32_t n_spec, const int32_t* mats_i, const float* mats_f,
                   int32_t n_mat, const int32_t* envi, const double* cam, const double* setd,
                   const int32_t* seti, int32_t spp, int32_t sample_begin, int32_t x0, int32_t y0,
-                  int32_t x1, int32_t y1, int32_t threads, double* xyz, const double* cie);
+                  int32_t x1, int32_t y1, int32_t threads, double* xyz, const double* cie,
+                  int32_t* counts);
 
 /* Building blocks of the path-tracing oracle, exported so tests can hold each
  * against the reference's own code (oracle/_ref/libref_pt.so). */

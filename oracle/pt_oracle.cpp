@@ -681,6 +681,65 @@ void Sample(const Scene& S, uint32_t pixel, uint32_t sample, double xyz[3])
 
 }  // namespace
 
+namespace {
+
+// Adaptive sampling settings (Utilities/AdaptiveSamplingConfig.h): off when
+// max_spp is 0.
+struct Adaptive {
+    int max_spp = 0;
+    int batch = 0;
+    double threshold = 0.01;
+};
+
+// The per-pixel sample loop of PathTracingSpectralRasterizer::IntegratePixel
+// (Rendering/PathTracingSpectralRasterizer.cpp:256-410).  Without adaptive
+// sampling: spp samples from sample_begin.  With it: batches of A.batch
+// samples from sample 0, a Welford running mean / M2 of each sample's
+// luminance (XYZ.Y), and after every batch, once 32 samples are in, the
+// convergence test -- standard error / |mean| below threshold * (1 - 4 / N),
+// or M2 < 1e-12 after 64 samples for a black pixel -- until it passes or
+// A.max_spp samples are taken.  emit(sample, xyz) sees every sample; the
+// return value is the number of samples taken.
+template <class F>
+int PixelSamples(const Scene& S, uint32_t pixel, int sample_begin, int spp, const Adaptive& A, F&& emit)
+{
+    double v[3];
+    if (A.max_spp <= 0) {
+        for (int s = 0; s < spp; ++s) {
+            const uint32_t sample = (uint32_t)(sample_begin + s);
+            Sample(S, pixel, sample, v);
+            emit(sample, v);
+        }
+        return spp;
+    }
+    double mean = 0.0, m2 = 0.0;
+    unsigned n = 0;
+    int idx = 0;
+    bool converged = false;
+    while (idx < A.max_spp && !converged) {
+        const int end = std::min(idx + A.batch, A.max_spp);
+        for (; idx < end; ++idx) {
+            Sample(S, pixel, (uint32_t)idx, v);
+            emit((uint32_t)idx, v);
+            ++n;
+            const double d = v[1] - mean;
+            mean += d / (double)n;
+            m2 += d * (v[1] - mean);
+        }
+        if (n >= 32) {
+            const double se = std::sqrt(m2 / (double)(n - 1) / (double)n), ma = std::fabs(mean);
+            if (ma > 1e-12) {
+                if (se / ma < A.threshold * (1.0 - 4.0 / (double)n)) converged = true;
+            } else if (m2 < 1e-12 && n >= 64) {
+                converged = true;
+            }
+        }
+    }
+    return idx;
+}
+
+}  // namespace
+
 /* GaussianPixelFilter::EvaluateFilter (Sampling/GaussianPixelFilter.h:67-78):
  * exp(-r^2 / (2 sigma^2)) / (2 pi sigma^2) inside the size x size box centred
  * on the pixel centre, 0 outside it. */
@@ -696,7 +755,8 @@ extern "C" int orc_pt_render(const float* tri9, int64_t n_tri, const int64_t* me
                              const float* spectra, int32_t n_spec, const int32_t* mats_i, const float* mats_f,
                              int32_t n_mat, const int32_t* envi, const double* cam, const double* setd,
                              const int32_t* seti, int32_t spp, int32_t sample_begin, int32_t x0, int32_t y0,
-                             int32_t x1, int32_t y1, int32_t threads, double* xyz, const double* cie)
+                             int32_t x1, int32_t y1, int32_t threads, double* xyz, const double* cie,
+                             int32_t* counts)
 {
     (void)n_spec;
     GetTables();
@@ -778,6 +838,13 @@ extern "C" int orc_pt_render(const float* tri9, int64_t n_tri, const int64_t* me
     for (size_t i = 0; i < S.lights.size(); ++i) S.lights[i].pdf = weight[i] / wsum;
     S.bvh = orc_bvh_build(tri9, n_tri);
     const int cw = x1 - x0, ch = y1 - y0;
+    Adaptive A;
+    if (seti[7] > 0) {
+        A.max_spp = seti[7];
+        A.batch = spp;
+        A.threshold = setd[5];
+        if (sample_begin != 0 || spp <= 0) { orc_bvh_destroy(S.bvh); return 1; }
+    }
     if (seti[6] == 1 && 0.5 * setd[3] <= 0.501) {
         // Too narrow for the filtered film (PixelBasedRasterizerHelper.cpp:143-149).
         const double k = 0.5 * setd[3] / setd[4];
@@ -800,10 +867,7 @@ extern "C" int orc_pt_render(const float* tri9, int64_t n_tri, const int64_t* me
             for (int py; (py = row.fetch_add(1)) < ey1;) {
                 for (int px = ex0; px < ex1; ++px) {
                     const uint32_t pixel = (uint32_t)(py * S.width + px);
-                    for (int s = 0; s < spp; ++s) {
-                        const uint32_t sample = (uint32_t)(sample_begin + s);
-                        double v[3];
-                        Sample(S, pixel, sample, v);
+                    auto splat = [&](uint32_t sample, const double* v) {
                         const uint32_t key = PathKey(S.seed, pixel, sample);
                         const double sx = px + Rand(key, 0) - 0.5, sy = py + Rand(key, 1) - 0.5;
                         const int qx0 = std::max(x0, (int)std::floor(sx - hw));
@@ -818,7 +882,10 @@ extern "C" int orc_pt_render(const float* tri9, int64_t n_tri, const int64_t* me
                                 for (int c = 0; c < 3; ++c) f[c] += w * v[c];
                                 f[3] += w;
                             }
-                    }
+                    };
+                    const int n = PixelSamples(S, pixel, sample_begin, spp, A, splat);
+                    if (counts && px >= x0 && px < x1 && py >= y0 && py < y1)
+                        counts[(size_t)(py - y0) * cw + (px - x0)] = n;
                 }
             }
         };
@@ -842,12 +909,11 @@ extern "C" int orc_pt_render(const float* tri9, int64_t n_tri, const int64_t* me
             for (int x = 0; x < cw; ++x) {
                 const uint32_t pixel = (uint32_t)((y0 + row) * S.width + (x0 + x));
                 double acc[3] = {0, 0, 0};
-                for (int s = 0; s < spp; ++s) {
-                    double v[3];
-                    Sample(S, pixel, (uint32_t)(sample_begin + s), v);
+                const int n = PixelSamples(S, pixel, sample_begin, spp, A, [&](uint32_t, const double* v) {
                     for (int c = 0; c < 3; ++c) acc[c] += v[c];
-                }
-                for (int c = 0; c < 3; ++c) xyz[3 * ((size_t)row * cw + x) + c] = acc[c] / spp;
+                });
+                for (int c = 0; c < 3; ++c) xyz[3 * ((size_t)row * cw + x) + c] = acc[c] / n;
+                if (counts) counts[(size_t)row * cw + x] = n;
             }
         }
     };

@@ -71,6 +71,18 @@ struct rtb200_job {
     float* sum = nullptr;
     float* comp = nullptr;
     double* wide = nullptr;            // FP64 running sum once past kWideSpp samples per pixel
+    // Adaptive sampling: lists of the pixels still sampled (current and
+    // next), samples per pixel, per-pixel sums of Y and Y^2, list length.
+    bool adaptive = false;
+    void* adapt_buf = nullptr;
+    size_t adapt_bytes = 0;
+    unsigned* px_list[2] = {nullptr, nullptr};
+    unsigned* counts = nullptr;
+    double* lum = nullptr;
+    int* d_n = nullptr;
+    int cur = 0;
+    int n_active = 0;                  // pixels the next request samples
+    int submitted_px = 0;              // pixels the request in flight samples
     long long spp_done = 0;
     long long samples = 0;
     double seconds = 0.0;
@@ -241,10 +253,22 @@ int EngineSubmit(rtb200_engine* e, rtb200_job* j, int spp)
                       s->d_spectra, s->d_lights, s->d_light_tris};
     d.cam = j->cam;
     d.set = j->set;
-    d.npix = j->npix;
+    int npx = j->npix;
+    if (j->adaptive) {
+        // One batch for each pixel still sampled, capped at the maximum; a
+        // job with nothing left is submitted with no samples and is done at
+        // once.
+        spp = (int)std::max(0ll, std::min((long long)spp, (long long)j->rs.adaptive_max_spp - j->spp_done));
+        npx = spp > 0 ? j->n_active : 0;
+        if (npx == 0) spp = 0;
+    }
+    d.npix = std::max(npx, 1);
+    d.px_list = j->adaptive ? j->px_list[j->cur] : nullptr;
+    d.lum = j->adaptive ? j->lum : nullptr;
     d.film = j->pass;
     d.sample_begin = (unsigned long long)j->spp_done;
-    d.total = (unsigned long long)j->npix * (unsigned long long)spp;
+    d.total = (unsigned long long)npx * (unsigned long long)spp;
+    j->submitted_px = npx;
     d.sample_ctr = e->d_ctr + entry;
     d.done_ctr = e->d_ctr + kMaxJobs + entry;
     cudaMemsetAsync(e->d_ctr + entry, 0, 8, ctx->stream);
@@ -376,8 +400,19 @@ int EngineRetire(rtb200_engine* e, rtb200_job* j)
         err = PtFold(j->pass, j->sum, j->comp, j->film_n, ctx->num_sms, ctx->stream);
     }
     if (err != cudaSuccess) return CudaCheck(ctx, err, "film fold");
+    if (j->adaptive && j->pending_spp > 0 && j->submitted_px > 0) {
+        err = PtConverge(j->px_list[j->cur], j->submitted_px, j->lum, j->counts, (int)j->pending_spp,
+                         j->rs.adaptive_max_spp, (double)j->rs.adaptive_threshold, j->px_list[j->cur ^ 1], j->d_n,
+                         ctx->num_sms, ctx->stream);
+        int n = 0;
+        if (err == cudaSuccess) err = cudaMemcpyAsync(&n, j->d_n, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream);
+        if (err == cudaSuccess) err = cudaStreamSynchronize(ctx->stream);
+        if (err != cudaSuccess) return CudaCheck(ctx, err, "adaptive convergence");
+        j->cur ^= 1;
+        j->n_active = n;
+    }
     j->spp_done += j->pending_spp;
-    j->samples += (long long)j->npix * j->pending_spp;
+    j->samples += (long long)j->submitted_px * j->pending_spp;
     j->pending_spp = 0;
     const int entry = j->entry;
     e->active.erase(std::find(e->active.begin(), e->active.end(), entry));
@@ -453,6 +488,8 @@ int rtb200_job_create(rtb200_scene* s, const rtb200_render_settings* rs, rtb200_
         !(rs->filter == RTB200_FILTER_GAUSSIAN && rs->filter_size > 0.0f && rs->filter_size <= 16.0f &&
           rs->filter_sigma > 0.0f))
         return SetError(ctx, RTB200_E_INVALID, "bad pixel filter settings");
+    if (rs->adaptive_max_spp < 0 || (rs->adaptive_max_spp > 0 && !(rs->adaptive_threshold > 0.0f)))
+        return SetError(ctx, RTB200_E_INVALID, "bad adaptive sampling settings");
     // Camera frame (pinhole; vertical field of view).
     const float* P = rs->cam_pos;
     double f[3] = {rs->cam_look[0] - P[0], rs->cam_look[1] - P[1], rs->cam_look[2] - P[2]};
@@ -518,6 +555,38 @@ int rtb200_job_create(rtb200_scene* s, const rtb200_render_settings* rs, rtb200_
     j->pass = (float*)j->film_buf;
     j->sum = (float*)((char*)j->film_buf + plane);
     j->comp = (float*)((char*)j->film_buf + 2 * plane);
+    j->n_active = j->npix;
+    if (rs->adaptive_max_spp > 0) {
+        // Pixel lists (two), sample counts, luminance sums, list length.
+        const size_t pl = Align(4 * (size_t)j->npix), pc = Align(4 * (size_t)j->npix),
+                     ps = Align(16 * (size_t)j->npix);
+        j->adapt_bytes = 2 * pl + pc + ps + 256;
+        rc = DevAllocCached(ctx, &j->adapt_buf, j->adapt_bytes);
+        if (rc) {
+            DevFreeCached(ctx, j->film_buf, j->film_bytes);
+            delete j;
+            return rc;
+        }
+        char* b = (char*)j->adapt_buf;
+        j->px_list[0] = (unsigned*)b;
+        j->px_list[1] = (unsigned*)(b + pl);
+        j->counts = (unsigned*)(b + 2 * pl);
+        j->lum = (double*)(b + 2 * pl + pc);
+        j->d_n = (int*)(b + 2 * pl + pc + ps);
+        j->adaptive = true;
+        std::vector<unsigned> all((size_t)j->npix);
+        for (size_t i = 0; i < all.size(); ++i) all[i] = (unsigned)i;
+        cudaError_t err = cudaMemsetAsync(j->counts, 0, pc + ps, ctx->stream);
+        // From pageable memory: returns once the host buffer has been staged.
+        if (err == cudaSuccess)
+            err = cudaMemcpyAsync(j->px_list[0], all.data(), 4 * all.size(), cudaMemcpyHostToDevice, ctx->stream);
+        if (err != cudaSuccess) {
+            DevFreeCached(ctx, j->adapt_buf, j->adapt_bytes);
+            DevFreeCached(ctx, j->film_buf, j->film_bytes);
+            delete j;
+            return CudaCheck(ctx, err, "adaptive sampling set-up");
+        }
+    }
     *out = j;
     return RTB200_OK;
 }
@@ -559,7 +628,12 @@ int rtb200_job_read_film(rtb200_job* j, float* xyz)
         if (e != cudaSuccess) return CudaCheck(ctx, e, "film readback");
         for (size_t i = 0; i < n; ++i) acc[i] = (double)sum[i] - (double)comp[i];
     }
-    if (j->channels == 3) {
+    if (j->channels == 3 && j->adaptive) {
+        std::vector<unsigned> cnt((size_t)j->npix);
+        const cudaError_t e = cudaMemcpy(cnt.data(), j->counts, 4 * cnt.size(), cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess) return CudaCheck(ctx, e, "film readback");
+        for (size_t i = 0; i < n; ++i) xyz[i] = cnt[i / 3] ? (float)(acc[i] / (double)cnt[i / 3]) : 0.0f;
+    } else if (j->channels == 3) {
         const double inv = j->spp_done > 0 ? 1.0 / (double)j->spp_done : 0.0;
         for (size_t i = 0; i < n; ++i) xyz[i] = (float)(acc[i] * inv);
     } else {
@@ -590,7 +664,8 @@ int rtb200_job_relmse(rtb200_job* j, const float* ref_xyz, double* relmse)
     cudaError_t e = cudaMemcpyAsync(d_ref, ref_xyz, 4 * n3, cudaMemcpyHostToDevice, ctx->stream);
     const double inv = j->spp_done > 0 ? 1.0 / (double)j->spp_done : 0.0;
     if (e == cudaSuccess)
-        e = PtRelMse(j->sum, j->comp, j->wide, d_ref, j->npix, j->channels, inv, d_out, ctx->num_sms, ctx->stream);
+        e = PtRelMse(j->sum, j->comp, j->wide, j->adaptive ? j->counts : nullptr, d_ref, j->npix, j->channels, inv,
+                     d_out, ctx->num_sms, ctx->stream);
     if (e == cudaSuccess) e = cudaMemcpyAsync(&sum, d_out, 8, cudaMemcpyDeviceToHost, ctx->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
     DevFreeCached(ctx, buf, Align(4 * n3) + 8);
@@ -599,9 +674,25 @@ int rtb200_job_relmse(rtb200_job* j, const float* ref_xyz, double* relmse)
     return RTB200_OK;
 }
 
+int rtb200_job_read_sample_counts(rtb200_job* j, uint32_t* counts)
+{
+    if (!j || !counts) return RTB200_E_INVALID;
+    rtb200_ctx* ctx = j->scene->ctx;
+    std::lock_guard<std::mutex> g(ctx->mu);
+    if (j->engine) return SetError(ctx, RTB200_E_NOT_READY, "job has a request in flight");
+    if (!j->adaptive) {
+        std::fill(counts, counts + j->npix, (uint32_t)j->spp_done);
+        return RTB200_OK;
+    }
+    cudaSetDevice(ctx->device);
+    return CudaCheck(ctx, cudaMemcpy(counts, j->counts, 4 * (size_t)j->npix, cudaMemcpyDeviceToHost),
+                     "sample count readback");
+}
+
 int rtb200_job_stats(const rtb200_job* j, rtb200_stats* out)
 {
     if (!j || !out) return RTB200_E_INVALID;
+    out->active_pixels = j->adaptive ? (j->spp_done < j->rs.adaptive_max_spp ? j->n_active : 0) : j->npix;
     out->spp = j->spp_done;
     out->samples = j->samples;
     out->segments = j->segments;
@@ -622,6 +713,7 @@ int rtb200_job_destroy(rtb200_job* j)
     // stream finishes before any later user of the block runs.
     DevFreeCached(ctx, j->film_buf, j->film_bytes);
     if (j->wide) DevFreeCached(ctx, j->wide, 8 * (size_t)j->film_n);
+    if (j->adapt_buf) DevFreeCached(ctx, j->adapt_buf, j->adapt_bytes);
     delete j;
     return RTB200_OK;
 }

@@ -61,6 +61,12 @@ __device__ __forceinline__ void Splat(const PtPaths& P, const PtJobDev& J, int s
     }
     if (active == 0) return;
     const float s = S.ynorm / (float)active;
+    if (J.lum && Y != 0.0f) {
+        // Adaptive sampling: the pixel's luminance sums for its convergence test.
+        const double y = (double)(Y * s);
+        atomicAdd(J.lum + 2 * (size_t)m.x, y);
+        atomicAdd(J.lum + 2 * (size_t)m.x + 1, y * y);
+    }
     if (S.filter != kFilterSplat) {
         float* px = J.film + 3 * (size_t)m.x;
         if (X != 0.0f) atomicAdd(px + 0, X * s);
@@ -227,7 +233,8 @@ KRegen(const PtJobDev* __restrict__ jobs, PtPaths P, PtQueues Q, int assign)
             const PtJobDev& J = jobs[jid];
             const unsigned long long g = a.base + (unsigned long long)(i - a.off);
             {   // PinholeCamera::GenerateRay (Cameras/PinholeCamera.cpp:182-210)
-                const uint32_t pixel = (uint32_t)(g % (unsigned long long)J.npix);
+                const uint32_t slot_px = (uint32_t)(g % (unsigned long long)J.npix);
+                const uint32_t pixel = J.px_list ? __ldg(J.px_list + slot_px) : slot_px;
                 const uint32_t sample = (uint32_t)(J.sample_begin + g / (unsigned long long)J.npix);
                 const uint32_t key = PathKey(J.set.seed, pixel, sample);
                 const int px = (int)(pixel % (uint32_t)J.cam.width), py = (int)(pixel / (uint32_t)J.cam.width);
@@ -784,14 +791,16 @@ __device__ __forceinline__ double FilmValue(const float* __restrict__ sum, const
 // 1e-10) against `ref` (XYZ per pixel): sum over pixels and channels of
 // (x - r)^2 / (r^2 + 1e-2), in FP64.
 __global__ void KRelMse(const float* __restrict__ sum, const float* __restrict__ comp, const double* __restrict__ wide,
-                        const float* __restrict__ ref, int npix, int channels, double inv_spp, double* out)
+                        const unsigned* __restrict__ counts, const float* __restrict__ ref, int npix, int channels,
+                        double inv_spp, double* out)
 {
     double acc = 0.0;
     const int n3 = 3 * npix;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n3; i += gridDim.x * blockDim.x) {
         double x;
         if (channels == 3) {
-            x = FilmValue(sum, comp, wide, i) * inv_spp;
+            const unsigned c = counts ? counts[i / 3] : 1u;
+            x = c ? FilmValue(sum, comp, wide, i) * (counts ? 1.0 / (double)c : inv_spp) : 0.0;
         } else {
             const int p = i / 3;
             const double w = FilmValue(sum, comp, wide, 4 * p + 3);
@@ -808,6 +817,32 @@ __global__ void KRelMse(const float* __restrict__ sum, const float* __restrict__
         acc = threadIdx.x < (blockDim.x >> 5) ? part[threadIdx.x] : 0.0;
         for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(kFull, acc, o);
         if (threadIdx.x == 0) atomicAdd(out, acc);
+    }
+}
+
+// Adaptive sampling after a batch of `batch` samples for each listed pixel
+// (PathTracingSpectralRasterizer.cpp:379-408 with the Welford mean / M2
+// formed from the sums of Y and Y^2): adds the batch to the pixel's count,
+// tests convergence once it has 32 samples, and appends pixels still below
+// the maximum and not converged to `next`.
+__global__ void KConverge(const unsigned* __restrict__ list, int n, const double* __restrict__ lum,
+                          unsigned* __restrict__ count, int batch, int max_spp, double threshold,
+                          unsigned* __restrict__ next, int* __restrict__ n_next)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const unsigned p = list[i];
+        const unsigned c = count[p] + (unsigned)batch;
+        count[p] = c;
+        bool converged = false;
+        if (c >= 32) {
+            const double N = (double)c, s1 = lum[2 * (size_t)p], s2 = lum[2 * (size_t)p + 1];
+            const double mean = s1 / N;
+            const double m2 = fmax(s2 - s1 * mean, 0.0);
+            const double se = sqrt(m2 / (N - 1.0) / N), ma = fabs(mean);
+            if (ma > 1e-12) converged = se / ma < threshold * (1.0 - 4.0 / N);
+            else converged = m2 < 1e-12 && c >= 64;
+        }
+        if (!converged && (int)c < max_spp) next[atomicAdd(n_next, 1)] = p;
     }
 }
 
@@ -889,12 +924,22 @@ cudaError_t PtFoldWide(float* pass, float* sum, float* comp, double* wide, int n
     return cudaGetLastError();
 }
 
-cudaError_t PtRelMse(const float* sum, const float* comp, const double* wide, const float* ref, int npix,
-                     int channels, double inv_spp, double* out, int sms, cudaStream_t st)
+cudaError_t PtRelMse(const float* sum, const float* comp, const double* wide, const unsigned* counts,
+                     const float* ref, int npix, int channels, double inv_spp, double* out, int sms, cudaStream_t st)
 {
     cudaError_t e = cudaMemsetAsync(out, 0, sizeof(double), st);
     if (e != cudaSuccess) return e;
-    KRelMse<<<sms * 2, 256, 0, st>>>(sum, comp, wide, ref, npix, channels, inv_spp, out);
+    KRelMse<<<sms * 2, 256, 0, st>>>(sum, comp, wide, counts, ref, npix, channels, inv_spp, out);
+    return cudaGetLastError();
+}
+
+cudaError_t PtConverge(const unsigned* list, int n, const double* lum, unsigned* count, int batch, int max_spp,
+                       double threshold, unsigned* next, int* n_next, int sms, cudaStream_t st)
+{
+    cudaError_t e = cudaMemsetAsync(n_next, 0, sizeof(int), st);
+    if (e != cudaSuccess || n == 0) return e;
+    KConverge<<<std::min(sms * 8, (n + 255) / 256), 256, 0, st>>>(list, n, lum, count, batch, max_spp, threshold,
+                                                                  next, n_next);
     return cudaGetLastError();
 }
 

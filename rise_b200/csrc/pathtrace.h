@@ -39,9 +39,15 @@ cudaError_t PtFold(float* pass, float* sum, float* comp, int n, int sms, cudaStr
 cudaError_t PtFoldWide(float* pass, float* sum, float* comp, double* wide, int n, bool first, int sms,
                        cudaStream_t st);
 // *out = sum over pixels and XYZ channels of (x - r)^2 / (r^2 + 1e-2), x the
-// resolved film (channels 3: sum * inv_spp; 4: weighted sum / weight), r the
-// device reference; FP64 accumulation.
-cudaError_t PtRelMse(const float* sum, const float* comp, const double* wide, const float* ref, int npix,
-                     int channels, double inv_spp, double* out, int sms, cudaStream_t st);
+// resolved film (channels 3: sum * inv_spp, or sum / counts[pixel] when
+// counts is given; 4: weighted sum / weight), r the device reference; FP64
+// accumulation.
+cudaError_t PtRelMse(const float* sum, const float* comp, const double* wide, const unsigned* counts,
+                     const float* ref, int npix, int channels, double inv_spp, double* out, int sms, cudaStream_t st);
+// Adaptive sampling after a batch: count[p] += batch for the n listed pixels,
+// convergence test, and the pixels left to sample appended to next (*n_next,
+// zeroed first).
+cudaError_t PtConverge(const unsigned* list, int n, const double* lum, unsigned* count, int batch, int max_spp,
+                       double threshold, unsigned* next, int* n_next, int sms, cudaStream_t st);
 
 }  // namespace rtb200

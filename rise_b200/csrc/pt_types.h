@@ -190,9 +190,11 @@ struct PtJobDev {
     PtScene scene;
     PtCamera cam;
     PtSettings set;
-    int npix;
+    int npix;                          // pixels this request samples (adaptive: unconverged ones)
     int pad;
-    float* film;                       // 3 floats per pixel, this request's samples
+    const unsigned* px_list;           // adaptive: the pixels sampled, else null (all pixels in order)
+    double* lum;                       // adaptive: per pixel sum of Y and of Y^2 over its samples, else null
+    float* film;                       // 3 (box, warp) or 4 (splat) floats per pixel, this request's samples
     unsigned long long sample_begin;   // first sample index (per pixel) of the request
     unsigned long long total;          // npix * spp of the request
     unsigned long long* sample_ctr;    // samples handed out so far (device)

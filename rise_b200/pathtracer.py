@@ -28,12 +28,13 @@ class RenderSettings(ctypes.Structure):
                 ("fov_deg", ctypes.c_float), ("lambda_min", ctypes.c_float), ("lambda_max", ctypes.c_float),
                 ("max_depth", ctypes.c_int32), ("rr_min_depth", ctypes.c_int32), ("rr_threshold", ctypes.c_float),
                 ("nee_per_lambda", ctypes.c_int32), ("seed", ctypes.c_uint32), ("max_paths", ctypes.c_int32),
-                ("filter", ctypes.c_int32), ("filter_size", ctypes.c_float), ("filter_sigma", ctypes.c_float)]
+                ("filter", ctypes.c_int32), ("filter_size", ctypes.c_float), ("filter_sigma", ctypes.c_float),
+                ("adaptive_max_spp", ctypes.c_int32), ("adaptive_threshold", ctypes.c_float)]
 
 
 class Stats(ctypes.Structure):
     _fields_ = [("spp", ctypes.c_int64), ("samples", ctypes.c_int64), ("segments", ctypes.c_int64),
-                ("shadow_rays", ctypes.c_int64), ("seconds", ctypes.c_double)]
+                ("shadow_rays", ctypes.c_int64), ("seconds", ctypes.c_double), ("active_pixels", ctypes.c_int64)]
 
 
 def upload_scene(ctx, desc, layout="f32"):
@@ -59,7 +60,8 @@ def settings_struct(st):
     return RenderSettings(st.width, st.height, (ctypes.c_float * 3)(*st.cam_pos), (ctypes.c_float * 3)(*st.cam_look),
                           (ctypes.c_float * 3)(*st.cam_up), st.fov_deg, st.lambda_min, st.lambda_max, st.max_depth,
                           st.rr_min_depth, st.rr_threshold, st.nee_per_lambda, st.seed, st.max_paths,
-                          getattr(st, "filter", 0), getattr(st, "filter_size", 2.0), getattr(st, "filter_sigma", 0.5))
+                          getattr(st, "filter", 0), getattr(st, "filter_size", 2.0), getattr(st, "filter_sigma", 0.5),
+                          getattr(st, "adaptive_max_spp", 0), getattr(st, "adaptive_threshold", 0.01))
 
 
 class SpectralRasterizer:
@@ -102,7 +104,15 @@ class SpectralRasterizer:
         s = Stats()
         check(lib().rtb200_job_stats(self.h, ctypes.byref(s)), self.ctx.h)
         return {"spp": s.spp, "samples": s.samples, "segments": s.segments, "shadow_rays": s.shadow_rays,
-                "seconds": s.seconds}
+                "seconds": s.seconds, "active_pixels": s.active_pixels}
+
+    def sample_counts(self):
+        """Samples each pixel took, (height, width) uint32 (adaptive sampling
+        stops converged pixels early)."""
+        st = self.settings
+        out = np.empty((st.height, st.width), np.uint32)
+        check(lib().rtb200_job_read_sample_counts(self.h, ctypes.c_void_p(out.ctypes.data)), self.ctx.h)
+        return out
 
     def close(self):
         if self.h:

@@ -145,6 +145,8 @@ class RenderSettings:
     filter: int = 0           # 0 box; 1 Gaussian (GaussianPixelFilter; splatted when size / 2 > 0.501)
     filter_size: float = 2.0  # Gaussian kernel width in pixels
     filter_sigma: float = 0.5 # Gaussian standard deviation in pixels
+    adaptive_max_spp: int = 0       # adaptive sampling: maximum samples per pixel (0 = off)
+    adaptive_threshold: float = 0.01  # adaptive sampling: relative standard error to converge
 
 
 @dataclass

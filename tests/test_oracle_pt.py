@@ -305,3 +305,46 @@ def test_narrow_gaussian_warps_camera_samples():
     box = oracle.pt_render(scenes.cornell_box(32, 32), 4)
     assert np.isfinite(full).all() and not np.allclose(full, box)
     assert abs(full[..., 1].mean() / box[..., 1].mean() - 1) < 0.1
+
+
+def _adaptive(desc, max_spp, threshold):
+    from rise_b200 import scenes
+    desc.settings = scenes.RenderSettings(**{**desc.settings.__dict__, "adaptive_max_spp": max_spp,
+                                             "adaptive_threshold": threshold})
+    return desc
+
+
+def test_adaptive_sampling_follows_the_reference_rule():
+    """Each pixel's sample count equals a direct restatement of the
+    reference's loop (PathTracingSpectralRasterizer.cpp:379-408) run on the
+    pixel's own per-sample luminances, and its value is the mean of those
+    samples."""
+    from rise_b200 import scenes
+    d = _adaptive(scenes.cornell_box(24, 24), 128, 0.2)
+    img, counts = oracle.pt_render(d, 8, return_counts=True)
+    assert ((counts % 8 == 0) | (counts == 128)).all()
+    assert (counts < 128).mean() > 0.2 and (counts == 128).mean() > 0.05, np.bincount(counts.ravel())
+    plain = scenes.cornell_box(24, 24)
+    for (x, y) in [(3, 3), (12, 12), (20, 5), (5, 20), (12, 2), (23, 23)]:
+        ys, acc = [], np.zeros(3)
+        mean = m2 = 0.0
+        n = 0
+        idx = 0
+        converged = False
+        while idx < 128 and not converged:
+            for s in range(idx, min(idx + 8, 128)):
+                v = oracle.pt_render(plain, 1, sample_begin=s, crop=(x, y, x + 1, y + 1), threads=1)[0, 0]
+                acc += v
+                n += 1
+                delta = v[1] - mean
+                mean += delta / n
+                m2 += delta * (v[1] - mean)
+            idx = min(idx + 8, 128)
+            if n >= 32:
+                se = np.sqrt(m2 / (n - 1) / n)
+                if abs(mean) > 1e-12:
+                    converged = se / abs(mean) < 0.2 * (1 - 4 / n)
+                else:
+                    converged = m2 < 1e-12 and n >= 64
+        assert counts[y, x] == idx, (x, y, counts[y, x], idx)
+        assert np.allclose(img[y, x], acc / idx, rtol=1e-12, atol=1e-300)

@@ -113,6 +113,62 @@ def test_gaussian_filter_rejects_bad_kernels(ctx):
         scene.close()
 
 
+def adaptive(desc, max_spp=256, threshold=0.15):
+    desc.settings = scenes.RenderSettings(**{**desc.settings.__dict__, "adaptive_max_spp": max_spp,
+                                              "adaptive_threshold": threshold})
+    return desc
+
+
+@pytest.mark.parametrize("gaussian", [False, True])
+def test_adaptive_sampling_same_seed_matches_oracle(ctx, gaussian):
+    """Batches of 16 samples for the pixels that have not converged: the
+    device's per-pixel counts and resolved film match the oracle's."""
+    d = adaptive(scenes.cornell_box(64, 64))
+    if gaussian:
+        d = filtered(d, 2.0, 0.5)
+    r = pathtracer.SpectralRasterizer(ctx, d)
+    try:
+        active = [r.stats()["active_pixels"]]
+        for _ in range(20):
+            r.rasterize_scene(16)
+            active.append(r.stats()["active_pixels"])
+        g = r.film().astype(np.float64)
+        counts = r.sample_counts()
+        st = r.stats()
+    finally:
+        r.close()
+    o, oc = oracle.pt_render(d, 16, return_counts=True)
+    assert active[0] == 64 * 64 and active[-1] == 0 and all(a >= b for a, b in zip(active, active[1:]))
+    assert st["spp"] == 256 and st["samples"] == int(counts.sum())
+    assert (counts < 256).mean() > 0.2 and (counts == 256).mean() > 0.05
+    assert (counts == oc).mean() > 0.9, (counts == oc).mean()
+    assert abs(counts.mean() / oc.mean() - 1) < 0.02
+    assert np.isfinite(g).all()
+    assert rel_mse(g, o) < 2e-3
+    assert abs(g[..., 1].mean() / o[..., 1].mean() - 1) < 5e-3
+
+
+def test_adaptive_relmse_uses_per_pixel_counts(ctx):
+    d = adaptive(scenes.cornell_box(32, 32), 64, 0.2)
+    ref = oracle.pt_render(scenes.cornell_box(32, 32), 64)
+    r = pathtracer.SpectralRasterizer(ctx, d)
+    try:
+        for _ in range(4):
+            r.rasterize_scene(16)
+        f = r.film().astype(np.float64)
+        assert abs(r.relmse(ref) / rel_mse(f, ref) - 1.0) < 1e-3
+        c = r.sample_counts()
+        assert c.min() >= 32 and c.max() == 64
+    finally:
+        r.close()
+    plain = pathtracer.SpectralRasterizer(ctx, scenes.cornell_box(16, 16))
+    try:
+        plain.rasterize_scene(8)
+        assert (plain.sample_counts() == 8).all() and plain.stats()["active_pixels"] == 256
+    finally:
+        plain.close()
+
+
 def small_spheres(nee_per_lambda=1):
     return scenes.spheres_scene(grid=64, n_spheres=8, sphere_tris=800, width=64, height=64,
                                 nee_per_lambda=nee_per_lambda)
