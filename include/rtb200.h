@@ -211,6 +211,25 @@ int rtb200_job_create(rtb200_scene* scene, const rtb200_render_settings* setting
 int rtb200_job_render(rtb200_job* job, int32_t spp);
 int rtb200_job_read_film(rtb200_job* job, float* xyz);
 int rtb200_job_read_sample_counts(rtb200_job* job, uint32_t* counts);
+
+/* Film to colour.  rtb200_job_read_rgb writes width*height*3 floats: each
+ * pixel's XYZ (as rtb200_job_read_film returns it) converted to linear
+ * Rec.709 RGB the way the rasterizer resolves a pixel, RISEPel(XYZPel)
+ * (ColorUtils::XYZtoRec709RGB, Utilities/Color/Color.cpp:214-228, with its
+ * chromaticity gamut move, Utilities/Color/ColorUtils.cpp:232-363).
+ * rtb200_job_read_display writes width*height*3 bytes for an 8-bit image
+ * file: that RGB scaled by 2^exposure_ev, passed through the tone curve
+ * (DisplayTransformWriter::WriteColor, Rendering/DisplayTransformWriter.cpp:45-62;
+ * curves of Rendering/DisplayTransform.h:80-222), sRGB-encoded, clamped to
+ * [0, 1] and truncated to 0..255 (the PNG / PPM / TGA writers'
+ * Integerize<sRGBPel>, e.g. RasterImages/PPMWriter.cpp WriteColor). */
+#define RTB200_TONE_NONE 0      /* clip negatives and non-finite values to 0 */
+#define RTB200_TONE_REINHARD 1
+#define RTB200_TONE_ACES 2
+#define RTB200_TONE_AGX 3
+#define RTB200_TONE_HABLE 4
+int rtb200_job_read_rgb(rtb200_job* job, float* rgb);
+int rtb200_job_read_display(rtb200_job* job, float exposure_ev, int32_t tone, uint8_t* rgb8);
 int rtb200_job_stats(const rtb200_job* job, rtb200_stats* out);
 /* relMSE of the job's film against a reference image (width*height*3 host
  * floats, XYZ): the mean over pixels and channels of (x - r)^2 / (r^2 + 1e-2),

@@ -244,6 +244,34 @@ def _bind_blocks(lib, prefix):
         f.argtypes = args
 
 
+def _bind_colour(lib, prefix):
+    f = getattr(lib, prefix + "xyz_to_rec709")
+    f.restype, f.argtypes = None, [_f64p, _f64p]
+    f = getattr(lib, prefix + "display")
+    f.restype, f.argtypes = None, [_f64p, _D, ctypes.c_int, _vp]
+
+
+def xyz_to_rec709(lib, prefix, xyz):
+    """Per-pixel XYZ -> linear Rec.709 of the port ('orc_pt_') or the
+    reference ('ref_pt_') over an (..., 3) array."""
+    x = np.ascontiguousarray(xyz, np.float64).reshape(-1, 3)
+    out = np.empty_like(x)
+    f = getattr(lib, prefix + "xyz_to_rec709")
+    for i in range(len(x)):
+        f(_p(x[i], _f64p), _p(out[i], _f64p))
+    return out.reshape(np.shape(xyz))
+
+
+def display8(lib, prefix, rgb, exposure_ev=0.0, tone=0):
+    """8-bit sRGB output of linear Rec.709 pixels, (..., 3) uint8."""
+    x = np.ascontiguousarray(rgb, np.float64).reshape(-1, 3)
+    out = np.empty(x.shape, np.uint8)
+    f = getattr(lib, prefix + "display")
+    for i in range(len(x)):
+        f(_p(x[i], _f64p), float(exposure_ev), int(tone), out[i].ctypes.data)
+    return out.reshape(np.shape(rgb))
+
+
 def port_blocks():
     """liboracle.so with the path-tracer building blocks bound (orc_pt_*)."""
     lib = port()
@@ -263,6 +291,7 @@ def port_blocks():
         lib.orc_pt_tables.argtypes = [_f64p, _f64p]
         lib.orc_pt_set_tables.restype = None
         lib.orc_pt_set_tables.argtypes = [_f64p, _f64p]
+        _bind_colour(lib, "orc_pt_")
         lib._blocks_bound = True
     return lib
 
@@ -290,6 +319,7 @@ def ref_blocks():
         lib.ref_pt_russian_roulette.argtypes = [ctypes.c_uint, ctypes.c_uint, _D, _D, _D, _D, _f64p]
         lib.ref_pt_tables.restype = None
         lib.ref_pt_tables.argtypes = [_f64p, _f64p]
+        _bind_colour(lib, "ref_pt_")
         _ref_pt = lib
     return _ref_pt
 

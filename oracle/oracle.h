@@ -89,6 +89,8 @@ int orc_pt_render(const float* tri9, int64_t n_tri, const int64_t* meshes, int32
 /* Building blocks of the path-tracing oracle, exported so tests can hold each
  * against the reference's own code (oracle/_ref/libref_pt.so). */
 double orc_pt_gaussian_weight(double size, double sigma, double dx, double dy);
+void   orc_pt_xyz_to_rec709(const double* xyz, double* rgb);
+void   orc_pt_display(const double* rgb, double exposure_ev, int tone, unsigned char* out3);
 void   orc_pt_sample_wavelengths(double u, double lmin, double lmax, double* lam4);
 int    orc_pt_xyz_from_nm(double nm, const double* cie, double* xyz3);
 double orc_pt_ggx_d(double alpha, double cos_h);

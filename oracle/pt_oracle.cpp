@@ -740,6 +740,108 @@ int PixelSamples(const Scene& S, uint32_t pixel, int sample_begin, int spp, cons
 
 }  // namespace
 
+// ---- colour resolve and 8-bit output ----------------------------------------
+
+namespace {
+
+struct Chroma {
+    double x, y;
+};
+
+// Rec.709 primaries and D65 white in CIE xy (Utilities/Color/ColorUtils.cpp:135-138).
+const Chroma kRed709 = {0.640, 0.330}, kGreen709 = {0.300, 0.600}, kBlue709 = {0.150, 0.060},
+             kWhite709 = {0.3127, 0.3290};
+
+// LineIntersection2D (ColorUtils.cpp:145-177): the line a0-a1 against b0-b1,
+// refused when |denominator| < 1e-12.
+bool LinesMeet(Chroma a0, Chroma a1, Chroma b0, Chroma b1, Chroma& at)
+{
+    const double den = (b1.y - b0.y) * (a1.x - a0.x) - (b1.x - b0.x) * (a1.y - a0.y);
+    if (den > -1e-12 && den < 1e-12) return false;
+    const double ua = ((b1.x - b0.x) * (a0.y - b0.y) - (b1.y - b0.y) * (a0.x - b0.x)) / den;
+    at.x = a0.x + ua * (a1.x - a0.x);
+    at.y = a0.y + ua * (a1.y - a0.y);
+    return true;
+}
+
+// IsPointOnLineSegment (ColorUtils.cpp:204-211): the parameter along x alone.
+bool OnSegment(Chroma s0, Chroma s1, Chroma p)
+{
+    const double v = (p.x - s0.x) / (s1.x - s0.x);
+    return v >= 1e-12 && v <= 1.0 - 1e-12;
+}
+
+// ClipAgainstGamutEdge (ColorUtils.cpp:213-229).
+bool GamutEdge(Chroma c, Chroma a, Chroma b, Chroma& at)
+{
+    if (!LinesMeet(kWhite709, c, a, b, at)) return false;
+    if (!OnSegment(a, b, at)) return false;
+    if (OnSegment(kWhite709, at, c)) {
+        at = c;
+        return true;
+    }
+    return OnSegment(kWhite709, c, at);
+}
+
+double ToneCurve(int tone, double x)
+{
+    // DisplayTransforms (Rendering/DisplayTransform.h:80-222).
+    const double s = (std::isfinite(x) && x > 0.0) ? x : 0.0;
+    auto unit = [](double y) { return std::min(std::max(y, 0.0), 1.0); };
+    auto hable = [](double v) {
+        return ((v * (0.15 * v + 0.10 * 0.50) + 0.20 * 0.02) / (v * (0.15 * v + 0.50) + 0.20 * 0.30)) - 0.02 / 0.30;
+    };
+    switch (tone) {
+    case 1: return s / (1.0 + s);
+    case 2: return unit(s * (2.51 * s + 0.03) / (s * (2.43 * s + 0.59) + 0.14));
+    case 3: return unit(0.5 + 0.5 * std::tanh(1.0 * (std::log10(s + 1e-10) - 0.0)));
+    case 4: return unit(hable(s * 2.0) / hable(11.2));
+    default: return s;
+    }
+}
+
+}  // namespace
+
+/* ColorUtils::XYZtoRec709RGB (Utilities/Color/Color.cpp:214-228): gamut
+ * move of the chromaticity (MoveXYZIntoRec709RGBGamut, ColorUtils.cpp:351-363:
+ * edges red-green, red-blue, blue-green in that order; xyY round trip,
+ * Color.cpp:169-193), then the XYZ -> Rec.709 matrix (Color.cpp:22-25). */
+extern "C" void orc_pt_xyz_to_rec709(const double* xyz, double* rgb)
+{
+    double X = xyz[0], Y = xyz[1], Z = xyz[2];
+    const double inv = 1.0 / (X + Y + Z);
+    const Chroma c = {X * inv, Y * inv};
+    Chroma at;
+    if (GamutEdge(c, kRed709, kGreen709, at) || GamutEdge(c, kRed709, kBlue709, at) ||
+        GamutEdge(c, kBlue709, kGreen709, at)) {
+        const double k = 1.0 / at.y * Y;
+        X = k * at.x;
+        Z = k * (1.0 - at.x - at.y);
+    }
+    rgb[0] = 3.240479 * X + -1.537150 * Y + -0.498535 * Z;
+    rgb[1] = -0.969256 * X + 1.875992 * Y + 0.041556 * Z;
+    rgb[2] = 0.055648 * X + -0.204043 * Y + 1.057311 * Z;
+}
+
+/* One pixel of an 8-bit output: exposure 2^ev and tone curve
+ * (DisplayTransformWriter::WriteColor, Rendering/DisplayTransformWriter.cpp:45-62),
+ * sRGB transfer (ColorUtils::SRGBTransferFunction, ColorUtils.cpp:21-32),
+ * clamp to [0, 1], x 255 truncated (Color_Template.h:115-134). */
+extern "C" void orc_pt_display(const double* rgb, double exposure_ev, int tone, unsigned char* out3)
+{
+    const double mul = std::pow(2.0, exposure_ev);
+    for (int k = 0; k < 3; ++k) {
+        const double x = ToneCurve(tone, rgb[k] * mul);
+        double v;
+        if (x == 0.0) v = 0.0;
+        else if (x <= 0.003040247678) v = 12.92 * x;
+        else v = 1.055 * std::pow(x, 1.0 / 2.4) - 0.055;
+        if (v > 1.0) v = 1.0;
+        if (v < 0.0) v = 0.0;
+        out3[k] = (unsigned char)(v * 255.0);
+    }
+}
+
 /* GaussianPixelFilter::EvaluateFilter (Sampling/GaussianPixelFilter.h:67-78):
  * exp(-r^2 / (2 sigma^2)) / (2 pi sigma^2) inside the size x size box centred
  * on the pixel centre, 0 outside it. */

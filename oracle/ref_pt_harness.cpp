@@ -25,6 +25,7 @@
 #include "Interfaces/ILog.h"
 #include "Interfaces/IOptions.h"
 #include "Sampling/GaussianPixelFilter.h"
+#include "Rendering/DisplayTransform.h"
 
 namespace RISE
 {
@@ -150,6 +151,27 @@ int ref_pt_russian_roulette(unsigned depth, unsigned min_depth, double threshold
         PathTransportUtilities::EvaluateRussianRoulette(depth, min_depth, threshold, cur, prev, u);
     *survival = r.survivalProb;
     return r.terminate ? 1 : 0;
+}
+
+// Per-pixel resolve of the rasterizer: RISEPel(XYZPel), the reference's
+// XYZ -> linear Rec.709 conversion with its chromaticity gamut move.
+void ref_pt_xyz_to_rec709(const double* xyz, double* rgb)
+{
+    const Rec709RGBPel r = ColorUtils::XYZtoRec709RGB(XYZPel(xyz[0], xyz[1], xyz[2]));
+    rgb[0] = r.r; rgb[1] = r.g; rgb[2] = r.b;
+}
+
+// LDR output of one pixel: DisplayTransformWriter::WriteColor's exposure
+// scale and tone curve, then the 8-bit writers' Integerize<sRGBPel>.
+void ref_pt_display(const double* rgb, double exposure_ev, int tone, unsigned char* out3)
+{
+    const double mul = std::pow(2.0, exposure_ev);
+    RISEPel scaled;
+    scaled.r = rgb[0] * mul; scaled.g = rgb[1] * mul; scaled.b = rgb[2] * mul;
+    const RISEPel mapped = DisplayTransforms::Apply((DISPLAY_TRANSFORM)tone, scaled);
+    const RISEColor c(mapped, 1.0);
+    const RGBA8 p = c.Integerize<sRGBPel, unsigned char>(255.0);
+    out3[0] = p.r; out3[1] = p.g; out3[2] = p.b;
 }
 
 double ref_pt_gaussian_weight(double size, double sigma, double dx, double dy)

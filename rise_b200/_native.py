@@ -50,6 +50,8 @@ SIGNATURES = {
     "rtb200_job_render": (ctypes.c_int, [_vp, _i32]),
     "rtb200_job_read_film": (ctypes.c_int, [_vp, _vp]),
     "rtb200_job_read_sample_counts": (ctypes.c_int, [_vp, _vp]),
+    "rtb200_job_read_rgb": (ctypes.c_int, [_vp, _vp]),
+    "rtb200_job_read_display": (ctypes.c_int, [_vp, ctypes.c_float, ctypes.c_int32, _vp]),
     "rtb200_job_stats": (ctypes.c_int, [_vp, _vp]),
     "rtb200_job_destroy": (ctypes.c_int, [_vp]),
     "rtb200_engine_create": (ctypes.c_int, [_vp, _i32, _pvp]),

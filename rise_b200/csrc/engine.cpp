@@ -689,6 +689,44 @@ int rtb200_job_read_sample_counts(rtb200_job* j, uint32_t* counts)
                      "sample count readback");
 }
 
+namespace {
+// Resolve the film on the device into a temporary buffer and copy it out.
+int ReadColor(rtb200_job* j, double ev_mul, int tone, float* rgb, uint8_t* rgb8)
+{
+    rtb200_ctx* ctx = j->scene->ctx;
+    std::lock_guard<std::mutex> g(ctx->mu);
+    if (j->engine) return SetError(ctx, RTB200_E_NOT_READY, "job has a request in flight");
+    cudaSetDevice(ctx->device);
+    const size_t bytes = (rgb ? 12 : 3) * (size_t)j->npix;
+    void* buf = nullptr;
+    const int rc = DevAllocCached(ctx, &buf, Align(bytes));
+    if (rc) return rc;
+    const double inv = j->spp_done > 0 ? 1.0 / (double)j->spp_done : 0.0;
+    cudaError_t e = PtResolveColor(j->sum, j->comp, j->wide, j->adaptive ? j->counts : nullptr, j->channels, inv,
+                                   j->npix, ev_mul, tone, rgb ? (float*)buf : nullptr,
+                                   rgb ? nullptr : (unsigned char*)buf, ctx->num_sms, ctx->stream);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(rgb ? (void*)rgb : (void*)rgb8, buf, bytes, cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    DevFreeCached(ctx, buf, Align(bytes));
+    return CudaCheck(ctx, e, "colour resolve");
+}
+}  // namespace
+
+int rtb200_job_read_rgb(rtb200_job* j, float* rgb)
+{
+    if (!j || !rgb) return RTB200_E_INVALID;
+    return ReadColor(j, 1.0, RTB200_TONE_NONE, rgb, nullptr);
+}
+
+int rtb200_job_read_display(rtb200_job* j, float exposure_ev, int32_t tone, uint8_t* rgb8)
+{
+    if (!j || !rgb8) return RTB200_E_INVALID;
+    if (tone < RTB200_TONE_NONE || tone > RTB200_TONE_HABLE || !std::isfinite(exposure_ev))
+        return SetError(j->scene->ctx, RTB200_E_INVALID, "bad display settings");
+    return ReadColor(j, std::pow(2.0, (double)exposure_ev), tone, nullptr, rgb8);
+}
+
 int rtb200_job_stats(const rtb200_job* j, rtb200_stats* out)
 {
     if (!j || !out) return RTB200_E_INVALID;

@@ -44,6 +44,12 @@ cudaError_t PtFoldWide(float* pass, float* sum, float* comp, double* wide, int n
 // accumulation.
 cudaError_t PtRelMse(const float* sum, const float* comp, const double* wide, const unsigned* counts,
                      const float* ref, int npix, int channels, double inv_spp, double* out, int sms, cudaStream_t st);
+// Resolve the film to colour (resolve.cu): linear Rec.709 into rgb (3 floats
+// per pixel) when rgb is given, else 8-bit sRGB after exposure (ev_mul) and
+// the RTB200_TONE_* curve into rgb8.
+cudaError_t PtResolveColor(const float* sum, const float* comp, const double* wide, const unsigned* counts,
+                           int channels, double inv_spp, int npix, double ev_mul, int tone, float* rgb,
+                           unsigned char* rgb8, int sms, cudaStream_t st);
 // Adaptive sampling after a batch: count[p] += batch for the n listed pixels,
 // convergence test, and the pixels left to sample appended to next (*n_next,
 // zeroed first).

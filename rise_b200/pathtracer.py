@@ -56,6 +56,20 @@ def upload_scene(ctx, desc, layout="f32"):
     return s
 
 
+# Tone curves of rtb200_job_read_display (RTB200_TONE_*).
+TONE_NONE, TONE_REINHARD, TONE_ACES, TONE_AGX, TONE_HABLE = range(5)
+
+
+def write_ppm(path, rgb8):
+    """Write an (height, width, 3) uint8 image as binary PPM (P6), rows top
+    to bottom, as the reference's PPM writer lays it out."""
+    rgb8 = np.ascontiguousarray(rgb8, np.uint8)
+    h, w = rgb8.shape[:2]
+    with open(path, "wb") as f:
+        f.write(b"P6\n%d %d\n255\n" % (w, h))
+        f.write(rgb8.tobytes())
+
+
 def settings_struct(st):
     return RenderSettings(st.width, st.height, (ctypes.c_float * 3)(*st.cam_pos), (ctypes.c_float * 3)(*st.cam_look),
                           (ctypes.c_float * 3)(*st.cam_up), st.fov_deg, st.lambda_min, st.lambda_max, st.max_depth,
@@ -105,6 +119,23 @@ class SpectralRasterizer:
         check(lib().rtb200_job_stats(self.h, ctypes.byref(s)), self.ctx.h)
         return {"spp": s.spp, "samples": s.samples, "segments": s.segments, "shadow_rays": s.shadow_rays,
                 "seconds": s.seconds, "active_pixels": s.active_pixels}
+
+    def rgb(self):
+        """Linear Rec.709 RGB per pixel (the rasterizer's resolve of each
+        pixel's XYZ), (height, width, 3) float32."""
+        st = self.settings
+        out = np.empty((st.height, st.width, 3), np.float32)
+        check(lib().rtb200_job_read_rgb(self.h, ctypes.c_void_p(out.ctypes.data)), self.ctx.h)
+        return out
+
+    def display(self, exposure_ev=0.0, tone=TONE_NONE):
+        """8-bit sRGB image for LDR files: exposure 2^ev, tone curve, sRGB
+        encode, clamp, truncate; (height, width, 3) uint8."""
+        st = self.settings
+        out = np.empty((st.height, st.width, 3), np.uint8)
+        check(lib().rtb200_job_read_display(self.h, float(exposure_ev), int(tone),
+                                            ctypes.c_void_p(out.ctypes.data)), self.ctx.h)
+        return out
 
     def sample_counts(self):
         """Samples each pixel took, (height, width) uint32 (adaptive sampling

@@ -120,6 +120,25 @@ def main():
     out["fresnel_avg"] = [[ni, nt, k, r.ref_pt_fresnel_avg(ni, nt, k)] for ni, nt, k in [(1, 0.2, 3.0), (1, 1.5, 0.0), (1, 2.9, 3.1)]]
     out["fms"] = [[f, e, r.ref_pt_fms(f, e)] for f, e in [(0.9, 0.6), (0.3, 0.99), (1.0, 0.3)]]
     out["power_heuristic"] = [[a, b, r.ref_pt_power_heuristic(a, b)] for a, b in [(1, 1), (0.2, 5), (3, 0.01)]]
+    cases = [[0.3, 0.5, 0.1], [0.9505, 1.0, 1.089], [0.0, 0.0, 0.0], [0.6, 0.05, 0.02], [0.05, 0.6, 0.01],
+             [0.1, 0.02, 0.9], [0.25, 0.1, 0.5], [1e-9, 2e-9, 3e-9], [2.5, 3.0, 0.2], [0.4, 0.4, -0.05]]
+    cases += rng.exponential(0.5, (30, 3)).tolist()
+    rows = []
+    for xyz in cases:
+        rgb, p = vec(np.zeros(3))
+        _, px = vec(xyz)
+        r.ref_pt_xyz_to_rec709(px, p)
+        rows.append([xyz, rgb.tolist()])
+    out["xyz_to_rec709"] = rows
+    rows = []
+    for xyz, rgb in out["xyz_to_rec709"]:
+        for tone in range(5):
+            for ev in (0.0, 1.0, -1.5):
+                o = (ctypes.c_ubyte * 3)()
+                _, pr = vec(rgb)
+                r.ref_pt_display(pr, ev, tone, o)
+                rows.append([rgb, ev, tone, list(o)])
+    out["display"] = rows
     out["gaussian_filter"] = [[s, g, dx, dy, r.ref_pt_gaussian_weight(s, g, dx, dy)]
                               for s, g in [(2.0, 0.5), (3.0, 1.0), (1.0, 0.3)]
                               for dx, dy in [(0, 0), (0.3, -0.2), (0.99, 0.5), (1.0, 0.0), (-1.01, 0.1), (1.4, 1.4)]]

@@ -121,6 +121,17 @@ def test_golden_mis_and_roulette(port):
             assert s.value == surv
 
 
+def test_golden_colour_resolve_and_display(port):
+    """XYZ -> linear Rec.709 with the gamut move, and the 8-bit encode with
+    exposure and each tone curve: bit-exact against the reference."""
+    for xyz, want in GOLDEN["xyz_to_rec709"]:
+        got = oracle.xyz_to_rec709(port, "orc_pt_", np.array(xyz))
+        assert np.array_equal(got, np.array(want)), (xyz, got, want)
+    for rgb, ev, tone, want in GOLDEN["display"]:
+        got = oracle.display8(port, "orc_pt_", np.array(rgb), ev, tone)
+        assert got.tolist() == want, (rgb, ev, tone, got, want)
+
+
 def test_golden_gaussian_filter(port):
     for size, sigma, dx, dy, want in GOLDEN["gaussian_filter"]:
         assert close(port.orc_pt_gaussian_weight(size, sigma, dx, dy), want, 1e-14), (size, sigma, dx, dy)
@@ -348,3 +359,19 @@ def test_adaptive_sampling_follows_the_reference_rule():
                     converged = m2 < 1e-12 and n >= 64
         assert counts[y, x] == idx, (x, y, counts[y, x], idx)
         assert np.allclose(img[y, x], acc / idx, rtol=1e-12, atol=1e-300)
+
+
+def test_random_colour_resolve_and_display(port, ref):
+    rng = np.random.default_rng(9)
+    x = np.concatenate([rng.exponential(1.0, (4000, 3)),
+                        rng.exponential(1.0, (1000, 1)) * np.array([[1.0, 0.02, 0.01]]),
+                        rng.exponential(1.0, (1000, 1)) * np.array([[0.01, 1.0, 0.03]]),
+                        rng.exponential(1.0, (1000, 1)) * np.array([[0.2, 0.05, 1.0]]),
+                        rng.normal(size=(500, 3)), np.zeros((2, 3))])
+    a = oracle.xyz_to_rec709(port, "orc_pt_", x)
+    b = oracle.xyz_to_rec709(ref, "ref_pt_", x)
+    assert np.array_equal(a, b, equal_nan=True)
+    for tone in range(5):
+        ev = float(rng.uniform(-3, 3))
+        assert np.array_equal(oracle.display8(port, "orc_pt_", b[:2000], ev, tone),
+                              oracle.display8(ref, "ref_pt_", b[:2000], ev, tone)), tone
