@@ -99,6 +99,37 @@ int rtb200_scene_add_mesh(rtb200_scene* scene, const float* xyz, int64_t n_verts
  * RTB200_E_INVALID, where the reference's unbounded stack
  * (Acceleration/BVH.h:1311-1320) would go on. */
 int rtb200_scene_commit(rtb200_scene* scene, int32_t layout);
+/* ---- .risemesh files ---------------------------------------------------- */
+
+/* A parsed .risemesh (the reference's mesh file, versions 1 to 5:
+ * TriangleMeshGeometryIndexed::Serialize / Deserialize,
+ * Geometry/TriangleMeshGeometryIndexed.cpp:585-980), with the BVH2 cache its
+ * v3+ files may carry (BVH::Serialize / Deserialize, Acceleration/BVH.h:338-423).
+ * rtb200_risemesh_parse reads a file's bytes; RTB200_E_INVALID for a
+ * malformed or truncated file, an index out of range, a cache whose leaf
+ * order does not list every triangle, or a v1..v3 file that carries a legacy
+ * BSP / octree block.  rtb200_risemesh_info: any output may
+ * be NULL; n_bvh_nodes is 0 without a cache.
+ *
+ * rtb200_scene_add_risemesh adds the mesh's triangles (vertex positions
+ * rounded to FP32; its own double-sided flag).  With use_cached_bvh and a
+ * cache in the file, the cache is checked (child pairs after their parent
+ * and in range, each node reached once, leaf ranges inside the leaf order,
+ * depth <= 1024, ordered boxes; RTB200_E_INVALID otherwise) and the scene's
+ * commit skips the SAH build of this mesh: a scene with a cached mesh is
+ * built in two levels, a top level over the meshes' root boxes and below it
+ * each mesh's own BVH2 (the cache, or the reference build of that mesh
+ * alone), then collapsed to four-wide nodes as the reference's loader does
+ * (BVH.h:414-418).  A scene of one cached mesh traverses the file's node
+ * layout unchanged. */
+typedef struct rtb200_risemesh rtb200_risemesh;
+int rtb200_risemesh_parse(const void* bytes, size_t n_bytes, rtb200_risemesh** out);
+int rtb200_risemesh_info(const rtb200_risemesh* mesh, int32_t* version, int64_t* n_points, int64_t* n_tri,
+                         int32_t* double_sided, int64_t* n_bvh_nodes);
+int rtb200_risemesh_destroy(rtb200_risemesh* mesh);
+int rtb200_scene_add_risemesh(rtb200_scene* scene, const rtb200_risemesh* mesh, int32_t material,
+                              int32_t use_cached_bvh);
+
 /* Node / triangle counts and device bytes of a committed scene. */
 int rtb200_scene_info(const rtb200_scene* scene, int64_t* n_tri, int64_t* n_nodes,
                       int64_t* device_bytes, double* build_seconds);
@@ -289,6 +320,10 @@ int rtb200_bvh_host_info(const rtb200_bvh_host* h, int64_t* n_nodes2, int64_t* n
  * prims: n_tri uint32; nodes4: 128 * n_nodes4 bytes. */
 int rtb200_bvh_host_export(const rtb200_bvh_host* h, void* nodes2, uint32_t* prims, void* nodes4);
 int rtb200_bvh_host_destroy(rtb200_bvh_host* h);
+/* The same for a .risemesh: its cached BVH2 as the scene commit would adopt
+ * it (checked, then collapsed), or the reference build of its triangles when
+ * the file has no cache or use_cached_bvh is 0. */
+int rtb200_bvh_host_from_risemesh(const rtb200_risemesh* mesh, int32_t use_cached_bvh, rtb200_bvh_host** out);
 
 /* ---- batched ray casting ----------------------------------------------- */
 

@@ -38,6 +38,11 @@ SIGNATURES = {
     "rtb200_bvh_host_info": (ctypes.c_int, [_vp, _pi64, _pi64]),
     "rtb200_bvh_host_export": (ctypes.c_int, [_vp, _vp, _vp, _vp]),
     "rtb200_bvh_host_destroy": (ctypes.c_int, [_vp]),
+    "rtb200_bvh_host_from_risemesh": (ctypes.c_int, [_vp, ctypes.c_int32, _vp]),
+    "rtb200_risemesh_parse": (ctypes.c_int, [_vp, ctypes.c_size_t, _vp]),
+    "rtb200_risemesh_info": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _vp]),
+    "rtb200_risemesh_destroy": (ctypes.c_int, [_vp]),
+    "rtb200_scene_add_risemesh": (ctypes.c_int, [_vp, _vp, ctypes.c_int32, ctypes.c_int32]),
     "rtb200_cast_closest": (ctypes.c_int, [_vp, _vp, _i64, _vp]),
     "rtb200_cast_any": (ctypes.c_int, [_vp, _vp, _i64, _vp]),
     "rtb200_cast_closest_device": (ctypes.c_int, [_vp, _vp, _i64, _vp, _vp]),

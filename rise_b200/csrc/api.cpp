@@ -290,6 +290,54 @@ int rtb200_scene_add_mesh(rtb200_scene* s, const float* xyz, int64_t n_verts, co
     return RTB200_OK;
 }
 
+int rtb200_scene_add_risemesh(rtb200_scene* s, const rtb200_risemesh* m, int32_t material, int32_t use_cached_bvh)
+{
+    if (!s || !m) return RTB200_E_INVALID;
+    std::vector<float> xyz;
+    std::vector<uint32_t> tri;
+    RisemeshTriangles(m, xyz, tri);
+    const std::vector<uint32_t>* prims = nullptr;
+    const std::vector<Node2>* nodes = use_cached_bvh ? RisemeshBvh(m, &prims) : nullptr;
+    if (nodes && !ValidBVH2(*nodes, prims->size()))
+        return SetError(s->ctx, RTB200_E_INVALID, "the mesh's cached BVH is malformed");
+    const int rc = rtb200_scene_add_mesh(s, xyz.data(), (int64_t)(xyz.size() / 3), tri.data(),
+                                         (int64_t)(tri.size() / 3), material, RisemeshDoubleSided(m) ? 1 : 0);
+    if (rc || !nodes || tri.empty()) return rc;
+    std::lock_guard<std::mutex> g(s->ctx->mu);
+    rtb200_scene::Mesh& mesh = s->meshes.back();
+    mesh.cached = true;
+    mesh.cache_nodes = *nodes;
+    mesh.cache_prims = *prims;
+    return RTB200_OK;
+}
+
+namespace {
+// The scene BVH: one reference build over all triangles, or, when a mesh
+// brings its own BVH2, the two-level merge of per-mesh trees.
+void BuildSceneBVH(rtb200_scene* s)
+{
+    bool any = false;
+    for (const auto& m : s->meshes) any = any || m.cached;
+    if (!any) {
+        BuildReferenceBVH(s->tri9.data(), (int64_t)s->tri_material.size(), 0, s->bvh);
+        return;
+    }
+    std::vector<BuiltBVH> own(s->meshes.size());
+    std::vector<MeshBVH2> parts;
+    for (size_t i = 0; i < s->meshes.size(); ++i) {
+        const auto& m = s->meshes[i];
+        if (m.count == 0) continue;
+        if (m.cached) {
+            parts.push_back({&m.cache_nodes, &m.cache_prims, m.first});
+        } else {
+            BuildReferenceBVH(s->tri9.data() + 9 * m.first, m.count, 0, own[i]);
+            parts.push_back({&own[i].nodes2, &own[i].prims, m.first});
+        }
+    }
+    MergeMeshBVHs(parts, s->bvh);
+}
+}  // namespace
+
 int rtb200_scene_commit(rtb200_scene* s, int32_t layout)
 {
     if (!s) return RTB200_E_INVALID;
@@ -301,7 +349,7 @@ int rtb200_scene_commit(rtb200_scene* s, int32_t layout)
     if (n_tri == 0) return SetError(ctx, RTB200_E_INVALID, "scene has no triangles");
     cudaSetDevice(ctx->device);
     const auto t0 = std::chrono::steady_clock::now();
-    BuildReferenceBVH(s->tri9.data(), n_tri, 0, s->bvh);
+    BuildSceneBVH(s);
     s->stack_bound = TraceStackBound(s->bvh);
     if (s->stack_bound > kTraceStackMax)
         return SetError(ctx, RTB200_E_INVALID, "BVH deeper than the traversal stack (" +
@@ -392,6 +440,28 @@ int rtb200_bvh_host_build(const float* tri9, int64_t n_tri, int32_t threads, rtb
     rtb200_bvh_host* h = new (std::nothrow) rtb200_bvh_host();
     if (!h) return RTB200_E_OOM;
     BuildReferenceBVH(tri9, n_tri, threads, h->b);
+    *out = h;
+    return RTB200_OK;
+}
+
+int rtb200_bvh_host_from_risemesh(const rtb200_risemesh* m, int32_t use_cached_bvh, rtb200_bvh_host** out)
+{
+    if (!m || !out) return RTB200_E_INVALID;
+    std::vector<float> xyz;
+    std::vector<uint32_t> tri;
+    RisemeshTriangles(m, xyz, tri);
+    const std::vector<uint32_t>* prims = nullptr;
+    const std::vector<Node2>* nodes = use_cached_bvh ? RisemeshBvh(m, &prims) : nullptr;
+    if (nodes && !ValidBVH2(*nodes, prims->size())) return RTB200_E_INVALID;
+    rtb200_bvh_host* h = new (std::nothrow) rtb200_bvh_host();
+    if (!h) return RTB200_E_OOM;
+    if (nodes) {
+        MergeMeshBVHs({MeshBVH2{nodes, prims, 0}}, h->b);
+    } else {
+        std::vector<float> tri9(9 * (tri.size() / 3));
+        for (size_t i = 0; i < tri.size(); ++i) std::memcpy(&tri9[3 * i], &xyz[3 * (size_t)tri[i]], 12);
+        BuildReferenceBVH(tri9.data(), (int64_t)(tri.size() / 3), 0, h->b);
+    }
     *out = h;
     return RTB200_OK;
 }

@@ -394,6 +394,110 @@ void BuildReferenceBVH(const float* tri9, int64_t n_tri, int threads, BuiltBVH& 
     Collapse(out.nodes2, out.nodes4);
 }
 
+bool ValidBVH2(const std::vector<Node2>& n2, size_t n_prims)
+{
+    if (n2.empty()) return false;
+    std::vector<uint8_t> seen(n2.size(), 0);
+    std::vector<std::pair<uint32_t, int>> stack = {{0u, 0}};
+    seen[0] = 1;
+    while (!stack.empty()) {
+        const uint32_t i = stack.back().first;
+        const int depth = stack.back().second;
+        stack.pop_back();
+        const Node2& n = n2[i];
+        for (int k = 0; k < 3; ++k)
+            if (!(n.bmin[k] <= n.bmax[k])) return false;   // inverted or NaN box
+        if (n.count > 0) {
+            if ((uint64_t)n.first_or_left + n.count > n_prims) return false;
+            continue;
+        }
+        const uint64_t l = n.first_or_left;
+        if (l <= i || l + 1 >= n2.size() || depth + 1 > kMaxBVH2Depth) return false;
+        for (uint64_t c = l; c <= l + 1; ++c) {
+            if (seen[c]) return false;
+            seen[c] = 1;
+            stack.push_back({(uint32_t)c, depth + 1});
+        }
+    }
+    return true;
+}
+
+void MergeMeshBVHs(const std::vector<MeshBVH2>& meshes, BuiltBVH& out)
+{
+    out.nodes2.clear();
+    out.prims.clear();
+    out.nodes4.clear();
+    if (meshes.empty()) return;
+    std::vector<int64_t> base(meshes.size());   // leaf-order offset of each mesh
+    for (size_t m = 0; m < meshes.size(); ++m) {
+        base[m] = (int64_t)out.prims.size();
+        for (uint32_t p : *meshes[m].prims) out.prims.push_back((uint32_t)(meshes[m].first + p));
+    }
+    // Copy mesh m's subtree rooted at `src` into slot `dst`, children pairs
+    // appended depth first.
+    std::function<void(size_t, uint32_t, uint32_t)> copy = [&](size_t m, uint32_t src, uint32_t dst) {
+        Node2 n = (*meshes[m].nodes2)[src];
+        if (n.count > 0) {
+            n.first_or_left = (uint32_t)(n.first_or_left + base[m]);
+            out.nodes2[dst] = n;
+            return;
+        }
+        const uint32_t l = (uint32_t)out.nodes2.size();
+        out.nodes2.resize(out.nodes2.size() + 2);
+        const uint32_t sl = n.first_or_left;
+        n.first_or_left = l;
+        out.nodes2[dst] = n;
+        copy(m, sl, l);
+        copy(m, sl + 1, l + 1);
+    };
+    std::vector<uint32_t> order(meshes.size());
+    for (size_t m = 0; m < meshes.size(); ++m) order[m] = (uint32_t)m;
+    auto root_of = [&](uint32_t m) -> const Node2& { return (*meshes[m].nodes2)[0]; };
+    // Top level over meshes order[lo, hi) into slot dst.
+    std::function<void(size_t, size_t, uint32_t)> top = [&](size_t lo, size_t hi, uint32_t dst) {
+        if (hi - lo == 1) {
+            copy(order[lo], 0, dst);
+            return;
+        }
+        Node2 n{};
+        float clo[3] = {INFINITY, INFINITY, INFINITY}, chi[3] = {-INFINITY, -INFINITY, -INFINITY};
+        for (int k = 0; k < 3; ++k) { n.bmin[k] = INFINITY; n.bmax[k] = -INFINITY; }
+        for (size_t i = lo; i < hi; ++i) {
+            const Node2& r = root_of(order[i]);
+            for (int k = 0; k < 3; ++k) {
+                n.bmin[k] = std::min(n.bmin[k], r.bmin[k]);
+                n.bmax[k] = std::max(n.bmax[k], r.bmax[k]);
+                const float c = 0.5f * (r.bmin[k] + r.bmax[k]);
+                clo[k] = std::min(clo[k], c);
+                chi[k] = std::max(chi[k], c);
+            }
+        }
+        int axis = 0;
+        for (int k = 1; k < 3; ++k)
+            if (chi[k] - clo[k] > chi[axis] - clo[axis]) axis = k;
+        const size_t mid = lo + (hi - lo) / 2;
+        std::nth_element(order.begin() + lo, order.begin() + mid, order.begin() + hi, [&](uint32_t a, uint32_t b) {
+            const float ca = root_of(a).bmin[axis] + root_of(a).bmax[axis];
+            const float cb = root_of(b).bmin[axis] + root_of(b).bmax[axis];
+            return ca < cb || (ca == cb && a < b);
+        });
+        const uint32_t l = (uint32_t)out.nodes2.size();
+        out.nodes2.resize(out.nodes2.size() + 2);
+        n.first_or_left = l;
+        n.count = 0;
+        n.axis = (uint8_t)axis;
+        out.nodes2[dst] = n;
+        top(lo, mid, l);
+        top(mid, hi, l + 1);
+    };
+    size_t total = 1;
+    for (const MeshBVH2& m : meshes) total += m.nodes2->size() + 1;
+    out.nodes2.reserve(total);
+    out.nodes2.emplace_back();
+    top(0, meshes.size(), 0);
+    Collapse(out.nodes2, out.nodes4);
+}
+
 std::vector<int32_t> BreadthFirstPositions(const BuiltBVH& b)
 {
     const size_t n = b.nodes4.size();

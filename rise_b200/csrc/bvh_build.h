@@ -49,6 +49,29 @@ struct BuiltBVH {
 // host cores.
 void BuildReferenceBVH(const float* tri9, int64_t n_tri, int threads, BuiltBVH& out);
 
+// A BVH2 read from a file (the reference's .risemesh cache): valid when every
+// internal node's child pair lies after it and inside the array, every node
+// is reached once from the root, leaf ranges lie inside the n_prims leaf-order
+// entries, and no path is deeper than kMaxBVH2Depth.
+constexpr int kMaxBVH2Depth = 1024;
+bool ValidBVH2(const std::vector<Node2>& nodes2, size_t n_prims);
+
+// One mesh's BVH2 (prims: mesh-local triangle indices in leaf order) and the
+// scene-wide index of its first triangle.
+struct MeshBVH2 {
+    const std::vector<Node2>* nodes2;
+    const std::vector<uint32_t>* prims;
+    int64_t first;
+};
+
+// Scene BVH over meshes with their own BVH2s (two levels, as the reference
+// keeps one BVH per mesh): a binary top level over the meshes' root boxes,
+// split at the median mesh centre along the widest axis, with each mesh's tree
+// copied below it in depth-first pair order and its leaf ranges moved to the
+// mesh's place in the scene-wide leaf order; then the BVH4 collapse.  One mesh
+// alone keeps its node array as it is.
+void MergeMeshBVHs(const std::vector<MeshBVH2>& meshes, BuiltBVH& out);
+
 // ---- device layouts -------------------------------------------------------
 
 // FP32 wide node: 4 child boxes as SoA float4 + child links, 128 bytes.

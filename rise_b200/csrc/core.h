@@ -41,6 +41,10 @@ struct rtb200_scene {
         int64_t first, count;
         int32_t material;
         int32_t double_sided;
+        // BVH2 read with the mesh (a .risemesh cache): mesh-local leaf order
+        bool cached = false;
+        std::vector<rtb200::Node2> cache_nodes;
+        std::vector<uint32_t> cache_prims;
     };
     std::vector<Mesh> meshes;
     // spectral shading data
@@ -90,6 +94,11 @@ int DevAllocCached(rtb200_ctx* ctx, void** p, size_t bytes);
 void DevFreeCached(rtb200_ctx* ctx, void* p, size_t bytes);
 void DevReleaseCache(rtb200_ctx* ctx);
 int SetError(rtb200_ctx* ctx, int code, const std::string& msg);
+// .risemesh accessors (risemesh.cpp).
+bool RisemeshTriangles(const rtb200_risemesh* m, std::vector<float>& xyz, std::vector<uint32_t>& tri);
+const std::vector<rtb200::Node2>* RisemeshBvh(const rtb200_risemesh* m, const std::vector<uint32_t>** prims);
+bool RisemeshDoubleSided(const rtb200_risemesh* m);
+
 int CudaCheck(rtb200_ctx* ctx, cudaError_t e, const char* what);
 
 // Shading tables of a committed scene (pt_api.cpp): per-triangle attributes

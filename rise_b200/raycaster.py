@@ -79,6 +79,12 @@ class Scene:
         idx = np.arange(3 * len(tri9), dtype=np.uint32).reshape(-1, 3)
         self.add_mesh(tri9.reshape(-1, 3), idx, material, double_sided)
 
+    def add_risemesh(self, mesh, material=0, use_cached_bvh=True):
+        """Add a parsed RiseMesh; its BVH2 cache (if any) replaces the SAH
+        build of this mesh when use_cached_bvh."""
+        check(lib().rtb200_scene_add_risemesh(self.h, mesh.h, int(material), int(bool(use_cached_bvh))), self.ctx.h)
+        self.n_tri += mesh.info()["n_tri"]
+
     def commit(self, layout="f32"):
         check(lib().rtb200_scene_commit(self.h, LAYOUTS[layout]), self.ctx.h)
         self.layout = layout
@@ -129,18 +135,58 @@ class RayCaster:
               self.scene.ctx.h)
 
 
-def build_host_bvh(tri9, threads=0):
-    """Build the reference BVH on the host: (nodes2, prims, nodes4) arrays."""
-    tri9 = np.ascontiguousarray(tri9, np.float32).reshape(-1, 9)
-    h = ctypes.c_void_p()
-    check(lib().rtb200_bvh_host_build(_ptr(tri9), len(tri9), threads, ctypes.byref(h)))
+class RiseMesh:
+    """A parsed .risemesh file (the reference's mesh format, v1..v5, with its
+    optional BVH2 cache)."""
+
+    def __init__(self, data):
+        data = bytes(data)
+        buf = ctypes.create_string_buffer(data, len(data))
+        h = ctypes.c_void_p()
+        check(lib().rtb200_risemesh_parse(buf, len(data), ctypes.byref(h)))
+        self.h = h
+
+    @classmethod
+    def from_file(cls, path):
+        with open(path, "rb") as f:
+            return cls(f.read())
+
+    def info(self):
+        v, ds = ctypes.c_int32(), ctypes.c_int32()
+        npt, ntri, nn = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int64()
+        check(lib().rtb200_risemesh_info(self.h, ctypes.byref(v), ctypes.byref(npt), ctypes.byref(ntri),
+                                         ctypes.byref(ds), ctypes.byref(nn)))
+        return {"version": v.value, "n_points": npt.value, "n_tri": ntri.value, "double_sided": bool(ds.value),
+                "n_bvh_nodes": nn.value}
+
+    def host_bvh(self, use_cached_bvh=True):
+        """(nodes2, prims, nodes4) as a scene commit would use them."""
+        h = ctypes.c_void_p()
+        check(lib().rtb200_bvh_host_from_risemesh(self.h, int(bool(use_cached_bvh)), ctypes.byref(h)))
+        return _export_host_bvh(h, self.info()["n_tri"])
+
+    def close(self):
+        if self.h:
+            lib().rtb200_risemesh_destroy(self.h)
+            self.h = None
+
+
+def _export_host_bvh(h, n_tri):
     try:
         n2, n4 = ctypes.c_int64(), ctypes.c_int64()
         check(lib().rtb200_bvh_host_info(h, ctypes.byref(n2), ctypes.byref(n4)))
         nodes2 = np.zeros(n2.value, NODE2_DTYPE)
-        prims = np.zeros(len(tri9), np.uint32)
+        prims = np.zeros(n_tri, np.uint32)
         nodes4 = np.zeros(n4.value, NODE4_DTYPE)
         check(lib().rtb200_bvh_host_export(h, _ptr(nodes2), _ptr(prims), _ptr(nodes4)))
         return nodes2, prims, nodes4
     finally:
         lib().rtb200_bvh_host_destroy(h)
+
+
+def build_host_bvh(tri9, threads=0):
+    """Build the reference BVH on the host: (nodes2, prims, nodes4) arrays."""
+    tri9 = np.ascontiguousarray(tri9, np.float32).reshape(-1, 9)
+    h = ctypes.c_void_p()
+    check(lib().rtb200_bvh_host_build(_ptr(tri9), len(tri9), threads, ctypes.byref(h)))
+    return _export_host_bvh(h, len(tri9))

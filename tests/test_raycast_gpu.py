@@ -164,3 +164,62 @@ def test_full_size_microbench_sample(ctx, layout):
     rep = closest_report(tri, rays[idx], hits[idx], ids, t)
     assert rep["bad"] == [] and rep["t_over"] == 0, {k: rep[k] for k in ("bad", "t_over", "max_ulp")}
     s.close()
+
+
+@pytest.mark.parametrize("layout", LAYOUTS)
+def test_risemesh_cache_traversal_matches_reference(ctx, layout):
+    """A scene of one .risemesh whose BVH2 cache is the reference's own tree
+    over the golden soup traverses that tree: the reference's hits."""
+    from risemesh_io import risemesh_bytes, soup_mesh
+    g = np.load(os.path.join(GOLDEN, "bvh_soup_2k.npz"))
+    pts, tris = soup_mesh(g["tri9"])
+    m = raycaster.RiseMesh(risemesh_bytes(pts, tris, nodes2=g["nodes2"], prims=g["prims"]))
+    s = raycaster.Scene(ctx)
+    try:
+        s.add_risemesh(m)
+        s.commit(layout)
+        rc = raycaster.RayCaster(s)
+        hits = rc.cast_rays(g["rays"])
+        rep = closest_report(g["tri9"], g["rays"], hits, g["ids"], g["t"])
+        assert rep["bad"] == [] and rep["t_over"] == 0, rep
+        occ = rc.cast_shadow_rays(g["shadow_rays"])
+        assert any_report(g["tri9"], g["shadow_rays"], occ, g["occluded"])["bad"] == []
+    finally:
+        s.close()
+        m.close()
+
+
+@pytest.mark.parametrize("layout", LAYOUTS)
+def test_two_level_scene_with_cached_and_built_meshes(ctx, layout):
+    """Cached meshes beside plain ones: the scene is a top level over per-mesh
+    trees; hits equal the oracle's over all triangles."""
+    from risemesh_io import risemesh_bytes, soup_mesh
+    parts = [scenes.soup_triangles(3000, seed=41), scenes.soup_triangles(2000, seed=42) + np.float32(0.4),
+             scenes.soup_triangles(1000, seed=43) - np.float32(0.3)]
+    s = raycaster.Scene(ctx)
+    meshes = []
+    try:
+        for k, tri in enumerate(parts):
+            if k == 1:
+                s.add_triangles(tri)           # built with the reference SAH at commit
+                continue
+            n2, prims, _ = raycaster.build_host_bvh(tri)
+            pts, tris = soup_mesh(tri)
+            m = raycaster.RiseMesh(risemesh_bytes(pts, tris, nodes2=n2, prims=prims))
+            meshes.append(m)
+            s.add_risemesh(m)
+        s.commit(layout)
+        allt = np.concatenate(parts)
+        rays = scenes.sphere_rays(50000, seed=44)
+        srays = scenes.sphere_rays(50000, seed=45, shadow=True)
+        rc = raycaster.RayCaster(s)
+        ob = oracle.BVH(allt, "port")
+        ids, t = ob.closest(rays)
+        rep = closest_report(allt, rays, rc.cast_rays(rays), ids, t)
+        assert rep["bad"] == [] and rep["t_over"] == 0, {k: rep[k] for k in ("bad", "t_over", "max_ulp")}
+        assert len(rep["excluded"]) <= 50
+        assert any_report(allt, srays, rc.cast_shadow_rays(srays), ob.any(srays))["bad"] == []
+    finally:
+        s.close()
+        for m in meshes:
+            m.close()
