@@ -163,6 +163,14 @@ typedef struct {
  * emits becomes one luminary (area light) at commit. */
 int rtb200_scene_add_spectrum(rtb200_scene* scene, const float* values, int32_t* id_out);
 int rtb200_scene_add_material(rtb200_scene* scene, const rtb200_material* m, int32_t* id_out);
+/* A binned spectrum as the reference's spectral painters hold it
+ * (SpectralPacket, Utilities/Color/SpectralPacket.h:80-100,285-297; made by
+ * Job::AddSpectralColorPainter, Job.cpp:1557-1582): n amplitudes over
+ * [lambda_begin, lambda_end]; the value at nm is the amplitude of the bin
+ * holding it, 0 outside the range.  Shares the id space of
+ * rtb200_scene_add_spectrum. */
+int rtb200_scene_add_spectral_packet(rtb200_scene* scene, float lambda_begin, float lambda_end, int32_t n,
+                                     const float* amplitudes, int32_t* id_out);
 /* Uniform sky: radiance spectrum for rays that escape (-1 = none); visible
  * selects whether camera rays see it directly. */
 int rtb200_scene_set_environment(rtb200_scene* scene, int32_t spectrum, int32_t visible);

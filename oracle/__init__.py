@@ -164,6 +164,28 @@ def cie_table():
     return np.array([d["x"], d["y"], d["z"]], np.float64)
 
 
+def spectrum_table(spectra):
+    """The spectrum table the oracle reads (the device's layout): a header of
+    4 floats per id -- {0, 380, 780, offset} for 81 grid samples, {n, begin,
+    end, offset} for a binned packet (an object with .begin, .end, .amps) --
+    then the samples; offset is the samples' float index stored as int32
+    bits."""
+    head = np.zeros((len(spectra), 4), np.float32)
+    data = []
+    off = 4 * len(spectra)
+    for i, sp in enumerate(spectra):
+        if hasattr(sp, "amps"):
+            vals = np.asarray(sp.amps, np.float32)
+            head[i, :3] = (len(vals), sp.begin, sp.end)
+        else:
+            vals = np.asarray(sp, np.float32).reshape(81)
+            head[i, :3] = (0.0, 380.0, 780.0)
+        head[i, 3] = np.array([off], np.int32).view(np.float32)[0]
+        data.append(vals)
+        off += len(vals)
+    return np.ascontiguousarray(np.concatenate([head.ravel()] + data).astype(np.float32))
+
+
 def pt_render(desc, spp, sample_begin=0, crop=None, threads=None, settings=None, return_counts=False):
     """Render a scenes.SceneDesc with the path-tracing oracle.
 
@@ -178,7 +200,7 @@ def pt_render(desc, spp, sample_begin=0, crop=None, threads=None, settings=None,
     x0, y0, x1, y1 = crop or (0, 0, st.width, st.height)
     tri9 = np.ascontiguousarray(desc.tri9, np.float32)
     meshes = np.array(desc.meshes, np.int64).reshape(-1, 4)
-    spectra = np.ascontiguousarray(np.array(desc.spectra, np.float32).reshape(-1, 81))
+    spectra = spectrum_table(desc.spectra)
     mats_i = np.array([[m.type, m.reflectance, m.emission, m.eta, m.kappa] for m in desc.materials], np.int32)
     mats_f = np.array([[m.alpha, m.ior] for m in desc.materials], np.float32)
     envi = np.array([desc.env, desc.env_visible], np.int32)
@@ -195,7 +217,7 @@ def pt_render(desc, spp, sample_begin=0, crop=None, threads=None, settings=None,
     i32 = ctypes.c_int32
     f.argtypes = [_f32p, _i64, _vp, i32, _f32p, i32, _vp, _f32p, i32, _vp, _f64p, _f64p, _vp, i32, i32,
                   i32, i32, i32, i32, i32, _f64p, _f64p, _vp]
-    rc = f(_p(tri9, _f32p), len(tri9), meshes.ctypes.data, len(meshes), _p(spectra, _f32p), len(spectra),
+    rc = f(_p(tri9, _f32p), len(tri9), meshes.ctypes.data, len(meshes), _p(spectra, _f32p), len(desc.spectra),
            mats_i.ctypes.data, _p(mats_f, _f32p), len(mats_i), envi.ctypes.data, _p(cam, _f64p), _p(setd, _f64p),
            seti.ctypes.data, int(spp), int(sample_begin), x0, y0, x1, y1, threads or os.cpu_count(),
            _p(out, _f64p), _p(cie, _f64p), counts.ctypes.data)
@@ -249,6 +271,9 @@ def _bind_colour(lib, prefix):
     f.restype, f.argtypes = None, [_f64p, _f64p]
     f = getattr(lib, prefix + "display")
     f.restype, f.argtypes = None, [_f64p, _D, ctypes.c_int, _vp]
+    if prefix == "ref_pt_":
+        f = lib.ref_pt_spectral_packet
+        f.restype, f.argtypes = None, [_f64p, _f64p, ctypes.c_int, _D, _D, _f64p, ctypes.c_int, _f64p]
 
 
 def xyz_to_rec709(lib, prefix, xyz):

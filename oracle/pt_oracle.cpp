@@ -28,6 +28,7 @@
 #include <algorithm>
 #include <atomic>
 #include <cmath>
+#include <cstring>
 #include <mutex>
 #include <thread>
 #include <vector>
@@ -357,13 +358,45 @@ inline bool Interp(double nm, int& i, int& j, double& w)
     w = x - i;
     return true;
 }
+// Spectrum table: per id a header of 4 floats, {0, 380, 780, offset} for 81
+// samples on the 5 nm grid (linear between them), {n, begin, end, offset}
+// for a binned packet (SpectralPacket::ValueAtNM,
+// Utilities/Color/SpectralPacket.h:285-297: the amplitude of bin
+// int((nm - begin) / delta), delta = (end - begin) / n, 0 outside; nm == end
+// reads the last bin); offset is the samples' float index (bits).
+struct SpecHeader {
+    double n, begin, end;
+    const float* s;
+};
+inline SpecHeader Header(const float* table, int id)
+{
+    const float* h = table + 4 * (size_t)id;
+    int32_t off;
+    std::memcpy(&off, h + 3, 4);
+    return {h[0], h[1], h[2], table + off};
+}
 inline double Spec(const Scene& S, int id, double nm)
 {
-    int i, j;
-    double w;
-    if (id < 0 || !Interp(nm, i, j, w)) return 0.0;
-    const float* s = S.spectra + 81 * (size_t)id;
-    return (double)s[i] + w * ((double)s[j] - (double)s[i]);
+    if (id < 0) return 0.0;
+    const SpecHeader h = Header(S.spectra, id);
+    if (h.n == 0.0) {
+        int i, j;
+        double w;
+        if (!Interp(nm, i, j, w)) return 0.0;
+        return (double)h.s[i] + w * ((double)h.s[j] - (double)h.s[i]);
+    }
+    if (nm < h.begin || nm > h.end) return 0.0;
+    const double delta = (h.end - h.begin) / h.n;
+    return (double)h.s[std::min((int)((nm - h.begin) / delta), (int)h.n - 1)];
+}
+// The spectrum at grid point k (380 + 5k nm) as the scene upload tabulates it.
+inline double GridValue(const float* table, int id, int k)
+{
+    const SpecHeader h = Header(table, id);
+    if (h.n == 0.0) return h.s[k];
+    const double nm = 380.0 + 5.0 * k;
+    if (nm < h.begin || nm > h.end) return 0.0;
+    return h.s[std::min((int)((nm - h.begin) * h.n / (h.end - h.begin)), (int)h.n - 1)];
 }
 inline double PowerHeuristic(double a, double b) { return a * a / (a * a + b * b); }
 
@@ -929,7 +962,7 @@ extern "C" int orc_pt_render(const float* tri9, int64_t n_tri, const int64_t* me
         S.ltris[lg.first + cum.size() - 1].cdf = 1.0;
         lg.area = area;
         double mean = 0.0;
-        for (int k = 0; k < 81; ++k) mean += spectra[81 * (size_t)emit + k];
+        for (int k = 0; k < 81; ++k) mean += GridValue(spectra, emit, k);
         mean /= 81.0;
         weight.push_back(area * std::max(mean, 1e-12));
         S.meshLight[m] = (int)S.lights.size();

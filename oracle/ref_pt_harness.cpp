@@ -26,6 +26,9 @@
 #include "Interfaces/IOptions.h"
 #include "Sampling/GaussianPixelFilter.h"
 #include "Rendering/DisplayTransform.h"
+#include "Interfaces/IFunction2D.h"
+#include "Utilities/PiecewiseLinearFunction.h"
+#include "Utilities/Color/SpectralPacket.h"
 
 namespace RISE
 {
@@ -172,6 +175,21 @@ void ref_pt_display(const double* rgb, double exposure_ev, int tone, unsigned ch
     const RISEColor c(mapped, 1.0);
     const RGBA8 p = c.Integerize<sRGBPel, unsigned char>(255.0);
     out3[0] = p.r; out3[1] = p.g; out3[2] = p.b;
+}
+
+// A spectral painter's spectrum as Job::AddSpectralColorPainter builds it
+// (piecewise-linear control points sampled into a SpectralPacket of n bins),
+// read back at the query wavelengths with SpectralPacket::ValueAtNM.  Query
+// wavelengths must lie below the packet's end (ValueAtNM reads one past its
+// bins there).
+void ref_pt_spectral_packet(const double* nm, const double* amp, int n, double begin, double end,
+                            const double* query, int nq, double* out)
+{
+    Implementation::PiecewiseLinearFunction1D* f = new Implementation::PiecewiseLinearFunction1D();
+    for (int i = 0; i < n; ++i) f->addControlPoint(std::make_pair(nm[i], amp[i]));
+    const SpectralPacket packet(begin, end, (unsigned)n, f);
+    for (int i = 0; i < nq; ++i) out[i] = packet.ValueAtNM(query[i]);
+    f->release();
 }
 
 double ref_pt_gaussian_weight(double size, double sigma, double dx, double dy)

@@ -48,7 +48,16 @@ struct rtb200_scene {
     };
     std::vector<Mesh> meshes;
     // spectral shading data
-    std::vector<float> spectra;                 // 81 samples per spectrum
+    std::vector<float> spectra;                 // 81 samples per spectrum (5 nm grid)
+    // Binned packets (SpectralPacket): spectrum id -> begin, end, amplitudes;
+    // `spectra` holds their values at the grid points for host-side use.
+    struct Packet {
+        int32_t id;
+        float begin, end;
+        std::vector<float> amps;
+    };
+    std::vector<Packet> packets;
+    size_t spectra_table_bytes = 0;
     std::vector<rtb200::PtMaterial> materials;
     bool mixed_shading = false;      // materials of more than one shading class
     int32_t env = -1, env_visible = 1;

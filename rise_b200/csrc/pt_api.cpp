@@ -119,7 +119,33 @@ int UploadShading(rtb200_scene* s)
     size_t total = 0;
     int rc = Upload(ctx, &s->d_attr, attr, total);
     if (!rc) rc = Upload(ctx, &s->d_mats, s->materials, total);
-    if (!rc) rc = Upload(ctx, &s->d_spectra, s->spectra, total);
+    // Spectrum table (Spec, pt_device.cuh): headers, then samples.
+    std::vector<float> table;
+    {
+        const size_t nspec = s->spectra.size() / RTB200_CIE_COUNT;
+        std::vector<const rtb200_scene::Packet*> packet(nspec, nullptr);
+        for (const auto& p : s->packets) packet[p.id] = &p;
+        table.resize(4 * nspec);
+        for (size_t id = 0; id < nspec; ++id) {
+            const int32_t off = (int32_t)table.size();
+            float* h = &table[4 * id];
+            if (packet[id]) {
+                h[0] = (float)packet[id]->amps.size();
+                h[1] = packet[id]->begin;
+                h[2] = packet[id]->end;
+                table.insert(table.end(), packet[id]->amps.begin(), packet[id]->amps.end());
+            } else {
+                h[0] = 0.0f;
+                h[1] = 380.0f;
+                h[2] = 780.0f;
+                table.insert(table.end(), s->spectra.begin() + id * RTB200_CIE_COUNT,
+                             s->spectra.begin() + (id + 1) * RTB200_CIE_COUNT);
+            }
+            std::memcpy(&table[4 * id + 3], &off, 4);
+        }
+    }
+    s->spectra_table_bytes = table.size() * sizeof(float);
+    if (!rc) rc = Upload(ctx, &s->d_spectra, table, total);
     if (!rc) rc = Upload(ctx, &s->d_lights, s->lights, total);
     if (!rc) rc = Upload(ctx, &s->d_light_tris, s->light_tris, total);
     s->shade_bytes = total;
@@ -132,7 +158,7 @@ void FreeShading(rtb200_scene* s)
     rtb200_ctx* ctx = s->ctx;
     DevFree(ctx, s->d_attr, s->tri_material.size() * sizeof(PtTriAttr));
     DevFree(ctx, s->d_mats, s->materials.size() * sizeof(PtMaterial));
-    DevFree(ctx, s->d_spectra, s->spectra.size() * sizeof(float));
+    DevFree(ctx, s->d_spectra, s->spectra_table_bytes);
     DevFree(ctx, s->d_lights, s->lights.size() * sizeof(PtLight));
     DevFree(ctx, s->d_light_tris, s->light_tris.size() * sizeof(PtLightTri));
     s->d_attr = nullptr;
@@ -159,6 +185,37 @@ int rtb200_scene_add_spectrum(rtb200_scene* s, const float* values, int32_t* id_
             return SetError(s->ctx, RTB200_E_INVALID, "spectrum values must be finite and non-negative");
     *id_out = (int32_t)(s->spectra.size() / RTB200_CIE_COUNT);
     s->spectra.insert(s->spectra.end(), values, values + RTB200_CIE_COUNT);
+    return RTB200_OK;
+}
+
+int rtb200_scene_add_spectral_packet(rtb200_scene* s, float lambda_begin, float lambda_end, int32_t n,
+                                     const float* amplitudes, int32_t* id_out)
+{
+    if (!s || !amplitudes || !id_out) return RTB200_E_INVALID;
+    std::lock_guard<std::mutex> g(s->ctx->mu);
+    if (s->committed) return SetError(s->ctx, RTB200_E_INVALID, "scene already committed");
+    if (n < 1 || n > (1 << 20) || !std::isfinite(lambda_begin) || !std::isfinite(lambda_end) ||
+        !(lambda_end > lambda_begin))
+        return SetError(s->ctx, RTB200_E_INVALID, "bad spectral packet range");
+    for (int32_t k = 0; k < n; ++k)
+        if (!std::isfinite(amplitudes[k]) || amplitudes[k] < 0.0f)
+            return SetError(s->ctx, RTB200_E_INVALID, "spectrum values must be finite and non-negative");
+    rtb200_scene::Packet p;
+    p.id = (int32_t)(s->spectra.size() / RTB200_CIE_COUNT);
+    p.begin = lambda_begin;
+    p.end = lambda_end;
+    p.amps.assign(amplitudes, amplitudes + n);
+    // Grid samples for the host's uses (conductor Fresnel averages, light
+    // selection weights), the packet's own value at each grid wavelength.
+    for (int k = 0; k < RTB200_CIE_COUNT; ++k) {
+        const double nm = 380.0 + 5.0 * k;
+        float v = 0.0f;
+        if (nm >= lambda_begin && nm <= lambda_end)
+            v = p.amps[std::min((int)((nm - lambda_begin) * n / ((double)lambda_end - lambda_begin)), n - 1)];
+        s->spectra.push_back(v);
+    }
+    *id_out = p.id;
+    s->packets.push_back(std::move(p));
     return RTB200_OK;
 }
 

@@ -48,17 +48,29 @@ __device__ __forceinline__ uint32_t Dim(int depth, int j) { return 8u + 32u * (u
 
 // ---- spectra -----------------------------------------------------------------
 
-// Linear interpolation on the 5 nm grid (InterpSPDIndices,
-// src/Library/Utilities/Color/ColorUtils.cpp:270-300); 0 outside 380..780 nm.
-__device__ __forceinline__ float Spec(const float* spectra, int id, float nm)
+// Spectrum table: one float4 header per spectrum id, then the samples.
+// Header {0, 380, 780, offset}: 81 samples on the 5 nm grid, linear between
+// them (InterpSPDIndices, src/Library/Utilities/Color/ColorUtils.cpp:270-300),
+// 0 outside 380..780 nm.  Header {n, begin, end, offset}: a binned packet of
+// n amplitudes over [begin, end], the bin holding nm returned as is, 0
+// outside (SpectralPacket::ValueAtNM, Utilities/Color/SpectralPacket.h:285-297;
+// nm == end reads the last bin).  offset is the samples' float index (bits).
+__device__ __forceinline__ float Spec(const float* table, int id, float nm)
 {
-    if (id < 0 || !(nm >= 380.0f) || nm > 780.0f) return 0.0f;
-    const float x = (nm - 380.0f) * 0.2f;
-    const int i = (int)floorf(x);
-    const int j = i + 1 > 80 ? 80 : i + 1;
-    const float w = x - (float)i;
-    const float* s = spectra + id * RTB200_CIE_COUNT;
-    return s[i] + w * (s[j] - s[i]);
+    if (id < 0) return 0.0f;
+    const float4 h = __ldg(reinterpret_cast<const float4*>(table) + id);
+    const float* s = table + __float_as_int(h.w);
+    if (!(nm >= h.y) || nm > h.z) return 0.0f;
+    if (h.x == 0.0f) {
+        const float x = (nm - 380.0f) * 0.2f;
+        const int i = (int)floorf(x);
+        const int j = i + 1 > 80 ? 80 : i + 1;
+        const float w = x - (float)i;
+        return __ldg(s + i) + w * (__ldg(s + j) - __ldg(s + i));
+    }
+    const int n = (int)h.x;
+    const int i = min((int)((nm - h.y) * h.x / (h.z - h.y)), n - 1);
+    return __ldg(s + i);
 }
 
 // ColorUtils::XYZFromNM (ColorUtils.cpp:313-325).

@@ -132,7 +132,7 @@ struct PtScene {
     int ntri;
     const PtTriAttr* attr;
     const PtMaterial* mats;
-    const float* spectra;      // n_spectra x 81 samples, 380..780 nm at 5 nm
+    const float* spectra;      // spectrum table: float4 header per id, then samples (Spec)
     const PtLight* lights;
     const PtLightTri* light_tris;
 };

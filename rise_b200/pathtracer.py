@@ -42,9 +42,14 @@ def upload_scene(ctx, desc, layout="f32"):
     s = Scene(ctx)
     L = lib()
     for sp in desc.spectra:
-        sp = np.ascontiguousarray(sp, np.float32)
         out = ctypes.c_int32()
-        check(L.rtb200_scene_add_spectrum(s.h, ctypes.c_void_p(sp.ctypes.data), ctypes.byref(out)), ctx.h)
+        if hasattr(sp, "amps"):
+            a = np.ascontiguousarray(sp.amps, np.float32)
+            check(L.rtb200_scene_add_spectral_packet(s.h, float(sp.begin), float(sp.end), len(a),
+                                                     ctypes.c_void_p(a.ctypes.data), ctypes.byref(out)), ctx.h)
+        else:
+            sp = np.ascontiguousarray(sp, np.float32)
+            check(L.rtb200_scene_add_spectrum(s.h, ctypes.c_void_p(sp.ctypes.data), ctypes.byref(out)), ctx.h)
     for m in desc.materials:
         cm = Material(m.type, m.reflectance, m.emission, m.eta, m.kappa, m.alpha, m.ior)
         out = ctypes.c_int32()

@@ -127,6 +127,61 @@ class Material:
 
 
 @dataclass
+class SpectralPacket:
+    """A binned spectrum (the reference's SpectralPacket): len(amps) bins over
+    [begin, end]; the value at nm is the amplitude of the bin holding it, 0
+    outside the range."""
+    begin: float
+    end: float
+    amps: np.ndarray
+
+    def value_at(self, nm):
+        nm = np.asarray(nm, np.float64)
+        n = len(self.amps)
+        delta = (float(self.end) - float(self.begin)) / n
+        idx = np.minimum(((nm - self.begin) / delta).astype(np.int64), n - 1)
+        inside = (nm >= self.begin) & (nm <= self.end)
+        return np.where(inside, np.asarray(self.amps, np.float64)[np.clip(idx, 0, n - 1)], 0.0)
+
+
+def spectral_painter(nm, amplitudes, nmbegin=400.0, nmend=700.0):
+    """The spectrum of the reference's spectral_painter chunk
+    (Job::AddSpectralColorPainter, Job.cpp:1557-1582): the control points
+    (nm, amplitude) define a piecewise-linear function, constant beyond the
+    first and last points (PiecewiseLinearFunction1D,
+    Utilities/PiecewiseLinearFunction.h:60-90); it is sampled at
+    nmbegin + i * (nmend - nmbegin) / n for the n = len(nm) bins of a
+    SpectralPacket (SpectralPacket.h:80-100).  The chunk's `scale` scales
+    only the painter's RGB colour, not its spectrum, so it has no argument
+    here."""
+    x = np.asarray(nm, np.float64)
+    y = np.asarray(amplitudes, np.float64)
+    order = np.argsort(x, kind="stable")
+    x, y = x[order], y[order]
+    n = len(x)
+    delta = (float(nmend) - float(nmbegin)) / n
+    amps = np.empty(n)
+    for i in range(n):
+        s = nmbegin + i * delta
+        if n < 2:
+            amps[i] = 1.0
+        elif s <= x[0]:
+            amps[i] = y[0]
+        elif s >= x[-1]:
+            amps[i] = y[-1]
+        else:
+            k = int(np.searchsorted(x, s, side="left"))
+            if x[k] == s:
+                amps[i] = y[k]
+            elif x[k - 1] == s:
+                amps[i] = y[k - 1]
+            else:
+                d = (s - x[k - 1]) / (x[k] - x[k - 1])
+                amps[i] = d * (y[k] - y[k - 1]) + y[k - 1]
+    return SpectralPacket(float(nmbegin), float(nmend), amps.astype(np.float32))
+
+
+@dataclass
 class RenderSettings:
     width: int = 256
     height: int = 256
@@ -153,7 +208,7 @@ class RenderSettings:
 class SceneDesc:
     tri9: np.ndarray = None
     meshes: list = field(default_factory=list)     # (first, count, material, double_sided)
-    spectra: list = field(default_factory=list)    # 81 floats each
+    spectra: list = field(default_factory=list)    # 81 floats each, or a SpectralPacket
     materials: list = field(default_factory=list)  # Material
     env: int = -1
     env_visible: int = 1
@@ -161,7 +216,7 @@ class SceneDesc:
     _tris: list = field(default_factory=list)
 
     def add_spectrum(self, s):
-        self.spectra.append(np.asarray(s, np.float32).reshape(81))
+        self.spectra.append(s if isinstance(s, SpectralPacket) else np.asarray(s, np.float32).reshape(81))
         return len(self.spectra) - 1
 
     def add_material(self, m):

@@ -139,6 +139,19 @@ def main():
                 r.ref_pt_display(pr, ev, tone, o)
                 rows.append([rgb, ev, tone, list(o)])
     out["display"] = rows
+    rows = []
+    for nm, amp, lo, hi in [([400, 450, 500, 600, 700], [0.1, 0.5, 0.2, 0.9, 0.3], 400, 700),
+                            ([380, 420, 430, 700, 780], [1.0, 0.0, 2.0, 0.5, 0.25], 390, 710),
+                            ([550], [0.7], 400, 700), ([700, 400, 550], [3.0, 1.0, 2.0], 380, 780),
+                            (list(np.arange(400, 701, 4.0)), list(rng.random(76)), 400, 700)]:
+        q = np.concatenate([np.linspace(lo - 10, hi - 1e-6, 41), [lo, lo + 1e-9]])
+        o, po = vec(np.zeros(len(q)))
+        _, pn = vec(nm)
+        _, pa = vec(amp)
+        _, pq = vec(q)
+        r.ref_pt_spectral_packet(pn, pa, len(nm), float(lo), float(hi), pq, len(q), po)
+        rows.append([list(map(float, nm)), list(map(float, amp)), lo, hi, q.tolist(), o.tolist()])
+    out["spectral_packet"] = rows
     out["gaussian_filter"] = [[s, g, dx, dy, r.ref_pt_gaussian_weight(s, g, dx, dy)]
                               for s, g in [(2.0, 0.5), (3.0, 1.0), (1.0, 0.3)]
                               for dx, dy in [(0, 0), (0.3, -0.2), (0.99, 0.5), (1.0, 0.0), (-1.01, 0.1), (1.4, 1.4)]]

@@ -375,3 +375,34 @@ def test_random_colour_resolve_and_display(port, ref):
         ev = float(rng.uniform(-3, 3))
         assert np.array_equal(oracle.display8(port, "orc_pt_", b[:2000], ev, tone),
                               oracle.display8(ref, "ref_pt_", b[:2000], ev, tone)), tone
+
+
+def test_golden_spectral_painter_packets():
+    """spectral_painter's binned spectrum (piecewise-linear control points
+    sampled into n bins, step lookup, 0 outside) against the reference's
+    PiecewiseLinearFunction1D + SpectralPacket; amplitudes are stored as
+    FP32."""
+    from rise_b200 import scenes
+    for nm, amp, lo, hi, q, want in GOLDEN["spectral_packet"]:
+        got = scenes.spectral_painter(nm, amp, lo, hi).value_at(np.array(q))
+        assert np.allclose(got, want, rtol=1e-7, atol=0), (nm, lo, hi)
+
+
+def test_random_spectral_painter_packets(ref):
+    from rise_b200 import scenes
+    rng = np.random.default_rng(10)
+    for _ in range(200):
+        n = int(rng.integers(1, 40))
+        nm = rng.uniform(360, 800, n)
+        amp = rng.exponential(1.0, n)
+        lo = float(rng.uniform(360, 500))
+        hi = float(lo + rng.uniform(50, 400))
+        q = np.concatenate([rng.uniform(lo - 20, hi, 200), [lo]])
+        q = q[q < hi]
+        want = np.zeros(len(q))
+        ref.ref_pt_spectral_packet(nm.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                                   amp.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), n, lo, hi,
+                                   q.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), len(q),
+                                   want.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
+        got = scenes.spectral_painter(nm, amp, lo, hi).value_at(q)
+        assert np.allclose(got, want, rtol=1e-7, atol=0)

@@ -206,6 +206,23 @@ def test_colour_resolve_matches_oracle(ctx, kind, tmp_path):
         r.close()
 
 
+def test_binned_spectral_packets_match_oracle(ctx):
+    """Spectra given as the reference's binned packets (spectral_painter:
+    73 control points on the 5 nm grid from 395 nm, 73 bins over 395..715 nm,
+    zero outside) render as the oracle's with the same packets."""
+    d = scenes.cornell_box(48, 48)
+    grid = np.arange(380.0, 781.0, 5.0)
+    d.spectra = [scenes.spectral_painter(grid[3:76], np.asarray(s, np.float64)[3:76], 395.0, 715.0)
+                 for s in d.spectra]
+    g, _ = render_gpu(ctx, d, 16)
+    o = oracle.pt_render(d, 16)
+    close = (np.abs(g - o) <= 1e-3 * (np.abs(o) + 1e-3)).all(axis=2)
+    assert close.mean() > 0.97, close.mean()
+    assert rel_mse(g, o) < 1e-3
+    b = oracle.pt_render(scenes.cornell_box(48, 48), 16)
+    assert rel_mse(o, b) > 1e-4          # the packets' steps and range change the image
+
+
 def small_spheres(nee_per_lambda=1):
     return scenes.spheres_scene(grid=64, n_spheres=8, sphere_tris=800, width=64, height=64,
                                 nee_per_lambda=nee_per_lambda)
