@@ -126,6 +126,8 @@ typedef struct rtb200_risemesh rtb200_risemesh;
 int rtb200_risemesh_parse(const void* bytes, size_t n_bytes, rtb200_risemesh** out);
 int rtb200_risemesh_info(const rtb200_risemesh* mesh, int32_t* version, int64_t* n_points, int64_t* n_tri,
                          int32_t* double_sided, int64_t* n_bvh_nodes);
+/* The mesh's triangles as 9 floats each (v0, v1, v2), FP32-rounded. */
+int rtb200_risemesh_triangles(const rtb200_risemesh* mesh, float* tri9);
 int rtb200_risemesh_destroy(rtb200_risemesh* mesh);
 int rtb200_scene_add_risemesh(rtb200_scene* scene, const rtb200_risemesh* mesh, int32_t material,
                               int32_t use_cached_bvh);

@@ -42,6 +42,7 @@ SIGNATURES = {
     "rtb200_risemesh_parse": (ctypes.c_int, [_vp, ctypes.c_size_t, _vp]),
     "rtb200_risemesh_info": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _vp]),
     "rtb200_risemesh_destroy": (ctypes.c_int, [_vp]),
+    "rtb200_risemesh_triangles": (ctypes.c_int, [_vp, _vp]),
     "rtb200_scene_add_risemesh": (ctypes.c_int, [_vp, _vp, ctypes.c_int32, ctypes.c_int32]),
     "rtb200_scene_add_spectral_packet": (ctypes.c_int, [_vp, ctypes.c_float, ctypes.c_float, ctypes.c_int32, _vp,
                                                         _vp]),

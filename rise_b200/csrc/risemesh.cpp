@@ -173,6 +173,14 @@ int rtb200_risemesh_info(const rtb200_risemesh* m, int32_t* version, int64_t* n_
     return RTB200_OK;
 }
 
+int rtb200_risemesh_triangles(const rtb200_risemesh* m, float* tri9)
+{
+    if (!m || (!tri9 && !m->tri.empty())) return RTB200_E_INVALID;
+    for (size_t i = 0; i < m->tri.size(); ++i)
+        for (int k = 0; k < 3; ++k) tri9[3 * i + k] = (float)m->points[3 * (size_t)m->tri[i] + k];
+    return RTB200_OK;
+}
+
 int rtb200_risemesh_destroy(rtb200_risemesh* m)
 {
     delete m;

@@ -159,6 +159,12 @@ class RiseMesh:
         return {"version": v.value, "n_points": npt.value, "n_tri": ntri.value, "double_sided": bool(ds.value),
                 "n_bvh_nodes": nn.value}
 
+    def triangles(self):
+        """(n, 9) float32 triangles (v0, v1, v2)."""
+        out = np.zeros((self.info()["n_tri"], 9), np.float32)
+        check(lib().rtb200_risemesh_triangles(self.h, _ptr(out)))
+        return out
+
     def host_bvh(self, use_cached_bvh=True):
         """(nodes2, prims, nodes4) as a scene commit would use them."""
         h = ctypes.c_void_p()

@@ -1,0 +1,440 @@
+"""Scene ingest: the reference's ASCII scene files (.RISEscene, "RISE ASCII
+SCENE 5..7") for the chunks this renderer draws, into a scenes.SceneDesc.
+
+The file is a list of chunks -- a keyword on its own line, "{" and "}" on
+their own lines around "parameter value..." lines -- with '#' line comments
+and /* */ block comments (src/Library/Parsers/README.md, Cst/Cst.cpp:80-115).
+Each supported chunk is restated from its parser in
+src/Library/Parsers/ChunkParserRegistry.cpp (defaults included):
+
+  spectral_painter            -> scenes.spectral_painter (binned SpectralPacket)
+  lambertian_material         -> Lambertian, reflectance painter
+  lambertian_luminaire_material -> emitter: radiance = exitance * scale / pi
+                                 (LambertianEmitter.cpp:72-87), reflective part
+                                 from a lambertian `material` or none
+  ggx_material                -> GGX conductor (rd none, isotropic alpha)
+  dielectric_material         -> smooth dielectric, constant IOR
+  clippedplane_geometry       -> two triangles (a, b, c), (a, c, d)
+  rawmesh_geometry            -> "tri" / "quad" lines (TriangleMeshLoaderRAW.cpp:33-110)
+  risemesh_geometry           -> the .risemesh reader of the C ABI
+  box_geometry                -> 12 triangles, centred on the origin
+  standard_object             -> position + Euler orientation (degrees, Z
+                                 then Y then X) + scale (Transformable.cpp:339-343,436-441)
+  film, pinhole_camera        -> image size, camera (vertical field of view)
+  pathtracing_spectral_rasterizer, pixelintegratingspectral_rasterizer
+                              -> samples, wavelength range, pixel filter
+                                 (default Gaussian 2.0 / 0.35), adaptive sampling,
+                                 Russian roulette, maximum depth (128)
+  pathtracing_shaderop, standard_shader, file_rasterizeroutput -> accepted
+
+A parameter or chunk that would change the image in a way this renderer
+cannot draw (other painters, materials, geometry, cameras, lights, modifiers,
+volumes, non-unit pixel aspect, hidden luminaires, ...) raises
+SceneFileError naming it.  Options that do not change the estimator's
+expectation (the pixel sampler, OIDN denoising of the output, light-BVH
+selection, hwss) are recorded in LoadedScene.notes.
+"""
+import math
+import os
+import re
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import scenes
+
+
+class SceneFileError(ValueError):
+    pass
+
+
+@dataclass
+class Chunk:
+    keyword: str
+    line: int
+    params: list = field(default_factory=list)   # (key, value string, line)
+
+    def get(self, key, default=None):
+        vals = [v for k, v, _ in self.params if k == key]
+        return vals[-1] if vals else default
+
+    def all(self, key):
+        return [v for k, v, _ in self.params if k == key]
+
+    def has(self, key):
+        return any(k == key for k, _, _ in self.params)
+
+
+@dataclass
+class LoadedScene:
+    desc: scenes.SceneDesc
+    spp: int
+    outputs: list = field(default_factory=list)
+    notes: list = field(default_factory=list)
+
+
+def _strip_comments(text):
+    text = re.sub(r"/\*.*?\*/", lambda m: "\n" * m.group(0).count("\n"), text, flags=re.S)
+    return [re.sub(r"#.*", "", ln).strip() for ln in text.split("\n")]
+
+
+def parse_chunks(text):
+    """The chunks of a scene file, in order."""
+    lines = _strip_comments(text)
+    i = 0
+    while i < len(lines) and not lines[i]:
+        i += 1
+    m = re.match(r"RISE ASCII SCENE (\d+)$", lines[i] if i < len(lines) else "")
+    if not m or not 5 <= int(m.group(1)) <= 7:
+        raise SceneFileError("not a RISE ASCII SCENE (versions 5 to 7) file")
+    i += 1
+    chunks = []
+    while i < len(lines):
+        ln = lines[i]
+        if not ln:
+            i += 1
+            continue
+        if len(ln.split()) != 1 or ln in ("{", "}"):
+            raise SceneFileError(f"line {i + 1}: expected a chunk name, got {ln!r}")
+        c = Chunk(ln, i + 1)
+        i += 1
+        while i < len(lines) and not lines[i]:
+            i += 1
+        if i >= len(lines) or lines[i] != "{":
+            raise SceneFileError(f"line {c.line}: chunk {ln} without '{{'")
+        i += 1
+        while i < len(lines) and lines[i] != "}":
+            if lines[i]:
+                parts = lines[i].split(None, 1)
+                c.params.append((parts[0], parts[1].strip() if len(parts) > 1 else "", i + 1))
+            i += 1
+        if i >= len(lines):
+            raise SceneFileError(f"line {c.line}: chunk {ln} without '}}'")
+        i += 1
+        chunks.append(c)
+    return chunks
+
+
+def _floats(s, n, what):
+    try:
+        v = [float(x) for x in s.split()]
+    except ValueError:
+        raise SceneFileError(f"{what}: expected {n} numbers, got {s!r}") from None
+    if len(v) != n:
+        raise SceneFileError(f"{what}: expected {n} numbers, got {s!r}")
+    return v
+
+
+def _bool(s):
+    return str(s).strip().lower() in ("true", "1", "yes", "on")
+
+
+def _number(s):
+    try:
+        return float(s)
+    except (TypeError, ValueError):
+        return None
+
+
+def _rot(ax, ay, az):
+    """Rx(ax) Ry(ay) Rz(az) for column vectors: Z applied first, then Y, then X."""
+    cx, sx, cy, sy, cz, sz = math.cos(ax), math.sin(ax), math.cos(ay), math.sin(ay), math.cos(az), math.sin(az)
+    rx = np.array([[1, 0, 0], [0, cx, -sx], [0, sx, cx]])
+    ry = np.array([[cy, 0, sy], [0, 1, 0], [-sy, 0, cy]])
+    rz = np.array([[cz, -sz, 0], [sz, cz, 0], [0, 0, 1]])
+    return rx @ ry @ rz
+
+
+def _box(w, h, d):
+    hw, hh, hd = 0.5 * w, 0.5 * h, 0.5 * d
+    c = np.array([[x, y, z] for x in (-hw, hw) for y in (-hh, hh) for z in (-hd, hd)])
+    # faces as corner indices (x, y, z bits: 4, 2, 1), wound for outward normals
+    quads = [(0, 1, 3, 2), (4, 6, 7, 5), (0, 4, 5, 1), (2, 3, 7, 6), (0, 2, 6, 4), (1, 5, 7, 3)]
+    tris = []
+    for a, b, cc, dd in quads:
+        tris.append(np.concatenate([c[a], c[b], c[cc]]))
+        tris.append(np.concatenate([c[a], c[cc], c[dd]]))
+    return np.array(tris)
+
+
+class _Loader:
+    def __init__(self, search):
+        self.search = search
+        self.desc = scenes.SceneDesc()
+        self.painters = {}       # name -> spectrum id
+        self.materials = {}      # name -> (material id, kind, reflectance id)
+        self.geometry = {}       # name -> ((n, 9) float64 triangles, double_sided)
+        self.spp = None
+        self.outputs = []
+        self.notes = []
+        self.st = {}
+
+    def path(self, name, what):
+        for d in self.search:
+            p = os.path.join(d, name)
+            if os.path.exists(p):
+                return p
+        raise SceneFileError(f"{what}: file {name!r} not found (searched {self.search})")
+
+    def refuse(self, c, why):
+        raise SceneFileError(f"line {c.line}: {c.keyword}: {why}")
+
+    def only(self, c, allowed):
+        for k, _, ln in c.params:
+            if k not in allowed:
+                raise SceneFileError(f"line {ln}: {c.keyword}: parameter {k!r} is not supported")
+
+    # ---- painters ----------------------------------------------------------
+    def spectral_painter(self, c):
+        self.only(c, {"name", "nmbegin", "nmend", "scale", "cp", "file"})
+        nm, amp = [], []
+        for cp in c.all("cp"):
+            a, b = _floats(cp, 2, "spectral_painter cp")
+            nm.append(a)
+            amp.append(b)
+        if c.has("file"):
+            with open(self.path(c.get("file"), "spectral_painter"), "r") as f:
+                for ln in f:
+                    parts = ln.split()
+                    try:
+                        a, b = float(parts[0]), float(parts[1])
+                    except (IndexError, ValueError):
+                        continue
+                    nm.append(a)
+                    amp.append(b)
+        if not nm:
+            self.refuse(c, "no samples")
+        sp = scenes.spectral_painter(nm, amp, float(c.get("nmbegin", 400.0)), float(c.get("nmend", 700.0)))
+        self.painters[c.get("name", "noname")] = self.desc.add_spectrum(sp)
+        if c.has("scale"):
+            self.notes.append(f"spectral_painter {c.get('name')}: scale applies to the RGB colour only")
+
+    def spectrum(self, c, name, allow_number=False):
+        """Spectrum id of a painter reference, or a flat spectrum for a number."""
+        if name in (None, "none"):
+            return -1
+        if name in self.painters:
+            return self.painters[name]
+        v = _number(name)
+        if allow_number and v is not None:
+            return self.desc.add_spectrum(np.full(81, v, np.float32))
+        self.refuse(c, f"unknown painter {name!r}")
+
+    def scaled(self, sid, k):
+        sp = self.desc.spectra[sid]
+        if isinstance(sp, scenes.SpectralPacket):
+            return self.desc.add_spectrum(scenes.SpectralPacket(sp.begin, sp.end,
+                                                                (np.asarray(sp.amps, np.float64) * k).astype(np.float32)))
+        return self.desc.add_spectrum((np.asarray(sp, np.float64) * k).astype(np.float32))
+
+    # ---- materials ---------------------------------------------------------
+    def add_material(self, c, m, kind, refl=-1):
+        self.materials[c.get("name", "noname")] = (self.desc.add_material(m), kind, refl)
+
+    def lambertian_material(self, c):
+        self.only(c, {"name", "reflectance"})
+        r = self.spectrum(c, c.get("reflectance", "none"))
+        self.add_material(c, scenes.Material(scenes.MAT_LAMBERTIAN, r), "lambertian", r)
+
+    def lambertian_luminaire_material(self, c):
+        self.only(c, {"name", "material", "exitance", "scale"})
+        ex = self.spectrum(c, c.get("exitance", "none"))
+        scale = float(c.get("scale", 1.0))
+        emit = self.scaled(ex, scale / math.pi) if ex >= 0 else -1
+        inner = c.get("material", "none")
+        refl = -1
+        if inner != "none":
+            if inner not in self.materials or self.materials[inner][1] != "lambertian":
+                self.refuse(c, f"reflective part {inner!r} must be a lambertian_material")
+            refl = self.materials[inner][2]
+        self.add_material(c, scenes.Material(scenes.MAT_LAMBERTIAN, refl, emit), "luminaire", refl)
+
+    def ggx_material(self, c):
+        self.only(c, {"name", "rd", "rs", "alphax", "alphay", "ior", "extinction", "fresnel_mode"})
+        if c.get("rd", "none") != "none":
+            self.refuse(c, "a diffuse layer (rd) is not supported")
+        if c.get("fresnel_mode", "conductor") != "conductor":
+            self.refuse(c, "only fresnel_mode conductor is supported")
+        ax, ay = _number(c.get("alphax", "0.15")), _number(c.get("alphay", "0.15"))
+        if ax is None or ay is None or ax != ay:
+            self.refuse(c, "alphax and alphay must be equal numbers (isotropic)")
+        rs = c.get("rs", "none")
+        spec = self.spectrum(c, rs)
+        eta = self.spectrum(c, c.get("ior", "2.45"), allow_number=True)
+        kap = self.spectrum(c, c.get("extinction", "3.45"), allow_number=True)
+        self.add_material(c, scenes.Material(scenes.MAT_GGX, spec, -1, eta, kap, float(ax), 1.5), "ggx")
+        if rs == "none":
+            self.notes.append(f"ggx_material {c.get('name')}: rs none read as a unit specular layer")
+
+    def dielectric_material(self, c):
+        self.only(c, {"name", "tau", "ior", "scattering"})
+        if c.get("tau", "none") != "none":
+            self.refuse(c, "an absorbing interior (tau) is not supported")
+        ior = _number(c.get("ior", "1.33"))
+        if ior is None:
+            self.refuse(c, "ior must be a number")
+        self.add_material(c, scenes.Material(scenes.MAT_DIELECTRIC, -1, -1, -1, -1, 0.0, float(ior)), "dielectric")
+        if c.has("scattering"):
+            self.notes.append(f"dielectric_material {c.get('name')}: scattering ignored (smooth interface)")
+
+    # ---- geometry ----------------------------------------------------------
+    def clippedplane_geometry(self, c):
+        self.only(c, {"name", "pta", "ptb", "ptc", "ptd", "doublesided"})
+        p = [np.array(_floats(c.get(k, "0 0 0"), 3, k)) for k in ("pta", "ptb", "ptc", "ptd")]
+        tris = np.array([np.concatenate([p[0], p[1], p[2]]), np.concatenate([p[0], p[2], p[3]])])
+        self.geometry[c.get("name", "noname")] = (tris, _bool(c.get("doublesided", "true")))
+
+    def rawmesh_geometry(self, c):
+        self.only(c, {"name", "file", "double_sided", "maxpolygons", "maxdepth"})
+        tris = []
+        with open(self.path(c.get("file", "none"), "rawmesh_geometry"), "r") as f:
+            for ln in f:
+                parts = ln.split()
+                if not parts:
+                    continue
+                if parts[0] == "tri":
+                    v = [float(x) for x in parts[1:10]]
+                    tris.append(v)
+                elif parts[0] == "quad":
+                    v = [float(x) for x in parts[1:13]]
+                    a, b, cc, d = v[0:3], v[3:6], v[6:9], v[9:12]
+                    tris.append(a + b + cc)
+                    tris.append(a + cc + d)
+        self.geometry[c.get("name", "noname")] = (np.array(tris, np.float64).reshape(-1, 9),
+                                                  _bool(c.get("double_sided", "false")))
+
+    def risemesh_geometry(self, c):
+        from .raycaster import RiseMesh
+        self.only(c, {"name", "file", "loadintomemory", "face_normals"})
+        m = RiseMesh.from_file(self.path(c.get("file", "none"), "risemesh_geometry"))
+        try:
+            self.geometry[c.get("name", "noname")] = (m.triangles().astype(np.float64), m.info()["double_sided"])
+        finally:
+            m.close()
+
+    def box_geometry(self, c):
+        self.only(c, {"name", "width", "height", "depth"})
+        self.geometry[c.get("name", "noname")] = (
+            _box(float(c.get("width", 1.0)), float(c.get("height", 1.0)), float(c.get("depth", 1.0))), False)
+
+    # ---- objects -----------------------------------------------------------
+    def standard_object(self, c):
+        self.only(c, {"name", "geometry", "material", "position", "orientation", "scale", "casts_shadows",
+                      "receives_shadows"})
+        g = c.get("geometry", "none")
+        if g not in self.geometry:
+            self.refuse(c, f"unknown geometry {g!r}")
+        mname = c.get("material", "none")
+        if mname not in self.materials:
+            self.refuse(c, f"unknown or missing material {mname!r}")
+        if not _bool(c.get("casts_shadows", "true")) or not _bool(c.get("receives_shadows", "true")):
+            self.refuse(c, "objects that cast or receive no shadows are not supported")
+        tris, ds = self.geometry[g]
+        pos = np.array(_floats(c.get("position", "0 0 0"), 3, "position"))
+        ori = np.radians(_floats(c.get("orientation", "0 0 0"), 3, "orientation"))
+        sc = np.array(_floats(c.get("scale", "1 1 1"), 3, "scale"))
+        r = _rot(*ori)
+        v = tris.reshape(-1, 3) * sc
+        world = (v @ r.T + pos).reshape(-1, 9)
+        self.desc.add_mesh(world.astype(np.float32), self.materials[mname][0], bool(ds))
+
+    # ---- camera, film, rasterizer -----------------------------------------
+    def film(self, c):
+        self.only(c, {"width", "height", "pixelAR"})
+        if float(c.get("pixelAR", 1.0)) != 1.0:
+            self.refuse(c, "pixel aspect ratios other than 1 are not supported")
+        self.st["width"] = int(c.get("width", 256))
+        self.st["height"] = int(c.get("height", 256))
+
+    def pinhole_camera(self, c):
+        self.only(c, {"name", "location", "lookat", "up", "fov", "orientation", "pitch", "roll", "yaw",
+                      "target_orientation", "theta", "phi", "exposure", "scanning_rate", "pixel_rate"})
+        for k in ("orientation", "target_orientation"):
+            if c.has(k) and any(x != 0.0 for x in map(float, c.get(k).split())):
+                self.refuse(c, f"{k} is not supported")
+        for k in ("pitch", "roll", "yaw", "theta", "phi"):
+            if c.has(k) and float(c.get(k)) != 0.0:
+                self.refuse(c, f"{k} is not supported")
+        self.st["cam_pos"] = tuple(_floats(c.get("location", "0 0 0"), 3, "location"))
+        self.st["cam_look"] = tuple(_floats(c.get("lookat", "0 0 -1"), 3, "lookat"))
+        self.st["cam_up"] = tuple(_floats(c.get("up", "0 1 0"), 3, "up"))
+        self.st["fov_deg"] = float(c.get("fov", 39.0))
+
+    def _raster_common(self, c, extra):
+        base = {"samples", "nmbegin", "nmend", "num_wavelengths", "hwss", "use_hwss", "spectral_samples",
+                "pixel_filter", "pixel_filter_width", "pixel_filter_height", "pixel_filter_paramA",
+                "pixel_filter_paramB", "pixel_sampler", "pixel_sampler_param", "blue_noise_sampler",
+                "adaptive_max_samples", "adaptive_threshold", "rr_min_depth", "rr_threshold", "show_luminaires",
+                "oidn_denoise", "oidn_quality", "oidn_device", "oidn_prefilter", "light_bvh", "defaultshader",
+                "progressive_rendering", "progressive_samples_per_pass"}
+        self.only(c, base | extra)
+        self.spp = int(c.get("samples", 32))
+        lo, hi = float(c.get("nmbegin", 380.0)), float(c.get("nmend", 780.0))
+        if lo < 380.0 or hi > 780.0 or not hi > lo:
+            self.refuse(c, "wavelength range must lie within 380..780 nm")
+        self.st["lambda_min"], self.st["lambda_max"] = lo, hi
+        filt = c.get("pixel_filter", "gaussian").strip('"').lower()
+        if filt == "gaussian":
+            self.st["filter"] = 1
+            self.st["filter_size"] = float(c.get("pixel_filter_paramA", 2.0))
+            self.st["filter_sigma"] = float(c.get("pixel_filter_paramB", 0.35))
+        elif filt == "box" and float(c.get("pixel_filter_width", 1.0)) == 1.0 \
+                and float(c.get("pixel_filter_height", 1.0)) == 1.0:
+            self.st["filter"] = 0
+        else:
+            self.refuse(c, f"pixel filter {filt!r} is not supported (gaussian, or box of width 1)")
+        if c.has("adaptive_max_samples"):
+            self.st["adaptive_max_spp"] = int(c.get("adaptive_max_samples"))
+            self.st["adaptive_threshold"] = float(c.get("adaptive_threshold", 0.01))
+        if c.has("rr_min_depth"):
+            self.st["rr_min_depth"] = int(c.get("rr_min_depth"))
+        if c.has("rr_threshold"):
+            self.st["rr_threshold"] = float(c.get("rr_threshold"))
+        if not _bool(c.get("show_luminaires", "true")):
+            self.refuse(c, "hidden luminaires (show_luminaires false) are not supported")
+        for k, why in (("pixel_sampler", "the pixel sampler (Sobol by default) is replaced by counter-based "
+                        "random numbers"), ("oidn_denoise", "the film is not denoised"),
+                       ("light_bvh", "lights are picked by emitted power")):
+            self.notes.append(f"{c.keyword}: {why}")
+        if not _bool(c.get("hwss", c.get("use_hwss", "false"))) or c.get("num_wavelengths", "4") != "4":
+            self.notes.append(f"{c.keyword}: rendered with hero-wavelength sampling of 4 wavelengths")
+
+    def pathtracing_spectral_rasterizer(self, c):
+        self._raster_common(c, set())
+        self.st["max_depth"] = 128
+
+    def pixelintegratingspectral_rasterizer(self, c):
+        self._raster_common(c, {"lum_samples", "max_recursion"})
+        self.st["max_depth"] = int(c.get("max_recursion", 10))
+
+    def file_rasterizeroutput(self, c):
+        self.outputs.append({k: v for k, v, _ in c.params})
+
+    def accept(self, c):
+        pass
+
+    pathtracing_shaderop = accept
+    standard_shader = accept
+
+
+def load_scene(path=None, text=None, search=()):
+    """Read a .RISEscene (or its text) into a LoadedScene.  Referenced files
+    are looked up in `search` (e.g. the reference's media root), then next to
+    the scene file, then in the working directory."""
+    if text is None:
+        with open(path, "r") as f:
+            text = f.read()
+    dirs = list(search) + ([os.path.dirname(os.path.abspath(path))] if path else []) + [os.getcwd()]
+    ld = _Loader(dirs)
+    for c in parse_chunks(text):
+        fn = getattr(ld, c.keyword, None)
+        if fn is None or c.keyword.startswith("_"):
+            raise SceneFileError(f"line {c.line}: chunk {c.keyword} is not supported")
+        fn(c)
+    if ld.spp is None:
+        raise SceneFileError("no spectral rasterizer chunk")
+    if not ld.desc.meshes:
+        raise SceneFileError("no objects")
+    st = scenes.RenderSettings(**{**scenes.RenderSettings().__dict__, "max_depth": 128, **ld.st})
+    ld.desc.settings = st
+    return LoadedScene(ld.desc, ld.spp, ld.outputs, ld.notes)
