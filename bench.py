@@ -235,6 +235,17 @@ def bench_large_scene(ctx, layout="f32"):
         r.close()
         out["relmse_vs_fp64_oracle_crop"] = {"crop": [x0, y0, x1, y1], "oracle_spp": int(z["spp"]), **rel}
     scene.close()
+    if layout == "f32":
+        # The same render over 8-bit quantised child boxes (64-byte nodes).
+        q = pathtracer.upload_scene(ctx, desc, "q8")
+        r = pathtracer.SpectralRasterizer(ctx, desc, scene=q)
+        r.rasterize_scene(4)
+        s0 = r.stats()
+        r.rasterize_scene(64)
+        s1 = r.stats()
+        out["q8_nodes_msamples_s"] = (s1["samples"] - s0["samples"]) / (s1["seconds"] - s0["seconds"]) / 1e6
+        r.close()
+        q.close()
     return out
 
 

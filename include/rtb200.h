@@ -199,7 +199,18 @@ typedef struct {
     float filter_sigma;       /* Gaussian: standard deviation in pixels, > 0 */
     int32_t adaptive_max_spp; /* adaptive sampling: maximum samples per pixel (0 = off) */
     float adaptive_threshold; /* adaptive sampling: relative standard error to converge (reference: 0.01) */
+    int32_t light_selection;  /* RTB200_LIGHTS_* */
 } rtb200_render_settings;
+
+/* Next-event luminary selection.  BVH: the reference's light BVH
+ * (Lights/LightBVH.cpp: importance = power / squared distance to the node's
+ * box, one random number rescaled down the tree; its pdf enters the MIS
+ * weights) when the scene has more than one luminary, as the reference does
+ * by default (StabilityConfig::useLightBVH, LightSampler.cpp:748-761).
+ * POWER: in proportion to emitted power alone (the reference's alias table,
+ * light_bvh false). */
+#define RTB200_LIGHTS_BVH 0
+#define RTB200_LIGHTS_POWER 1
 
 /* Pixel filters.  BOX: uniform jitter in the pixel, the pixel is the mean of
  * its own samples.  GAUSSIAN: the reference's GaussianPixelFilter

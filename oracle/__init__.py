@@ -208,7 +208,8 @@ def pt_render(desc, spp, sample_begin=0, crop=None, threads=None, settings=None,
     setd = np.array([st.lambda_min, st.lambda_max, st.rr_threshold, getattr(st, "filter_size", 2.0),
                      getattr(st, "filter_sigma", 0.5), getattr(st, "adaptive_threshold", 0.01)], np.float64)
     seti = np.array([st.width, st.height, st.max_depth, st.rr_min_depth, st.nee_per_lambda, st.seed,
-                     getattr(st, "filter", 0), getattr(st, "adaptive_max_spp", 0)], np.int32)
+                     getattr(st, "filter", 0), getattr(st, "adaptive_max_spp", 0),
+                     getattr(st, "light_selection", 0)], np.int32)
     out = np.zeros((y1 - y0, x1 - x0, 3), np.float64)
     counts = np.zeros((y1 - y0, x1 - x0), np.int32)
     cie = np.ascontiguousarray(cie_table())
@@ -274,6 +275,26 @@ def _bind_colour(lib, prefix):
     if prefix == "ref_pt_":
         f = lib.ref_pt_spectral_packet
         f.restype, f.argtypes = None, [_f64p, _f64p, ctypes.c_int, _D, _D, _f64p, ctypes.c_int, _f64p]
+
+
+def light_bvh(lib, prefix, pos, power, pts, xi):
+    """The light BVH over point lights of the port ('orc_pt_') or the
+    reference ('ref_pt_'): (picked light, its probability) per query and the
+    (m, n) probabilities of every light from every query point."""
+    pos = np.ascontiguousarray(pos, np.float64).reshape(-1, 3)
+    power = np.ascontiguousarray(power, np.float64)
+    pts = np.ascontiguousarray(pts, np.float64).reshape(-1, 3)
+    xi = np.ascontiguousarray(xi, np.float64)
+    n, m = len(pos), len(pts)
+    picked = np.zeros(m, np.int32)
+    pdf = np.zeros(m)
+    pdf_all = np.zeros((m, n))
+    f = getattr(lib, prefix + "light_bvh")
+    f.restype = None
+    f.argtypes = [ctypes.c_int, _f64p, _f64p, ctypes.c_int, _f64p, _f64p, _vp, _f64p, _f64p]
+    f(n, _p(pos, _f64p), _p(power, _f64p), m, _p(pts, _f64p), _p(xi, _f64p), picked.ctypes.data,
+      _p(pdf, _f64p), _p(pdf_all, _f64p))
+    return picked, pdf, pdf_all
 
 
 def xyz_to_rec709(lib, prefix, xyz):

@@ -67,8 +67,8 @@ int  orc_ray_triangle(const double* o, const double* d, const double* v0, const 
  *   cam:    10 doubles (pos, look, up, vertical fov in degrees)
  *   setd:   6 doubles (lambda_min, lambda_max, rr_threshold, filter size, filter sigma,
  *           adaptive threshold)
- *   seti:   8 int32 (width, height, max_depth, rr_min_depth, nee_per_lambda, seed, filter,
- *           adaptive maximum samples per pixel or 0)
+ *   seti:   9 int32 (width, height, max_depth, rr_min_depth, nee_per_lambda, seed, filter,
+ *           adaptive maximum samples per pixel or 0, light selection: 0 light BVH, 1 power)
  * filter 0 is the box film (mean of the pixel's own samples); filter 1 is the
  * Gaussian pixel filter: with size / 2 > 0.501 the samples of every pixel
  * within the support are splatted and a pixel is sum(w XYZ) / sum(w); a
@@ -92,6 +92,8 @@ int orc_pt_render(const float* tri9, int64_t n_tri, const int64_t* meshes, int32
 /* Building blocks of the path-tracing oracle, exported so tests can hold each
  * against the reference's own code (oracle/_ref/libref_pt.so). */
 double orc_pt_gaussian_weight(double size, double sigma, double dx, double dy);
+void   orc_pt_light_bvh(int n, const double* pos, const double* power, int m, const double* pts, const double* xi,
+                        int* picked, double* pdf, double* pdf_all);
 void   orc_pt_xyz_to_rec709(const double* xyz, double* rgb);
 void   orc_pt_display(const double* rgb, double exposure_ev, int tone, unsigned char* out3);
 void   orc_pt_sample_wavelengths(double u, double lmin, double lmax, double* lam4);

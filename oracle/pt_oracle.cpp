@@ -323,7 +323,112 @@ double Fms(double favg, double eavg)
 
 struct Ggx { double alpha, spec, eta, k, favg; };
 
-struct Light { int first, count, emit; double area, pdf; };
+struct Light { int first, count, emit; double area, pdf; int bvhPos = 0; };
+
+// Light BVH (Lights/LightBVH.cpp:132-531): preorder nodes over the
+// luminaries, the left child after its parent.
+struct LightNode {
+    double lo[3], hi[3], power;
+    int right = 0, light = -1, count = 0, start = 0;
+};
+struct LightPrimD {
+    double lo[3], hi[3], c[3], power;
+    int light;
+};
+
+// BuildRecursive (LightBVH.cpp:291-421): union box and summed power; split
+// on the widest axis of the box centres at the power-weighted mean centre.
+int BuildLightBvh(std::vector<LightPrimD>& prims, int start, int end, int& pos, std::vector<LightNode>& nodes,
+                  std::vector<int>& posOf)
+{
+    const int idx = (int)nodes.size();
+    nodes.emplace_back();
+    LightNode n;
+    n.power = prims[start].power;
+    for (int k = 0; k < 3; ++k) { n.lo[k] = prims[start].lo[k]; n.hi[k] = prims[start].hi[k]; }
+    for (int i = start + 1; i < end; ++i) {
+        for (int k = 0; k < 3; ++k) { n.lo[k] = std::min(n.lo[k], prims[i].lo[k]); n.hi[k] = std::max(n.hi[k], prims[i].hi[k]); }
+        n.power += prims[i].power;
+    }
+    n.count = end - start;
+    n.start = pos;
+    if (end - start == 1) {
+        n.light = prims[start].light;
+        posOf[n.light] = pos++;
+        nodes[idx] = n;
+        return idx;
+    }
+    double clo[3], chi[3];
+    for (int k = 0; k < 3; ++k) clo[k] = chi[k] = prims[start].c[k];
+    for (int i = start + 1; i < end; ++i)
+        for (int k = 0; k < 3; ++k) { clo[k] = std::min(clo[k], prims[i].c[k]); chi[k] = std::max(chi[k], prims[i].c[k]); }
+    const double ex[3] = {chi[0] - clo[0], chi[1] - clo[1], chi[2] - clo[2]};
+    int axis = 0;
+    if (ex[1] > ex[0]) axis = 1;
+    if (ex[2] > (axis == 0 ? ex[0] : ex[1])) axis = 2;
+    int mid;
+    if (ex[axis] < 1e-10) {
+        mid = start + (end - start) / 2;
+    } else {
+        double ws = 0.0, tp = 0.0;
+        for (int i = start; i < end; ++i) { ws += prims[i].c[axis] * prims[i].power; tp += prims[i].power; }
+        const double split = tp > 0.0 ? ws / tp : 0.5 * (clo[axis] + chi[axis]);
+        auto it = std::partition(prims.begin() + start, prims.begin() + end,
+                                 [&](const LightPrimD& p) { return p.c[axis] < split; });
+        mid = (int)(it - prims.begin());
+        if (mid == start || mid == end) mid = start + (end - start) / 2;
+    }
+    nodes[idx] = n;
+    BuildLightBvh(prims, start, mid, pos, nodes, posOf);
+    nodes[idx].right = (int)nodes.size();
+    BuildLightBvh(prims, mid, end, pos, nodes, posOf);
+    return idx;
+}
+
+// NodeImportance (LightBVH.cpp:169-217), full-sphere cone.
+double LightImportance(const LightNode& n, const double p[3])
+{
+    if (!(n.power > 0)) return 0.0;
+    double d2 = 0.0;
+    for (int k = 0; k < 3; ++k) {
+        const double d = p[k] < n.lo[k] ? n.lo[k] - p[k] : (p[k] > n.hi[k] ? p[k] - n.hi[k] : 0.0);
+        d2 += d * d;
+    }
+    return n.power / std::max(d2, 1e-4);
+}
+
+// Sample (LightBVH.cpp:423-482): -1 with pdf 0 when nothing can be picked.
+int SampleLightBvh(const std::vector<LightNode>& nodes, const double p[3], double xi, double& pdf)
+{
+    pdf = 1.0;
+    int i = 0;
+    while (nodes[i].count > 1) {
+        const int r = nodes[i].right;
+        const double il = LightImportance(nodes[i + 1], p), ir = LightImportance(nodes[r], p), tot = il + ir;
+        if (!(tot > 0)) { pdf = 0.0; return -1; }
+        const double pl = il / tot;
+        if (xi < pl) { pdf *= pl; xi = xi / pl; i = i + 1; }
+        else { pdf *= 1.0 - pl; xi = (xi - pl) / (1.0 - pl); i = r; }
+    }
+    return nodes[i].light;
+}
+
+// Pdf (LightBVH.cpp:484-531).
+double LightBvhPdf(const std::vector<LightNode>& nodes, int pos, const double p[3])
+{
+    double pdf = 1.0;
+    int i = 0;
+    while (nodes[i].count > 1) {
+        const int r = nodes[i].right;
+        const double il = LightImportance(nodes[i + 1], p), ir = LightImportance(nodes[r], p), tot = il + ir;
+        if (!(tot > 0)) return 0.0;
+        const double pl = il / tot;
+        const LightNode& L = nodes[i + 1];
+        if (pos >= L.start && pos < L.start + L.count) { pdf *= pl; i = i + 1; }
+        else { pdf *= 1.0 - pl; i = r; }
+    }
+    return pdf;
+}
 struct LTri { V v0, e1, e2; double cdf; };
 
 struct Scene {
@@ -342,6 +447,8 @@ struct Scene {
     double lmin, lmax, rrThreshold, ynorm;
     int width, height, maxDepth, rrMinDepth, neePerLambda;
     uint32_t seed;
+    bool lightBvh = false;                 // luminaries picked with the light BVH
+    std::vector<LightNode> lightNodes;
     V pos, fwd, right, up;
     // Gaussian pixel filter too narrow for the filtered film: the camera
     // sample is warped about the pixel centre (warpSigma > 0), else 0.
@@ -490,17 +597,22 @@ void Sample(const Scene& S, uint32_t pixel, uint32_t sample, double xyz[3])
 {
     const uint32_t key = PathKey(S.seed, pixel, sample);
     const int px = (int)(pixel % (uint32_t)S.width), py = (int)(pixel / (uint32_t)S.width);
-    double ox = Rand(key, 0), oy = Rand(key, 1);
+    // Screen position, pixel centres on integer coordinates, rows downwards:
+    // ptOnScreen = (x + u - 1/2, (height - y) + v - 1/2)
+    // (PathTracingSpectralRasterizer.cpp:321-331, BoxPixelFilter.h:54-58), or
+    // GaussianPixelFilter::warp about the pixel centre
+    // (Sampling/GaussianPixelFilter.h:109-127); the pinhole maps it to the
+    // direction W + (x - width/2) h ar / width (-U) + (height/2 - y_row) h / height V
+    // (PinholeCamera.cpp:85-89,182-192,209-214).
+    const double ox = Rand(key, 0), oy = Rand(key, 1);
+    double fx = px + ox - 0.5, fy = py + 0.5 - oy;
     if (S.warpSigma > 0.0) {
-        // GaussianPixelFilter::warp (Sampling/GaussianPixelFilter.h:109-127),
-        // about the pixel centre (PathTracingSpectralRasterizer.cpp:327-328).
         const double v = std::max(S.warpTrunc + (1.0 - S.warpTrunc) * ox, 1e-30);
         const double r = S.warpSigma * std::sqrt(-2.0 * std::log(v));
         const double th = 2.0 * kPi * oy;
-        ox = 0.5 + r * std::cos(th);
-        oy = 0.5 + r * std::sin(th);
+        fx = px + r * std::cos(th);
+        fy = py - r * std::sin(th);
     }
-    const double fx = px + ox, fy = py + oy;
     const double sx = 2.0 * fx / S.width - 1.0, sy = 1.0 - 2.0 * fy / S.height;
     V d = Norm(S.fwd + S.right * sx + S.up * sy);
     V o = S.pos;
@@ -540,7 +652,9 @@ void Sample(const Scene& S, uint32_t pixel, uint32_t sample, double xyz[3])
             if (bsdfPdf > 0 && light >= 0) {
                 const Light& lg = S.lights[light];
                 const double cosL = std::fabs(Dot(d, ng));
-                if (cosL > 0 && lg.area > 0) w = PowerHeuristic(bsdfPdf, lg.pdf * t * t / (lg.area * cosL));
+                const double po[3] = {o.x, o.y, o.z};   // the previous vertex
+                const double psel = S.lightBvh ? LightBvhPdf(S.lightNodes, lg.bvhPos, po) : lg.pdf;
+                if (cosL > 0 && lg.area > 0) w = PowerHeuristic(bsdfPdf, psel * t * t / (lg.area * cosL));
             }
             for (int k = 0; k < 4; ++k) L[k] += thr[k] * Spec(S, emit, lam[k]) * w;
         }
@@ -572,12 +686,19 @@ void Sample(const Scene& S, uint32_t pixel, uint32_t sample, double xyz[3])
                 if (!S.lights.empty()) {
                     const double ul = Rand(key, Dim(depth, 4 * k));
                     int li = 0;
-                    double acc = 0.0;
-                    for (li = 0; li < (int)S.lights.size() - 1; ++li) {
-                        acc += S.lights[li].pdf;
-                        if (ul < acc) break;
+                    double psel;
+                    if (S.lightBvh) {
+                        const double pp[3] = {p.x, p.y, p.z};
+                        li = SampleLightBvh(S.lightNodes, pp, ul, psel);
+                    } else {
+                        double acc = 0.0;
+                        for (li = 0; li < (int)S.lights.size() - 1; ++li) {
+                            acc += S.lights[li].pdf;
+                            if (ul < acc) break;
+                        }
+                        psel = S.lights[li].pdf;
                     }
-                    if (li != light) {
+                    if (li >= 0 && li != light && psel > 0) {
                         const Light& lg = S.lights[li];
                         const double ux = Rand(key, Dim(depth, 4 * k + 1)), uy = Rand(key, Dim(depth, 4 * k + 2)),
                                      uz = Rand(key, Dim(depth, 4 * k + 3));
@@ -595,12 +716,12 @@ void Sample(const Scene& S, uint32_t pixel, uint32_t sample, double xyz[3])
                         const double pd[3] = {p.x, p.y, p.z}, ld[3] = {toL.x, toL.y, toL.z};
                         if (cosL > 0 && cosS > 0 && !orc_any_d(S.bvh, pd, ld, dist - 0.001)) {
                             const double geom = lg.area * cosL / (dist * dist);
-                            const double plight = lg.pdf * dist * dist / (lg.area * cosL);
+                            const double plight = psel * dist * dist / (lg.area * cosL);
                             for (int j = 0; j < 4; ++j) {
                                 if (S.neePerLambda && j != k) continue;
                                 double f, pb;
                                 EvalBsdf(S, mat, lam[j], ns, gnv, r, toL, f, pb);
-                                const double w = (pb > 0 ? PowerHeuristic(plight, pb) : 1.0) / lg.pdf;
+                                const double w = (pb > 0 ? PowerHeuristic(plight, pb) : 1.0) / psel;
                                 L[j] += thr[j] * Spec(S, lg.emit, lam[j]) * cosS * geom * f * w;
                             }
                         }
@@ -875,6 +996,34 @@ extern "C" void orc_pt_display(const double* rgb, double exposure_ev, int tone, 
     }
 }
 
+/* The light BVH on its own, for the comparison with the reference's: n
+ * point lights (positions 3n, powers n; boxes widened by 1e-12 as
+ * EnsureBoxHasVolume does), m queries (points 3m, random numbers m): picked
+ * light and selection probability per query, and the probability of every
+ * light from every query point (m x n). */
+extern "C" void orc_pt_light_bvh(int n, const double* pos, const double* power, int m, const double* pts,
+                                 const double* xi, int* picked, double* pdf, double* pdf_all)
+{
+    std::vector<LightPrimD> prims(n);
+    for (int i = 0; i < n; ++i) {
+        for (int k = 0; k < 3; ++k) {
+            prims[i].lo[k] = pos[3 * i + k] - 1e-12;
+            prims[i].hi[k] = pos[3 * i + k] + 1e-12;
+            prims[i].c[k] = 0.5 * (prims[i].lo[k] + prims[i].hi[k]);
+        }
+        prims[i].power = power[i];
+        prims[i].light = i;
+    }
+    std::vector<LightNode> nodes;
+    std::vector<int> posOf(n, 0);
+    int at = 0;
+    BuildLightBvh(prims, 0, n, at, nodes, posOf);
+    for (int q = 0; q < m; ++q) {
+        picked[q] = SampleLightBvh(nodes, pts + 3 * q, xi[q], pdf[q]);
+        for (int i = 0; i < n; ++i) pdf_all[(size_t)q * n + i] = LightBvhPdf(nodes, posOf[i], pts + 3 * q);
+    }
+}
+
 /* GaussianPixelFilter::EvaluateFilter (Sampling/GaussianPixelFilter.h:67-78):
  * exp(-r^2 / (2 sigma^2)) / (2 pi sigma^2) inside the size x size box centred
  * on the pixel centre, 0 outside it. */
@@ -933,6 +1082,7 @@ extern "C" int orc_pt_render(const float* tri9, int64_t n_tri, const int64_t* me
     S.triMesh.assign((size_t)n_tri, 0);
     S.meshLight.assign((size_t)n_mesh, -1);
     std::vector<double> weight;
+    std::vector<LightPrimD> lightPrims;
     for (int m = 0; m < n_mesh; ++m) {
         const int64_t first = meshes[4 * m], count = meshes[4 * m + 1];
         for (int64_t t = first; t < first + count; ++t) S.triMesh[t] = m;
@@ -965,12 +1115,33 @@ extern "C" int orc_pt_render(const float* tri9, int64_t n_tri, const int64_t* me
         for (int k = 0; k < 81; ++k) mean += GridValue(spectra, emit, k);
         mean /= 81.0;
         weight.push_back(area * std::max(mean, 1e-12));
+        LightPrimD q;
+        for (int k = 0; k < 3; ++k) { q.lo[k] = INFINITY; q.hi[k] = -INFINITY; }
+        for (int64_t t = first; t < first + count; ++t)
+            for (int j = 0; j < 9; ++j) {
+                q.lo[j % 3] = std::min(q.lo[j % 3], (double)tri9[9 * t + j]);
+                q.hi[j % 3] = std::max(q.hi[j % 3], (double)tri9[9 * t + j]);
+            }
+        for (int k = 0; k < 3; ++k) {
+            if (q.lo[k] == q.hi[k]) { q.lo[k] -= 1e-12; q.hi[k] += 1e-12; }   // EnsureBoxHasVolume
+            q.c[k] = 0.5 * (q.lo[k] + q.hi[k]);
+        }
+        q.power = weight.back();
+        q.light = (int)S.lights.size();
+        lightPrims.push_back(q);
         S.meshLight[m] = (int)S.lights.size();
         S.lights.push_back(lg);
     }
     double wsum = 0.0;
     for (double w : weight) wsum += w;
     for (size_t i = 0; i < S.lights.size(); ++i) S.lights[i].pdf = weight[i] / wsum;
+    if (seti[8] == 0 && S.lights.size() > 1) {
+        std::vector<int> posOf(S.lights.size(), 0);
+        int pos = 0;
+        BuildLightBvh(lightPrims, 0, (int)lightPrims.size(), pos, S.lightNodes, posOf);
+        for (size_t i = 0; i < S.lights.size(); ++i) S.lights[i].bvhPos = posOf[i];
+        S.lightBvh = true;
+    }
     S.bvh = orc_bvh_build(tri9, n_tri);
     const int cw = x1 - x0, ch = y1 - y0;
     Adaptive A;
@@ -1004,7 +1175,7 @@ extern "C" int orc_pt_render(const float* tri9, int64_t n_tri, const int64_t* me
                     const uint32_t pixel = (uint32_t)(py * S.width + px);
                     auto splat = [&](uint32_t sample, const double* v) {
                         const uint32_t key = PathKey(S.seed, pixel, sample);
-                        const double sx = px + Rand(key, 0) - 0.5, sy = py + Rand(key, 1) - 0.5;
+                        const double sx = px + Rand(key, 0) - 0.5, sy = py + 0.5 - Rand(key, 1);
                         const int qx0 = std::max(x0, (int)std::floor(sx - hw));
                         const int qx1 = std::min(x1 - 1, (int)std::floor(sx + hw));
                         const int qy0 = std::max(y0, (int)std::floor(sy - hw));

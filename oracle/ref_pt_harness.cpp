@@ -26,6 +26,8 @@
 #include "Interfaces/IOptions.h"
 #include "Sampling/GaussianPixelFilter.h"
 #include "Rendering/DisplayTransform.h"
+#include "Lights/LightSampler.h"
+#include "Lights/LightBVH.h"
 #include "Interfaces/IFunction2D.h"
 #include "Utilities/PiecewiseLinearFunction.h"
 #include "Utilities/Color/SpectralPacket.h"
@@ -190,6 +192,31 @@ void ref_pt_spectral_packet(const double* nm, const double* amp, int n, double b
     const SpectralPacket packet(begin, end, (unsigned)n, f);
     for (int i = 0; i < nq; ++i) out[i] = packet.ValueAtNM(query[i]);
     f->release();
+}
+
+// The reference's light BVH over point-like entries (no luminary objects:
+// each entry's box is its position, widened by EnsureBoxHasVolume), sampled
+// and evaluated at the query points.
+void ref_pt_light_bvh(int n, const double* pos, const double* power, int m, const double* pts, const double* xi,
+                      int* picked, double* pdf, double* pdf_all)
+{
+    std::vector<Implementation::LightEntry> entries(n);
+    for (int i = 0; i < n; ++i) {
+        entries[i].pLight = 0;
+        entries[i].lumIndex = 0xFFFFFFFFu;
+        entries[i].exitance = power[i];
+        entries[i].position = Point3(pos[3 * i], pos[3 * i + 1], pos[3 * i + 2]);
+    }
+    Implementation::LuminaryManager::LuminariesList none;
+    Implementation::LightBVH bvh;
+    bvh.Build(entries, none);
+    for (int q = 0; q < m; ++q) {
+        const Point3 p(pts[3 * q], pts[3 * q + 1], pts[3 * q + 2]);
+        Scalar pd = 0;
+        picked[q] = (int)bvh.Sample(p, Vector3(0, 1, 0), xi[q], pd);
+        pdf[q] = pd;
+        for (int i = 0; i < n; ++i) pdf_all[(size_t)q * n + i] = bvh.Pdf((unsigned)i, p, Vector3(0, 1, 0));
+    }
 }
 
 double ref_pt_gaussian_weight(double size, double sigma, double dx, double dy)

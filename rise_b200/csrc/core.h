@@ -60,6 +60,7 @@ struct rtb200_scene {
     size_t spectra_table_bytes = 0;
     std::vector<rtb200::PtMaterial> materials;
     bool mixed_shading = false;      // materials of more than one shading class
+    int shade_class = -1;            // otherwise the one class (RTB200_MAT_* type), set at commit
     int32_t env = -1, env_visible = 1;
     std::vector<rtb200::PtLight> lights;        // built at commit
     std::vector<rtb200::PtLightTri> light_tris;
@@ -69,6 +70,8 @@ struct rtb200_scene {
     float* d_spectra = nullptr;
     rtb200::PtLight* d_lights = nullptr;
     rtb200::PtLightTri* d_light_tris = nullptr;
+    std::vector<rtb200::PtLightNode> light_nodes;  // light BVH, built at commit
+    rtb200::PtLightNode* d_light_nodes = nullptr;
     size_t shade_bytes = 0;
     bool committed = false;
     int32_t layout = RTB200_BVH_F32;

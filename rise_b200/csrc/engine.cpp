@@ -124,6 +124,7 @@ struct rtb200_engine {
     bool gspill = false;
     const rtb200_scene* gscene = nullptr;  // the shared scene, or null when jobs differ
     bool gclassify = false;
+    int gshade_class = -1;
     long long seg_seen = 0, shadow_seen = 0;
 };
 
@@ -138,11 +139,14 @@ PtLaunch MakeLaunch(const rtb200_engine* e)
     L.spill = false;
     L.uniform = !e->active.empty();
     L.classify = false;
+    L.shade_class = e->active.empty() ? -1 : e->owner[e->active[0]]->scene->shade_class;
     for (int k : e->active) {
         L.spill |= e->owner[k]->scene->stack_bound > kTraceStackShared;
         L.classify |= e->owner[k]->scene->mixed_shading;
         L.uniform &= e->owner[k]->scene == e->owner[e->active[0]]->scene;
+        if (e->owner[k]->scene->shade_class != L.shade_class) L.shade_class = -1;
     }
+    if (L.classify) L.shade_class = -1;
     L.scene = L.uniform ? e->h_table[e->active[0]].scene : PtScene{};
     L.paths = e->paths;
     L.queues = e->queues;
@@ -250,7 +254,7 @@ int EngineSubmit(rtb200_engine* e, rtb200_job* j, int spp)
     rtb200_scene* s = j->scene;
     PtJobDev& d = e->h_table[entry];
     d.scene = PtScene{s->d_nodes, s->layout, (int)s->n_nodes, s->d_tris, (int)s->tri_material.size(), s->d_attr, s->d_mats,
-                      s->d_spectra, s->d_lights, s->d_light_tris};
+                      s->d_spectra, s->d_lights, s->d_light_tris, s->d_light_nodes};
     d.cam = j->cam;
     d.set = j->set;
     int npx = j->npix;
@@ -317,7 +321,7 @@ int EngineStep(rtb200_engine* e, int iterations, bool graph)
     if (graph) {
         const rtb200_scene* us = L.uniform ? e->owner[e->active[0]]->scene : nullptr;
         if (!e->ggraph || e->glayout != L.layout || e->gspill != L.spill ||
-            e->gscene != us || e->gclassify != L.classify) {
+            e->gscene != us || e->gclassify != L.classify || e->gshade_class != L.shade_class) {
             DropGraph(e);
             cudaGraph_t g = nullptr;
             err = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
@@ -337,6 +341,7 @@ int EngineStep(rtb200_engine* e, int iterations, bool graph)
             e->gspill = L.spill;
             e->gscene = us;
             e->gclassify = L.classify;
+            e->gshade_class = L.shade_class;
         }
         const int reps = (iterations + kGraphIters - 1) / kGraphIters;
         for (int r = 0; r < reps && err == cudaSuccess; ++r) err = cudaGraphLaunch(e->gexec, st);
@@ -488,6 +493,8 @@ int rtb200_job_create(rtb200_scene* s, const rtb200_render_settings* rs, rtb200_
         !(rs->filter == RTB200_FILTER_GAUSSIAN && rs->filter_size > 0.0f && rs->filter_size <= 16.0f &&
           rs->filter_sigma > 0.0f))
         return SetError(ctx, RTB200_E_INVALID, "bad pixel filter settings");
+    if (rs->light_selection != RTB200_LIGHTS_BVH && rs->light_selection != RTB200_LIGHTS_POWER)
+        return SetError(ctx, RTB200_E_INVALID, "bad light selection");
     if (rs->adaptive_max_spp < 0 || (rs->adaptive_max_spp > 0 && !(rs->adaptive_threshold > 0.0f)))
         return SetError(ctx, RTB200_E_INVALID, "bad adaptive sampling settings");
     // Camera frame (pinhole; vertical field of view).
@@ -532,6 +539,7 @@ int rtb200_job_create(rtb200_scene* s, const rtb200_render_settings* rs, rtb200_
     st.env_visible = s->env_visible;
     st.n_lights = (int)s->lights.size();
     st.n_spectra = (int)(s->spectra.size() / RTB200_CIE_COUNT);
+    st.light_bvh = rs->light_selection == RTB200_LIGHTS_BVH ? 1 : 0;
     const bool gauss = rs->filter == RTB200_FILTER_GAUSSIAN;
     st.filter = !gauss ? kFilterBox : (0.5 * rs->filter_size > 0.501 ? kFilterSplat : kFilterWarp);
     st.filt_half = gauss ? 0.5f * rs->filter_size : 0.5f;

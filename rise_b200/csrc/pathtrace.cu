@@ -35,6 +35,80 @@ constexpr int kShadeBlock = 256;
 constexpr int kPathLeaves = 1;
 constexpr float kInv4Pi = 0.07957747154594767f;
 
+// ---- light BVH -------------------------------------------------------------
+
+// LightBVH::NodeImportance (Lights/LightBVH.cpp:169-217) for full-sphere
+// cones: power / max(squared distance from p to the node's box, 1e-4).
+__device__ __forceinline__ float LightImportance(const PtLightNode* __restrict__ nodes, int i, V3 p)
+{
+    const float4 a = __ldg(reinterpret_cast<const float4*>(nodes + i));       // lo xyz, hi x
+    const float4 b = __ldg(reinterpret_cast<const float4*>(nodes + i) + 1);   // hi yz, power, right
+    if (!(b.z > 0.0f)) return 0.0f;
+    const float lo[3] = {a.x, a.y, a.z}, hi[3] = {a.w, b.x, b.y}, q[3] = {p.x, p.y, p.z};
+    float d2 = 0.0f;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const float d = q[k] < lo[k] ? lo[k] - q[k] : (q[k] > hi[k] ? q[k] - hi[k] : 0.0f);
+        d2 += d * d;
+    }
+    return b.z / fmaxf(d2, 1e-4f);
+}
+
+// LightBVH::Sample (LightBVH.cpp:423-482): from the root, pick a child in
+// proportion to its importance, reusing the rescaled random number; returns
+// the luminary and its selection probability (0: nothing to pick).
+__device__ int SampleLightBvh(const PtLightNode* __restrict__ nodes, V3 p, float xi, float& pdf)
+{
+    pdf = 1.0f;
+    int i = 0;
+    for (int guard = 0; guard < 64; ++guard) {
+        const int4 c = __ldg(reinterpret_cast<const int4*>(nodes + i) + 2);   // light, count, start, pad
+        if (c.y <= 1) return c.x;
+        const int right = __float_as_int(__ldg(reinterpret_cast<const float4*>(nodes + i) + 1).w);
+        const float il = LightImportance(nodes, i + 1, p), ir = LightImportance(nodes, right, p);
+        const float total = il + ir;
+        if (!(total > 0.0f)) { pdf = 0.0f; return -1; }
+        const float pl = il / total;
+        if (xi < pl) {
+            pdf *= pl;
+            xi = xi / pl;
+            i = i + 1;
+        } else {
+            pdf *= 1.0f - pl;
+            xi = (xi - pl) / (1.0f - pl);
+            i = right;
+        }
+    }
+    pdf = 0.0f;
+    return -1;
+}
+
+// LightBVH::Pdf (LightBVH.cpp:484-531): the probability that SampleLightBvh
+// picks the luminary at leaf position `pos` from p.
+__device__ float LightBvhPdf(const PtLightNode* __restrict__ nodes, int pos, V3 p)
+{
+    float pdf = 1.0f;
+    int i = 0;
+    for (int guard = 0; guard < 64; ++guard) {
+        const int4 c = __ldg(reinterpret_cast<const int4*>(nodes + i) + 2);
+        if (c.y <= 1) return pdf;
+        const int right = __float_as_int(__ldg(reinterpret_cast<const float4*>(nodes + i) + 1).w);
+        const float il = LightImportance(nodes, i + 1, p), ir = LightImportance(nodes, right, p);
+        const float total = il + ir;
+        if (!(total > 0.0f)) return 0.0f;
+        const float pl = il / total;
+        const int4 lc = __ldg(reinterpret_cast<const int4*>(nodes + i + 1) + 2);
+        if (pos >= lc.z && pos < lc.z + lc.y) {
+            pdf *= pl;
+            i = i + 1;
+        } else {
+            pdf *= 1.0f - pl;
+            i = right;
+        }
+    }
+    return 0.0f;
+}
+
 // ---- film ------------------------------------------------------------------
 
 // XYZ of one finished sample: sum over active wavelengths of
@@ -75,13 +149,13 @@ __device__ __forceinline__ void Splat(const PtPaths& P, const PtJobDev& J, int s
         return;
     }
     // FilteredFilm::Splat (Rendering/FilteredFilm.cpp:42-98): the sample's
-    // screen position (uniform in its pixel, pixel centres on integer
-    // coordinates) adds w XYZ and w to every pixel within the Gaussian's
+    // screen position (the camera's, see KRegen: uniform in its pixel, pixel
+    // centres on integer coordinates) adds w XYZ and w to every pixel within the Gaussian's
     // support, w = exp(-r^2 / 2 sigma^2) / (2 pi sigma^2)
     // (GaussianPixelFilter.h:67-78).
     const int W = J.cam.width, H = J.cam.height;
     const int px = (int)(m.x % (uint32_t)W), py = (int)(m.x / (uint32_t)W);
-    const float sx = (float)px + Rand(m.w, 0) - 0.5f, sy = (float)py + Rand(m.w, 1) - 0.5f;
+    const float sx = (float)px + Rand(m.w, 0) - 0.5f, sy = (float)py + 0.5f - Rand(m.w, 1);
     const float hw = S.filt_half;
     const int x0 = max(0, (int)floorf(sx - hw)), x1 = min(W - 1, (int)floorf(sx + hw));
     const int y0 = max(0, (int)floorf(sy - hw)), y1 = min(H - 1, (int)floorf(sy + hw));
@@ -238,20 +312,26 @@ KRegen(const PtJobDev* __restrict__ jobs, PtPaths P, PtQueues Q, int assign)
                 const uint32_t sample = (uint32_t)(J.sample_begin + g / (unsigned long long)J.npix);
                 const uint32_t key = PathKey(J.set.seed, pixel, sample);
                 const int px = (int)(pixel % (uint32_t)J.cam.width), py = (int)(pixel / (uint32_t)J.cam.width);
-                // Box pixel filter of width 1 (and the splatted Gaussian):
-                // uniform jitter inside the pixel.  A Gaussian too narrow for
-                // the filtered film moves the sample about the pixel centre by
-                // the truncated kernel's inverse CDF (GaussianPixelFilter.h:109-127).
-                float ox = Rand(key, 0), oy = Rand(key, 1);
+                // Screen position in pixel units, pixel centres on integer
+                // coordinates, rows counted downwards: the reference's
+                // ptOnScreen = (x + u - 1/2, (height - y) + v - 1/2) for the
+                // box filter and the filtered film
+                // (PathTracingSpectralRasterizer.cpp:321-331, BoxPixelFilter.h:54-58),
+                // or the pixel centre moved by the truncated Gaussian's
+                // inverse CDF for a narrow Gaussian (GaussianPixelFilter.h:109-127).
+                const float ox = Rand(key, 0), oy = Rand(key, 1);
+                float fx, fy;
                 if (J.set.filter == kFilterWarp) {
                     const float v = fmaxf(J.set.filt_trunc + (1.0f - J.set.filt_trunc) * ox, 1e-30f);
                     const float r = J.set.filt_sigma * sqrtf(-2.0f * logf(v));
                     float sn, cs;
                     sincospif(2.0f * oy, &sn, &cs);
-                    ox = 0.5f + r * cs;
-                    oy = 0.5f + r * sn;
+                    fx = (float)px + r * cs;
+                    fy = (float)py - r * sn;
+                } else {
+                    fx = (float)px + ox - 0.5f;
+                    fy = (float)py + 0.5f - oy;
                 }
-                const float fx = (float)px + ox, fy = (float)py + oy;
                 const float sx = 2.0f * fx / (float)J.cam.width - 1.0f;
                 const float sy = 1.0f - 2.0f * fy / (float)J.cam.height;
                 const V3 d = normalize(mk(J.cam.fwd[0] + sx * J.cam.right[0] + sy * J.cam.up[0],
@@ -383,9 +463,9 @@ __device__ __forceinline__ void PushShadow(const PtQueues& Q, V3 o, V3 d, float 
 // the GGX pair, or for Lambertian the same-side gate and pdf |nv|/pi
 // (LambertianBRDF::valueNM + LambertianSPF::Pdf, ShouldReflect at
 // LambertianBRDF.cpp:44-75).  The sampling pdf is wavelength-independent.
-__device__ __forceinline__ GgxPair NeePair(const PtMaterial& M, const GgxPoint& gp, V3 ns, V3 ng, V3 r, V3 v)
+__device__ __forceinline__ GgxPair NeePair(int mtype, const GgxPoint& gp, V3 ns, V3 ng, V3 r, V3 v)
 {
-    if (M.type == kMatGGX) return GgxPairAt(gp, dot(r, ns) < 0.0f ? -ns : ns, ng, r, v);
+    if (mtype == kMatGGX) return GgxPairAt(gp, dot(r, ns) < 0.0f ? -ns : ns, ng, r, v);
     GgxPair q;
     const float nr = dot(ns, r), nv = dot(ns, v);
     const bool same = (nr >= kNearZero && nv >= kNearZero) || (nr <= -kNearZero && nv <= -kNearZero);
@@ -396,11 +476,11 @@ __device__ __forceinline__ GgxPair NeePair(const PtMaterial& M, const GgxPoint& 
 }
 
 // The BSDF value at one wavelength for a next-event pair.
-__device__ __forceinline__ float NeeValue(const PtMaterial& M, const float* spectra, float lam, const GgxPair& q,
-                                          float eavg)
+__device__ __forceinline__ float NeeValue(int mtype, const PtMaterial& M, const float* spectra, float lam,
+                                          const GgxPair& q, float eavg)
 {
     if (!q.ok) return 0.0f;
-    if (M.type == kMatGGX) return GgxValueAt(q, GgxAt(M, spectra, lam), eavg);
+    if (mtype == kMatGGX) return GgxValueAt(q, GgxAt(M, spectra, lam), eavg);
     return Spec(spectra, M.refl, lam) * kInvPi;
 }
 
@@ -432,17 +512,19 @@ KClassify(const PtJobDev* __restrict__ jobs, PtPaths P, PtQueues Q)
     }
 }
 
-// classified: the paths come from KClassify's class ranges, else straight from
-// the active queue (scenes with one shading class skip the sort).
-__global__ void __launch_bounds__(kShadeBlock)
-KShade(const PtJobDev* __restrict__ jobs, PtPaths P, PtQueues Q, int classified)
+// CLS >= 0: every path to shade escaped or hit a material of shading class
+// CLS (0 Lambertian, 1 GGX, 2 dielectric), so the other models' code is left
+// out and the kernel needs fewer registers; the paths come from KClassify's
+// queue of that class (from_class) or, for scenes of one class, straight from
+// the active queue.  CLS = -1 shades any material from the active queue.
+template <int CLS>
+__global__ void __launch_bounds__(kShadeBlock, CLS == 1 || CLS < 0 ? 2 : 3)
+KShade(const PtJobDev* __restrict__ jobs, PtPaths P, PtQueues Q, int from_class)
 {
-    const int c0 = Q.cnt[kCntClass], c1 = Q.cnt[kCntClass + 1];
-    const int n = classified ? c0 + c1 + Q.cnt[kCntClass + 2] : Q.cnt[kCntActive];
+    const int n = (CLS >= 0 && from_class) ? Q.cnt[kCntClass + (CLS < 0 ? 0 : CLS)] : Q.cnt[kCntActive];
+    const int* __restrict__ src = (CLS >= 0 && from_class) ? Q.shade + (CLS < 0 ? 0 : CLS) * Q.capacity : Q.active;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const int slot = !classified ? Q.active[i]
-                       : i < c0 ? Q.shade[i]
-                       : (i < c0 + c1 ? Q.shade[Q.capacity + (i - c0)] : Q.shade[2 * Q.capacity + (i - c0 - c1)]);
+        const int slot = src[i];
         const float4 aux = P.aux[slot];
         const PtJobDev& J = jobs[__float_as_int(aux.z)];
         const PtScene& S = J.scene;
@@ -498,6 +580,7 @@ KShade(const PtJobDev* __restrict__ jobs, PtPaths P, PtQueues Q, int classified)
             if ((at.mat & kAttrDoubleSided) && dot(ng, d) > 0.0f) ng = -ng;
             const V3 gnv = dot(ng, d) < 0.0f ? ng : -ng;   // geometric normal facing the ray
             const PtMaterial M = S.mats[mi];
+            const int mtype = CLS < 0 ? M.type : CLS;
 
             // PART 1: emission with MIS against light sampling (:4424-4518).
             if (M.emit >= 0 && (m.z & kFlagConsiderEmission) && dot(-d, ng) > 0.0f) {
@@ -505,7 +588,10 @@ KShade(const PtJobDev* __restrict__ jobs, PtPaths P, PtQueues Q, int classified)
                 if (bsdfPdf > 0.0f && at.light >= 0) {
                     const PtLight lg = S.lights[at.light];
                     const float cosL = fabsf(dot(d, ng));
-                    if (cosL > 0.0f && lg.area > 0.0f) w = PowerHeuristic(bsdfPdf, lg.pdf * (t * t) / (lg.area * cosL));
+                    // Selection probability from the previous vertex (the ray's origin).
+                    const float psel = (set.light_bvh && S.light_nodes) ? LightBvhPdf(S.light_nodes, lg.bvh_pos, xyz(ro))
+                                                                         : lg.pdf;
+                    if (cosL > 0.0f && lg.area > 0.0f) w = PowerHeuristic(bsdfPdf, psel * (t * t) / (lg.area * cosL));
                 }
                 for (int k = 0; k < 4; ++k)
                     if (!(term & (1u << k))) Set(L, k, Get(L, k) + Get(thr, k) * Spec(S.spectra, M.emit, lam[k]) * w);
@@ -516,7 +602,7 @@ KShade(const PtJobDev* __restrict__ jobs, PtPaths P, PtQueues Q, int classified)
             float npdf = 0.0f;       // continuation pdf for the next emission MIS (0 = delta)
             unsigned nflags = kFlagConsiderEmission;
 
-            if (M.type == kMatDielectric) {
+            if (mtype == kMatDielectric) {
                 // Smooth dielectric: Fresnel choice between reflection and
                 // refraction (DielectricSPF.cpp:120-300).  With a constant index
                 // every wavelength follows the hero's direction with the same
@@ -542,7 +628,7 @@ KShade(const PtJobDev* __restrict__ jobs, PtPaths P, PtQueues Q, int classified)
                 const V3 ns = ng;
                 const V3 r = -d;
                 GgxPoint gp{1.0f, 0.0f, 0.0f, 0.0f};
-                if (M.type == kMatGGX) gp = GgxPointAt(M.alpha, fabsf(dot(r, ns)));
+                if (mtype == kMatGGX) gp = GgxPointAt(M.alpha, fabsf(dot(r, ns)));
                 // PART 2: next-event estimation (LightSampler::EvaluateDirectLightingNM,
                 // LightSampler.cpp:1942-2361): one area-light sample and one sky
                 // sample per wavelength (reference) or one shared sample.
@@ -553,14 +639,19 @@ KShade(const PtJobDev* __restrict__ jobs, PtPaths P, PtQueues Q, int classified)
                     if (set.n_lights > 0) {
                         const float ul = Rand(key, Dim(depth, 4 * k + 0));
                         int li = 0;
-                        {
+                        float psel;
+                        if (set.light_bvh && S.light_nodes) {
+                            li = SampleLightBvh(S.light_nodes, p, ul, psel);
+                        } else {
                             float acc = 0.0f;
                             for (li = 0; li < set.n_lights - 1; ++li) {
                                 acc += S.lights[li].pdf;
                                 if (ul < acc) break;
                             }
+                            psel = S.lights[li].pdf;
                         }
-                        if (li != at.light) {   // no self-illumination
+                        // No sample when nothing can be picked, nor from a luminary to itself.
+                        if (li >= 0 && li != at.light && psel > 0.0f) {
                             const PtLight lg = S.lights[li];
                             const float ux = Rand(key, Dim(depth, 4 * k + 1));
                             const float uy = Rand(key, Dim(depth, 4 * k + 2));
@@ -583,17 +674,17 @@ KShade(const PtJobDev* __restrict__ jobs, PtPaths P, PtQueues Q, int classified)
                             const float cosL = dot(-toL, nl);
                             if (cosL > 0.0f && cosS > 0.0f) {
                                 const float geom = lg.area * cosL / (dist * dist);
-                                const float plight = lg.pdf * (dist * dist) / (lg.area * cosL);
+                                const float plight = psel * (dist * dist) / (lg.area * cosL);
                                 float4 c = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
                                 bool any = false;
-                                const GgxPair bq = NeePair(M, gp, ns, gnv, r, toL);
+                                const GgxPair bq = NeePair(mtype, gp, ns, gnv, r, toL);
                                 const float pb = bq.pdf;
                                 #pragma unroll 1
                                 for (int j = 0; j < 4; ++j) {
                                     if (term & (1u << j)) continue;
                                     if (set.nee_per_lambda && j != k) continue;
-                                    const float f = NeeValue(M, S.spectra, lam[j], bq, gp.eavg);
-                                    const float w = (pb > 0.0f ? PowerHeuristic(plight, pb) : 1.0f) / lg.pdf;
+                                    const float f = NeeValue(mtype, M, S.spectra, lam[j], bq, gp.eavg);
+                                    const float w = (pb > 0.0f ? PowerHeuristic(plight, pb) : 1.0f) / psel;
                                     const float v = Get(thr, j) * Spec(S.spectra, lg.emit, lam[j]) * cosS * geom * f * w;
                                     Set(c, j, v);
                                     any |= v != 0.0f;
@@ -615,13 +706,13 @@ KShade(const PtJobDev* __restrict__ jobs, PtPaths P, PtQueues Q, int classified)
                         if (cosE > 0.0f) {
                             float4 c = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
                             bool any = false;
-                            const GgxPair bq = NeePair(M, gp, ns, gnv, r, dir);
+                            const GgxPair bq = NeePair(mtype, gp, ns, gnv, r, dir);
                             const float pb = bq.pdf;
                             #pragma unroll 1
                             for (int j = 0; j < 4; ++j) {
                                 if (term & (1u << j)) continue;
                                 if (set.nee_per_lambda && j != k) continue;
-                                const float f = NeeValue(M, S.spectra, lam[j], bq, gp.eavg);
+                                const float f = NeeValue(mtype, M, S.spectra, lam[j], bq, gp.eavg);
                                 const float w = pb > 0.0f ? PowerHeuristic(kInv4Pi, pb) : 1.0f;
                                 const float v = Get(thr, j) * Spec(S.spectra, set.env, lam[j]) * f * cosE / kInv4Pi * w;
                                 Set(c, j, v);
@@ -638,7 +729,7 @@ KShade(const PtJobDev* __restrict__ jobs, PtPaths P, PtQueues Q, int classified)
                 V3 tx, ty;
                 Basis(w, tx, ty);
                 const float u1 = Rand(key, Dim(depth, 16)), u2 = Rand(key, Dim(depth, 17));
-                if (M.type == kMatGGX) {
+                if (mtype == kMatGGX) {
                     const GgxParams g0 = GgxAt(M, S.spectra, lam[0]);
                     const float cosR = dot(r, w);
                     const float ws = g0.spec;
@@ -903,8 +994,20 @@ cudaError_t PtIteration(const PtLaunch& L, int iter, cudaStream_t st)
     cudaMemsetAsync(L.queues.trace_ctr, 0, 2 * sizeof(unsigned long long), st);
     if (L.layout == RTB200_BVH_Q8) LaunchTrace<QNode4>(L, st, true);
     else LaunchTrace<GpuNode4>(L, st, true);
-    if (L.classify) KClassify<<<shadeGrid, kShadeBlock, 0, st>>>(L.jobs, L.paths, L.queues);
-    KShade<<<shadeGrid, kShadeBlock, 0, st>>>(L.jobs, L.paths, L.queues, L.classify ? 1 : 0);
+    if (L.classify) {
+        KClassify<<<shadeGrid, kShadeBlock, 0, st>>>(L.jobs, L.paths, L.queues);
+        KShade<0><<<shadeGrid, kShadeBlock, 0, st>>>(L.jobs, L.paths, L.queues, 1);
+        KShade<1><<<shadeGrid, kShadeBlock, 0, st>>>(L.jobs, L.paths, L.queues, 1);
+        KShade<2><<<shadeGrid, kShadeBlock, 0, st>>>(L.jobs, L.paths, L.queues, 1);
+    } else if (L.shade_class == 0) {
+        KShade<0><<<shadeGrid, kShadeBlock, 0, st>>>(L.jobs, L.paths, L.queues, 0);
+    } else if (L.shade_class == 1) {
+        KShade<1><<<shadeGrid, kShadeBlock, 0, st>>>(L.jobs, L.paths, L.queues, 0);
+    } else if (L.shade_class == 2) {
+        KShade<2><<<shadeGrid, kShadeBlock, 0, st>>>(L.jobs, L.paths, L.queues, 0);
+    } else {
+        KShade<-1><<<shadeGrid, kShadeBlock, 0, st>>>(L.jobs, L.paths, L.queues, 0);
+    }
     if (L.layout == RTB200_BVH_Q8) LaunchTrace<QNode4>(L, st, false);
     else LaunchTrace<GpuNode4>(L, st, false);
     KSwap<<<1, 1, 0, st>>>(L.queues.cnt);

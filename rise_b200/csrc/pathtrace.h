@@ -17,6 +17,7 @@ struct PtLaunch {
     bool spill;        // some job's BVH needs the local-memory stack continuation
     bool uniform;      // every job renders `scene`
     bool classify;     // some job's scene mixes shading classes: sort paths before shading
+    int shade_class;   // without sorting: the one shading class of every job's scene, or -1
     PtScene scene;
     PtPaths paths;
     PtQueues queues;

@@ -34,6 +34,69 @@ int Upload(rtb200_ctx* ctx, T** dst, const std::vector<T>& src, size_t& total)
     return RTB200_OK;
 }
 
+// Light BVH over the luminaries (LightBVH::Build / BuildRecursive,
+// Lights/LightBVH.cpp:219-421): each luminary is a primitive with its
+// bounding box (degenerate axes widened by 1e-12, BoundingBox::EnsureBoxHasVolume)
+// and its selection power; a node holds the union box and the summed power;
+// a node of several primitives splits them on the widest axis of their box
+// centres at the power-weighted mean centre (std::partition; the middle
+// index when one side is empty or the extent is below 1e-10); nodes in
+// preorder.  Luminaries are area emitters, whose cones are full spheres.
+struct LightPrim {
+    double lo[3], hi[3], c[3];
+    double power;
+    int light;
+};
+
+int BuildLightNodes(std::vector<LightPrim>& prims, int start, int end, int& pos, std::vector<PtLightNode>& nodes,
+                    std::vector<PtLight>& lights)
+{
+    const int idx = (int)nodes.size();
+    nodes.emplace_back();
+    PtLightNode n{};
+    double lo[3], hi[3], power = prims[start].power;
+    for (int k = 0; k < 3; ++k) { lo[k] = prims[start].lo[k]; hi[k] = prims[start].hi[k]; }
+    for (int i = start + 1; i < end; ++i) {
+        for (int k = 0; k < 3; ++k) { lo[k] = std::min(lo[k], prims[i].lo[k]); hi[k] = std::max(hi[k], prims[i].hi[k]); }
+        power += prims[i].power;
+    }
+    for (int k = 0; k < 3; ++k) { n.lo[k] = (float)lo[k]; n.hi[k] = (float)hi[k]; }
+    n.power = (float)power;
+    n.count = end - start;
+    n.start = pos;
+    if (end - start == 1) {
+        n.light = prims[start].light;
+        lights[n.light].bvh_pos = pos++;
+        nodes[idx] = n;
+        return idx;
+    }
+    double clo[3], chi[3];
+    for (int k = 0; k < 3; ++k) clo[k] = chi[k] = prims[start].c[k];
+    for (int i = start + 1; i < end; ++i)
+        for (int k = 0; k < 3; ++k) { clo[k] = std::min(clo[k], prims[i].c[k]); chi[k] = std::max(chi[k], prims[i].c[k]); }
+    const double ex[3] = {chi[0] - clo[0], chi[1] - clo[1], chi[2] - clo[2]};
+    int axis = 0;
+    if (ex[1] > ex[0]) axis = 1;
+    if (ex[2] > (axis == 0 ? ex[0] : ex[1])) axis = 2;
+    int mid;
+    if (ex[axis] < 1e-10) {
+        mid = start + (end - start) / 2;
+    } else {
+        double ws = 0.0, tp = 0.0;
+        for (int i = start; i < end; ++i) { ws += prims[i].c[axis] * prims[i].power; tp += prims[i].power; }
+        const double split = tp > 0.0 ? ws / tp : 0.5 * (clo[axis] + chi[axis]);
+        auto it = std::partition(prims.begin() + start, prims.begin() + end,
+                                 [&](const LightPrim& p) { return p.c[axis] < split; });
+        mid = (int)(it - prims.begin());
+        if (mid == start || mid == end) mid = start + (end - start) / 2;
+    }
+    nodes[idx] = n;
+    BuildLightNodes(prims, start, mid, pos, nodes, lights);
+    nodes[idx].right = (int)nodes.size();
+    BuildLightNodes(prims, mid, end, pos, nodes, lights);
+    return idx;
+}
+
 }  // namespace
 
 int UploadShading(rtb200_scene* s)
@@ -42,6 +105,7 @@ int UploadShading(rtb200_scene* s)
     if (s->materials.empty()) return RTB200_OK;  // ray casting only
     const size_t nm = s->materials.size();
     for (const PtMaterial& m : s->materials) s->mixed_shading |= m.type != s->materials[0].type;
+    s->shade_class = s->mixed_shading ? -1 : s->materials[0].type;
     // GGX conductors: tabulate F_avg(lambda) on the 5 nm grid as an extra
     // spectrum, and make sure the device holds the E_ss / E_avg tables.
     for (PtMaterial& m : s->materials) {
@@ -68,6 +132,7 @@ int UploadShading(rtb200_scene* s)
     s->light_tris.clear();
     std::vector<int> meshLight(s->meshes.size(), -1);
     std::vector<double> weight;
+    std::vector<LightPrim> boxes;
     for (size_t mi = 0; mi < s->meshes.size(); ++mi) {
         const auto& mesh = s->meshes[mi];
         const PtMaterial& mat = s->materials[mesh.material];
@@ -78,8 +143,14 @@ int UploadShading(rtb200_scene* s)
         L.emit = mat.emit;
         double area = 0.0;
         std::vector<double> cum;
+        LightPrim box{};
+        for (int k = 0; k < 3; ++k) { box.lo[k] = INFINITY; box.hi[k] = -INFINITY; }
         for (int64_t t = mesh.first; t < mesh.first + mesh.count; ++t) {
             const float* v = &s->tri9[9 * (size_t)t];
+            for (int j = 0; j < 9; ++j) {
+                box.lo[j % 3] = std::min(box.lo[j % 3], (double)v[j]);
+                box.hi[j % 3] = std::max(box.hi[j % 3], (double)v[j]);
+            }
             PtLightTri lt{};
             for (int k = 0; k < 3; ++k) { lt.v0[k] = v[k]; lt.e1[k] = v[3 + k] - v[k]; lt.e2[k] = v[6 + k] - v[k]; }
             const double cx = (double)lt.e1[1] * lt.e2[2] - (double)lt.e1[2] * lt.e2[1];
@@ -98,12 +169,30 @@ int UploadShading(rtb200_scene* s)
         for (int k = 0; k < RTB200_CIE_COUNT; ++k) mean += s->spectra[(size_t)mat.emit * RTB200_CIE_COUNT + k];
         mean /= RTB200_CIE_COUNT;
         weight.push_back(area * std::max(mean, 1e-12));
+        boxes.push_back(box);
         meshLight[mi] = (int)s->lights.size();
         s->lights.push_back(L);
     }
     double wsum = 0.0;
     for (double w : weight) wsum += w;
     for (size_t i = 0; i < s->lights.size(); ++i) s->lights[i].pdf = (float)(weight[i] / wsum);
+    s->light_nodes.clear();
+    if (s->lights.size() > 1) {
+        std::vector<LightPrim> prims(s->lights.size());
+        for (size_t i = 0; i < s->lights.size(); ++i) {
+            LightPrim& q = prims[i];
+            q = boxes[i];
+            for (int k = 0; k < 3; ++k) {
+                if (q.lo[k] == q.hi[k]) { q.lo[k] -= 1e-12; q.hi[k] += 1e-12; }
+                q.c[k] = 0.5 * (q.lo[k] + q.hi[k]);
+            }
+            q.power = weight[i];
+            q.light = (int)i;
+        }
+        int pos = 0;
+        s->light_nodes.reserve(2 * prims.size());
+        BuildLightNodes(prims, 0, (int)prims.size(), pos, s->light_nodes, s->lights);
+    }
     // Per-triangle attributes in leaf order.
     const size_t ntri = s->tri_material.size();
     std::vector<int> triMesh(ntri);
@@ -148,6 +237,7 @@ int UploadShading(rtb200_scene* s)
     if (!rc) rc = Upload(ctx, &s->d_spectra, table, total);
     if (!rc) rc = Upload(ctx, &s->d_lights, s->lights, total);
     if (!rc) rc = Upload(ctx, &s->d_light_tris, s->light_tris, total);
+    if (!rc && !s->light_nodes.empty()) rc = Upload(ctx, &s->d_light_nodes, s->light_nodes, total);
     s->shade_bytes = total;
     if (rc) FreeShading(s);
     return rc;
@@ -161,6 +251,8 @@ void FreeShading(rtb200_scene* s)
     DevFree(ctx, s->d_spectra, s->spectra_table_bytes);
     DevFree(ctx, s->d_lights, s->lights.size() * sizeof(PtLight));
     DevFree(ctx, s->d_light_tris, s->light_tris.size() * sizeof(PtLightTri));
+    DevFree(ctx, s->d_light_nodes, s->light_nodes.size() * sizeof(PtLightNode));
+    s->d_light_nodes = nullptr;
     s->d_attr = nullptr;
     s->d_mats = nullptr;
     s->d_spectra = nullptr;

@@ -35,9 +35,24 @@ struct PtLight {
     int first;       // first entry in the light-triangle array
     int count;
     float area;      // total area of the luminary
-    float pdf;       // selection probability
+    float pdf;       // selection probability by power
     int emit;        // emitted radiance spectrum
-    int pad[3];
+    int bvh_pos;     // leaf position in the light BVH's order
+    int pad[2];
+};
+
+// Light BVH node (LightBVHNode, Lights/LightBVH.h:100-115), preorder: the
+// left child follows its parent, `right` is the right child's index.  A leaf
+// (count 1) holds luminary `light`; `start` is the subtree's first leaf
+// position.  Luminaries emit over the full sphere, so no cone is stored.
+struct PtLightNode {
+    float lo[3], hi[3];
+    float power;
+    int right;
+    int light;
+    int count;
+    int start;
+    int pad;
 };
 
 struct PtLightTri {
@@ -74,6 +89,7 @@ struct PtSettings {
     float filt_norm;         // 1 / (2 pi sigma^2)
     float filt_sigma;        // Gaussian sigma in pixels (warp mode)
     float filt_trunc;        // exp(-K^2 / 2), K = half-width / sigma (warp mode)
+    int light_bvh;           // pick NEE luminaries with the light BVH (when the scene has one)
 };
 
 // Film modes of PtSettings::filter.  The reference splats into a filtered
@@ -135,6 +151,7 @@ struct PtScene {
     const float* spectra;      // spectrum table: float4 header per id, then samples (Spec)
     const PtLight* lights;
     const PtLightTri* light_tris;
+    const PtLightNode* light_nodes;   // light BVH (null with fewer than two luminaries)
 };
 
 struct PtPaths {

@@ -29,7 +29,8 @@ class RenderSettings(ctypes.Structure):
                 ("max_depth", ctypes.c_int32), ("rr_min_depth", ctypes.c_int32), ("rr_threshold", ctypes.c_float),
                 ("nee_per_lambda", ctypes.c_int32), ("seed", ctypes.c_uint32), ("max_paths", ctypes.c_int32),
                 ("filter", ctypes.c_int32), ("filter_size", ctypes.c_float), ("filter_sigma", ctypes.c_float),
-                ("adaptive_max_spp", ctypes.c_int32), ("adaptive_threshold", ctypes.c_float)]
+                ("adaptive_max_spp", ctypes.c_int32), ("adaptive_threshold", ctypes.c_float),
+                ("light_selection", ctypes.c_int32)]
 
 
 class Stats(ctypes.Structure):
@@ -80,7 +81,8 @@ def settings_struct(st):
                           (ctypes.c_float * 3)(*st.cam_up), st.fov_deg, st.lambda_min, st.lambda_max, st.max_depth,
                           st.rr_min_depth, st.rr_threshold, st.nee_per_lambda, st.seed, st.max_paths,
                           getattr(st, "filter", 0), getattr(st, "filter_size", 2.0), getattr(st, "filter_sigma", 0.5),
-                          getattr(st, "adaptive_max_spp", 0), getattr(st, "adaptive_threshold", 0.01))
+                          getattr(st, "adaptive_max_spp", 0), getattr(st, "adaptive_threshold", 0.01),
+                          getattr(st, "light_selection", 0))
 
 
 class SpectralRasterizer:

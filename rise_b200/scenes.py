@@ -202,6 +202,7 @@ class RenderSettings:
     filter_sigma: float = 0.5 # Gaussian standard deviation in pixels
     adaptive_max_spp: int = 0       # adaptive sampling: maximum samples per pixel (0 = off)
     adaptive_threshold: float = 0.01  # adaptive sampling: relative standard error to converge
+    light_selection: int = 0  # 0 light BVH (more than one luminary), 1 by emitted power
 
 
 @dataclass

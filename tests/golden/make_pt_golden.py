@@ -152,6 +152,19 @@ def main():
         r.ref_pt_spectral_packet(pn, pa, len(nm), float(lo), float(hi), pq, len(q), po)
         rows.append([list(map(float, nm)), list(map(float, amp)), lo, hi, q.tolist(), o.tolist()])
     out["spectral_packet"] = rows
+    lrng = np.random.default_rng(77)
+    rows = []
+    for n in (2, 3, 7, 40):
+        pos = lrng.uniform(-1, 1, (n, 3))
+        if n == 7:
+            pos[:, 1] = 0.5                      # a flat row of lights (zero extent on one axis)
+        power = lrng.exponential(1.0, n)
+        pts = lrng.uniform(-1.5, 1.5, (25, 3))
+        xi = lrng.random(25)
+        picked, pdf, pdf_all = oracle.light_bvh(r, "ref_pt_", pos, power, pts, xi)
+        rows.append([pos.tolist(), power.tolist(), pts.tolist(), xi.tolist(), picked.tolist(), pdf.tolist(),
+                     pdf_all.tolist()])
+    out["light_bvh"] = rows
     out["gaussian_filter"] = [[s, g, dx, dy, r.ref_pt_gaussian_weight(s, g, dx, dy)]
                               for s, g in [(2.0, 0.5), (3.0, 1.0), (1.0, 0.3)]
                               for dx, dy in [(0, 0), (0.3, -0.2), (0.99, 0.5), (1.0, 0.0), (-1.01, 0.1), (1.4, 1.4)]]

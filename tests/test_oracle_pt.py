@@ -406,3 +406,26 @@ def test_random_spectral_painter_packets(ref):
                                    want.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
         got = scenes.spectral_painter(nm, amp, lo, hi).value_at(q)
         assert np.allclose(got, want, rtol=1e-7, atol=0)
+
+
+def test_golden_light_bvh(port):
+    """Light BVH build, stochastic pick and pdf against the reference's
+    LightBVH (point lights; one set lies in a plane)."""
+    for pos, power, pts, xi, picked, pdf, pdf_all in GOLDEN["light_bvh"]:
+        p, d, a = oracle.light_bvh(port, "orc_pt_", pos, power, pts, xi)
+        assert p.tolist() == picked
+        assert np.allclose(d, pdf, rtol=1e-12, atol=0) and np.allclose(a, pdf_all, rtol=1e-12, atol=0)
+        assert np.allclose(np.array(pdf_all).sum(axis=1), 1.0)
+
+
+def test_random_light_bvh(port, ref):
+    rng = np.random.default_rng(11)
+    for n in (2, 5, 16, 100, 333):
+        pos = rng.normal(size=(n, 3)) * rng.uniform(0.1, 10)
+        power = rng.exponential(1.0, n) * (rng.random(n) < 0.9)
+        pts = rng.normal(size=(60, 3)) * 3
+        xi = rng.random(60)
+        a = oracle.light_bvh(port, "orc_pt_", pos, power, pts, xi)
+        b = oracle.light_bvh(ref, "ref_pt_", pos, power, pts, xi)
+        assert np.array_equal(a[0], b[0])
+        assert np.allclose(a[1], b[1], rtol=1e-12, atol=0) and np.allclose(a[2], b[2], rtol=1e-12, atol=0)

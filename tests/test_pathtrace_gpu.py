@@ -223,6 +223,42 @@ def test_binned_spectral_packets_match_oracle(ctx):
     assert rel_mse(o, b) > 1e-4          # the packets' steps and range change the image
 
 
+def many_lights(light_selection):
+    """The Cornell box with five more small emitters of different power on
+    the walls and floor."""
+    d = scenes.cornell_box(48, 48)
+    d.settings = scenes.RenderSettings(**{**d.settings.__dict__, "light_selection": light_selection})
+    rng = np.random.default_rng(5)
+    for i in range(5):
+        e = d.add_spectrum(scenes.flat_spectrum(float(rng.uniform(2, 40)), 400, 700, 0.0))
+        m = d.add_material(scenes.Material(scenes.MAT_LAMBERTIAN, -1, e))
+        x, z = rng.uniform(0.1, 0.8, 2)
+        s = 0.08
+        y = 0.001
+        # on the floor, facing up
+        d.add_mesh(scenes._quad([x, y, z], [x, y, z + s], [x + s, y, z + s], [x + s, y, z]), m, False)
+    return d
+
+
+@pytest.mark.parametrize("light_selection", [0, 1])
+def test_many_lights_same_seed_matches_oracle(ctx, light_selection):
+    """Six luminaries: next-event luminaries picked by the light BVH (the
+    reference's default) or by power; device and oracle agree."""
+    d = many_lights(light_selection)
+    g, _ = render_gpu(ctx, d, 16)
+    o = oracle.pt_render(d, 16)
+    close = (np.abs(g - o) <= 1e-3 * (np.abs(o) + 1e-3)).all(axis=2)
+    assert close.mean() > 0.95, close.mean()
+    assert rel_mse(g, o) < 1e-3
+
+
+def test_light_bvh_and_power_selection_converge_to_the_same_image(ctx):
+    a, _ = render_gpu(ctx, many_lights(0), 1024)
+    b, _ = render_gpu(ctx, many_lights(1), 1024)
+    assert abs(a[..., 1].mean() / b[..., 1].mean() - 1) < 5e-3
+    assert rel_mse(a, b) < 2e-2
+
+
 def small_spheres(nee_per_lambda=1):
     return scenes.spheres_scene(grid=64, n_spheres=8, sphere_tris=800, width=64, height=64,
                                 nee_per_lambda=nee_per_lambda)
