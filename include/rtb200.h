@@ -173,6 +173,27 @@ int rtb200_scene_add_material(rtb200_scene* scene, const rtb200_material* m, int
  * rtb200_scene_add_spectrum. */
 int rtb200_scene_add_spectral_packet(rtb200_scene* scene, float lambda_begin, float lambda_end, int32_t n,
                                      const float* amplitudes, int32_t* id_out);
+
+/* RGB colours as spectra, as the reference's RGB painters evaluate them
+ * (UniformColorPainter::GetColorNM, Painters/UniformColorPainter.h:40-76):
+ * the Jakob-Hanika sigmoid polynomial of the colour in linear Rec.709,
+ * S(l) = scale * s(c0 t^2 + c1 t + c2), t = (l - 380) / 400, 0 outside
+ * 380..780 nm, s(x) = 1/2 + x / (2 sqrt(1 + x^2)).  ALBEDO clamps the colour
+ * to [0, 1] (scale 1; RGBAlbedoSpectrum, the reference painters' default);
+ * UNBOUNDED divides it by its largest channel, which becomes the scale
+ * (RGBUnboundedSpectrum).  rtb200_rgb_uplift writes (c0, c1, c2, scale) and
+ * needs no device; its coefficient table is built on first use (a few seconds
+ * on all host cores) by the reference's generator steps
+ * (tools/JakobHanikaLUTGen.cpp, Rec.709, 64^3 cells per largest channel).
+ * rtb200_rgb_uplift_table copies that table (3 * 64^3 cells of c0, c1, c2,
+ * floats, ordered [largest channel][z][x][y]).  rtb200_scene_add_rgb_spectrum
+ * adds such a spectrum to a scene's table (id space of
+ * rtb200_scene_add_spectrum). */
+#define RTB200_RGB_ALBEDO 0
+#define RTB200_RGB_UNBOUNDED 1
+int rtb200_rgb_uplift(const double* rgb, int32_t kind, double* coeffs_and_scale);
+int rtb200_rgb_uplift_table(float* coeffs);
+int rtb200_scene_add_rgb_spectrum(rtb200_scene* scene, const double* coeffs_and_scale, int32_t* id_out);
 /* Uniform sky: radiance spectrum for rays that escape (-1 = none); visible
  * selects whether camera rays see it directly. */
 int rtb200_scene_set_environment(rtb200_scene* scene, int32_t spectrum, int32_t visible);

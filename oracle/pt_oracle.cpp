@@ -486,6 +486,13 @@ inline double Spec(const Scene& S, int id, double nm)
 {
     if (id < 0) return 0.0;
     const SpecHeader h = Header(S.spectra, id);
+    if (h.n < 0.0) {
+        // RGBSigmoidPolynomial::Eval (Utilities/Color/RGBSigmoidPolynomial.h:58-70) x scale.
+        if (nm < 380.0 || nm > 780.0) return 0.0;
+        const double t = (nm - 380.0) / 400.0;
+        const double x = (double)h.s[0] * t * t + (double)h.s[1] * t + (double)h.s[2];
+        return (double)h.s[3] * (0.5 + x / (2.0 * std::sqrt(1.0 + x * x)));
+    }
     if (h.n == 0.0) {
         int i, j;
         double w;
@@ -500,6 +507,11 @@ inline double Spec(const Scene& S, int id, double nm)
 inline double GridValue(const float* table, int id, int k)
 {
     const SpecHeader h = Header(table, id);
+    if (h.n < 0.0) {
+        const double t = (5.0 * k) / 400.0;
+        const double x = (double)h.s[0] * t * t + (double)h.s[1] * t + (double)h.s[2];
+        return (float)((double)h.s[3] * (0.5 + x / (2.0 * std::sqrt(1.0 + x * x))));
+    }
     if (h.n == 0.0) return h.s[k];
     const double nm = 380.0 + 5.0 * k;
     if (nm < h.begin || nm > h.end) return 0.0;

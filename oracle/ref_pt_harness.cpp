@@ -28,6 +28,7 @@
 #include "Rendering/DisplayTransform.h"
 #include "Lights/LightSampler.h"
 #include "Lights/LightBVH.h"
+#include "Utilities/Color/RGBSpectra.h"
 #include "Interfaces/IFunction2D.h"
 #include "Utilities/PiecewiseLinearFunction.h"
 #include "Utilities/Color/SpectralPacket.h"
@@ -67,6 +68,15 @@ namespace RISE
 }
 
 using namespace RISE;
+
+// The baked table the reference's singleton would load is generated code
+// that the harness does not build; tables are loaded from memory instead.
+namespace RISE
+{
+	extern const unsigned int kSpectrumLUTResolution = 0;
+	extern const unsigned int kSpectrumLUTNumFloats = 0;
+	extern const float kSpectrumLUTFloats[1] = {0.0f};
+}
 
 namespace {
 inline Vector3 V(const double* p) { return Vector3(p[0], p[1], p[2]); }
@@ -217,6 +227,32 @@ void ref_pt_light_bvh(int n, const double* pos, const double* power, int m, cons
         pdf[q] = pd;
         for (int i = 0; i < n; ++i) pdf_all[(size_t)q * n + i] = bvh.Pdf((unsigned)i, p, Vector3(0, 1, 0));
     }
+}
+
+// RGB -> spectrum with the reference's table code over a table given in
+// memory (the body of its generator's .coeff file): the albedo sigmoid's
+// coefficients, and the spectrum of the given kind (0 albedo, 1 unbounded)
+// at the query wavelengths.
+int ref_pt_rgb_uplift(const float* table, unsigned n_floats, const double* rgb, int kind, const double* nm, int nq,
+                      double* coeffs, double* values)
+{
+    static RGBToSpectrumTable t;
+    static const float* loaded = nullptr;
+    if (loaded != table) {
+        if (!t.LoadFromMemory(64, table, n_floats)) return 0;
+        loaded = table;
+    }
+    const RISEPel p(rgb[0], rgb[1], rgb[2]);
+    const RGBSigmoidPolynomial poly = t(LUTTargetPel(p));
+    coeffs[0] = poly.c0; coeffs[1] = poly.c1; coeffs[2] = poly.c2;
+    if (kind == 0) {
+        const RGBAlbedoSpectrum s = RGBAlbedoSpectrum::FromRGB(p, t);
+        for (int i = 0; i < nq; ++i) values[i] = s.Eval(nm[i]);
+    } else {
+        const RGBUnboundedSpectrum s = RGBUnboundedSpectrum::FromRGB(p, t);
+        for (int i = 0; i < nq; ++i) values[i] = s.Eval(nm[i]);
+    }
+    return 1;
 }
 
 double ref_pt_gaussian_weight(double size, double sigma, double dx, double dy)

@@ -57,6 +57,12 @@ struct rtb200_scene {
         std::vector<float> amps;
     };
     std::vector<Packet> packets;
+    // RGB colours' sigmoid polynomials: spectrum id -> c0, c1, c2, scale.
+    struct Sigmoid {
+        int32_t id;
+        float c[4];
+    };
+    std::vector<Sigmoid> sigmoids;
     size_t spectra_table_bytes = 0;
     std::vector<rtb200::PtMaterial> materials;
     bool mixed_shading = false;      // materials of more than one shading class

@@ -213,12 +213,19 @@ int UploadShading(rtb200_scene* s)
     {
         const size_t nspec = s->spectra.size() / RTB200_CIE_COUNT;
         std::vector<const rtb200_scene::Packet*> packet(nspec, nullptr);
+        std::vector<const rtb200_scene::Sigmoid*> sigmoid(nspec, nullptr);
         for (const auto& p : s->packets) packet[p.id] = &p;
+        for (const auto& q : s->sigmoids) sigmoid[q.id] = &q;
         table.resize(4 * nspec);
         for (size_t id = 0; id < nspec; ++id) {
             const int32_t off = (int32_t)table.size();
             float* h = &table[4 * id];
-            if (packet[id]) {
+            if (sigmoid[id]) {
+                h[0] = -1.0f;
+                h[1] = 380.0f;
+                h[2] = 780.0f;
+                table.insert(table.end(), sigmoid[id]->c, sigmoid[id]->c + 4);
+            } else if (packet[id]) {
                 h[0] = (float)packet[id]->amps.size();
                 h[1] = packet[id]->begin;
                 h[2] = packet[id]->end;
@@ -308,6 +315,28 @@ int rtb200_scene_add_spectral_packet(rtb200_scene* s, float lambda_begin, float 
     }
     *id_out = p.id;
     s->packets.push_back(std::move(p));
+    return RTB200_OK;
+}
+
+int rtb200_scene_add_rgb_spectrum(rtb200_scene* s, const double* cs, int32_t* id_out)
+{
+    if (!s || !cs || !id_out) return RTB200_E_INVALID;
+    std::lock_guard<std::mutex> g(s->ctx->mu);
+    if (s->committed) return SetError(s->ctx, RTB200_E_INVALID, "scene already committed");
+    for (int k = 0; k < 4; ++k)
+        if (!std::isfinite(cs[k])) return SetError(s->ctx, RTB200_E_INVALID, "sigmoid coefficients must be finite");
+    if (cs[3] < 0.0) return SetError(s->ctx, RTB200_E_INVALID, "spectrum scale must be non-negative");
+    rtb200_scene::Sigmoid q;
+    q.id = (int32_t)(s->spectra.size() / RTB200_CIE_COUNT);
+    for (int k = 0; k < 4; ++k) q.c[k] = (float)cs[k];
+    // Grid samples for the host's uses, as the device evaluates the spectrum.
+    for (int k = 0; k < RTB200_CIE_COUNT; ++k) {
+        const double t = (5.0 * k) / 400.0;
+        const double x = (double)q.c[0] * t * t + (double)q.c[1] * t + (double)q.c[2];
+        s->spectra.push_back((float)((double)q.c[3] * (0.5 + x / (2.0 * std::sqrt(1.0 + x * x)))));
+    }
+    *id_out = q.id;
+    s->sigmoids.push_back(q);
     return RTB200_OK;
 }
 

@@ -54,13 +54,23 @@ __device__ __forceinline__ uint32_t Dim(int depth, int j) { return 8u + 32u * (u
 // 0 outside 380..780 nm.  Header {n, begin, end, offset}: a binned packet of
 // n amplitudes over [begin, end], the bin holding nm returned as is, 0
 // outside (SpectralPacket::ValueAtNM, Utilities/Color/SpectralPacket.h:285-297;
-// nm == end reads the last bin).  offset is the samples' float index (bits).
+// nm == end reads the last bin).  Header {-1, 380, 780, offset}: an RGB
+// colour's sigmoid polynomial (c0, c1, c2, scale), scale * s(c0 t^2 + c1 t +
+// c2) with t = (nm - 380) / 400 (RGBSigmoidPolynomial::Eval,
+// Utilities/Color/RGBSigmoidPolynomial.h:58-70).  offset is the samples'
+// float index (bits).
 __device__ __forceinline__ float Spec(const float* table, int id, float nm)
 {
     if (id < 0) return 0.0f;
     const float4 h = __ldg(reinterpret_cast<const float4*>(table) + id);
     const float* s = table + __float_as_int(h.w);
     if (!(nm >= h.y) || nm > h.z) return 0.0f;
+    if (h.x < 0.0f) {
+        const float4 c = make_float4(__ldg(s), __ldg(s + 1), __ldg(s + 2), __ldg(s + 3));
+        const float t = (nm - 380.0f) / 400.0f;
+        const float x = c.x * t * t + c.y * t + c.z;
+        return c.w * (0.5f + x / (2.0f * sqrtf(1.0f + x * x)));
+    }
     if (h.x == 0.0f) {
         const float x = (nm - 380.0f) * 0.2f;
         const int i = (int)floorf(x);

@@ -8,6 +8,8 @@ Each supported chunk is restated from its parser in
 src/Library/Parsers/ChunkParserRegistry.cpp (defaults included):
 
   spectral_painter            -> scenes.spectral_painter (binned SpectralPacket)
+  uniformcolor_painter        -> scenes.rgb_spectrum (Jakob-Hanika albedo uplift of the
+                                 colour in linear Rec.709; sRGB colours linearised)
   lambertian_material         -> Lambertian, reflectance painter
   lambertian_luminaire_material -> emitter: radiance = exitance * scale / pi
                                  (LambertianEmitter.cpp:72-87), reflective part
@@ -209,6 +211,21 @@ class _Loader:
         if c.has("scale"):
             self.notes.append(f"spectral_painter {c.get('name')}: scale applies to the RGB colour only")
 
+    def uniformcolor_painter(self, c):
+        # Job::AddUniformColorPainter (Job.cpp:2452-2484): the colour in its
+        # colour space, converted to linear Rec.709; the painter's spectrum
+        # is the albedo uplift (UniformColorPainter's default role).
+        self.only(c, {"name", "color", "colorspace"})
+        rgb = np.array(_floats(c.get("color", "0 0 0"), 3, "color"))
+        space = c.get("colorspace", "Rec709RGB_Linear")
+        if space == "sRGB":
+            # ColorUtils::SRGBTransferFunctionInverse (ColorUtils.cpp:34-45).
+            rgb = np.array([0.0 if v == 0 else (v / 12.92 if v <= 0.03928 else ((v + 0.055) / 1.055) ** 2.4)
+                            for v in rgb])
+        elif space not in ("Rec709RGB_Linear", "RISERGB"):
+            self.refuse(c, f"colour space {space!r} is not supported (Rec709RGB_Linear, RISERGB, sRGB)")
+        self.painters[c.get("name", "noname")] = self.desc.add_spectrum(scenes.rgb_spectrum(rgb, scenes.RGB_ALBEDO))
+
     def spectrum(self, c, name, allow_number=False):
         """Spectrum id of a painter reference, or a flat spectrum for a number."""
         if name in (None, "none"):
@@ -222,6 +239,8 @@ class _Loader:
 
     def scaled(self, sid, k):
         sp = self.desc.spectra[sid]
+        if isinstance(sp, scenes.SigmoidSpectrum):
+            return self.desc.add_spectrum(scenes.SigmoidSpectrum(sp.c0, sp.c1, sp.c2, sp.scale * k))
         if isinstance(sp, scenes.SpectralPacket):
             return self.desc.add_spectrum(scenes.SpectralPacket(sp.begin, sp.end,
                                                                 (np.asarray(sp.amps, np.float64) * k).astype(np.float32)))

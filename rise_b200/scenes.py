@@ -144,6 +144,38 @@ class SpectralPacket:
         return np.where(inside, np.asarray(self.amps, np.float64)[np.clip(idx, 0, n - 1)], 0.0)
 
 
+@dataclass
+class SigmoidSpectrum:
+    """An RGB colour's spectrum: scale * s(c0 t^2 + c1 t + c2), t = (nm -
+    380) / 400 on 380..780 nm, s(x) = 1/2 + x / (2 sqrt(1 + x^2))."""
+    c0: float
+    c1: float
+    c2: float
+    scale: float = 1.0
+
+    def value_at(self, nm):
+        nm = np.asarray(nm, np.float64)
+        t = (nm - 380.0) / 400.0
+        x = self.c0 * t * t + self.c1 * t + self.c2
+        v = self.scale * (0.5 + x / (2.0 * np.sqrt(1.0 + x * x)))
+        return np.where((nm >= 380.0) & (nm <= 780.0), v, 0.0)
+
+
+RGB_ALBEDO, RGB_UNBOUNDED = 0, 1
+
+
+def rgb_spectrum(rgb, kind=RGB_ALBEDO):
+    """The spectrum the reference's RGB painters give a linear Rec.709
+    colour (Jakob-Hanika uplift, computed by the library's table): ALBEDO
+    clamps to [0, 1], UNBOUNDED keeps the largest channel as a scale."""
+    import ctypes
+    from ._native import check, lib
+    c = np.ascontiguousarray(rgb, np.float64).reshape(3)
+    out = np.zeros(4)
+    check(lib().rtb200_rgb_uplift(c.ctypes.data_as(ctypes.c_void_p), int(kind), out.ctypes.data_as(ctypes.c_void_p)))
+    return SigmoidSpectrum(*out.tolist())
+
+
 def spectral_painter(nm, amplitudes, nmbegin=400.0, nmend=700.0):
     """The spectrum of the reference's spectral_painter chunk
     (Job::AddSpectralColorPainter, Job.cpp:1557-1582): the control points
@@ -217,7 +249,8 @@ class SceneDesc:
     _tris: list = field(default_factory=list)
 
     def add_spectrum(self, s):
-        self.spectra.append(s if isinstance(s, SpectralPacket) else np.asarray(s, np.float32).reshape(81))
+        self.spectra.append(s if isinstance(s, (SpectralPacket, SigmoidSpectrum))
+                            else np.asarray(s, np.float32).reshape(81))
         return len(self.spectra) - 1
 
     def add_material(self, m):

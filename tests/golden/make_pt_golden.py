@@ -165,6 +165,23 @@ def main():
         rows.append([pos.tolist(), power.tolist(), pts.tolist(), xi.tolist(), picked.tolist(), pdf.tolist(),
                      pdf_all.tolist()])
     out["light_bvh"] = rows
+    lut_path = os.path.join(os.path.dirname(HERE), "..", "oracle", "_ref", "rec709.coeff")
+    table = np.ascontiguousarray(np.fromfile(lut_path, dtype=np.uint8)[20:].view(np.float32))
+    urng = np.random.default_rng(91)
+    colours = [[0.0, 0.0, 0.0], [1.0, 1.0, 1.0], [0.8, 0.1, 0.05], [0.1, 0.7, 0.2], [0.05, 0.1, 0.9],
+               [0.5, 0.5, 0.5], [0.18, 0.18, 0.18], [3.0, 2.0, 1.0], [15.0, 15.0, 15.0]]
+    colours += urng.random((12, 3)).tolist()
+    qnm = np.linspace(375, 785, 42)
+    rows = []
+    P = ctypes.c_void_p
+    for rgb in colours:
+        for kind in (0, 1):
+            c, vals = np.zeros(3), np.zeros(len(qnm))
+            rr = np.ascontiguousarray(rgb, np.float64)
+            r.ref_pt_rgb_uplift(table.ctypes.data_as(P), ctypes.c_uint(table.size), rr.ctypes.data_as(P), kind,
+                                qnm.ctypes.data_as(P), len(qnm), c.ctypes.data_as(P), vals.ctypes.data_as(P))
+            rows.append([rgb, kind, c.tolist(), qnm.tolist(), vals.tolist()])
+    out["rgb_uplift"] = rows
     out["gaussian_filter"] = [[s, g, dx, dy, r.ref_pt_gaussian_weight(s, g, dx, dy)]
                               for s, g in [(2.0, 0.5), (3.0, 1.0), (1.0, 0.3)]
                               for dx, dy in [(0, 0), (0.3, -0.2), (0.99, 0.5), (1.0, 0.0), (-1.01, 0.1), (1.4, 1.4)]]

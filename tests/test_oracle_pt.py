@@ -429,3 +429,57 @@ def test_random_light_bvh(port, ref):
         b = oracle.light_bvh(ref, "ref_pt_", pos, power, pts, xi)
         assert np.array_equal(a[0], b[0])
         assert np.allclose(a[1], b[1], rtol=1e-12, atol=0) and np.allclose(a[2], b[2], rtol=1e-12, atol=0)
+
+
+REF_LUT = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "oracle", "_ref", "rec709.coeff")
+
+
+def test_rgb_uplift_table_equals_the_reference_generators():
+    """The library's RGB -> spectrum table, built by the reference generator's
+    steps, equals the table the reference's own generator writes, bit for
+    bit."""
+    if not os.path.exists(REF_LUT):
+        pytest.skip("reference table not generated (no reference tree)")
+    from rise_b200._native import lib
+    ours = np.zeros(3 * 64 ** 3 * 3, np.float32)
+    lib().rtb200_rgb_uplift_table(ours.ctypes.data)
+    ref = np.fromfile(REF_LUT, dtype=np.uint8)[20:].view(np.float32)
+    assert np.array_equal(ours, ref)
+
+
+def test_rgb_uplift_lookup_matches_reference(ref):
+    """Albedo and unbounded spectra of random colours: the library's lookup
+    against the reference's RGBToSpectrumTable / RGB*Spectrum on the same
+    table."""
+    if not os.path.exists(REF_LUT):
+        pytest.skip("reference table not generated (no reference tree)")
+    from rise_b200 import scenes
+    table = np.ascontiguousarray(np.fromfile(REF_LUT, dtype=np.uint8)[20:].view(np.float32))
+    f = ref.ref_pt_rgb_uplift
+    f.restype = ctypes.c_int
+    P = ctypes.c_void_p
+    rng = np.random.default_rng(12)
+    nm = np.linspace(370, 790, 60)
+    colours = [rng.random(3) for _ in range(150)] + [rng.random(3) * rng.uniform(1, 20) for _ in range(50)] + \
+        [np.array(v, np.float64) for v in ([0, 0, 0], [1, 1, 1], [1, 0, 0], [0, 1, 0], [0, 0, 1], [0.5, 0.5, 0.5])]
+    for rgb in colours:
+        rgb = np.ascontiguousarray(rgb, np.float64)
+        for kind in (0, 1):
+            coeffs, vals = np.zeros(3), np.zeros(len(nm))
+            assert f(table.ctypes.data_as(P), ctypes.c_uint(table.size), rgb.ctypes.data_as(P), kind,
+                     nm.ctypes.data_as(P), len(nm), coeffs.ctypes.data_as(P), vals.ctypes.data_as(P)) == 1
+            s = scenes.rgb_spectrum(rgb, kind)
+            if kind == 0:
+                assert np.array_equal([s.c0, s.c1, s.c2], coeffs), (rgb, s, coeffs)
+            assert np.allclose(s.value_at(nm), vals, rtol=1e-12, atol=1e-300), (rgb, kind)
+
+
+def test_golden_rgb_uplift():
+    """RGB -> spectrum of fixed colours (albedo and unbounded) against values
+    from the reference's own table code and generator."""
+    from rise_b200 import scenes
+    for rgb, kind, coeffs, nm, vals in GOLDEN["rgb_uplift"]:
+        s = scenes.rgb_spectrum(rgb, kind)
+        if kind == 0:
+            assert [s.c0, s.c1, s.c2] == coeffs, (rgb, kind)
+        assert np.allclose(s.value_at(nm), vals, rtol=1e-12, atol=1e-300), (rgb, kind)

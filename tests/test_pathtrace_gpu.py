@@ -259,6 +259,21 @@ def test_light_bvh_and_power_selection_converge_to_the_same_image(ctx):
     assert rel_mse(a, b) < 2e-2
 
 
+def test_rgb_spectra_same_seed_matches_oracle(ctx):
+    """Reflectances and emission given as RGB colours (Jakob-Hanika sigmoid
+    spectra, albedo and unbounded) render as the oracle's."""
+    d = scenes.cornell_box(48, 48)
+    cols = {0: ([0.75, 0.75, 0.75], 0), 1: ([0.63, 0.06, 0.05], 0), 2: ([0.12, 0.45, 0.09], 0),
+            3: ([17.0, 12.0, 4.0], 1)}
+    d.spectra = [scenes.rgb_spectrum(*cols[i]) for i in range(len(d.spectra))]
+    g, _ = render_gpu(ctx, d, 16)
+    o = oracle.pt_render(d, 16)
+    close = (np.abs(g - o) <= 1e-3 * (np.abs(o) + 1e-3)).all(axis=2)
+    assert close.mean() > 0.97, close.mean()
+    assert rel_mse(g, o) < 1e-3
+    assert g[..., 0].mean() > g[..., 2].mean()     # the warm light tints the image
+
+
 def small_spheres(nee_per_lambda=1):
     return scenes.spheres_scene(grid=64, n_spheres=8, sphere_tris=800, width=64, height=64,
                                 nee_per_lambda=nee_per_lambda)

@@ -225,3 +225,35 @@ def test_reference_cornell_scene_loads():
     emit = [m for m in d.materials if m.emission >= 0]
     assert len(emit) == 1
     assert all(isinstance(sp, scenes.SpectralPacket) for sp in d.spectra)
+
+
+def test_uniformcolor_painters_become_rgb_spectra():
+    text = SCENE.replace("""spectral_painter
+{
+	name	white
+	cp		400 0.5
+	cp		700 0.9
+	nmbegin	400
+	nmend	700
+}""", """uniformcolor_painter
+{
+	name		white
+	color		0.8 0.6 0.2
+}
+
+uniformcolor_painter
+{
+	name		srgbwhite
+	color		0.5 0.5 0.5
+	colorspace	sRGB
+}""")
+    s = scenefile.load_scene(text=text)
+    sp = s.desc.spectra[s.desc.materials[0].reflectance]
+    assert isinstance(sp, scenes.SigmoidSpectrum) and sp.scale == 1.0
+    want = scenes.rgb_spectrum([0.8, 0.6, 0.2])
+    assert (sp.c0, sp.c1, sp.c2) == (want.c0, want.c1, want.c2)
+    lin = ((0.5 + 0.055) / 1.055) ** 2.4
+    g = [x for x in s.desc.spectra if isinstance(x, scenes.SigmoidSpectrum)][1]
+    assert abs(g.value_at([550.0])[0] - lin) < 0.02
+    with pytest.raises(scenefile.SceneFileError, match="colour space"):
+        scenefile.load_scene(text=text.replace("colorspace	sRGB", "colorspace	ProPhotoRGB"))
