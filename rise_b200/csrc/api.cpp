@@ -127,7 +127,7 @@ cudaError_t PipelinedCast(rtb200_scene* s, const rtb200_ray* rays, int64_t n, vo
                           int& rc, Trace trace)
 {
     rtb200_ctx* ctx = s->ctx;
-    const int64_t chunk = std::max<int64_t>(std::min<int64_t>(n, int64_t(1) << 17), (n + 15) / 16);
+    const int64_t chunk = std::max<int64_t>(std::min<int64_t>(n, int64_t(1) << 18), (n + 7) / 8);
     const int nbuf = n > chunk ? 2 : 1;
     rc = EnsureStage(s, (size_t)nbuf * chunk * sizeof(rtb200_ray), (size_t)nbuf * chunk * out_bytes_per_ray);
     if (rc) return cudaSuccess;
