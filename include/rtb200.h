@@ -194,6 +194,12 @@ int rtb200_scene_add_spectral_packet(rtb200_scene* scene, float lambda_begin, fl
 int rtb200_rgb_uplift(const double* rgb, int32_t kind, double* coeffs_and_scale);
 int rtb200_rgb_uplift_table(float* coeffs);
 int rtb200_scene_add_rgb_spectrum(rtb200_scene* scene, const double* coeffs_and_scale, int32_t* id_out);
+/* A black body of the given temperature (K): scale * Planck's function of the
+ * wavelength in metres, divided by its value at 0.0029 / T m when normalize
+ * is set (Job::AddBlackBodyPainter / BlackBodyPainter::GetColorNM,
+ * Painters/BlackBodyPainter.cpp:26-43,103-106,152-170).  Same id space. */
+int rtb200_scene_add_blackbody(rtb200_scene* scene, double temperature, double scale, int32_t normalize,
+                               int32_t* id_out);
 /* Uniform sky: radiance spectrum for rays that escape (-1 = none); visible
  * selects whether camera rays see it directly. */
 int rtb200_scene_set_environment(rtb200_scene* scene, int32_t spectrum, int32_t visible);

@@ -174,7 +174,10 @@ def spectrum_table(spectra):
     data = []
     off = 4 * len(spectra)
     for i, sp in enumerate(spectra):
-        if hasattr(sp, "c0"):
+        if hasattr(sp, "temperature"):
+            vals = np.array([sp.temperature, sp.effective_scale()], np.float32)
+            head[i, :3] = (-2.0, 0.0, 1e30)
+        elif hasattr(sp, "c0"):
             vals = np.array([sp.c0, sp.c1, sp.c2, sp.scale], np.float32)
             head[i, :3] = (-1.0, 380.0, 780.0)
         elif hasattr(sp, "amps"):

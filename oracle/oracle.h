@@ -62,7 +62,8 @@ int  orc_ray_triangle(const double* o, const double* d, const double* v0, const 
  *   spectra: the spectrum table of n_spec ids: a header of 4 floats per id,
  *           {0, 380, 780, offset} for 81 samples on the 5 nm grid or
  *           {n, begin, end, offset} for a binned packet, {-1, 380, 780, offset}
- *           for an RGB colour's sigmoid (c0, c1, c2, scale), then the samples
+ *           for an RGB colour's sigmoid (c0, c1, c2, scale), {-2, 0, 1e30, offset}
+ *           for a black body (temperature, scale), then the samples
  *   mats_i: n_mat x 5 int32 (type, reflectance, emission, eta, kappa)
  *   mats_f: n_mat x 2 float (alpha, ior)
  *   cam:    10 doubles (pos, look, up, vertical fov in degrees)

@@ -475,6 +475,16 @@ struct SpecHeader {
     double n, begin, end;
     const float* s;
 };
+// BlackBodyPainter::GetColorNM (Painters/BlackBodyPainter.cpp:26-43,103-106):
+// scale * Planck's function of nm * 1e-9 m; s = (temperature, scale).
+inline double Blackbody(const float* s, double nm)
+{
+    const double c = 2.99792458e8, h = 6.6260755e-34, k = 1.380658e-23;
+    const double c1 = 2.0 * kPi * h * (c * c), c2 = (h * c) / k;
+    const double lam = nm * 1e-9, t = s[0];
+    return (double)s[1] * (c1 / std::pow(lam, 5.0) * (1.0 / (std::exp(c2 / (lam * t)) - 1.0)));
+}
+
 inline SpecHeader Header(const float* table, int id)
 {
     const float* h = table + 4 * (size_t)id;
@@ -486,6 +496,7 @@ inline double Spec(const Scene& S, int id, double nm)
 {
     if (id < 0) return 0.0;
     const SpecHeader h = Header(S.spectra, id);
+    if (h.n == -2.0) return Blackbody(h.s, nm);
     if (h.n < 0.0) {
         // RGBSigmoidPolynomial::Eval (Utilities/Color/RGBSigmoidPolynomial.h:58-70) x scale.
         if (nm < 380.0 || nm > 780.0) return 0.0;
@@ -507,6 +518,7 @@ inline double Spec(const Scene& S, int id, double nm)
 inline double GridValue(const float* table, int id, int k)
 {
     const SpecHeader h = Header(table, id);
+    if (h.n == -2.0) return (float)Blackbody(h.s, 380.0 + 5.0 * k);
     if (h.n < 0.0) {
         const double t = (5.0 * k) / 400.0;
         const double x = (double)h.s[0] * t * t + (double)h.s[1] * t + (double)h.s[2];

@@ -63,6 +63,12 @@ struct rtb200_scene {
         float c[4];
     };
     std::vector<Sigmoid> sigmoids;
+    // Black bodies: spectrum id -> temperature, scale.
+    struct Blackbody {
+        int32_t id;
+        float t, scale;
+    };
+    std::vector<Blackbody> blackbodies;
     size_t spectra_table_bytes = 0;
     std::vector<rtb200::PtMaterial> materials;
     bool mixed_shading = false;      // materials of more than one shading class

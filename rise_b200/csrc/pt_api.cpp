@@ -214,13 +214,21 @@ int UploadShading(rtb200_scene* s)
         const size_t nspec = s->spectra.size() / RTB200_CIE_COUNT;
         std::vector<const rtb200_scene::Packet*> packet(nspec, nullptr);
         std::vector<const rtb200_scene::Sigmoid*> sigmoid(nspec, nullptr);
+        std::vector<const rtb200_scene::Blackbody*> blackbody(nspec, nullptr);
+        for (const auto& q : s->blackbodies) blackbody[q.id] = &q;
         for (const auto& p : s->packets) packet[p.id] = &p;
         for (const auto& q : s->sigmoids) sigmoid[q.id] = &q;
         table.resize(4 * nspec);
         for (size_t id = 0; id < nspec; ++id) {
             const int32_t off = (int32_t)table.size();
             float* h = &table[4 * id];
-            if (sigmoid[id]) {
+            if (blackbody[id]) {
+                h[0] = -2.0f;
+                h[1] = 0.0f;
+                h[2] = 1e30f;
+                table.push_back(blackbody[id]->t);
+                table.push_back(blackbody[id]->scale);
+            } else if (sigmoid[id]) {
                 h[0] = -1.0f;
                 h[1] = 380.0f;
                 h[2] = 780.0f;
@@ -315,6 +323,37 @@ int rtb200_scene_add_spectral_packet(rtb200_scene* s, float lambda_begin, float 
     }
     *id_out = p.id;
     s->packets.push_back(std::move(p));
+    return RTB200_OK;
+}
+
+namespace {
+// Planck's radiation function as the reference writes it
+// (BlackBodyPainter::IntensityForWavelength, BlackBodyPainter.cpp:26-43),
+// wavelength in metres.
+double Planck(double t, double lambda)
+{
+    const double c = 2.99792458e8, h = 6.6260755e-34, k = 1.380658e-23;
+    const double c1 = 2.0 * 3.14159265358979323846 * h * (c * c), c2 = (h * c) / k;
+    return c1 / std::pow(lambda, 5.0) * (1.0 / (std::exp(c2 / (lambda * t)) - 1.0));
+}
+}  // namespace
+
+int rtb200_scene_add_blackbody(rtb200_scene* s, double temperature, double scale, int32_t normalize, int32_t* id_out)
+{
+    if (!s || !id_out) return RTB200_E_INVALID;
+    std::lock_guard<std::mutex> g(s->ctx->mu);
+    if (s->committed) return SetError(s->ctx, RTB200_E_INVALID, "scene already committed");
+    if (!(temperature > 0.0) || !std::isfinite(temperature) || !(scale >= 0.0) || !std::isfinite(scale))
+        return SetError(s->ctx, RTB200_E_INVALID, "bad black body");
+    // With normalize, the scale is divided by the function's value at
+    // 0.0029 / T metres (BlackBodyPainter::RegenerateData, :163-168, with
+    // PeakNMFromTemperature, :60-63).
+    if (normalize) scale /= Planck(temperature, 0.0029 / temperature);
+    rtb200_scene::Blackbody q{(int32_t)(s->spectra.size() / RTB200_CIE_COUNT), (float)temperature, (float)scale};
+    for (int k = 0; k < RTB200_CIE_COUNT; ++k)
+        s->spectra.push_back((float)((double)q.scale * Planck((double)q.t, (380.0 + 5.0 * k) * 1e-9)));
+    *id_out = q.id;
+    s->blackbodies.push_back(q);
     return RTB200_OK;
 }
 

@@ -57,14 +57,24 @@ __device__ __forceinline__ uint32_t Dim(int depth, int j) { return 8u + 32u * (u
 // nm == end reads the last bin).  Header {-1, 380, 780, offset}: an RGB
 // colour's sigmoid polynomial (c0, c1, c2, scale), scale * s(c0 t^2 + c1 t +
 // c2) with t = (nm - 380) / 400 (RGBSigmoidPolynomial::Eval,
-// Utilities/Color/RGBSigmoidPolynomial.h:58-70).  offset is the samples'
-// float index (bits).
+// Utilities/Color/RGBSigmoidPolynomial.h:58-70).  Header {-2, 0, 1e30,
+// offset}: a black body (temperature, scale): scale * C1 / l^5 /
+// (exp(C2 / (l T)) - 1) with l = nm * 1e-9 m, C1 = 2 pi h c^2, C2 = h c / k
+// (BlackBodyPainter::GetColorNM, Painters/BlackBodyPainter.cpp:26-43,103-106).
+// offset is the samples' float index (bits).
 __device__ __forceinline__ float Spec(const float* table, int id, float nm)
 {
     if (id < 0) return 0.0f;
     const float4 h = __ldg(reinterpret_cast<const float4*>(table) + id);
     const float* s = table + __float_as_int(h.w);
     if (!(nm >= h.y) || nm > h.z) return 0.0f;
+    if (h.x == -2.0f) {
+        // C1 / l^5 with l in nm: 2 pi h c^2 * 1e45 / nm^5; C2 / (l T) = h c / k * 1e9 / (nm T).
+        const float T = __ldg(s), k = __ldg(s + 1);
+        const float n2 = nm * nm;
+        const float first = 3.7417749e29f / (n2 * n2 * nm);
+        return k * first / (expf(1.4387687e7f / (nm * T)) - 1.0f);
+    }
     if (h.x < 0.0f) {
         const float4 c = make_float4(__ldg(s), __ldg(s + 1), __ldg(s + 2), __ldg(s + 3));
         const float t = (nm - 380.0f) / 400.0f;

@@ -44,7 +44,10 @@ def upload_scene(ctx, desc, layout="f32"):
     L = lib()
     for sp in desc.spectra:
         out = ctypes.c_int32()
-        if hasattr(sp, "c0"):
+        if hasattr(sp, "temperature"):
+            check(L.rtb200_scene_add_blackbody(s.h, float(sp.temperature), float(sp.scale), int(bool(sp.normalize)),
+                                               ctypes.byref(out)), ctx.h)
+        elif hasattr(sp, "c0"):
             cs = np.array([sp.c0, sp.c1, sp.c2, sp.scale], np.float64)
             check(L.rtb200_scene_add_rgb_spectrum(s.h, ctypes.c_void_p(cs.ctypes.data), ctypes.byref(out)), ctx.h)
         elif hasattr(sp, "amps"):

@@ -8,6 +8,8 @@ Each supported chunk is restated from its parser in
 src/Library/Parsers/ChunkParserRegistry.cpp (defaults included):
 
   spectral_painter            -> scenes.spectral_painter (binned SpectralPacket)
+  blackbody_painter           -> scenes.BlackbodySpectrum (Planck, optionally unit peak)
+  scene_options               -> accepted (scene_unit does not affect a pinhole camera)
   uniformcolor_painter        -> scenes.rgb_spectrum (Jakob-Hanika albedo uplift of the
                                  colour in linear Rec.709; sRGB colours linearised)
   lambertian_material         -> Lambertian, reflectance painter
@@ -226,6 +228,18 @@ class _Loader:
             self.refuse(c, f"colour space {space!r} is not supported (Rec709RGB_Linear, RISERGB, sRGB)")
         self.painters[c.get("name", "noname")] = self.desc.add_spectrum(scenes.rgb_spectrum(rgb, scenes.RGB_ALBEDO))
 
+    def blackbody_painter(self, c):
+        # Job::AddBlackBodyPainter: only temperature, scale and normalize
+        # reach the spectrum (nmbegin / nmend / numfreq shape the RGB colour).
+        self.only(c, {"name", "temperature", "nmbegin", "nmend", "numfreq", "scale", "normalize"})
+        sp = scenes.BlackbodySpectrum(float(c.get("temperature", 5600.0)), float(c.get("scale", 1.0)),
+                                      _bool(c.get("normalize", "true")))
+        self.painters[c.get("name", "noname")] = self.desc.add_spectrum(sp)
+
+    def scene_options(self, c):
+        # scene_unit sets the lens units of physical cameras; a pinhole has none.
+        self.only(c, {"scene_unit"})
+
     def spectrum(self, c, name, allow_number=False):
         """Spectrum id of a painter reference, or a flat spectrum for a number."""
         if name in (None, "none"):
@@ -241,6 +255,8 @@ class _Loader:
         sp = self.desc.spectra[sid]
         if isinstance(sp, scenes.SigmoidSpectrum):
             return self.desc.add_spectrum(scenes.SigmoidSpectrum(sp.c0, sp.c1, sp.c2, sp.scale * k))
+        if isinstance(sp, scenes.BlackbodySpectrum):
+            return self.desc.add_spectrum(scenes.BlackbodySpectrum(sp.temperature, sp.scale * k, sp.normalize))
         if isinstance(sp, scenes.SpectralPacket):
             return self.desc.add_spectrum(scenes.SpectralPacket(sp.begin, sp.end,
                                                                 (np.asarray(sp.amps, np.float64) * k).astype(np.float32)))

@@ -17,6 +17,8 @@ All geometry is float32.  Rays are packed 8 floats each:
 """
 from dataclasses import dataclass, field
 
+import math
+
 import numpy as np
 
 CUBE_CENTRE = np.array([0.5, 0.5, 0.5], np.float64)
@@ -161,6 +163,33 @@ class SigmoidSpectrum:
         return np.where((nm >= 380.0) & (nm <= 780.0), v, 0.0)
 
 
+@dataclass
+class BlackbodySpectrum:
+    """A black body: scale * Planck's function (wavelength in metres), the
+    scale divided by the function's value at 0.0029 / T m when normalize
+    (BlackBodyPainter)."""
+    temperature: float
+    scale: float = 1.0
+    normalize: bool = True
+
+    @staticmethod
+    def planck(t, lam):
+        c, h, k = 2.99792458e8, 6.6260755e-34, 1.380658e-23
+        c1, c2 = 2.0 * math.pi * h * (c * c), (h * c) / k
+        return c1 / np.power(lam, 5.0) * (1.0 / (np.exp(c2 / (lam * t)) - 1.0))
+
+    def effective_scale(self):
+        s = float(self.scale)
+        if self.normalize:
+            s /= float(self.planck(float(self.temperature), 0.0029 / float(self.temperature)))
+        return s
+
+    def value_at(self, nm):
+        t = float(np.float32(self.temperature))
+        k = float(np.float32(self.effective_scale()))
+        return k * self.planck(t, np.asarray(nm, np.float64) * 1e-9)
+
+
 RGB_ALBEDO, RGB_UNBOUNDED = 0, 1
 
 
@@ -249,7 +278,7 @@ class SceneDesc:
     _tris: list = field(default_factory=list)
 
     def add_spectrum(self, s):
-        self.spectra.append(s if isinstance(s, (SpectralPacket, SigmoidSpectrum))
+        self.spectra.append(s if isinstance(s, (SpectralPacket, SigmoidSpectrum, BlackbodySpectrum))
                             else np.asarray(s, np.float32).reshape(81))
         return len(self.spectra) - 1
 

@@ -274,6 +274,16 @@ def test_rgb_spectra_same_seed_matches_oracle(ctx):
     assert g[..., 0].mean() > g[..., 2].mean()     # the warm light tints the image
 
 
+def test_blackbody_light_same_seed_matches_oracle(ctx):
+    d = scenes.cornell_box(48, 48)
+    d.spectra[3] = scenes.BlackbodySpectrum(3200.0, 25.0, True)
+    g, _ = render_gpu(ctx, d, 16)
+    o = oracle.pt_render(d, 16)
+    close = (np.abs(g - o) <= 1e-3 * (np.abs(o) + 1e-3)).all(axis=2)
+    assert close.mean() > 0.97, close.mean()
+    assert rel_mse(g, o) < 1e-3 and g[..., 1].mean() > 0
+
+
 def small_spheres(nee_per_lambda=1):
     return scenes.spheres_scene(grid=64, n_spheres=8, sphere_tris=800, width=64, height=64,
                                 nee_per_lambda=nee_per_lambda)

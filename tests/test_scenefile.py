@@ -257,3 +257,34 @@ uniformcolor_painter
     assert abs(g.value_at([550.0])[0] - lin) < 0.02
     with pytest.raises(scenefile.SceneFileError, match="colour space"):
         scenefile.load_scene(text=text.replace("colorspace	sRGB", "colorspace	ProPhotoRGB"))
+
+
+def test_blackbody_painter_and_scene_options():
+    text = SCENE.replace("""spectral_painter
+{
+	name	light
+	cp		400 10
+	cp		700 10
+	scale	4
+}""", """scene_options
+{
+	scene_unit	0.001
+}
+
+blackbody_painter
+{
+	name		light
+	temperature	3000
+	scale		20
+}""")
+    s = scenefile.load_scene(text=text)
+    emit = s.desc.spectra[s.desc.materials[1].emission]
+    assert isinstance(emit, scenes.BlackbodySpectrum) and emit.normalize
+    # Unit peak at 0.0029 / T metres, times the painter and luminaire scales over pi.
+    peak = 0.0029 / 3000 * 1e9
+    assert abs(emit.value_at([peak])[0] / (20 * 3.0 / math.pi) - 1) < 1e-6
+    nm = np.array([400.0, 550.0, 700.0])
+    h, c, k = 6.6260755e-34, 2.99792458e8, 1.380658e-23
+    lam = nm * 1e-9
+    planck = 2 * math.pi * h * c * c / lam ** 5 / (np.exp(h * c / (k * lam * 3000)) - 1)
+    assert np.allclose(emit.value_at(nm) / planck, planck[1] * 0 + emit.value_at([550.0])[0] / planck[1], rtol=1e-6)
