@@ -163,8 +163,18 @@ def bench_path_tracer(ctx, rank, cpu_baseline=True):
                      "segments_per_sample": st["segments"] / st["samples"],
                      "shadow_rays_per_sample": st["shadow_rays"] / st["samples"]}
         r.close()
-    # relMSE against the FP64 oracle's converged image (per-wavelength NEE).
+    # The same (per-wavelength NEE) over 8-bit quantised child boxes.
     desc.settings.nee_per_lambda = 1
+    sq = pathtracer.upload_scene(ctx, desc, "q8")
+    r = pathtracer.SpectralRasterizer(ctx, desc, scene=sq)
+    r.rasterize_scene(16)
+    t0 = r.stats()["seconds"]
+    for _ in range(4):
+        r.rasterize_scene(16)
+    out["q8_nodes_msamples_s"] = npix * 16 / ((r.stats()["seconds"] - t0) / 4) / 1e6
+    r.close()
+    sq.close()
+    # relMSE against the FP64 oracle's converged image (per-wavelength NEE).
     ref = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "tests", "golden",
                                "cornell_fp64_16384spp.npz"))["xyz"].astype(np.float64)
     rel, secs = {}, {}
