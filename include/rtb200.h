@@ -200,6 +200,12 @@ int rtb200_scene_add_rgb_spectrum(rtb200_scene* scene, const double* coeffs_and_
  * Painters/BlackBodyPainter.cpp:26-43,103-106,152-170).  Same id space. */
 int rtb200_scene_add_blackbody(rtb200_scene* scene, double temperature, double scale, int32_t normalize,
                                int32_t* id_out);
+/* A point light (omni_light: Job::AddPointOmniLight, Lights/PointLight.h:49-57):
+ * next-event estimation gives it the luminance of colour x power at every
+ * wavelength, times cos / distance^2 (LightSampler.cpp:2097-2130); it joins
+ * the luminaries in light selection with weight max(colour) x power x 4 pi
+ * (its radiant exitance) and cannot be hit by rays. */
+int rtb200_scene_add_point_light(rtb200_scene* scene, const float* position, const float* color, float power);
 /* Uniform sky: radiance spectrum for rays that escape (-1 = none); visible
  * selects whether camera rays see it directly. */
 int rtb200_scene_set_environment(rtb200_scene* scene, int32_t spectrum, int32_t visible);

@@ -323,7 +323,14 @@ double Fms(double favg, double eavg)
 
 struct Ggx { double alpha, spec, eta, k, favg; };
 
-struct Light { int first, count, emit; double area, pdf; int bvhPos = 0; };
+struct Light {
+    int first, count, emit;
+    double area, pdf;
+    int bvhPos = 0;
+    int kind = 0;      // 1: point light at pos with flat luminance le
+    double le = 0.0;
+    V pos = {0, 0, 0};
+};
 
 // Light BVH (Lights/LightBVH.cpp:132-531): preorder nodes over the
 // luminaries, the left child after its parent.
@@ -722,7 +729,24 @@ void Sample(const Scene& S, uint32_t pixel, uint32_t sample, double xyz[3])
                         }
                         psel = S.lights[li].pdf;
                     }
-                    if (li >= 0 && li != light && psel > 0) {
+                    if (li >= 0 && S.lights[li].kind == 1 && psel > 0) {
+                        // Point light (LightSampler.cpp:2097-2130): luminance of
+                        // colour x power at every wavelength, cos / d^2, no MIS.
+                        const Light& lg = S.lights[li];
+                        V toL = lg.pos - p;
+                        const double dist = std::sqrt(Dot(toL, toL));
+                        toL = toL * (1.0 / dist);
+                        const double cosS = Dot(toL, ns);
+                        const double pd[3] = {p.x, p.y, p.z}, ld[3] = {toL.x, toL.y, toL.z};
+                        if (cosS > 0 && !orc_any_d(S.bvh, pd, ld, dist - 0.001)) {
+                            for (int j = 0; j < 4; ++j) {
+                                if (S.neePerLambda && j != k) continue;
+                                double f, pb;
+                                EvalBsdf(S, mat, lam[j], ns, gnv, r, toL, f, pb);
+                                L[j] += thr[j] * lg.le * f * cosS / (dist * dist) / psel;
+                            }
+                        }
+                    } else if (li >= 0 && li != light && psel > 0) {
                         const Light& lg = S.lights[li];
                         const double ux = Rand(key, Dim(depth, 4 * k + 1)), uy = Rand(key, Dim(depth, 4 * k + 2)),
                                      uz = Rand(key, Dim(depth, 4 * k + 3));
@@ -1064,7 +1088,7 @@ extern "C" int orc_pt_render(const float* tri9, int64_t n_tri, const int64_t* me
                              int32_t n_mat, const int32_t* envi, const double* cam, const double* setd,
                              const int32_t* seti, int32_t spp, int32_t sample_begin, int32_t x0, int32_t y0,
                              int32_t x1, int32_t y1, int32_t threads, double* xyz, const double* cie,
-                             int32_t* counts)
+                             int32_t* counts, int32_t n_point, const double* points)
 {
     (void)n_spec;
     GetTables();
@@ -1154,6 +1178,33 @@ extern "C" int orc_pt_render(const float* tri9, int64_t n_tri, const int64_t* me
         q.light = (int)S.lights.size();
         lightPrims.push_back(q);
         S.meshLight[m] = (int)S.lights.size();
+        S.lights.push_back(lg);
+    }
+    // Point lights (Lights/PointLight.h:49-57; LightSampler.cpp:655-668 weighs
+    // every light by its radiant exitance: max(colour x power) x 4 pi here
+    // against area x pi x mean radiance for a luminary, so with the common pi
+    // dropped, max(colour x power) x 4).
+    for (int i = 0; i < n_point; ++i) {
+        const double* q7 = points + 7 * i;
+        Light lg;
+        lg.first = lg.count = 0;
+        lg.emit = -1;
+        lg.area = 0.0;
+        lg.kind = 1;
+        lg.pos = {(double)(float)q7[0], (double)(float)q7[1], (double)(float)q7[2]};
+        lg.le = (double)(float)(0.2126 * (float)q7[3] * (float)q7[6] + 0.7152 * (float)q7[4] * (float)q7[6] +
+                                0.0722 * (float)q7[5] * (float)q7[6]);
+        weight.push_back(std::max({(double)(float)q7[3], (double)(float)q7[4], (double)(float)q7[5]}) *
+                         (double)(float)q7[6] * 4.0);
+        LightPrimD q;
+        for (int k = 0; k < 3; ++k) {
+            q.lo[k] = (double)(float)q7[k] - 1e-12;
+            q.hi[k] = (double)(float)q7[k] + 1e-12;
+            q.c[k] = 0.5 * (q.lo[k] + q.hi[k]);
+        }
+        q.power = weight.back();
+        q.light = (int)S.lights.size();
+        lightPrims.push_back(q);
         S.lights.push_back(lg);
     }
     double wsum = 0.0;

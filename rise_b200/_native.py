@@ -47,6 +47,7 @@ SIGNATURES = {
     "rtb200_rgb_uplift_table": (ctypes.c_int, [_vp]),
     "rtb200_scene_add_rgb_spectrum": (ctypes.c_int, [_vp, _vp, _vp]),
     "rtb200_scene_add_blackbody": (ctypes.c_int, [_vp, ctypes.c_double, ctypes.c_double, ctypes.c_int32, _vp]),
+    "rtb200_scene_add_point_light": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_float]),
     "rtb200_scene_add_risemesh": (ctypes.c_int, [_vp, _vp, ctypes.c_int32, ctypes.c_int32]),
     "rtb200_scene_add_spectral_packet": (ctypes.c_int, [_vp, ctypes.c_float, ctypes.c_float, ctypes.c_int32, _vp,
                                                         _vp]),

@@ -83,6 +83,10 @@ struct rtb200_scene {
     rtb200::PtLight* d_lights = nullptr;
     rtb200::PtLightTri* d_light_tris = nullptr;
     std::vector<rtb200::PtLightNode> light_nodes;  // light BVH, built at commit
+    struct PointLight {
+        float pos[3], color[3], power;
+    };
+    std::vector<PointLight> point_lights;
     rtb200::PtLightNode* d_light_nodes = nullptr;
     size_t shade_bytes = 0;
     bool committed = false;

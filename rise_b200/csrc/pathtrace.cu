@@ -651,7 +651,30 @@ KShade(const PtJobDev* __restrict__ jobs, PtPaths P, PtQueues Q, int from_class)
                             psel = S.lights[li].pdf;
                         }
                         // No sample when nothing can be picked, nor from a luminary to itself.
-                        if (li >= 0 && li != at.light && psel > 0.0f) {
+                        if (li >= 0 && S.lights[li].kind == 1 && psel > 0.0f) {
+                            // Point light (LightSampler.cpp:2097-2130): luminance of
+                            // colour x power, cos / d^2, no MIS (a delta light).
+                            const PtLight lg = S.lights[li];
+                            V3 toL = mk(lg.pos[0], lg.pos[1], lg.pos[2]) - p;
+                            const float dist = sqrtf(dot(toL, toL));
+                            toL = toL * (1.0f / dist);
+                            const float cosS = dot(toL, ns);
+                            if (cosS > 0.0f) {
+                                float4 c = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+                                bool any = false;
+                                const GgxPair bq = NeePair(mtype, gp, ns, gnv, r, toL);
+                                #pragma unroll 1
+                                for (int j = 0; j < 4; ++j) {
+                                    if (term & (1u << j)) continue;
+                                    if (set.nee_per_lambda && j != k) continue;
+                                    const float f = NeeValue(mtype, M, S.spectra, lam[j], bq, gp.eavg);
+                                    const float v = Get(thr, j) * lg.le * f * cosS / (dist * dist) / psel;
+                                    Set(c, j, v);
+                                    any |= v != 0.0f;
+                                }
+                                if (any) PushShadow(Q, OffsetRay(p, ng, toL), toL, dist - 0.001f, slot, c);
+                            }
+                        } else if (li >= 0 && li != at.light && psel > 0.0f) {
                             const PtLight lg = S.lights[li];
                             const float ux = Rand(key, Dim(depth, 4 * k + 1));
                             const float uy = Rand(key, Dim(depth, 4 * k + 2));

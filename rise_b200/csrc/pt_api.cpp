@@ -173,6 +173,26 @@ int UploadShading(rtb200_scene* s)
         meshLight[mi] = (int)s->lights.size();
         s->lights.push_back(L);
     }
+    // Point lights (PointLight.h:49-57, LightSampler.cpp:655-668): the
+    // reference weighs a light by its radiant exitance, max(colour x power) x
+    // 4 pi for a point light and area x pi x radiance for a luminary.  The
+    // luminary weights above omit the common factor pi, so the point light's
+    // weight drops it too: max(colour x power) x 4.
+    for (const auto& pl : s->point_lights) {
+        PtLight L{};
+        L.kind = 1;
+        L.emit = -1;
+        L.first = L.count = 0;
+        L.le = (float)(0.2126 * pl.color[0] * pl.power + 0.7152 * pl.color[1] * pl.power +
+                       0.0722 * pl.color[2] * pl.power);
+        for (int k = 0; k < 3; ++k) L.pos[k] = pl.pos[k];
+        LightPrim box{};
+        for (int k = 0; k < 3; ++k) { box.lo[k] = box.hi[k] = pl.pos[k]; }
+        weight.push_back(std::max({(double)pl.color[0], (double)pl.color[1], (double)pl.color[2]}) * pl.power *
+                         4.0);
+        boxes.push_back(box);
+        s->lights.push_back(L);
+    }
     double wsum = 0.0;
     for (double w : weight) wsum += w;
     for (size_t i = 0; i < s->lights.size(); ++i) s->lights[i].pdf = (float)(weight[i] / wsum);
@@ -354,6 +374,22 @@ int rtb200_scene_add_blackbody(rtb200_scene* s, double temperature, double scale
         s->spectra.push_back((float)((double)q.scale * Planck((double)q.t, (380.0 + 5.0 * k) * 1e-9)));
     *id_out = q.id;
     s->blackbodies.push_back(q);
+    return RTB200_OK;
+}
+
+int rtb200_scene_add_point_light(rtb200_scene* s, const float* position, const float* color, float power)
+{
+    if (!s || !position || !color) return RTB200_E_INVALID;
+    std::lock_guard<std::mutex> g(s->ctx->mu);
+    if (s->committed) return SetError(s->ctx, RTB200_E_INVALID, "scene already committed");
+    for (int k = 0; k < 3; ++k)
+        if (!std::isfinite(position[k]) || !std::isfinite(color[k]) || color[k] < 0.0f)
+            return SetError(s->ctx, RTB200_E_INVALID, "bad point light");
+    if (!std::isfinite(power) || power < 0.0f) return SetError(s->ctx, RTB200_E_INVALID, "bad point light");
+    rtb200_scene::PointLight pl;
+    for (int k = 0; k < 3; ++k) { pl.pos[k] = position[k]; pl.color[k] = color[k]; }
+    pl.power = power;
+    s->point_lights.push_back(pl);
     return RTB200_OK;
 }
 

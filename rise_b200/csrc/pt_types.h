@@ -38,7 +38,10 @@ struct PtLight {
     float pdf;       // selection probability by power
     int emit;        // emitted radiance spectrum
     int bvh_pos;     // leaf position in the light BVH's order
-    int pad[2];
+    int kind;        // 0: a mesh luminary; 1: a point light at pos, radiance-like `le`
+    float le;        // point light: luminance of colour x power (flat over wavelength)
+    float pos[3];
+    int pad;
 };
 
 // Light BVH node (LightBVHNode, Lights/LightBVH.h:100-115), preorder: the

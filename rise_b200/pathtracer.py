@@ -64,6 +64,10 @@ def upload_scene(ctx, desc, layout="f32"):
     check(L.rtb200_scene_set_environment(s.h, desc.env, desc.env_visible), ctx.h)
     for first, count, mat, ds in desc.meshes:
         s.add_triangles(desc.tri9[first:first + count], material=mat, double_sided=ds)
+    for pos, color, power in getattr(desc, "point_lights", []):
+        p3 = (ctypes.c_float * 3)(*pos)
+        c3 = (ctypes.c_float * 3)(*color)
+        check(L.rtb200_scene_add_point_light(s.h, p3, c3, float(power)), ctx.h)
     s.commit(layout)
     return s
 

@@ -10,6 +10,8 @@ src/Library/Parsers/ChunkParserRegistry.cpp (defaults included):
   spectral_painter            -> scenes.spectral_painter (binned SpectralPacket)
   blackbody_painter           -> scenes.BlackbodySpectrum (Planck, optionally unit peak)
   scene_options               -> accepted (scene_unit does not affect a pinhole camera)
+  omni_light                  -> point light: position, linear RGB colour x power
+                                 (ChunkParserRegistry.cpp:6855-6865, Lights/PointLight.h)
   uniformcolor_painter        -> scenes.rgb_spectrum (Jakob-Hanika albedo uplift of the
                                  colour in linear Rec.709; sRGB colours linearised)
   lambertian_material         -> Lambertian, reflectance painter
@@ -235,6 +237,13 @@ class _Loader:
         sp = scenes.BlackbodySpectrum(float(c.get("temperature", 5600.0)), float(c.get("scale", 1.0)),
                                       _bool(c.get("normalize", "true")))
         self.painters[c.get("name", "noname")] = self.desc.add_spectrum(sp)
+
+    def omni_light(self, c):
+        # Job::AddPointOmniLight; shootphotons only matters to photon mapping.
+        self.only(c, {"name", "power", "position", "color", "shootphotons"})
+        pos = _floats(c.get("position", "0 0 0"), 3, "omni_light position")
+        col = _floats(c.get("color", "0 0 0"), 3, "omni_light color")
+        self.desc.add_point_light(pos, col, _floats(c.get("power", "1.0"), 1, "omni_light power")[0])
 
     def scene_options(self, c):
         # scene_unit sets the lens units of physical cameras; a pinhole has none.

@@ -274,6 +274,7 @@ class SceneDesc:
     materials: list = field(default_factory=list)  # Material
     env: int = -1
     env_visible: int = 1
+    point_lights: list = field(default_factory=list)  # (position, colour, power)
     settings: RenderSettings = field(default_factory=RenderSettings)
     _tris: list = field(default_factory=list)
 
@@ -281,6 +282,10 @@ class SceneDesc:
         self.spectra.append(s if isinstance(s, (SpectralPacket, SigmoidSpectrum, BlackbodySpectrum))
                             else np.asarray(s, np.float32).reshape(81))
         return len(self.spectra) - 1
+
+    def add_point_light(self, position, color, power=1.0):
+        """An omni_light (Lights/PointLight.h): radiant intensity colour x power."""
+        self.point_lights.append((tuple(float(v) for v in position), tuple(float(v) for v in color), float(power)))
 
     def add_material(self, m):
         self.materials.append(m)

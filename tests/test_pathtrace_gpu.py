@@ -284,6 +284,31 @@ def test_blackbody_light_same_seed_matches_oracle(ctx):
     assert rel_mse(g, o) < 1e-3 and g[..., 1].mean() > 0
 
 
+@pytest.mark.parametrize("selection", [0, 1])
+def test_point_lights_same_seed_match_oracle(ctx, selection):
+    """omni_light point lights beside the Cornell area light: flat luminance
+    of colour x power, cos / d^2, chosen by the light BVH or by power."""
+    d = scenes.cornell_box(48, 48)
+    d.add_point_light((0.3, 0.8, 0.2), (1.0, 0.8, 0.6), 0.4)
+    d.add_point_light((0.8, 0.7, 0.6), (0.2, 0.4, 1.0), 0.7)
+    d.settings.light_selection = selection
+    g, _ = render_gpu(ctx, d, 16)
+    o = oracle.pt_render(d, 16)
+    close = (np.abs(g - o) <= 1e-3 * (np.abs(o) + 1e-3)).all(axis=2)
+    assert close.mean() > 0.97, close.mean()
+    assert rel_mse(g, o) < 1e-3 and g[..., 1].mean() > 0
+
+
+def test_point_light_only_scene(ctx):
+    """A scene lit by one point light alone (no luminary meshes)."""
+    d = scenes.cornell_box(32, 32)
+    d.materials[d.meshes[-1][2]] = d.materials[0]
+    d.add_point_light((0.5, 0.8, 0.5), (1.0, 1.0, 1.0), 1.0)
+    g, _ = render_gpu(ctx, d, 8)
+    o = oracle.pt_render(d, 8)
+    assert rel_mse(g, o) < 1e-3 and o[..., 1].mean() > 0
+
+
 def small_spheres(nee_per_lambda=1):
     return scenes.spheres_scene(grid=64, n_spheres=8, sphere_tris=800, width=64, height=64,
                                 nee_per_lambda=nee_per_lambda)

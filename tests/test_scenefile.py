@@ -288,3 +288,25 @@ blackbody_painter
     lam = nm * 1e-9
     planck = 2 * math.pi * h * c * c / lam ** 5 / (np.exp(h * c / (k * lam * 3000)) - 1)
     assert np.allclose(emit.value_at(nm) / planck, planck[1] * 0 + emit.value_at([550.0])[0] / planck[1], rtol=1e-6)
+
+
+def test_omni_light_becomes_point_light():
+    text = SCENE + """
+omni_light
+{
+	name		bulb
+	power		2.5
+	position	0.1 0.2 0.3
+	color		1.0 0.5 0.25
+	shootphotons	FALSE
+}
+"""
+    s = scenefile.load_scene(text=text)
+    assert s.desc.point_lights == [((0.1, 0.2, 0.3), (1.0, 0.5, 0.25), 2.5)]
+
+
+@pytest.mark.skipif(not os.path.isdir(REF), reason="reference scenes not present")
+def test_reference_pointlight_cornell_loads():
+    p = os.path.join(REF, "scenes", "Tests", "Spectral", "cornellbox_pointlight_spectral.RISEscene")
+    s = scenefile.load_scene(p, search=[REF])
+    assert len(s.desc.point_lights) == 1 and s.desc.n_tri > 0
