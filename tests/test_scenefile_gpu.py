@@ -11,8 +11,21 @@ from test_scenefile import SCENE
 pytestmark = pytest.mark.gpu
 
 
-def test_ingested_scene_matches_oracle():
-    s = scenefile.load_scene(text=SCENE.replace("\tpixel_filter\tbox\n", ""))
+OMNI = """
+omni_light
+{
+	name		bulb
+	power		0.5
+	position	0.3 0.8 0.4
+	color		1.0 0.9 0.7
+}
+"""
+
+
+@pytest.mark.parametrize("extra", ["", OMNI], ids=["area", "area+omni"])
+def test_ingested_scene_matches_oracle(extra):
+    s = scenefile.load_scene(text=SCENE.replace("\tpixel_filter\tbox\n", "") + extra)
+    assert len(s.desc.point_lights) == (1 if extra else 0)
     ctx = raycaster.Context(0)
     try:
         r = pathtracer.SpectralRasterizer(ctx, s.desc)
