@@ -38,6 +38,11 @@ WORKLOAD = ("raycast microbench: 1,000,000-triangle soup, 4,194,304 rays from a 
             "closest-hit, reference BVH (SAH 32 bins, leaf 4) collapsed to 4-wide nodes with 8-bit quantised "
             "child boxes (rounded outward)")
 METRIC = "Mrays/s"
+# The reference arm runs the reference's own BVH, whose child boxes are FP32
+# (it has no quantised node format).
+REF_WORKLOAD = ("raycast microbench: 1,000,000-triangle soup, 4,194,304 rays from a radius-2 sphere, "
+                "closest-hit, the reference's own BVH (SAH 32 bins, leaf 4, FP32 child boxes) and "
+                "double-precision ray/triangle test on the host cores")
 
 
 def parse():
@@ -74,12 +79,13 @@ def load_peaks():
     return 6650.0, "fallback"
 
 
-def profiled_traffic(name):
-    """Per-launch DRAM bytes from a committed ncu summary (profiles/<name>.md)."""
+def profiled(name, key):
+    """A figure of the committed ncu capture of a kernel (its summary under
+    profiles/ holds `key: value` lines), or None."""
     path = os.path.join(ROOT, "profiles", name + ".md")
     if not os.path.exists(path):
         return None
-    m = re.search(r"traffic_bytes_per_launch:\s*([0-9.eE+]+)", open(path).read())
+    m = re.search(re.escape(key) + r":\s*([0-9.eE+]+)", open(path).read())
     return float(m.group(1)) if m else None
 
 
@@ -137,70 +143,107 @@ def cpu_reference_time(tri, rays, seconds=12.0, threads=None):
     return n / dt / 1e6, kind, threads, n
 
 
+C1_SCENE = os.path.join(ROOT, "tests", "golden", "cornell_c1.RISEscene")
+C1_REF = os.path.join(ROOT, "tests", "golden", "cornell_c1_ref_fp64.npz")
+C1_CHECKPOINTS = (16, 64, 256, 512, 1024, 2048)
+
+
+def relmse(img, ref):
+    return float(np.mean((img - ref) ** 2 / (ref ** 2 + 1e-2)))
+
+
+def convergence(ctx, desc, ref, settings, checkpoints=C1_CHECKPOINTS, crop=None):
+    """relMSE against `ref` at each checkpoint spp of one progressive render,
+    device seconds at each, and the first checkpoint at relMSE <= 1e-3 with
+    its Msamples/s (samples to that point / device seconds to that point)."""
+    from rise_b200 import pathtracer
+    r = pathtracer.SpectralRasterizer(ctx, desc, settings=settings)
+    rel, secs, done = {}, {}, 0
+    x0, y0, x1, y1 = crop or (0, 0, settings.width, settings.height)
+    for target in checkpoints:
+        r.rasterize_scene(target - done)
+        done = target
+        rel[str(target)] = relmse(r.film()[y0:y1, x0:x1].astype(np.float64), ref)
+        secs[str(target)] = r.stats()["seconds"]
+    r.close()
+    out = {"relmse": rel, "device_seconds": secs}
+    reach = [int(k) for k, v in rel.items() if v <= 1e-3]
+    if reach:
+        k = min(reach)
+        out["spp_to_relmse_1e-3"] = k
+        out["device_seconds_to_relmse_1e-3"] = secs[str(k)]
+        out["msamples_s_at_relmse_1e-3"] = settings.width * settings.height * k / secs[str(k)] / 1e6
+    return out
+
+
 def bench_path_tracer(ctx, rank, cpu_baseline=True):
-    """Spectral Cornell box (32 triangles, 256x256, 16 spp, 4 wavelengths per
-    sample, max depth 8, Russian roulette from depth 3): device throughput in
-    Msamples/s for both NEE modes, and relMSE at 16 .. 1024 spp against the
-    FP64 oracle's 16384-spp image (tests/golden/cornell_fp64_16384spp.npz,
-    independent seed), with the spp and device time to reach relMSE <= 1e-3."""
-    from rise_b200 import pathtracer, scenes
-    out = {"workload": "spectral Cornell box: 32 triangles, 256x256, 16 spp, HWSS 4 wavelengths, "
-                       "max depth 8, RR from depth 3, seed 1"}
-    desc = scenes.cornell_box(256, 256)
+    """C1 spectral Cornell box, read from its scene file in the reference's
+    scene language (tests/golden/cornell_c1.RISEscene: 32 triangles,
+    256x256, 16 spp, HWSS 4 wavelengths, at most 7 diffuse bounces, Russian
+    roulette from depth 3, the reference's Owen-scrambled Sobol sampler).
+    Device throughput in Msamples/s (Sobol and hash samplers, per-wavelength
+    and shared NEE, 8-bit nodes); relMSE at 16 .. 2048 spp against the
+    reference renderer's own 16384-spp FP64 image with the spp, device time
+    and Msamples/s at relMSE <= 1e-3 for both samplers; and the reference
+    renderer itself (Job::Rasterize, oracle/_ref) timed on the host cores."""
+    import dataclasses
+    from rise_b200 import pathtracer, scenefile
+    ls = scenefile.load_scene(C1_SCENE)
+    desc, base = ls.desc, ls.desc.settings
+    out = {"workload": "C1 spectral Cornell box from its .RISEscene: 32 triangles, 256x256, 16 spp, HWSS 4 "
+                       "wavelengths, at most 7 diffuse bounces (8 vertices), RR from depth 3, Sobol sampler"}
     scene = pathtracer.upload_scene(ctx, desc)
-    npix = 256 * 256
-    for nee, name in ((1, "nee_per_wavelength"), (0, "nee_shared")):
-        desc.settings.nee_per_lambda = nee
-        r = pathtracer.SpectralRasterizer(ctx, desc, scene=scene)
+    npix = base.width * base.height
+
+    def throughput(st, dev_scene):
+        r = pathtracer.SpectralRasterizer(ctx, desc, scene=dev_scene, settings=st)
         r.rasterize_scene(16)   # warm-up pass
         t0 = r.stats()["seconds"]
         reps = 4
         for _ in range(reps):
             r.rasterize_scene(16)
-        st = r.stats()
-        dt = (st["seconds"] - t0) / reps
-        out[name] = {"msamples_s": npix * 16 / dt / 1e6, "ms_per_16spp": dt * 1e3,
-                     "segments_per_sample": st["segments"] / st["samples"],
-                     "shadow_rays_per_sample": st["shadow_rays"] / st["samples"]}
+        stt = r.stats()
+        dt = (stt["seconds"] - t0) / reps
         r.close()
-    # The same (per-wavelength NEE) over 8-bit quantised child boxes.
-    desc.settings.nee_per_lambda = 1
+        return {"msamples_s": npix * 16 / dt / 1e6, "ms_per_16spp": dt * 1e3,
+                "segments_per_sample": stt["segments"] / stt["samples"],
+                "shadow_rays_per_sample": stt["shadow_rays"] / stt["samples"]}
+
+    out["nee_per_wavelength"] = throughput(base, scene)
+    out["nee_per_wavelength_hash_sampler"] = throughput(dataclasses.replace(base, sampler=0), scene)
+    out["nee_shared"] = throughput(dataclasses.replace(base, nee_per_lambda=0), scene)
     sq = pathtracer.upload_scene(ctx, desc, "q8")
-    r = pathtracer.SpectralRasterizer(ctx, desc, scene=sq)
-    r.rasterize_scene(16)
-    t0 = r.stats()["seconds"]
-    for _ in range(4):
-        r.rasterize_scene(16)
-    out["q8_nodes_msamples_s"] = npix * 16 / ((r.stats()["seconds"] - t0) / 4) / 1e6
-    r.close()
+    out["q8_nodes_msamples_s"] = throughput(base, sq)["msamples_s"]
     sq.close()
-    # relMSE against the FP64 oracle's converged image (per-wavelength NEE).
-    ref = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "tests", "golden",
-                               "cornell_fp64_16384spp.npz"))["xyz"].astype(np.float64)
-    rel, secs = {}, {}
-    r = pathtracer.SpectralRasterizer(ctx, desc, scene=scene)
-    done = 0
-    for target in (16, 64, 256, 512, 1024):
-        r.rasterize_scene(target - done)
-        done = target
-        img = r.film().astype(np.float64)
-        rel[str(target)] = float(np.mean((img - ref) ** 2 / (ref ** 2 + 1e-2)))
-        secs[str(target)] = r.stats()["seconds"]
-    r.close()
-    out["relmse_vs_fp64_oracle_16384spp"] = rel
-    reach = [int(k) for k, v in rel.items() if v <= 1e-3]
-    if reach:
-        out["spp_to_relmse_1e-3"] = min(reach)
-        out["device_seconds_to_relmse_1e-3"] = secs[str(min(reach))]
+    if os.path.exists(C1_REF):
+        ref = np.load(C1_REF)["xyz"].astype(np.float64)
+        out["vs_reference_fp64_16384spp"] = {
+            "sobol": convergence(ctx, desc, ref, dataclasses.replace(base, seed=7)),
+            "hash": convergence(ctx, desc, ref, dataclasses.replace(base, seed=7, sampler=0))}
     if cpu_baseline and rank == 0:
         import oracle
-        oracle.pt_render(desc, 1, crop=(0, 0, 8, 8))   # one-time table setup outside the timing
-        t0 = time.perf_counter()
-        crop = (0, 96, 256, 160)   # 64 rows, 16 spp
-        oracle.pt_render(desc, 16, crop=crop)
-        dt = time.perf_counter() - t0
-        out["cpu_baseline"] = {"value": 256 * 64 * 16 / dt / 1e6, "unit": "Msamples/s", "cores": os.cpu_count(),
-                               "kind": "port", "sample": "rows 96-159 of the 256x256 image, 16 spp"}
+        if oracle.rise_ref() is not None:
+            # The reference renderer's own pipeline on every host core.
+            rr = oracle.RefRenderer(C1_SCENE)
+            rr.render()   # scene preparation and first-touch outside the timing
+            t0 = time.perf_counter()
+            reps = 2
+            for _ in range(reps):
+                rr.render()
+            dt = (time.perf_counter() - t0) / reps
+            rr.close()
+            out["cpu_baseline"] = {"value": npix * 16 / dt / 1e6, "unit": "Msamples/s",
+                                   "cores": oracle.RISE_THREADS, "kind": "reference",
+                                   "sample": "the whole 256x256 image at 16 spp through the reference's "
+                                             "Job::Rasterize, twice"}
+        else:
+            oracle.pt_render(desc, 1, crop=(0, 0, 8, 8))   # one-time table setup outside the timing
+            t0 = time.perf_counter()
+            oracle.pt_render(desc, 16, crop=(0, 96, 256, 160))
+            dt = time.perf_counter() - t0
+            out["cpu_baseline"] = {"value": 256 * 64 * 16 / dt / 1e6, "unit": "Msamples/s",
+                                   "cores": os.cpu_count(), "kind": "port",
+                                   "sample": "rows 96-159 of the 256x256 image, 16 spp"}
     scene.close()
     return out
 
@@ -401,7 +444,7 @@ def run_reference(args):
         "impl": "reference", "metric": METRIC, "value": v, "unit": "Mrays/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic (seeded)", "config": {"workload": WORKLOAD, "n_tri": N_TRI, "n_rays": N_RAYS},
+        "data": "synthetic (seeded)", "config": {"workload": REF_WORKLOAD, "n_tri": N_TRI, "n_rays": N_RAYS},
         "cpu_baseline": {"value": v, "unit": "Mrays/s", "cores": threads, "kind": kind,
                          "sample": f"{sample} rays per step of the {N_RAYS}-ray set, BVH build excluded"},
         "e2e": {"value": v, "unit": "Mrays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -523,7 +566,8 @@ def main():
 
     peak, peak_kind = load_peaks()
     achieved = BYTES_CLOSEST * N_RAYS / (ms_step * 1e-3) / 1e9
-    traffic = profiled_traffic("raycast_closest_q8_soup1M")
+    prof = "raycast_closest_q8_soup1M"
+    traffic = profiled(prof, "traffic_bytes_per_launch")
     info = sf.info()
 
     out = {
@@ -537,7 +581,14 @@ def main():
                    "bvh_build_s": round(info["build_seconds"], 3), "hit_rate": round(hit_rate, 6)},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
-                     "algorithmic_bytes_per_ray": BYTES_CLOSEST},
+                     "traffic_source": f"ncu capture of this kernel on this workload (profiles/{prof})",
+                     "algorithmic_bytes_per_ray": BYTES_CLOSEST,
+                     # HBM does not bind this kernel (the scene is L2-resident):
+                     # its limiters are the L1/texture pipe and instruction
+                     # issue under divergence, from the same ncu capture.
+                     "limiter": {"l1tex_throughput_pct": profiled(prof, "l1tex_throughput_pct"),
+                                 "issue_active_pct": profiled(prof, "issue_active_pct"),
+                                 "threads_per_warp_instruction": profiled(prof, "threads_per_warp_instruction")}},
         "variants_mrays_s": variants,
         "e2e": {"value": e2e, "unit": "Mrays/s", "h2d_bytes_per_step": 32 * N_RAYS,
                 "d2h_bytes_per_step": 16 * N_RAYS},
@@ -552,6 +603,10 @@ def main():
     sq.close()
     if not args.no_path_tracer:
         out["path_tracer"] = bench_path_tracer(ctx, rank, cpu_baseline=world == 1 and not args.no_cpu_baseline)
+        # The headline path-tracing metric: Msamples/s at relMSE <= 1e-3
+        # against the reference renderer's FP64 16384-spp image.
+        conv = out["path_tracer"].get("vs_reference_fp64_16384spp", {})
+        out["msamples_s_at_relmse_1e-3"] = {f"C1_{k}": v.get("msamples_s_at_relmse_1e-3") for k, v in conv.items()}
         if not args.no_large:
             out["path_tracer_large"] = bench_large_scene(ctx)
         if not args.no_batch:

@@ -233,7 +233,30 @@ typedef struct {
     int32_t adaptive_max_spp; /* adaptive sampling: maximum samples per pixel (0 = off) */
     float adaptive_threshold; /* adaptive sampling: relative standard error to converge (reference: 0.01) */
     int32_t light_selection;  /* RTB200_LIGHTS_* */
+    int32_t sampler;          /* RTB200_SAMPLER_* */
+    /* Per-type bounce limits (StabilityConfig::maxDiffuseBounce /
+     * maxGlossyBounce / maxTransmissionBounce, PathTransportUtilities.h:170-221):
+     * when bounce_limits is set, a path ends once a scatter of a type would
+     * make that type's count exceed its limit (diffuse: Lambertian and the GGX
+     * multiple-scattering lobe; glossy: GGX specular and dielectric
+     * reflection; transmission: dielectric refraction).  max_depth still caps
+     * the number of path vertices (the reference's default is 128). */
+    int32_t bounce_limits;
+    int32_t max_diffuse_bounce, max_glossy_bounce, max_transmission_bounce;
 } rtb200_render_settings;
+
+/* Random numbers of the path decisions.  HASH: a counter-based hash of
+ * (seed, pixel, sample, dimension) with a fixed dimension layout.  SOBOL: the
+ * reference's sampler (Utilities/SobolSampler.h, Sampling/SobolSequence.h:55-206):
+ * Owen-scrambled padded Sobol (dimension d uses Sobol dimension d & 1 scrambled
+ * with HashCombine(seed, d)), the pixel's seed HashCombine(x, y) (rows from the
+ * top; with a nonzero job seed s, HashCombine(HashCombine(x, y), s)), sample
+ * index = the pixel's sample number; bounce `depth` draws dimensions
+ * (16 + depth) * 32 + j in the order the reference's integrator consumes them
+ * (StartStream(16 + depth), PathTracingIntegrator.cpp:4112), camera jitter and
+ * the hero wavelength dimensions 0, 1, 2. */
+#define RTB200_SAMPLER_HASH 0
+#define RTB200_SAMPLER_SOBOL 1
 
 /* Next-event luminary selection.  BVH: the reference's light BVH
  * (Lights/LightBVH.cpp: importance = power / squared distance to the node's
@@ -388,11 +411,21 @@ int rtb200_cast_any(rtb200_scene* scene, const rtb200_ray* rays, int64_t n, uint
 
 /* Device buffers (device pointers), asynchronous on `stream`, a
  * cudaStream_t taken as is (NULL is the CUDA default stream, as everywhere
- * in CUDA).  The caller synchronises. */
+ * in CUDA).  The caller synchronises.  Every cast on one scene uses the
+ * scene's one work counter (the atomic that hands rays to warps): casts on
+ * the same scene whose work overlaps on the GPU (different streams or host
+ * threads) race on it and must be ordered by the caller, e.g. on one stream.
+ * The kernels record a traversal-stack overflow in the scene's device error
+ * word instead of failing; commit refuses BVHs whose exact stack bound the
+ * kernels cannot hold, so it stays clear for committed scenes, and
+ * rtb200_scene_device_status reads it: it waits for `stream`, returns
+ * RTB200_E_DEVICE (and clears the word) if any cast on the scene since the
+ * last check set it, else RTB200_OK. */
 int rtb200_cast_closest_device(rtb200_scene* scene, const rtb200_ray* d_rays, int64_t n,
                                rtb200_hit* d_hits, void* stream);
 int rtb200_cast_any_device(rtb200_scene* scene, const rtb200_ray* d_rays, int64_t n,
                            uint8_t* d_occluded, void* stream);
+int rtb200_scene_device_status(rtb200_scene* scene, void* stream);
 
 /* Closest hit that allocates no device memory (no counterpart in the
  * reference: the reference renderer allocates on the host and never on a
@@ -407,7 +440,10 @@ int rtb200_cast_any_device(rtb200_scene* scene, const rtb200_ray* d_rays, int64_
  * before any stream capture.  Every call shares the array and clears it on
  * its stream first, so calls whose work overlaps on the GPU race on it and
  * must be serialised by the caller.  At most RTB200_NOALLOC_MAX_RAYS rays per
- * call; larger n is rejected with RTB200_E_INVALID. */
+ * call; larger n is rejected with RTB200_E_INVALID.  The kernel's error word
+ * (a traversal-stack overflow, which commit's exact stack bound rules out for
+ * committed scenes) sits in the same array and is not reported by this entry:
+ * reading it would need a synchronisation this entry exists to avoid. */
 #define RTB200_NOALLOC_SCRATCH_BYTES 256
 #define RTB200_NOALLOC_MAX_RAYS 2147483647LL
 int rtb200_cast_closest_noalloc(rtb200_scene* scene, const rtb200_ray* d_rays, int64_t n,

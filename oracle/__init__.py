@@ -192,6 +192,12 @@ def spectrum_table(spectra):
     return np.ascontiguousarray(np.concatenate([head.ravel()] + data).astype(np.float32))
 
 
+def _bounce_limits(st):
+    lim = [getattr(st, "max_diffuse_bounce", None), getattr(st, "max_glossy_bounce", None),
+           getattr(st, "max_transmission_bounce", None)]
+    return (int(any(v is not None for v in lim)),) + tuple(int(v) if v is not None else 255 for v in lim)
+
+
 def pt_render(desc, spp, sample_begin=0, crop=None, threads=None, settings=None, return_counts=False):
     """Render a scenes.SceneDesc with the path-tracing oracle.
 
@@ -215,7 +221,7 @@ def pt_render(desc, spp, sample_begin=0, crop=None, threads=None, settings=None,
                      getattr(st, "filter_sigma", 0.5), getattr(st, "adaptive_threshold", 0.01)], np.float64)
     seti = np.array([st.width, st.height, st.max_depth, st.rr_min_depth, st.nee_per_lambda, st.seed,
                      getattr(st, "filter", 0), getattr(st, "adaptive_max_spp", 0),
-                     getattr(st, "light_selection", 0)], np.int32)
+                     getattr(st, "light_selection", 0), getattr(st, "sampler", 0)] + list(_bounce_limits(st)), np.int32)
     out = np.zeros((y1 - y0, x1 - x0, 3), np.float64)
     counts = np.zeros((y1 - y0, x1 - x0), np.int32)
     cie = np.ascontiguousarray(cie_table())
@@ -384,3 +390,157 @@ def energy_tables(lib, prefix):
     eavg = np.zeros(32)
     getattr(lib, prefix + "tables")(_p(ess, _f64p), _p(eavg, _f64p))
     return ess.reshape(32, 32), eavg
+
+
+# ---- the reference renderer (oracle/_ref/librise_ref.so) ----------------------
+
+_rise = None
+
+
+RISE_THREADS = os.cpu_count() or 1
+
+
+def rise_ref():
+    """The reference renderer's library with our harness
+    (oracle/ref_render_harness.cpp, recipe oracle/rise_ref.mk), or None where
+    it was not built.  Its render thread pool is set to every host core
+    (RISE_THREADS) through an options file (RISE_OPTIONS_FILE,
+    force_number_of_threads, render_thread_reserve_count 0: the reference's
+    benchmark mode), written before the library first reads its options."""
+    global _rise
+    if _rise is None:
+        path = os.path.join(_HERE, "_ref", "librise_ref.so")
+        if not os.path.exists(path):
+            return None
+        import tempfile
+        fd, opts = tempfile.mkstemp(prefix="rise_options_", suffix=".options")
+        with os.fdopen(fd, "w") as f:
+            f.write(f"force_number_of_threads {RISE_THREADS}\nrender_thread_reserve_count 0\n")
+        os.environ["RISE_OPTIONS_FILE"] = opts
+        lib = ctypes.CDLL(path)
+        lib.rr_load.restype = _vp
+        lib.rr_load.argtypes = [ctypes.c_char_p]
+        lib.rr_free.argtypes = [_vp]
+        lib.rr_size.restype = ctypes.c_int
+        lib.rr_size.argtypes = [_vp, _u32p, _u32p]
+        lib.rr_render.restype = ctypes.c_int
+        lib.rr_render.argtypes = [_vp, _f64p, ctypes.c_uint, ctypes.c_uint]
+        lib.rr_integrate.restype = ctypes.c_int
+        lib.rr_integrate.argtypes = [_vp] + [ctypes.c_uint] * 6 + [ctypes.c_int, ctypes.c_int, _f64p]
+        _rise = lib
+    return _rise
+
+
+_RISE_CWD = None
+
+
+class _StdoutToStderr:
+    """The reference library logs on the process's standard output and into a
+    log file in the working directory; while it runs, route the output to
+    standard error and work in a scratch directory, so a caller's output and
+    folders stay its own."""
+
+    def __enter__(self):
+        import sys
+        import tempfile
+        global _RISE_CWD
+        if _RISE_CWD is None:
+            _RISE_CWD = tempfile.mkdtemp(prefix="rise_ref_")
+        sys.stdout.flush()
+        self.saved = os.dup(1)
+        os.dup2(2, 1)
+        self.cwd = os.getcwd()
+        os.chdir(_RISE_CWD)
+        return self
+
+    def __exit__(self, *a):
+        import ctypes.util
+        libc = ctypes.CDLL(ctypes.util.find_library("c"))
+        libc.fflush(None)
+        os.chdir(self.cwd)
+        os.dup2(self.saved, 1)
+        os.close(self.saved)
+
+
+class RefRenderer:
+    """A .RISEscene loaded into the reference renderer.
+
+    render(): the reference's whole pipeline (Job::Rasterize); returns the
+    resolved linear Rec.709 image (height, width, 3) in float64.
+    integrate(spp, batch, rect): the reference's per-sample function over a
+    box-filter pixel loop with the batch number mixed into the Sobol seed
+    (batch 0 = the reference's own seed); returns mean XYZ per pixel.
+    Referenced files resolve against the scene's folder."""
+
+    def __init__(self, scene_path):
+        lib = rise_ref()
+        if lib is None:
+            raise OSError("oracle/_ref/librise_ref.so is not built (make -C oracle rise)")
+        self.lib = lib
+        path = os.path.abspath(scene_path)
+        with _StdoutToStderr():
+            self.h = lib.rr_load(path.encode())
+        if not self.h:
+            raise RuntimeError(f"the reference could not load {scene_path}")
+        w, h = ctypes.c_uint(), ctypes.c_uint()
+        if not lib.rr_size(self.h, ctypes.byref(w), ctypes.byref(h)):
+            raise RuntimeError("scene has no film")
+        self.width, self.height = w.value, h.value
+
+    def render(self):
+        out = np.zeros((self.height, self.width, 3), np.float64)
+        with _StdoutToStderr():
+            ok = self.lib.rr_render(self.h, _p(out, _f64p), self.width, self.height)
+        if not ok:
+            raise RuntimeError("reference render failed")
+        return out
+
+    def integrate(self, spp, batch=0, rect=None, threads=None, independent=False):
+        x0, y0, x1, y1 = rect if rect is not None else (0, 0, self.width, self.height)
+        out = np.zeros((y1 - y0, x1 - x0, 3), np.float64)
+        n = threads or os.cpu_count() or 1
+        with _StdoutToStderr():
+            ok = self.lib.rr_integrate(self.h, x0, y0, x1, y1, spp, batch, n, int(bool(independent)),
+                                       _p(out, _f64p))
+        if not ok:
+            raise RuntimeError("reference integrate failed")
+        return out
+
+    def close(self):
+        if self.h:
+            self.lib.rr_free(self.h)
+            self.h = None
+
+
+def sobol(index, dim, seed, kind="port"):
+    """Scrambled Sobol values: the port's 32-bit integers, or the reference's
+    SobolSequence::Sample doubles (value / 2^32)."""
+    index = np.ascontiguousarray(index, np.uint32)
+    dim = np.ascontiguousarray(np.broadcast_to(dim, index.shape), np.uint32)
+    seed = np.ascontiguousarray(np.broadcast_to(seed, index.shape), np.uint32)
+    n = index.size
+    if kind == "port":
+        lib = port()
+        out = np.zeros(n, np.uint32)
+        lib.orc_pt_sobol.restype = None
+        lib.orc_pt_sobol.argtypes = [_u32p, _u32p, _u32p, _i64, _u32p]
+        lib.orc_pt_sobol(_p(index, _u32p), _p(dim, _u32p), _p(seed, _u32p), n, _p(out, _u32p))
+        return out
+    lib = ref_blocks()
+    out = np.zeros(n, np.float64)
+    lib.ref_pt_sobol.restype = None
+    lib.ref_pt_sobol.argtypes = [_u32p, _u32p, _u32p, _i64, _f64p]
+    lib.ref_pt_sobol(_p(index, _u32p), _p(dim, _u32p), _p(seed, _u32p), n, _p(out, _f64p))
+    return out
+
+
+def hash_combine(a, b, kind="port"):
+    a = np.ascontiguousarray(a, np.uint32)
+    b = np.ascontiguousarray(np.broadcast_to(b, a.shape), np.uint32)
+    lib, name = (port(), "orc_pt_hash_combine") if kind == "port" else (ref_blocks(), "ref_pt_hash_combine")
+    f = getattr(lib, name)
+    f.restype = None
+    f.argtypes = [_u32p, _u32p, _i64, _u32p]
+    out = np.zeros(a.size, np.uint32)
+    f(_p(a, _u32p), _p(b, _u32p), a.size, _p(out, _u32p))
+    return out

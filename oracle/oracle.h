@@ -70,8 +70,10 @@ int  orc_ray_triangle(const double* o, const double* d, const double* v0, const 
  *   setd:   6 doubles (lambda_min, lambda_max, rr_threshold, filter size, filter sigma,
  *           adaptive threshold)
  *   points: n_point x 7 doubles (position, colour, power) of point lights
- *   seti:   9 int32 (width, height, max_depth, rr_min_depth, nee_per_lambda, seed, filter,
- *           adaptive maximum samples per pixel or 0, light selection: 0 light BVH, 1 power)
+ *   seti:   14 int32 (width, height, max_depth, rr_min_depth, nee_per_lambda, seed, filter,
+ *           adaptive maximum samples per pixel or 0, light selection: 0 light BVH, 1 power,
+ *           sampler: 0 hash, 1 Owen-scrambled Sobol, bounce limits on, maximum diffuse,
+ *           glossy and transmission bounces)
  * filter 0 is the box film (mean of the pixel's own samples); filter 1 is the
  * Gaussian pixel filter: with size / 2 > 0.501 the samples of every pixel
  * within the support are splatted and a pixel is sum(w XYZ) / sum(w); a
@@ -119,6 +121,10 @@ double orc_pt_fms(double favg, double eavg);
 double orc_pt_power_heuristic(double a, double b);
 int    orc_pt_russian_roulette(int depth, int min_depth, double threshold, double cur, double prev, double u,
                                double* survival);
+/* The reference's padded Owen-scrambled Sobol (Sampling/SobolSequence.h):
+ * the 32-bit scrambled value per (index, dimension, seed), and HashCombine. */
+void   orc_pt_sobol(const uint32_t* index, const uint32_t* dim, const uint32_t* seed, int64_t n, uint32_t* out);
+void   orc_pt_hash_combine(const uint32_t* a, const uint32_t* b, int64_t n, uint32_t* out);
 void   orc_pt_tables(double* ess, double* eavg);
 void   orc_pt_set_tables(const double* ess, const double* eavg);
 

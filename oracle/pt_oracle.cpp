@@ -59,6 +59,70 @@ inline double Rand(uint32_t key, uint32_t dim)
 }
 inline uint32_t Dim(int depth, int j) { return 8u + 32u * (uint32_t)depth + (uint32_t)j; }
 
+// The reference's sampler (Sampling/SobolSequence.h:55-206,
+// Utilities/SobolSampler.h): padded Owen-scrambled Sobol.
+inline uint32_t HashCombine(uint32_t a, uint32_t b)
+{
+    a ^= b + 0x9e3779b9u + (a << 6) + (a >> 2);
+    a ^= a >> 16; a *= 0x85ebca6bu;
+    a ^= a >> 13; a *= 0xc2b2ae35u;
+    a ^= a >> 16;
+    return a;
+}
+inline uint32_t ReverseBits(uint32_t n)
+{
+    n = (n << 16) | (n >> 16);
+    n = ((n & 0x00ff00ffu) << 8) | ((n & 0xff00ff00u) >> 8);
+    n = ((n & 0x0f0f0f0fu) << 4) | ((n & 0xf0f0f0f0u) >> 4);
+    n = ((n & 0x33333333u) << 2) | ((n & 0xccccccccu) >> 2);
+    n = ((n & 0x55555555u) << 1) | ((n & 0xaaaaaaaau) >> 1);
+    return n;
+}
+inline uint32_t SobolBits(uint32_t index, uint32_t dim, uint32_t seed)
+{
+    uint32_t v = 0;
+    if (dim & 1u) {
+        for (uint32_t i = index, d = 1u << 31; i; i >>= 1, d ^= d >> 1)
+            if (i & 1u) v ^= d;
+    } else {
+        v = ReverseBits(index);
+    }
+    const uint32_t s = HashCombine(seed, dim);
+    v = ReverseBits(v);
+    v ^= v * 0x3d20adeau;
+    v += s;
+    v *= (s >> 16) | 1u;
+    v ^= v * 0x05526c56u;
+    v ^= v * 0x53a22864u;
+    return ReverseBits(v);
+}
+// As the device draws it: the top 24 bits.
+inline double SobolSample(uint32_t index, uint32_t dim, uint32_t seed)
+{
+    return (double)(SobolBits(index, dim, seed) >> 8) * (1.0 / 16777216.0);
+}
+inline uint32_t SobolPixelSeed(uint32_t x, uint32_t y, uint32_t seed)
+{
+    const uint32_t s = HashCombine(x, y);
+    return seed ? HashCombine(s, seed) : s;
+}
+
+// Numbers of one path vertex: the fixed hash layout, or the reference's
+// StartStream(16 + depth) and dimensions in draw order (the device's
+// VertexRng).
+struct VertexRng {
+    uint32_t key, index;
+    int depth;
+    bool sobol;
+    uint32_t cur;
+    double next(int j)
+    {
+        if (sobol) return SobolSample(index, (16u + (uint32_t)depth) * 32u + cur++, key);
+        return Rand(key, Dim(depth, j));
+    }
+    void skip(int n) { cur += (uint32_t)n; }
+};
+
 struct V { double x, y, z; };
 inline V operator+(V a, V b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
 inline V operator-(V a, V b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
@@ -447,12 +511,16 @@ struct Scene {
     const float* mf;
     const double* cie;
     std::vector<Light> lights;
+    std::vector<double> aliasProb;         // alias table over the luminaries (power selection)
+    std::vector<int> aliasOf;
     std::vector<LTri> ltris;
     std::vector<int> meshLight;
     orc_bvh* bvh;
     int env, envVisible;
     double lmin, lmax, rrThreshold, ynorm;
     int width, height, maxDepth, rrMinDepth, neePerLambda;
+    int sampler = 0;                       // 0 hash, 1 Sobol
+    int maxBounce[3] = {255, 255, 255};    // diffuse, glossy, transmission
     uint32_t seed;
     bool lightBvh = false;                 // luminaries picked with the light BVH
     std::vector<LightNode> lightNodes;
@@ -624,9 +692,22 @@ double DielectricR(double cosI, double cosT, double ni, double nt)
     return std::min(1.0, num / den);
 }
 
+// Hash key, or the pixel's Sobol seed, and the camera's numbers (dimensions
+// 0-2: jitter x, y, hero wavelength).
+inline uint32_t SampleKey(const Scene& S, uint32_t pixel, uint32_t sample)
+{
+    if (S.sampler == 1)
+        return SobolPixelSeed(pixel % (uint32_t)S.width, pixel / (uint32_t)S.width, S.seed);
+    return PathKey(S.seed, pixel, sample);
+}
+inline double CameraRand(const Scene& S, uint32_t key, uint32_t sample, uint32_t dim)
+{
+    return S.sampler == 1 ? SobolSample(sample, dim, key) : Rand(key, dim);
+}
+
 void Sample(const Scene& S, uint32_t pixel, uint32_t sample, double xyz[3])
 {
-    const uint32_t key = PathKey(S.seed, pixel, sample);
+    const uint32_t key = SampleKey(S, pixel, sample);
     const int px = (int)(pixel % (uint32_t)S.width), py = (int)(pixel / (uint32_t)S.width);
     // Screen position, pixel centres on integer coordinates, rows downwards:
     // ptOnScreen = (x + u - 1/2, (height - y) + v - 1/2)
@@ -635,7 +716,7 @@ void Sample(const Scene& S, uint32_t pixel, uint32_t sample, double xyz[3])
     // (Sampling/GaussianPixelFilter.h:109-127); the pinhole maps it to the
     // direction W + (x - width/2) h ar / width (-U) + (height/2 - y_row) h / height V
     // (PinholeCamera.cpp:85-89,182-192,209-214).
-    const double ox = Rand(key, 0), oy = Rand(key, 1);
+    const double ox = CameraRand(S, key, sample, 0), oy = CameraRand(S, key, sample, 1);
     double fx = px + ox - 0.5, fy = py + 0.5 - oy;
     if (S.warpSigma > 0.0) {
         const double v = std::max(S.warpTrunc + (1.0 - S.warpTrunc) * ox, 1e-30);
@@ -648,10 +729,12 @@ void Sample(const Scene& S, uint32_t pixel, uint32_t sample, double xyz[3])
     V d = Norm(S.fwd + S.right * sx + S.up * sy);
     V o = S.pos;
     double lam[4];
-    Wavelengths(Rand(key, 2), S.lmin, S.lmax, lam);
+    Wavelengths(CameraRand(S, key, sample, 2), S.lmin, S.lmax, lam);
     double thr[4] = {1, 1, 1, 1}, L[4] = {0, 0, 0, 0};
     double bsdfPdf = 0.0;
+    int bounces[3] = {0, 0, 0};
     for (int depth = 0; depth < S.maxDepth; ++depth) {
+        VertexRng rng{key, sample, depth, S.sampler == 1, 0u};
         double mx = 0.0;
         bool bad = false;
         for (double v : thr) { if (!std::isfinite(v)) bad = true; mx = std::max(mx, std::fabs(v)); }
@@ -692,6 +775,7 @@ void Sample(const Scene& S, uint32_t pixel, uint32_t sample, double xyz[3])
         double kray[4] = {0, 0, 0, 0};
         V nd;
         double npdf = 0.0;
+        int btype = 0;   // continuation: 0 diffuse, 1 glossy, 2 transmission
         if (type == 2) {
             // Smooth dielectric (DielectricSPF.cpp:120-300); constant index:
             // the wavelength bundle continues together.
@@ -708,25 +792,32 @@ void Sample(const Scene& S, uint32_t pixel, uint32_t sample, double xyz[3])
                 tdir = Norm(d * eta + nn * (eta * cosI - cosT));
                 R = DielectricR(cosI, cosT, n1, n2);
             }
-            nd = Rand(key, Dim(depth, 18)) < R ? Norm(d + nn * (2.0 * cosI)) : tdir;
+            rng.skip(2);   // ScatterNM's 2D sample, unused by a smooth interface
+            if (rng.next(18) < R) {
+                nd = Norm(d + nn * (2.0 * cosI));
+                btype = 1;
+            } else {
+                nd = tdir;
+                btype = 2;
+            }
             for (double& k : kray) k = 1.0;
         } else {
             const V ns = ng, r = -d;
             const int nsamp = S.neePerLambda ? 4 : 1;
             for (int k = 0; k < nsamp; ++k) {
                 if (!S.lights.empty()) {
-                    const double ul = Rand(key, Dim(depth, 4 * k));
+                    const double ul = rng.next(4 * k);
                     int li = 0;
                     double psel;
                     if (S.lightBvh) {
                         const double pp[3] = {p.x, p.y, p.z};
                         li = SampleLightBvh(S.lightNodes, pp, ul, psel);
                     } else {
-                        double acc = 0.0;
-                        for (li = 0; li < (int)S.lights.size() - 1; ++li) {
-                            acc += S.lights[li].pdf;
-                            if (ul < acc) break;
-                        }
+                        // AliasTable::Sample.
+                        const int nl = (int)S.lights.size();
+                        const double sc = ul * nl;
+                        const int idx = std::min((int)sc, nl - 1);
+                        li = (sc - idx < S.aliasProb[idx]) ? idx : S.aliasOf[idx];
                         psel = S.lights[li].pdf;
                     }
                     if (li >= 0 && S.lights[li].kind == 1 && psel > 0) {
@@ -748,11 +839,14 @@ void Sample(const Scene& S, uint32_t pixel, uint32_t sample, double xyz[3])
                         }
                     } else if (li >= 0 && li != light && psel > 0) {
                         const Light& lg = S.lights[li];
-                        const double ux = Rand(key, Dim(depth, 4 * k + 1)), uy = Rand(key, Dim(depth, 4 * k + 2)),
-                                     uz = Rand(key, Dim(depth, 4 * k + 3));
-                        int ts = lg.first + lg.count - 1;
-                        for (int q = lg.first; q < lg.first + lg.count; ++q)
-                            if (S.ltris[q].cdf >= uz) { ts = q; break; }
+                        const double ux = rng.next(4 * k + 1), uy = rng.next(4 * k + 2), uz = rng.next(4 * k + 3);
+                        // std::lower_bound over the areas CDF (TriangleMeshGeometryIndexed.cpp:207-217).
+                        int ts = lg.first, hi = lg.first + lg.count - 1;
+                        while (ts < hi) {
+                            const int mid = (ts + hi) >> 1;
+                            if (S.ltris[mid].cdf >= uz) hi = mid;
+                            else ts = mid + 1;
+                        }
                         const LTri& lt = S.ltris[ts];
                         const double sa = std::sqrt(1.0 - ux);
                         const V pl = lt.v0 + lt.e1 * (1.0 - sa) + lt.e2 * (sa * uy);
@@ -773,10 +867,15 @@ void Sample(const Scene& S, uint32_t pixel, uint32_t sample, double xyz[3])
                                 L[j] += thr[j] * Spec(S, lg.emit, lam[j]) * cosS * geom * f * w;
                             }
                         }
+                    } else if (!(li >= 0 && S.lights[li].kind == 1 && psel > 0)) {
+                        // Nothing to sample, or the luminary being shaded: the
+                        // reference still draws the point's three numbers
+                        // (LightSampler.cpp:2064-2096).
+                        rng.skip(3);
                     }
                 }
                 if (S.env >= 0) {
-                    const double u1 = Rand(key, Dim(depth, 20 + 2 * k)), u2 = Rand(key, Dim(depth, 21 + 2 * k));
+                    const double u1 = rng.next(20 + 2 * k), u2 = rng.next(21 + 2 * k);
                     const double z = 1.0 - 2.0 * u1, rr = std::sqrt(std::max(0.0, 1.0 - z * z));
                     const V dir = {rr * std::cos(2.0 * kPi * u2), rr * std::sin(2.0 * kPi * u2), z};
                     const double cosE = Dot(dir, ns);
@@ -796,7 +895,8 @@ void Sample(const Scene& S, uint32_t pixel, uint32_t sample, double xyz[3])
             const V gn = gnv;
             V tx, ty;
             Frame(w, tx, ty);
-            const double u1 = Rand(key, Dim(depth, 16)), u2 = Rand(key, Dim(depth, 17));
+            const double ulobe = type == 1 ? rng.next(18) : 0.0;   // GGXSPF draws the lobe first
+            const double u1 = rng.next(16), u2 = rng.next(17);
             if (type == 1) {
                 const Ggx g0 = GgxAt(S, mat, lam[0]);
                 const double cosR = Dot(r, w);
@@ -805,7 +905,8 @@ void Sample(const Scene& S, uint32_t pixel, uint32_t sample, double xyz[3])
                 const double pSpec = ws / total, pMS = wms / total;
                 const double msz = MsZ(g0.alpha);
                 double khero;
-                if (Rand(key, Dim(depth, 18)) < pSpec) {
+                if (ulobe < pSpec) {
+                    btype = 1;
                     const V wl = {Dot(r, tx), Dot(r, ty), Dot(r, w)};
                     const V ml = VndfLocal(wl, g0.alpha, u1, u2);
                     const V mh = Norm(tx * ml.x + ty * ml.y + w * ml.z);
@@ -848,6 +949,7 @@ void Sample(const Scene& S, uint32_t pixel, uint32_t sample, double xyz[3])
                 for (int k = 0; k < 4; ++k) kray[k] = Spec(S, refl, lam[k]);
             }
         }
+        if (type != 2) rng.skip(1);   // the integrator's choice among the scattered rays (a dielectric's is its Fresnel choice)
         double prevMax = 0, currMax = 0;
         for (int k = 0; k < 4; ++k) {
             prevMax = std::max(prevMax, std::fabs(thr[k]));
@@ -855,10 +957,15 @@ void Sample(const Scene& S, uint32_t pixel, uint32_t sample, double xyz[3])
         }
         if (currMax <= kNearZero) break;
         double survival;
-        if (RussianRoulette(depth, S.rrMinDepth, S.rrThreshold, currMax, prevMax, Rand(key, Dim(depth, 19)), survival))
+        if (depth >= S.rrMinDepth &&
+            RussianRoulette(depth, S.rrMinDepth, S.rrThreshold, currMax, prevMax, rng.next(19), survival))
             break;
+        if (depth < S.rrMinDepth) survival = 1.0;
         if (survival != 1.0)
             for (double& k : kray) k /= survival;
+        // Per-type bounce limits, after Russian roulette
+        // (PropagateBounceLimits, PathTransportUtilities.h:170-221).
+        if (++bounces[btype] > S.maxBounce[btype]) break;
         if (depth + 1 >= S.maxDepth) break;
         for (int k = 0; k < 4; ++k) thr[k] *= kray[k];
         bsdfPdf = npdf;
@@ -1110,6 +1217,9 @@ extern "C" int orc_pt_render(const float* tri9, int64_t n_tri, const int64_t* me
     S.rrMinDepth = seti[3];
     S.neePerLambda = seti[4];
     S.seed = (uint32_t)seti[5];
+    S.sampler = seti[9];
+    if (seti[10])
+        for (int k = 0; k < 3; ++k) S.maxBounce[k] = std::min(seti[11 + k], 255);
     {
         const double lo = std::max(S.lmin, 380.0), hi = std::min(S.lmax, 780.0);
         const int f = (int)((lo - 380.0) / 5.0), l = (int)((hi - 380.0) / 5.0);
@@ -1186,6 +1296,9 @@ extern "C" int orc_pt_render(const float* tri9, int64_t n_tri, const int64_t* me
     // dropped, max(colour x power) x 4).
     for (int i = 0; i < n_point; ++i) {
         const double* q7 = points + 7 * i;
+        // Lights of zero exitance are dropped (LightSampler::Prepare).
+        if (!(std::max({(double)(float)q7[3], (double)(float)q7[4], (double)(float)q7[5]}) * (double)(float)q7[6] > 0))
+            continue;
         Light lg;
         lg.first = lg.count = 0;
         lg.emit = -1;
@@ -1210,6 +1323,30 @@ extern "C" int orc_pt_render(const float* tri9, int64_t n_tri, const int64_t* me
     double wsum = 0.0;
     for (double w : weight) wsum += w;
     for (size_t i = 0; i < S.lights.size(); ++i) S.lights[i].pdf = weight[i] / wsum;
+    {
+        // Vose's alias table (Utilities/AliasTable.h:34-101), the stack order
+        // of the reference; thresholds rounded to FP32 as the device keeps them.
+        const size_t n = weight.size();
+        std::vector<double> scaled(n);
+        S.aliasProb.assign(n, 1.0);
+        S.aliasOf.resize(n);
+        std::vector<int> small, large;
+        for (size_t i = 0; i < n; ++i) {
+            scaled[i] = weight[i] / wsum * (double)n;
+            S.aliasOf[i] = (int)i;
+            (scaled[i] < 1.0 ? small : large).push_back((int)i);
+        }
+        while (!small.empty() && !large.empty()) {
+            const int sm = small.back(), lg = large.back();
+            small.pop_back();
+            large.pop_back();
+            S.aliasProb[sm] = scaled[sm];
+            S.aliasOf[sm] = lg;
+            scaled[lg] = (scaled[lg] + scaled[sm]) - 1.0;
+            (scaled[lg] < 1.0 ? small : large).push_back(lg);
+        }
+        for (double& x : S.aliasProb) x = (double)(float)x;
+    }
     if (seti[8] == 0 && S.lights.size() > 1) {
         std::vector<int> posOf(S.lights.size(), 0);
         int pos = 0;
@@ -1249,8 +1386,9 @@ extern "C" int orc_pt_render(const float* tri9, int64_t n_tri, const int64_t* me
                 for (int px = ex0; px < ex1; ++px) {
                     const uint32_t pixel = (uint32_t)(py * S.width + px);
                     auto splat = [&](uint32_t sample, const double* v) {
-                        const uint32_t key = PathKey(S.seed, pixel, sample);
-                        const double sx = px + Rand(key, 0) - 0.5, sy = py + 0.5 - Rand(key, 1);
+                        const uint32_t key = SampleKey(S, pixel, sample);
+                        const double sx = px + CameraRand(S, key, sample, 0) - 0.5,
+                                     sy = py + 0.5 - CameraRand(S, key, sample, 1);
                         const int qx0 = std::max(x0, (int)std::floor(sx - hw));
                         const int qx1 = std::min(x1 - 1, (int)std::floor(sx + hw));
                         const int qy0 = std::max(y0, (int)std::floor(sy - hw));
@@ -1352,6 +1490,17 @@ double orc_pt_ms_sample_cos(double alpha, double u) { return MsSampleCos(alpha, 
 double orc_pt_fresnel_avg(double ni, double nt, double k) { return FresnelAvg(ni, nt, k); }
 double orc_pt_fms(double favg, double eavg) { return Fms(favg, eavg); }
 double orc_pt_power_heuristic(double a, double b) { return PowerHeuristic(a, b); }
+
+// The device's Sobol sampler: out[i] = the 32-bit scrambled value of sample
+// index[i], dimension dim[i], seed seed[i]; hc[i] = HashCombine(a[i], b[i]).
+void orc_pt_sobol(const uint32_t* index, const uint32_t* dim, const uint32_t* seed, int64_t n, uint32_t* out)
+{
+    for (int64_t i = 0; i < n; ++i) out[i] = SobolBits(index[i], dim[i], seed[i]);
+}
+void orc_pt_hash_combine(const uint32_t* a, const uint32_t* b, int64_t n, uint32_t* out)
+{
+    for (int64_t i = 0; i < n; ++i) out[i] = HashCombine(a[i], b[i]);
+}
 
 int orc_pt_russian_roulette(int depth, int min_depth, double threshold, double cur, double prev, double u,
                             double* survival)

@@ -32,6 +32,7 @@
 #include "Interfaces/IFunction2D.h"
 #include "Utilities/PiecewiseLinearFunction.h"
 #include "Utilities/Color/SpectralPacket.h"
+#include "Sampling/SobolSequence.h"
 
 namespace RISE
 {
@@ -261,6 +262,18 @@ double ref_pt_gaussian_weight(double size, double sigma, double dx, double dy)
     const double w = f->EvaluateFilter(dx, dy);
     f->release();
     return w;
+}
+
+// The reference's padded Owen-scrambled Sobol: out[i] = the 32-bit
+// scrambled value of SobolSequence::Sample(index[i], dim[i], seed[i]) (its
+// double is this value / 2^32), and HashCombine(a[i], b[i]).
+void ref_pt_sobol(const uint32_t* index, const uint32_t* dim, const uint32_t* seed, int64_t n, double* out)
+{
+    for (int64_t i = 0; i < n; ++i) out[i] = SobolSequence::Sample(index[i], dim[i], seed[i]);
+}
+void ref_pt_hash_combine(const uint32_t* a, const uint32_t* b, int64_t n, uint32_t* out)
+{
+    for (int64_t i = 0; i < n; ++i) out[i] = SobolSequence::HashCombine(a[i], b[i]);
 }
 
 }  // extern "C"

@@ -56,6 +56,7 @@ SIGNATURES = {
     "rtb200_cast_closest_device": (ctypes.c_int, [_vp, _vp, _i64, _vp, _vp]),
     "rtb200_cast_any_device": (ctypes.c_int, [_vp, _vp, _i64, _vp, _vp]),
     "rtb200_cast_closest_noalloc": (ctypes.c_int, [_vp, _vp, _i64, _vp, _vp]),
+    "rtb200_scene_device_status": (ctypes.c_int, [_vp, _vp]),
     "rtb200_scene_add_spectrum": (ctypes.c_int, [_vp, _vp, _vp]),
     "rtb200_scene_add_material": (ctypes.c_int, [_vp, _vp, _vp]),
     "rtb200_scene_set_environment": (ctypes.c_int, [_vp, _i32, _i32]),

@@ -517,6 +517,16 @@ int rtb200_cast_any_device(rtb200_scene* s, const rtb200_ray* d_rays, int64_t n,
                      "any-hit launch");
 }
 
+int rtb200_scene_device_status(rtb200_scene* s, void* stream)
+{
+    if (!s) return RTB200_E_INVALID;
+    rtb200_ctx* ctx = s->ctx;
+    std::lock_guard<std::mutex> g(ctx->mu);
+    if (!s->committed) return SetError(ctx, RTB200_E_INVALID, "scene not committed");
+    cudaSetDevice(ctx->device);
+    return CheckErrWord(s, (cudaStream_t)stream);
+}
+
 int rtb200_cast_closest(rtb200_scene* s, const rtb200_ray* rays, int64_t n, rtb200_hit* hits)
 {
     if (!s) return RTB200_E_INVALID;

@@ -88,6 +88,8 @@ struct rtb200_scene {
     };
     std::vector<PointLight> point_lights;
     rtb200::PtLightNode* d_light_nodes = nullptr;
+    std::vector<rtb200::PtLightAlias> light_alias;  // built at commit
+    rtb200::PtLightAlias* d_light_alias = nullptr;
     size_t shade_bytes = 0;
     bool committed = false;
     int32_t layout = RTB200_BVH_F32;

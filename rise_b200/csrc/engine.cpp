@@ -254,7 +254,7 @@ int EngineSubmit(rtb200_engine* e, rtb200_job* j, int spp)
     rtb200_scene* s = j->scene;
     PtJobDev& d = e->h_table[entry];
     d.scene = PtScene{s->d_nodes, s->layout, (int)s->n_nodes, s->d_tris, (int)s->tri_material.size(), s->d_attr, s->d_mats,
-                      s->d_spectra, s->d_lights, s->d_light_tris, s->d_light_nodes};
+                      s->d_spectra, s->d_lights, s->d_light_tris, s->d_light_nodes, s->d_light_alias};
     d.cam = j->cam;
     d.set = j->set;
     int npx = j->npix;
@@ -497,6 +497,11 @@ int rtb200_job_create(rtb200_scene* s, const rtb200_render_settings* rs, rtb200_
         return SetError(ctx, RTB200_E_INVALID, "bad light selection");
     if (rs->adaptive_max_spp < 0 || (rs->adaptive_max_spp > 0 && !(rs->adaptive_threshold > 0.0f)))
         return SetError(ctx, RTB200_E_INVALID, "bad adaptive sampling settings");
+    if (rs->sampler != RTB200_SAMPLER_HASH && rs->sampler != RTB200_SAMPLER_SOBOL)
+        return SetError(ctx, RTB200_E_INVALID, "bad sampler");
+    if (rs->bounce_limits && (rs->max_diffuse_bounce < 0 || rs->max_glossy_bounce < 0 ||
+                              rs->max_transmission_bounce < 0))
+        return SetError(ctx, RTB200_E_INVALID, "bad bounce limits");
     // Camera frame (pinhole; vertical field of view).
     const float* P = rs->cam_pos;
     double f[3] = {rs->cam_look[0] - P[0], rs->cam_look[1] - P[1], rs->cam_look[2] - P[2]};
@@ -540,6 +545,13 @@ int rtb200_job_create(rtb200_scene* s, const rtb200_render_settings* rs, rtb200_
     st.n_lights = (int)s->lights.size();
     st.n_spectra = (int)(s->spectra.size() / RTB200_CIE_COUNT);
     st.light_bvh = rs->light_selection == RTB200_LIGHTS_BVH ? 1 : 0;
+    st.sampler = rs->sampler == RTB200_SAMPLER_SOBOL ? kSamplerSobol : kSamplerHash;
+    {
+        // Counts are kept in a byte each and a path has at most 255 vertices,
+        // so 255 means no limit.
+        const int32_t lim[3] = {rs->max_diffuse_bounce, rs->max_glossy_bounce, rs->max_transmission_bounce};
+        for (int k = 0; k < 3; ++k) st.max_bounce[k] = rs->bounce_limits ? std::min(lim[k], 255) : 255;
+    }
     const bool gauss = rs->filter == RTB200_FILTER_GAUSSIAN;
     st.filter = !gauss ? kFilterBox : (0.5 * rs->filter_size > 0.501 ? kFilterSplat : kFilterWarp);
     st.filt_half = gauss ? 0.5f * rs->filter_size : 0.5f;

@@ -155,7 +155,11 @@ __device__ __forceinline__ void Splat(const PtPaths& P, const PtJobDev& J, int s
     // (GaussianPixelFilter.h:67-78).
     const int W = J.cam.width, H = J.cam.height;
     const int px = (int)(m.x % (uint32_t)W), py = (int)(m.x / (uint32_t)W);
-    const float sx = (float)px + Rand(m.w, 0) - 0.5f, sy = (float)py + 0.5f - Rand(m.w, 1);
+    // The camera's jitter numbers again (hash key or Sobol seed in m.w, sample in m.y).
+    const bool sobol = S.sampler == kSamplerSobol;
+    const float ox = sobol ? SobolSample(m.y, 0, m.w) : Rand(m.w, 0);
+    const float oy = sobol ? SobolSample(m.y, 1, m.w) : Rand(m.w, 1);
+    const float sx = (float)px + ox - 0.5f, sy = (float)py + 0.5f - oy;
     const float hw = S.filt_half;
     const int x0 = max(0, (int)floorf(sx - hw)), x1 = min(W - 1, (int)floorf(sx + hw));
     const int y0 = max(0, (int)floorf(sy - hw)), y1 = min(H - 1, (int)floorf(sy + hw));
@@ -310,8 +314,11 @@ KRegen(const PtJobDev* __restrict__ jobs, PtPaths P, PtQueues Q, int assign)
                 const uint32_t slot_px = (uint32_t)(g % (unsigned long long)J.npix);
                 const uint32_t pixel = J.px_list ? __ldg(J.px_list + slot_px) : slot_px;
                 const uint32_t sample = (uint32_t)(J.sample_begin + g / (unsigned long long)J.npix);
-                const uint32_t key = PathKey(J.set.seed, pixel, sample);
                 const int px = (int)(pixel % (uint32_t)J.cam.width), py = (int)(pixel / (uint32_t)J.cam.width);
+                const bool sobol = J.set.sampler == kSamplerSobol;
+                // Hash key, or the pixel's Sobol seed (camera dimensions 0-2).
+                const uint32_t key = sobol ? SobolPixelSeed((uint32_t)px, (uint32_t)py, J.set.seed)
+                                           : PathKey(J.set.seed, pixel, sample);
                 // Screen position in pixel units, pixel centres on integer
                 // coordinates, rows counted downwards: the reference's
                 // ptOnScreen = (x + u - 1/2, (height - y) + v - 1/2) for the
@@ -319,7 +326,8 @@ KRegen(const PtJobDev* __restrict__ jobs, PtPaths P, PtQueues Q, int assign)
                 // (PathTracingSpectralRasterizer.cpp:321-331, BoxPixelFilter.h:54-58),
                 // or the pixel centre moved by the truncated Gaussian's
                 // inverse CDF for a narrow Gaussian (GaussianPixelFilter.h:109-127).
-                const float ox = Rand(key, 0), oy = Rand(key, 1);
+                const float ox = sobol ? SobolSample(sample, 0, key) : Rand(key, 0);
+                const float oy = sobol ? SobolSample(sample, 1, key) : Rand(key, 1);
                 float fx, fy;
                 if (J.set.filter == kFilterWarp) {
                     const float v = fmaxf(J.set.filt_trunc + (1.0f - J.set.filt_trunc) * ox, 1e-30f);
@@ -337,7 +345,8 @@ KRegen(const PtJobDev* __restrict__ jobs, PtPaths P, PtQueues Q, int assign)
                 const V3 d = normalize(mk(J.cam.fwd[0] + sx * J.cam.right[0] + sy * J.cam.up[0],
                                           J.cam.fwd[1] + sx * J.cam.right[1] + sy * J.cam.up[1],
                                           J.cam.fwd[2] + sx * J.cam.right[2] + sy * J.cam.up[2]));
-                const float hero = J.set.lmin + Rand(key, 2) * (J.set.lmax - J.set.lmin);
+                const float hero = J.set.lmin + (sobol ? SobolSample(sample, 2, key) : Rand(key, 2)) *
+                                                    (J.set.lmax - J.set.lmin);
                 P.ray_o[slot] = make_float4(J.cam.pos[0], J.cam.pos[1], J.cam.pos[2], 0.0f);
                 P.ray_d[slot] = make_float4(d.x, d.y, d.z, __int_as_float(0x7f800000));
                 P.thr[slot] = make_float4(1.0f, 1.0f, 1.0f, 1.0f);
@@ -535,7 +544,8 @@ KShade(const PtJobDev* __restrict__ jobs, PtPaths P, PtQueues Q, int from_class)
         float4 thr = P.thr[slot];
         float4 L = P.L[slot];
         const int depth = (int)(m.z & kFlagDepthMask);
-        const uint32_t key = m.w;
+        // Random numbers: hash key or Sobol seed in meta.w, sample index in meta.y.
+        VertexRng rng{m.w, m.y, depth, set.sampler == kSamplerSobol, 0u};
         const float bsdfPdf = aux.y;
         const unsigned term = (m.z >> kTermShift) & 0xfu;
         float lam[4];
@@ -601,6 +611,7 @@ KShade(const PtJobDev* __restrict__ jobs, PtPaths P, PtQueues Q, int from_class)
             V3 nd;
             float npdf = 0.0f;       // continuation pdf for the next emission MIS (0 = delta)
             unsigned nflags = kFlagConsiderEmission;
+            int btype = kBounceDiffuse;   // ScatteredRay type of the continuation
 
             if (mtype == kMatDielectric) {
                 // Smooth dielectric: Fresnel choice between reflection and
@@ -620,8 +631,16 @@ KShade(const PtJobDev* __restrict__ jobs, PtPaths P, PtQueues Q, int from_class)
                     tdir = normalize(d * eta + nn * (eta * cosI - cosT));
                     R = DielectricR(cosI, cosT, n1, n2);
                 }
-                if (Rand(key, Dim(depth, 18)) < R) nd = normalize(d + nn * (2.0f * cosI));
-                else nd = tdir;
+                // The reference's ScatterNM draws a 2D sample first, which the
+                // smooth interface does not use (DielectricSPF.cpp:421).
+                rng.skip(2);
+                if (rng.next(18) < R) {
+                    nd = normalize(d + nn * (2.0f * cosI));
+                    btype = kBounceGlossy;
+                } else {
+                    nd = tdir;
+                    btype = kBounceTransmission;
+                }
                 for (int k = 0; k < 4; ++k) Set(kray, k, (term & (1u << k)) ? 0.0f : 1.0f);
                 nflags |= kFlagSpecular;
             } else {
@@ -637,17 +656,18 @@ KShade(const PtJobDev* __restrict__ jobs, PtPaths P, PtQueues Q, int from_class)
                 for (int k = 0; k < nsamp; ++k) {
                     if (set.nee_per_lambda && (term & (1u << k))) continue;
                     if (set.n_lights > 0) {
-                        const float ul = Rand(key, Dim(depth, 4 * k + 0));
+                        const float ul = rng.next(4 * k + 0);
                         int li = 0;
                         float psel;
                         if (set.light_bvh && S.light_nodes) {
                             li = SampleLightBvh(S.light_nodes, p, ul, psel);
                         } else {
-                            float acc = 0.0f;
-                            for (li = 0; li < set.n_lights - 1; ++li) {
-                                acc += S.lights[li].pdf;
-                                if (ul < acc) break;
-                            }
+                            // Alias table (AliasTable::Sample): one number
+                            // picks an entry and decides between it and its alias.
+                            const float sc = ul * (float)set.n_lights;
+                            const int idx = min((int)sc, set.n_lights - 1);
+                            const PtLightAlias al = S.light_alias[idx];
+                            li = (sc - (float)idx < al.prob) ? idx : al.alias;
                             psel = S.lights[li].pdf;
                         }
                         // No sample when nothing can be picked, nor from a luminary to itself.
@@ -659,7 +679,7 @@ KShade(const PtJobDev* __restrict__ jobs, PtPaths P, PtQueues Q, int from_class)
                             const float dist = sqrtf(dot(toL, toL));
                             toL = toL * (1.0f / dist);
                             const float cosS = dot(toL, ns);
-                            if (cosS > 0.0f) {
+                            if (dist > 0.0f && cosS > 0.0f) {
                                 float4 c = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
                                 bool any = false;
                                 const GgxPair bq = NeePair(mtype, gp, ns, gnv, r, toL);
@@ -676,13 +696,18 @@ KShade(const PtJobDev* __restrict__ jobs, PtPaths P, PtQueues Q, int from_class)
                             }
                         } else if (li >= 0 && li != at.light && psel > 0.0f) {
                             const PtLight lg = S.lights[li];
-                            const float ux = Rand(key, Dim(depth, 4 * k + 1));
-                            const float uy = Rand(key, Dim(depth, 4 * k + 2));
-                            const float uz = Rand(key, Dim(depth, 4 * k + 3));
-                            // First triangle whose area CDF reaches uz (std::lower_bound).
-                            int tsel = lg.first + lg.count - 1;
-                            for (int q = lg.first; q < lg.first + lg.count; ++q)
-                                if (S.light_tris[q].cdf >= uz) { tsel = q; break; }
+                            const float ux = rng.next(4 * k + 1);
+                            const float uy = rng.next(4 * k + 2);
+                            const float uz = rng.next(4 * k + 3);
+                            // First triangle whose area CDF reaches uz: binary
+                            // search (std::lower_bound over the areas CDF,
+                            // TriangleMeshGeometryIndexed.cpp:207-217).
+                            int tsel = lg.first, hi = lg.first + lg.count - 1;
+                            while (tsel < hi) {
+                                const int mid = (tsel + hi) >> 1;
+                                if (__ldg(&S.light_tris[mid].cdf) >= uz) hi = mid;
+                                else tsel = mid + 1;
+                            }
                             const PtLightTri lt = S.light_tris[tsel];
                             // GeometricUtilities::PointOnTriangle (GeometricUtilities.cpp:543-569).
                             const float sa = sqrtf(1.0f - ux);
@@ -714,12 +739,18 @@ KShade(const PtJobDev* __restrict__ jobs, PtPaths P, PtQueues Q, int from_class)
                                 }
                                 if (any) PushShadow(Q, OffsetRay(p, ng, toL), toL, dist - 0.001f, slot, c);
                             }
+                        } else if (!(li >= 0 && S.lights[li].kind == 1 && psel > 0.0f)) {
+                            // Nothing to sample, or the luminary being shaded:
+                            // the reference still draws the point's three
+                            // numbers (LightSampler.cpp:2064-2096).
+                            rng.skip(3);
                         }
                     }
                     if (set.env >= 0) {
                         // Uniform-sky NEE: uniform directions, pdf 1/(4 pi)
                         // (LightSampler.cpp:2277-2359).
-                        const float u1 = Rand(key, Dim(depth, 20 + 2 * k)), u2 = Rand(key, Dim(depth, 21 + 2 * k));
+                        const float u1 = rng.next(20 + 2 * k);
+                        const float u2 = rng.next(21 + 2 * k);
                         const float z = 1.0f - 2.0f * u1;
                         const float rr = sqrtf(fmaxf(0.0f, 1.0f - z * z));
                         float sp, cp;
@@ -751,7 +782,10 @@ KShade(const PtJobDev* __restrict__ jobs, PtPaths P, PtQueues Q, int from_class)
                 const V3 gn = gnv;
                 V3 tx, ty;
                 Basis(w, tx, ty);
-                const float u1 = Rand(key, Dim(depth, 16)), u2 = Rand(key, Dim(depth, 17));
+                // GGXSPF::ScatterNM draws the lobe choice before the
+                // direction (GGXSPF.cpp:478-520); LambertianSPF the direction.
+                const float ulobe = mtype == kMatGGX ? rng.next(18) : 0.0f;
+                const float u1 = rng.next(16), u2 = rng.next(17);
                 if (mtype == kMatGGX) {
                     const GgxParams g0 = GgxAt(M, S.spectra, lam[0]);
                     const float cosR = dot(r, w);
@@ -762,7 +796,8 @@ KShade(const PtJobDev* __restrict__ jobs, PtPaths P, PtQueues Q, int from_class)
                     const float pSpec = ws / total, pMS = wms / total;
                     const float msz = gp.msz;
                     float khero = 0.0f;
-                    if (Rand(key, Dim(depth, 18)) < pSpec) {
+                    if (ulobe < pSpec) {
+                        btype = kBounceGlossy;
                         const V3 mh = VndfSample(r, tx, ty, w, g0.alpha, u1, u2);
                         const float rm = dot(r, mh);
                         if (!(rm > 0.0f)) break;
@@ -818,6 +853,9 @@ KShade(const PtJobDev* __restrict__ jobs, PtPaths P, PtQueues Q, int from_class)
                     if (!(dot(nd, gn) > 0.0f)) break;
                     for (int k = 0; k < 4; ++k) Set(kray, k, (term & (1u << k)) ? 0.0f : Spec(S.spectra, M.refl, lam[k]));
                 }
+                // The integrator's choice among the scattered rays
+                // (ScatteredRayContainer::RandomlySelect; one ray here).
+                rng.skip(1);
             }
             // Russian roulette on the max over wavelengths (:4738-4769,
             // PathTransportUtilities.h:86-110).
@@ -830,11 +868,20 @@ KShade(const PtJobDev* __restrict__ jobs, PtPaths P, PtQueues Q, int from_class)
             if (currMax <= kNearZero) break;
             if (depth >= set.rr_min_depth) {
                 const float prob = fminf(1.0f, currMax / fmaxf(prevMax, set.rr_threshold));
-                if (Rand(key, Dim(depth, 19)) >= prob) break;
+                if (rng.next(19) >= prob) break;
                 if (prob > 0.0f && prob < 1.0f) {
                     const float s = 1.0f / prob;
                     kray = make_float4(kray.x * s, kray.y * s, kray.z * s, kray.w * s);
                 }
+            }
+            // Per-type bounce limits (PropagateBounceLimits,
+            // PathTransportUtilities.h:170-221), checked after Russian roulette
+            // as the reference does (:4770-4790).
+            unsigned bounces = __float_as_uint(aux.w);
+            {
+                const unsigned c = ((bounces >> (8 * btype)) & 0xffu) + 1u;
+                if ((int)c > set.max_bounce[btype]) break;
+                bounces = (bounces & ~(0xffu << (8 * btype))) | (c << (8 * btype));
             }
             if (depth + 1 >= set.max_depth) break;
             thr = make_float4(thr.x * kray.x, thr.y * kray.y, thr.z * kray.z, thr.w * kray.w);
@@ -842,7 +889,7 @@ KShade(const PtJobDev* __restrict__ jobs, PtPaths P, PtQueues Q, int from_class)
             P.ray_o[slot] = make_float4(no.x, no.y, no.z, 0.0f);
             P.ray_d[slot] = make_float4(nd.x, nd.y, nd.z, __int_as_float(0x7f800000));
             P.thr[slot] = thr;
-            P.aux[slot] = make_float4(aux.x, npdf, aux.z, 0.0f);
+            P.aux[slot] = make_float4(aux.x, npdf, aux.z, __uint_as_float(bounces));
             m.z = (m.z & ~(kFlagDepthMask | kFlagSpecular)) | (unsigned)(depth + 1) | nflags;
             P.meta[slot].z = m.z;
             cont = true;

@@ -97,6 +97,40 @@ int BuildLightNodes(std::vector<LightPrim>& prims, int start, int end, int& pos,
     return idx;
 }
 
+// Walker's alias table by Vose's algorithm (Utilities/AliasTable.h:34-101):
+// weights scaled so each entry's fair share is 1, entries below 1 ("small")
+// and at or above ("large") kept on stacks; the top small entry keeps its
+// scaled weight as its threshold and takes the top large entry as its alias,
+// whose weight gives up the difference; leftovers keep themselves.  The same
+// stack order as the reference, so a number maps to the same luminary.
+std::vector<PtLightAlias> BuildAlias(const std::vector<double>& w)
+{
+    const size_t n = w.size();
+    std::vector<PtLightAlias> out(n);
+    double total = 0.0;
+    for (double x : w) total += x;
+    if (n == 0 || !(total > 0.0)) return out;
+    std::vector<double> scaled(n), prob(n, 1.0);
+    std::vector<unsigned> alias(n);
+    std::vector<unsigned> small, large;
+    for (size_t i = 0; i < n; ++i) {
+        scaled[i] = w[i] / total * (double)n;
+        alias[i] = (unsigned)i;
+        (scaled[i] < 1.0 ? small : large).push_back((unsigned)i);
+    }
+    while (!small.empty() && !large.empty()) {
+        const unsigned sm = small.back(), lg = large.back();
+        small.pop_back();
+        large.pop_back();
+        prob[sm] = scaled[sm];
+        alias[sm] = lg;
+        scaled[lg] = (scaled[lg] + scaled[sm]) - 1.0;
+        (scaled[lg] < 1.0 ? small : large).push_back(lg);
+    }
+    for (size_t i = 0; i < n; ++i) out[i] = PtLightAlias{(float)prob[i], (int)alias[i]};
+    return out;
+}
+
 }  // namespace
 
 int UploadShading(rtb200_scene* s)
@@ -179,6 +213,10 @@ int UploadShading(rtb200_scene* s)
     // luminary weights above omit the common factor pi, so the point light's
     // weight drops it too: max(colour x power) x 4.
     for (const auto& pl : s->point_lights) {
+        // A light that emits nothing is left out, as LightSampler::Prepare
+        // keeps only lights of positive exitance.
+        const double wp = std::max({(double)pl.color[0], (double)pl.color[1], (double)pl.color[2]}) * pl.power * 4.0;
+        if (!(wp > 0.0)) continue;
         PtLight L{};
         L.kind = 1;
         L.emit = -1;
@@ -188,14 +226,14 @@ int UploadShading(rtb200_scene* s)
         for (int k = 0; k < 3; ++k) L.pos[k] = pl.pos[k];
         LightPrim box{};
         for (int k = 0; k < 3; ++k) { box.lo[k] = box.hi[k] = pl.pos[k]; }
-        weight.push_back(std::max({(double)pl.color[0], (double)pl.color[1], (double)pl.color[2]}) * pl.power *
-                         4.0);
+        weight.push_back(wp);
         boxes.push_back(box);
         s->lights.push_back(L);
     }
     double wsum = 0.0;
     for (double w : weight) wsum += w;
     for (size_t i = 0; i < s->lights.size(); ++i) s->lights[i].pdf = (float)(weight[i] / wsum);
+    s->light_alias = BuildAlias(weight);
     s->light_nodes.clear();
     if (s->lights.size() > 1) {
         std::vector<LightPrim> prims(s->lights.size());
@@ -273,6 +311,7 @@ int UploadShading(rtb200_scene* s)
     if (!rc) rc = Upload(ctx, &s->d_lights, s->lights, total);
     if (!rc) rc = Upload(ctx, &s->d_light_tris, s->light_tris, total);
     if (!rc && !s->light_nodes.empty()) rc = Upload(ctx, &s->d_light_nodes, s->light_nodes, total);
+    if (!rc && !s->light_alias.empty()) rc = Upload(ctx, &s->d_light_alias, s->light_alias, total);
     s->shade_bytes = total;
     if (rc) FreeShading(s);
     return rc;
@@ -287,7 +326,9 @@ void FreeShading(rtb200_scene* s)
     DevFree(ctx, s->d_lights, s->lights.size() * sizeof(PtLight));
     DevFree(ctx, s->d_light_tris, s->light_tris.size() * sizeof(PtLightTri));
     DevFree(ctx, s->d_light_nodes, s->light_nodes.size() * sizeof(PtLightNode));
+    DevFree(ctx, s->d_light_alias, s->light_alias.size() * sizeof(PtLightAlias));
     s->d_light_nodes = nullptr;
+    s->d_light_alias = nullptr;
     s->d_attr = nullptr;
     s->d_mats = nullptr;
     s->d_spectra = nullptr;

@@ -46,6 +46,77 @@ __device__ __forceinline__ float Rand(uint32_t key, uint32_t dim)
 // roulette 19, sky sample i at j = 20 + 2i, 21 + 2i.
 __device__ __forceinline__ uint32_t Dim(int depth, int j) { return 8u + 32u * (uint32_t)depth + (uint32_t)j; }
 
+// ---- the reference's sampler: Owen-scrambled padded Sobol ------------------
+// SobolSequence (Sampling/SobolSequence.h:55-206): dimension d of sample i is
+// Sobol dimension d & 1 of i (dimension 0 the bit-reversed index, dimension 1
+// the XOR of the direction numbers v_0 = 2^31, v_{k+1} = v_k ^ (v_k >> 1) over
+// the set bits of i), Owen-scrambled by the Laine-Karras hash seeded with
+// HashCombine(seed, d) (Burley 2020, "Practical Hash-based Owen Scrambling").
+
+// HashCombine: a ^= b + golden + (a << 6) + (a >> 2), then MurmurHash3's
+// fmix32 finaliser.
+__device__ __forceinline__ uint32_t HashCombine(uint32_t a, uint32_t b)
+{
+    a ^= b + 0x9e3779b9u + (a << 6) + (a >> 2);
+    a ^= a >> 16; a *= 0x85ebca6bu;
+    a ^= a >> 13; a *= 0xc2b2ae35u;
+    a ^= a >> 16;
+    return a;
+}
+
+__device__ __forceinline__ uint32_t SobolDim1(uint32_t i)
+{
+    uint32_t v = 0, d = 1u << 31;
+    while (i) {
+        if (i & 1u) v ^= d;
+        d ^= d >> 1;
+        i >>= 1;
+    }
+    return v;
+}
+
+__device__ __forceinline__ float SobolSample(uint32_t index, uint32_t dim, uint32_t seed)
+{
+    uint32_t v = (dim & 1u) ? SobolDim1(index) : __brev(index);
+    const uint32_t s = HashCombine(seed, dim);
+    v = __brev(v);
+    v ^= v * 0x3d20adeau;
+    v += s;
+    v *= (s >> 16) | 1u;
+    v ^= v * 0x05526c56u;
+    v ^= v * 0x53a22864u;
+    v = __brev(v);
+    return (float)(v >> 8) * (1.0f / 16777216.0f);   // the top 24 bits: < 1 in FP32
+}
+
+// Sobol seed of a pixel: the reference's HashCombine(x, y); a nonzero job seed
+// is mixed in so that renders with different seeds are independent.
+__device__ __forceinline__ uint32_t SobolPixelSeed(uint32_t x, uint32_t y, uint32_t seed)
+{
+    const uint32_t s = HashCombine(x, y);
+    return seed ? HashCombine(s, seed) : s;
+}
+
+// Random numbers of one path vertex.  Hash mode: Rand(key, Dim(depth, j))
+// with the fixed layout above.  Sobol mode: the reference's
+// StartStream(16 + depth) then dimensions in the order they are drawn
+// (`cur`), so each call site names its hash-layout slot j and the Sobol
+// dimension follows the draw order; skip(n) consumes dimensions that the
+// reference draws but this vertex does not use.
+struct VertexRng {
+    uint32_t key;      // hash key, or the pixel's Sobol seed
+    uint32_t index;    // sample index (Sobol)
+    int depth;
+    int sobol;
+    uint32_t cur;
+    __device__ __forceinline__ float next(int j)
+    {
+        if (sobol) return SobolSample(index, (16u + (uint32_t)depth) * 32u + cur++, key);
+        return Rand(key, Dim(depth, j));
+    }
+    __device__ __forceinline__ void skip(int n) { cur += (uint32_t)n; }
+};
+
 // ---- spectra -----------------------------------------------------------------
 
 // Spectrum table: one float4 header per spectrum id, then the samples.

@@ -58,6 +58,14 @@ struct PtLightNode {
     int pad;
 };
 
+// Alias table over the luminaries for selection by power (Walker's alias
+// method, built with Vose's algorithm: Utilities/AliasTable.h): entry i keeps
+// i with probability prob, else gives alias.
+struct PtLightAlias {
+    float prob;
+    int alias;
+};
+
 struct PtLightTri {
     float v0[3];
     float e1[3];
@@ -93,7 +101,18 @@ struct PtSettings {
     float filt_sigma;        // Gaussian sigma in pixels (warp mode)
     float filt_trunc;        // exp(-K^2 / 2), K = half-width / sigma (warp mode)
     int light_bvh;           // pick NEE luminaries with the light BVH (when the scene has one)
+    int sampler;             // kSamplerHash / kSamplerSobol
+    int max_bounce[3];       // diffuse, glossy, transmission scatters a path may take (255 = no limit)
 };
+
+constexpr int kSamplerHash = 0;
+constexpr int kSamplerSobol = 1;
+
+// Bounce types (ScatteredRay::ScatRayType): the counters live in aux.w, one
+// byte each.
+constexpr int kBounceDiffuse = 0;
+constexpr int kBounceGlossy = 1;
+constexpr int kBounceTransmission = 2;
 
 // Film modes of PtSettings::filter.  The reference splats into a filtered
 // film only when the filter's half-support exceeds 0.501 pixel
@@ -155,6 +174,7 @@ struct PtScene {
     const PtLight* lights;
     const PtLightTri* light_tris;
     const PtLightNode* light_nodes;   // light BVH (null with fewer than two luminaries)
+    const PtLightAlias* light_alias;  // alias table over the luminaries (power selection)
 };
 
 struct PtPaths {

@@ -6,6 +6,8 @@
 // busy on the long tail of incoherent rays.  Rays are read as two 16-byte
 // vector loads and hits written as one 16-byte store; the traversal stack
 // lives in shared memory ([depth][thread], conflict-free).
+#include <atomic>
+
 #include "core.h"
 #include "raycast.cuh"
 
@@ -78,13 +80,21 @@ int GridFor(K kernel, int num_sms)
 }
 
 // One launch over `n` rays with the work counter and error word given.  The
-// grid is the kernel's occupancy times the SM count, cached per instantiation.
+// grid is the kernel's occupancy times the SM count, cached per instantiation
+// and device (devices of one process may differ).
+constexpr int kGridDevices = 64;
+
 template <class NodeT, bool ANY, bool SPILL>
 void Launch(const rtb200_scene* s, const rtb200_ray* d_rays, int64_t n, rtb200_hit* hits, uint8_t* occ,
             unsigned long long* counter, unsigned* err, cudaStream_t stream)
 {
-    static int grid = 0;
-    if (!grid) grid = GridFor(KTrace<NodeT, ANY, SPILL>, s->ctx->num_sms);
+    static std::atomic<int> grids[kGridDevices];
+    const int dev = s->ctx->device;
+    int grid = (dev >= 0 && dev < kGridDevices) ? grids[dev].load(std::memory_order_relaxed) : 0;
+    if (!grid) {
+        grid = GridFor(KTrace<NodeT, ANY, SPILL>, s->ctx->num_sms);
+        if (dev >= 0 && dev < kGridDevices) grids[dev].store(grid, std::memory_order_relaxed);
+    }
     KTrace<NodeT, ANY, SPILL><<<grid, kTraceBlock, 0, stream>>>((const NodeT*)s->d_nodes, s->d_tris, d_rays, n,
                                                                 (int)s->tri_material.size(), hits, occ, counter, err);
 }

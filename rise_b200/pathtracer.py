@@ -30,7 +30,9 @@ class RenderSettings(ctypes.Structure):
                 ("nee_per_lambda", ctypes.c_int32), ("seed", ctypes.c_uint32), ("max_paths", ctypes.c_int32),
                 ("filter", ctypes.c_int32), ("filter_size", ctypes.c_float), ("filter_sigma", ctypes.c_float),
                 ("adaptive_max_spp", ctypes.c_int32), ("adaptive_threshold", ctypes.c_float),
-                ("light_selection", ctypes.c_int32)]
+                ("light_selection", ctypes.c_int32), ("sampler", ctypes.c_int32), ("bounce_limits", ctypes.c_int32),
+                ("max_diffuse_bounce", ctypes.c_int32), ("max_glossy_bounce", ctypes.c_int32),
+                ("max_transmission_bounce", ctypes.c_int32)]
 
 
 class Stats(ctypes.Structure):
@@ -92,7 +94,17 @@ def settings_struct(st):
                           st.rr_min_depth, st.rr_threshold, st.nee_per_lambda, st.seed, st.max_paths,
                           getattr(st, "filter", 0), getattr(st, "filter_size", 2.0), getattr(st, "filter_sigma", 0.5),
                           getattr(st, "adaptive_max_spp", 0), getattr(st, "adaptive_threshold", 0.01),
-                          getattr(st, "light_selection", 0))
+                          getattr(st, "light_selection", 0), getattr(st, "sampler", 0),
+                          *bounce_limits(st))
+
+
+def bounce_limits(st):
+    """(bounce_limits, max diffuse, max glossy, max transmission) of a
+    scenes.RenderSettings: limits are on when any of them is set."""
+    lim = [getattr(st, "max_diffuse_bounce", None), getattr(st, "max_glossy_bounce", None),
+           getattr(st, "max_transmission_bounce", None)]
+    on = any(v is not None for v in lim)
+    return (int(on),) + tuple(int(v) if v is not None else 255 for v in lim)
 
 
 class SpectralRasterizer:

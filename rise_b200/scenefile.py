@@ -410,7 +410,8 @@ class _Loader:
                 "pixel_filter_paramB", "pixel_sampler", "pixel_sampler_param", "blue_noise_sampler",
                 "adaptive_max_samples", "adaptive_threshold", "rr_min_depth", "rr_threshold", "show_luminaires",
                 "oidn_denoise", "oidn_quality", "oidn_device", "oidn_prefilter", "light_bvh", "defaultshader",
-                "progressive_rendering", "progressive_samples_per_pass"}
+                "progressive_rendering", "progressive_samples_per_pass", "max_diffuse_bounce", "max_glossy_bounce",
+                "max_transmission_bounce", "max_translucent_bounce", "max_volume_bounce"}
         self.only(c, base | extra)
         self.spp = int(c.get("samples", 32))
         lo, hi = float(c.get("nmbegin", 380.0)), float(c.get("nmend", 780.0))
@@ -434,10 +435,18 @@ class _Loader:
             self.st["rr_min_depth"] = int(c.get("rr_min_depth"))
         if c.has("rr_threshold"):
             self.st["rr_threshold"] = float(c.get("rr_threshold"))
+        # Per-type bounce limits (StabilityConfig); translucent and volume
+        # bounces cannot occur with the materials read here.
+        for k in ("max_diffuse_bounce", "max_glossy_bounce", "max_transmission_bounce"):
+            if c.has(k):
+                self.st[k] = int(c.get(k))
+        # The reference's integrator always draws its path decisions from its
+        # Owen-scrambled Sobol sampler (PathTracingSpectralRasterizer.cpp:206-479).
+        self.st["sampler"] = scenes.SAMPLER_SOBOL
         if not _bool(c.get("show_luminaires", "true")):
             self.refuse(c, "hidden luminaires (show_luminaires false) are not supported")
-        for k, why in (("pixel_sampler", "the pixel sampler (Sobol by default) is replaced by counter-based "
-                        "random numbers"), ("oidn_denoise", "the film is not denoised"),
+        for k, why in (("pixel_sampler", "camera jitter is drawn from the path's Sobol dimensions 0 and 1, "
+                        "whatever pixel sampler is named"), ("oidn_denoise", "the film is not denoised"),
                        ("light_bvh", "lights are picked by emitted power")):
             self.notes.append(f"{c.keyword}: {why}")
         if not _bool(c.get("hwss", c.get("use_hwss", "false"))) or c.get("num_wavelengths", "4") != "4":

@@ -242,6 +242,10 @@ def spectral_painter(nm, amplitudes, nmbegin=400.0, nmend=700.0):
     return SpectralPacket(float(nmbegin), float(nmend), amps.astype(np.float32))
 
 
+SAMPLER_HASH = 0    # counter-based hash of (seed, pixel, sample, dimension)
+SAMPLER_SOBOL = 1   # the reference's Owen-scrambled padded Sobol
+
+
 @dataclass
 class RenderSettings:
     width: int = 256
@@ -264,6 +268,10 @@ class RenderSettings:
     adaptive_max_spp: int = 0       # adaptive sampling: maximum samples per pixel (0 = off)
     adaptive_threshold: float = 0.01  # adaptive sampling: relative standard error to converge
     light_selection: int = 0  # 0 light BVH (more than one luminary), 1 by emitted power
+    sampler: int = 0          # 0 counter-based hash, 1 the reference's Owen-scrambled Sobol
+    max_diffuse_bounce: int = None       # per-type bounce limits (None = unlimited)
+    max_glossy_bounce: int = None
+    max_transmission_bounce: int = None
 
 
 @dataclass

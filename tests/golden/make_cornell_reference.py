@@ -1,14 +1,27 @@
-"""Generate tests/golden/cornell_fp64_16384spp.npz: the converged spectral
-Cornell box (256x256, HWSS 4 wavelengths, max depth 8, Russian roulette from
-depth 3, per-wavelength next-event estimation) rendered by the FP64 oracle
-(oracle/pt_oracle.cpp) at 16384 samples per pixel with seed 424242, which no
-GPU run uses.  Stored as float32 XYZ (256, 256, 3).
+"""Generate the C1 Cornell box fixtures from the reference renderer itself
+(oracle/_ref/librise_ref.so, built from the reference sources by
+oracle/rise_ref.mk), on tests/golden/cornell_c1.RISEscene:
 
-The oracle's noise at 16384 spp (relMSE ~2e-5) is far below the 1e-3 level the
-relMSE figures are judged at, so GPU relMSE against this image measures the
-GPU's own noise plus any bias.
+* cornell_c1_ref_fp64.npz -- the converged image: mean XYZ (256, 256, 3)
+  of 16384 samples per pixel in FP64 (stored as float32), through the
+  reference's per-sample function with its own pixel seeding
+  HashCombine(x, y) (oracle.RefRenderer.integrate, batch 0).  Its noise
+  (relMSE ~3e-5) is far below the 1e-3 level that relMSE figures are judged
+  at, so a GPU image's relMSE against it measures the GPU's noise plus any
+  bias.
+* cornell_c1_ref_k16.npz -- per-pixel mean and variance (ddof 1) of XYZ over
+  16 independent batches of 16 samples per pixel (batches 1..16: the batch
+  number mixed into the Sobol seed), for the per-pixel z-test of the GPU
+  path tracer against the reference at equal samples per pixel.
+* cornell_c1_ref_k16_independent.npz -- the same with the reference's
+  IndependentSampler (uniform numbers from a Mersenne twister) in place of
+  its Sobol sampler: the reference integrator's estimate without the small
+  bias its padded Sobol sequence carries (images about 0.1-0.3 % brighter
+  than with independent numbers), for a tight test of the image mean.
 
-    make -C oracle && python tests/golden/make_cornell_reference.py   # ~30 min on 8 cores
+    make -C oracle && python tests/golden/make_cornell_reference.py [k16|k16i|fp64]
+    (k16, k16i: ~40 s each, fp64: ~45 min on 8 cores; rows are checkpointed under
+    oracle/_ref/ so an interrupted run resumes)
 """
 import os
 import sys
@@ -17,28 +30,48 @@ import time
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
 
 import oracle  # noqa: E402
-from rise_b200 import scenes  # noqa: E402
 
-SPP = 16384
-SEED = 424242
-CHUNK = 256
+SCENE = os.path.join(HERE, "cornell_c1.RISEscene")
+K, K_SPP = 16, 16
+FP64_SPP = 16384
+ROWS = 8
+
+
+def make_k16(r, independent=False):
+    t0 = time.time()
+    b = np.array([r.integrate(K_SPP, batch=k, independent=independent) for k in range(1, K + 1)])
+    name = "cornell_c1_ref_k16_independent.npz" if independent else "cornell_c1_ref_k16.npz"
+    np.savez_compressed(os.path.join(HERE, name), mean=b.mean(0).astype(np.float32),
+                        var=b.var(0, ddof=1).astype(np.float32), k=K, spp=K_SPP)
+    print(f"{name}: {time.time() - t0:.0f} s", flush=True)
+
+
+def make_fp64(r):
+    ck = os.path.join(ROOT, "oracle", "_ref", "cornell_c1_fp64_rows.npy")
+    img = np.load(ck) if os.path.exists(ck) else np.full((r.height, r.width, 3), np.nan)
+    t0 = time.time()
+    for y0 in range(0, r.height, ROWS):
+        if not np.isnan(img[y0:y0 + ROWS]).any():
+            continue
+        img[y0:y0 + ROWS] = r.integrate(FP64_SPP, batch=0, rect=(0, y0, r.width, y0 + ROWS))
+        np.save(ck, img)
+        print(f"rows {y0 + ROWS}/{r.height}, {time.time() - t0:.0f} s", flush=True)
+    np.savez_compressed(os.path.join(HERE, "cornell_c1_ref_fp64.npz"), xyz=img.astype(np.float32), spp=FP64_SPP)
 
 
 def main():
-    desc = scenes.cornell_box(256, 256)
-    settings = scenes.RenderSettings(**{**desc.settings.__dict__, "seed": SEED})
-    acc = np.zeros((256, 256, 3), np.float64)
-    t0 = time.time()
-    for begin in range(0, SPP, CHUNK):
-        acc += oracle.pt_render(desc, CHUNK, sample_begin=begin, settings=settings) * CHUNK
-        print(f"{begin + CHUNK}/{SPP} spp, {time.time() - t0:.0f} s", flush=True)
-    img = (acc / SPP).astype(np.float32)
-    path = os.path.join(HERE, "cornell_fp64_16384spp.npz")
-    np.savez_compressed(path, xyz=img, spp=SPP, seed=SEED)
-    print("wrote", path, os.path.getsize(path), "bytes")
+    which = sys.argv[1:] or ["k16", "k16i", "fp64"]
+    r = oracle.RefRenderer(SCENE)
+    if "k16" in which:
+        make_k16(r)
+    if "k16i" in which:
+        make_k16(r, independent=True)
+    if "fp64" in which:
+        make_fp64(r)
 
 
 if __name__ == "__main__":

@@ -1,0 +1,105 @@
+"""Write the C1 spectral Cornell box as a scene in the reference's own scene
+language: tests/golden/cornell_c1.RISEscene plus one RAW triangle file per
+object (tests/golden/cornell_c1_*.raw).
+
+The same files are loaded by the reference renderer (its .RISEscene parser,
+through oracle/_ref/librise_ref.so) and by this package's scene ingest
+(rise_b200.scenefile), so both render one scene description.
+
+Geometry is scenes.cornell_box()'s 32 triangles: five unit-square walls as
+triangle meshes (not clipped planes, which the reference intersects as
+bilinear patches), two boxes rotated about the vertical axis, and a
+0.25 x 0.25 light quad just below the ceiling facing down (one-sided).
+Spectra are spectral_painter chunks with 30 control points every 10 nm on
+400..700 nm, so the reference's painter (control points sampled into 30
+bins, step lookup) gives exactly: white 0.75; red 0.6 on [600, 700], 0.05
+below; green 0.6 on [500, 570), 0.05 elsewhere; light exitance 15 with
+scale pi, i.e. radiance 15 (LambertianEmitter divides by pi).  HWSS with 4
+wavelengths on 400..700 nm, box pixel filter of width 1, Russian roulette
+from depth 3, at most 7 diffuse bounces (8 path vertices, the config's max
+depth 8), 256 x 256, 16 samples per pixel.
+
+    python tests/golden/make_cornell_scene.py
+"""
+import math
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+
+from rise_b200 import scenes  # noqa: E402
+
+NAME = "cornell_c1"
+
+
+def band(lo, hi, inside, outside):
+    """Control points every 10 nm: `inside` for lo <= nm < hi, else `outside`."""
+    nm = np.arange(400, 700, 10)
+    return [(float(n), inside if lo <= n < hi else outside) for n in nm]
+
+
+SPECTRA = {
+    "pnt_white": band(400, 710, 0.75, 0.75),
+    "pnt_red": band(600, 710, 0.6, 0.05),
+    "pnt_green": band(500, 570, 0.6, 0.05),
+    "pnt_light": band(400, 710, 15.0, 15.0),
+}
+
+
+def scene_text(width=256, height=256, spp=16):
+    d = scenes.cornell_box(width, height)
+    st = d.settings
+    groups = [("walls_white", 0, "white", True), ("wall_red", 1, "red", True),
+              ("wall_green", 2, "green", True), ("boxes", 3, "white", True), ("light", 4, "light", False)]
+    raw = {}
+    for name, mesh, _, _ in groups:
+        first, count, _, _ = d.meshes[mesh]
+        raw[name] = d.tri9[first:first + count]
+    out = ["RISE ASCII SCENE 7", "",
+           "# The C1 spectral Cornell box (written by tests/golden/make_cornell_scene.py).", ""]
+    # The rasterizer's default shader must exist, even though the spectral
+    # path tracer integrates on its own.
+    out += ["pathtracing_shaderop", "{", "\tname\t\tpt", "}", "",
+            "standard_shader", "{", "\tname\t\tglobal", "\tshaderop\tpt", "}", ""]
+    out += ["pathtracing_spectral_rasterizer", "{",
+            f"\tsamples\t\t\t\t{spp}", f"\tnmbegin\t\t\t\t{st.lambda_min:g}", f"\tnmend\t\t\t\t{st.lambda_max:g}",
+            "\thwss\t\t\t\ttrue", "\tspectral_samples\t1", "\tpixel_filter\t\tbox", "\tpixel_filter_width\t1",
+            "\tpixel_filter_height\t1", f"\trr_min_depth\t\t{st.rr_min_depth}",
+            f"\tmax_diffuse_bounce\t{st.max_depth - 1}", "}", ""]
+    out += ["film", "{", f"\twidth\t\t{width}", f"\theight\t\t{height}", "}", ""]
+    out += ["pinhole_camera", "{", "\tlocation\t%g %g %g" % st.cam_pos, "\tlookat\t\t%g %g %g" % st.cam_look,
+            "\tup\t\t\t%g %g %g" % st.cam_up, f"\tfov\t\t\t{st.fov_deg:g}", "}", ""]
+    for name, cps in SPECTRA.items():
+        out += ["spectral_painter", "{", f"\tname\t\t{name}", "\tnmbegin\t\t400", "\tnmend\t\t700"]
+        out += [f"\tcp\t\t\t{a:g} {b:g}" for a, b in cps]
+        out += ["}", ""]
+    for m in ("white", "red", "green"):
+        out += ["lambertian_material", "{", f"\tname\t\t{m}", f"\treflectance\tpnt_{m}", "}", ""]
+    out += ["lambertian_luminaire_material", "{", "\tname\t\tlight", "\texitance\tpnt_light",
+            f"\tscale\t\t{math.pi:.17g}", "\tmaterial\tnone", "}", ""]
+    for name, _, mat, ds in groups:
+        out += ["rawmesh_geometry", "{", f"\tname\t\tg_{name}", f"\tfile\t\t{NAME}_{name}.raw",
+                f"\tdouble_sided\t{'true' if ds else 'false'}", "}", ""]
+        out += ["standard_object", "{", f"\tname\t\to_{name}", f"\tgeometry\tg_{name}", f"\tmaterial\t{mat}",
+                "}", ""]
+    return "\n".join(out), raw
+
+
+def raw_text(tri9):
+    return "".join("tri " + " ".join(f"{float(v):.9g}" for v in t) + "\n" for t in tri9)
+
+
+def main():
+    text, raw = scene_text()
+    with open(os.path.join(HERE, NAME + ".RISEscene"), "w") as f:
+        f.write(text)
+    for name, tri9 in raw.items():
+        with open(os.path.join(HERE, f"{NAME}_{name}.raw"), "w") as f:
+            f.write(raw_text(tri9))
+
+
+if __name__ == "__main__":
+    main()

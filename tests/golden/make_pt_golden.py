@@ -193,6 +193,18 @@ def main():
         rows.append([depth, mind, thr, cur, prev, u, t, s.value])
     out["russian_roulette"] = rows
 
+    # Owen-scrambled Sobol (Sampling/SobolSequence.h): value * 2^32 as an
+    # integer, for indices, dimensions and seeds including the edges.
+    srng = np.random.default_rng(17)
+    idx = np.concatenate([[0, 1, 2, 3, 255, 256, 65535, 2**31, 2**32 - 1],
+                          srng.integers(0, 2**32, 55, dtype=np.uint64)]).astype(np.uint32)
+    dim = np.concatenate([[0, 1, 2, 3, 31, 32, 543, 544, 1023], srng.integers(0, 1024, 55)]).astype(np.uint32)
+    seed = srng.integers(0, 2**32, idx.size, dtype=np.uint64).astype(np.uint32)
+    vals = oracle.sobol(idx, dim, seed, "ref")
+    out["sobol"] = [[int(a), int(b), int(c), int(round(v * 4294967296.0))] for a, b, c, v in zip(idx, dim, seed, vals)]
+    hc = oracle.hash_combine(idx, seed, "ref")
+    out["hash_combine"] = [[int(a), int(c), int(h)] for a, c, h in zip(idx, seed, hc)]
+
     ess, eavg = oracle.energy_tables(r, "ref_pt_")
     out["energy_tables"] = {"ess": ess.round(8).tolist(), "eavg": eavg.round(8).tolist()}
 

@@ -96,3 +96,27 @@ def any_report(tri9, rays, occ, ref_occ):
             for c in cand)
         (excluded if marginal else bad).append(int(i))
     return {"n": len(rays), "bad": bad, "excluded": excluded}
+
+
+# ---- image statistics ---------------------------------------------------------
+# Per-pixel z-test of two renderers at equal samples per pixel: each side gives
+# K independent batches; z = (mean_a - mean_b) / sqrt(var_a / K + var_b / K)
+# per pixel and channel (var with ddof 1).  With Gaussian batch means, |z| > 3
+# has probability 0.27 %; the test allows three times that, which covers the
+# heavier tails of a statistic whose variances are themselves estimated from
+# 16 batches (about 0.5 % expected).
+Z_LIMIT = 3.0
+Z_GAUSS_RATE = 0.0027
+Z_ALLOWED_RATE = 3 * Z_GAUSS_RATE
+
+
+def z_scores(mean_a, var_a, k_a, mean_b, var_b, k_b):
+    """z per pixel and channel where either side has any variance."""
+    den = np.sqrt(var_a / k_a + var_b / k_b)
+    ok = den > 0
+    return (mean_a - mean_b)[ok] / den[ok], ok
+
+
+def rel_mse(x, ref):
+    """Mean over pixels and channels of (x - r)^2 / (r^2 + 1e-2)."""
+    return float(np.mean((x - ref) ** 2 / (ref ** 2 + 1e-2)))

@@ -132,6 +132,17 @@ def test_golden_colour_resolve_and_display(port):
         assert got.tolist() == want, (rgb, ev, tone, got, want)
 
 
+def test_golden_sobol_and_hash_combine():
+    # The reference's padded Owen-scrambled Sobol and its pixel-seed hash
+    # (Sampling/SobolSequence.h:55-206), bit for bit.
+    g = np.array(GOLDEN["sobol"], np.uint64)
+    got = oracle.sobol(g[:, 0].astype(np.uint32), g[:, 1].astype(np.uint32), g[:, 2].astype(np.uint32))
+    assert np.array_equal(got.astype(np.uint64), g[:, 3])
+    h = np.array(GOLDEN["hash_combine"], np.uint64)
+    assert np.array_equal(oracle.hash_combine(h[:, 0].astype(np.uint32), h[:, 1].astype(np.uint32)).astype(np.uint64),
+                          h[:, 2])
+
+
 def test_golden_gaussian_filter(port):
     for size, sigma, dx, dy, want in GOLDEN["gaussian_filter"]:
         assert close(port.orc_pt_gaussian_weight(size, sigma, dx, dy), want, 1e-14), (size, sigma, dx, dy)
@@ -273,6 +284,17 @@ def test_random_roulette_and_mis(port, ref):
         assert t1 == t2 and (t1 or s1.value == s2.value)
         a, b = rng.exponential(1, 2)
         assert port.orc_pt_power_heuristic(a, b) == ref.ref_pt_power_heuristic(a, b)
+
+
+def test_random_sobol_and_hash_combine(ref):
+    rng = np.random.default_rng(5)
+    n = 200000
+    idx = rng.integers(0, 2**32, n, dtype=np.uint64).astype(np.uint32)
+    dim = rng.integers(0, 4096, n).astype(np.uint32)
+    seed = rng.integers(0, 2**32, n, dtype=np.uint64).astype(np.uint32)
+    assert np.array_equal(oracle.sobol(idx, dim, seed).astype(np.float64) / 4294967296.0,
+                          oracle.sobol(idx, dim, seed, "ref"))
+    assert np.array_equal(oracle.hash_combine(idx, seed), oracle.hash_combine(idx, seed, "ref"))
 
 
 def test_random_gaussian_filter(port, ref):

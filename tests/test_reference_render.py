@@ -1,0 +1,92 @@
+"""The path-tracing oracle against the reference renderer itself (CPU).
+
+The reference fixtures (tests/golden/cornell_c1_ref_k16.npz: per-pixel mean
+and variance of XYZ over 16 independent batches of 16 samples per pixel;
+generator tests/golden/make_cornell_reference.py) come from the reference
+renderer's own integrator (oracle/_ref/librise_ref.so, built from its
+sources) on the C1 Cornell box scene tests/golden/cornell_c1.RISEscene, which
+this package's scene ingest reads too.  The oracle restates the device path
+tracer in FP64 with the same Sobol sampler, so holding it to the reference
+here pins the restatement that the GPU tests compare against sample by
+sample.
+"""
+import dataclasses
+import os
+
+import numpy as np
+import pytest
+
+import oracle
+from rise_b200 import scenefile
+from parity import Z_ALLOWED_RATE, Z_LIMIT, rel_mse, z_scores
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+SCENE = os.path.join(GOLDEN, "cornell_c1.RISEscene")
+ROWS = (96, 160)   # 64 rows x 256 columns keeps the CPU test short
+
+
+def ref_k16(independent=False):
+    f = np.load(os.path.join(GOLDEN, "cornell_c1_ref_k16_independent.npz" if independent else "cornell_c1_ref_k16.npz"))
+    return f["mean"].astype(np.float64), f["var"].astype(np.float64), int(f["k"]), int(f["spp"])
+
+
+# The reference's padded Sobol sampler makes its images about 0.1-0.3 %
+# brighter than the same integrator given independent numbers (measured with
+# the harness's IndependentSampler switch); the restatement's own Sobol draws
+# land about 0.2 % below its hash-sampler images.  Image means against the
+# Sobol fixture are therefore held to 0.5 %, against the independent-sampler
+# fixture to the statistics alone.
+SOBOL_MEAN_TOL = 5e-3
+
+
+def test_scene_ingest_reads_the_reference_settings():
+    ls = scenefile.load_scene(SCENE)
+    st = ls.desc.settings
+    assert (st.width, st.height, ls.spp) == (256, 256, 16)
+    assert st.sampler == 1 and st.max_diffuse_bounce == 7 and st.rr_min_depth == 3
+    assert (st.lambda_min, st.lambda_max) == (400.0, 700.0) and st.filter == 0
+    assert ls.desc.n_tri == 32
+
+
+@pytest.mark.parametrize("sampler", [0, 1], ids=["hash_vs_independent", "sobol_vs_sobol"])
+def test_oracle_matches_reference_renderer_z_test(sampler):
+    """16 batches of 16 spp of the restatement against the reference's 16:
+    the hash sampler against the reference with independent numbers, the
+    Sobol sampler against the reference's own Sobol sampler."""
+    mr, vr, k, spp = ref_k16(independent=sampler == 0)
+    ls = scenefile.load_scene(SCENE)
+    st = ls.desc.settings
+    y0, y1 = ROWS
+    crop = (0, y0, st.width, y1)
+    g = np.array([oracle.pt_render(ls.desc, spp, crop=crop,
+                                   settings=dataclasses.replace(st, seed=500 + b, sampler=sampler))
+                  for b in range(k)])
+    z, _ = z_scores(g.mean(0), g.var(0, ddof=1), k, mr[y0:y1], vr[y0:y1], k)
+    assert (np.abs(z) > Z_LIMIT).mean() <= Z_ALLOWED_RATE, (np.abs(z) > Z_LIMIT).mean()
+    # Image mean: within 4 standard errors of the batch-to-batch spread.
+    se = np.sqrt(g[..., 1].mean(axis=(1, 2)).var(ddof=1) / k + vr[y0:y1, :, 1].mean() / k / g[0, ..., 1].size)
+    tol = 4 * se + (SOBOL_MEAN_TOL * mr[y0:y1, :, 1].mean() if sampler else 0.0)
+    assert abs(g[..., 1].mean() - mr[y0:y1, :, 1].mean()) < tol
+
+
+def test_harness_pixel_loop_matches_the_reference_pipeline():
+    """The fixtures come from the reference's per-sample function under a
+    box-filter pixel loop restated in the harness; the reference's own
+    Job::Rasterize of the same scene must give the same picture: image means
+    within 1 %, and its relMSE against the 256-spp fixture (converted to
+    Rec.709 like the reference's film) at the level of one 16-spp batch."""
+    if oracle.rise_ref() is None:
+        pytest.skip("oracle/_ref/librise_ref.so not built (no reference tree)")
+    mr, vr, k, spp = ref_k16()
+    lib = oracle.port_blocks()
+    to_rgb = lambda xyz: oracle.xyz_to_rec709(lib, "orc_pt_", xyz.reshape(-1, 3)).reshape(xyz.shape)
+    r = oracle.RefRenderer(SCENE)
+    try:
+        full = r.render()
+        one = r.integrate(spp, batch=99)
+    finally:
+        r.close()
+    ref_rgb = to_rgb(mr)
+    assert abs(full.mean() / ref_rgb.mean() - 1) < 0.01
+    e_full, e_one = rel_mse(full, ref_rgb), rel_mse(to_rgb(one), ref_rgb)
+    assert 0.6 < e_full / e_one < 1.6, (e_full, e_one)
