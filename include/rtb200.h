@@ -92,6 +92,20 @@ int rtb200_scene_create(rtb200_ctx* ctx, rtb200_scene** out);
 int rtb200_scene_add_mesh(rtb200_scene* scene, const float* xyz, int64_t n_verts,
                           const uint32_t* tri, int64_t n_tri, int32_t material,
                           int32_t double_sided);
+/* The same with vertex normals for shading (ITriangleMeshGeometryIndexed's
+ * normal list and per-corner normal indices, IndexedTriangle::iNormals):
+ * normals holds n_normals float triples, tri_normals n_tri index triples
+ * into it.  The path tracer shades with the normal interpolated at the hit,
+ * n0 + (n1 - n0) a + (n2 - n0) b normalised
+ * (Geometry/TriangleMeshGeometryIndexedSpecializations.h:194-199,
+ * Objects/Object.cpp:543), the face normal oriented to its side serving as
+ * the geometric normal; a double-sided mesh turns each towards the incoming
+ * ray (TriangleMeshGeometryIndexed.cpp:170-188).  Normals must be finite and
+ * nonzero; they are stored unit length in a 32-bit octahedral encoding. */
+int rtb200_scene_add_mesh_normals(rtb200_scene* scene, const float* xyz, int64_t n_verts,
+                                  const uint32_t* tri, int64_t n_tri, const float* normals,
+                                  int64_t n_normals, const uint32_t* tri_normals, int32_t material,
+                                  int32_t double_sided);
 /* Build the BVH on the host (all cores) and upload it.  layout is one of
  * RTB200_BVH_*.  Meshes cannot be added after commit.  The device traversal
  * stack holds at most 128 deferred nodes; a BVH whose worst root-to-node path
@@ -112,7 +126,9 @@ int rtb200_scene_commit(rtb200_scene* scene, int32_t layout);
  * be NULL; n_bvh_nodes is 0 without a cache.
  *
  * rtb200_scene_add_risemesh adds the mesh's triangles (vertex positions
- * rounded to FP32; its own double-sided flag).  With use_cached_bvh and a
+ * rounded to FP32; its own double-sided flag) and, unless the file marks the
+ * mesh as shaded with face normals, its vertex normals for smooth shading
+ * (as rtb200_scene_add_mesh_normals).  With use_cached_bvh and a
  * cache in the file, the cache is checked (child pairs after their parent
  * and in range, each node reached once, leaf ranges inside the leaf order,
  * depth <= 1024, ordered boxes; RTB200_E_INVALID otherwise) and the scene's
@@ -128,6 +144,9 @@ int rtb200_risemesh_info(const rtb200_risemesh* mesh, int32_t* version, int64_t*
                          int32_t* double_sided, int64_t* n_bvh_nodes);
 /* The mesh's triangles as 9 floats each (v0, v1, v2), FP32-rounded. */
 int rtb200_risemesh_triangles(const rtb200_risemesh* mesh, float* tri9);
+/* The vertex normals of each triangle's corners, 9 floats per triangle;
+ * RTB200_E_INVALID when the mesh shades with face normals or has none. */
+int rtb200_risemesh_normals(const rtb200_risemesh* mesh, float* nrm9);
 int rtb200_risemesh_destroy(rtb200_risemesh* mesh);
 int rtb200_scene_add_risemesh(rtb200_scene* scene, const rtb200_risemesh* mesh, int32_t material,
                               int32_t use_cached_bvh);
@@ -148,7 +167,7 @@ int rtb200_scene_destroy(rtb200_scene* scene);
 /* Material models (reference classes under src/Library/Materials/). */
 #define RTB200_MAT_LAMBERTIAN 0   /* LambertianSPF + LambertianBRDF */
 #define RTB200_MAT_GGX        1   /* GGXSPF + GGXBRDF, conductor Fresnel */
-#define RTB200_MAT_DIELECTRIC 2   /* DielectricSPF, smooth, no BSDF */
+#define RTB200_MAT_DIELECTRIC 2   /* DielectricSPF, no BSDF */
 
 typedef struct {
     int32_t type;         /* RTB200_MAT_* */
@@ -156,7 +175,9 @@ typedef struct {
     int32_t emission;     /* spectrum id of emitted radiance (-1 = none);
                              LambertianEmitter: one-sided, radiance = spectrum */
     int32_t eta, kappa;   /* GGX conductor spectra (-1 = unused) */
-    float alpha;          /* GGX roughness */
+    float alpha;          /* GGX roughness; for a dielectric, the Phong exponent of
+                             its transmitted lobe (the reference's `scattering`,
+                             DielectricSPF.cpp:248-272; 0 or >= 1e6: smooth) */
     float ior;            /* dielectric index of refraction */
 } rtb200_material;
 

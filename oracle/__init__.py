@@ -229,13 +229,17 @@ def pt_render(desc, spp, sample_begin=0, crop=None, threads=None, settings=None,
     f.restype = ctypes.c_int
     i32 = ctypes.c_int32
     f.argtypes = [_f32p, _i64, _vp, i32, _f32p, i32, _vp, _f32p, i32, _vp, _f64p, _f64p, _vp, i32, i32,
-                  i32, i32, i32, i32, i32, _f64p, _f64p, _vp, i32, _f64p]
+                  i32, i32, i32, i32, i32, _f64p, _f64p, _vp, i32, _f64p, _f32p]
     points = np.array([list(p) + list(c) + [w] for p, c, w in getattr(desc, "point_lights", [])],
                       np.float64).reshape(-1, 7)
+    nrm9 = getattr(desc, "nrm9", None)
+    if nrm9 is not None:
+        nrm9 = np.ascontiguousarray(nrm9, np.float32)
     rc = f(_p(tri9, _f32p), len(tri9), meshes.ctypes.data, len(meshes), _p(spectra, _f32p), len(desc.spectra),
            mats_i.ctypes.data, _p(mats_f, _f32p), len(mats_i), envi.ctypes.data, _p(cam, _f64p), _p(setd, _f64p),
            seti.ctypes.data, int(spp), int(sample_begin), x0, y0, x1, y1, threads or os.cpu_count(),
-           _p(out, _f64p), _p(cie, _f64p), counts.ctypes.data, len(points), _p(points, _f64p))
+           _p(out, _f64p), _p(cie, _f64p), counts.ctypes.data, len(points), _p(points, _f64p),
+           _p(nrm9, _f32p) if nrm9 is not None else None)
     if rc != 0:
         raise RuntimeError("oracle path tracer rejected the scene")
     return (out, counts) if return_counts else out

@@ -70,6 +70,8 @@ int  orc_ray_triangle(const double* o, const double* d, const double* v0, const 
  *   setd:   6 doubles (lambda_min, lambda_max, rr_threshold, filter size, filter sigma,
  *           adaptive threshold)
  *   points: n_point x 7 doubles (position, colour, power) of point lights
+ *   nrm9:   n_tri x 9 floats, the vertex normals of each triangle's corners
+ *           (all zero: a flat triangle), or null
  *   seti:   14 int32 (width, height, max_depth, rr_min_depth, nee_per_lambda, seed, filter,
  *           adaptive maximum samples per pixel or 0, light selection: 0 light BVH, 1 power,
  *           sampler: 0 hash, 1 Owen-scrambled Sobol, bounce limits on, maximum diffuse,
@@ -92,7 +94,8 @@ int orc_pt_render(const float* tri9, int64_t n_tri, const int64_t* meshes, int32
                   int32_t n_mat, const int32_t* envi, const double* cam, const double* setd,
                   const int32_t* seti, int32_t spp, int32_t sample_begin, int32_t x0, int32_t y0,
                   int32_t x1, int32_t y1, int32_t threads, double* xyz, const double* cie,
-                  int32_t* counts, int32_t n_point, const double* points);
+                  int32_t* counts, int32_t n_point, const double* points,
+                  const float* nrm9);
 
 /* Building blocks of the path-tracing oracle, exported so tests can hold each
  * against the reference's own code (oracle/_ref/libref_pt.so). */

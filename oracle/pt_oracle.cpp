@@ -502,8 +502,28 @@ double LightBvhPdf(const std::vector<LightNode>& nodes, int pos, const double p[
 }
 struct LTri { V v0, e1, e2; double cdf; };
 
+// Octahedral unit-vector encoding as the device stores vertex normals
+// (Cigolle et al., JCGT 3(2), 2014; OctEncode, rise_b200/csrc/pt_types.h):
+// FP32 encode, decode back to a unit vector.
+inline unsigned OctEncode(float x, float y, float z)
+{
+    const float s = std::fabs(x) + std::fabs(y) + std::fabs(z);
+    float u = s > 0.0f ? x / s : 0.0f, v = s > 0.0f ? y / s : 0.0f;
+    if (z < 0.0f) {
+        const float fu = (1.0f - std::fabs(v)) * (u >= 0.0f ? 1.0f : -1.0f);
+        const float fv = (1.0f - std::fabs(u)) * (v >= 0.0f ? 1.0f : -1.0f);
+        u = fu;
+        v = fv;
+    }
+    const int qu = (int)std::rint(std::fmin(std::fmax(u, -1.0f), 1.0f) * 32767.0f);
+    const int qv = (int)std::rint(std::fmin(std::fmax(v, -1.0f), 1.0f) * 32767.0f);
+    return ((unsigned)qu & 0xffffu) | ((unsigned)qv << 16);
+}
+
 struct Scene {
     const float* tri9;
+    const float* nrm9 = nullptr;           // vertex normals per triangle corner, or null (face normals)
+    std::vector<unsigned> octN;            // their encodings, 3 per triangle (all zero: a flat triangle)
     std::vector<int> triMesh;
     const int64_t* meshes;
     const float* spectra;
@@ -692,6 +712,32 @@ double DielectricR(double cosI, double cosT, double ni, double nt)
     return std::min(1.0, num / den);
 }
 
+V OctDecode(unsigned q)
+{
+    const double u = (double)(float)((short)(q & 0xffffu) * (1.0f / 32767.0f));
+    const double v = (double)(float)((short)(q >> 16) * (1.0f / 32767.0f));
+    double x = u, y = v;
+    const double z = 1.0 - std::fabs(u) - std::fabs(v);
+    if (z < 0.0) {
+        x = (1.0 - std::fabs(v)) * (u >= 0.0 ? 1.0 : -1.0);
+        y = (1.0 - std::fabs(u)) * (v >= 0.0 ? 1.0 : -1.0);
+    }
+    return Norm(V{x, y, z});
+}
+
+// The reference's Moller-Trumbore barycentrics (alpha, beta) of a hit
+// triangle (RayTriangleIntersection.cpp:36-60).
+void Barycentrics(V o, V d, V a, V b, V c, double& al, double& be)
+{
+    const V ea = b - a, eb = c - a;
+    const V pv = Cross(d, eb);
+    const double det = Dot(ea, pv);
+    const V tv = o - a;
+    const V qv = Cross(tv, ea);
+    al = Dot(tv, pv) / det;
+    be = Dot(d, qv) / det;
+}
+
 // Hash key, or the pixel's Sobol seed, and the camera's numbers (dimensions
 // 0-2: jitter x, y, hero wavelength).
 inline uint32_t SampleKey(const Scene& S, uint32_t pixel, uint32_t sample)
@@ -753,12 +799,28 @@ void Sample(const Scene& S, uint32_t pixel, uint32_t sample, double xyz[3])
         const float* tv = S.tri9 + 9 * (size_t)prim;
         const V a = {tv[0], tv[1], tv[2]}, b = {tv[3], tv[4], tv[5]}, c = {tv[6], tv[7], tv[8]};
         const V nface = Norm(Cross(b - a, c - a));
-        V ng = nface;
         const int mesh = S.triMesh[prim];
         const int mat = (int)S.meshes[4 * mesh + 2];
         const bool ds = S.meshes[4 * mesh + 3] != 0;
         const int light = S.meshLight[mesh];
-        if (ds && Dot(ng, d) > 0) ng = -ng;
+        // Shading normal: vertex normals interpolated at the hit, normalised
+        // (TriangleMeshGeometryIndexedSpecializations.h:194-199, Object.cpp:543);
+        // geometric normal: the face normal on the shading normal's side.
+        V ns0 = nface;
+        if (!S.octN.empty() && (S.octN[3 * prim] | S.octN[3 * prim + 1] | S.octN[3 * prim + 2])) {
+            double al, be;
+            Barycentrics(o, d, a, b, c, al, be);
+            const V n0 = OctDecode(S.octN[3 * prim]), n1 = OctDecode(S.octN[3 * prim + 1]),
+                    n2 = OctDecode(S.octN[3 * prim + 2]);
+            ns0 = Norm(n0 + (n1 - n0) * al + (n2 - n0) * be);
+        }
+        V ng = Dot(nface, ns0) < 0 ? -nface : nface;
+        V nsv = ns0;
+        // Double-sided: both turned towards the ray (TriangleMeshGeometryIndexed.cpp:170-188).
+        if (ds) {
+            if (Dot(nsv, d) > 0) nsv = -nsv;
+            if (Dot(ng, d) > 0) ng = -ng;
+        }
         const V gnv = Dot(ng, d) < 0 ? ng : -ng;
         const int type = S.mi[5 * mat], refl = S.mi[5 * mat + 1], emit = S.mi[5 * mat + 2];
         if (emit >= 0 && Dot(-d, ng) > 0) {
@@ -780,8 +842,8 @@ void Sample(const Scene& S, uint32_t pixel, uint32_t sample, double xyz[3])
             // Smooth dielectric (DielectricSPF.cpp:120-300); constant index:
             // the wavelength bundle continues together.
             const double ior = S.mf[2 * mat + 1];
-            const bool entering = Dot(d, nface) < 0;
-            const V nn = entering ? nface : -nface;
+            const bool entering = Dot(d, ns0) < 0;
+            const V nn = entering ? ns0 : -ns0;
             const double n1 = entering ? 1.0 : ior, n2 = entering ? ior : 1.0;
             const double cosI = -Dot(d, nn), eta = n1 / n2;
             const double s2t = eta * eta * std::max(0.0, 1.0 - cosI * cosI);
@@ -792,17 +854,44 @@ void Sample(const Scene& S, uint32_t pixel, uint32_t sample, double xyz[3])
                 tdir = Norm(d * eta + nn * (eta * cosI - cosT));
                 R = DielectricR(cosI, cosT, n1, n2);
             }
-            rng.skip(2);   // ScatterNM's 2D sample, unused by a smooth interface
-            if (rng.next(18) < R) {
-                nd = Norm(d + nn * (2.0 * cosI));
-                btype = 1;
-            } else {
+            // ScatterNM's two numbers tilt the transmitted direction by the
+            // material's Phong lobe (DielectricSPF.cpp:248-272; none at an
+            // exponent of 0 or >= 1e6, mf[0] holding it for a dielectric).
+            const double u1 = rng.next(16), u2 = rng.next(17);
+            const double expo = S.mf[2 * mat];
+            bool refr = s2t < 1.0;
+            if (refr && expo > 0 && expo < 1e6) {
+                const double al = std::acos(std::pow(u1, 1.0 / (expo + 1.0)));
+                if (al > 0 && al < 0.5 * kPi) {
+                    V tx, ty;
+                    Frame(tdir, tx, ty);
+                    const double ph = 2.0 * kPi * u2;
+                    tdir = Norm(tdir * std::cos(al) + (tx * std::cos(ph) + ty * std::sin(ph)) * std::sin(al));
+                }
+            }
+            // Transmission must cross the surface; reflection must stay above
+            // the geometric surface, mirrored about it under total internal
+            // reflection (:221-243, :274-279).
+            if (refr && !(Dot(tdir, nn) < -kNearZero)) refr = false;
+            V rdir = Norm(d + nn * (2.0 * cosI));
+            bool refl = true;
+            if (!(Dot(rdir, gnv) > 0)) {
+                if (R >= 1.0) rdir = Norm(d - gnv * (2.0 * Dot(d, gnv)));
+                else refl = false;
+            }
+            // RandomlySelect over (transmitted 1 - R, reflected R).
+            if (rng.next(18) < 1.0 - R) {
+                if (!refr) break;
                 nd = tdir;
                 btype = 2;
+            } else {
+                if (!refl) break;
+                nd = rdir;
+                btype = 1;
             }
             for (double& k : kray) k = 1.0;
         } else {
-            const V ns = ng, r = -d;
+            const V ns = nsv, r = -d;
             const int nsamp = S.neePerLambda ? 4 : 1;
             for (int k = 0; k < nsamp; ++k) {
                 if (!S.lights.empty()) {
@@ -1195,12 +1284,29 @@ extern "C" int orc_pt_render(const float* tri9, int64_t n_tri, const int64_t* me
                              int32_t n_mat, const int32_t* envi, const double* cam, const double* setd,
                              const int32_t* seti, int32_t spp, int32_t sample_begin, int32_t x0, int32_t y0,
                              int32_t x1, int32_t y1, int32_t threads, double* xyz, const double* cie,
-                             int32_t* counts, int32_t n_point, const double* points)
+                             int32_t* counts, int32_t n_point, const double* points, const float* nrm9)
 {
     (void)n_spec;
     GetTables();
     Scene S;
     S.tri9 = tri9;
+    S.nrm9 = nrm9;
+    if (nrm9) {
+        // Encode as the device does: unit length in FP32, then OctEncode; a
+        // triangle without normals (all zero) stays flat.
+        S.octN.assign(3 * (size_t)n_tri, 0u);
+        for (int64_t t = 0; t < n_tri; ++t) {
+            const float* q = nrm9 + 9 * t;
+            bool any = false;
+            for (int k = 0; k < 9; ++k) any |= q[k] != 0.0f;
+            if (!any) continue;
+            for (int j = 0; j < 3; ++j) {
+                const float* n = q + 3 * j;
+                const float l = std::sqrt(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]);
+                S.octN[3 * t + j] = OctEncode(n[0] / l, n[1] / l, n[2] / l);
+            }
+        }
+    }
     S.meshes = meshes;
     S.spectra = spectra;
     S.mi = mats_i;

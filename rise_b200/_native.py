@@ -43,6 +43,7 @@ SIGNATURES = {
     "rtb200_risemesh_info": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _vp]),
     "rtb200_risemesh_destroy": (ctypes.c_int, [_vp]),
     "rtb200_risemesh_triangles": (ctypes.c_int, [_vp, _vp]),
+    "rtb200_risemesh_normals": (ctypes.c_int, [_vp, _vp]),
     "rtb200_rgb_uplift": (ctypes.c_int, [_vp, ctypes.c_int32, _vp]),
     "rtb200_rgb_uplift_table": (ctypes.c_int, [_vp]),
     "rtb200_scene_add_rgb_spectrum": (ctypes.c_int, [_vp, _vp, _vp]),
@@ -57,6 +58,8 @@ SIGNATURES = {
     "rtb200_cast_any_device": (ctypes.c_int, [_vp, _vp, _i64, _vp, _vp]),
     "rtb200_cast_closest_noalloc": (ctypes.c_int, [_vp, _vp, _i64, _vp, _vp]),
     "rtb200_scene_device_status": (ctypes.c_int, [_vp, _vp]),
+    "rtb200_scene_add_mesh_normals": (ctypes.c_int, [_vp, _vp, _i64, _vp, _i64, _vp, _i64, _vp, ctypes.c_int32,
+                                                     ctypes.c_int32]),
     "rtb200_scene_add_spectrum": (ctypes.c_int, [_vp, _vp, _vp]),
     "rtb200_scene_add_material": (ctypes.c_int, [_vp, _vp, _vp]),
     "rtb200_scene_set_environment": (ctypes.c_int, [_vp, _i32, _i32]),

@@ -5,6 +5,7 @@
 // a status code and leave a message in rtb200_last_error instead of logging.
 #include <algorithm>
 #include <chrono>
+#include <cmath>
 #include <cstring>
 #include <new>
 
@@ -265,19 +266,28 @@ int rtb200_scene_create(rtb200_ctx* ctx, rtb200_scene** out)
     return RTB200_OK;
 }
 
-int rtb200_scene_add_mesh(rtb200_scene* s, const float* xyz, int64_t n_verts, const uint32_t* tri,
-                          int64_t n_tri, int32_t material, int32_t double_sided)
+static int AddMesh(rtb200_scene* s, const float* xyz, int64_t n_verts, const uint32_t* tri, int64_t n_tri,
+            const float* nrm, int64_t n_nrm, const uint32_t* tri_nrm, int32_t material, int32_t double_sided)
 {
-    if (!s) return RTB200_E_INVALID;
     rtb200_ctx* ctx = s->ctx;
     std::lock_guard<std::mutex> g(ctx->mu);
     if (s->committed) return SetError(ctx, RTB200_E_INVALID, "scene already committed");
     if (n_verts < 0 || n_tri < 0 || (n_tri > 0 && (!xyz || !tri)))
         return SetError(ctx, RTB200_E_INVALID, "bad mesh arguments");
+    if (nrm && (n_nrm < 0 || (n_tri > 0 && !tri_nrm)))
+        return SetError(ctx, RTB200_E_INVALID, "bad normal arguments");
     if ((int64_t)(s->tri_material.size()) + n_tri > (int64_t)INT32_MAX)
         return SetError(ctx, RTB200_E_INVALID, "too many triangles");
     for (int64_t i = 0; i < 3 * n_tri; ++i)
         if ((int64_t)tri[i] >= n_verts) return SetError(ctx, RTB200_E_INVALID, "triangle index out of range");
+    if (nrm)
+        for (int64_t i = 0; i < 3 * n_tri; ++i) {
+            if ((int64_t)tri_nrm[i] >= n_nrm) return SetError(ctx, RTB200_E_INVALID, "normal index out of range");
+            const float* n = nrm + 3 * (size_t)tri_nrm[i];
+            if (!(std::isfinite(n[0]) && std::isfinite(n[1]) && std::isfinite(n[2])) ||
+                !(n[0] * n[0] + n[1] * n[1] + n[2] * n[2] > 0.0f))
+                return SetError(ctx, RTB200_E_INVALID, "normals must be finite and nonzero");
+        }
     s->meshes.push_back({(int64_t)s->tri_material.size(), n_tri, material, double_sided ? 1 : 0});
     const size_t base = s->tri9.size();
     s->tri9.resize(base + 9 * (size_t)n_tri);
@@ -287,7 +297,34 @@ int rtb200_scene_add_mesh(rtb200_scene* s, const float* xyz, int64_t n_verts, co
             std::memcpy(dst + 9 * i + 3 * j, xyz + 3 * (size_t)tri[3 * i + j], 12);
     s->tri_material.insert(s->tri_material.end(), (size_t)n_tri, material);
     s->tri_double_sided.insert(s->tri_double_sided.end(), (size_t)n_tri, (uint8_t)(double_sided ? 1 : 0));
+    if (nrm || !s->tri_nrm9.empty()) {
+        s->tri_nrm9.resize(s->tri9.size(), 0.0f);
+        s->tri_smooth.resize(s->tri_material.size(), 0);
+    }
+    if (nrm) {
+        float* nd = s->tri_nrm9.data() + base;
+        for (int64_t i = 0; i < n_tri; ++i)
+            for (int j = 0; j < 3; ++j)
+                std::memcpy(nd + 9 * i + 3 * j, nrm + 3 * (size_t)tri_nrm[3 * i + j], 12);
+        std::fill(s->tri_smooth.end() - n_tri, s->tri_smooth.end(), (uint8_t)1);
+    }
     return RTB200_OK;
+}
+
+int rtb200_scene_add_mesh(rtb200_scene* s, const float* xyz, int64_t n_verts, const uint32_t* tri,
+                          int64_t n_tri, int32_t material, int32_t double_sided)
+{
+    if (!s) return RTB200_E_INVALID;
+    return AddMesh(s, xyz, n_verts, tri, n_tri, nullptr, 0, nullptr, material, double_sided);
+}
+
+int rtb200_scene_add_mesh_normals(rtb200_scene* s, const float* xyz, int64_t n_verts, const uint32_t* tri,
+                                  int64_t n_tri, const float* normals, int64_t n_normals, const uint32_t* tri_normals,
+                                  int32_t material, int32_t double_sided)
+{
+    if (!s) return RTB200_E_INVALID;
+    if (!normals) return SetError(s->ctx, RTB200_E_INVALID, "no normals given");
+    return AddMesh(s, xyz, n_verts, tri, n_tri, normals, n_normals, tri_normals, material, double_sided);
 }
 
 int rtb200_scene_add_risemesh(rtb200_scene* s, const rtb200_risemesh* m, int32_t material, int32_t use_cached_bvh)
@@ -300,8 +337,15 @@ int rtb200_scene_add_risemesh(rtb200_scene* s, const rtb200_risemesh* m, int32_t
     const std::vector<Node2>* nodes = use_cached_bvh ? RisemeshBvh(m, &prims) : nullptr;
     if (nodes && !ValidBVH2(*nodes, prims->size()))
         return SetError(s->ctx, RTB200_E_INVALID, "the mesh's cached BVH is malformed");
-    const int rc = rtb200_scene_add_mesh(s, xyz.data(), (int64_t)(xyz.size() / 3), tri.data(),
-                                         (int64_t)(tri.size() / 3), material, RisemeshDoubleSided(m) ? 1 : 0);
+    std::vector<float> nrm;
+    std::vector<uint32_t> tri_nrm;
+    const bool smooth = RisemeshNormals(m, nrm, tri_nrm);
+    const int rc = smooth ? rtb200_scene_add_mesh_normals(s, xyz.data(), (int64_t)(xyz.size() / 3), tri.data(),
+                                                          (int64_t)(tri.size() / 3), nrm.data(),
+                                                          (int64_t)(nrm.size() / 3), tri_nrm.data(), material,
+                                                          RisemeshDoubleSided(m) ? 1 : 0)
+                          : rtb200_scene_add_mesh(s, xyz.data(), (int64_t)(xyz.size() / 3), tri.data(),
+                                                  (int64_t)(tri.size() / 3), material, RisemeshDoubleSided(m) ? 1 : 0);
     if (rc || !nodes || tri.empty()) return rc;
     std::lock_guard<std::mutex> g(s->ctx->mu);
     rtb200_scene::Mesh& mesh = s->meshes.back();

@@ -37,6 +37,10 @@ struct rtb200_scene {
     std::vector<float> tri9;
     std::vector<int32_t> tri_material;
     std::vector<uint8_t> tri_double_sided;
+    // Vertex normals (9 floats per triangle, corner order) of meshes added
+    // with normals; empty until the first such mesh, then as long as tri9.
+    std::vector<float> tri_nrm9;
+    std::vector<uint8_t> tri_smooth;
     struct Mesh {
         int64_t first, count;
         int32_t material;
@@ -90,6 +94,8 @@ struct rtb200_scene {
     rtb200::PtLightNode* d_light_nodes = nullptr;
     std::vector<rtb200::PtLightAlias> light_alias;  // built at commit
     rtb200::PtLightAlias* d_light_alias = nullptr;
+    std::vector<uint4> tri_normals;      // leaf order, built at commit (OctEncode)
+    uint4* d_tri_normals = nullptr;
     size_t shade_bytes = 0;
     bool committed = false;
     int32_t layout = RTB200_BVH_F32;
@@ -128,6 +134,7 @@ int SetError(rtb200_ctx* ctx, int code, const std::string& msg);
 bool RisemeshTriangles(const rtb200_risemesh* m, std::vector<float>& xyz, std::vector<uint32_t>& tri);
 const std::vector<rtb200::Node2>* RisemeshBvh(const rtb200_risemesh* m, const std::vector<uint32_t>** prims);
 bool RisemeshDoubleSided(const rtb200_risemesh* m);
+bool RisemeshNormals(const rtb200_risemesh* m, std::vector<float>& nrm, std::vector<uint32_t>& tri_nrm);
 
 int CudaCheck(rtb200_ctx* ctx, cudaError_t e, const char* what);
 

@@ -254,7 +254,8 @@ int EngineSubmit(rtb200_engine* e, rtb200_job* j, int spp)
     rtb200_scene* s = j->scene;
     PtJobDev& d = e->h_table[entry];
     d.scene = PtScene{s->d_nodes, s->layout, (int)s->n_nodes, s->d_tris, (int)s->tri_material.size(), s->d_attr, s->d_mats,
-                      s->d_spectra, s->d_lights, s->d_light_tris, s->d_light_nodes, s->d_light_alias};
+                      s->d_spectra, s->d_lights, s->d_light_tris, s->d_light_nodes, s->d_light_alias,
+                      s->d_tri_normals};
     d.cam = j->cam;
     d.set = j->set;
     int npx = j->npix;

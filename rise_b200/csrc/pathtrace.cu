@@ -582,12 +582,27 @@ KShade(const PtJobDev* __restrict__ jobs, PtPaths P, PtQueues Q, int from_class)
             const float* tb = reinterpret_cast<const float*>(S.tris + hslot);
             const float4 A = ldg4(tb), B = ldg4(tb + 4), C = ldg4(tb + 8);
             const V3 nface = normalize(cross(xyz(B) - xyz(A), xyz(C) - xyz(A)));
-            V3 ng = nface;
             const PtTriAttr at = S.attr[hslot];
             const int mi = at.mat & kAttrMatMask;
-            // Double-sided meshes face the incoming ray
+            // Shading normal: the vertex normals interpolated at the hit,
+            // n0 + (n1 - n0) a + (n2 - n0) b normalised, else the face normal
+            // (TriangleMeshGeometryIndexedSpecializations.h:194-199,
+            // Object.cpp:543); the geometric normal is the face normal turned
+            // to the shading normal's side.
+            V3 ns0 = nface;
+            if (at.mat & kAttrSmooth) {
+                const uint4 q = __ldg(S.tri_normals + hslot);
+                const V3 n0 = OctDecode(q.x), n1 = OctDecode(q.y), n2 = OctDecode(q.z);
+                ns0 = normalize(n0 + (n1 - n0) * h.z + (n2 - n0) * h.w);
+            }
+            V3 ng = dot(nface, ns0) < 0.0f ? -nface : nface;
+            V3 ns = ns0;
+            // Double-sided meshes turn both towards the incoming ray
             // (TriangleMeshGeometryIndexed.cpp:170-188).
-            if ((at.mat & kAttrDoubleSided) && dot(ng, d) > 0.0f) ng = -ng;
+            if (at.mat & kAttrDoubleSided) {
+                if (dot(ns, d) > 0.0f) ns = -ns;
+                if (dot(ng, d) > 0.0f) ng = -ng;
+            }
             const V3 gnv = dot(ng, d) < 0.0f ? ng : -ng;   // geometric normal facing the ray
             const PtMaterial M = S.mats[mi];
             const int mtype = CLS < 0 ? M.type : CLS;
@@ -618,8 +633,8 @@ KShade(const PtJobDev* __restrict__ jobs, PtPaths P, PtQueues Q, int from_class)
                 // refraction (DielectricSPF.cpp:120-300).  With a constant index
                 // every wavelength follows the hero's direction with the same
                 // weight, so the bundle continues together.
-                const bool entering = dot(d, nface) < 0.0f;
-                const V3 nn = entering ? nface : -nface;
+                const bool entering = dot(d, ns0) < 0.0f;
+                const V3 nn = entering ? ns0 : -ns0;
                 const float n1 = entering ? 1.0f : M.ior, n2 = entering ? M.ior : 1.0f;
                 const float cosI = -dot(d, nn);
                 const float eta = n1 / n2;
@@ -631,20 +646,49 @@ KShade(const PtJobDev* __restrict__ jobs, PtPaths P, PtQueues Q, int from_class)
                     tdir = normalize(d * eta + nn * (eta * cosI - cosT));
                     R = DielectricR(cosI, cosT, n1, n2);
                 }
-                // The reference's ScatterNM draws a 2D sample first, which the
-                // smooth interface does not use (DielectricSPF.cpp:421).
-                rng.skip(2);
-                if (rng.next(18) < R) {
-                    nd = normalize(d + nn * (2.0f * cosI));
-                    btype = kBounceGlossy;
-                } else {
+                // ScatterNM's two numbers (DielectricSPF.cpp:421) tilt the
+                // transmitted direction by a Phong lobe of the material's
+                // exponent: acos(u^(1/(n+1))) off it, uniform in azimuth
+                // (GenerateScatteredRay, :248-272; none at 0 or >= 1e6).
+                const float u1 = rng.next(16), u2 = rng.next(17);
+                bool refr = s2t < 1.0f;
+                if (refr && M.alpha > 0.0f && M.alpha < 1e6f) {
+                    const float a = acosf(powf(u1, 1.0f / (M.alpha + 1.0f)));
+                    if (a > 0.0f && a < 0.5f * kPi) {
+                        V3 tx, ty;
+                        Basis(tdir, tx, ty);
+                        float sp, cp, sa, ca;
+                        __sincosf(2.0f * kPi * u2, &sp, &cp);
+                        sincosf(a, &sa, &ca);
+                        tdir = normalize(tdir * ca + (tx * cp + ty * sp) * sa);
+                    }
+                }
+                // The transmitted ray must cross the surface (:274-279); the
+                // reflected one must stay above the geometric surface, and
+                // under total internal reflection mirrors about the geometric
+                // normal instead (:221-243).
+                if (refr && !(dot(tdir, nn) < -kNearZero)) refr = false;
+                V3 rdir = normalize(d + nn * (2.0f * cosI));
+                bool refl = true;
+                if (!(dot(rdir, gnv) > 0.0f)) {
+                    if (R >= 1.0f) rdir = normalize(d - gnv * (2.0f * dot(d, gnv)));
+                    else refl = false;
+                }
+                // RandomlySelect over (transmitted 1 - R, reflected R)
+                // (ScatteredRayContainer.cpp:43-70); a lobe the reference
+                // drops ends the path here with the same expectation.
+                if (rng.next(18) < 1.0f - R) {
+                    if (!refr) break;
                     nd = tdir;
                     btype = kBounceTransmission;
+                } else {
+                    if (!refl) break;
+                    nd = rdir;
+                    btype = kBounceGlossy;
                 }
                 for (int k = 0; k < 4; ++k) Set(kray, k, (term & (1u << k)) ? 0.0f : 1.0f);
                 nflags |= kFlagSpecular;
             } else {
-                const V3 ns = ng;
                 const V3 r = -d;
                 GgxPoint gp{1.0f, 0.0f, 0.0f, 0.0f};
                 if (mtype == kMatGGX) gp = GgxPointAt(M.alpha, fabsf(dot(r, ns)));

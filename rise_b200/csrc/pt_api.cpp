@@ -263,6 +263,24 @@ int UploadShading(rtb200_scene* s)
         attr[slot].mat = (mesh.material & kAttrMatMask) | (mesh.double_sided ? kAttrDoubleSided : 0);
         attr[slot].light = meshLight[mi];
     }
+    // Vertex normals in leaf order, unit length, octahedron-encoded; the
+    // triangles of meshes without normals keep their face normal.
+    s->tri_normals.clear();
+    if (!s->tri_smooth.empty()) {
+        s->tri_normals.assign(ntri, make_uint4(0, 0, 0, 0));
+        for (size_t slot = 0; slot < ntri; ++slot) {
+            const uint32_t t = s->bvh.prims[slot];
+            if (!s->tri_smooth[t]) continue;
+            unsigned q[3];
+            for (int j = 0; j < 3; ++j) {
+                const float* n = &s->tri_nrm9[9 * (size_t)t + 3 * j];
+                const float l = std::sqrt(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]);
+                q[j] = OctEncode(n[0] / l, n[1] / l, n[2] / l);
+            }
+            s->tri_normals[slot] = make_uint4(q[0], q[1], q[2], 0);
+            attr[slot].mat |= kAttrSmooth;
+        }
+    }
     size_t total = 0;
     int rc = Upload(ctx, &s->d_attr, attr, total);
     if (!rc) rc = Upload(ctx, &s->d_mats, s->materials, total);
@@ -312,6 +330,7 @@ int UploadShading(rtb200_scene* s)
     if (!rc) rc = Upload(ctx, &s->d_light_tris, s->light_tris, total);
     if (!rc && !s->light_nodes.empty()) rc = Upload(ctx, &s->d_light_nodes, s->light_nodes, total);
     if (!rc && !s->light_alias.empty()) rc = Upload(ctx, &s->d_light_alias, s->light_alias, total);
+    if (!rc && !s->tri_normals.empty()) rc = Upload(ctx, &s->d_tri_normals, s->tri_normals, total);
     s->shade_bytes = total;
     if (rc) FreeShading(s);
     return rc;
@@ -327,6 +346,8 @@ void FreeShading(rtb200_scene* s)
     DevFree(ctx, s->d_light_tris, s->light_tris.size() * sizeof(PtLightTri));
     DevFree(ctx, s->d_light_nodes, s->light_nodes.size() * sizeof(PtLightNode));
     DevFree(ctx, s->d_light_alias, s->light_alias.size() * sizeof(PtLightAlias));
+    DevFree(ctx, s->d_tri_normals, s->tri_normals.size() * sizeof(uint4));
+    s->d_tri_normals = nullptr;
     s->d_light_nodes = nullptr;
     s->d_light_alias = nullptr;
     s->d_attr = nullptr;

@@ -208,6 +208,20 @@ __device__ __forceinline__ V3 cross(V3 a, V3 b) { return {a.y * b.z - a.z * b.y,
 __device__ __forceinline__ V3 normalize(V3 a) { return a * rsqrtf(fmaxf(dot(a, a), 1e-30f)); }
 __device__ __forceinline__ V3 xyz(float4 v) { return {v.x, v.y, v.z}; }
 
+// Unit vector from its octahedral encoding (OctEncode in pt_types.h).
+__device__ __forceinline__ V3 OctDecode(unsigned q)
+{
+    const float u = (float)(short)(q & 0xffffu) * (1.0f / 32767.0f);
+    const float v = (float)(short)(q >> 16) * (1.0f / 32767.0f);
+    float x = u, y = v;
+    const float z = 1.0f - fabsf(u) - fabsf(v);
+    if (z < 0.0f) {
+        x = (1.0f - fabsf(v)) * (u >= 0.0f ? 1.0f : -1.0f);
+        y = (1.0f - fabsf(u)) * (v >= 0.0f ? 1.0f : -1.0f);
+    }
+    return normalize(mk(x, y, z));
+}
+
 // Orthonormal basis around unit n (Duff et al., JCGT 6(1), 2017).
 __device__ __forceinline__ void Basis(V3 n, V3& t, V3& b)
 {

@@ -1,6 +1,7 @@
 // pt_types.h -- device-side scene, job and queue descriptors of the spectral
 // path tracer (pathtrace.cu), shared with the host code that fills them.
 #pragma once
+#include <cmath>
 #include <cstdint>
 #include <cuda_runtime.h>
 
@@ -131,6 +132,7 @@ struct PtTriAttr {
 };
 
 constexpr int kAttrDoubleSided = 1 << 30;
+constexpr int kAttrSmooth = 1 << 29;   // interpolated vertex normals (PtScene::tri_normals)
 constexpr int kAttrMatMask = (1 << 24) - 1;
 
 // Path flags (meta.z).
@@ -175,7 +177,32 @@ struct PtScene {
     const PtLightTri* light_tris;
     const PtLightNode* light_nodes;   // light BVH (null with fewer than two luminaries)
     const PtLightAlias* light_alias;  // alias table over the luminaries (power selection)
+    // Vertex normals of triangles marked kAttrSmooth, in leaf order: x, y, z
+    // hold the three vertices' unit normals octahedron-encoded (two signed
+    // 16-bit components each, OctDecode in pt_device.cuh); null when no mesh
+    // of the scene has normals.
+    const uint4* tri_normals;
 };
+
+// Octahedral encoding of a unit vector (Cigolle et al., "A Survey of
+// Efficient Representations for Independent Unit Vectors", JCGT 3(2), 2014):
+// project onto the octahedron |x| + |y| + |z| = 1, fold the lower half over
+// the upper, keep (x, y) as signed 16-bit fractions.  FP32 throughout so
+// host and restatement encode bit for bit.
+RTB_HD unsigned OctEncode(float x, float y, float z)
+{
+    const float s = fabsf(x) + fabsf(y) + fabsf(z);
+    float u = s > 0.0f ? x / s : 0.0f, v = s > 0.0f ? y / s : 0.0f;
+    if (z < 0.0f) {
+        const float fu = (1.0f - fabsf(v)) * (u >= 0.0f ? 1.0f : -1.0f);
+        const float fv = (1.0f - fabsf(u)) * (v >= 0.0f ? 1.0f : -1.0f);
+        u = fu;
+        v = fv;
+    }
+    const int qu = (int)rintf(fminf(fmaxf(u, -1.0f), 1.0f) * 32767.0f);
+    const int qv = (int)rintf(fminf(fmaxf(v, -1.0f), 1.0f) * 32767.0f);
+    return ((unsigned)qu & 0xffffu) | ((unsigned)qv << 16);
+}
 
 struct PtPaths {
     float4* ray_o;   // origin, tmin

@@ -34,6 +34,8 @@ struct rtb200_risemesh {
     bool double_sided = false;
     std::vector<double> points;        // 3 per point
     std::vector<uint32_t> tri;         // point indices, 3 per triangle
+    std::vector<double> normals;       // 3 per normal (none when the mesh uses face normals)
+    std::vector<uint32_t> tri_nrm;     // normal indices, 3 per triangle
     bool has_bvh = false;
     std::vector<Node2> nodes2;
     std::vector<uint32_t> prims;
@@ -85,13 +87,16 @@ bool Parse(const uint8_t* bytes, size_t len, rtb200_risemesh& m)
     m.points.resize(3 * (size_t)n);
     if (!r.Bytes(m.points.data(), 24 * (size_t)n)) return false;
     const uint32_t n_points = n;
-    if (!r.U32(n) || !r.Fits(n, 24) || !r.Skip(24 * (size_t)n)) return false;     // normals
+    if (!r.U32(n) || !r.Fits(n, 24)) return false;     // normals
+    m.normals.resize(3 * (size_t)n);
+    if (!r.Bytes(m.normals.data(), 24 * (size_t)n)) return false;
     const uint32_t n_normals = n;
     if (!r.U32(n) || !r.Fits(n, 16) || !r.Skip(16 * (size_t)n)) return false;     // texture coordinates
     const uint32_t n_coords = n;
     if (ver >= 5 && !(r.U32(n) && r.Fits(n, 24) && r.Skip(24 * (size_t)n))) return false;   // colours
     if (!r.U32(n) || !r.Fits(n, 36)) return false;
     m.tri.resize(3 * (size_t)n);
+    m.tri_nrm.resize(3 * (size_t)n);
     for (uint32_t t = 0; t < n; ++t)
         for (int i = 0; i < 3; ++i) {
             uint32_t v[3];
@@ -103,6 +108,7 @@ bool Parse(const uint8_t* bytes, size_t len, rtb200_risemesh& m)
             if (n_normals > 0 && !m.face_normals && v[1] >= n_normals) return false;
             if (n_coords > 0 && v[2] >= n_coords) return false;
             m.tri[3 * (size_t)t + i] = v[0];
+            m.tri_nrm[3 * (size_t)t + i] = v[1];
         }
     const uint32_t n_tri = n;
     if (!r.Char(c)) return false;
@@ -181,6 +187,14 @@ int rtb200_risemesh_triangles(const rtb200_risemesh* m, float* tri9)
     return RTB200_OK;
 }
 
+int rtb200_risemesh_normals(const rtb200_risemesh* m, float* nrm9)
+{
+    if (!m || m->face_normals || m->normals.empty() || (!nrm9 && !m->tri.empty())) return RTB200_E_INVALID;
+    for (size_t i = 0; i < m->tri_nrm.size(); ++i)
+        for (int k = 0; k < 3; ++k) nrm9[3 * i + k] = (float)m->normals[3 * (size_t)m->tri_nrm[i] + k];
+    return RTB200_OK;
+}
+
 int rtb200_risemesh_destroy(rtb200_risemesh* m)
 {
     delete m;
@@ -207,5 +221,16 @@ const std::vector<Node2>* RisemeshBvh(const rtb200_risemesh* m, const std::vecto
 }
 
 bool RisemeshDoubleSided(const rtb200_risemesh* m) { return m->double_sided; }
+
+// Vertex normals for shading: the file's normal list and per-corner indices,
+// unless the mesh shades with face normals or stores no normals.
+bool RisemeshNormals(const rtb200_risemesh* m, std::vector<float>& nrm, std::vector<uint32_t>& tri_nrm)
+{
+    if (m->face_normals || m->normals.empty()) return false;
+    nrm.resize(m->normals.size());
+    for (size_t i = 0; i < m->normals.size(); ++i) nrm[i] = (float)m->normals[i];
+    tri_nrm = m->tri_nrm;
+    return true;
+}
 
 }  // namespace rtb200

@@ -64,8 +64,11 @@ def upload_scene(ctx, desc, layout="f32"):
         out = ctypes.c_int32()
         check(L.rtb200_scene_add_material(s.h, ctypes.byref(cm), ctypes.byref(out)), ctx.h)
     check(L.rtb200_scene_set_environment(s.h, desc.env, desc.env_visible), ctx.h)
-    for first, count, mat, ds in desc.meshes:
-        s.add_triangles(desc.tri9[first:first + count], material=mat, double_sided=ds)
+    nrm9 = desc.nrm9 if hasattr(desc, "nrm9") else None
+    for k, (first, count, mat, ds) in enumerate(desc.meshes):
+        smooth = nrm9 is not None and desc._nrms[k] is not None
+        s.add_triangles(desc.tri9[first:first + count], material=mat, double_sided=ds,
+                        normals9=nrm9[first:first + count] if smooth else None)
     for pos, color, power in getattr(desc, "point_lights", []):
         p3 = (ctypes.c_float * 3)(*pos)
         c3 = (ctypes.c_float * 3)(*color)

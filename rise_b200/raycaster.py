@@ -73,11 +73,21 @@ class Scene:
                                           int(material), int(bool(double_sided))), self.ctx.h)
         self.n_tri += len(tri)
 
-    def add_triangles(self, tri9, material=0, double_sided=True):
-        """Add a triangle soup given as (n, 9) floats: v0, v1, v2 per row."""
+    def add_triangles(self, tri9, material=0, double_sided=True, normals9=None):
+        """Add a triangle soup given as (n, 9) floats: v0, v1, v2 per row;
+        normals9, the same shape, gives vertex normals per corner for smooth
+        shading."""
         tri9 = np.ascontiguousarray(tri9, np.float32).reshape(-1, 9)
         idx = np.arange(3 * len(tri9), dtype=np.uint32).reshape(-1, 3)
-        self.add_mesh(tri9.reshape(-1, 3), idx, material, double_sided)
+        if normals9 is None:
+            self.add_mesh(tri9.reshape(-1, 3), idx, material, double_sided)
+            return
+        nrm = np.ascontiguousarray(normals9, np.float32).reshape(-1, 3)
+        xyz = tri9.reshape(-1, 3)
+        check(lib().rtb200_scene_add_mesh_normals(self.h, _ptr(xyz), len(xyz), _ptr(idx), len(idx), _ptr(nrm),
+                                                  len(nrm), _ptr(idx), int(material), int(bool(double_sided))),
+              self.ctx.h)
+        self.n_tri += len(idx)
 
     def add_risemesh(self, mesh, material=0, use_cached_bvh=True):
         """Add a parsed RiseMesh; its BVH2 cache (if any) replaces the SAH
@@ -163,6 +173,14 @@ class RiseMesh:
         """(n, 9) float32 triangles (v0, v1, v2)."""
         out = np.zeros((self.info()["n_tri"], 9), np.float32)
         check(lib().rtb200_risemesh_triangles(self.h, _ptr(out)))
+        return out
+
+    def normals(self):
+        """(n, 9) float32 vertex normals per triangle corner, or None when the
+        mesh shades with face normals."""
+        out = np.zeros((self.info()["n_tri"], 9), np.float32)
+        if lib().rtb200_risemesh_normals(self.h, _ptr(out)) != 0:
+            return None
         return out
 
     def host_bvh(self, use_cached_bvh=True):

@@ -311,22 +311,26 @@ class _Loader:
             self.notes.append(f"ggx_material {c.get('name')}: rs none read as a unit specular layer")
 
     def dielectric_material(self, c):
+        # Job::AddDielectricMaterial: tau (interior transmittance per unit
+        # length), ior, scattering (the Phong exponent of the transmitted
+        # lobe, default 10000; 1e6 and above is a smooth interface).
         self.only(c, {"name", "tau", "ior", "scattering"})
-        if c.get("tau", "none") != "none":
-            self.refuse(c, "an absorbing interior (tau) is not supported")
+        tau = c.get("tau", "none")
+        if tau != "none" and any(x != 1.0 for x in _floats(tau, len(tau.split()), "tau")):
+            self.refuse(c, "an absorbing interior (tau other than 1) is not supported")
         ior = _number(c.get("ior", "1.33"))
-        if ior is None:
-            self.refuse(c, "ior must be a number")
-        self.add_material(c, scenes.Material(scenes.MAT_DIELECTRIC, -1, -1, -1, -1, 0.0, float(ior)), "dielectric")
-        if c.has("scattering"):
-            self.notes.append(f"dielectric_material {c.get('name')}: scattering ignored (smooth interface)")
+        scat = _number(c.get("scattering", "10000"))
+        if ior is None or scat is None:
+            self.refuse(c, "ior and scattering must be numbers")
+        self.add_material(c, scenes.Material(scenes.MAT_DIELECTRIC, -1, -1, -1, -1, float(min(scat, 1e6)), float(ior)),
+                          "dielectric")
 
     # ---- geometry ----------------------------------------------------------
     def clippedplane_geometry(self, c):
         self.only(c, {"name", "pta", "ptb", "ptc", "ptd", "doublesided"})
         p = [np.array(_floats(c.get(k, "0 0 0"), 3, k)) for k in ("pta", "ptb", "ptc", "ptd")]
         tris = np.array([np.concatenate([p[0], p[1], p[2]]), np.concatenate([p[0], p[2], p[3]])])
-        self.geometry[c.get("name", "noname")] = (tris, _bool(c.get("doublesided", "true")))
+        self.geometry[c.get("name", "noname")] = (tris, _bool(c.get("doublesided", "true")), None)
 
     def rawmesh_geometry(self, c):
         self.only(c, {"name", "file", "double_sided", "maxpolygons", "maxdepth"})
@@ -345,21 +349,45 @@ class _Loader:
                     tris.append(a + b + cc)
                     tris.append(a + cc + d)
         self.geometry[c.get("name", "noname")] = (np.array(tris, np.float64).reshape(-1, 9),
-                                                  _bool(c.get("double_sided", "false")))
+                                                  _bool(c.get("double_sided", "false")), None)
 
     def risemesh_geometry(self, c):
         from .raycaster import RiseMesh
         self.only(c, {"name", "file", "loadintomemory", "face_normals"})
         m = RiseMesh.from_file(self.path(c.get("file", "none"), "risemesh_geometry"))
         try:
-            self.geometry[c.get("name", "noname")] = (m.triangles().astype(np.float64), m.info()["double_sided"])
+            # The file's own face-normals flag decides between its vertex
+            # normals and face normals (TriangleMeshGeometryIndexed.cpp:444-490).
+            nrm = m.normals()
+            self.geometry[c.get("name", "noname")] = (m.triangles().astype(np.float64), m.info()["double_sided"],
+                                                      None if nrm is None else nrm.astype(np.float64))
         finally:
             m.close()
+
+    def rawmesh2_geometry(self, c):
+        # TriangleMeshLoaderRAW2 (Geometry/TriangleMeshLoaderRAW2.cpp): a
+        # "vertices triangles" header, "v x y z nx ny nz u v [r g b]" lines,
+        # then "t a b c" lines indexing vertices, normals and coordinates alike;
+        # face_normals shades with face normals instead.
+        self.only(c, {"name", "file", "double_sided", "face_normals", "maxpolygons", "maxdepth"})
+        with open(self.path(c.get("file", "none"), "rawmesh2_geometry"), "r") as f:
+            lines = [ln.split() for ln in f if ln.strip()]
+        try:
+            nv, nt = int(lines[0][0]), int(lines[0][1])
+            verts = np.array([[float(x) for x in ln[1:7]] for ln in lines[1:1 + nv]], np.float64).reshape(-1, 6)
+            idx = np.array([[int(x) for x in ln[1:4]] for ln in lines[1 + nv:1 + nv + nt]], np.int64).reshape(-1, 3)
+        except (IndexError, ValueError):
+            self.refuse(c, "malformed RAW2 file")
+        if len(verts) != nv or len(idx) != nt or (nt and (idx.min() < 0 or idx.max() >= nv)):
+            self.refuse(c, "malformed RAW2 file")
+        tris = verts[idx, 0:3].reshape(-1, 9)
+        nrm = None if _bool(c.get("face_normals", "false")) else verts[idx, 3:6].reshape(-1, 9)
+        self.geometry[c.get("name", "noname")] = (tris, _bool(c.get("double_sided", "false")), nrm)
 
     def box_geometry(self, c):
         self.only(c, {"name", "width", "height", "depth"})
         self.geometry[c.get("name", "noname")] = (
-            _box(float(c.get("width", 1.0)), float(c.get("height", 1.0)), float(c.get("depth", 1.0))), False)
+            _box(float(c.get("width", 1.0)), float(c.get("height", 1.0)), float(c.get("depth", 1.0))), False, None)
 
     # ---- objects -----------------------------------------------------------
     def standard_object(self, c):
@@ -373,14 +401,17 @@ class _Loader:
             self.refuse(c, f"unknown or missing material {mname!r}")
         if not _bool(c.get("casts_shadows", "true")) or not _bool(c.get("receives_shadows", "true")):
             self.refuse(c, "objects that cast or receive no shadows are not supported")
-        tris, ds = self.geometry[g]
+        tris, ds, nrm = self.geometry[g]
         pos = np.array(_floats(c.get("position", "0 0 0"), 3, "position"))
         ori = np.radians(_floats(c.get("orientation", "0 0 0"), 3, "orientation"))
         sc = np.array(_floats(c.get("scale", "1 1 1"), 3, "scale"))
         r = _rot(*ori)
         v = tris.reshape(-1, 3) * sc
         world = (v @ r.T + pos).reshape(-1, 9)
-        self.desc.add_mesh(world.astype(np.float32), self.materials[mname][0], bool(ds))
+        # Normals go through the inverse transpose of rotation x scale
+        # (Object.cpp:543): R S^-1 n; the device normalises after interpolating.
+        wn = None if nrm is None else ((nrm.reshape(-1, 3) / sc) @ r.T).reshape(-1, 9).astype(np.float32)
+        self.desc.add_mesh(world.astype(np.float32), self.materials[mname][0], bool(ds), normals9=wn)
 
     # ---- camera, film, rasterizer -----------------------------------------
     def film(self, c):

@@ -285,6 +285,7 @@ class SceneDesc:
     point_lights: list = field(default_factory=list)  # (position, colour, power)
     settings: RenderSettings = field(default_factory=RenderSettings)
     _tris: list = field(default_factory=list)
+    _nrms: list = field(default_factory=list)
 
     def add_spectrum(self, s):
         self.spectra.append(s if isinstance(s, (SpectralPacket, SigmoidSpectrum, BlackbodySpectrum))
@@ -299,12 +300,24 @@ class SceneDesc:
         self.materials.append(m)
         return len(self.materials) - 1
 
-    def add_mesh(self, tri9, material, double_sided=True):
+    def add_mesh(self, tri9, material, double_sided=True, normals9=None):
+        """normals9: vertex normals per triangle corner, (n, 9), for smooth
+        shading (None: face normals)."""
         tri9 = np.asarray(tri9, np.float32).reshape(-1, 9)
         first = sum(len(t) for t in self._tris)
         self._tris.append(tri9)
+        self._nrms.append(None if normals9 is None else np.asarray(normals9, np.float32).reshape(-1, 9))
         self.meshes.append((first, len(tri9), material, int(bool(double_sided))))
         self.tri9 = np.concatenate(self._tris).astype(np.float32)
+
+    @property
+    def nrm9(self):
+        """Vertex normals of every triangle corner, zeros for flat meshes; None
+        when no mesh has normals."""
+        if not any(n is not None for n in self._nrms):
+            return None
+        return np.concatenate([n if n is not None else np.zeros((len(t), 9), np.float32)
+                               for n, t in zip(self._nrms, self._tris)]).astype(np.float32)
 
     @property
     def n_tri(self):
@@ -395,6 +408,13 @@ def uv_sphere(center, radius, n_tri):
         if i < nv - 2:
             tris.append(np.concatenate([b, d, c], axis=1))
     return np.concatenate(tris).astype(np.float32)
+
+
+def sphere_normals(tri9, center):
+    """Vertex normals of a sphere's triangle corners: the unit direction from
+    the centre to each vertex, (n, 9) float32."""
+    v = np.asarray(tri9, np.float64).reshape(-1, 3) - np.asarray(center, np.float64)
+    return (v / np.linalg.norm(v, axis=1, keepdims=True)).reshape(-1, 9).astype(np.float32)
 
 
 def gold_like_spectra():

@@ -18,8 +18,12 @@ oracle/rise_ref.mk), on tests/golden/cornell_c1.RISEscene:
   its Sobol sampler: the reference integrator's estimate without the small
   bias its padded Sobol sequence carries (images about 0.1-0.3 % brighter
   than with independent numbers), for a tight test of the image mean.
+* cornell_smooth_ref_k16_independent.npz -- 16 x 16 spp with independent
+  numbers of tests/golden/cornell_smooth.RISEscene, the box with a smooth-
+  shaded Lambertian sphere and a smooth-shaded glass sphere (vertex normals
+  from RAW2 files): the z-test of interpolated shading normals.
 
-    make -C oracle && python tests/golden/make_cornell_reference.py [k16|k16i|fp64]
+    make -C oracle && python tests/golden/make_cornell_reference.py [k16|k16i|smooth|fp64]
     (k16, k16i: ~40 s each, fp64: ~45 min on 8 cores; rows are checkpointed under
     oracle/_ref/ so an interrupted run resumes)
 """
@@ -41,10 +45,10 @@ FP64_SPP = 16384
 ROWS = 8
 
 
-def make_k16(r, independent=False):
+def make_k16(r, independent=False, name=None):
     t0 = time.time()
     b = np.array([r.integrate(K_SPP, batch=k, independent=independent) for k in range(1, K + 1)])
-    name = "cornell_c1_ref_k16_independent.npz" if independent else "cornell_c1_ref_k16.npz"
+    name = name or ("cornell_c1_ref_k16_independent.npz" if independent else "cornell_c1_ref_k16.npz")
     np.savez_compressed(os.path.join(HERE, name), mean=b.mean(0).astype(np.float32),
                         var=b.var(0, ddof=1).astype(np.float32), k=K, spp=K_SPP)
     print(f"{name}: {time.time() - t0:.0f} s", flush=True)
@@ -64,7 +68,7 @@ def make_fp64(r):
 
 
 def main():
-    which = sys.argv[1:] or ["k16", "k16i", "fp64"]
+    which = sys.argv[1:] or ["k16", "k16i", "smooth", "fp64"]
     r = oracle.RefRenderer(SCENE)
     if "k16" in which:
         make_k16(r)
@@ -72,6 +76,9 @@ def main():
         make_k16(r, independent=True)
     if "fp64" in which:
         make_fp64(r)
+    if "smooth" in which:
+        make_k16(oracle.RefRenderer(os.path.join(HERE, "cornell_smooth.RISEscene")), independent=True,
+                 name="cornell_smooth_ref_k16_independent.npz")
 
 
 if __name__ == "__main__":

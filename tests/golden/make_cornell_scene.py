@@ -19,7 +19,8 @@ wavelengths on 400..700 nm, box pixel filter of width 1, Russian roulette
 from depth 3, at most 7 diffuse bounces (8 path vertices, the config's max
 depth 8), 256 x 256, 16 samples per pixel.
 
-    python tests/golden/make_cornell_scene.py
+    python tests/golden/make_cornell_scene.py           (the C1 scene)
+    python tests/golden/make_cornell_scene.py smooth    (the smooth-shaded variant)
 """
 import math
 import os
@@ -101,5 +102,58 @@ def main():
             f.write(raw_text(tri9))
 
 
-if __name__ == "__main__":
+if __name__ == "__main__" and not sys.argv[1:]:
     main()
+
+
+# ---- a smooth-shaded variant --------------------------------------------------
+# The C1 box without its two boxes, holding two UV spheres of 960 triangles
+# with vertex normals (RAW2 files, which carry a normal per vertex): a
+# Lambertian white one and a smooth dielectric (IOR 1.5) one.  Written by
+# `python tests/golden/make_cornell_scene.py smooth`.
+SMOOTH = "cornell_smooth"
+SPHERES = [("sphere_matte", (0.3, 0.18, 0.55), 0.18, "white"), ("sphere_glass", (0.7, 0.2, 0.35), 0.2, "glass")]
+
+
+def raw2_text(center, radius, n_tri):
+    tri9 = scenes.uv_sphere(center, radius, n_tri).astype(np.float64)
+    nrm9 = scenes.sphere_normals(tri9, center).astype(np.float64)
+    v = tri9.reshape(-1, 3)
+    n = nrm9.reshape(-1, 3)
+    lines = [f"{len(v)} {len(tri9)}"]
+    lines += [f"v {a[0]:.9g} {a[1]:.9g} {a[2]:.9g} {b[0]:.9g} {b[1]:.9g} {b[2]:.9g} 0 0" for a, b in zip(v, n)]
+    lines += [f"t {3 * i} {3 * i + 1} {3 * i + 2}" for i in range(len(tri9))]
+    return "\n".join(lines) + "\n"
+
+
+def smooth_scene_text():
+    text, _ = scene_text()
+    text = text.replace("# The C1 spectral Cornell box (written by tests/golden/make_cornell_scene.py).",
+                        "# The C1 box with two smooth-shaded spheres (written by tests/golden/make_cornell_scene.py).")
+    text = text.replace(f"\tfile\t\t{NAME}_", "\tfile\t\tcornell_c1_")
+    # No boxes; the spheres instead.
+    cut = text.index("rawmesh_geometry\n{\n\tname\t\tg_boxes")
+    end = text.index("rawmesh_geometry\n{\n\tname\t\tg_light")
+    text = text[:cut] + text[end:]
+    text = text.replace("max_diffuse_bounce\t7", "max_diffuse_bounce\t7\n\tmax_glossy_bounce\t8\n"
+                        "\tmax_transmission_bounce\t8")
+    extra = ["dielectric_material", "{", "\tname\t\tglass", "\ttau\t\t\t1.0", "\tior\t\t\t1.5",
+             "\tscattering\t1000000", "}", ""]
+    for name, c, r, mat in SPHERES:
+        extra += ["rawmesh2_geometry", "{", f"\tname\t\tg_{name}", f"\tfile\t\t{SMOOTH}_{name}.raw2",
+                  "\tdouble_sided\tfalse", "}", ""]
+        extra += ["standard_object", "{", f"\tname\t\to_{name}", f"\tgeometry\tg_{name}", f"\tmaterial\t{mat}",
+                  "}", ""]
+    return text + "\n".join(extra)
+
+
+def main_smooth():
+    with open(os.path.join(HERE, SMOOTH + ".RISEscene"), "w") as f:
+        f.write(smooth_scene_text())
+    for name, c, r, _ in SPHERES:
+        with open(os.path.join(HERE, f"{SMOOTH}_{name}.raw2"), "w") as f:
+            f.write(raw2_text(c, r, 960))
+
+
+if __name__ == "__main__" and sys.argv[1:] == ["smooth"]:
+    main_smooth()

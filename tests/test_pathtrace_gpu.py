@@ -367,6 +367,7 @@ def many_emitters_box():
     first, count, mat, ds = d.meshes[-1]
     d.meshes.pop()
     d._tris.pop()
+    d._nrms.pop()
     y = 0.999
     d.add_mesh(tessellated_quad([0.375, y, 0.375], [0.25, 0, 0], [0, 0, 0.25], 40), mat, double_sided=False)
     for k, v in enumerate((2.0, 5.0, 9.0, 0.5)):

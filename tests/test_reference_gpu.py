@@ -99,3 +99,29 @@ def test_same_random_numbers_as_the_oracle(ctx, c1, sampler):
     assert close.mean() > 0.97, close.mean()
     assert rel_mse(g, o) < 1e-4
     assert abs(g[..., 1].mean() / o[..., 1].mean() - 1) < 2e-3
+
+
+def test_smooth_shading_normals_z_test_against_the_reference(ctx):
+    """Vertex normals interpolated on the device (octahedral encoding), a
+    smooth Lambertian and a smooth glass sphere: z-test against the
+    reference given independent numbers."""
+    f = np.load(os.path.join(GOLDEN, "cornell_smooth_ref_k16_independent.npz"))
+    mr, vr, k, spp = f["mean"].astype(np.float64), f["var"].astype(np.float64), int(f["k"]), int(f["spp"])
+    ls = scenefile.load_scene(os.path.join(GOLDEN, "cornell_smooth.RISEscene"))
+    g = np.array([render(ctx, ls.desc, spp, seed=2001 + b, sampler=0) for b in range(k)])
+    z, _ = z_scores(g.mean(0), g.var(0, ddof=1), k, mr, vr, k)
+    assert (np.abs(z) > Z_LIMIT).mean() <= Z_ALLOWED_RATE, (np.abs(z) > Z_LIMIT).mean()
+    se = np.sqrt(g[..., 1].mean(axis=(1, 2)).var(ddof=1) / k + vr[..., 1].mean() / k / mr[..., 1].size)
+    assert abs(g[..., 1].mean() - mr[..., 1].mean()) < 4 * se
+
+
+@pytest.mark.parametrize("sampler", [0, 1])
+def test_smooth_shading_same_random_numbers_as_the_oracle(ctx, sampler):
+    ls = scenefile.load_scene(os.path.join(GOLDEN, "cornell_smooth.RISEscene"))
+    st = dataclasses.replace(ls.desc.settings, seed=5, sampler=sampler)
+    g = render(ctx, ls.desc, 16, seed=5, sampler=sampler)[128:192]
+    o = oracle.pt_render(ls.desc, 16, crop=(0, 128, st.width, 192), settings=st)
+    close = (np.abs(g - o) <= 1e-3 * (np.abs(o) + 1e-3)).all(axis=2)
+    assert close.mean() > 0.95, close.mean()
+    assert rel_mse(g, o) < 1e-3
+    assert abs(g[..., 1].mean() / o[..., 1].mean() - 1) < 2e-3

@@ -90,3 +90,28 @@ def test_harness_pixel_loop_matches_the_reference_pipeline():
     assert abs(full.mean() / ref_rgb.mean() - 1) < 0.01
     e_full, e_one = rel_mse(full, ref_rgb), rel_mse(to_rgb(one), ref_rgb)
     assert 0.6 < e_full / e_one < 1.6, (e_full, e_one)
+
+
+def test_smooth_shading_normals_match_the_reference():
+    """Interpolated vertex normals (a smooth Lambertian sphere and a smooth
+    glass sphere read from RAW2 files): the restatement's 16 batches against
+    the reference's 16 (independent numbers) on the rows through both
+    spheres; the same scene shaded with face normals fails the same test."""
+    f = np.load(os.path.join(GOLDEN, "cornell_smooth_ref_k16_independent.npz"))
+    mr, vr, k, spp = f["mean"].astype(np.float64), f["var"].astype(np.float64), int(f["k"]), int(f["spp"])
+    ls = scenefile.load_scene(os.path.join(GOLDEN, "cornell_smooth.RISEscene"))
+    st = ls.desc.settings
+    assert sum(n is not None for n in ls.desc._nrms) == 2
+    y0, y1 = 128, 192
+    crop = (0, y0, st.width, y1)
+
+    def rate(desc):
+        g = np.array([oracle.pt_render(desc, spp, crop=crop, settings=dataclasses.replace(st, seed=700 + b, sampler=0))
+                      for b in range(k)])
+        z, _ = z_scores(g.mean(0), g.var(0, ddof=1), k, mr[y0:y1], vr[y0:y1], k)
+        return float((np.abs(z) > Z_LIMIT).mean())
+
+    assert rate(ls.desc) <= Z_ALLOWED_RATE
+    flat = dataclasses.replace(ls.desc)
+    flat._nrms = [None] * len(ls.desc._nrms)
+    assert rate(flat) > 2 * Z_ALLOWED_RATE
