@@ -49,6 +49,7 @@ extern "C" {
 /* BVH device layouts for rtb200_scene_commit. */
 #define RTB200_BVH_F32     0  /* FP32 child boxes, 128-byte 4-wide nodes */
 #define RTB200_BVH_Q8      1  /* 8-bit conservative child boxes, 64-byte nodes */
+#define RTB200_BVH_W8      2  /* 8-wide nodes with 8-bit conservative child boxes, 80 bytes */
 
 typedef struct rtb200_ctx rtb200_ctx;
 typedef struct rtb200_scene rtb200_scene;
@@ -275,9 +276,16 @@ typedef struct {
  * index = the pixel's sample number; bounce `depth` draws dimensions
  * (16 + depth) * 32 + j in the order the reference's integrator consumes them
  * (StartStream(16 + depth), PathTracingIntegrator.cpp:4112), camera jitter and
- * the hero wavelength dimensions 0, 1, 2. */
+ * the hero wavelength dimensions 0, 1, 2.  With one seed per pixel, and
+ * dimension pairs that replay one Sobol pair under another scramble, a pixel
+ * rendered this way does not converge to its integral (the reference's
+ * images carry the same per-pixel error).  SOBOL_SHUFFLED: the same with the
+ * sample index first Owen-scrambled by a seed per dimension pair (Burley's
+ * decorrelation of padded dimensions, JCGT 9(4), 2020), which keeps the
+ * stratification and converges. */
 #define RTB200_SAMPLER_HASH 0
 #define RTB200_SAMPLER_SOBOL 1
+#define RTB200_SAMPLER_SOBOL_SHUFFLED 2
 
 /* Next-event luminary selection.  BVH: the reference's light BVH
  * (Lights/LightBVH.cpp: importance = power / squared distance to the node's

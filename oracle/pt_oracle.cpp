@@ -96,9 +96,21 @@ inline uint32_t SobolBits(uint32_t index, uint32_t dim, uint32_t seed)
     v ^= v * 0x53a22864u;
     return ReverseBits(v);
 }
-// As the device draws it: the top 24 bits.
-inline double SobolSample(uint32_t index, uint32_t dim, uint32_t seed)
+inline uint32_t OwenScrambleBits(uint32_t v, uint32_t s)
 {
+    v = ReverseBits(v);
+    v ^= v * 0x3d20adeau;
+    v += s;
+    v *= (s >> 16) | 1u;
+    v ^= v * 0x05526c56u;
+    v ^= v * 0x53a22864u;
+    return ReverseBits(v);
+}
+// As the device draws it: the top 24 bits; shuffle: the index first
+// Owen-scrambled with a seed per dimension pair (Burley, JCGT 9(4), 2020).
+inline double SobolSample(uint32_t index, uint32_t dim, uint32_t seed, bool shuffle = false)
+{
+    if (shuffle) index = OwenScrambleBits(index, HashCombine(HashCombine(seed, 0x5bd1e995u), dim >> 1));
     return (double)(SobolBits(index, dim, seed) >> 8) * (1.0 / 16777216.0);
 }
 inline uint32_t SobolPixelSeed(uint32_t x, uint32_t y, uint32_t seed)
@@ -113,11 +125,11 @@ inline uint32_t SobolPixelSeed(uint32_t x, uint32_t y, uint32_t seed)
 struct VertexRng {
     uint32_t key, index;
     int depth;
-    bool sobol;
+    int mode;          // 0 hash, 1 Sobol, 2 Sobol with shuffled indices
     uint32_t cur;
     double next(int j)
     {
-        if (sobol) return SobolSample(index, (16u + (uint32_t)depth) * 32u + cur++, key);
+        if (mode) return SobolSample(index, (16u + (uint32_t)depth) * 32u + cur++, key, mode == 2);
         return Rand(key, Dim(depth, j));
     }
     void skip(int n) { cur += (uint32_t)n; }
@@ -539,7 +551,7 @@ struct Scene {
     int env, envVisible;
     double lmin, lmax, rrThreshold, ynorm;
     int width, height, maxDepth, rrMinDepth, neePerLambda;
-    int sampler = 0;                       // 0 hash, 1 Sobol
+    int sampler = 0;                       // 0 hash, 1 Sobol, 2 Sobol with shuffled indices
     int maxBounce[3] = {255, 255, 255};    // diffuse, glossy, transmission
     uint32_t seed;
     bool lightBvh = false;                 // luminaries picked with the light BVH
@@ -742,13 +754,13 @@ void Barycentrics(V o, V d, V a, V b, V c, double& al, double& be)
 // 0-2: jitter x, y, hero wavelength).
 inline uint32_t SampleKey(const Scene& S, uint32_t pixel, uint32_t sample)
 {
-    if (S.sampler == 1)
+    if (S.sampler != 0)
         return SobolPixelSeed(pixel % (uint32_t)S.width, pixel / (uint32_t)S.width, S.seed);
     return PathKey(S.seed, pixel, sample);
 }
 inline double CameraRand(const Scene& S, uint32_t key, uint32_t sample, uint32_t dim)
 {
-    return S.sampler == 1 ? SobolSample(sample, dim, key) : Rand(key, dim);
+    return S.sampler != 0 ? SobolSample(sample, dim, key, S.sampler == 2) : Rand(key, dim);
 }
 
 void Sample(const Scene& S, uint32_t pixel, uint32_t sample, double xyz[3])
@@ -780,7 +792,7 @@ void Sample(const Scene& S, uint32_t pixel, uint32_t sample, double xyz[3])
     double bsdfPdf = 0.0;
     int bounces[3] = {0, 0, 0};
     for (int depth = 0; depth < S.maxDepth; ++depth) {
-        VertexRng rng{key, sample, depth, S.sampler == 1, 0u};
+        VertexRng rng{key, sample, depth, S.sampler, 0u};
         double mx = 0.0;
         bool bad = false;
         for (double v : thr) { if (!std::isfinite(v)) bad = true; mx = std::max(mx, std::fabs(v)); }

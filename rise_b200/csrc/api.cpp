@@ -388,7 +388,8 @@ int rtb200_scene_commit(rtb200_scene* s, int32_t layout)
     rtb200_ctx* ctx = s->ctx;
     std::lock_guard<std::mutex> g(ctx->mu);
     if (s->committed) return SetError(ctx, RTB200_E_INVALID, "scene already committed");
-    if (layout != RTB200_BVH_F32 && layout != RTB200_BVH_Q8) return SetError(ctx, RTB200_E_INVALID, "unknown BVH layout");
+    if (layout != RTB200_BVH_F32 && layout != RTB200_BVH_Q8 && layout != RTB200_BVH_W8)
+        return SetError(ctx, RTB200_E_INVALID, "unknown BVH layout");
     const int64_t n_tri = (int64_t)s->tri_material.size();
     if (n_tri == 0) return SetError(ctx, RTB200_E_INVALID, "scene has no triangles");
     cudaSetDevice(ctx->device);
@@ -399,12 +400,30 @@ int rtb200_scene_commit(rtb200_scene* s, int32_t layout)
         return SetError(ctx, RTB200_E_INVALID, "BVH deeper than the traversal stack (" +
                         std::to_string(s->stack_bound) + " > " + std::to_string(kTraceStackMax) + " entries)");
     std::vector<GpuTri> tris;
-    EncodeTriangles(s->tri9.data(), s->bvh, tris);
     std::vector<GpuNode4> nf;
     std::vector<QNode4> nq;
+    std::vector<WNode8> nw;
     const void* nodes_src;
     size_t nodes_bytes;
-    if (layout == RTB200_BVH_Q8) {
+    int64_t n_nodes = (int64_t)s->bvh.nodes4.size();
+    if (layout == RTB200_BVH_W8) {
+        int depth = 0;
+        if (!EncodeWideNodes(s->bvh, nw, s->leaf_prims, depth))
+            return SetError(ctx, RTB200_E_INVALID, "a BVH leaf holds more than 24 triangles");
+        // One stack entry per node level below the root.
+        if (depth - 1 > kW8MaxLevels)
+            return SetError(ctx, RTB200_E_INVALID, "BVH deeper than the eight-wide traversal stack (" +
+                            std::to_string(depth - 1) + " > " + std::to_string(kW8MaxLevels) + " levels)");
+        EncodeWideTriangles(s->tri9.data(), s->leaf_prims, tris);
+        nodes_src = nw.data();
+        nodes_bytes = nw.size() * sizeof(WNode8);
+        n_nodes = (int64_t)nw.size();
+    } else {
+        s->leaf_prims = s->bvh.prims;
+        EncodeTriangles(s->tri9.data(), s->bvh, tris);
+    }
+    if (layout == RTB200_BVH_W8) {
+    } else if (layout == RTB200_BVH_Q8) {
         EncodeQuantNodes(s->bvh, nq);
         nodes_src = nq.data();
         nodes_bytes = nq.size() * sizeof(QNode4);
@@ -432,7 +451,7 @@ int rtb200_scene_commit(rtb200_scene* s, int32_t layout)
     s->nodes_bytes = nodes_bytes;
     s->d_tris = (GpuTri*)dt;
     s->tris_bytes = tris.size() * sizeof(GpuTri);
-    s->n_nodes = (int64_t)s->bvh.nodes4.size();
+    s->n_nodes = n_nodes;
     s->layout = layout;
     rc = UploadShading(s);
     if (rc) {

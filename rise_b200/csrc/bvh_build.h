@@ -112,7 +112,31 @@ struct alignas(16) GpuTri {
 };
 static_assert(sizeof(GpuTri) == 48, "GpuTri must be 48 bytes");
 
-// Both device layouts store the nodes in breadth-first order (root first), so
+// Eight-wide compressed node, 80 bytes (bvh_wide.cpp): per-node origin,
+// power-of-two scale exponents and internal-child mask; the first internal
+// child's node index (the others follow in slot order) and the first
+// triangle of the leaf slots; per slot a meta byte (leaf: triangle count in
+// unary in bits 5-7 above a 5-bit offset from tri_base; 0 otherwise) and
+// 8-bit conservative bounds per axis.
+struct alignas(16) WNode8 {
+    float px, py, pz;
+    int8_t ex, ey, ez;
+    uint8_t imask;
+    uint32_t child_base;
+    uint32_t tri_base;
+    uint8_t meta[8];
+    uint8_t qlox[8], qloy[8], qloz[8];
+    uint8_t qhix[8], qhiy[8], qhiz[8];
+};
+static_assert(sizeof(WNode8) == 80, "WNode8 must be 80 bytes");
+
+// Collapse the BVH2 of `b` to eight-wide nodes in breadth-first order;
+// prims receives the triangle order the nodes' triangle bases index, depth
+// the number of node levels.  False when a leaf holds more than 24 triangles.
+bool EncodeWideNodes(const BuiltBVH& b, std::vector<WNode8>& nodes, std::vector<uint32_t>& prims, int& depth);
+void EncodeWideTriangles(const float* tri9, const std::vector<uint32_t>& prims, std::vector<GpuTri>& out);
+
+// Both four-wide device layouts store the nodes in breadth-first order (root first), so
 // the top levels, which every ray visits, share cache lines and pages.
 void EncodeGpuNodes(const BuiltBVH& b, std::vector<GpuNode4>& out);
 void EncodeQuantNodes(const BuiltBVH& b, std::vector<QNode4>& out);
@@ -130,5 +154,10 @@ int TraceStackBound(const BuiltBVH& b);
 // exceeds kTraceStackMax is refused at commit.
 constexpr int kTraceStackShared = 40;
 constexpr int kTraceStackMax = 128;
+// Eight-wide traversal: one stack entry per node level below the root, the
+// rest for postponed triangle groups; trees deeper than kW8MaxLevels levels
+// below the root are refused at commit.
+constexpr int kW8StackEntries = 24;
+constexpr int kW8MaxLevels = 12;
 
 }  // namespace rtb200

@@ -103,6 +103,7 @@ struct rtb200_scene {
     int32_t stack_bound = 0;         // TraceStackBound of the committed BVH
     double build_seconds = 0.0;
     rtb200::BuiltBVH bvh;            // kept for the path tracer's emitter tables
+    std::vector<uint32_t> leaf_prims;   // triangle order of d_tris (input index per slot)
     // device data
     void* d_nodes = nullptr;
     size_t nodes_bytes = 0;

@@ -486,6 +486,8 @@ int rtb200_job_create(rtb200_scene* s, const rtb200_render_settings* rs, rtb200_
     *out = nullptr;
     if (!s->committed || s->materials.empty())
         return SetError(ctx, RTB200_E_INVALID, "scene must be committed with materials");
+    if (s->layout == RTB200_BVH_W8)
+        return SetError(ctx, RTB200_E_INVALID, "the path tracer runs on the F32 and Q8 BVH layouts");
     if (rs->width <= 0 || rs->height <= 0 || (int64_t)rs->width * rs->height > (1ll << 28) || rs->max_depth < 1 ||
         rs->max_depth > 255 || !(rs->lambda_max > rs->lambda_min) || rs->lambda_min < 380.0f ||
         rs->lambda_max > 780.0f || !(rs->fov_deg > 0.0f && rs->fov_deg < 180.0f))
@@ -498,7 +500,8 @@ int rtb200_job_create(rtb200_scene* s, const rtb200_render_settings* rs, rtb200_
         return SetError(ctx, RTB200_E_INVALID, "bad light selection");
     if (rs->adaptive_max_spp < 0 || (rs->adaptive_max_spp > 0 && !(rs->adaptive_threshold > 0.0f)))
         return SetError(ctx, RTB200_E_INVALID, "bad adaptive sampling settings");
-    if (rs->sampler != RTB200_SAMPLER_HASH && rs->sampler != RTB200_SAMPLER_SOBOL)
+    if (rs->sampler != RTB200_SAMPLER_HASH && rs->sampler != RTB200_SAMPLER_SOBOL &&
+        rs->sampler != RTB200_SAMPLER_SOBOL_SHUFFLED)
         return SetError(ctx, RTB200_E_INVALID, "bad sampler");
     if (rs->bounce_limits && (rs->max_diffuse_bounce < 0 || rs->max_glossy_bounce < 0 ||
                               rs->max_transmission_bounce < 0))
@@ -546,7 +549,8 @@ int rtb200_job_create(rtb200_scene* s, const rtb200_render_settings* rs, rtb200_
     st.n_lights = (int)s->lights.size();
     st.n_spectra = (int)(s->spectra.size() / RTB200_CIE_COUNT);
     st.light_bvh = rs->light_selection == RTB200_LIGHTS_BVH ? 1 : 0;
-    st.sampler = rs->sampler == RTB200_SAMPLER_SOBOL ? kSamplerSobol : kSamplerHash;
+    st.sampler = rs->sampler == RTB200_SAMPLER_SOBOL ? kSamplerSobol
+                 : rs->sampler == RTB200_SAMPLER_SOBOL_SHUFFLED ? kSamplerSobolShuffled : kSamplerHash;
     {
         // Counts are kept in a byte each and a path has at most 255 vertices,
         // so 255 means no limit.

@@ -156,9 +156,9 @@ __device__ __forceinline__ void Splat(const PtPaths& P, const PtJobDev& J, int s
     const int W = J.cam.width, H = J.cam.height;
     const int px = (int)(m.x % (uint32_t)W), py = (int)(m.x / (uint32_t)W);
     // The camera's jitter numbers again (hash key or Sobol seed in m.w, sample in m.y).
-    const bool sobol = S.sampler == kSamplerSobol;
-    const float ox = sobol ? SobolSample(m.y, 0, m.w) : Rand(m.w, 0);
-    const float oy = sobol ? SobolSample(m.y, 1, m.w) : Rand(m.w, 1);
+    const bool sobol = S.sampler != kSamplerHash, shuf = S.sampler == kSamplerSobolShuffled;
+    const float ox = sobol ? SobolSample(m.y, 0, m.w, shuf) : Rand(m.w, 0);
+    const float oy = sobol ? SobolSample(m.y, 1, m.w, shuf) : Rand(m.w, 1);
     const float sx = (float)px + ox - 0.5f, sy = (float)py + 0.5f - oy;
     const float hw = S.filt_half;
     const int x0 = max(0, (int)floorf(sx - hw)), x1 = min(W - 1, (int)floorf(sx + hw));
@@ -315,7 +315,7 @@ KRegen(const PtJobDev* __restrict__ jobs, PtPaths P, PtQueues Q, int assign)
                 const uint32_t pixel = J.px_list ? __ldg(J.px_list + slot_px) : slot_px;
                 const uint32_t sample = (uint32_t)(J.sample_begin + g / (unsigned long long)J.npix);
                 const int px = (int)(pixel % (uint32_t)J.cam.width), py = (int)(pixel / (uint32_t)J.cam.width);
-                const bool sobol = J.set.sampler == kSamplerSobol;
+                const bool sobol = J.set.sampler != kSamplerHash, shuf = J.set.sampler == kSamplerSobolShuffled;
                 // Hash key, or the pixel's Sobol seed (camera dimensions 0-2).
                 const uint32_t key = sobol ? SobolPixelSeed((uint32_t)px, (uint32_t)py, J.set.seed)
                                            : PathKey(J.set.seed, pixel, sample);
@@ -326,8 +326,8 @@ KRegen(const PtJobDev* __restrict__ jobs, PtPaths P, PtQueues Q, int assign)
                 // (PathTracingSpectralRasterizer.cpp:321-331, BoxPixelFilter.h:54-58),
                 // or the pixel centre moved by the truncated Gaussian's
                 // inverse CDF for a narrow Gaussian (GaussianPixelFilter.h:109-127).
-                const float ox = sobol ? SobolSample(sample, 0, key) : Rand(key, 0);
-                const float oy = sobol ? SobolSample(sample, 1, key) : Rand(key, 1);
+                const float ox = sobol ? SobolSample(sample, 0, key, shuf) : Rand(key, 0);
+                const float oy = sobol ? SobolSample(sample, 1, key, shuf) : Rand(key, 1);
                 float fx, fy;
                 if (J.set.filter == kFilterWarp) {
                     const float v = fmaxf(J.set.filt_trunc + (1.0f - J.set.filt_trunc) * ox, 1e-30f);
@@ -345,7 +345,7 @@ KRegen(const PtJobDev* __restrict__ jobs, PtPaths P, PtQueues Q, int assign)
                 const V3 d = normalize(mk(J.cam.fwd[0] + sx * J.cam.right[0] + sy * J.cam.up[0],
                                           J.cam.fwd[1] + sx * J.cam.right[1] + sy * J.cam.up[1],
                                           J.cam.fwd[2] + sx * J.cam.right[2] + sy * J.cam.up[2]));
-                const float hero = J.set.lmin + (sobol ? SobolSample(sample, 2, key) : Rand(key, 2)) *
+                const float hero = J.set.lmin + (sobol ? SobolSample(sample, 2, key, shuf) : Rand(key, 2)) *
                                                     (J.set.lmax - J.set.lmin);
                 P.ray_o[slot] = make_float4(J.cam.pos[0], J.cam.pos[1], J.cam.pos[2], 0.0f);
                 P.ray_d[slot] = make_float4(d.x, d.y, d.z, __int_as_float(0x7f800000));
@@ -545,7 +545,7 @@ KShade(const PtJobDev* __restrict__ jobs, PtPaths P, PtQueues Q, int from_class)
         float4 L = P.L[slot];
         const int depth = (int)(m.z & kFlagDepthMask);
         // Random numbers: hash key or Sobol seed in meta.w, sample index in meta.y.
-        VertexRng rng{m.w, m.y, depth, set.sampler == kSamplerSobol, 0u};
+        VertexRng rng{m.w, m.y, depth, set.sampler, 0u};
         const float bsdfPdf = aux.y;
         const unsigned term = (m.z >> kTermShift) & 0xfu;
         float lam[4];

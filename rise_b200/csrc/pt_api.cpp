@@ -258,7 +258,7 @@ int UploadShading(rtb200_scene* s)
         for (int64_t t = s->meshes[mi].first; t < s->meshes[mi].first + s->meshes[mi].count; ++t) triMesh[t] = (int)mi;
     std::vector<PtTriAttr> attr(ntri);
     for (size_t slot = 0; slot < ntri; ++slot) {
-        const int mi = triMesh[s->bvh.prims[slot]];
+        const int mi = triMesh[s->leaf_prims[slot]];
         const auto& mesh = s->meshes[mi];
         attr[slot].mat = (mesh.material & kAttrMatMask) | (mesh.double_sided ? kAttrDoubleSided : 0);
         attr[slot].light = meshLight[mi];
@@ -269,7 +269,7 @@ int UploadShading(rtb200_scene* s)
     if (!s->tri_smooth.empty()) {
         s->tri_normals.assign(ntri, make_uint4(0, 0, 0, 0));
         for (size_t slot = 0; slot < ntri; ++slot) {
-            const uint32_t t = s->bvh.prims[slot];
+            const uint32_t t = s->leaf_prims[slot];
             if (!s->tri_smooth[t]) continue;
             unsigned q[3];
             for (int j = 0; j < 3; ++j) {

@@ -75,17 +75,27 @@ __device__ __forceinline__ uint32_t SobolDim1(uint32_t i)
     return v;
 }
 
-__device__ __forceinline__ float SobolSample(uint32_t index, uint32_t dim, uint32_t seed)
+// Owen scrambling by the Laine-Karras hash on the bit-reversed value.
+__device__ __forceinline__ uint32_t OwenScramble(uint32_t v, uint32_t s)
 {
-    uint32_t v = (dim & 1u) ? SobolDim1(index) : __brev(index);
-    const uint32_t s = HashCombine(seed, dim);
     v = __brev(v);
     v ^= v * 0x3d20adeau;
     v += s;
     v *= (s >> 16) | 1u;
     v ^= v * 0x05526c56u;
     v ^= v * 0x53a22864u;
-    v = __brev(v);
+    return __brev(v);
+}
+
+// shuffle: the sample index is first Owen-scrambled with a seed per
+// dimension pair (2k, 2k + 1), Burley's decorrelation of padded dimensions
+// ("Practical Hash-based Owen Scrambling", JCGT 9(4), 2020, section 4), so
+// different pairs no longer replay one Sobol pair under another scramble;
+// the reference pads without it.
+__device__ __forceinline__ float SobolSample(uint32_t index, uint32_t dim, uint32_t seed, bool shuffle = false)
+{
+    if (shuffle) index = OwenScramble(index, HashCombine(HashCombine(seed, 0x5bd1e995u), dim >> 1));
+    const uint32_t v = OwenScramble((dim & 1u) ? SobolDim1(index) : __brev(index), HashCombine(seed, dim));
     return (float)(v >> 8) * (1.0f / 16777216.0f);   // the top 24 bits: < 1 in FP32
 }
 
@@ -107,11 +117,12 @@ struct VertexRng {
     uint32_t key;      // hash key, or the pixel's Sobol seed
     uint32_t index;    // sample index (Sobol)
     int depth;
-    int sobol;
+    int mode;          // kSamplerHash / kSamplerSobol / kSamplerSobolShuffled
     uint32_t cur;
     __device__ __forceinline__ float next(int j)
     {
-        if (sobol) return SobolSample(index, (16u + (uint32_t)depth) * 32u + cur++, key);
+        if (mode != kSamplerHash)
+            return SobolSample(index, (16u + (uint32_t)depth) * 32u + cur++, key, mode == kSamplerSobolShuffled);
         return Rand(key, Dim(depth, j));
     }
     __device__ __forceinline__ void skip(int n) { cur += (uint32_t)n; }

@@ -102,12 +102,13 @@ struct PtSettings {
     float filt_sigma;        // Gaussian sigma in pixels (warp mode)
     float filt_trunc;        // exp(-K^2 / 2), K = half-width / sigma (warp mode)
     int light_bvh;           // pick NEE luminaries with the light BVH (when the scene has one)
-    int sampler;             // kSamplerHash / kSamplerSobol
+    int sampler;             // kSamplerHash / kSamplerSobol / kSamplerSobolShuffled
     int max_bounce[3];       // diffuse, glossy, transmission scatters a path may take (255 = no limit)
 };
 
 constexpr int kSamplerHash = 0;
 constexpr int kSamplerSobol = 1;
+constexpr int kSamplerSobolShuffled = 2;
 
 // Bounce types (ScatteredRay::ScatRayType): the counters live in aux.w, one
 // byte each.

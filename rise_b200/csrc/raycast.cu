@@ -70,6 +70,49 @@ KTrace(const NodeT* __restrict__ nodes, const GpuTri* __restrict__ tris,
 
 namespace {
 
+// Node visits per lane between ray refills of the eight-wide kernel.
+constexpr int kW8Budget = 16;
+
+template <bool ANY>
+__global__ void __launch_bounds__(kTraceBlock, 8)
+KTraceW8(const WNode8* __restrict__ nodes, const GpuTri* __restrict__ tris, const rtb200_ray* __restrict__ rays,
+         long long n, rtb200_hit* __restrict__ hits, uint8_t* __restrict__ occ, unsigned long long* counter,
+         unsigned* err)
+{
+    __shared__ uint2 sstack[kW8Stack * kTraceBlock];
+    uint2* stk = sstack + threadIdx.x;
+    WarpFeed feed{0ull, 0ull, false};
+    W8State s;
+    long long ray = -1;
+    for (;;) {
+        const long long got = FeedTake(feed, ray < 0, (unsigned long long)n, counter);
+        if (got >= 0) {
+            ray = got;
+            StartRayW8(s, LoadRay(rays, ray));
+        }
+        if (__all_sync(kFull, ray < 0)) break;
+        if (ray >= 0 && TraceW8<ANY>(s, nodes, tris, stk, err, kW8Budget)) {
+            if (ANY) {
+                occ[ray] = s.bestSlot >= 0 ? 1 : 0;
+            } else {
+                float4 out;
+                if (s.bestSlot >= 0) {
+                    const float* tb = reinterpret_cast<const float*>(tris + s.bestSlot);
+                    const float4 A = ldg4(tb), B = ldg4(tb + 4), C = ldg4(tb + 8);
+                    out.x = (float)RefineT(s.p.o, s.d, A, B, C);
+                    out.y = A.w;
+                    out.z = s.ba;
+                    out.w = s.bb;
+                } else {
+                    out = make_float4(-1.0f, __int_as_float(-1), 0.0f, 0.0f);
+                }
+                *reinterpret_cast<float4*>(hits + ray) = out;
+            }
+            ray = -1;
+        }
+    }
+}
+
 template <class K>
 int GridFor(K kernel, int num_sms)
 {
@@ -105,7 +148,17 @@ cudaError_t Dispatch(const rtb200_scene* s, const rtb200_ray* d_rays, int64_t n,
 {
     if (n <= 0) return cudaSuccess;
     const bool spill = s->stack_bound > kTraceStack;
-    if (s->layout == RTB200_BVH_Q8) {
+    if (s->layout == RTB200_BVH_W8) {
+        static std::atomic<int> grids[kGridDevices];
+        const int dev = s->ctx->device;
+        int grid = (dev >= 0 && dev < kGridDevices) ? grids[dev].load(std::memory_order_relaxed) : 0;
+        if (!grid) {
+            grid = GridFor(KTraceW8<ANY>, s->ctx->num_sms);
+            if (dev >= 0 && dev < kGridDevices) grids[dev].store(grid, std::memory_order_relaxed);
+        }
+        KTraceW8<ANY><<<grid, kTraceBlock, 0, stream>>>((const WNode8*)s->d_nodes, s->d_tris, d_rays, n, hits, occ,
+                                                        counter, err);
+    } else if (s->layout == RTB200_BVH_Q8) {
         if (spill) Launch<QNode4, ANY, true>(s, d_rays, n, hits, occ, counter, err, stream);
         else Launch<QNode4, ANY, false>(s, d_rays, n, hits, occ, counter, err, stream);
     } else {

@@ -391,6 +391,168 @@ __device__ __forceinline__ bool TraceRound(TraceState& s, const NodeT* __restric
     return s.node == kEmpty && s.leaf == kEmpty;
 }
 
+// ---- eight-wide compressed nodes (WNode8, bvh_wide.cpp) -------------------
+// Per-lane traversal after Ylitie, Karras and Laine (HPG 2017): a node group
+// (first internal child's index; hit children in bits 24-31 in visiting
+// order, the node's internal-child mask in bits 0-7) and a triangle group
+// (first triangle; hit triangles in bits 0-23).  A node's hit children are
+// visited in slot order s ^ oct, oct the ray's non-negative direction signs,
+// which the build made roughly near to far; groups wait on a stack of one
+// entry per tree level, bounded at commit.
+
+constexpr int kW8Stack = kW8StackEntries;   // uint2 entries per thread in shared memory
+constexpr int kW8Levels = kW8MaxLevels;      // node groups the stack keeps room for
+
+struct W8State {
+    RayPre p;
+    float d[3];
+    float best;
+    int bestSlot;
+    float ba, bb;
+    unsigned oct;
+    uint2 ng;          // node group
+    int sp;
+    int visits;        // iterations spent on this ray (bounded)
+};
+
+// A ray takes at most this many iterations (each visits one node or tests
+// one triangle group; a tree of n triangles has fewer than n nodes), else its
+// traversal stops with the error flag raised.
+constexpr int kW8MaxIterations = 1 << 22;
+
+__device__ __forceinline__ void StartRayW8(W8State& s, const Ray& r)
+{
+    Prepare(r, s.p);
+    s.d[0] = r.d[0]; s.d[1] = r.d[1]; s.d[2] = r.d[2];
+    s.best = r.tmax;
+    s.bestSlot = -1;
+    s.ba = s.bb = 0.0f;
+    s.oct = (r.d[0] >= 0.0f ? 1u : 0u) | (r.d[1] >= 0.0f ? 2u : 0u) | (r.d[2] >= 0.0f ? 4u : 0u);
+    // The root as the one internal child (slot 0) of a virtual parent at 0.
+    s.ng = make_uint2(0u, (1u << (24 + s.oct)) | 1u);
+    s.sp = 0;
+    s.visits = 0;
+}
+
+// Child slabs of one node: the node group of its hit internal children and
+// the triangle group of its hit leaf slots.
+__device__ __forceinline__ void IntersectW8(const WNode8* __restrict__ nodes, unsigned ni, const RayPre& p,
+                                            unsigned oct, float best, uint2& ng, uint2& tg)
+{
+    const uint4* base = reinterpret_cast<const uint4*>(nodes + ni);
+    const uint4 w0 = __ldg(base), w1 = __ldg(base + 1), w2 = __ldg(base + 2), w3 = __ldg(base + 3),
+                w4 = __ldg(base + 4);
+    const float org[3] = {__uint_as_float(w0.x), __uint_as_float(w0.y), __uint_as_float(w0.z)};
+    const unsigned em = w0.w;
+    const int e[3] = {(int)(int8_t)(em & 0xffu), (int)(int8_t)((em >> 8) & 0xffu), (int)(int8_t)((em >> 16) & 0xffu)};
+    const unsigned imask = em >> 24;
+    // Bounds per axis as two words of four bytes (slots 0-3, 4-7); near and
+    // far planes by the direction's sign (see SlabF32).
+    const unsigned lo[3][2] = {{w2.x, w2.y}, {w2.z, w2.w}, {w3.x, w3.y}};
+    const unsigned hi[3][2] = {{w3.z, w3.w}, {w4.x, w4.y}, {w4.z, w4.w}};
+    unsigned qn[3][2], qf[3][2];
+    float a[3], sc[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const bool neg = p.inv[k] < 0.0f;
+        qn[k][0] = neg ? hi[k][0] : lo[k][0];
+        qn[k][1] = neg ? hi[k][1] : lo[k][1];
+        qf[k][0] = neg ? lo[k][0] : hi[k][0];
+        qf[k][1] = neg ? lo[k][1] : hi[k][1];
+        a[k] = (org[k] - p.o[k]) * p.inv[k];
+        sc[k] = __int_as_float((e[k] + 127) << 23) * p.inv[k];
+    }
+    unsigned hitsN = 0u, hitsT = 0u;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        const int h = i >> 2, sh = 8 * (i & 3);
+        float tl[3], th[3];
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            tl[k] = fmaf((float)((qn[k][h] >> sh) & 0xffu), sc[k], a[k]);
+            th[k] = fmaf((float)((qf[k][h] >> sh) & 0xffu), sc[k], a[k]);
+        }
+        const float tn = Max3(tl[0], tl[1], fmaxf(tl[2], p.tmin));
+        const float tf = Min3(th[0], th[1], fminf(th[2], best));
+        if (tn <= tf) {
+            if ((imask >> i) & 1u) {
+                hitsN |= 1u << (24 + (i ^ oct));
+            } else {
+                const unsigned meta = ((i < 4 ? w1.z : w1.w) >> sh) & 0xffu;
+                hitsT |= (meta >> 5) << (meta & 31u);
+            }
+        }
+    }
+    ng = make_uint2(w1.x, hitsN | imask);
+    tg = make_uint2(w1.y, hitsT);
+}
+
+// Lanes below which a warp postpones its triangle tests (pushes the
+// triangle group and keeps descending), after Ylitie et al.
+constexpr int kW8TriLanes = 8;
+
+// Traverses for at most `budget` iterations; returns true when the ray is
+// finished.  The current group `ng` is a node group (hits in bits 24-31) or,
+// popped from the stack, a postponed triangle group (bits 0-23 only).  A
+// triangle group is postponed while fewer than kW8TriLanes lanes of the warp
+// have triangles to test and the stack keeps room for one node group per
+// level (kW8Levels).  ANY: stop at the first accepted hit.
+template <bool ANY>
+__device__ __forceinline__ bool TraceW8(W8State& s, const WNode8* __restrict__ nodes,
+                                        const GpuTri* __restrict__ tris, uint2* stk, unsigned* err, int budget)
+{
+    for (int it = 0; it < budget; ++it) {
+        if (++s.visits > kW8MaxIterations) {
+            atomicOr(err, kErrStackOverflow);
+            return true;
+        }
+        uint2 tg = make_uint2(0u, 0u);
+        if (s.ng.y & 0xff000000u) {
+            const unsigned j = (unsigned)__ffs(s.ng.y >> 24) - 1u;
+            s.ng.y &= ~(1u << (24 + j));
+            const unsigned slot = j ^ s.oct;
+            const unsigned ni = s.ng.x + (unsigned)__popc(s.ng.y & 0xffu & ((1u << slot) - 1u));
+            if (s.ng.y & 0xff000000u) {
+                if (s.sp < kW8Stack) { stk[s.sp * kTraceBlock] = s.ng; ++s.sp; }
+                else atomicOr(err, kErrStackOverflow);
+            }
+            IntersectW8(nodes, ni, s.p, s.oct, s.best, s.ng, tg);
+        } else {
+            tg = s.ng;   // a postponed triangle group (or nothing)
+            s.ng = make_uint2(0u, 0u);
+        }
+        while (tg.y) {
+            // Postpone only with a node group to continue with, so a popped
+            // triangle group is always tested (the ray keeps progressing).
+            if ((s.ng.y & 0xff000000u) && s.sp < kW8Stack - kW8Levels &&
+                __popc(__ballot_sync(__activemask(), true)) < kW8TriLanes) {
+                stk[s.sp * kTraceBlock] = tg;
+                ++s.sp;
+                break;
+            }
+            const unsigned k = (unsigned)__ffs(tg.y) - 1u;
+            tg.y &= tg.y - 1u;
+            const unsigned slot = tg.x + k;
+            const float* tb = reinterpret_cast<const float*>(tris + slot);
+            const float4 A = ldg4(tb), B = ldg4(tb + 4), C = ldg4(tb + 8);
+            float t, al, be;
+            if (Watertight(s.p, A, B, C, s.best, t, al, be)) {
+                s.bestSlot = (int)slot;
+                if (ANY) return true;
+                s.best = t;
+                s.ba = al;
+                s.bb = be;
+            }
+        }
+        if (!(s.ng.y & 0xff000000u)) {
+            if (s.sp == 0) return true;
+            --s.sp;
+            s.ng = stk[s.sp * kTraceBlock];
+        }
+    }
+    return false;
+}
+
 // Warp-cooperative ray supply: a lane whose ray is finished takes the next
 // index from a warp-local chunk; the chunk is refilled from the global
 // counter kChunk rays at a time (one atomic per chunk per warp).

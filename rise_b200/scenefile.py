@@ -472,8 +472,11 @@ class _Loader:
             if c.has(k):
                 self.st[k] = int(c.get(k))
         # The reference's integrator always draws its path decisions from its
-        # Owen-scrambled Sobol sampler (PathTracingSpectralRasterizer.cpp:206-479).
-        self.st["sampler"] = scenes.SAMPLER_SOBOL
+        # Owen-scrambled Sobol sampler (PathTracingSpectralRasterizer.cpp:206-479);
+        # rendered here with the sample index shuffled per dimension pair, which
+        # converges per pixel where the reference's padding does not
+        # (scenes.SAMPLER_SOBOL is the reference's sequence as it is).
+        self.st["sampler"] = scenes.SAMPLER_SOBOL_SHUFFLED
         if not _bool(c.get("show_luminaires", "true")):
             self.refuse(c, "hidden luminaires (show_luminaires false) are not supported")
         for k, why in (("pixel_sampler", "camera jitter is drawn from the path's Sobol dimensions 0 and 1, "

@@ -244,6 +244,7 @@ def spectral_painter(nm, amplitudes, nmbegin=400.0, nmend=700.0):
 
 SAMPLER_HASH = 0    # counter-based hash of (seed, pixel, sample, dimension)
 SAMPLER_SOBOL = 1   # the reference's Owen-scrambled padded Sobol
+SAMPLER_SOBOL_SHUFFLED = 2   # the same with the index shuffled per dimension pair (converges per pixel)
 
 
 @dataclass

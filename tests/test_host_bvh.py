@@ -79,3 +79,44 @@ def test_traversal_stack_bounds():
     # ... and the nested-cluster scene needs the local-memory continuation.
     b = stack_bound(raycaster.build_host_bvh(scenes.nested_clusters())[2])
     assert 40 < b <= 128
+
+
+# ---- the eight-wide layout (rise_b200/csrc/bvh_wide.cpp) --------------------
+
+def _w8_checker(tmp_path_factory):
+    import subprocess
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    src = os.path.join(root, "rise_b200", "csrc")
+    exe = str(tmp_path_factory.mktemp("w8") / "w8_check")
+    subprocess.run(["g++", "-O2", "-std=c++17", "-I", src, os.path.join(root, "tests", "cpp", "w8_check.cpp"),
+                    os.path.join(src, "bvh_build.cpp"), os.path.join(src, "bvh_wide.cpp"), "-o", exe, "-lpthread"],
+                   check=True)
+    return exe
+
+
+@pytest.fixture(scope="module")
+def w8_check(tmp_path_factory):
+    return _w8_checker(tmp_path_factory)
+
+
+@pytest.mark.parametrize("case", ["soup", "tiny1", "tiny5", "deep"])
+def test_wide_nodes_are_conservative_and_find_every_closest_hit(w8_check, tmp_path, case):
+    """The eight-wide encoding: each triangle once, links and runs in range,
+    every 8-bit child box containing its triangles, and the device's
+    traversal rules (octant order, groups, one stack entry per level) finding
+    the brute-force closest hit of every ray."""
+    import subprocess
+    from rise_b200 import scenes
+    if case == "soup":
+        tri, rays = scenes.soup_triangles(20000, seed=4), scenes.sphere_rays(1500, seed=4)
+    elif case == "deep":
+        tri = scenes.nested_clusters()
+        rays = scenes.cluster_rays(tri, 1500, seed=5)
+    else:
+        n = 1 if case == "tiny1" else 5
+        tri, rays = scenes.soup_triangles(n, seed=n), scenes.sphere_rays(500, seed=n)
+    tp, rp = tmp_path / "tri.bin", tmp_path / "rays.bin"
+    np.ascontiguousarray(tri, np.float32).tofile(tp)
+    np.ascontiguousarray(rays, np.float32).tofile(rp)
+    out = subprocess.run([w8_check, str(tp), str(rp)], capture_output=True, text=True)
+    assert out.returncode == 0 and out.stdout.startswith("ok"), out.stdout + out.stderr

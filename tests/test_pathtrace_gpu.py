@@ -328,7 +328,7 @@ def test_materials_same_seed_matches_oracle(ctx, nee_per_lambda):
     assert abs(g[..., 1].mean() / o[..., 1].mean() - 1) < 5e-3
 
 
-@pytest.mark.parametrize("sampler,limits", [(0, (2, 1, 3)), (1, None), (1, (1, 2, 2))])
+@pytest.mark.parametrize("sampler,limits", [(0, (2, 1, 3)), (1, None), (1, (1, 2, 2)), (2, None)])
 def test_sampler_and_bounce_limits_same_seed_match_oracle(ctx, sampler, limits):
     """The reference's Sobol sampler and per-type bounce limits on GGX,
     glass, Lambertian and sky: same numbers, same decisions as the oracle."""
@@ -440,22 +440,6 @@ def test_full_size_cornell(ctx):
     # Same random numbers as the oracle: compare a crop.
     o = oracle.pt_render(d, 16, crop=(96, 96, 160, 160))
     assert rel_mse(g[96:160, 96:160], o) < 1e-3
-
-
-def test_full_config_against_fp64_oracle_image(ctx):
-    """The full Cornell configuration (256x256, per-wavelength NEE) at 256 spp
-    against the FP64 oracle's 16384-spp image of an independent seed
-    (tests/golden/cornell_fp64_16384spp.npz): the relMSE is the GPU's own
-    noise (1.6e-3 at 256 spp; the reference image adds ~2e-5), and the
-    image-wide and per-wall means agree within 0.5 % (no bias)."""
-    import os
-    ref = np.load(os.path.join(os.path.dirname(__file__), "golden", "cornell_fp64_16384spp.npz"))["xyz"]
-    ref = ref.astype(np.float64)
-    g, _ = render_gpu(ctx, scenes.cornell_box(256, 256), 256, chunks=[64, 64, 128])
-    assert rel_mse(g, ref) < 2.5e-3
-    assert abs(g.mean() / ref.mean() - 1.0) < 5e-3
-    for sl in (np.s_[:, :64], np.s_[:, 192:], np.s_[192:, 64:192], np.s_[:32, 64:192]):
-        assert abs(g[sl].mean() / ref[sl].mean() - 1.0) < 1e-2, sl
 
 
 def test_large_scene_against_fp64_oracle_crop(ctx):

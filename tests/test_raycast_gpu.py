@@ -19,7 +19,7 @@ from parity import any_report, closest_report
 pytestmark = pytest.mark.gpu
 
 GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
-LAYOUTS = ["f32", "q8"]
+LAYOUTS = ["f32", "q8", "w8"]
 
 
 @pytest.fixture(scope="module")
@@ -123,13 +123,19 @@ def test_layouts_agree_and_are_deterministic(ctx):
     rays = scenes.sphere_rays(500000, seed=5)
     sf, rf = make_caster(ctx, tri, "f32")
     sq, rq = make_caster(ctx, tri, "q8")
+    sw, rw = make_caster(ctx, tri, "w8")
     a = rf.cast_rays(rays)
     b = rq.cast_rays(rays)
     c = rf.cast_rays(rays)
+    w = rw.cast_rays(rays)
+    w2 = rw.cast_rays(rays)
     assert (a["prim"] == c["prim"]).all() and (a["t"] == c["t"]).all()
+    assert (w["prim"] == w2["prim"]).all() and (w["t"] == w2["t"]).all()
     assert (a["prim"] == b["prim"]).mean() > 0.99999
+    assert (a["prim"] == w["prim"]).mean() > 0.99999
     sf.close()
     sq.close()
+    sw.close()
 
 
 def test_device_api_matches_host_api(ctx):

@@ -56,14 +56,14 @@ def render(ctx, desc, spp, **settings):
         r.close()
 
 
-@pytest.mark.parametrize("sampler", [1, 0], ids=["sobol_vs_sobol", "hash_vs_independent"])
+@pytest.mark.parametrize("sampler", [1, 0, 2], ids=["sobol_vs_sobol", "hash_vs_independent", "shuffled_vs_independent"])
 def test_z_test_against_the_reference_renderer(ctx, c1, sampler):
     """The device's Sobol sampler against the reference's own (its default),
     and the hash sampler against the reference given independent numbers.
     The reference's padded Sobol sequence makes its images about 0.1-0.3 %
     brighter than with independent numbers, so image means against it are
     held to 0.5 %, and to the statistics alone otherwise."""
-    name = "cornell_c1_ref_k16.npz" if sampler else "cornell_c1_ref_k16_independent.npz"
+    name = "cornell_c1_ref_k16.npz" if sampler == 1 else "cornell_c1_ref_k16_independent.npz"
     f = np.load(os.path.join(GOLDEN, name))
     mr, vr, k, spp = f["mean"].astype(np.float64), f["var"].astype(np.float64), int(f["k"]), int(f["spp"])
     # Seeds other than the reference's batches 1..16, so no Sobol stream is shared.
@@ -76,21 +76,27 @@ def test_z_test_against_the_reference_renderer(ctx, c1, sampler):
     zy, _ = z_scores(g.mean(0)[..., 1], g.var(0, ddof=1)[..., 1], k, mr[..., 1], vr[..., 1], k)
     assert (np.abs(zy) > Z_LIMIT).mean() <= Z_ALLOWED_RATE
     se = np.sqrt(g[..., 1].mean(axis=(1, 2)).var(ddof=1) / k + vr[..., 1].mean() / k / mr[..., 1].size)
-    tol = 4 * se + (5e-3 * mr[..., 1].mean() if sampler else 0.0)
+    tol = 4 * se + (5e-3 * mr[..., 1].mean() if sampler == 1 else 0.0)
     assert abs(g[..., 1].mean() - mr[..., 1].mean()) < tol
 
 
 def test_relmse_against_the_reference_fp64_image(ctx, c1):
+    """1024 spp of the shuffled Sobol sampler against the reference's
+    16384-spp FP64 image (its integrator given independent numbers)."""
     path = os.path.join(GOLDEN, "cornell_c1_ref_fp64.npz")
     if not os.path.exists(path):
         pytest.skip("reference FP64 image not generated (tests/golden/make_cornell_reference.py fp64)")
     ref = np.load(path)["xyz"].astype(np.float64)
-    g = render(ctx, c1.desc, 1024, seed=7)
+    g = render(ctx, c1.desc, 1024, seed=7, sampler=2)
     e = rel_mse(g, ref)
     assert e < 1e-3, e
+    # No bias beyond the samplers' (0.5 %): the image and each wall.
+    assert abs(g.mean() / ref.mean() - 1.0) < 5e-3
+    for sl in (np.s_[:, :64], np.s_[:, 192:], np.s_[192:, 64:192], np.s_[:32, 64:192]):
+        assert abs(g[sl].mean() / ref[sl].mean() - 1.0) < 1e-2, sl
 
 
-@pytest.mark.parametrize("sampler", [1, 0])
+@pytest.mark.parametrize("sampler", [2, 1, 0])
 def test_same_random_numbers_as_the_oracle(ctx, c1, sampler):
     st = dataclasses.replace(c1.desc.settings, seed=3, sampler=sampler)
     g = render(ctx, c1.desc, 16, seed=3, sampler=sampler)[96:160]

@@ -43,17 +43,18 @@ def test_scene_ingest_reads_the_reference_settings():
     ls = scenefile.load_scene(SCENE)
     st = ls.desc.settings
     assert (st.width, st.height, ls.spp) == (256, 256, 16)
-    assert st.sampler == 1 and st.max_diffuse_bounce == 7 and st.rr_min_depth == 3
+    assert st.sampler == 2 and st.max_diffuse_bounce == 7 and st.rr_min_depth == 3
     assert (st.lambda_min, st.lambda_max) == (400.0, 700.0) and st.filter == 0
     assert ls.desc.n_tri == 32
 
 
-@pytest.mark.parametrize("sampler", [0, 1], ids=["hash_vs_independent", "sobol_vs_sobol"])
+@pytest.mark.parametrize("sampler", [0, 1, 2], ids=["hash_vs_independent", "sobol_vs_sobol", "shuffled_vs_independent"])
 def test_oracle_matches_reference_renderer_z_test(sampler):
     """16 batches of 16 spp of the restatement against the reference's 16:
-    the hash sampler against the reference with independent numbers, the
-    Sobol sampler against the reference's own Sobol sampler."""
-    mr, vr, k, spp = ref_k16(independent=sampler == 0)
+    the hash sampler and the shuffled Sobol sampler against the reference
+    with independent numbers, the reference's Sobol sampler against the
+    reference's own."""
+    mr, vr, k, spp = ref_k16(independent=sampler != 1)
     ls = scenefile.load_scene(SCENE)
     st = ls.desc.settings
     y0, y1 = ROWS
@@ -65,7 +66,7 @@ def test_oracle_matches_reference_renderer_z_test(sampler):
     assert (np.abs(z) > Z_LIMIT).mean() <= Z_ALLOWED_RATE, (np.abs(z) > Z_LIMIT).mean()
     # Image mean: within 4 standard errors of the batch-to-batch spread.
     se = np.sqrt(g[..., 1].mean(axis=(1, 2)).var(ddof=1) / k + vr[y0:y1, :, 1].mean() / k / g[0, ..., 1].size)
-    tol = 4 * se + (SOBOL_MEAN_TOL * mr[y0:y1, :, 1].mean() if sampler else 0.0)
+    tol = 4 * se + (SOBOL_MEAN_TOL * mr[y0:y1, :, 1].mean() if sampler == 1 else 0.0)
     assert abs(g[..., 1].mean() - mr[y0:y1, :, 1].mean()) < tol
 
 
