@@ -4,8 +4,9 @@ Workload (one "step"): one pass of 4,194,304 closest-hit rays over a
 1,000,000-triangle soup (centroids uniform in the unit cube, vertices offset
 by N(0, 0.01^2); rays from a radius-2 sphere towards uniform targets in the
 cube; seed 7), through the reference's BVH (SAH 32 bins, leaf 4, collapsed to
-4-wide nodes) with 8-bit quantised child boxes (the FP32-node layout is
-reported as a variant; both return the same hits).  Metric: Mrays/s.
+4-wide nodes) with 8-bit quantised child boxes (the FP32-node and
+binary16-node layouts are reported as variants; all return the same hits).
+Metric: Mrays/s.
 
   python bench.py [--gpus N --steps K --warmup W] [--impl reference]
 
@@ -60,6 +61,9 @@ def parse():
                    help="run only the path-tracer measurement and print its JSON (for profiling)")
     p.add_argument("--large-only", action="store_true",
                    help="run only the large-scene path-tracer measurement and print its JSON (for profiling)")
+    p.add_argument("--serving-full", action="store_true",
+                   help="run only the serving configuration at full size (20 req/s for 60 s over the whole "
+                        "batched-scenes distribution, 120 GB device budget; many minutes) and print its JSON")
     return p.parse_args()
 
 
@@ -323,7 +327,7 @@ def bench_batch(ctx):
     params = scenes.batch_scene_params()
     t0 = time.perf_counter()
     descs = [scenes.batch_scene(p) for p in params]
-    devs = [pathtracer.upload_scene(ctx, d) for d in descs]
+    devs = [pathtracer.upload_scene(ctx, d, "q8") for d in descs]
     setup = time.perf_counter() - t0
     spp = [p["spp"] for p in params]
     total = sum(p["res"] ** 2 * p["spp"] for p in params)
@@ -333,7 +337,8 @@ def bench_batch(ctx):
     eng = pathtracer.Engine(ctx, best.capacity)
     eng.set_poll(best.poll)
     out = {"workload": "48 scenes, triangles log-uniform 10k-1M, resolutions {128,256,512,1024}^2, "
-                       "spp log-uniform 4-256, max depth 8-16, FP32 BVH", "samples": total,
+                       "spp log-uniform 4-256, max depth 8-16, BVHs with 8-bit quantised child boxes",
+           "samples": total,
            "triangles": int(sum(p["n_tri"] for p in params)), "scene_setup_s": round(setup, 2),
            "autotune": {"capacity": best.capacity, "poll": best.poll, "seconds": round(tune_s, 2),
                         "tried": [[c.capacity, c.poll, round(c.msamples_s, 1)] for c in tried]}}
@@ -343,9 +348,12 @@ def bench_batch(ctx):
         eng.render([w], [1])
         w.close()
         one = [pathtracer.SpectralRasterizer(ctx, d, scene=s) for d, s in zip(descs, devs)]
+        per_scene = []
         t0 = time.perf_counter()
         for r, s in zip(one, spp):
+            t1 = time.perf_counter()
             eng.render([r], [s], use_graph=False)
+            per_scene.append(time.perf_counter() - t1)
         t_one = time.perf_counter() - t0
         bat = [pathtracer.SpectralRasterizer(ctx, d, scene=s) for d, s in zip(descs, devs)]
         t0 = time.perf_counter()
@@ -362,6 +370,22 @@ def bench_batch(ctx):
                     "batched_graph": {"seconds": t_bat, "msamples_s": total / t_bat / 1e6},
                     "speedup": t_one / t_bat, "speedup_vs_plain": t_plain / t_bat,
                     "films_equal_first6": bool(same)})
+        # Where the time goes: throughput of each resolution class rendered
+        # alone on the engine.  When the classes that hold most samples
+        # already run at the batch's rate alone, batching has only the small
+        # images' tails to remove.
+        by_res = {}
+        for p, sec in zip(params, per_scene):
+            c = by_res.setdefault(str(p["res"]), {"scenes": 0, "samples": 0, "seconds": 0.0})
+            c["scenes"] += 1
+            c["samples"] += p["res"] ** 2 * p["spp"]
+            c["seconds"] += sec
+        for c in by_res.values():
+            c["msamples_s_alone"] = c["samples"] / c["seconds"] / 1e6
+            c["share_of_samples"] = c["samples"] / total
+        big = by_res.get("1024", {})
+        out["limiter"] = {"one_by_one_by_resolution": by_res,
+                          "batched_over_1024_alone": (total / t_bat / 1e6) / big["msamples_s_alone"] if big else None}
         for r in one + bat + plain:
             r.close()
         # Small requests (the same 48 scenes at 128x128, 16 spp): the plain
@@ -393,15 +417,17 @@ def bench_batch(ctx):
     return out
 
 
-def bench_serving(ctx, rate=20.0, duration=8.0, resolutions=(128, 256)):
+def bench_serving(ctx, rate=20.0, duration=8.0, resolutions=(128, 256), n_scenes=12, max_tri=300_000,
+                  layout="q8", timeout=600.0):
     """Serving loop: Poisson arrivals, progressive 16 -> 64 -> 256 spp per
     request, scenes drawn from a resident pool of the batched-scenes
-    distribution (resolutions limited to `resolutions` so a run fits in the
-    bench); continuous batching vs one request at a time."""
+    distribution (`n_scenes` scenes of up to `max_tri` triangles at
+    `resolutions`); continuous batching vs one request at a time on the same
+    engine and kernels."""
     from rise_b200 import pathtracer, scenes, serving
-    params = scenes.batch_scene_params(n=12, seed=5, max_tri=300_000, resolutions=resolutions)
+    params = scenes.batch_scene_params(n=n_scenes, seed=5, max_tri=max_tri, resolutions=resolutions)
     descs = [scenes.batch_scene(p) for p in params]
-    devs = [pathtracer.upload_scene(ctx, d) for d in descs]
+    devs = [pathtracer.upload_scene(ctx, d, layout) for d in descs]
     pool = list(zip(descs, devs))
     arrivals = serving.poisson_arrivals(rate, duration, seed=9)
 
@@ -413,17 +439,87 @@ def bench_serving(ctx, rate=20.0, duration=8.0, resolutions=(128, 256)):
             st = scenes.RenderSettings(**{**descs[k].settings.__dict__, "seed": 1000 + i})
             reqs.append(serving.Request(i, t, k, st))
         return reqs
-    out = {"workload": f"Poisson {rate}/s for {duration}s, progressive 16/64/256 spp, 12 resident scenes "
-                       f"(triangles 10k-300k, resolutions {list(resolutions)}, depth 8-16)",
-           "requests": len(arrivals)}
+    out = {"workload": f"Poisson {rate}/s for {duration}s, progressive 16/64/256 spp, {n_scenes} resident scenes "
+                       f"(triangles 10k-{max_tri // 1000}k, resolutions {list(resolutions)}, depth 8-16, "
+                       f"{layout} BVHs)", "requests": len(arrivals)}
     try:
         # Warm-up: first launches of every kernel instantiation serving uses.
         serving.serve(ctx, pool, make(arrivals[:12]), mode="continuous")
-        out["continuous"] = serving.serve(ctx, pool, make(), mode="continuous")
-        out["fifo"] = serving.serve(ctx, pool, make(), mode="fifo")
+        out["continuous"] = serving.serve(ctx, pool, make(), mode="continuous", timeout=timeout)
+        out["fifo"] = serving.serve(ctx, pool, make(), mode="fifo", timeout=timeout)
     finally:
         for s in devs:
             s.close()
+    return out
+
+
+def bench_serving_cpu(ctx, n_requests=6, rate=0.2, seed=13):
+    """The serving comparison against the reference renderer, on a stated
+    subset of the request stream: 6 requests (Poisson, 0.2/s) over 4
+    resident scenes of the batched distribution restricted to 128 x 128
+    pixels and 10k-60k triangles, each asking for 16, then 64, then 256 spp.
+    The reference renders them one at a time on all host cores (its own
+    per-pixel integrator through oracle.RefRenderer, pixels in parallel; the
+    scenes written in its scene language and loaded before the stream
+    starts); the device serves the same requests (same scenes, arrival
+    times) continuously and one at a time.  Reported: p50 / p99 latency per
+    level on each arm and the ratio of the reference's p99 to the device's."""
+    import shutil
+    import tempfile
+    import oracle
+    from oracle.scene_writer import write_risescene
+    from rise_b200 import pathtracer, scenes, serving
+    if oracle.rise_ref() is None:
+        return {"unavailable": "the reference renderer (oracle/_ref/librise_ref.so) is not built"}
+    params = scenes.batch_scene_params(n=4, seed=17, max_tri=60_000, resolutions=(128,))
+    descs = [scenes.batch_scene(p) for p in params]
+    rng = np.random.default_rng(seed)
+    times = np.cumsum(rng.exponential(1.0 / rate, n_requests))
+    picks = rng.integers(len(descs), size=n_requests)
+    levels = (16, 64, 256)
+    tmp = tempfile.mkdtemp(prefix="rise_serving_")
+    out = {"subset": f"{n_requests} requests, Poisson {rate}/s, 4 resident scenes of the batched distribution "
+                     f"at 128x128 with {min(p['n_tri'] for p in params) // 1000}k-"
+                     f"{max(p['n_tri'] for p in params) // 1000}k triangles, levels 16/64/256 spp",
+           "cpu_threads": oracle.RISE_THREADS}
+    try:
+        refs = [oracle.RefRenderer(write_risescene(d, tmp, f"s{i}", spp=16)) for i, d in enumerate(descs)]
+        lat = {lv: [] for lv in levels}
+        t0 = time.perf_counter()
+        for i, (t, k) in enumerate(zip(times, picks)):
+            now = time.perf_counter() - t0
+            if now < t:
+                time.sleep(t - now)
+            done = 0
+            for lv in levels:
+                refs[k].integrate(lv - done, batch=1000 * i + lv)
+                done = lv
+                lat[lv].append(time.perf_counter() - t0 - t)
+        wall = time.perf_counter() - t0
+        for r in refs:
+            r.close()
+        samples = sum(256 * 128 * 128 for _ in picks)
+        out["cpu_reference"] = {"wall_s": wall, "msamples_s": samples / wall / 1e6, "latency": {
+            str(lv): {"p50_s": float(np.percentile(v, 50)), "p99_s": float(np.percentile(v, 99))}
+            for lv, v in lat.items()}}
+    finally:
+        shutil.rmtree(tmp, ignore_errors=True)
+    devs = [pathtracer.upload_scene(ctx, d, "q8") for d in descs]
+    try:
+        pool = list(zip(descs, devs))
+
+        def make():
+            return [serving.Request(i, float(t), int(k), scenes.RenderSettings(
+                **{**descs[int(k)].settings.__dict__, "seed": 1000 + i})) for i, (t, k) in enumerate(zip(times, picks))]
+        serving.serve(ctx, pool, make()[:2], mode="continuous")   # warm-up
+        for mode in ("continuous", "fifo"):
+            out["gpu_" + mode] = serving.serve(ctx, pool, make(), mode=mode)
+    finally:
+        for d in devs:
+            d.close()
+    out["p99_ratio_cpu_over_gpu"] = {
+        mode: {lv: out["cpu_reference"]["latency"][lv]["p99_s"] / out["gpu_" + mode]["latency"][lv]["p99_s"]
+               for lv in out["cpu_reference"]["latency"]} for mode in ("continuous", "fifo")}
     return out
 
 
@@ -469,6 +565,14 @@ def main():
 
     rank, world, local = dist_info()
     torch.cuda.set_device(local)
+    if args.serving_full:
+        ctx = raycaster.Context(local, 120 * 10**9)
+        res = bench_serving(ctx, rate=20.0, duration=60.0, resolutions=scenes.RESOLUTIONS, n_scenes=48,
+                            max_tri=1_000_000, timeout=3600.0)
+        res["budget_bytes"] = 120 * 10**9
+        print(json.dumps({"serving_full": res}))
+        ctx.close()
+        return
     if args.pt_only or args.large_only:
         ctx = raycaster.Context(local)
         print(json.dumps(bench_large_scene(ctx) if args.large_only else bench_path_tracer(ctx, rank, cpu_baseline=False)))
@@ -489,7 +593,10 @@ def main():
     sq = raycaster.Scene(ctx)
     sq.add_triangles(tri)
     sq.commit("q8")
-    rf, rq = raycaster.RayCaster(sf), raycaster.RayCaster(sq)
+    sh16 = raycaster.Scene(ctx)
+    sh16.add_triangles(tri)
+    sh16.commit("f16")
+    rf, rq, rh = raycaster.RayCaster(sf), raycaster.RayCaster(sq), raycaster.RayCaster(sh16)
 
     stream = torch.cuda.current_stream()
     sh = stream.cuda_stream
@@ -546,7 +653,8 @@ def main():
         return a.elapsed_time(b) / n
 
     variants = {}
-    for name, fn, rc in (("closest_f32", step_closest, rf), ("any_f32", step_any, rf), ("any_q8", step_any, rq)):
+    for name, fn, rc in (("closest_f32", step_closest, rf), ("any_f32", step_any, rf), ("any_q8", step_any, rq),
+                         ("closest_f16", step_closest, rh), ("any_f16", step_any, rh)):
         variants[name] = N_RAYS / (timed(fn, rc) * 1e-3) / 1e6
     hit_rate = float((d_hits[:, 1].view(torch.int32) >= 0).float().mean())
 
@@ -608,6 +716,7 @@ def main():
                                "sample": f"first {n} rays of the {N_RAYS}-ray set, closest-hit, BVH build excluded"}
     sf.close()
     sq.close()
+    sh16.close()
     if not args.no_path_tracer:
         out["path_tracer"] = bench_path_tracer(ctx, rank, cpu_baseline=world == 1 and not args.no_cpu_baseline)
         # The headline path-tracing metric: Msamples/s at relMSE <= 1e-3
@@ -619,6 +728,8 @@ def main():
         if not args.no_batch:
             out["batch"] = bench_batch(ctx)
             out["serving"] = bench_serving(ctx)
+            if world == 1 and not args.no_cpu_baseline:
+                out["serving_vs_reference"] = bench_serving_cpu(ctx)
     ctx.close()
     if world > 1:
         dist.barrier()

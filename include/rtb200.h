@@ -50,6 +50,7 @@ extern "C" {
 #define RTB200_BVH_F32     0  /* FP32 child boxes, 128-byte 4-wide nodes */
 #define RTB200_BVH_Q8      1  /* 8-bit conservative child boxes, 64-byte nodes */
 #define RTB200_BVH_W8      2  /* 8-wide nodes with 8-bit conservative child boxes, 80 bytes */
+#define RTB200_BVH_F16     3  /* binary16 child boxes rounded outward, 64-byte nodes */
 
 typedef struct rtb200_ctx rtb200_ctx;
 typedef struct rtb200_scene rtb200_scene;
@@ -175,11 +176,15 @@ typedef struct {
     int32_t reflectance;  /* spectrum id: Lambertian albedo (-1 = black) */
     int32_t emission;     /* spectrum id of emitted radiance (-1 = none);
                              LambertianEmitter: one-sided, radiance = spectrum */
-    int32_t eta, kappa;   /* GGX conductor spectra (-1 = unused) */
+    int32_t eta, kappa;   /* GGX conductor spectra (-1 = unused); for a dielectric,
+                             eta >= 0 names a spectrum holding its index of
+                             refraction per wavelength (a dispersive IOR: the
+                             reference's `ior` scalar painter evaluated by
+                             IScalarPainter::GetValueAtNM), else `ior` holds */
     float alpha;          /* GGX roughness; for a dielectric, the Phong exponent of
                              its transmitted lobe (the reference's `scattering`,
                              DielectricSPF.cpp:248-272; 0 or >= 1e6: smooth) */
-    float ior;            /* dielectric index of refraction */
+    float ior;            /* dielectric index of refraction (constant) */
 } rtb200_material;
 
 /* Returns the new spectrum / material id in *id_out.  Materials are
@@ -265,7 +270,29 @@ typedef struct {
      * the number of path vertices (the reference's default is 128). */
     int32_t bounce_limits;
     int32_t max_diffuse_bounce, max_glossy_bounce, max_transmission_bounce;
+    /* Wavelength sampling (SpectralConfig, Utilities/SpectralConfig.h;
+     * PathTracingSpectralRasterizer::IntegratePixelSpectral,
+     * Rendering/PathTracingSpectralRasterizer.cpp:121-198).
+     * RTB200_SPECTRAL_HWSS: four wavelengths per path, a quarter of the range
+     * apart (the reference's `hwss true`).  At a dielectric whose index of
+     * refraction differs between the hero and a companion wavelength, the
+     * companions end and the hero continues alone, its sample counted as one
+     * wavelength (SampledWavelengths::TerminateSecondary; the reference instead
+     * continues each wavelength on its own single-wavelength path from there,
+     * PathTracingIntegrator.cpp:4336-4365 — the same expectation).
+     * RTB200_SPECTRAL_SINGLE: one wavelength per path (the reference's default,
+     * `hwss false`: IntegrateRayNM), lambda_min + floor(u * num_wavelengths) *
+     * (lambda_max - lambda_min) / num_wavelengths when 0 < num_wavelengths <
+     * 10000, else uniform in the range.  spectral_samples (0 = 1) paths are
+     * traced per pixel sample and averaged (nSpectralSamples); each draws its
+     * own position in the pixel.  Adaptive sampling needs spectral_samples 1. */
+    int32_t spectral_mode;
+    int32_t num_wavelengths;
+    int32_t spectral_samples;
 } rtb200_render_settings;
+
+#define RTB200_SPECTRAL_HWSS 0
+#define RTB200_SPECTRAL_SINGLE 1
 
 /* Random numbers of the path decisions.  HASH: a counter-based hash of
  * (seed, pixel, sample, dimension) with a fixed dimension layout.  SOBOL: the

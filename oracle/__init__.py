@@ -221,7 +221,9 @@ def pt_render(desc, spp, sample_begin=0, crop=None, threads=None, settings=None,
                      getattr(st, "filter_sigma", 0.5), getattr(st, "adaptive_threshold", 0.01)], np.float64)
     seti = np.array([st.width, st.height, st.max_depth, st.rr_min_depth, st.nee_per_lambda, st.seed,
                      getattr(st, "filter", 0), getattr(st, "adaptive_max_spp", 0),
-                     getattr(st, "light_selection", 0), getattr(st, "sampler", 0)] + list(_bounce_limits(st)), np.int32)
+                     getattr(st, "light_selection", 0), getattr(st, "sampler", 0)] + list(_bounce_limits(st)) +
+                    [getattr(st, "spectral_mode", 0), getattr(st, "num_wavelengths", 0),
+                     getattr(st, "spectral_samples", 1)], np.int32)
     out = np.zeros((y1 - y0, x1 - x0, 3), np.float64)
     counts = np.zeros((y1 - y0, x1 - x0), np.int32)
     cie = np.ascontiguousarray(cie_table())

@@ -72,10 +72,16 @@ int  orc_ray_triangle(const double* o, const double* d, const double* v0, const 
  *   points: n_point x 7 doubles (position, colour, power) of point lights
  *   nrm9:   n_tri x 9 floats, the vertex normals of each triangle's corners
  *           (all zero: a flat triangle), or null
- *   seti:   14 int32 (width, height, max_depth, rr_min_depth, nee_per_lambda, seed, filter,
+ *   seti:   17 int32 (width, height, max_depth, rr_min_depth, nee_per_lambda, seed, filter,
  *           adaptive maximum samples per pixel or 0, light selection: 0 light BVH, 1 power,
- *           sampler: 0 hash, 1 Owen-scrambled Sobol, bounce limits on, maximum diffuse,
- *           glossy and transmission bounces)
+ *           sampler: 0 hash, 1 Owen-scrambled Sobol, 2 the same with shuffled indices,
+ *           bounce limits on, maximum diffuse, glossy and transmission bounces,
+ *           spectral mode: 0 hero + 3 companions, 1 one wavelength per path,
+ *           wavelength bins of the single mode (0 = continuous), spectral samples
+ *           per pixel sample)
+ * A dielectric whose eta (mats_i column 3) names a spectrum refracts with that
+ * index per wavelength; where the hero's and a companion's differ, the
+ * companions end and the hero continues alone.
  * filter 0 is the box film (mean of the pixel's own samples); filter 1 is the
  * Gaussian pixel filter: with size / 2 > 0.501 the samples of every pixel
  * within the support are splatted and a pixel is sum(w XYZ) / sum(w); a

@@ -553,6 +553,10 @@ struct Scene {
     int width, height, maxDepth, rrMinDepth, neePerLambda;
     int sampler = 0;                       // 0 hash, 1 Sobol, 2 Sobol with shuffled indices
     int maxBounce[3] = {255, 255, 255};    // diffuse, glossy, transmission
+    int single = 0;                        // one wavelength per path (IntegrateRayNM)
+    int numWl = 0;                         // single: wavelength bins (0 = continuous)
+    double wlStep = 0.0;                   // single: (lmax - lmin) / numWl
+    int spectral = 1;                      // paths per pixel sample (nSpectralSamples)
     uint32_t seed;
     bool lightBvh = false;                 // luminaries picked with the light BVH
     std::vector<LightNode> lightNodes;
@@ -786,8 +790,18 @@ void Sample(const Scene& S, uint32_t pixel, uint32_t sample, double xyz[3])
     const double sx = 2.0 * fx / S.width - 1.0, sy = 1.0 - 2.0 * fy / S.height;
     V d = Norm(S.fwd + S.right * sx + S.up * sy);
     V o = S.pos;
+    // The hero of an equidistant bundle, or one wavelength, binned as the
+    // reference's single-wavelength loop bins it
+    // (PathTracingSpectralRasterizer.cpp:180-183); the companions of a
+    // single-wavelength path start terminated.  The bin index is taken in
+    // FP32 as the device takes it.
     double lam[4];
-    Wavelengths(CameraRand(S, key, sample, 2), S.lmin, S.lmax, lam);
+    const double uw = CameraRand(S, key, sample, 2);
+    Wavelengths(uw, S.lmin, S.lmax, lam);
+    if (S.single && S.numWl)
+        lam[0] = S.lmin + std::min((int)((float)uw * (float)S.numWl), S.numWl - 1) * S.wlStep;
+    unsigned term = S.single ? 0xeu : 0u;
+    auto live = [&](int k) { return !((term >> k) & 1u); };
     double thr[4] = {1, 1, 1, 1}, L[4] = {0, 0, 0, 0};
     double bsdfPdf = 0.0;
     int bounces[3] = {0, 0, 0};
@@ -803,7 +817,8 @@ void Sample(const Scene& S, uint32_t pixel, uint32_t sample, double xyz[3])
         if (prim < 0) {
             if (S.env >= 0 && (depth > 0 || S.envVisible)) {
                 const double w = bsdfPdf > 0 ? PowerHeuristic(bsdfPdf, kInv4Pi) : 1.0;
-                for (int k = 0; k < 4; ++k) L[k] += thr[k] * Spec(S, S.env, lam[k]) * w;
+                for (int k = 0; k < 4; ++k)
+                    if (live(k)) L[k] += thr[k] * Spec(S, S.env, lam[k]) * w;
             }
             break;
         }
@@ -844,16 +859,26 @@ void Sample(const Scene& S, uint32_t pixel, uint32_t sample, double xyz[3])
                 const double psel = S.lightBvh ? LightBvhPdf(S.lightNodes, lg.bvhPos, po) : lg.pdf;
                 if (cosL > 0 && lg.area > 0) w = PowerHeuristic(bsdfPdf, psel * t * t / (lg.area * cosL));
             }
-            for (int k = 0; k < 4; ++k) L[k] += thr[k] * Spec(S, emit, lam[k]) * w;
+            for (int k = 0; k < 4; ++k)
+                if (live(k)) L[k] += thr[k] * Spec(S, emit, lam[k]) * w;
         }
         double kray[4] = {0, 0, 0, 0};
         V nd;
         double npdf = 0.0;
         int btype = 0;   // continuation: 0 diffuse, 1 glossy, 2 transmission
         if (type == 2) {
-            // Smooth dielectric (DielectricSPF.cpp:120-300); constant index:
-            // the wavelength bundle continues together.
-            const double ior = S.mf[2 * mat + 1];
+            // Smooth dielectric (DielectricSPF.cpp:120-300) at the hero's
+            // index; a constant index keeps the bundle together, a companion
+            // whose index differs by more than 1e-8 ends with the others
+            // (TerminateSecondary, PathTracingIntegrator.cpp:4658-4677).
+            const int iorSpec = S.mi[5 * mat + 3];
+            const double ior = iorSpec >= 0 ? Spec(S, iorSpec, lam[0]) : (double)S.mf[2 * mat + 1];
+            if (iorSpec >= 0 && (term & 0xeu) != 0xeu)
+                for (int k = 1; k < 4; ++k)
+                    if (live(k) && std::fabs(Spec(S, iorSpec, lam[k]) - ior) > 1e-8) {
+                        term |= 0xeu;
+                        break;
+                    }
             const bool entering = Dot(d, ns0) < 0;
             const V nn = entering ? ns0 : -ns0;
             const double n1 = entering ? 1.0 : ior, n2 = entering ? ior : 1.0;
@@ -901,11 +926,12 @@ void Sample(const Scene& S, uint32_t pixel, uint32_t sample, double xyz[3])
                 nd = rdir;
                 btype = 1;
             }
-            for (double& k : kray) k = 1.0;
+            for (int k = 0; k < 4; ++k) kray[k] = live(k) ? 1.0 : 0.0;
         } else {
             const V ns = nsv, r = -d;
             const int nsamp = S.neePerLambda ? 4 : 1;
             for (int k = 0; k < nsamp; ++k) {
+                if (S.neePerLambda && !live(k)) continue;
                 if (!S.lights.empty()) {
                     const double ul = rng.next(4 * k);
                     int li = 0;
@@ -932,7 +958,7 @@ void Sample(const Scene& S, uint32_t pixel, uint32_t sample, double xyz[3])
                         const double pd[3] = {p.x, p.y, p.z}, ld[3] = {toL.x, toL.y, toL.z};
                         if (cosS > 0 && !orc_any_d(S.bvh, pd, ld, dist - 0.001)) {
                             for (int j = 0; j < 4; ++j) {
-                                if (S.neePerLambda && j != k) continue;
+                                if ((S.neePerLambda && j != k) || !live(j)) continue;
                                 double f, pb;
                                 EvalBsdf(S, mat, lam[j], ns, gnv, r, toL, f, pb);
                                 L[j] += thr[j] * lg.le * f * cosS / (dist * dist) / psel;
@@ -961,7 +987,7 @@ void Sample(const Scene& S, uint32_t pixel, uint32_t sample, double xyz[3])
                             const double geom = lg.area * cosL / (dist * dist);
                             const double plight = psel * dist * dist / (lg.area * cosL);
                             for (int j = 0; j < 4; ++j) {
-                                if (S.neePerLambda && j != k) continue;
+                                if ((S.neePerLambda && j != k) || !live(j)) continue;
                                 double f, pb;
                                 EvalBsdf(S, mat, lam[j], ns, gnv, r, toL, f, pb);
                                 const double w = (pb > 0 ? PowerHeuristic(plight, pb) : 1.0) / psel;
@@ -983,7 +1009,7 @@ void Sample(const Scene& S, uint32_t pixel, uint32_t sample, double xyz[3])
                     const double pd[3] = {p.x, p.y, p.z}, ed[3] = {dir.x, dir.y, dir.z};
                     if (cosE > 0 && !orc_any_d(S.bvh, pd, ed, 1e300)) {
                         for (int j = 0; j < 4; ++j) {
-                            if (S.neePerLambda && j != k) continue;
+                            if ((S.neePerLambda && j != k) || !live(j)) continue;
                             double f, pb;
                             EvalBsdf(S, mat, lam[j], ns, gnv, r, dir, f, pb);
                             const double w = pb > 0 ? PowerHeuristic(kInv4Pi, pb) : 1.0;
@@ -1039,20 +1065,22 @@ void Sample(const Scene& S, uint32_t pixel, uint32_t sample, double xyz[3])
                     khero = fms * cosO / (mpdf * pMS);
                 }
                 if (!(npdf > 0)) break;
-                kray[0] = khero;
+                kray[0] = live(0) ? khero : 0.0;
                 const double cosV = std::fabs(Dot(nd, ns));
-                for (int k = 1; k < 4; ++k) kray[k] = GgxValue(GgxAt(S, mat, lam[k]), w, gnv, r, nd) * cosV / npdf;
+                for (int k = 1; k < 4; ++k)
+                    kray[k] = live(k) ? GgxValue(GgxAt(S, mat, lam[k]), w, gnv, r, nd) * cosV / npdf : 0.0;
             } else {
                 const double phi = 2.0 * kPi * u1, sint = std::sqrt(u2), cost = std::sqrt(1.0 - u2);
                 nd = Norm(tx * (std::cos(phi) * sint) + ty * (std::sin(phi) * sint) + w * cost);
                 npdf = std::fabs(Dot(nd, w)) * kInvPi;
                 if (!(Dot(nd, gn) > 0)) break;
-                for (int k = 0; k < 4; ++k) kray[k] = Spec(S, refl, lam[k]);
+                for (int k = 0; k < 4; ++k) kray[k] = live(k) ? Spec(S, refl, lam[k]) : 0.0;
             }
         }
         if (type != 2) rng.skip(1);   // the integrator's choice among the scattered rays (a dielectric's is its Fresnel choice)
         double prevMax = 0, currMax = 0;
         for (int k = 0; k < 4; ++k) {
+            if (!live(k)) continue;
             prevMax = std::max(prevMax, std::fabs(thr[k]));
             currMax = std::max(currMax, std::fabs(thr[k] * kray[k]));
         }
@@ -1078,7 +1106,7 @@ void Sample(const Scene& S, uint32_t pixel, uint32_t sample, double xyz[3])
     for (int k = 0; k < 4; ++k) {
         int i, j;
         double wgt;
-        if (!Interp(lam[k], i, j, wgt)) continue;
+        if (!live(k) || !Interp(lam[k], i, j, wgt)) continue;
         for (int c = 0; c < 3; ++c) {
             const double* tab = S.cie + 81 * c;
             xyz[c] += (tab[i] + wgt * (tab[j] - tab[i])) * L[k];
@@ -1108,18 +1136,20 @@ struct Adaptive {
 // luminance (XYZ.Y), and after every batch, once 32 samples are in, the
 // convergence test -- standard error / |mean| below threshold * (1 - 4 / N),
 // or M2 < 1e-12 after 64 samples for a black pixel -- until it passes or
-// A.max_spp samples are taken.  emit(sample, xyz) sees every sample; the
-// return value is the number of samples taken.
+// A.max_spp samples are taken.  emit(path, xyz) sees every path (a pixel
+// sample is S.spectral paths, numbered sample * S.spectral + j); the return
+// value is the number of pixel samples taken.
 template <class F>
 int PixelSamples(const Scene& S, uint32_t pixel, int sample_begin, int spp, const Adaptive& A, F&& emit)
 {
     double v[3];
     if (A.max_spp <= 0) {
-        for (int s = 0; s < spp; ++s) {
-            const uint32_t sample = (uint32_t)(sample_begin + s);
-            Sample(S, pixel, sample, v);
-            emit(sample, v);
-        }
+        for (int s = 0; s < spp; ++s)
+            for (int j = 0; j < S.spectral; ++j) {
+                const uint32_t path = (uint32_t)((sample_begin + s) * S.spectral + j);
+                Sample(S, pixel, path, v);
+                emit(path, v);
+            }
         return spp;
     }
     double mean = 0.0, m2 = 0.0;
@@ -1338,12 +1368,16 @@ extern "C" int orc_pt_render(const float* tri9, int64_t n_tri, const int64_t* me
     S.sampler = seti[9];
     if (seti[10])
         for (int k = 0; k < 3; ++k) S.maxBounce[k] = std::min(seti[11 + k], 255);
+    S.single = seti[14] == 1;
+    S.numWl = seti[15] > 0 && seti[15] < 10000 ? seti[15] : 0;
+    S.spectral = std::max(1, (int)seti[16]);
     {
         const double lo = std::max(S.lmin, 380.0), hi = std::min(S.lmax, 780.0);
         const int f = (int)((lo - 380.0) / 5.0), l = (int)((hi - 380.0) / 5.0);
         double ky = 0.0;
         for (int i = f; i < l; ++i) ky += 0.5 * (cie[81 + i] + cie[81 + i + 1]) * 5.0;
         S.ynorm = ky > 0 ? (S.lmax - S.lmin) / ky : 0.0;
+        S.wlStep = S.numWl ? (float)((S.lmax - S.lmin) / S.numWl) : 0.0;
     }
     const V pos = {cam[0], cam[1], cam[2]}, look = {cam[3], cam[4], cam[5]}, upv = {cam[6], cam[7], cam[8]};
     const V f = Norm(look - pos);
@@ -1546,8 +1580,9 @@ extern "C" int orc_pt_render(const float* tri9, int64_t n_tri, const int64_t* me
             for (int x = 0; x < cw; ++x) {
                 const uint32_t pixel = (uint32_t)((y0 + row) * S.width + (x0 + x));
                 double acc[3] = {0, 0, 0};
+                const double inv = 1.0 / S.spectral;
                 const int n = PixelSamples(S, pixel, sample_begin, spp, A, [&](uint32_t, const double* v) {
-                    for (int c = 0; c < 3; ++c) acc[c] += v[c];
+                    for (int c = 0; c < 3; ++c) acc[c] += v[c] * inv;
                 });
                 for (int c = 0; c < 3; ++c) xyz[3 * ((size_t)row * cw + x) + c] = acc[c] / n;
                 if (counts) counts[(size_t)row * cw + x] = n;

@@ -14,7 +14,7 @@ OK = 0
 E_INVALID, E_OOM, E_BUDGET, E_TIMEOUT, E_DEVICE, E_NOT_READY = 1, 2, 3, 4, 5, 6
 STATUS_NAMES = {0: "OK", 1: "E_INVALID", 2: "E_OOM", 3: "E_BUDGET", 4: "E_TIMEOUT",
                 5: "E_DEVICE", 6: "E_NOT_READY"}
-BVH_F32, BVH_Q8, BVH_W8 = 0, 1, 2
+BVH_F32, BVH_Q8, BVH_W8, BVH_F16 = 0, 1, 2, 3
 
 _vp = ctypes.c_void_p
 _i64 = ctypes.c_int64

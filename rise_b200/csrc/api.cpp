@@ -388,7 +388,7 @@ int rtb200_scene_commit(rtb200_scene* s, int32_t layout)
     rtb200_ctx* ctx = s->ctx;
     std::lock_guard<std::mutex> g(ctx->mu);
     if (s->committed) return SetError(ctx, RTB200_E_INVALID, "scene already committed");
-    if (layout != RTB200_BVH_F32 && layout != RTB200_BVH_Q8 && layout != RTB200_BVH_W8)
+    if (layout != RTB200_BVH_F32 && layout != RTB200_BVH_Q8 && layout != RTB200_BVH_W8 && layout != RTB200_BVH_F16)
         return SetError(ctx, RTB200_E_INVALID, "unknown BVH layout");
     const int64_t n_tri = (int64_t)s->tri_material.size();
     if (n_tri == 0) return SetError(ctx, RTB200_E_INVALID, "scene has no triangles");
@@ -402,6 +402,7 @@ int rtb200_scene_commit(rtb200_scene* s, int32_t layout)
     std::vector<GpuTri> tris;
     std::vector<GpuNode4> nf;
     std::vector<QNode4> nq;
+    std::vector<HNode4> nh;
     std::vector<WNode8> nw;
     const void* nodes_src;
     size_t nodes_bytes;
@@ -427,6 +428,10 @@ int rtb200_scene_commit(rtb200_scene* s, int32_t layout)
         EncodeQuantNodes(s->bvh, nq);
         nodes_src = nq.data();
         nodes_bytes = nq.size() * sizeof(QNode4);
+    } else if (layout == RTB200_BVH_F16) {
+        EncodeHalfNodes(s->bvh, nh);
+        nodes_src = nh.data();
+        nodes_bytes = nh.size() * sizeof(HNode4);
     } else {
         EncodeGpuNodes(s->bvh, nf);
         nodes_src = nf.data();

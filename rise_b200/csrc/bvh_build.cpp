@@ -21,6 +21,7 @@
 #include <cmath>
 #include <cstring>
 #include <functional>
+#include <limits>
 #include <mutex>
 #include <thread>
 
@@ -596,6 +597,55 @@ void EncodeQuantNodes(const BuiltBVH& b, std::vector<QNode4>& out)
                 d.qlo[k][i] = (uint8_t)ql;
                 d.qhi[k][i] = (uint8_t)qh;
             }
+        }
+    }
+}
+
+float HalfToFloat(uint16_t h)
+{
+    const int sign = h >> 15, exp = (h >> 10) & 0x1f, man = h & 0x3ff;
+    float v;
+    if (exp == 0) v = std::ldexp((float)man, -24);                       // zero / subnormal
+    else if (exp == 31) v = man ? std::numeric_limits<float>::quiet_NaN() : std::numeric_limits<float>::infinity();
+    else v = std::ldexp((float)(man | 0x400), exp - 25);
+    return sign ? -v : v;
+}
+
+uint16_t FloatToHalfDirected(float x, int dir)
+{
+    // Non-negative halves order like their bit patterns; find the largest
+    // half <= |x| by binary search over 0x0000..0x7c00 (0 .. +inf).
+    const float a = std::fabs(x);
+    uint16_t lo = 0, hi = 0x7c00;
+    while (lo < hi) {
+        const uint16_t mid = (uint16_t)((lo + hi + 1) / 2);
+        if (HalfToFloat(mid) <= a) lo = mid; else hi = (uint16_t)(mid - 1);
+    }
+    uint16_t mag = lo;   // largest half <= |x|
+    const bool exact = HalfToFloat(mag) == a;
+    // Rounding |x| down moves a positive x down and a negative x up.
+    const bool wantDown = x >= 0.0f ? dir < 0 : dir > 0;
+    if (!exact && !wantDown) mag = (uint16_t)(mag + 1);   // next half up (0x7c00 = inf at the top)
+    return (uint16_t)((x < 0.0f ? 0x8000 : 0) | mag);
+}
+
+void EncodeHalfNodes(const BuiltBVH& b, std::vector<HNode4>& out)
+{
+    out.resize(b.nodes4.size());
+    const std::vector<int32_t> pos = BreadthFirstPositions(b);
+    for (size_t n = 0; n < b.nodes4.size(); ++n) {
+        const Node4& s = b.nodes4[n];
+        HNode4& d = out[pos[n]];
+        for (int i = 0; i < 4; ++i) {
+            const bool valid = i < s.nchild;
+            // An empty slot gets the empty box (lo = +inf, hi = -inf).
+            d.lox[i] = valid ? FloatToHalfDirected(s.minx[i], -1) : 0x7c00;
+            d.loy[i] = valid ? FloatToHalfDirected(s.miny[i], -1) : 0x7c00;
+            d.loz[i] = valid ? FloatToHalfDirected(s.minz[i], -1) : 0x7c00;
+            d.hix[i] = valid ? FloatToHalfDirected(s.maxx[i], +1) : 0xfc00;
+            d.hiy[i] = valid ? FloatToHalfDirected(s.maxy[i], +1) : 0xfc00;
+            d.hiz[i] = valid ? FloatToHalfDirected(s.maxz[i], +1) : 0xfc00;
+            d.child[i] = !valid ? INT32_MIN : Link(s, i, pos);
         }
     }
 }

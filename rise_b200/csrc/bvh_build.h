@@ -104,6 +104,23 @@ struct alignas(16) QNode4 {
 };
 static_assert(sizeof(QNode4) == 64, "QNode4 must be 64 bytes");
 
+// Half-precision wide node, 64 bytes: the FP32 node's child boxes as IEEE
+// binary16 (lower bounds rounded towards -inf, upper bounds towards +inf, so
+// each decoded box contains the FP32 box; coordinates beyond the half range
+// become -inf / +inf), the same links (kEmpty for an empty slot) and no
+// counts (leaves end at the triangle flagged last, as for GpuNode4).
+struct alignas(16) HNode4 {
+    uint16_t lox[4], loy[4], loz[4];
+    uint16_t hix[4], hiy[4], hiz[4];
+    int32_t child[4];
+};
+static_assert(sizeof(HNode4) == 64, "HNode4 must be 64 bytes");
+
+// binary16 <-> float on the host: the value of a half, and the half nearest
+// to x in the given direction (-1 down, +1 up), exactly.
+float HalfToFloat(uint16_t h);
+uint16_t FloatToHalfDirected(float x, int dir);
+
 // One triangle in leaf order: v0.w carries the input triangle index.
 struct alignas(16) GpuTri {
     float v0[4];
@@ -140,6 +157,7 @@ void EncodeWideTriangles(const float* tri9, const std::vector<uint32_t>& prims, 
 // the top levels, which every ray visits, share cache lines and pages.
 void EncodeGpuNodes(const BuiltBVH& b, std::vector<GpuNode4>& out);
 void EncodeQuantNodes(const BuiltBVH& b, std::vector<QNode4>& out);
+void EncodeHalfNodes(const BuiltBVH& b, std::vector<HNode4>& out);
 void EncodeTriangles(const float* tri9, const BuiltBVH& b, std::vector<GpuTri>& out);
 
 // Upper bound on the traversal stack depth of the BVH4: the largest sum of

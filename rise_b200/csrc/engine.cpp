@@ -84,6 +84,7 @@ struct rtb200_job {
     int n_active = 0;                  // pixels the next request samples
     int submitted_px = 0;              // pixels the request in flight samples
     long long spp_done = 0;
+    int spectral = 1;                  // paths per pixel sample (spectral samples)
     long long samples = 0;
     double seconds = 0.0;
     long long segments = 0, shadow_rays = 0;
@@ -271,8 +272,10 @@ int EngineSubmit(rtb200_engine* e, rtb200_job* j, int spp)
     d.px_list = j->adaptive ? j->px_list[j->cur] : nullptr;
     d.lum = j->adaptive ? j->lum : nullptr;
     d.film = j->pass;
-    d.sample_begin = (unsigned long long)j->spp_done;
-    d.total = (unsigned long long)npx * (unsigned long long)spp;
+    // Paths are counted per spectral sample: pixel sample s of a pixel is
+    // paths s * spectral .. s * spectral + spectral - 1.
+    d.sample_begin = (unsigned long long)j->spp_done * (unsigned long long)j->spectral;
+    d.total = (unsigned long long)npx * (unsigned long long)spp * (unsigned long long)j->spectral;
     j->submitted_px = npx;
     d.sample_ctr = e->d_ctr + entry;
     d.done_ctr = e->d_ctr + kMaxJobs + entry;
@@ -487,7 +490,7 @@ int rtb200_job_create(rtb200_scene* s, const rtb200_render_settings* rs, rtb200_
     if (!s->committed || s->materials.empty())
         return SetError(ctx, RTB200_E_INVALID, "scene must be committed with materials");
     if (s->layout == RTB200_BVH_W8)
-        return SetError(ctx, RTB200_E_INVALID, "the path tracer runs on the F32 and Q8 BVH layouts");
+        return SetError(ctx, RTB200_E_INVALID, "the path tracer runs on the four-wide BVH layouts (F32, Q8, F16)");
     if (rs->width <= 0 || rs->height <= 0 || (int64_t)rs->width * rs->height > (1ll << 28) || rs->max_depth < 1 ||
         rs->max_depth > 255 || !(rs->lambda_max > rs->lambda_min) || rs->lambda_min < 380.0f ||
         rs->lambda_max > 780.0f || !(rs->fov_deg > 0.0f && rs->fov_deg < 180.0f))
@@ -506,6 +509,11 @@ int rtb200_job_create(rtb200_scene* s, const rtb200_render_settings* rs, rtb200_
     if (rs->bounce_limits && (rs->max_diffuse_bounce < 0 || rs->max_glossy_bounce < 0 ||
                               rs->max_transmission_bounce < 0))
         return SetError(ctx, RTB200_E_INVALID, "bad bounce limits");
+    if ((rs->spectral_mode != RTB200_SPECTRAL_HWSS && rs->spectral_mode != RTB200_SPECTRAL_SINGLE) ||
+        rs->num_wavelengths < 0 || rs->spectral_samples < 0 || rs->spectral_samples > 256)
+        return SetError(ctx, RTB200_E_INVALID, "bad spectral settings");
+    if (rs->spectral_samples > 1 && rs->adaptive_max_spp > 0)
+        return SetError(ctx, RTB200_E_INVALID, "adaptive sampling needs one spectral sample per pixel sample");
     // Camera frame (pinhole; vertical field of view).
     const float* P = rs->cam_pos;
     double f[3] = {rs->cam_look[0] - P[0], rs->cam_look[1] - P[1], rs->cam_look[2] - P[2]};
@@ -557,6 +565,11 @@ int rtb200_job_create(rtb200_scene* s, const rtb200_render_settings* rs, rtb200_
         const int32_t lim[3] = {rs->max_diffuse_bounce, rs->max_glossy_bounce, rs->max_transmission_bounce};
         for (int k = 0; k < 3; ++k) st.max_bounce[k] = rs->bounce_limits ? std::min(lim[k], 255) : 255;
     }
+    st.single = rs->spectral_mode == RTB200_SPECTRAL_SINGLE ? 1 : 0;
+    st.num_wl = rs->num_wavelengths > 0 && rs->num_wavelengths < 10000 ? rs->num_wavelengths : 0;
+    st.wl_step = st.num_wl ? (float)(((double)rs->lambda_max - rs->lambda_min) / st.num_wl) : 0.0f;
+    j->spectral = std::max(1, (int)rs->spectral_samples);
+    st.inv_spectral = 1.0f / (float)j->spectral;
     const bool gauss = rs->filter == RTB200_FILTER_GAUSSIAN;
     st.filter = !gauss ? kFilterBox : (0.5 * rs->filter_size > 0.501 ? kFilterSplat : kFilterWarp);
     st.filt_half = gauss ? 0.5f * rs->filter_size : 0.5f;

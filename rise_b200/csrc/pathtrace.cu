@@ -113,7 +113,9 @@ __device__ float LightBvhPdf(const PtLightNode* __restrict__ nodes, int pos, V3 
 
 // XYZ of one finished sample: sum over active wavelengths of
 // XYZ(lambda_i) * L_i, scaled by (lmax - lmin) / k_y / active
-// (PathTracingSpectralRasterizer.cpp:141-174).
+// (PathTracingSpectralRasterizer.cpp:141-198); a pixel sample of several
+// spectral samples is their mean (1 / nSpectralSamples on the mean films; the
+// filtered film's weights normalise it by themselves).
 __device__ __forceinline__ void Splat(const PtPaths& P, const PtJobDev& J, int slot, uint4 m)
 {
     const PtSettings& S = J.set;
@@ -134,7 +136,7 @@ __device__ __forceinline__ void Splat(const PtPaths& P, const PtJobDev& J, int s
         }
     }
     if (active == 0) return;
-    const float s = S.ynorm / (float)active;
+    const float s = S.ynorm / (float)active * (S.filter == kFilterSplat ? 1.0f : S.inv_spectral);
     if (J.lum && Y != 0.0f) {
         // Adaptive sampling: the pixel's luminance sums for its convergence test.
         const double y = (double)(Y * s);
@@ -345,14 +347,23 @@ KRegen(const PtJobDev* __restrict__ jobs, PtPaths P, PtQueues Q, int assign)
                 const V3 d = normalize(mk(J.cam.fwd[0] + sx * J.cam.right[0] + sy * J.cam.up[0],
                                           J.cam.fwd[1] + sx * J.cam.right[1] + sy * J.cam.up[1],
                                           J.cam.fwd[2] + sx * J.cam.right[2] + sy * J.cam.up[2]));
-                const float hero = J.set.lmin + (sobol ? SobolSample(sample, 2, key, shuf) : Rand(key, 2)) *
-                                                    (J.set.lmax - J.set.lmin);
+                // Wavelength: the hero of an equidistant bundle, or one
+                // wavelength, binned as the reference's single-wavelength loop
+                // bins it (lambda_begin + int(u * n) * step,
+                // PathTracingSpectralRasterizer.cpp:180-183); the companions of a
+                // single-wavelength path start terminated.
+                const float uw = sobol ? SobolSample(sample, 2, key, shuf) : Rand(key, 2);
+                const float hero = J.set.num_wl && J.set.single
+                                       ? J.set.lmin + (float)min((int)(uw * (float)J.set.num_wl), J.set.num_wl - 1) *
+                                                          J.set.wl_step
+                                       : J.set.lmin + uw * (J.set.lmax - J.set.lmin);
                 P.ray_o[slot] = make_float4(J.cam.pos[0], J.cam.pos[1], J.cam.pos[2], 0.0f);
                 P.ray_d[slot] = make_float4(d.x, d.y, d.z, __int_as_float(0x7f800000));
                 P.thr[slot] = make_float4(1.0f, 1.0f, 1.0f, 1.0f);
                 P.L[slot] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
                 P.aux[slot] = make_float4(hero, 0.0f, __int_as_float(jid), 0.0f);
-                P.meta[slot] = make_uint4(pixel, sample, kFlagConsiderEmission, key);
+                P.meta[slot] = make_uint4(pixel, sample,
+                                          kFlagConsiderEmission | (J.set.single ? (0xeu << kTermShift) : 0u), key);
                 got = true;
             }
         }
@@ -547,7 +558,7 @@ KShade(const PtJobDev* __restrict__ jobs, PtPaths P, PtQueues Q, int from_class)
         // Random numbers: hash key or Sobol seed in meta.w, sample index in meta.y.
         VertexRng rng{m.w, m.y, depth, set.sampler, 0u};
         const float bsdfPdf = aux.y;
-        const unsigned term = (m.z >> kTermShift) & 0xfu;
+        unsigned term = (m.z >> kTermShift) & 0xfu;
         float lam[4];
         Wavelengths(aux.x, set.lmin, set.lmax, lam);
         const V3 d = xyz(rd);
@@ -630,12 +641,27 @@ KShade(const PtJobDev* __restrict__ jobs, PtPaths P, PtQueues Q, int from_class)
 
             if (mtype == kMatDielectric) {
                 // Smooth dielectric: Fresnel choice between reflection and
-                // refraction (DielectricSPF.cpp:120-300).  With a constant index
-                // every wavelength follows the hero's direction with the same
-                // weight, so the bundle continues together.
+                // refraction (DielectricSPF.cpp:120-300) at the hero's index.
+                // With a constant index every wavelength follows the hero's
+                // direction with the same weight, so the bundle continues
+                // together; where a companion's index differs from the hero's
+                // (by more than 1e-8, GetSpecularInfoNM), the companions end
+                // and the hero goes on alone (TerminateSecondary,
+                // PathTracingIntegrator.cpp:4658-4677).
+                const float ior = M.eta >= 0 ? Spec(S.spectra, M.eta, lam[0]) : M.ior;
+                if (M.eta >= 0 && (term & 0xeu) != 0xeu) {
+                    #pragma unroll 1
+                    for (int k = 1; k < 4; ++k) {
+                        if (!(term & (1u << k)) && fabsf(Spec(S.spectra, M.eta, lam[k]) - ior) > 1e-8f) {
+                            term |= 0xeu;
+                            m.z |= 0xeu << kTermShift;
+                            break;
+                        }
+                    }
+                }
                 const bool entering = dot(d, ns0) < 0.0f;
                 const V3 nn = entering ? ns0 : -ns0;
-                const float n1 = entering ? 1.0f : M.ior, n2 = entering ? M.ior : 1.0f;
+                const float n1 = entering ? 1.0f : ior, n2 = entering ? ior : 1.0f;
                 const float cosI = -dot(d, nn);
                 const float eta = n1 / n2;
                 const float s2t = eta * eta * fmaxf(0.0f, 1.0f - cosI * cosI);
@@ -1107,6 +1133,7 @@ cudaError_t PtIteration(const PtLaunch& L, int iter, cudaStream_t st)
     KRegen<<<shadeGrid, kShadeBlock, 0, st>>>(L.jobs, L.paths, L.queues, 1);
     cudaMemsetAsync(L.queues.trace_ctr, 0, 2 * sizeof(unsigned long long), st);
     if (L.layout == RTB200_BVH_Q8) LaunchTrace<QNode4>(L, st, true);
+    else if (L.layout == RTB200_BVH_F16) LaunchTrace<HNode4>(L, st, true);
     else LaunchTrace<GpuNode4>(L, st, true);
     if (L.classify) {
         KClassify<<<shadeGrid, kShadeBlock, 0, st>>>(L.jobs, L.paths, L.queues);
@@ -1123,6 +1150,7 @@ cudaError_t PtIteration(const PtLaunch& L, int iter, cudaStream_t st)
         KShade<-1><<<shadeGrid, kShadeBlock, 0, st>>>(L.jobs, L.paths, L.queues, 0);
     }
     if (L.layout == RTB200_BVH_Q8) LaunchTrace<QNode4>(L, st, false);
+    else if (L.layout == RTB200_BVH_F16) LaunchTrace<HNode4>(L, st, false);
     else LaunchTrace<GpuNode4>(L, st, false);
     KSwap<<<1, 1, 0, st>>>(L.queues.cnt);
     return cudaGetLastError();

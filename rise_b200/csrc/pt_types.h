@@ -104,6 +104,10 @@ struct PtSettings {
     int light_bvh;           // pick NEE luminaries with the light BVH (when the scene has one)
     int sampler;             // kSamplerHash / kSamplerSobol / kSamplerSobolShuffled
     int max_bounce[3];       // diffuse, glossy, transmission scatters a path may take (255 = no limit)
+    int single;              // 1: one wavelength per path (IntegrateRayNM); 0: hero + 3 companions
+    int num_wl;              // single: wavelength bins (0 = continuous)
+    float wl_step;           // single: (lmax - lmin) / num_wl
+    float inv_spectral;      // 1 / paths per pixel sample (nSpectralSamples)
 };
 
 constexpr int kSamplerHash = 0;

@@ -161,6 +161,9 @@ cudaError_t Dispatch(const rtb200_scene* s, const rtb200_ray* d_rays, int64_t n,
     } else if (s->layout == RTB200_BVH_Q8) {
         if (spill) Launch<QNode4, ANY, true>(s, d_rays, n, hits, occ, counter, err, stream);
         else Launch<QNode4, ANY, false>(s, d_rays, n, hits, occ, counter, err, stream);
+    } else if (s->layout == RTB200_BVH_F16) {
+        if (spill) Launch<HNode4, ANY, true>(s, d_rays, n, hits, occ, counter, err, stream);
+        else Launch<HNode4, ANY, false>(s, d_rays, n, hits, occ, counter, err, stream);
     } else {
         if (spill) Launch<GpuNode4, ANY, true>(s, d_rays, n, hits, occ, counter, err, stream);
         else Launch<GpuNode4, ANY, false>(s, d_rays, n, hits, occ, counter, err, stream);

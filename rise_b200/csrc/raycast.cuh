@@ -14,6 +14,7 @@
 #pragma once
 #include <climits>
 #include <cstdint>
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
 #include "bvh_build.h"
@@ -223,6 +224,45 @@ __device__ __forceinline__ void SlabQ8(const QNode4* nodes, int ni, const RayPre
     }
 }
 
+// Half-precision node: the FP32 slab test on child boxes widened to binary16
+// (outward), planes picked by the direction's sign as in SlabF32.
+__device__ __forceinline__ float2 Halves(unsigned w)
+{
+    return __half22float2(*reinterpret_cast<const __half2*>(&w));
+}
+__device__ __forceinline__ void SlabF16(const HNode4* nodes, int ni, const RayPre& p, float best, ChildHits& h)
+{
+    const int4* base = reinterpret_cast<const int4*>(nodes + ni);
+    const int4 w0 = __ldg(base + 0), w1 = __ldg(base + 1), w2 = __ldg(base + 2), w3 = __ldg(base + 3);
+    // Words (two halves each): lo x, y, z then hi x, y, z, children 0-1 and 2-3.
+    const unsigned lo[3][2] = {{(unsigned)w0.x, (unsigned)w0.y}, {(unsigned)w0.z, (unsigned)w0.w},
+                               {(unsigned)w1.x, (unsigned)w1.y}};
+    const unsigned hi[3][2] = {{(unsigned)w1.z, (unsigned)w1.w}, {(unsigned)w2.x, (unsigned)w2.y},
+                               {(unsigned)w2.z, (unsigned)w2.w}};
+    float tl[3][4], th[3][4];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const bool neg = p.inv[k] < 0.0f;
+#pragma unroll
+        for (int j = 0; j < 2; ++j) {
+            const float2 n = Halves(neg ? hi[k][j] : lo[k][j]), f = Halves(neg ? lo[k][j] : hi[k][j]);
+            tl[k][2 * j] = (n.x - p.o[k]) * p.inv[k];
+            tl[k][2 * j + 1] = (n.y - p.o[k]) * p.inv[k];
+            th[k][2 * j] = (f.x - p.o[k]) * p.inv[k];
+            th[k][2 * j + 1] = (f.y - p.o[k]) * p.inv[k];
+        }
+    }
+    h.c[0] = w3.x; h.c[1] = w3.y; h.c[2] = w3.z; h.c[3] = w3.w;
+    h.mask = 0;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        const float tn = Max3(tl[0][i], tl[1][i], fmaxf(tl[2][i], p.tmin));
+        const float tf = Min3(th[0][i], th[1][i], fminf(th[2][i], best));
+        h.t[i] = tn;
+        if (tn <= tf && h.c[i] != kEmpty) h.mask |= 1u << i;
+    }
+}
+
 template <class NodeT>
 struct Slab;
 template <>
@@ -237,6 +277,13 @@ struct Slab<QNode4> {
     __device__ __forceinline__ static void Run(const QNode4* n, int i, const RayPre& p, float b, ChildHits& h)
     {
         SlabQ8(n, i, p, b, h);
+    }
+};
+template <>
+struct Slab<HNode4> {
+    __device__ __forceinline__ static void Run(const HNode4* n, int i, const RayPre& p, float b, ChildHits& h)
+    {
+        SlabF16(n, i, p, b, h);
     }
 };
 

@@ -32,7 +32,8 @@ class RenderSettings(ctypes.Structure):
                 ("adaptive_max_spp", ctypes.c_int32), ("adaptive_threshold", ctypes.c_float),
                 ("light_selection", ctypes.c_int32), ("sampler", ctypes.c_int32), ("bounce_limits", ctypes.c_int32),
                 ("max_diffuse_bounce", ctypes.c_int32), ("max_glossy_bounce", ctypes.c_int32),
-                ("max_transmission_bounce", ctypes.c_int32)]
+                ("max_transmission_bounce", ctypes.c_int32), ("spectral_mode", ctypes.c_int32),
+                ("num_wavelengths", ctypes.c_int32), ("spectral_samples", ctypes.c_int32)]
 
 
 class Stats(ctypes.Structure):
@@ -98,7 +99,8 @@ def settings_struct(st):
                           getattr(st, "filter", 0), getattr(st, "filter_size", 2.0), getattr(st, "filter_sigma", 0.5),
                           getattr(st, "adaptive_max_spp", 0), getattr(st, "adaptive_threshold", 0.01),
                           getattr(st, "light_selection", 0), getattr(st, "sampler", 0),
-                          *bounce_limits(st))
+                          *bounce_limits(st), getattr(st, "spectral_mode", 0), getattr(st, "num_wavelengths", 0),
+                          getattr(st, "spectral_samples", 1))
 
 
 def bounce_limits(st):

@@ -25,7 +25,7 @@ NODE4_DTYPE = np.dtype([("minx", "<f4", 4), ("miny", "<f4", 4), ("minz", "<f4", 
                         ("child", "<i4", 4), ("count", "<u2", 4), ("nchild", "u1"),
                         ("axis", "u1"), ("pad", "u1", 6)])
 
-LAYOUTS = {"f32": _native.BVH_F32, "q8": _native.BVH_Q8, "w8": _native.BVH_W8}
+LAYOUTS = {"f32": _native.BVH_F32, "q8": _native.BVH_Q8, "w8": _native.BVH_W8, "f16": _native.BVH_F16}
 
 
 def _ptr(a):

@@ -19,7 +19,12 @@ src/Library/Parsers/ChunkParserRegistry.cpp (defaults included):
                                  (LambertianEmitter.cpp:72-87), reflective part
                                  from a lambertian `material` or none
   ggx_material                -> GGX conductor (rd none, isotropic alpha)
-  dielectric_material         -> smooth dielectric, constant IOR
+  scalar_painter              -> a scalar per wavelength: value, values r g b,
+                                 file of (nm, value) lines, sellmeier
+  dielectric_material         -> smooth dielectric: IOR constant or per wavelength
+                                 (scalar painter, inline r g b, number), transmitted
+                                 Phong lobe (scattering), clear interior (tau 1)
+  rawmesh2_geometry           -> vertices with normals (smooth shading)
   clippedplane_geometry       -> two triangles (a, b, c), (a, c, d)
   rawmesh_geometry            -> "tri" / "quad" lines (TriangleMeshLoaderRAW.cpp:33-110)
   risemesh_geometry           -> the .risemesh reader of the C ABI
@@ -30,15 +35,19 @@ src/Library/Parsers/ChunkParserRegistry.cpp (defaults included):
   pathtracing_spectral_rasterizer, pixelintegratingspectral_rasterizer
                               -> samples, wavelength range, pixel filter
                                  (default Gaussian 2.0 / 0.35), adaptive sampling,
-                                 Russian roulette, maximum depth (128)
+                                 Russian roulette, maximum depth (128), per-type
+                                 bounce limits, light BVH or power selection,
+                                 hero bundles (hwss true) or one wavelength per
+                                 path in num_wavelengths bins (the default),
+                                 spectral_samples
   pathtracing_shaderop, standard_shader, file_rasterizeroutput -> accepted
 
 A parameter or chunk that would change the image in a way this renderer
 cannot draw (other painters, materials, geometry, cameras, lights, modifiers,
 volumes, non-unit pixel aspect, hidden luminaires, ...) raises
 SceneFileError naming it.  Options that do not change the estimator's
-expectation (the pixel sampler, OIDN denoising of the output, light-BVH
-selection, hwss) are recorded in LoadedScene.notes.
+expectation (the pixel sampler, OIDN denoising of the output) are recorded
+in LoadedScene.notes.
 """
 import math
 import os
@@ -135,6 +144,43 @@ def _bool(s):
     return str(s).strip().lower() in ("true", "1", "yes", "on")
 
 
+_GRID = np.arange(81, dtype=np.float64) * 5.0 + 380.0   # the device's spectral grid (nm)
+
+
+def _uniform_scalar(v):
+    return lambda nm: np.full(np.shape(nm), float(v))
+
+
+def _rgb_scalar(r, g, b):
+    # RGBScalarPainter::GetValueAtNM: b up to 450 nm, g at 550, r from 650,
+    # linear between.
+    def fn(nm):
+        nm = np.asarray(nm, np.float64)
+        lo = b + (nm - 450.0) / 100.0 * (g - b)
+        hi = g + (nm - 550.0) / 100.0 * (r - g)
+        return np.where(nm <= 450.0, b, np.where(nm >= 650.0, r, np.where(nm <= 550.0, lo, hi)))
+    return fn
+
+
+def _piecewise_scalar(pts):
+    # PiecewiseLinearScalarPainter::EvalAtNM: clamped to the end values.
+    pts = sorted(pts)
+    xs = np.array([p[0] for p in pts]), np.array([p[1] for p in pts])
+    return lambda nm: np.interp(np.asarray(nm, np.float64), xs[0], xs[1])
+
+
+def _sellmeier_scalar(b1, b2, b3, c1, c2, c3):
+    # SellmeierScalarPainter::EvalAtNM: n^2 = 1 + sum B l^2 / (l^2 - C), l in um.
+    def fn(nm):
+        l2 = (np.asarray(nm, np.float64) * 1e-3) ** 2
+        n2 = 1.0
+        for b, cc in ((b1, c1), (b2, c2), (b3, c3)):
+            den = l2 - cc
+            n2 = n2 + np.where(np.abs(den) < 1e-9, 0.0, b * l2 / np.where(den == 0, 1.0, den))
+        return np.where(n2 > 0, np.sqrt(np.maximum(n2, 0.0)), 1.0)
+    return fn
+
+
 def _number(s):
     try:
         return float(s)
@@ -168,6 +214,7 @@ class _Loader:
         self.search = search
         self.desc = scenes.SceneDesc()
         self.painters = {}       # name -> spectrum id
+        self.scalars = {}        # name -> function of wavelength (nm, array) -> value
         self.materials = {}      # name -> (material id, kind, reflectance id)
         self.geometry = {}       # name -> ((n, 9) float64 triangles, double_sided)
         self.spp = None
@@ -238,6 +285,63 @@ class _Loader:
                                       _bool(c.get("normalize", "true")))
         self.painters[c.get("name", "noname")] = self.desc.add_spectrum(sp)
 
+    def scalar_painter(self, c):
+        # Physical scalars per wavelength (ScalarPainterAsciiChunkParser,
+        # Parsers/ChunkParserRegistry.cpp:1216-1330): `value` (uniform),
+        # `values r g b` (RGBScalarPainter), `file` of "nm value" lines
+        # (PiecewiseLinearScalarPainter, clamped at its ends), `sellmeier B1 B2
+        # B3 C1 C2 C3` (SellmeierScalarPainter, lambda in micrometres).
+        forms = ("value", "values", "file", "sellmeier")
+        self.only(c, {"name"} | set(forms))
+        present = [k for k in forms if c.has(k)]
+        if len(present) != 1:
+            self.refuse(c, "exactly one of value, values, file or sellmeier is supported")
+        form = present[0]
+        if form == "value":
+            v = _floats(c.get("value"), 1, "scalar_painter value")[0]
+            fn = _uniform_scalar(v)
+        elif form == "values":
+            fn = _rgb_scalar(*_floats(c.get("values"), 3, "scalar_painter values"))
+        elif form == "file":
+            pts = []
+            with open(self.path(c.get("file"), "scalar_painter"), "r") as f:
+                for ln in f:
+                    parts = ln.split()
+                    if not parts or parts[0].startswith("#"):
+                        continue
+                    try:
+                        pts.append((float(parts[0]), float(parts[1])))
+                    except (IndexError, ValueError):
+                        continue
+            if not pts:
+                self.refuse(c, "file produced no samples")
+            fn = _piecewise_scalar(pts)
+        else:
+            fn = _sellmeier_scalar(*_floats(c.get("sellmeier"), 6, "scalar_painter sellmeier"))
+        self.scalars[c.get("name", "noname")] = fn
+
+    def _scalar(self, c, value, default):
+        """A material's scalar slot (Job.cpp ResolveScalarPainterArg): a
+        scalar_painter name, an inline `r g b` triple or a single number."""
+        value = c.get(value, default)
+        if value in self.scalars:
+            return self.scalars[value]
+        parts = value.split()
+        if len(parts) == 3:
+            return _rgb_scalar(*_floats(value, 3, "scalar"))
+        v = _number(value)
+        if v is None:
+            self.refuse(c, f"unknown scalar painter {value!r}")
+        return _uniform_scalar(v)
+
+    def _scalar_spectrum(self, c, key, default):
+        """A physical-scalar slot as a spectrum id on the device's 5 nm grid
+        (a painter name is read as its spectrum)."""
+        value = c.get(key, default)
+        if value in self.painters:
+            return self.painters[value]
+        return self.desc.add_spectrum(self._scalar(c, key, default)(_GRID).astype(np.float32))
+
     def omni_light(self, c):
         # Job::AddPointOmniLight; shootphotons only matters to photon mapping.
         self.only(c, {"name", "power", "position", "color", "shootphotons"})
@@ -302,27 +406,34 @@ class _Loader:
         ax, ay = _number(c.get("alphax", "0.15")), _number(c.get("alphay", "0.15"))
         if ax is None or ay is None or ax != ay:
             self.refuse(c, "alphax and alphay must be equal numbers (isotropic)")
+        # rs "none" is the job's built-in black painter (Job.cpp:536-540):
+        # no specular layer at all.
         rs = c.get("rs", "none")
-        spec = self.spectrum(c, rs)
-        eta = self.spectrum(c, c.get("ior", "2.45"), allow_number=True)
-        kap = self.spectrum(c, c.get("extinction", "3.45"), allow_number=True)
+        spec = self.desc.add_spectrum(np.zeros(81, np.float32)) if rs == "none" else self.spectrum(c, rs)
+        eta = self._scalar_spectrum(c, "ior", "2.45")
+        kap = self._scalar_spectrum(c, "extinction", "3.45")
         self.add_material(c, scenes.Material(scenes.MAT_GGX, spec, -1, eta, kap, float(ax), 1.5), "ggx")
-        if rs == "none":
-            self.notes.append(f"ggx_material {c.get('name')}: rs none read as a unit specular layer")
 
     def dielectric_material(self, c):
         # Job::AddDielectricMaterial: tau (interior transmittance per unit
         # length), ior, scattering (the Phong exponent of the transmitted
         # lobe, default 10000; 1e6 and above is a smooth interface).
+        # The index of refraction is a scalar painter evaluated per
+        # wavelength (DielectricSPF::GetSpecularInfoNM): constant, or
+        # tabulated on the 5 nm grid (exact for piecewise-linear painters
+        # whose knots lie on it, as the RGB triple's 450/550/650 do).
         self.only(c, {"name", "tau", "ior", "scattering"})
-        tau = c.get("tau", "none")
-        if tau != "none" and any(x != 1.0 for x in _floats(tau, len(tau.split()), "tau")):
+        if c.get("tau", "none") != "none" and np.any(self._scalar(c, "tau", "none")(_GRID) != 1.0):
             self.refuse(c, "an absorbing interior (tau other than 1) is not supported")
-        ior = _number(c.get("ior", "1.33"))
-        scat = _number(c.get("scattering", "10000"))
-        if ior is None or scat is None:
-            self.refuse(c, "ior and scattering must be numbers")
-        self.add_material(c, scenes.Material(scenes.MAT_DIELECTRIC, -1, -1, -1, -1, float(min(scat, 1e6)), float(ior)),
+        ior = self._scalar(c, "ior", "1.33")(_GRID)
+        scat = self._scalar(c, "scattering", "10000")(_GRID)
+        if np.any(scat != scat[0]):
+            self.refuse(c, "a scattering exponent that varies with wavelength is not supported")
+        if np.all(ior == ior[0]):
+            eta, n = -1, float(ior[0])
+        else:
+            eta, n = self.desc.add_spectrum(ior.astype(np.float32)), float(ior[34])
+        self.add_material(c, scenes.Material(scenes.MAT_DIELECTRIC, -1, -1, eta, -1, float(min(scat[0], 1e6)), n),
                           "dielectric")
 
     # ---- geometry ----------------------------------------------------------
@@ -442,7 +553,8 @@ class _Loader:
                 "adaptive_max_samples", "adaptive_threshold", "rr_min_depth", "rr_threshold", "show_luminaires",
                 "oidn_denoise", "oidn_quality", "oidn_device", "oidn_prefilter", "light_bvh", "defaultshader",
                 "progressive_rendering", "progressive_samples_per_pass", "max_diffuse_bounce", "max_glossy_bounce",
-                "max_transmission_bounce", "max_translucent_bounce", "max_volume_bounce"}
+                "max_transmission_bounce", "max_translucent_bounce", "max_volume_bounce", "radiance_map",
+                "radiance_scale", "radiance_background", "radiance_orient"}
         self.only(c, base | extra)
         self.spp = int(c.get("samples", 32))
         lo, hi = float(c.get("nmbegin", 380.0)), float(c.get("nmend", 780.0))
@@ -479,12 +591,49 @@ class _Loader:
         self.st["sampler"] = scenes.SAMPLER_SOBOL_SHUFFLED
         if not _bool(c.get("show_luminaires", "true")):
             self.refuse(c, "hidden luminaires (show_luminaires false) are not supported")
-        for k, why in (("pixel_sampler", "camera jitter is drawn from the path's Sobol dimensions 0 and 1, "
-                        "whatever pixel sampler is named"), ("oidn_denoise", "the film is not denoised"),
-                       ("light_bvh", "lights are picked by emitted power")):
-            self.notes.append(f"{c.keyword}: {why}")
-        if not _bool(c.get("hwss", c.get("use_hwss", "false"))) or c.get("num_wavelengths", "4") != "4":
-            self.notes.append(f"{c.keyword}: rendered with hero-wavelength sampling of 4 wavelengths")
+        if c.has("pixel_sampler"):
+            self.notes.append(f"{c.keyword}: camera jitter is drawn from the path's Sobol dimensions 0 and 1, "
+                              "whatever pixel sampler is named")
+        # The reference denoises with OIDN unless told not to (RasterizerDefaults::oidnDenoise).
+        if _bool(c.get("oidn_denoise", "true")):
+            self.notes.append(f"{c.keyword}: the film is not denoised")
+        # Environment (RadianceMapConfig): a painter seen by escaping rays
+        # through the light-probe mapping (Rendering/RadianceMap.h), times
+        # radiance_scale; drawn here when the painter is uniform (a spectral
+        # or uniform-colour painter: the same radiance in every direction,
+        # so the orientation does not matter), visible to camera rays when
+        # radiance_background (default true).
+        env = c.get("radiance_map", "none")
+        if env != "none":
+            if env not in self.painters:
+                self.refuse(c, f"radiance_map {env!r}: only uniform painters (spectral_painter, "
+                               "uniformcolor_painter, blackbody_painter) are supported")
+            scale = float(c.get("radiance_scale", 1.0))
+            sid = self.painters[env]
+            if scale != 1.0:
+                import dataclasses
+                sp = self.desc.spectra[sid]
+                if isinstance(sp, np.ndarray):
+                    sp = (sp * scale).astype(np.float32)
+                elif hasattr(sp, "amps"):
+                    sp = dataclasses.replace(sp, amps=np.asarray(sp.amps) * scale)
+                else:
+                    sp = dataclasses.replace(sp, scale=sp.scale * scale)
+                sid = self.desc.add_spectrum(sp)
+            self.desc.env = sid
+            self.desc.env_visible = int(_bool(c.get("radiance_background", "true")))
+        # StabilityConfig::useLightBVH (default true): the light BVH, else
+        # the alias table over emitted power.
+        self.st["light_selection"] = 0 if _bool(c.get("light_bvh", "true")) else 1
+        # SpectralConfig (Utilities/SpectralConfig.h): hero-wavelength bundles
+        # with `hwss true`, else one wavelength per path in num_wavelengths
+        # bins (default 10); spectral_samples paths per pixel sample.
+        hwss = _bool(c.get("hwss", c.get("use_hwss", "false")))
+        self.st["spectral_mode"] = scenes.SPECTRAL_HWSS if hwss else scenes.SPECTRAL_SINGLE
+        self.st["num_wavelengths"] = int(c.get("num_wavelengths", 10))
+        self.st["spectral_samples"] = int(c.get("spectral_samples", 1))
+        if self.st["num_wavelengths"] < 1 or not 1 <= self.st["spectral_samples"] <= 256:
+            self.refuse(c, "num_wavelengths must be positive and spectral_samples within 1..256")
 
     def pathtracing_spectral_rasterizer(self, c):
         self._raster_common(c, set())

@@ -245,6 +245,8 @@ def spectral_painter(nm, amplitudes, nmbegin=400.0, nmend=700.0):
 SAMPLER_HASH = 0    # counter-based hash of (seed, pixel, sample, dimension)
 SAMPLER_SOBOL = 1   # the reference's Owen-scrambled padded Sobol
 SAMPLER_SOBOL_SHUFFLED = 2   # the same with the index shuffled per dimension pair (converges per pixel)
+SPECTRAL_HWSS = 0    # hero wavelength + 3 companions per path (the reference's hwss true)
+SPECTRAL_SINGLE = 1  # one wavelength per path (the reference's default, hwss false)
 
 
 @dataclass
@@ -269,10 +271,13 @@ class RenderSettings:
     adaptive_max_spp: int = 0       # adaptive sampling: maximum samples per pixel (0 = off)
     adaptive_threshold: float = 0.01  # adaptive sampling: relative standard error to converge
     light_selection: int = 0  # 0 light BVH (more than one luminary), 1 by emitted power
-    sampler: int = 0          # 0 counter-based hash, 1 the reference's Owen-scrambled Sobol
+    sampler: int = 0          # 0 counter-based hash, 1 the reference's Owen-scrambled Sobol, 2 shuffled Sobol
     max_diffuse_bounce: int = None       # per-type bounce limits (None = unlimited)
     max_glossy_bounce: int = None
     max_transmission_bounce: int = None
+    spectral_mode: int = 0    # 0 hero + 3 companions (hwss true), 1 one wavelength per path (hwss false)
+    num_wavelengths: int = 0  # single-wavelength mode: wavelength bins (0 = continuous)
+    spectral_samples: int = 1 # paths per pixel sample
 
 
 @dataclass

@@ -26,8 +26,15 @@ oracle/rise_ref.mk), on tests/golden/cornell_c1.RISEscene:
   numbers of tests/golden/cornell_smooth.RISEscene, the box with a smooth-
   shaded Lambertian sphere and a smooth-shaded glass sphere (vertex normals
   from RAW2 files): the z-test of interpolated shading normals.
+* cornell_nm_ref_k16_independent.npz, cornell_prism_ref_k16_independent.npz,
+  cornell_prism_nm_ref_k16_independent.npz -- the same for the wavelength-
+  sampling variants (tests/golden/make_cornell_scene.py variants): one
+  wavelength per path in 10 bins; a dispersive glass prism under hero-
+  wavelength bundles; the prism with one wavelength per path in 30 bins and
+  two spectral samples per pixel sample (the prism scenes at 16 batches of 64
+  samples per pixel).
 
-    make -C oracle && python tests/golden/make_cornell_reference.py [k16|k16i|smooth|fp64]
+    make -C oracle && python tests/golden/make_cornell_reference.py [k16|k16i|smooth|variants|fp64]
     (k16, k16i: ~40 s each, fp64: ~45 min on 8 cores; rows are checkpointed under
     oracle/_ref/ so an interrupted run resumes)
 """
@@ -49,12 +56,12 @@ FP64_SPP = 16384
 ROWS = 8
 
 
-def make_k16(r, independent=False, name=None):
+def make_k16(r, independent=False, name=None, spp=K_SPP):
     t0 = time.time()
-    b = np.array([r.integrate(K_SPP, batch=k, independent=independent) for k in range(1, K + 1)])
+    b = np.array([r.integrate(spp, batch=k, independent=independent) for k in range(1, K + 1)])
     name = name or ("cornell_c1_ref_k16_independent.npz" if independent else "cornell_c1_ref_k16.npz")
     np.savez_compressed(os.path.join(HERE, name), mean=b.mean(0).astype(np.float32),
-                        var=b.var(0, ddof=1).astype(np.float32), k=K, spp=K_SPP)
+                        var=b.var(0, ddof=1).astype(np.float32), k=K, spp=spp)
     print(f"{name}: {time.time() - t0:.0f} s", flush=True)
 
 
@@ -72,7 +79,7 @@ def make_fp64(r):
 
 
 def main():
-    which = sys.argv[1:] or ["k16", "k16i", "smooth", "fp64"]
+    which = sys.argv[1:] or ["k16", "k16i", "smooth", "variants", "fp64"]
     r = oracle.RefRenderer(SCENE)
     if "k16" in which:
         make_k16(r)
@@ -83,6 +90,12 @@ def main():
     if "smooth" in which:
         make_k16(oracle.RefRenderer(os.path.join(HERE, "cornell_smooth.RISEscene")), independent=True,
                  name="cornell_smooth_ref_k16_independent.npz")
+    if "variants" in which:
+        # The prism's caustics make single pixels heavy-tailed; 64 samples
+        # per batch bring the batch means nearer to normal for the z-test.
+        for v, spp in (("cornell_nm", K_SPP), ("cornell_prism", 64), ("cornell_prism_nm", 64)):
+            make_k16(oracle.RefRenderer(os.path.join(HERE, v + ".RISEscene")), independent=True,
+                     name=v + "_ref_k16_independent.npz", spp=spp)
 
 
 if __name__ == "__main__":

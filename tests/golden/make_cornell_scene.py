@@ -21,6 +21,7 @@ depth 8), 256 x 256, 16 samples per pixel.
 
     python tests/golden/make_cornell_scene.py           (the C1 scene)
     python tests/golden/make_cornell_scene.py smooth    (the smooth-shaded variant)
+    python tests/golden/make_cornell_scene.py variants  (single-wavelength and dispersive variants)
 """
 import math
 import os
@@ -157,3 +158,76 @@ def main_smooth():
 
 if __name__ == "__main__" and sys.argv[1:] == ["smooth"]:
     main_smooth()
+
+
+# ---- wavelength-sampling variants ---------------------------------------------
+# cornell_nm: the C1 scene with `hwss false`, the reference's default of one
+# wavelength per path in num_wavelengths (default 10) bins.
+# cornell_prism: the C1 walls and light around a closed triangular glass
+# prism (single-sided, outward winding) whose index of refraction varies with
+# wavelength, raised 0.02 off the floor (`ior 1.3 1.5 2`: the reference's RGBScalarPainter, 2.0 at 450 nm
+# and below, 1.5 at 550, 1.3 from 650), rendered with hero-wavelength
+# bundles; cornell_prism_nm the same with one wavelength per path in 30 bins
+# and two spectral samples per pixel sample.
+#     python tests/golden/make_cornell_scene.py variants
+PRISM = [(0.32, 0.02, 0.30), (0.68, 0.02, 0.30), (0.50, 0.02, 0.58)]
+PRISM_HEIGHT = 0.42
+
+
+def prism_tri9():
+    a, b, c = (np.array(p, np.float64) for p in PRISM)
+    up = np.array([0.0, PRISM_HEIGHT, 0.0])
+    A, B, C = a + up, b + up, c + up
+    tris = [(a, b, c), (A, C, B)]                         # bottom (facing down), top (facing up)
+    for p, q in ((a, b), (b, c), (c, a)):                 # sides, counter-clockwise seen from outside
+        P, Q = p + up, q + up
+        tris += [(p, Q, q), (p, P, Q)]
+    t = np.array([np.concatenate(x) for x in tris])
+    cen = np.mean([a, b, c], axis=0) + 0.5 * up
+    tt = t.reshape(-1, 3, 3)
+    n = np.cross(tt[:, 1] - tt[:, 0], tt[:, 2] - tt[:, 0])
+    assert ((n * (tt.mean(axis=1) - cen)).sum(axis=1) > 0).all()
+    return t
+
+
+def nm_scene_text():
+    text, _ = scene_text()
+    text = text.replace("# The C1 spectral Cornell box (written by tests/golden/make_cornell_scene.py).",
+                        "# The C1 box, one wavelength per path (written by tests/golden/make_cornell_scene.py).")
+    return text.replace("\thwss\t\t\t\ttrue\n", "\thwss\t\t\t\tfalse\n")
+
+
+def prism_scene_text(hwss=True):
+    text, _ = scene_text()
+    what = "hero-wavelength bundles" if hwss else "one wavelength per path"
+    text = text.replace("# The C1 spectral Cornell box (written by tests/golden/make_cornell_scene.py).",
+                        f"# The C1 box around a dispersive glass prism, {what} "
+                        "(written by tests/golden/make_cornell_scene.py).")
+    text = text.replace(f"\tfile\t\t{NAME}_", "\tfile\t\tcornell_c1_")
+    cut = text.index("rawmesh_geometry\n{\n\tname\t\tg_boxes")
+    end = text.index("rawmesh_geometry\n{\n\tname\t\tg_light")
+    text = text[:cut] + text[end:]
+    text = text.replace("max_diffuse_bounce\t7", "max_diffuse_bounce\t7\n\tmax_glossy_bounce\t8\n"
+                        "\tmax_transmission_bounce\t8")
+    if not hwss:
+        text = text.replace("\thwss\t\t\t\ttrue\n\tspectral_samples\t1\n",
+                            "\thwss\t\t\t\tfalse\n\tnum_wavelengths\t\t30\n\tspectral_samples\t2\n")
+    extra = ["dielectric_material", "{", "\tname\t\tglass", "\ttau\t\t\t1.0", "\tior\t\t\t1.3 1.5 2",
+             "\tscattering\t1000000", "}", "",
+             "rawmesh_geometry", "{", "\tname\t\tg_prism", "\tfile\t\tcornell_prism_prism.raw",
+             "\tdouble_sided\tfalse", "}", "",
+             "standard_object", "{", "\tname\t\to_prism", "\tgeometry\tg_prism", "\tmaterial\tglass", "}", ""]
+    return text + "\n".join(extra)
+
+
+def main_variants():
+    for name, text in (("cornell_nm", nm_scene_text()), ("cornell_prism", prism_scene_text(True)),
+                       ("cornell_prism_nm", prism_scene_text(False))):
+        with open(os.path.join(HERE, name + ".RISEscene"), "w") as f:
+            f.write(text)
+    with open(os.path.join(HERE, "cornell_prism_prism.raw"), "w") as f:
+        f.write(raw_text(prism_tri9()))
+
+
+if __name__ == "__main__" and sys.argv[1:] == ["variants"]:
+    main_variants()

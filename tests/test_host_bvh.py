@@ -120,3 +120,61 @@ def test_wide_nodes_are_conservative_and_find_every_closest_hit(w8_check, tmp_pa
     np.ascontiguousarray(rays, np.float32).tofile(rp)
     out = subprocess.run([w8_check, str(tp), str(rp)], capture_output=True, text=True)
     assert out.returncode == 0 and out.stdout.startswith("ok"), out.stdout + out.stderr
+
+
+# ---- the half-precision layout (EncodeHalfNodes in rise_b200/csrc/bvh_build.cpp) ----
+
+@pytest.fixture(scope="module")
+def f16_check(tmp_path_factory):
+    import subprocess
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    src = os.path.join(root, "rise_b200", "csrc")
+    exe = str(tmp_path_factory.mktemp("f16") / "f16_check")
+    subprocess.run(["g++", "-O2", "-std=c++17", "-I", src, os.path.join(root, "tests", "cpp", "f16_check.cpp"),
+                    os.path.join(src, "bvh_build.cpp"), "-o", exe, "-lpthread"], check=True)
+    return exe
+
+
+def test_half_values_are_ieee_binary16(f16_check, tmp_path):
+    import subprocess
+    out = tmp_path / "h.bin"
+    subprocess.run([f16_check, "halves", str(out)], check=True)
+    got = np.fromfile(out, np.float32)
+    want = np.arange(65536, dtype=np.uint16).view(np.float16).astype(np.float32)
+    nan = np.isnan(want)
+    assert (np.isnan(got) == nan).all() and (got[~nan] == want[~nan]).all()
+
+
+def test_directed_rounding_to_half_brackets_every_float(f16_check, tmp_path):
+    """Down and up roundings: down <= x <= up, equal when x is a half, else
+    neighbours; beyond the half range the outward side is infinite."""
+    import subprocess
+    rng = np.random.default_rng(3)
+    x = np.concatenate([rng.uniform(-2, 2, 20000), rng.normal(0, 1e-5, 2000), rng.uniform(-7e4, 7e4, 2000),
+                        np.arange(-2048, 2048, dtype=np.float16).astype(np.float64) / 256.0,
+                        [0.0, -0.0, 65504.0, -65504.0, 65520.0, 1e6, -1e6, 6e-8, -6e-8, 1e-9]]).astype(np.float32)
+    inp, out = tmp_path / "x.bin", tmp_path / "r.bin"
+    x.tofile(inp)
+    subprocess.run([f16_check, "round", str(inp), str(out)], check=True)
+    r = np.fromfile(out, np.uint16).reshape(-1, 2)
+    dn, up = r[:, 0].view(np.float16).astype(np.float64), r[:, 1].view(np.float16).astype(np.float64)
+    xd = x.astype(np.float64)
+    assert (dn <= xd).all() and (up >= xd).all()
+    with np.errstate(over="ignore"):
+        exact = x.astype(np.float16).astype(np.float64) == xd
+    assert (dn[exact] == xd[exact]).all() and (up[exact] == xd[exact]).all()
+    fin = ~exact & np.isfinite(dn) & np.isfinite(up)
+    assert (np.nextafter(dn[fin].astype(np.float16), np.float16(np.inf)).astype(np.float64) == up[fin]).all()
+    assert np.isinf(up[xd > 65504]).all() and np.isinf(dn[xd < -65504]).all()
+
+
+@pytest.mark.parametrize("case", ["soup", "tiny1", "deep"])
+def test_half_nodes_contain_the_fp32_boxes(f16_check, tmp_path, case):
+    import subprocess
+    from rise_b200 import scenes
+    tri = {"soup": lambda: scenes.soup_triangles(20000, seed=4), "tiny1": lambda: scenes.soup_triangles(1, seed=1),
+           "deep": scenes.nested_clusters}[case]()
+    tp = tmp_path / "tri.bin"
+    np.ascontiguousarray(tri, np.float32).tofile(tp)
+    out = subprocess.run([f16_check, "nodes", str(tp)], capture_output=True, text=True)
+    assert out.returncode == 0 and out.stdout.startswith("ok"), out.stdout + out.stderr

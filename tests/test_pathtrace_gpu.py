@@ -43,7 +43,7 @@ def rel_mse(x, ref):
 
 
 @pytest.mark.parametrize("nee_per_lambda", [1, 0])
-@pytest.mark.parametrize("layout", ["f32", "q8"])
+@pytest.mark.parametrize("layout", ["f32", "q8", "f16"])
 def test_same_seed_matches_oracle(ctx, nee_per_lambda, layout):
     d = scenes.cornell_box(64, 64, nee_per_lambda=nee_per_lambda)
     g, st = render_gpu(ctx, d, 16, layout)

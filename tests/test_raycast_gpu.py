@@ -19,7 +19,7 @@ from parity import any_report, closest_report
 pytestmark = pytest.mark.gpu
 
 GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
-LAYOUTS = ["f32", "q8", "w8"]
+LAYOUTS = ["f32", "q8", "w8", "f16"]
 
 
 @pytest.fixture(scope="module")
@@ -124,6 +124,7 @@ def test_layouts_agree_and_are_deterministic(ctx):
     sf, rf = make_caster(ctx, tri, "f32")
     sq, rq = make_caster(ctx, tri, "q8")
     sw, rw = make_caster(ctx, tri, "w8")
+    sh, rh = make_caster(ctx, tri, "f16")
     a = rf.cast_rays(rays)
     b = rq.cast_rays(rays)
     c = rf.cast_rays(rays)
@@ -133,6 +134,9 @@ def test_layouts_agree_and_are_deterministic(ctx):
     assert (w["prim"] == w2["prim"]).all() and (w["t"] == w2["t"]).all()
     assert (a["prim"] == b["prim"]).mean() > 0.99999
     assert (a["prim"] == w["prim"]).mean() > 0.99999
+    h = rh.cast_rays(rays)
+    assert (a["prim"] == h["prim"]).mean() > 0.99999
+    sh.close()
     sf.close()
     sq.close()
     sw.close()

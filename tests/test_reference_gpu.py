@@ -131,3 +131,57 @@ def test_smooth_shading_same_random_numbers_as_the_oracle(ctx, sampler):
     assert close.mean() > 0.95, close.mean()
     assert rel_mse(g, o) < 1e-3
     assert abs(g[..., 1].mean() / o[..., 1].mean() - 1) < 2e-3
+
+
+VARIANTS = ["cornell_nm", "cornell_prism", "cornell_prism_nm"]
+
+
+def _variant(name):
+    f = np.load(os.path.join(GOLDEN, name + "_ref_k16_independent.npz"))
+    ls = scenefile.load_scene(os.path.join(GOLDEN, name + ".RISEscene"))
+    return ls, f["mean"].astype(np.float64), f["var"].astype(np.float64), int(f["k"]), int(f["spp"])
+
+
+@pytest.mark.parametrize("sampler", [0, 2], ids=["hash", "shuffled"])
+@pytest.mark.parametrize("name", VARIANTS)
+def test_wavelength_sampling_z_test_against_the_reference(ctx, name, sampler):
+    """One wavelength per path in bins (the reference's default, hwss false)
+    and a dispersive glass prism under hero bundles and under single
+    wavelengths with two spectral samples: 16 GPU batches against the
+    reference's 16 (independent numbers), every pixel; image means per
+    channel within 4 standard errors."""
+    ls, mr, vr, k, spp = _variant(name)
+    g = np.array([render(ctx, ls.desc, spp, seed=3001 + b, sampler=sampler) for b in range(k)])
+    assert np.isfinite(g).all()
+    z, _ = z_scores(g.mean(0), g.var(0, ddof=1), k, mr, vr, k)
+    rate = float((np.abs(z) > Z_LIMIT).mean())
+    assert rate <= Z_ALLOWED_RATE, rate
+    for c in range(3):
+        se = np.sqrt(g[..., c].mean(axis=(1, 2)).var(ddof=1) / k + vr[..., c].mean() / k / mr[..., c].size)
+        assert abs(g[..., c].mean() - mr[..., c].mean()) < 4 * se, c
+
+
+@pytest.mark.parametrize("name", VARIANTS)
+def test_wavelength_sampling_same_random_numbers_as_the_oracle(ctx, name):
+    ls, _, _, _, _ = _variant(name)
+    st = dataclasses.replace(ls.desc.settings, seed=3, sampler=2)
+    g = render(ctx, ls.desc, 16, seed=3, sampler=2)[128:192]
+    o = oracle.pt_render(ls.desc, 16, crop=(0, 128, st.width, 192), settings=st)
+    close = (np.abs(g - o) <= 1e-3 * (np.abs(o) + 1e-3)).all(axis=2)
+    assert close.mean() > 0.97, close.mean()
+    assert rel_mse(g, o) < 1e-4
+
+
+def test_spectral_settings_are_checked(ctx, c1):
+    """Adaptive sampling needs one spectral sample per pixel sample; unknown
+    modes and negative counts are refused."""
+    from rise_b200._native import RTB200Error
+    scene = pathtracer.upload_scene(ctx, c1.desc)
+    try:
+        for bad in (dict(spectral_mode=2), dict(num_wavelengths=-1), dict(spectral_samples=-1),
+                    dict(spectral_samples=2, adaptive_max_spp=64)):
+            st = dataclasses.replace(c1.desc.settings, **bad)
+            with pytest.raises(RTB200Error):
+                pathtracer.SpectralRasterizer(ctx, c1.desc, "f32", scene=scene, settings=st)
+    finally:
+        scene.close()

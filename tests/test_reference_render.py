@@ -116,3 +116,56 @@ def test_smooth_shading_normals_match_the_reference():
     flat = dataclasses.replace(ls.desc)
     flat._nrms = [None] * len(ls.desc._nrms)
     assert rate(flat) > 2 * Z_ALLOWED_RATE
+
+
+def _variant(name):
+    f = np.load(os.path.join(GOLDEN, name + "_ref_k16_independent.npz"))
+    ls = scenefile.load_scene(os.path.join(GOLDEN, name + ".RISEscene"))
+    return ls, f["mean"].astype(np.float64), f["var"].astype(np.float64), int(f["k"]), int(f["spp"])
+
+
+def _z_rate(desc, st, mr, vr, k, spp, rows, seed0):
+    y0, y1 = rows
+    g = np.array([oracle.pt_render(desc, spp, crop=(0, y0, st.width, y1),
+                                   settings=dataclasses.replace(st, seed=seed0 + b, sampler=0))
+                  for b in range(k)])
+    z, _ = z_scores(g.mean(0), g.var(0, ddof=1), k, mr[y0:y1], vr[y0:y1], k)
+    return float((np.abs(z) > Z_LIMIT).mean()), g
+
+
+def test_single_wavelength_mode_matches_the_reference():
+    """`hwss false` (the reference's default): one wavelength per path from
+    10 bins of 30 nm (IntegrateRayNM).  The restatement's 16 batches against
+    the reference's 16; the same scene rendered with continuous hero bundles
+    fails the test (the bins shift Z by about 3 %)."""
+    ls, mr, vr, k, spp = _variant("cornell_nm")
+    st = ls.desc.settings
+    assert (st.spectral_mode, st.num_wavelengths, st.spectral_samples) == (1, 10, 1)
+    rate, g = _z_rate(ls.desc, st, mr, vr, k, spp, ROWS, 900)
+    assert rate <= Z_ALLOWED_RATE, rate
+    y0, y1 = ROWS
+    se = np.sqrt(g[..., 2].mean(axis=(1, 2)).var(ddof=1) / k + vr[y0:y1, :, 2].mean() / k / g[0, ..., 2].size)
+    assert abs(g[..., 2].mean() - mr[y0:y1, :, 2].mean()) < 4 * se
+    hwss = dataclasses.replace(st, spectral_mode=0)
+    assert _z_rate(ls.desc, hwss, mr, vr, k, spp, ROWS, 900)[0] > 2 * Z_ALLOWED_RATE
+
+
+@pytest.mark.parametrize("name", ["cornell_prism", "cornell_prism_nm"])
+def test_dispersive_glass_matches_the_reference(name):
+    """A glass prism whose index runs from 2.0 (450 nm) to 1.3 (650 nm):
+    under hero bundles the companions end at the prism and the hero goes on
+    alone; one wavelength per path (30 bins, two spectral samples per pixel
+    sample) refracts each at its own index.  The restatement against the
+    reference (16 batches of 64 samples per pixel: the caustics make single
+    samples heavy-tailed) on the rows through the prism; the prism read with
+    a constant index of 1.5 fails the same test."""
+    ls, mr, vr, k, spp = _variant(name)
+    st = ls.desc.settings
+    glass = [m for m in ls.desc.materials if m.type == 2]
+    assert len(glass) == 1 and glass[0].eta >= 0
+    rows = (192, 224)   # the prism's lower half and the floor in front of it
+    rate, _ = _z_rate(ls.desc, st, mr, vr, k, spp, rows, 1100)
+    assert rate <= Z_ALLOWED_RATE, rate
+    const = dataclasses.replace(ls.desc)
+    const.materials = [dataclasses.replace(m, eta=-1, ior=1.5) if m.type == 2 else m for m in ls.desc.materials]
+    assert _z_rate(const, st, mr, vr, k, spp, rows, 1100)[0] > 2 * Z_ALLOWED_RATE

@@ -30,7 +30,7 @@ def _cast(L, fn, s, d_rays, n, d_out, st, ctx):
     _native.check(fn(s.h, ctypes.c_void_p(d_rays.data_ptr()), n, ctypes.c_void_p(d_out.data_ptr()), st), ctx.h)
 
 
-@pytest.mark.parametrize("case", ["f32", "q8", "deep"])
+@pytest.mark.parametrize("case", ["f32", "q8", "f16", "deep"])
 def test_noalloc_matches_device_entry_point_and_reference_twice(case):
     torch = pytest.importorskip("torch")
     L = _native.lib()
@@ -43,7 +43,7 @@ def test_noalloc_matches_device_entry_point_and_reference_twice(case):
     with raycaster.Context(0) as ctx:
         s = raycaster.Scene(ctx)
         s.add_triangles(tri)
-        s.commit("q8" if case == "q8" else "f32")
+        s.commit(case if case in ("q8", "f16") else "f32")
         d_rays = torch.from_numpy(rays).cuda()
         d_ref = torch.empty((len(rays), 4), dtype=torch.float32, device="cuda")
         st = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
