@@ -237,6 +237,27 @@ int rtb200_scene_add_point_light(rtb200_scene* scene, const float* position, con
  * selects whether camera rays see it directly. */
 int rtb200_scene_set_environment(rtb200_scene* scene, int32_t spectrum, int32_t visible);
 
+/* Image environment: the rasterizer's radiance_map bound to an HDR texture
+ * painter (RadianceMapConfig, Utilities/RadianceMapConfig.h; RadianceMap,
+ * Rendering/RadianceMap.h; Job::AddHDRTexturePainter, Job.cpp:2216-2265).
+ * rgb: width x height linear Rec.709 texels, rows top to bottom, as the
+ * reference's HDR reader delivers them (rtb200_hdr_decode).  A world
+ * direction is rotated by the Euler angles orientation_deg (x, y, z in
+ * degrees, radiance_orient; null = none), mapped to the light-probe (angular)
+ * image, read with the bilinear filter at the base level, uplifted to a
+ * spectrum per lookup (RGBUnboundedSpectrum) and scaled by `scale`
+ * (radiance_scale).  Next-event estimation draws directions from the
+ * reference's 64 x 64 importance table (EnvironmentSampler) with
+ * power-heuristic MIS against BSDF sampling.  visible: camera rays see the
+ * map (radiance_background).  Replaces a uniform sky and vice versa. */
+int rtb200_scene_set_environment_map(rtb200_scene* scene, const float* rgb, int32_t width, int32_t height,
+                                     float scale, const float* orientation_deg, int32_t visible);
+
+/* Decodes a Radiance HDR (RGBE) file held in memory as the reference's
+ * HDRReader does (RasterImages/HDRReader.cpp): *width, *height, and with rgb
+ * non-null width x height x 3 floats, rows top to bottom. */
+int rtb200_hdr_decode(const uint8_t* bytes, int64_t n, int32_t* width, int32_t* height, float* rgb);
+
 /* ---- render jobs (the rasterizer) -------------------------------------- */
 
 /* Settings of one progressive render.  Replaces the parameters of

@@ -10,6 +10,7 @@ Only tests/, `__graft_entry__.smoke()` and bench.py's CPU-baseline leg may
 import this package.  The product (rise_b200) never does.
 """
 import ctypes
+import math
 import os
 
 import numpy as np
@@ -156,6 +157,28 @@ def closest_brute(tri9, rays):
     return ids, t
 
 
+class _OrcEnvImage(ctypes.Structure):
+    _fields_ = [("rgb", _f32p), ("width", ctypes.c_int32), ("height", ctypes.c_int32), ("scale", ctypes.c_double),
+                ("orient_rad", ctypes.c_double * 3), ("uplift", _f32p)]
+
+
+_UPLIFT = None
+
+
+def uplift_table():
+    """The Jakob-Hanika RGB -> sigmoid-coefficient table (3 x 64^3 x 3
+    floats) as rise_b200 generates it (held to the reference generator's
+    output by tests/test_oracle_pt.py): data for the oracle's image
+    environment, which restates the lookup itself."""
+    global _UPLIFT
+    if _UPLIFT is None:
+        from rise_b200 import _native
+        t = np.empty(3 * 64 ** 3 * 3, np.float32)
+        _native.check(_native.lib().rtb200_rgb_uplift_table(t.ctypes.data_as(ctypes.c_void_p)))
+        _UPLIFT = t
+    return _UPLIFT
+
+
 def cie_table():
     """The reference's CIE 1931 table (tests/golden/cie1931_5nm.json), 3 x 81."""
     import json
@@ -231,17 +254,26 @@ def pt_render(desc, spp, sample_begin=0, crop=None, threads=None, settings=None,
     f.restype = ctypes.c_int
     i32 = ctypes.c_int32
     f.argtypes = [_f32p, _i64, _vp, i32, _f32p, i32, _vp, _f32p, i32, _vp, _f64p, _f64p, _vp, i32, i32,
-                  i32, i32, i32, i32, i32, _f64p, _f64p, _vp, i32, _f64p, _f32p]
+                  i32, i32, i32, i32, i32, _f64p, _f64p, _vp, i32, _f64p, _f32p, _vp]
     points = np.array([list(p) + list(c) + [w] for p, c, w in getattr(desc, "point_lights", [])],
                       np.float64).reshape(-1, 7)
     nrm9 = getattr(desc, "nrm9", None)
     if nrm9 is not None:
         nrm9 = np.ascontiguousarray(nrm9, np.float32)
+    env_arg, keep = None, None
+    em = getattr(desc, "env_map", None)
+    if em is not None:
+        rgb = np.ascontiguousarray(em.rgb, np.float32)
+        table = uplift_table()
+        ei = _OrcEnvImage(rgb.ctypes.data_as(_f32p), rgb.shape[1], rgb.shape[0], float(em.scale),
+                          (ctypes.c_double * 3)(*[math.radians(a) for a in em.orient_deg]),
+                          table.ctypes.data_as(_f32p))
+        env_arg, keep = ctypes.byref(ei), (rgb, table, ei)
     rc = f(_p(tri9, _f32p), len(tri9), meshes.ctypes.data, len(meshes), _p(spectra, _f32p), len(desc.spectra),
            mats_i.ctypes.data, _p(mats_f, _f32p), len(mats_i), envi.ctypes.data, _p(cam, _f64p), _p(setd, _f64p),
            seti.ctypes.data, int(spp), int(sample_begin), x0, y0, x1, y1, threads or os.cpu_count(),
            _p(out, _f64p), _p(cie, _f64p), counts.ctypes.data, len(points), _p(points, _f64p),
-           _p(nrm9, _f32p) if nrm9 is not None else None)
+           _p(nrm9, _f32p) if nrm9 is not None else None, env_arg)
     if rc != 0:
         raise RuntimeError("oracle path tracer rejected the scene")
     return (out, counts) if return_counts else out

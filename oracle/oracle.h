@@ -94,14 +94,22 @@ int  orc_ray_triangle(const double* o, const double* d, const double* v0, const 
  * samples each crop pixel took.
  *   envi:   2 int32 (environment spectrum or -1, visible)
  *   cie:    3 x 81 doubles, the reference's CIE 1931 table (x, y, z bars)
+ *   env_image: an image environment (replaces the uniform sky) or null
  * Returns 0 on success. */
+typedef struct {
+    const float* rgb;        /* width x height x 3 linear Rec.709, rows top to bottom */
+    int32_t width, height;
+    double scale;            /* radiance_scale */
+    double orient_rad[3];    /* radiance_orient, radians */
+    const float* uplift;     /* the Jakob-Hanika table, 3 x 64^3 x 3 floats */
+} OrcEnvImage;
 int orc_pt_render(const float* tri9, int64_t n_tri, const int64_t* meshes, int32_t n_mesh,
                   const float* spectra, int32_t n_spec, const int32_t* mats_i, const float* mats_f,
                   int32_t n_mat, const int32_t* envi, const double* cam, const double* setd,
                   const int32_t* seti, int32_t spp, int32_t sample_begin, int32_t x0, int32_t y0,
                   int32_t x1, int32_t y1, int32_t threads, double* xyz, const double* cie,
                   int32_t* counts, int32_t n_point, const double* points,
-                  const float* nrm9);
+                  const float* nrm9, const OrcEnvImage* env_image);
 
 /* Building blocks of the path-tracing oracle, exported so tests can hold each
  * against the reference's own code (oracle/_ref/libref_pt.so). */

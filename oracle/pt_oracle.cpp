@@ -532,7 +532,204 @@ inline unsigned OctEncode(float x, float y, float z)
     return ((unsigned)qu & 0xffffu) | ((unsigned)qv << 16);
 }
 
+// The image environment (a radiance_map bound to an HDR texture painter),
+// restated in FP64: Rendering/RadianceMap.h (light-probe mapping, rotation
+// XRotation * YRotation * ZRotation applied as Vector3Ops::Transform),
+// RasterImages/BilinRasterImageAccessor.h GetPel (u = s W + 1/2, v = t H +
+// 1/2, clamp to edge), Painters/TexturePainter.cpp:200-240 with
+// Utilities/Color/RGBSpectra.h:81-100 (unbounded uplift per lookup from the
+// Jakob-Hanika table, RGBToSpectrumTable.cpp:161-243), and
+// Rendering/EnvironmentSampler.cpp (64 x 64 tables weighted by max channel x
+// sin(theta) / theta, Sample / Pdf with theta / (4 pi^2 sin theta)).
+struct EnvImage {
+    const float* rgb = nullptr;   // w x h x 3, rows top to bottom
+    int w = 0, h = 0;
+    double scale = 1.0;
+    double rot[3][3];             // world -> map: map_i = sum_j rot[i][j] world_j
+    const float* table = nullptr; // 3 x 64^3 x 3 sigmoid coefficients
+    std::vector<double> marg, cond;   // 65, 64 x 65
+
+    void Rotation(const double o[3])
+    {
+        // Matrix4 storage _rc, XRotation / YRotation / ZRotation, product
+        // ret._rc = sum_k a._kc b._rk, Transform out_c = sum_r m._rc v_r.
+        auto ident = [](double m[4][4]) {
+            for (int i = 0; i < 4; ++i)
+                for (int j = 0; j < 4; ++j) m[i][j] = i == j;
+        };
+        double X[4][4], Y[4][4], Z[4][4];
+        ident(X); ident(Y); ident(Z);
+        X[1][1] = std::cos(o[0]); X[1][2] = std::sin(o[0]); X[2][1] = -std::sin(o[0]); X[2][2] = std::cos(o[0]);
+        Y[2][2] = std::cos(o[1]); Y[2][0] = std::sin(o[1]); Y[0][2] = -std::sin(o[1]); Y[0][0] = std::cos(o[1]);
+        Z[0][0] = std::cos(o[2]); Z[0][1] = std::sin(o[2]); Z[1][0] = -std::sin(o[2]); Z[1][1] = std::cos(o[2]);
+        auto mul = [](const double a[4][4], const double b[4][4], double r[4][4]) {
+            for (int rr = 0; rr < 4; ++rr)
+                for (int c = 0; c < 4; ++c) {
+                    double t = 0;
+                    for (int k = 0; k < 4; ++k) t += a[k][c] * b[rr][k];
+                    r[rr][c] = t;
+                }
+        };
+        double XY[4][4], M[4][4];
+        mul(X, Y, XY);
+        mul(XY, Z, M);
+        for (int c = 0; c < 3; ++c)
+            for (int r = 0; r < 3; ++r) rot[c][r] = M[r][c];
+    }
+    void Bilinear(double s, double t, double out[3]) const
+    {
+        if (!std::isfinite(s) || !std::isfinite(t)) { out[0] = out[1] = out[2] = 0; return; }
+        double u = std::min(std::max(s * w + 0.5, 0.0), (double)(w - 1));
+        double v = std::min(std::max(t * h + 0.5, 0.0), (double)(h - 1));
+        const double ulo = std::floor(u), vlo = std::floor(v), ut = u - ulo, vt = v - vlo;
+        const int xlo = (int)ulo, ylo = (int)vlo, xhi = std::min(xlo + 1, w - 1), yhi = std::min(ylo + 1, h - 1);
+        auto px = [&](int x, int y, int k) { return (double)rgb[3 * ((size_t)y * w + x) + k]; };
+        for (int k = 0; k < 3; ++k)
+            out[k] = px(xlo, ylo, k) * ((1 - ut) * (1 - vt)) + px(xlo, yhi, k) * ((1 - ut) * vt) +
+                     px(xhi, ylo, k) * (ut * (1 - vt)) + px(xhi, yhi, k) * (ut * vt);
+    }
+    static void ProbeST(const double m[3], double& s, double& t)
+    {
+        const double den = std::sqrt(m[0] * m[0] + m[1] * m[1]);
+        if (den < 1e-12) { s = t = 0.5; return; }
+        const double r = 0.159154943 * std::acos(std::max(-1.0, std::min(1.0, -m[2]))) / den;
+        s = 0.5 + m[0] * r;
+        t = 0.5 - m[1] * r;
+    }
+    static double Jacobian(double s, double t)
+    {
+        const double dx = s - 0.5, dy = -(t - 0.5), rt = std::sqrt(dx * dx + dy * dy), th = rt * 2 * kPi;
+        if (th < 1e-6 || rt > 0.5) return 1.0 / (4 * kPi);
+        const double st = std::sin(th);
+        if (st < 1e-10) return 0.0;
+        return th / (4 * kPi * kPi * st);
+    }
+    void ToMap(V d, double m[3]) const
+    {
+        const double w3[3] = {d.x, d.y, d.z};
+        for (int i = 0; i < 3; ++i) m[i] = rot[i][0] * w3[0] + rot[i][1] * w3[1] + rot[i][2] * w3[2];
+    }
+    // Coefficients and scale of the radiance spectrum in world direction d.
+    void Lookup(V d, double c[3], double& sc) const
+    {
+        double m[3], s, t, px[3];
+        ToMap(d, m);
+        ProbeST(m, s, t);
+        Bilinear(s, t, px);
+        const double mx = std::max(px[0], std::max(px[1], px[2]));
+        c[0] = c[1] = c[2] = 0.0;
+        if (mx > 1e-9) Uplift(px[0] / mx, px[1] / mx, px[2] / mx, c);
+        sc = mx * scale;
+    }
+    void Uplift(double r, double g, double b, double c[3]) const
+    {
+        constexpr int R = 64;
+        r = std::min(std::max(r, 0.0), 1.0); g = std::min(std::max(g, 0.0), 1.0); b = std::min(std::max(b, 0.0), 1.0);
+        int mc; double z, x, y;
+        if (r >= g && r >= b) { mc = 0; z = r; x = z > 1e-9 ? g / z : 0; y = z > 1e-9 ? b / z : 0; }
+        else if (g >= r && g >= b) { mc = 1; z = g; x = z > 1e-9 ? b / z : 0; y = z > 1e-9 ? r / z : 0; }
+        else { mc = 2; z = b; x = z > 1e-9 ? r / z : 0; y = z > 1e-9 ? g / z : 0; }
+        const double fz = std::min(std::max(std::asin(std::sqrt(std::min(std::max(z, 0.0), 1.0))) * (2 / kPi) * (R - 1), 0.0), (double)(R - 1));
+        const double fx = std::min(std::max(x * (R - 1), 0.0), (double)(R - 1)), fy = std::min(std::max(y * (R - 1), 0.0), (double)(R - 1));
+        const int iz = (int)fz, ix = (int)fx, iy = (int)fy;
+        const double tz = fz - iz, tx = fx - ix, ty = fy - iy;
+        auto cell = [&](int zz, int xx, int yy, int k) {
+            zz = std::min(zz, R - 1); xx = std::min(xx, R - 1); yy = std::min(yy, R - 1);
+            return (double)table[3 * ((((size_t)mc * R + zz) * R + xx) * R + yy) + k];
+        };
+        for (int k = 0; k < 3; ++k) {
+            const double a00 = cell(iz, ix, iy, k) + (cell(iz, ix + 1, iy, k) - cell(iz, ix, iy, k)) * tx;
+            const double a01 = cell(iz + 1, ix, iy, k) + (cell(iz + 1, ix + 1, iy, k) - cell(iz + 1, ix, iy, k)) * tx;
+            const double a10 = cell(iz, ix, iy + 1, k) + (cell(iz, ix + 1, iy + 1, k) - cell(iz, ix, iy + 1, k)) * tx;
+            const double a11 = cell(iz + 1, ix, iy + 1, k) + (cell(iz + 1, ix + 1, iy + 1, k) - cell(iz + 1, ix, iy + 1, k)) * tx;
+            const double b0 = a00 + (a10 - a00) * ty, b1 = a01 + (a11 - a01) * ty;
+            c[k] = b0 + (b1 - b0) * tz;
+        }
+    }
+    static double Spectrum(const double c[3], double sc, double nm)
+    {
+        if (nm < 380.0 || nm > 780.0) return 0.0;
+        const double t = (nm - 380.0) / 400.0, x = c[0] * t * t + c[1] * t + c[2];
+        return sc * (0.5 + x / (2.0 * std::sqrt(1.0 + x * x)));
+    }
+    void Build()
+    {
+        constexpr int R = 64;
+        cond.assign((size_t)R * (R + 1), 0.0);
+        marg.assign(R + 1, 0.0);
+        for (int v = 0; v < R; ++v) {
+            double* row = &cond[(size_t)v * (R + 1)];
+            for (int u = 0; u < R; ++u) {
+                const double s = (u + 0.5) / R, t = (v + 0.5) / R;
+                double px[3];
+                Bilinear(s, t, px);
+                const double lum = std::max(px[0], std::max(px[1], px[2])) * scale;
+                const double dx = s - 0.5, dy = -(t - 0.5), rt = std::sqrt(dx * dx + dy * dy), th = rt * 2 * kPi;
+                double wgt = th < 1e-6 ? 1.0 : std::sin(th) / th;
+                if (rt > 0.5) wgt = 0.0;
+                row[u + 1] = row[u] + lum * wgt;
+            }
+        }
+        for (int v = 0; v < R; ++v) marg[v + 1] = marg[v] + cond[(size_t)v * (R + 1) + R];
+        const double tot = marg[R];
+        if (!(tot > 0)) return;
+        for (int v = 0; v < R; ++v) {
+            double* row = &cond[(size_t)v * (R + 1)];
+            const double rt = row[R];
+            if (rt > 0)
+                for (int u = 0; u <= R; ++u) row[u] /= rt;
+            row[R] = 1.0;
+        }
+        for (double& m : marg) m /= tot;
+        marg[R] = 1.0;
+    }
+    static int SampleCdf(const double* cdf, int n, double xi, double& frac)
+    {
+        int lo = 0, hi = n;
+        while (lo + 1 < hi) {
+            const int mid = (lo + hi) / 2;
+            if (cdf[mid] <= xi) lo = mid; else hi = mid;
+        }
+        const double wd = cdf[lo + 1] - cdf[lo];
+        frac = wd > 0 ? (xi - cdf[lo]) / wd : 0.0;
+        return lo;
+    }
+    double Sample(double u1, double u2, V& d) const
+    {
+        constexpr int R = 64;
+        double fv, fu;
+        const int v = SampleCdf(marg.data(), R, u2, fv);
+        const double* row = &cond[(size_t)v * (R + 1)];
+        const int u = SampleCdf(row, R, u1, fu);
+        const double s = (u + fu) / R, t = (v + fv) / R;
+        const double dx = s - 0.5, dy = -(t - 0.5), rt = std::sqrt(dx * dx + dy * dy);
+        double m[3] = {0, 0, -1};
+        if (rt >= 1e-12) {
+            const double th = rt * 2 * kPi;
+            m[0] = dx * std::sin(th) / rt;
+            m[1] = dy * std::sin(th) / rt;
+            m[2] = -std::cos(th);
+        }
+        d = {rot[0][0] * m[0] + rot[1][0] * m[1] + rot[2][0] * m[2], rot[0][1] * m[0] + rot[1][1] * m[1] + rot[2][1] * m[2],
+             rot[0][2] * m[0] + rot[1][2] * m[1] + rot[2][2] * m[2]};
+        return (marg[v + 1] - marg[v]) * R * (row[u + 1] - row[u]) * R * Jacobian(s, t);
+    }
+    double Pdf(V d) const
+    {
+        constexpr int R = 64;
+        double m[3], s, t;
+        ToMap(d, m);
+        ProbeST(m, s, t);
+        s = std::max(0.0, std::min(0.999999, s));
+        t = std::max(0.0, std::min(0.999999, t));
+        const int u = std::min((int)(s * R), R - 1), v = std::min((int)(t * R), R - 1);
+        const double* row = &cond[(size_t)v * (R + 1)];
+        return (marg[v + 1] - marg[v]) * R * (row[u + 1] - row[u]) * R * Jacobian(s, t);
+    }
+};
+
 struct Scene {
+    EnvImage envImg;                       // used when envImg.rgb is set
     const float* tri9;
     const float* nrm9 = nullptr;           // vertex normals per triangle corner, or null (face normals)
     std::vector<unsigned> octN;            // their encodings, 3 per triangle (all zero: a flat triangle)
@@ -815,7 +1012,16 @@ void Sample(const Scene& S, uint32_t pixel, uint32_t sample, double xyz[3])
         double t;
         const int prim = orc_closest_d(S.bvh, od, dd, &t);
         if (prim < 0) {
-            if (S.env >= 0 && (depth > 0 || S.envVisible)) {
+            if (S.envImg.rgb && (depth > 0 || S.envVisible)) {
+                double c[3], sc, w = 1.0;
+                S.envImg.Lookup(d, c, sc);
+                if (bsdfPdf > 0) {
+                    const double ep = S.envImg.Pdf(d);
+                    if (ep > 0) w = PowerHeuristic(bsdfPdf, ep);
+                }
+                for (int k = 0; k < 4; ++k)
+                    if (live(k)) L[k] += thr[k] * EnvImage::Spectrum(c, sc, lam[k]) * w;
+            } else if (S.env >= 0 && (depth > 0 || S.envVisible)) {
                 const double w = bsdfPdf > 0 ? PowerHeuristic(bsdfPdf, kInv4Pi) : 1.0;
                 for (int k = 0; k < 4; ++k)
                     if (live(k)) L[k] += thr[k] * Spec(S, S.env, lam[k]) * w;
@@ -1001,19 +1207,30 @@ void Sample(const Scene& S, uint32_t pixel, uint32_t sample, double xyz[3])
                         rng.skip(3);
                     }
                 }
-                if (S.env >= 0) {
+                if (S.env >= 0 || S.envImg.rgb) {
+                    // Environment NEE (LightSampler.cpp:2271-2359): the image's
+                    // importance tables, or uniform directions for a uniform sky.
                     const double u1 = rng.next(20 + 2 * k), u2 = rng.next(21 + 2 * k);
-                    const double z = 1.0 - 2.0 * u1, rr = std::sqrt(std::max(0.0, 1.0 - z * z));
-                    const V dir = {rr * std::cos(2.0 * kPi * u2), rr * std::sin(2.0 * kPi * u2), z};
+                    V dir;
+                    double epdf, ec[3] = {0, 0, 0}, esc = 0;
+                    if (S.envImg.rgb) {
+                        epdf = S.envImg.Sample(u1, u2, dir);
+                        if (epdf > 0) S.envImg.Lookup(dir, ec, esc);
+                    } else {
+                        const double z = 1.0 - 2.0 * u1, rr = std::sqrt(std::max(0.0, 1.0 - z * z));
+                        dir = {rr * std::cos(2.0 * kPi * u2), rr * std::sin(2.0 * kPi * u2), z};
+                        epdf = kInv4Pi;
+                    }
                     const double cosE = Dot(dir, ns);
                     const double pd[3] = {p.x, p.y, p.z}, ed[3] = {dir.x, dir.y, dir.z};
-                    if (cosE > 0 && !orc_any_d(S.bvh, pd, ed, 1e300)) {
+                    if (cosE > 0 && epdf > 0 && !orc_any_d(S.bvh, pd, ed, 1e300)) {
                         for (int j = 0; j < 4; ++j) {
                             if ((S.neePerLambda && j != k) || !live(j)) continue;
                             double f, pb;
                             EvalBsdf(S, mat, lam[j], ns, gnv, r, dir, f, pb);
-                            const double w = pb > 0 ? PowerHeuristic(kInv4Pi, pb) : 1.0;
-                            L[j] += thr[j] * Spec(S, S.env, lam[j]) * f * cosE / kInv4Pi * w;
+                            const double w = pb > 0 ? PowerHeuristic(epdf, pb) : 1.0;
+                            const double le = S.envImg.rgb ? EnvImage::Spectrum(ec, esc, lam[j]) : Spec(S, S.env, lam[j]);
+                            L[j] += thr[j] * le * f * cosE / epdf * w;
                         }
                     }
                 }
@@ -1326,11 +1543,21 @@ extern "C" int orc_pt_render(const float* tri9, int64_t n_tri, const int64_t* me
                              int32_t n_mat, const int32_t* envi, const double* cam, const double* setd,
                              const int32_t* seti, int32_t spp, int32_t sample_begin, int32_t x0, int32_t y0,
                              int32_t x1, int32_t y1, int32_t threads, double* xyz, const double* cie,
-                             int32_t* counts, int32_t n_point, const double* points, const float* nrm9)
+                             int32_t* counts, int32_t n_point, const double* points, const float* nrm9,
+                             const OrcEnvImage* env_image)
 {
     (void)n_spec;
     GetTables();
     Scene S;
+    if (env_image && env_image->rgb) {
+        S.envImg.rgb = env_image->rgb;
+        S.envImg.w = env_image->width;
+        S.envImg.h = env_image->height;
+        S.envImg.scale = env_image->scale;
+        S.envImg.table = env_image->uplift;
+        S.envImg.Rotation(env_image->orient_rad);
+        S.envImg.Build();
+    }
     S.tri9 = tri9;
     S.nrm9 = nrm9;
     if (nrm9) {

@@ -78,6 +78,15 @@ struct rtb200_scene {
     bool mixed_shading = false;      // materials of more than one shading class
     int shade_class = -1;            // otherwise the one class (RTB200_MAT_* type), set at commit
     int32_t env = -1, env_visible = 1;
+    // Image environment (rtb200_scene_set_environment_map): RGB texels, the
+    // world -> map rotation, radiance scale, importance-sampling tables.
+    std::vector<float4> env_texels;
+    int env_w = 0, env_h = 0;
+    float env_rot[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
+    float env_scale = 1.0f;
+    std::vector<float> env_marginal, env_conditional;
+    void* d_env = nullptr;           // one block: PtEnvMap, texels, tables, uplift table
+    size_t env_bytes = 0;
     std::vector<rtb200::PtLight> lights;        // built at commit
     std::vector<rtb200::PtLightTri> light_tris;
     // device copies (path tracer)
@@ -136,6 +145,11 @@ bool RisemeshTriangles(const rtb200_risemesh* m, std::vector<float>& xyz, std::v
 const std::vector<rtb200::Node2>* RisemeshBvh(const rtb200_risemesh* m, const std::vector<uint32_t>** prims);
 bool RisemeshDoubleSided(const rtb200_risemesh* m);
 bool RisemeshNormals(const rtb200_risemesh* m, std::vector<float>& nrm, std::vector<uint32_t>& tri_nrm);
+// Image environments (envmap.cpp) and the RGB uplift table (rgb_uplift.cpp).
+void EnvRotation(const double orient_rad[3], float rot[9]);
+void BuildEnvTables(const std::vector<float4>& texels, int width, int height, float scale,
+                    std::vector<float>& marginal, std::vector<float>& conditional);
+const std::vector<float>& UpliftTable();
 
 int CudaCheck(rtb200_ctx* ctx, cudaError_t e, const char* what);
 

@@ -125,6 +125,7 @@ struct rtb200_engine {
     bool gspill = false;
     const rtb200_scene* gscene = nullptr;  // the shared scene, or null when jobs differ
     bool gclassify = false;
+    bool genv_image = false;
     int gshade_class = -1;
     long long seg_seen = 0, shadow_seen = 0;
 };
@@ -140,8 +141,10 @@ PtLaunch MakeLaunch(const rtb200_engine* e)
     L.spill = false;
     L.uniform = !e->active.empty();
     L.classify = false;
+    L.env_image = false;
     L.shade_class = e->active.empty() ? -1 : e->owner[e->active[0]]->scene->shade_class;
     for (int k : e->active) {
+        L.env_image |= e->owner[k]->scene->d_env != nullptr;
         L.spill |= e->owner[k]->scene->stack_bound > kTraceStackShared;
         L.classify |= e->owner[k]->scene->mixed_shading;
         L.uniform &= e->owner[k]->scene == e->owner[e->active[0]]->scene;
@@ -256,7 +259,7 @@ int EngineSubmit(rtb200_engine* e, rtb200_job* j, int spp)
     PtJobDev& d = e->h_table[entry];
     d.scene = PtScene{s->d_nodes, s->layout, (int)s->n_nodes, s->d_tris, (int)s->tri_material.size(), s->d_attr, s->d_mats,
                       s->d_spectra, s->d_lights, s->d_light_tris, s->d_light_nodes, s->d_light_alias,
-                      s->d_tri_normals};
+                      s->d_tri_normals, (const PtEnvMap*)s->d_env};
     d.cam = j->cam;
     d.set = j->set;
     int npx = j->npix;
@@ -325,7 +328,8 @@ int EngineStep(rtb200_engine* e, int iterations, bool graph)
     if (graph) {
         const rtb200_scene* us = L.uniform ? e->owner[e->active[0]]->scene : nullptr;
         if (!e->ggraph || e->glayout != L.layout || e->gspill != L.spill ||
-            e->gscene != us || e->gclassify != L.classify || e->gshade_class != L.shade_class) {
+            e->gscene != us || e->gclassify != L.classify || e->gshade_class != L.shade_class ||
+            e->genv_image != L.env_image) {
             DropGraph(e);
             cudaGraph_t g = nullptr;
             err = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
@@ -345,6 +349,7 @@ int EngineStep(rtb200_engine* e, int iterations, bool graph)
             e->gspill = L.spill;
             e->gscene = us;
             e->gclassify = L.classify;
+            e->genv_image = L.env_image;
             e->gshade_class = L.shade_class;
         }
         const int reps = (iterations + kGraphIters - 1) / kGraphIters;

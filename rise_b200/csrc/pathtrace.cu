@@ -23,6 +23,7 @@
 
 #include "bsdf.cuh"
 #include "core.h"
+#include "env_map.h"
 #include "pathtrace.h"
 #include "pt_device.cuh"
 #include "raycast.cuh"
@@ -107,6 +108,16 @@ __device__ float LightBvhPdf(const PtLightNode* __restrict__ nodes, int pos, V3 
         }
     }
     return 0.0f;
+}
+
+// ---- image environment (env_map.h), out of line: rarely taken, and inlined
+// it would add to the shading kernels' register pressure ----------------------
+
+__device__ __noinline__ EnvSpec EnvLookupAt(const PtEnvMap* E, V3 d) { return EnvLookup(*E, d.x, d.y, d.z); }
+__device__ __noinline__ float EnvPdfAt(const PtEnvMap* E, V3 d) { return EnvPdf(*E, d.x, d.y, d.z); }
+__device__ __noinline__ float EnvSampleAt(const PtEnvMap* E, float u1, float u2, V3& d)
+{
+    return EnvSample(*E, u1, u2, d.x, d.y, d.z);
 }
 
 // ---- film ------------------------------------------------------------------
@@ -537,7 +548,8 @@ KClassify(const PtJobDev* __restrict__ jobs, PtPaths P, PtQueues Q)
 // out and the kernel needs fewer registers; the paths come from KClassify's
 // queue of that class (from_class) or, for scenes of one class, straight from
 // the active queue.  CLS = -1 shades any material from the active queue.
-template <int CLS>
+// ENV: compiled with the image-environment code (some job's scene has one).
+template <int CLS, bool ENV>
 __global__ void __launch_bounds__(kShadeBlock, CLS == 1 || CLS < 0 ? 2 : 3)
 KShade(const PtJobDev* __restrict__ jobs, PtPaths P, PtQueues Q, int from_class)
 {
@@ -568,8 +580,19 @@ KShade(const PtJobDev* __restrict__ jobs, PtPaths P, PtQueues Q, int from_class)
         do {
             if (hslot < 0) {
                 // Escaped: uniform sky (IntegrateRayHWSS :5076-5120 for camera
-                // rays; :4235-4303 with MIS against sky NEE for continuations).
-                if (set.env >= 0 && (depth > 0 || set.env_visible)) {
+                // rays; :4235-4303 with MIS against sky NEE for continuations),
+                // or the image environment, weighted against its
+                // importance sampling by EnvironmentSampler::Pdf (:4255-4283).
+                if (ENV && S.env_map && (depth > 0 || set.env_visible)) {
+                    const EnvSpec es = EnvLookupAt(S.env_map, d);
+                    float w = 1.0f;
+                    if (bsdfPdf > 0.0f) {
+                        const float ep = EnvPdfAt(S.env_map, d);
+                        if (ep > 0.0f) w = PowerHeuristic(bsdfPdf, ep);
+                    }
+                    for (int k = 0; k < 4; ++k)
+                        if (!(term & (1u << k))) Set(L, k, Get(L, k) + Get(thr, k) * EnvSpectrum(es, lam[k]) * w);
+                } else if (set.env >= 0 && (depth > 0 || set.env_visible)) {
                     const float w = bsdfPdf > 0.0f ? PowerHeuristic(bsdfPdf, kInv4Pi) : 1.0f;
                     for (int k = 0; k < 4; ++k)
                         if (!(term & (1u << k)))
@@ -816,18 +839,29 @@ KShade(const PtJobDev* __restrict__ jobs, PtPaths P, PtQueues Q, int from_class)
                             rng.skip(3);
                         }
                     }
-                    if (set.env >= 0) {
-                        // Uniform-sky NEE: uniform directions, pdf 1/(4 pi)
-                        // (LightSampler.cpp:2277-2359).
+                    if (set.env >= 0 || (ENV && S.env_map)) {
+                        // Environment NEE (LightSampler.cpp:2271-2359): the
+                        // image environment's importance table
+                        // (EnvironmentSampler::Sample), or for a uniform sky
+                        // uniform directions with pdf 1/(4 pi).
                         const float u1 = rng.next(20 + 2 * k);
                         const float u2 = rng.next(21 + 2 * k);
-                        const float z = 1.0f - 2.0f * u1;
-                        const float rr = sqrtf(fmaxf(0.0f, 1.0f - z * z));
-                        float sp, cp;
-                        __sincosf(2.0f * kPi * u2, &sp, &cp);
-                        const V3 dir = mk(rr * cp, rr * sp, z);
+                        V3 dir;
+                        float epdf;
+                        EnvSpec es{0.0f, 0.0f, 0.0f, 0.0f};
+                        if (ENV && S.env_map) {
+                            epdf = EnvSampleAt(S.env_map, u1, u2, dir);
+                            if (epdf > 0.0f) es = EnvLookupAt(S.env_map, dir);
+                        } else {
+                            const float z = 1.0f - 2.0f * u1;
+                            const float rr = sqrtf(fmaxf(0.0f, 1.0f - z * z));
+                            float sp, cp;
+                            __sincosf(2.0f * kPi * u2, &sp, &cp);
+                            dir = mk(rr * cp, rr * sp, z);
+                            epdf = kInv4Pi;
+                        }
                         const float cosE = dot(dir, ns);
-                        if (cosE > 0.0f) {
+                        if (cosE > 0.0f && epdf > 0.0f) {
                             float4 c = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
                             bool any = false;
                             const GgxPair bq = NeePair(mtype, gp, ns, gnv, r, dir);
@@ -837,8 +871,10 @@ KShade(const PtJobDev* __restrict__ jobs, PtPaths P, PtQueues Q, int from_class)
                                 if (term & (1u << j)) continue;
                                 if (set.nee_per_lambda && j != k) continue;
                                 const float f = NeeValue(mtype, M, S.spectra, lam[j], bq, gp.eavg);
-                                const float w = pb > 0.0f ? PowerHeuristic(kInv4Pi, pb) : 1.0f;
-                                const float v = Get(thr, j) * Spec(S.spectra, set.env, lam[j]) * f * cosE / kInv4Pi * w;
+                                const float w = pb > 0.0f ? PowerHeuristic(epdf, pb) : 1.0f;
+                                const float le = (ENV && S.env_map) ? EnvSpectrum(es, lam[j])
+                                                                    : Spec(S.spectra, set.env, lam[j]);
+                                const float v = Get(thr, j) * le * f * cosE / epdf * w;
                                 Set(c, j, v);
                                 any |= v != 0.0f;
                             }
@@ -1126,6 +1162,14 @@ cudaError_t PtSetGgxTables(const float* ess, const float* eavg, const float* msz
     return e;
 }
 
+template <int CLS>
+void LaunchShade(const PtLaunch& L, int from_class, cudaStream_t st)
+{
+    const int grid = L.sms * 8;
+    if (L.env_image) KShade<CLS, true><<<grid, kShadeBlock, 0, st>>>(L.jobs, L.paths, L.queues, from_class);
+    else KShade<CLS, false><<<grid, kShadeBlock, 0, st>>>(L.jobs, L.paths, L.queues, from_class);
+}
+
 cudaError_t PtIteration(const PtLaunch& L, int iter, cudaStream_t st)
 {
     const int shadeGrid = L.sms * 8;
@@ -1137,17 +1181,19 @@ cudaError_t PtIteration(const PtLaunch& L, int iter, cudaStream_t st)
     else LaunchTrace<GpuNode4>(L, st, true);
     if (L.classify) {
         KClassify<<<shadeGrid, kShadeBlock, 0, st>>>(L.jobs, L.paths, L.queues);
-        KShade<0><<<shadeGrid, kShadeBlock, 0, st>>>(L.jobs, L.paths, L.queues, 1);
-        KShade<1><<<shadeGrid, kShadeBlock, 0, st>>>(L.jobs, L.paths, L.queues, 1);
-        KShade<2><<<shadeGrid, kShadeBlock, 0, st>>>(L.jobs, L.paths, L.queues, 1);
+        LaunchShade<0>(L, 1, st);
+        LaunchShade<1>(L, 1, st);
+        // Dielectrics shade neither escaped rays nor next events.
+        KShade<2, false><<<shadeGrid, kShadeBlock, 0, st>>>(L.jobs, L.paths, L.queues, 1);
     } else if (L.shade_class == 0) {
-        KShade<0><<<shadeGrid, kShadeBlock, 0, st>>>(L.jobs, L.paths, L.queues, 0);
+        LaunchShade<0>(L, 0, st);
     } else if (L.shade_class == 1) {
-        KShade<1><<<shadeGrid, kShadeBlock, 0, st>>>(L.jobs, L.paths, L.queues, 0);
+        LaunchShade<1>(L, 0, st);
     } else if (L.shade_class == 2) {
-        KShade<2><<<shadeGrid, kShadeBlock, 0, st>>>(L.jobs, L.paths, L.queues, 0);
+        // A dielectric-only scene: this kernel also shades the escaped rays.
+        LaunchShade<2>(L, 0, st);
     } else {
-        KShade<-1><<<shadeGrid, kShadeBlock, 0, st>>>(L.jobs, L.paths, L.queues, 0);
+        LaunchShade<-1>(L, 0, st);
     }
     if (L.layout == RTB200_BVH_Q8) LaunchTrace<QNode4>(L, st, false);
     else if (L.layout == RTB200_BVH_F16) LaunchTrace<HNode4>(L, st, false);

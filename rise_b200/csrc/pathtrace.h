@@ -18,6 +18,7 @@ struct PtLaunch {
     bool uniform;      // every job renders `scene`
     bool classify;     // some job's scene mixes shading classes: sort paths before shading
     int shade_class;   // without sorting: the one shading class of every job's scene, or -1
+    bool env_image;    // some job's scene has an image environment (shading kernels carry its code)
     PtScene scene;
     PtPaths paths;
     PtQueues queues;

@@ -10,6 +10,7 @@
 
 #include "cie1931.h"
 #include "core.h"
+#include "env_map.h"
 #include "ggx_tables.h"
 #include "pathtrace.h"
 
@@ -132,6 +133,47 @@ std::vector<PtLightAlias> BuildAlias(const std::vector<double>& w)
 }
 
 }  // namespace
+
+// The image environment as one device block: the PtEnvMap descriptor, its
+// texels, the sampling tables and the RGB uplift table, 16-byte aligned.
+int UploadEnv(rtb200_scene* s, size_t& total)
+{
+    rtb200_ctx* ctx = s->ctx;
+    const std::vector<float>& up = UpliftTable();
+    auto al = [](size_t b) { return (b + 255) & ~size_t(255); };
+    const size_t o_tex = al(sizeof(PtEnvMap));
+    const size_t o_marg = o_tex + al(s->env_texels.size() * sizeof(float4));
+    const size_t o_cond = o_marg + al(s->env_marginal.size() * sizeof(float));
+    const size_t o_up = o_cond + al(s->env_conditional.size() * sizeof(float));
+    const size_t bytes = o_up + al(up.size() * sizeof(float));
+    std::vector<unsigned char> host(bytes, 0);
+    void* d = nullptr;
+    int rc = DevAlloc(ctx, &d, bytes);
+    if (rc) return rc;
+    unsigned char* base = (unsigned char*)d;
+    PtEnvMap E{};
+    E.texels = (const float4*)(base + o_tex);
+    E.width = s->env_w;
+    E.height = s->env_h;
+    std::memcpy(E.rot, s->env_rot, sizeof(E.rot));
+    E.scale = s->env_scale;
+    E.marginal = (const float*)(base + o_marg);
+    E.conditional = (const float*)(base + o_cond);
+    E.uplift = (const float*)(base + o_up);
+    std::memcpy(host.data(), &E, sizeof(E));
+    std::memcpy(host.data() + o_tex, s->env_texels.data(), s->env_texels.size() * sizeof(float4));
+    std::memcpy(host.data() + o_marg, s->env_marginal.data(), s->env_marginal.size() * sizeof(float));
+    std::memcpy(host.data() + o_cond, s->env_conditional.data(), s->env_conditional.size() * sizeof(float));
+    std::memcpy(host.data() + o_up, up.data(), up.size() * sizeof(float));
+    if (cudaMemcpy(d, host.data(), bytes, cudaMemcpyHostToDevice) != cudaSuccess) {
+        DevFree(ctx, d, bytes);
+        return CudaCheck(ctx, cudaGetLastError(), "environment upload");
+    }
+    s->d_env = d;
+    s->env_bytes = bytes;
+    total += bytes;
+    return RTB200_OK;
+}
 
 int UploadShading(rtb200_scene* s)
 {
@@ -331,6 +373,7 @@ int UploadShading(rtb200_scene* s)
     if (!rc && !s->light_nodes.empty()) rc = Upload(ctx, &s->d_light_nodes, s->light_nodes, total);
     if (!rc && !s->light_alias.empty()) rc = Upload(ctx, &s->d_light_alias, s->light_alias, total);
     if (!rc && !s->tri_normals.empty()) rc = Upload(ctx, &s->d_tri_normals, s->tri_normals, total);
+    if (!rc && s->env_w > 0) rc = UploadEnv(s, total);
     s->shade_bytes = total;
     if (rc) FreeShading(s);
     return rc;
@@ -347,6 +390,9 @@ void FreeShading(rtb200_scene* s)
     DevFree(ctx, s->d_light_nodes, s->light_nodes.size() * sizeof(PtLightNode));
     DevFree(ctx, s->d_light_alias, s->light_alias.size() * sizeof(PtLightAlias));
     DevFree(ctx, s->d_tri_normals, s->tri_normals.size() * sizeof(uint4));
+    DevFree(ctx, s->d_env, s->env_bytes);
+    s->d_env = nullptr;
+    s->env_bytes = 0;
     s->d_tri_normals = nullptr;
     s->d_light_nodes = nullptr;
     s->d_light_alias = nullptr;
@@ -501,6 +547,37 @@ int rtb200_scene_add_material(rtb200_scene* s, const rtb200_material* m, int32_t
     return RTB200_OK;
 }
 
+int rtb200_scene_set_environment_map(rtb200_scene* s, const float* rgb, int32_t width, int32_t height, float scale,
+                                     const float* orientation_deg, int32_t visible)
+{
+    if (!s) return RTB200_E_INVALID;
+    std::lock_guard<std::mutex> g(s->ctx->mu);
+    if (s->committed) return SetError(s->ctx, RTB200_E_INVALID, "scene already committed");
+    if (!rgb || width <= 0 || height <= 0 || (int64_t)width * height > (1ll << 26) || !std::isfinite(scale) ||
+        scale < 0.0f)
+        return SetError(s->ctx, RTB200_E_INVALID, "bad environment map");
+    const size_t n = (size_t)width * height;
+    std::vector<float4> tex(n);
+    for (size_t i = 0; i < n; ++i) {
+        const float r = rgb[3 * i], gg = rgb[3 * i + 1], b = rgb[3 * i + 2];
+        if (!std::isfinite(r) || !std::isfinite(gg) || !std::isfinite(b))
+            return SetError(s->ctx, RTB200_E_INVALID, "environment map holds a non-finite texel");
+        tex[i] = make_float4(r, gg, b, 0.0f);
+    }
+    double orient[3] = {0.0, 0.0, 0.0};
+    if (orientation_deg)
+        for (int k = 0; k < 3; ++k) orient[k] = (double)orientation_deg[k] * (3.14159265358979323846 / 180.0);
+    s->env_texels.swap(tex);
+    s->env_w = width;
+    s->env_h = height;
+    s->env_scale = scale;
+    EnvRotation(orient, s->env_rot);
+    BuildEnvTables(s->env_texels, width, height, scale, s->env_marginal, s->env_conditional);
+    s->env = -1;
+    s->env_visible = visible ? 1 : 0;
+    return RTB200_OK;
+}
+
 int rtb200_scene_set_environment(rtb200_scene* s, int32_t spectrum, int32_t visible)
 {
     if (!s) return RTB200_E_INVALID;
@@ -510,6 +587,8 @@ int rtb200_scene_set_environment(rtb200_scene* s, int32_t spectrum, int32_t visi
         return SetError(s->ctx, RTB200_E_INVALID, "bad environment spectrum");
     s->env = spectrum;
     s->env_visible = visible ? 1 : 0;
+    s->env_texels.clear();
+    s->env_w = s->env_h = 0;
     return RTB200_OK;
 }
 

@@ -169,6 +169,8 @@ enum PtCounter : int {
     kCntCount = 16,
 };
 
+struct PtEnvMap;   // env_map.h
+
 struct PtScene {
     const void* nodes;
     int layout;
@@ -187,6 +189,9 @@ struct PtScene {
     // 16-bit components each, OctDecode in pt_device.cuh); null when no mesh
     // of the scene has normals.
     const uint4* tri_normals;
+    // Image environment (env_map.h), or null: then PtSettings::env names a
+    // uniform sky's spectrum, or none.
+    const PtEnvMap* env_map;
 };
 
 // Octahedral encoding of a unit vector (Cigolle et al., "A Survey of

@@ -223,6 +223,8 @@ inline float Lerp(float a, float b, double t) { return (float)((double)a * (1.0 
 
 }  // namespace
 
+const std::vector<float>& UpliftTable() { return Table(); }
+
 void RgbToSigmoid(const double rgb_in[3], double c[3])
 {
     const std::vector<float>& T = Table();

@@ -65,6 +65,12 @@ def upload_scene(ctx, desc, layout="f32"):
         out = ctypes.c_int32()
         check(L.rtb200_scene_add_material(s.h, ctypes.byref(cm), ctypes.byref(out)), ctx.h)
     check(L.rtb200_scene_set_environment(s.h, desc.env, desc.env_visible), ctx.h)
+    em = getattr(desc, "env_map", None)
+    if em is not None:
+        rgb = np.ascontiguousarray(em.rgb, np.float32)
+        o3 = (ctypes.c_float * 3)(*em.orient_deg)
+        check(L.rtb200_scene_set_environment_map(s.h, ctypes.c_void_p(rgb.ctypes.data), rgb.shape[1], rgb.shape[0],
+                                                 float(em.scale), o3, desc.env_visible), ctx.h)
     nrm9 = desc.nrm9 if hasattr(desc, "nrm9") else None
     for k, (first, count, mat, ds) in enumerate(desc.meshes):
         smooth = nrm9 is not None and desc._nrms[k] is not None

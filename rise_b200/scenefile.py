@@ -12,6 +12,8 @@ src/Library/Parsers/ChunkParserRegistry.cpp (defaults included):
   scene_options               -> accepted (scene_unit does not affect a pinhole camera)
   omni_light                  -> point light: position, linear RGB colour x power
                                  (ChunkParserRegistry.cpp:6855-6865, Lights/PointLight.h)
+  hdr_painter                 -> a Radiance HDR image (scale, shift; bilinear, clamp),
+                                 drawn as the rasterizer's radiance_map (scenes.EnvMap)
   uniformcolor_painter        -> scenes.rgb_spectrum (Jakob-Hanika albedo uplift of the
                                  colour in linear Rec.709; sRGB colours linearised)
   lambertian_material         -> Lambertian, reflectance painter
@@ -181,6 +183,25 @@ def _sellmeier_scalar(b1, b2, b3, c1, c2, c3):
     return fn
 
 
+def read_hdr(path):
+    """A Radiance HDR (RGBE) file as (height, width, 3) float32 linear RGB,
+    rows top to bottom (the reference's HDRReader, through rtb200_hdr_decode)."""
+    import ctypes
+    from . import _native
+    with open(path, "rb") as f:
+        data = f.read()
+    buf = np.frombuffer(data, np.uint8)
+    w, h = ctypes.c_int32(), ctypes.c_int32()
+    L = _native.lib()
+    if L.rtb200_hdr_decode(ctypes.c_void_p(buf.ctypes.data), len(buf), ctypes.byref(w), ctypes.byref(h), None):
+        raise SceneFileError(f"{path}: not a readable Radiance HDR file")
+    out = np.empty((h.value, w.value, 3), np.float32)
+    if L.rtb200_hdr_decode(ctypes.c_void_p(buf.ctypes.data), len(buf), ctypes.byref(w), ctypes.byref(h),
+                           ctypes.c_void_p(out.ctypes.data)):
+        raise SceneFileError(f"{path}: not a readable Radiance HDR file")
+    return out
+
+
 def _number(s):
     try:
         return float(s)
@@ -215,6 +236,7 @@ class _Loader:
         self.desc = scenes.SceneDesc()
         self.painters = {}       # name -> spectrum id
         self.scalars = {}        # name -> function of wavelength (nm, array) -> value
+        self.images = {}         # name -> (height, width, 3) float32 linear RGB (hdr_painter)
         self.materials = {}      # name -> (material id, kind, reflectance id)
         self.geometry = {}       # name -> ((n, 9) float64 triangles, double_sided)
         self.spp = None
@@ -284,6 +306,25 @@ class _Loader:
         sp = scenes.BlackbodySpectrum(float(c.get("temperature", 5600.0)), float(c.get("scale", 1.0)),
                                       _bool(c.get("normalize", "true")))
         self.painters[c.get("name", "noname")] = self.desc.add_spectrum(sp)
+
+    def hdr_painter(self, c):
+        # Job::AddHDRTexturePainter (Job.cpp:2216-2265): the Radiance HDR
+        # image, times `scale` then plus `shift` per channel, read with the
+        # bilinear filter (the default filter_type) and clamp-to-edge wrap.
+        self.only(c, {"name", "file", "scale", "shift", "lowmemory", "filter_type", "wrap_s", "wrap_t"})
+        if c.get("filter_type", "bilinear") not in ("bilinear", "Bilinear"):
+            self.refuse(c, "only the bilinear texture filter is supported")
+        for k in ("wrap_s", "wrap_t"):
+            if c.get(k, "clamp") != "clamp":
+                self.refuse(c, f"{k} other than clamp is not supported")
+        rgb = read_hdr(self.path(c.get("file", "none"), "hdr_painter"))
+        scale = np.array(_floats(c.get("scale", "1 1 1"), 3, "hdr_painter scale"), np.float32)
+        shift = np.array(_floats(c.get("shift", "0 0 0"), 3, "hdr_painter shift"), np.float32)
+        if np.any(scale != 1):
+            rgb = rgb * scale
+        if np.any(shift != 0):
+            rgb = rgb + shift
+        self.images[c.get("name", "noname")] = np.ascontiguousarray(rgb, np.float32)
 
     def scalar_painter(self, c):
         # Physical scalars per wavelength (ScalarPainterAsciiChunkParser,
@@ -604,7 +645,12 @@ class _Loader:
         # so the orientation does not matter), visible to camera rays when
         # radiance_background (default true).
         env = c.get("radiance_map", "none")
-        if env != "none":
+        if env in self.images:
+            self.desc.env = -1
+            self.desc.env_map = scenes.EnvMap(self.images[env], float(c.get("radiance_scale", 1.0)),
+                                              tuple(_floats(c.get("radiance_orient", "0 0 0"), 3, "radiance_orient")))
+            self.desc.env_visible = int(_bool(c.get("radiance_background", "true")))
+        elif env != "none":
             if env not in self.painters:
                 self.refuse(c, f"radiance_map {env!r}: only uniform painters (spectral_painter, "
                                "uniformcolor_painter, blackbody_painter) are supported")
@@ -622,6 +668,8 @@ class _Loader:
                 sid = self.desc.add_spectrum(sp)
             self.desc.env = sid
             self.desc.env_visible = int(_bool(c.get("radiance_background", "true")))
+            if c.get("radiance_orient", "0 0 0").split() != ["0", "0", "0"]:
+                self.notes.append(f"{c.keyword}: radiance_orient does not change a uniform painter's sky")
         # StabilityConfig::useLightBVH (default true): the light BVH, else
         # the alias table over emitted power.
         self.st["light_selection"] = 0 if _bool(c.get("light_bvh", "true")) else 1

@@ -281,6 +281,15 @@ class RenderSettings:
 
 
 @dataclass
+class EnvMap:
+    """An image environment: the rasterizer's radiance_map bound to an HDR
+    texture painter (light-probe mapping, bilinear, per-lookup RGB uplift)."""
+    rgb: np.ndarray                       # (height, width, 3) linear Rec.709, rows top to bottom
+    scale: float = 1.0                    # radiance_scale
+    orient_deg: tuple = (0.0, 0.0, 0.0)   # radiance_orient (x, y, z Euler angles)
+
+
+@dataclass
 class SceneDesc:
     tri9: np.ndarray = None
     meshes: list = field(default_factory=list)     # (first, count, material, double_sided)
@@ -288,6 +297,7 @@ class SceneDesc:
     materials: list = field(default_factory=list)  # Material
     env: int = -1
     env_visible: int = 1
+    env_map: object = None     # EnvMap: an image environment (replaces env)
     point_lights: list = field(default_factory=list)  # (position, colour, power)
     settings: RenderSettings = field(default_factory=RenderSettings)
     _tris: list = field(default_factory=list)

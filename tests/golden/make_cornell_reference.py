@@ -33,8 +33,11 @@ oracle/rise_ref.mk), on tests/golden/cornell_c1.RISEscene:
   wavelength bundles; the prism with one wavelength per path in 30 bins and
   two spectral samples per pixel sample (the prism scenes at 16 batches of 64
   samples per pixel).
+* cornell_env_ref_k16_independent.npz -- the same for
+  tests/golden/cornell_env.RISEscene (tests/golden/make_env_scene.py): a
+  scene lit only by an HDR light probe, rotated and scaled, 128 x 128.
 
-    make -C oracle && python tests/golden/make_cornell_reference.py [k16|k16i|smooth|variants|fp64]
+    make -C oracle && python tests/golden/make_cornell_reference.py [k16|k16i|smooth|variants|env|fp64]
     (k16, k16i: ~40 s each, fp64: ~45 min on 8 cores; rows are checkpointed under
     oracle/_ref/ so an interrupted run resumes)
 """
@@ -79,7 +82,7 @@ def make_fp64(r):
 
 
 def main():
-    which = sys.argv[1:] or ["k16", "k16i", "smooth", "variants", "fp64"]
+    which = sys.argv[1:] or ["k16", "k16i", "smooth", "variants", "env", "fp64"]
     r = oracle.RefRenderer(SCENE)
     if "k16" in which:
         make_k16(r)
@@ -90,6 +93,9 @@ def main():
     if "smooth" in which:
         make_k16(oracle.RefRenderer(os.path.join(HERE, "cornell_smooth.RISEscene")), independent=True,
                  name="cornell_smooth_ref_k16_independent.npz")
+    if "env" in which:
+        make_k16(oracle.RefRenderer(os.path.join(HERE, "cornell_env.RISEscene")), independent=True,
+                 name="cornell_env_ref_k16_independent.npz")
     if "variants" in which:
         # The prism's caustics make single pixels heavy-tailed; 64 samples
         # per batch bring the batch means nearer to normal for the z-test.

@@ -169,3 +169,61 @@ def test_dispersive_glass_matches_the_reference(name):
     const = dataclasses.replace(ls.desc)
     const.materials = [dataclasses.replace(m, eta=-1, ior=1.5) if m.type == 2 else m for m in ls.desc.materials]
     assert _z_rate(const, st, mr, vr, k, spp, rows, 1100)[0] > 2 * Z_ALLOWED_RATE
+
+
+def test_image_environment_matches_the_reference():
+    """A scene lit only by an HDR light probe: the angular mapping after a
+    30-degree turn about y, bilinear texels, the unbounded spectral uplift per
+    lookup, radiance scale 1.5, next events from the 64 x 64 importance
+    tables with power-heuristic MIS.  The restatement's 16 batches against
+    the reference's 16; the probe left unturned fails the same test."""
+    ls, mr, vr, k, spp = _variant("cornell_env")
+    st = ls.desc.settings
+    em = ls.desc.env_map
+    assert em is not None and em.orient_deg == (0.0, 30.0, 0.0) and em.scale == 1.5
+    rows = (0, st.height)
+    rate, g = _z_rate(ls.desc, st, mr, vr, k, spp, rows, 1300)
+    assert rate <= Z_ALLOWED_RATE, rate
+    for c in range(3):
+        se = np.sqrt(g[..., c].mean(axis=(1, 2)).var(ddof=1) / k + vr[..., c].mean() / k / g[0, ..., c].size)
+        assert abs(g[..., c].mean() - mr[..., c].mean()) < 4 * se, c
+    plain = dataclasses.replace(ls.desc, env_map=dataclasses.replace(em, orient_deg=(0.0, 0.0, 0.0)))
+    assert _z_rate(plain, st, mr, vr, k, spp, rows, 1300)[0] > 2 * Z_ALLOWED_RATE
+
+
+def test_hdr_reader_decodes_rgbe_as_the_reference(tmp_path):
+    """The probe file through rtb200_hdr_decode against a direct decode of
+    its run-length RGBE bytes: value = 2^(e - 136) (byte + 1/2), 0 for e = 0
+    (HDRReader::ReadColor); a truncated file is refused."""
+    path = os.path.join(GOLDEN, "cornell_env_probe.hdr")
+    img = scenefile.read_hdr(path)
+    data = open(path, "rb").read()
+    head = data.index(b"-Y ")
+    line_end = data.index(b"\n", head)
+    h, w = int(data[head:line_end].split()[1]), int(data[head:line_end].split()[3])
+    assert img.shape == (h, w, 3)
+    pos = line_end + 1
+    px = np.zeros((h, w, 4), np.uint8)
+    for y in range(h):
+        assert data[pos:pos + 2] == b"\x02\x02"
+        pos += 4
+        for comp in range(4):
+            x = 0
+            while x < w:
+                n = data[pos]
+                pos += 1
+                if n > 128:
+                    px[y, x:x + n - 128, comp] = data[pos]
+                    pos += 1
+                    x += n - 128
+                else:
+                    px[y, x:x + n, comp] = np.frombuffer(data[pos:pos + n], np.uint8)
+                    pos += n
+                    x += n
+    e = px[..., 3].astype(np.int32)
+    want = np.where(e[..., None] == 0, 0.0, np.ldexp(1.0, e[..., None] - 136) * (px[..., :3] + 0.5))
+    assert np.array_equal(img, want.astype(np.float32))
+    bad = tmp_path / "truncated.hdr"
+    bad.write_bytes(data[:len(data) // 2])
+    with pytest.raises(scenefile.SceneFileError):
+        scenefile.read_hdr(str(bad))
