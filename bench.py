@@ -4,9 +4,9 @@ Workload (one "step"): one pass of 4,194,304 closest-hit rays over a
 1,000,000-triangle soup (centroids uniform in the unit cube, vertices offset
 by N(0, 0.01^2); rays from a radius-2 sphere towards uniform targets in the
 cube; seed 7), through the reference's BVH (SAH 32 bins, leaf 4, collapsed to
-4-wide nodes) with 8-bit quantised child boxes (the FP32-node and
-binary16-node layouts are reported as variants; all return the same hits).
-Metric: Mrays/s.
+4-wide nodes) with FP16-quantised child boxes (binary16 rounded outward,
+the configuration's quantised format; the FP32-node and 8-bit-node layouts
+are reported as variants; all return the same hits).  Metric: Mrays/s.
 
   python bench.py [--gpus N --steps K --warmup W] [--impl reference]
 
@@ -36,8 +36,8 @@ SEED = 7
 BYTES_CLOSEST = 48  # ray in 32 B + hit out 16 B
 BYTES_ANY = 33      # ray in 32 B + occlusion flag 1 B
 WORKLOAD = ("raycast microbench: 1,000,000-triangle soup, 4,194,304 rays from a radius-2 sphere, "
-            "closest-hit, reference BVH (SAH 32 bins, leaf 4) collapsed to 4-wide nodes with 8-bit quantised "
-            "child boxes (rounded outward)")
+            "closest-hit, reference BVH (SAH 32 bins, leaf 4) collapsed to 4-wide nodes with FP16-quantised "
+            "child boxes (binary16, rounded outward)")
 METRIC = "Mrays/s"
 # The reference arm runs the reference's own BVH, whose child boxes are FP32
 # (it has no quantised node format).
@@ -418,7 +418,7 @@ def bench_batch(ctx):
 
 
 def bench_serving(ctx, rate=20.0, duration=8.0, resolutions=(128, 256), n_scenes=12, max_tri=300_000,
-                  layout="q8", timeout=600.0):
+                  layout="q8", timeout=600.0, caps=()):
     """Serving loop: Poisson arrivals, progressive 16 -> 64 -> 256 spp per
     request, scenes drawn from a resident pool of the batched-scenes
     distribution (`n_scenes` scenes of up to `max_tri` triangles at
@@ -446,6 +446,11 @@ def bench_serving(ctx, rate=20.0, duration=8.0, resolutions=(128, 256), n_scenes
         # Warm-up: first launches of every kernel instantiation serving uses.
         serving.serve(ctx, pool, make(arrivals[:12]), mode="continuous")
         out["continuous"] = serving.serve(ctx, pool, make(), mode="continuous", timeout=timeout)
+        # Continuous batching with at most `cap` requests in flight: under
+        # overload an unbounded mix interleaves every resident scene's paths.
+        for cap in caps:
+            out[f"continuous_max{cap}"] = serving.serve(ctx, pool, make(), mode="continuous", timeout=timeout,
+                                                        max_active=cap)
         out["fifo"] = serving.serve(ctx, pool, make(), mode="fifo", timeout=timeout)
     finally:
         for s in devs:
@@ -568,7 +573,7 @@ def main():
     if args.serving_full:
         ctx = raycaster.Context(local, 120 * 10**9)
         res = bench_serving(ctx, rate=20.0, duration=60.0, resolutions=scenes.RESOLUTIONS, n_scenes=48,
-                            max_tri=1_000_000, timeout=3600.0)
+                            max_tri=1_000_000, timeout=3600.0, caps=(8,))
         res["budget_bytes"] = 120 * 10**9
         print(json.dumps({"serving_full": res}))
         ctx.close()
@@ -617,17 +622,17 @@ def main():
             dist.barrier()
         torch.cuda.synchronize()
 
-    # Headline: 8-bit quantised child boxes (conservative, the same hits as
-    # FP32 nodes: tests/test_raycast_gpu.py); FP32 nodes are a variant.
+    # Headline: FP16-quantised child boxes (conservative, the same hits as
+    # FP32 nodes: tests/test_raycast_gpu.py); FP32 and 8-bit nodes are variants.
     for _ in range(max(3, args.warmup)):
-        step_closest(rq)
+        step_closest(rh)
     barrier()
     clocks = ClockSampler(local)
     clocks.start()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
     for _ in range(args.steps):
-        step_closest(rq)
+        step_closest(rh)
     e1.record(stream)
     barrier()
     clk = clocks.stop()
@@ -653,8 +658,8 @@ def main():
         return a.elapsed_time(b) / n
 
     variants = {}
-    for name, fn, rc in (("closest_f32", step_closest, rf), ("any_f32", step_any, rf), ("any_q8", step_any, rq),
-                         ("closest_f16", step_closest, rh), ("any_f16", step_any, rh)):
+    for name, fn, rc in (("closest_f32", step_closest, rf), ("any_f32", step_any, rf), ("closest_q8", step_closest, rq),
+                         ("any_q8", step_any, rq), ("any_f16", step_any, rh)):
         variants[name] = N_RAYS / (timed(fn, rc) * 1e-3) / 1e6
     hit_rate = float((d_hits[:, 1].view(torch.int32) >= 0).float().mean())
 
@@ -665,12 +670,12 @@ def main():
     from rise_b200._native import check, lib
     import ctypes
     for _ in range(2):
-        check(lib().rtb200_cast_closest(sq.h, ctypes.c_void_p(h_rays.ctypes.data), N_RAYS,
+        check(lib().rtb200_cast_closest(sh16.h, ctypes.c_void_p(h_rays.ctypes.data), N_RAYS,
                                         ctypes.c_void_p(h_hits.ctypes.data)), ctx.h)
     barrier()
     t0 = time.perf_counter()
     for _ in range(args.e2e_steps):
-        check(lib().rtb200_cast_closest(sq.h, ctypes.c_void_p(h_rays.ctypes.data), N_RAYS,
+        check(lib().rtb200_cast_closest(sh16.h, ctypes.c_void_p(h_rays.ctypes.data), N_RAYS,
                                         ctypes.c_void_p(h_hits.ctypes.data)), ctx.h)
     e2e_s = (time.perf_counter() - t0) / args.e2e_steps
     if world > 1:
@@ -681,15 +686,15 @@ def main():
 
     peak, peak_kind = load_peaks()
     achieved = BYTES_CLOSEST * N_RAYS / (ms_step * 1e-3) / 1e9
-    prof = "raycast_closest_q8_soup1M"
+    prof = "raycast_closest_f16_soup1M"
     traffic = profiled(prof, "traffic_bytes_per_launch")
-    info = sf.info()
+    info = sh16.info()
 
     out = {
         "metric": METRIC, "value": value, "unit": "Mrays/s", "n_gpus": world, "steps": args.steps,
         "warmup": max(3, args.warmup), "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded: triangles seed 7, rays seed 7 + 1000*rank)",
-        "config": {"workload": WORKLOAD, "n_tri": N_TRI, "n_rays_per_gpu": N_RAYS, "layout": "q8",
+        "config": {"workload": WORKLOAD, "n_tri": N_TRI, "n_rays_per_gpu": N_RAYS, "layout": "f16",
                    "parallelism": f"replicas x{world}",
                    "l2_policy": "inputs larger than L2 (rays 134 MB per pass); scene (nodes + triangles) stays resident",
                    "bvh_nodes": info["n_nodes"], "scene_device_bytes": info["device_bytes"],

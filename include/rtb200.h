@@ -45,6 +45,8 @@ extern "C" {
 #define RTB200_E_TIMEOUT   4  /* a bounded device wait gave up */
 #define RTB200_E_DEVICE    5  /* CUDA error or device-side error word set */
 #define RTB200_E_NOT_READY 6  /* asynchronous work still in flight */
+#define RTB200_E_CANCELLED 7  /* a progress callback stopped the render; the film
+                                 holds the pixel samples completed */
 
 /* BVH device layouts for rtb200_scene_commit. */
 #define RTB200_BVH_F32     0  /* FP32 child boxes, 128-byte 4-wide nodes */
@@ -416,6 +418,22 @@ int rtb200_job_read_sample_counts(rtb200_job* job, uint32_t* counts);
 int rtb200_job_read_rgb(rtb200_job* job, float* rgb);
 int rtb200_job_read_display(rtb200_job* job, float exposure_ev, int32_t tone, uint8_t* rgb8);
 int rtb200_job_stats(const rtb200_job* job, rtb200_stats* out);
+
+/* Progress of a render (IRasterizer::SetProgressCallback with
+ * IProgressCallback::Progress, Interfaces/IProgressCallback.h:20-50; called
+ * by PixelBasedRasterizerHelper between regions, which stops the render when
+ * it returns false, PixelBasedRasterizerHelper.cpp:1512-1530).  While
+ * rtb200_job_render or rtb200_engine_render runs, fn(user, progress, total)
+ * is called on the calling thread after every engine step with the pixel
+ * samples finished so far and asked for in this call (progress is
+ * fractional: paths finished / paths per pixel sample).  Returning 0 stops
+ * the request: no new pixel samples start, those already started finish,
+ * every pixel keeps the same whole number of samples, and the call returns
+ * RTB200_E_CANCELLED with the film holding them.  fn runs with the
+ * context's lock held and must not call into rtb200 on the same context.
+ * fn = null removes the callback. */
+typedef int32_t (*rtb200_progress_fn)(void* user, double progress, double total);
+int rtb200_job_set_progress(rtb200_job* job, rtb200_progress_fn fn, void* user);
 /* relMSE of the job's film against a reference image (width*height*3 host
  * floats, XYZ): the mean over pixels and channels of (x - r)^2 / (r^2 + 1e-2),
  * reduced on the device in FP64.  Films keep a Kahan-compensated FP32 running
@@ -453,6 +471,11 @@ int rtb200_engine_submit(rtb200_engine* engine, rtb200_job* job, int32_t spp);
 int rtb200_engine_step(rtb200_engine* engine, int32_t iterations, int32_t use_graph);
 int rtb200_engine_progress(const rtb200_engine* engine, const rtb200_job* job, int64_t* done, int64_t* total);
 int rtb200_engine_retire(rtb200_engine* engine, rtb200_job* job);
+/* Stops a submitted job's request as a progress callback returning 0 does:
+ * no new pixel samples start; after the samples started finish, progress
+ * reports done == total and the job can be retired (a served request that
+ * is abandoned or cancelled by its client). */
+int rtb200_engine_cancel(rtb200_engine* engine, rtb200_job* job);
 int rtb200_engine_destroy(rtb200_engine* engine);
 /* Wavefront iterations rtb200_engine_render runs between host polls of the
  * jobs' progress (default 4; rounded up to even, 2 .. 1024).  Fewer polls

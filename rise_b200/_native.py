@@ -11,9 +11,9 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "_lib", "librtb200.so")
 
 OK = 0
-E_INVALID, E_OOM, E_BUDGET, E_TIMEOUT, E_DEVICE, E_NOT_READY = 1, 2, 3, 4, 5, 6
+E_INVALID, E_OOM, E_BUDGET, E_TIMEOUT, E_DEVICE, E_NOT_READY, E_CANCELLED = 1, 2, 3, 4, 5, 6, 7
 STATUS_NAMES = {0: "OK", 1: "E_INVALID", 2: "E_OOM", 3: "E_BUDGET", 4: "E_TIMEOUT",
-                5: "E_DEVICE", 6: "E_NOT_READY"}
+                5: "E_DEVICE", 6: "E_NOT_READY", 7: "E_CANCELLED"}
 BVH_F32, BVH_Q8, BVH_W8, BVH_F16 = 0, 1, 2, 3
 
 _vp = ctypes.c_void_p
@@ -79,6 +79,8 @@ SIGNATURES = {
     "rtb200_engine_step": (ctypes.c_int, [_vp, _i32, _i32]),
     "rtb200_engine_progress": (ctypes.c_int, [_vp, _vp, _pi64, _pi64]),
     "rtb200_engine_retire": (ctypes.c_int, [_vp, _vp]),
+    "rtb200_engine_cancel": (ctypes.c_int, [_vp, _vp]),
+    "rtb200_job_set_progress": (ctypes.c_int, [_vp, _vp, _vp]),
     "rtb200_engine_destroy": (ctypes.c_int, [_vp]),
     "rtb200_engine_set_poll": (ctypes.c_int, [_vp, ctypes.c_int32]),
     "rtb200_job_relmse": (ctypes.c_int, [_vp, _vp, ctypes.POINTER(ctypes.c_double)]),

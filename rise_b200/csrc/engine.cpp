@@ -85,6 +85,8 @@ struct rtb200_job {
     int submitted_px = 0;              // pixels the request in flight samples
     long long spp_done = 0;
     int spectral = 1;                  // paths per pixel sample (spectral samples)
+    rtb200_progress_fn progress = nullptr;   // rtb200_job_set_progress
+    void* progress_user = nullptr;
     long long samples = 0;
     double seconds = 0.0;
     long long segments = 0, shadow_rays = 0;
@@ -395,6 +397,24 @@ int EngineStep(rtb200_engine* e, int iterations, bool graph)
 
 bool JobDone(const rtb200_engine* e, int entry) { return e->h_ctr[kMaxJobs + entry] >= e->total[entry]; }
 
+// Cuts a job's request in flight to the pixel samples already started: its
+// total becomes the paths issued so far (exact: the device is idle after a
+// step) rounded up to whole pixel samples, so every pixel ends with the same
+// count; the table change reaches the device before the next step's
+// KAssign.
+void CancelEntry(rtb200_engine* e, rtb200_job* j)
+{
+    const int entry = j->entry;
+    const unsigned long long unit = (unsigned long long)std::max(j->submitted_px, 1) * (unsigned long long)j->spectral;
+    unsigned long long t = (e->h_ctr[entry] + unit - 1) / unit * unit;
+    if (t > e->total[entry]) t = e->total[entry];
+    e->total[entry] = t;
+    e->h_table[entry].total = t;
+    e->changed.push_back(entry);
+    e->dirty = true;
+    j->pending_spp = (long long)(t / unit);
+}
+
 int EngineRetire(rtb200_engine* e, rtb200_job* j)
 {
     rtb200_ctx* ctx = e->ctx;
@@ -462,9 +482,22 @@ int EngineRender(rtb200_engine* e, rtb200_job* const* jobs, const int32_t* spp, 
     }
     cudaEventRecord(e->e0, ctx->stream);
     const long long kMaxSteps = 1ll << 18;
+    std::vector<char> cancelled((size_t)n, 0);
+    bool any_cancel = false;
     for (long long step = 0;; ++step) {
         const int rc = EngineStep(e, e->poll, graph);
         if (rc) return rc;
+        for (int i = 0; i < n; ++i) {
+            rtb200_job* j = jobs[i];
+            if (!j->progress || cancelled[i]) continue;
+            const double unit = (double)std::max(j->submitted_px, 1) * (double)j->spectral;
+            const double done = (double)e->h_ctr[kMaxJobs + j->entry] / unit, tot = (double)e->total[j->entry] / unit;
+            if (!j->progress(j->progress_user, done, tot)) {
+                CancelEntry(e, j);
+                cancelled[i] = 1;
+                any_cancel = true;
+            }
+        }
         bool all = true;
         for (int i = 0; i < n; ++i) all = all && JobDone(e, jobs[i]->entry);
         if (all) break;
@@ -479,7 +512,9 @@ int EngineRender(rtb200_engine* e, rtb200_job* const* jobs, const int32_t* spp, 
         const int rc = EngineRetire(e, jobs[i]);
         if (rc) return rc;
     }
-    return CudaCheck(ctx, cudaStreamSynchronize(ctx->stream), "film fold");
+    const int rc = CudaCheck(ctx, cudaStreamSynchronize(ctx->stream), "film fold");
+    if (rc) return rc;
+    return any_cancel ? SetError(ctx, RTB200_E_CANCELLED, "stopped by the progress callback") : RTB200_OK;
 }
 
 }  // namespace
@@ -849,6 +884,24 @@ int rtb200_engine_retire(rtb200_engine* e, rtb200_job* job)
     const int rc = EngineRetire(e, job);
     if (rc) return rc;
     return CudaCheck(e->ctx, cudaStreamSynchronize(e->ctx->stream), "film fold");
+}
+
+int rtb200_engine_cancel(rtb200_engine* e, rtb200_job* job)
+{
+    if (!e || !job) return RTB200_E_INVALID;
+    std::lock_guard<std::mutex> g(e->ctx->mu);
+    if (job->engine != e) return SetError(e->ctx, RTB200_E_INVALID, "job is not submitted to this engine");
+    CancelEntry(e, job);
+    return RTB200_OK;
+}
+
+int rtb200_job_set_progress(rtb200_job* job, rtb200_progress_fn fn, void* user)
+{
+    if (!job) return RTB200_E_INVALID;
+    std::lock_guard<std::mutex> g(job->scene->ctx->mu);
+    job->progress = fn;
+    job->progress_user = user;
+    return RTB200_OK;
 }
 
 int rtb200_engine_set_poll(rtb200_engine* e, int32_t iterations)

@@ -118,6 +118,9 @@ def bounce_limits(st):
     return (int(on),) + tuple(int(v) if v is not None else 255 for v in lim)
 
 
+PROGRESS_FN = ctypes.CFUNCTYPE(ctypes.c_int32, ctypes.c_void_p, ctypes.c_double, ctypes.c_double)
+
+
 class SpectralRasterizer:
     """One progressive spectral path-traced image of one scene."""
 
@@ -133,8 +136,25 @@ class SpectralRasterizer:
         self.h = h
 
     def rasterize_scene(self, spp):
-        """Add `spp` samples per pixel (blocking)."""
-        check(lib().rtb200_job_render(self.h, int(spp)), self.ctx.h)
+        """Add `spp` samples per pixel (blocking).  Returns False when the
+        progress callback stopped the pass (the film then holds the whole
+        pixel samples finished), else True."""
+        rc = lib().rtb200_job_render(self.h, int(spp))
+        if rc == _native.E_CANCELLED:
+            return False
+        check(rc, self.ctx.h)
+        return True
+
+    def set_progress(self, fn):
+        """fn(progress, total) -> bool, called after every engine step of a
+        render (IProgressCallback::Progress); False stops the render.  None
+        removes it."""
+        if fn is None:
+            self._progress = None
+            check(lib().rtb200_job_set_progress(self.h, None, None), self.ctx.h)
+            return
+        self._progress = PROGRESS_FN(lambda user, done, total: 1 if fn(done, total) else 0)
+        check(lib().rtb200_job_set_progress(self.h, ctypes.cast(self._progress, ctypes.c_void_p), None), self.ctx.h)
 
     def relmse(self, ref_xyz):
         """relMSE of the film against `ref_xyz` ((height, width, 3) XYZ),
@@ -212,7 +232,11 @@ class Engine:
         n = len(rasterizers)
         jobs = (ctypes.c_void_p * n)(*[r.h.value for r in rasterizers])
         counts = (ctypes.c_int32 * n)(*[int(s) for s in spp])
-        check(lib().rtb200_engine_render(self.h, jobs, counts, n, int(bool(use_graph))), self.ctx.h)
+        rc = lib().rtb200_engine_render(self.h, jobs, counts, n, int(bool(use_graph)))
+        if rc == _native.E_CANCELLED:
+            return False
+        check(rc, self.ctx.h)
+        return True
 
     def set_poll(self, iterations):
         """Wavefront iterations between host progress polls in `render`."""
@@ -232,6 +256,11 @@ class Engine:
 
     def retire(self, rasterizer):
         check(lib().rtb200_engine_retire(self.h, rasterizer.h), self.ctx.h)
+
+    def cancel(self, rasterizer):
+        """Start no more pixel samples of the job's request; retire it once
+        progress reports done == total."""
+        check(lib().rtb200_engine_cancel(self.h, rasterizer.h), self.ctx.h)
 
     def close(self):
         if self.h:

@@ -46,10 +46,12 @@ def poisson_arrivals(rate, duration, seed):
 
 
 def serve(ctx, pool, requests, mode="continuous", capacity=1 << 21, step_iters=2, use_graph=True,
-          timeout=600.0):
+          timeout=600.0, max_active=None):
     """Run `requests` (list of Request, arrival-ordered) against `pool`
     (list of (SceneDesc, committed raycaster.Scene)).  Returns a summary
-    dict with per-level latency percentiles and aggregate throughput."""
+    dict with per-level latency percentiles and aggregate throughput.
+    max_active caps the requests in flight in continuous mode (admission
+    waits for a slot; None: only the memory budget limits them)."""
     eng = Engine(ctx, capacity)
     pending = deque(sorted(requests, key=lambda r: r.arrival))
     active = []
@@ -62,7 +64,7 @@ def serve(ctx, pool, requests, mode="continuous", capacity=1 << 21, step_iters=2
             if now > timeout:
                 raise RuntimeError("serving run exceeded its time limit")
             # Admission: arrived requests whose film fits the memory budget.
-            limit = 1 if mode == "fifo" else None
+            limit = 1 if mode == "fifo" else max_active
             while pending and pending[0].arrival <= now and (limit is None or len(active) < limit):
                 r = pending[0]
                 desc, scene = pool[r.scene]
@@ -111,4 +113,4 @@ def serve(ctx, pool, requests, mode="continuous", capacity=1 << 21, step_iters=2
             lat[str(lvl)] = {"p50_s": float(np.percentile(v, 50)), "p99_s": float(np.percentile(v, 99)),
                              "mean_s": float(v.mean())}
     return {"mode": mode, "requests": len(finished), "wall_s": wall, "msamples_s": samples / wall / 1e6,
-            "latency": lat}
+            "max_active": max_active if mode == "continuous" else 1, "latency": lat}

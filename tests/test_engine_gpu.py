@@ -6,6 +6,8 @@ wavefront: the same job rendered alone, in a batch, from a captured CUDA
 graph, or submitted while other jobs are in flight gives the same image up
 to the order of floating-point film additions (relative 1e-5).
 """
+import dataclasses
+
 import numpy as np
 import pytest
 
@@ -163,3 +165,67 @@ def test_autotune_picks_a_config_and_poll_does_not_change_images(ctx):
     finally:
         for s in devs:
             s.close()
+
+
+def test_progress_callback_reports_and_can_stop_a_render(ctx):
+    """IProgressCallback semantics: progress grows to the total; a callback
+    that returns True leaves the image unchanged; one that returns False
+    stops the pass with every pixel at the same whole number of samples, so
+    the film equals an uninterrupted render of that many samples."""
+    d = scenes.cornell_box(128, 128)
+    scene = pathtracer.upload_scene(ctx, d)
+    try:
+        ref = pathtracer.SpectralRasterizer(ctx, d, scene=scene)
+        ref.rasterize_scene(64)
+        seen = []
+        r = pathtracer.SpectralRasterizer(ctx, d, scene=scene)
+        r.set_progress(lambda p, t: seen.append((p, t)) or True)
+        assert r.rasterize_scene(64)
+        assert seen and all(t == 64 for _, t in seen) and seen[-1][0] == 64
+        assert all(a[0] <= b[0] for a, b in zip(seen, seen[1:]))
+        assert np.allclose(r.film(), ref.film(), rtol=1e-5, atol=1e-7)
+        stop = pathtracer.SpectralRasterizer(ctx, d, scene=scene)
+        stop.set_progress(lambda p, t: False)
+        assert stop.rasterize_scene(4096) is False
+        k = stop.stats()["spp"]
+        assert 0 < k < 4096
+        part = pathtracer.SpectralRasterizer(ctx, d, scene=scene)
+        part.rasterize_scene(k)
+        assert np.allclose(stop.film(), part.film(), rtol=1e-5, atol=1e-7)
+        # The next pass continues from sample k.
+        stop.set_progress(None)
+        assert stop.rasterize_scene(8)
+        assert stop.stats()["spp"] == k + 8
+        for x in (ref, r, stop, part):
+            x.close()
+    finally:
+        scene.close()
+
+
+def test_engine_cancel_stops_a_served_request(ctx):
+    d = scenes.cornell_box(128, 128)
+    scene = pathtracer.upload_scene(ctx, d)
+    eng = pathtracer.Engine(ctx)
+    try:
+        a = pathtracer.SpectralRasterizer(ctx, d, scene=scene)
+        b = pathtracer.SpectralRasterizer(ctx, d, scene=scene, settings=dataclasses.replace(d.settings, seed=5))
+        eng.submit(a, 4096)
+        eng.submit(b, 16)
+        eng.step(4)
+        eng.cancel(a)
+        for _ in range(10000):
+            da, ta = eng.progress(a)
+            db, tb = eng.progress(b)
+            if da >= ta and db >= tb:
+                break
+            eng.step(4)
+        assert da == ta and ta < 4096 * 128 * 128 and ta % (128 * 128) == 0
+        eng.retire(a)
+        eng.retire(b)
+        assert a.stats()["spp"] == ta // (128 * 128) and b.stats()["spp"] == 16
+        assert np.isfinite(a.film()).all()
+        a.close()
+        b.close()
+    finally:
+        eng.close()
+        scene.close()
