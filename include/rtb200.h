@@ -254,6 +254,10 @@ int rtb200_scene_set_environment(rtb200_scene* scene, int32_t spectrum, int32_t 
  * map (radiance_background).  Replaces a uniform sky and vice versa. */
 int rtb200_scene_set_environment_map(rtb200_scene* scene, const float* rgb, int32_t width, int32_t height,
                                      float scale, const float* orientation_deg, int32_t visible);
+/* Replaces the image environment's rotation by a world -> map matrix
+ * (row major, map_i = sum_j rot9[3 i + j] world_j): a host holding the
+ * radiance map's transform (RadianceMap::GetTransform) passes it as is. */
+int rtb200_scene_set_environment_rotation(rtb200_scene* scene, const float* rot9);
 
 /* Decodes a Radiance HDR (RGBE) file held in memory as the reference's
  * HDRReader does (RasterImages/HDRReader.cpp): *width, *height, and with rgb

@@ -83,4 +83,25 @@ $(OUT)/librise_ref.so: $(LIB_OBJ) $(EXT_OBJ) $(OBJDIR)/ref_lut_data.o $(OBJDIR)/
 
 objects: $(LIB_OBJ) $(EXT_OBJ)
 
-.PHONY: all objects
+# The RISE-side adapter (rise_b200/adapter/: scene extraction and the GPU
+# rasterizer, product code compiled against the reference's headers) with
+# its test driver tests/cpp/rise_adapter_check.cpp, linked against the
+# reference library above and rtb200's; the run paths are relative, so the
+# program also runs where the repository is copied.
+ROOT       := $(abspath $(HERE)..)
+ADAPTER    := $(ROOT)/rise_b200/adapter
+ADAPTER_SRC = $(ADAPTER)/rise_extract.cpp $(ADAPTER)/gpu_rasterizer.cpp $(ROOT)/tests/cpp/rise_adapter_check.cpp
+
+adapter: $(OUT)/rise_adapter_check
+
+$(OUT)/rise_adapter_check: $(ADAPTER_SRC) $(ADAPTER)/rise_extract.h $(ADAPTER)/gpu_rasterizer.h $(OUT)/librise_ref.so \
+                           $(ROOT)/rise_b200/_lib/librtb200.so $(ROOT)/include/rtb200.h
+	$(CXX) $(filter-out -fPIC,$(RISE_FLAGS)) -I$(ROOT)/include -I$(ADAPTER) $(ADAPTER_SRC) -o $@ \
+	    -L$(OUT) -lrise_ref -L$(ROOT)/rise_b200/_lib -lrtb200 \
+	    -Wl,-rpath,'$$ORIGIN' -Wl,-rpath,'$$ORIGIN/../../rise_b200/_lib' $(SHARED_STDCXX) -lpthread
+
+# Exit status 0 when the reference tree is present.
+has-reference:
+	@test -d $(REFLIB)
+
+.PHONY: all objects adapter has-reference

@@ -65,6 +65,7 @@ SIGNATURES = {
     "rtb200_scene_set_environment": (ctypes.c_int, [_vp, _i32, _i32]),
     "rtb200_scene_set_environment_map": (ctypes.c_int, [_vp, _vp, _i32, _i32, ctypes.c_float, _vp, _i32]),
     "rtb200_hdr_decode": (ctypes.c_int, [_vp, _i64, _vp, _vp, _vp]),
+    "rtb200_scene_set_environment_rotation": (ctypes.c_int, [_vp, _vp]),
     "rtb200_job_create": (ctypes.c_int, [_vp, _vp, _vp]),
     "rtb200_job_render": (ctypes.c_int, [_vp, _i32]),
     "rtb200_job_read_film": (ctypes.c_int, [_vp, _vp]),

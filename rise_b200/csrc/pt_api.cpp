@@ -578,6 +578,18 @@ int rtb200_scene_set_environment_map(rtb200_scene* s, const float* rgb, int32_t 
     return RTB200_OK;
 }
 
+int rtb200_scene_set_environment_rotation(rtb200_scene* s, const float* rot9)
+{
+    if (!s || !rot9) return RTB200_E_INVALID;
+    std::lock_guard<std::mutex> g(s->ctx->mu);
+    if (s->committed) return SetError(s->ctx, RTB200_E_INVALID, "scene already committed");
+    if (s->env_w <= 0) return SetError(s->ctx, RTB200_E_INVALID, "scene has no image environment");
+    for (int k = 0; k < 9; ++k)
+        if (!std::isfinite(rot9[k])) return SetError(s->ctx, RTB200_E_INVALID, "bad environment rotation");
+    std::copy(rot9, rot9 + 9, s->env_rot);
+    return RTB200_OK;
+}
+
 int rtb200_scene_set_environment(rtb200_scene* s, int32_t spectrum, int32_t visible)
 {
     if (!s) return RTB200_E_INVALID;
