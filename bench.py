@@ -64,6 +64,7 @@ def parse():
     p.add_argument("--serving-full", action="store_true",
                    help="run only the serving configuration at full size (20 req/s for 60 s over the whole "
                         "batched-scenes distribution, 120 GB device budget; many minutes) and print its JSON")
+    p.add_argument("--serving-skip", default="", help="--serving-full: comma list of arms to leave out (continuous, fifo)")
     return p.parse_args()
 
 
@@ -262,9 +263,10 @@ def bench_path_tracer(ctx, rank, cpu_baseline=True):
 def bench_large_scene(ctx, layout="f32"):
     """Large scene: 1024x1024 fBm heightfield (2,093,058 triangles) + 64 spheres
     of 20,000 triangles (half GGX conductors, half glass), area light and sky;
-    1024x1024 pixels, 64 spp, 4 wavelengths, max depth 16.  relMSE at 64 and
-    256 spp over the 128x128 image centre against the FP64 oracle's 2048-spp
-    render of that crop (tests/golden/spheres_fp64_crop.npz, independent seed)."""
+    1024x1024 pixels, 64 spp, 4 wavelengths, max depth 16.  relMSE at 64, 256
+    and 1024 spp (shuffled Sobol sampler) over the 128x128 image centre
+    against the reference renderer's 4096-spp render of that crop
+    (tests/golden/spheres_crop_ref_4096.npz, independent numbers)."""
     from rise_b200 import pathtracer, scenes
     desc = scenes.spheres_scene()
     t0 = time.perf_counter()
@@ -286,20 +288,22 @@ def bench_large_scene(ctx, layout="f32"):
            "shadow_rays_per_sample": (s1["shadow_rays"] - s0["shadow_rays"]) / n,
            "mrays_s": ((s1["segments"] - s0["segments"]) + (s1["shadow_rays"] - s0["shadow_rays"])) / dt / 1e6}
     r.close()
-    ref_path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "tests", "golden", "spheres_fp64_crop.npz")
+    ref_path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "tests", "golden", "spheres_crop_ref_4096.npz")
     if os.path.exists(ref_path):
         z = np.load(ref_path)
         ref = z["xyz"].astype(np.float64)
         x0, y0, x1, y1 = (int(v) for v in z["crop"])
-        r = pathtracer.SpectralRasterizer(ctx, desc, scene=scene)
+        st = scenes.RenderSettings(**{**desc.settings.__dict__, "sampler": scenes.SAMPLER_SOBOL_SHUFFLED, "seed": 7})
+        r = pathtracer.SpectralRasterizer(ctx, desc, scene=scene, settings=st)
         rel, done = {}, 0
-        for target in (64, 256):
+        for target in (64, 256, 1024):
             r.rasterize_scene(target - done)
             done = target
             img = r.film()[y0:y1, x0:x1].astype(np.float64)
             rel[str(target)] = float(np.mean((img - ref) ** 2 / (ref ** 2 + 1e-2)))
         r.close()
-        out["relmse_vs_fp64_oracle_crop"] = {"crop": [x0, y0, x1, y1], "oracle_spp": int(z["spp"]), **rel}
+        out["relmse_vs_reference_crop"] = {"crop": [x0, y0, x1, y1], "reference_spp": int(z["spp"]),
+                                           "sampler": "sobol_shuffled", **rel}
     scene.close()
     if layout == "f32":
         # The same render over 8-bit quantised child boxes (64-byte nodes).
@@ -418,7 +422,7 @@ def bench_batch(ctx):
 
 
 def bench_serving(ctx, rate=20.0, duration=8.0, resolutions=(128, 256), n_scenes=12, max_tri=300_000,
-                  layout="q8", timeout=600.0, caps=()):
+                  layout="q8", timeout=600.0, caps=(), followup_caps=(), skip=()):
     """Serving loop: Poisson arrivals, progressive 16 -> 64 -> 256 spp per
     request, scenes drawn from a resident pool of the batched-scenes
     distribution (`n_scenes` scenes of up to `max_tri` triangles at
@@ -445,13 +449,18 @@ def bench_serving(ctx, rate=20.0, duration=8.0, resolutions=(128, 256), n_scenes
     try:
         # Warm-up: first launches of every kernel instantiation serving uses.
         serving.serve(ctx, pool, make(arrivals[:12]), mode="continuous")
-        out["continuous"] = serving.serve(ctx, pool, make(), mode="continuous", timeout=timeout)
+        if "continuous" not in skip:
+            out["continuous"] = serving.serve(ctx, pool, make(), mode="continuous", timeout=timeout)
         # Continuous batching with at most `cap` requests in flight: under
         # overload an unbounded mix interleaves every resident scene's paths.
         for cap in caps:
             out[f"continuous_max{cap}"] = serving.serve(ctx, pool, make(), mode="continuous", timeout=timeout,
                                                         max_active=cap)
-        out["fifo"] = serving.serve(ctx, pool, make(), mode="fifo", timeout=timeout)
+        for cap in followup_caps:
+            out[f"continuous_followup{cap}"] = serving.serve(ctx, pool, make(), mode="continuous", timeout=timeout,
+                                                             max_followup=cap)
+        if "fifo" not in skip:
+            out["fifo"] = serving.serve(ctx, pool, make(), mode="fifo", timeout=timeout)
     finally:
         for s in devs:
             s.close()
@@ -573,7 +582,8 @@ def main():
     if args.serving_full:
         ctx = raycaster.Context(local, 120 * 10**9)
         res = bench_serving(ctx, rate=20.0, duration=60.0, resolutions=scenes.RESOLUTIONS, n_scenes=48,
-                            max_tri=1_000_000, timeout=3600.0, caps=(8,))
+                            max_tri=1_000_000, timeout=3600.0, followup_caps=(4,),
+                            skip=tuple(x for x in args.serving_skip.split(",") if x))
         res["budget_bytes"] = 120 * 10**9
         print(json.dumps({"serving_full": res}))
         ctx.close()

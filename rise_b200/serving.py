@@ -46,26 +46,33 @@ def poisson_arrivals(rate, duration, seed):
 
 
 def serve(ctx, pool, requests, mode="continuous", capacity=1 << 21, step_iters=2, use_graph=True,
-          timeout=600.0, max_active=None):
+          timeout=600.0, max_active=None, max_followup=None):
     """Run `requests` (list of Request, arrival-ordered) against `pool`
     (list of (SceneDesc, committed raycaster.Scene)).  Returns a summary
     dict with per-level latency percentiles and aggregate throughput.
     max_active caps the requests in flight in continuous mode (admission
-    waits for a slot; None: only the memory budget limits them)."""
+    waits for a slot; None: only the memory budget limits them).
+    max_followup caps, in continuous mode, the requests whose later levels
+    (after the first) are in flight at once: first levels always start as
+    they arrive, the others wait their turn in order of arrival, so an
+    overloaded server keeps fast first previews without interleaving every
+    resident scene's paths."""
     eng = Engine(ctx, capacity)
     pending = deque(sorted(requests, key=lambda r: r.arrival))
+    later = deque()          # requests whose next level waits for a follow-up slot
     active = []
     finished = []
     samples = 0
     t0 = time.perf_counter()
     try:
-        while pending or active:
+        while pending or active or later:
             now = time.perf_counter() - t0
             if now > timeout:
                 raise RuntimeError("serving run exceeded its time limit")
             # Admission: arrived requests whose film fits the memory budget.
             limit = 1 if mode == "fifo" else max_active
-            while pending and pending[0].arrival <= now and (limit is None or len(active) < limit):
+            inflight = len(active) + len(later)
+            while pending and pending[0].arrival <= now and (limit is None or inflight < limit):
                 r = pending[0]
                 desc, scene = pool[r.scene]
                 try:
@@ -77,6 +84,7 @@ def serve(ctx, pool, requests, mode="continuous", capacity=1 << 21, step_iters=2
                 pending.popleft()
                 eng.submit(r.job, r.levels[0])
                 active.append(r)
+                inflight += 1
             if not active:
                 if pending:
                     time.sleep(max(0.0, min(0.01, pending[0].arrival - (time.perf_counter() - t0))))
@@ -91,17 +99,23 @@ def serve(ctx, pool, requests, mode="continuous", capacity=1 << 21, step_iters=2
                 samples += total
                 r.done_at.append(now - r.arrival)
                 r.level += 1
+                active.remove(r)
                 if r.level < len(r.levels):
-                    eng.submit(r.job, r.levels[r.level] - r.levels[r.level - 1])
+                    later.append(r)
                 else:
                     r.job.close()
                     r.job = None
-                    active.remove(r)
                     finished.append(r)
+            # Next levels, within the follow-up cap.
+            while later and (mode == "fifo" or max_followup is None or
+                             sum(1 for a in active if a.level > 0) < max(1, max_followup)):
+                r = later.popleft()
+                eng.submit(r.job, r.levels[r.level] - r.levels[r.level - 1])
+                active.append(r)
         wall = time.perf_counter() - t0
     finally:
         eng.close()   # detaches any job still submitted
-        for r in active:
+        for r in list(active) + list(later):
             if r.job is not None:
                 r.job.close()
                 r.job = None
@@ -113,4 +127,5 @@ def serve(ctx, pool, requests, mode="continuous", capacity=1 << 21, step_iters=2
             lat[str(lvl)] = {"p50_s": float(np.percentile(v, 50)), "p99_s": float(np.percentile(v, 99)),
                              "mean_s": float(v.mean())}
     return {"mode": mode, "requests": len(finished), "wall_s": wall, "msamples_s": samples / wall / 1e6,
-            "max_active": max_active if mode == "continuous" else 1, "latency": lat}
+            "max_active": max_active if mode == "continuous" else 1,
+            "max_followup": max_followup if mode == "continuous" else None, "latency": lat}

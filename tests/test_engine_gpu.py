@@ -98,8 +98,9 @@ def test_continuous_submission_equals_alone(ctx):
         eng.close()
 
 
-@pytest.mark.parametrize("mode", ["continuous", "fifo"])
-def test_serving_levels_complete_and_match_alone(ctx, mode):
+@pytest.mark.parametrize("mode,caps", [("continuous", {}), ("fifo", {}), ("continuous", {"max_active": 2}),
+                                       ("continuous", {"max_followup": 1})])
+def test_serving_levels_complete_and_match_alone(ctx, mode, caps):
     from rise_b200 import serving
     descs = [scenes.cornell_box(32, 32), scenes.spheres_scene(grid=32, n_spheres=4, sphere_tris=400,
                                                               width=24, height=24, max_depth=8)]
@@ -111,7 +112,7 @@ def test_serving_levels_complete_and_match_alone(ctx, mode):
         st = scenes.RenderSettings(**{**descs[k].settings.__dict__, "seed": 500 + i})
         reqs.append(serving.Request(i, t, k, st, levels=(4, 8)))
     try:
-        res = serving.serve(ctx, pool, reqs, mode=mode, capacity=1 << 14)
+        res = serving.serve(ctx, pool, reqs, mode=mode, capacity=1 << 14, **caps)
         assert res["requests"] == 5 and set(res["latency"]) == {"4", "8"}
         assert all(len(r.done_at) == 2 and r.done_at[0] <= r.done_at[1] for r in reqs)
         assert res["latency"]["8"]["p99_s"] >= res["latency"]["4"]["p50_s"]

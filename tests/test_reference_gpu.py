@@ -188,3 +188,38 @@ def test_spectral_settings_are_checked(ctx, c1):
                 pathtracer.SpectralRasterizer(ctx, c1.desc, "f32", scene=scene, settings=st)
     finally:
         scene.close()
+
+
+def test_large_scene_crop_z_test_against_the_reference(ctx):
+    """The 3,373,060-triangle scene (fBm heightfield, 32 GGX and 32 glass
+    spheres, area light, uniform sky): 16 GPU batches of 16 spp of the full
+    image against the reference renderer's 16 batches of its 128 x 128
+    centre crop (tests/golden/make_spheres_reference.py); image means per
+    channel within 4 standard errors."""
+    from rise_b200 import scenes
+    path = os.path.join(GOLDEN, "spheres_crop_ref_k16_independent.npz")
+    if not os.path.exists(path):
+        pytest.skip("reference crop not generated (tests/golden/make_spheres_reference.py k16)")
+    f = np.load(path)
+    mr, vr, k, spp = f["mean"].astype(np.float64), f["var"].astype(np.float64), int(f["k"]), int(f["spp"])
+    x0, y0, x1, y1 = (int(v) for v in f["crop"])
+    d = scenes.spheres_scene()
+    scene = pathtracer.upload_scene(ctx, d, "f16")
+    try:
+        g = []
+        for b in range(k):
+            st = dataclasses.replace(d.settings, seed=4001 + b, sampler=2)
+            r = pathtracer.SpectralRasterizer(ctx, d, scene=scene, settings=st)
+            r.rasterize_scene(spp)
+            g.append(r.film()[y0:y1, x0:x1].astype(np.float64))
+            r.close()
+    finally:
+        scene.close()
+    g = np.array(g)
+    assert np.isfinite(g).all()
+    z, _ = z_scores(g.mean(0), g.var(0, ddof=1), k, mr, vr, k)
+    rate = float((np.abs(z) > Z_LIMIT).mean())
+    assert rate <= Z_ALLOWED_RATE, rate
+    for c in range(3):
+        se = np.sqrt(g[..., c].mean(axis=(1, 2)).var(ddof=1) / k + vr[..., c].mean() / k / mr[..., c].size)
+        assert abs(g[..., c].mean() - mr[..., c].mean()) < 4 * se, c
