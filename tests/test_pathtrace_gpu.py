@@ -442,15 +442,15 @@ def test_full_size_cornell(ctx):
     assert rel_mse(g[96:160, 96:160], o) < 1e-3
 
 
-def test_large_scene_against_fp64_oracle_crop(ctx):
+def test_large_scene_against_the_reference_crop(ctx):
     """The large spheres scene (3,373,060 triangles, GGX conductors, glass,
-    area light and sky; 1024x1024, depth 16) at 256 spp against the FP64
-    oracle's 2048-spp render of the 128x128 image centre
-    (tests/golden/spheres_fp64_crop.npz, independent seed): relMSE at the
-    GPU's noise level (0.050 measured; the oracle image adds ~0.005) and the
-    crop's mean and quadrant means within 1 % / 2 % (no bias)."""
+    area light and sky; 1024x1024, depth 16) at 256 spp against the
+    reference renderer's 4096-spp render of the 128x128 image centre
+    (tests/golden/spheres_crop_ref_4096.npz, independent numbers): relMSE at
+    the GPU's noise level and the crop's mean and quadrant means within
+    1 % / 2 % (no bias)."""
     import os
-    z = np.load(os.path.join(os.path.dirname(__file__), "golden", "spheres_fp64_crop.npz"))
+    z = np.load(os.path.join(os.path.dirname(__file__), "golden", "spheres_crop_ref_4096.npz"))
     ref = z["xyz"].astype(np.float64)
     x0, y0, x1, y1 = (int(v) for v in z["crop"])
     g, st = render_gpu(ctx, scenes.spheres_scene(), 256, chunks=[128, 128])
