@@ -397,7 +397,7 @@ double Fms(double favg, double eavg)
     return den < 1e-10 ? 0.0 : favg * favg * eavg / den;
 }
 
-struct Ggx { double alpha, spec, eta, k, favg; };
+struct Ggx { double alpha, spec, eta, k, favg, amb; };
 
 struct Light {
     int first, count, emit;
@@ -861,15 +861,20 @@ inline bool RussianRoulette(int depth, int minDepth, double threshold, double cu
     return false;
 }
 
-Ggx GgxAt(const Scene& S, int mat, double lam)
+// amb: the index of the medium around the hit, the top of the path's
+// index-of-refraction stack (PathTracingIntegrator.cpp:4315-4322), which the
+// conductor Fresnel and its hemispherical average take as the incident index
+// (GGXBRDF.cpp:430-434,476-481).
+Ggx GgxAt(const Scene& S, int mat, double lam, double amb)
 {
     Ggx g;
+    g.amb = amb;
     g.alpha = std::max((double)S.mf[2 * mat], 1e-4);
     const int refl = S.mi[5 * mat + 1], eta = S.mi[5 * mat + 3], kap = S.mi[5 * mat + 4];
     g.spec = refl >= 0 ? Spec(S, refl, lam) : 1.0;
     g.eta = eta >= 0 ? Spec(S, eta, lam) : (double)S.mf[2 * mat + 1];
     g.k = kap >= 0 ? Spec(S, kap, lam) : 0.0;
-    g.favg = FresnelAvg(1.0, g.eta, g.k);
+    g.favg = FresnelAvg(amb, g.eta, g.k);
     return g;
 }
 
@@ -883,7 +888,7 @@ double GgxValue(const Ggx& g, V n, V gn, V r, V v)
     const double G2 = 1.0 / (1.0 + Lambda(g.alpha, nv) + Lambda(g.alpha, nr));
     double f = 0.0;
     const double sf = GgxD(g.alpha, Dot(h, n)) * G2 / (4.0 * nv * nr);
-    if (sf > 0) f = g.spec * ConductorF(Dot(r, h), 1.0, g.eta, g.k) * sf;
+    if (sf > 0) f = g.spec * ConductorF(Dot(r, h), g.amb, g.eta, g.k) * sf;
     const double eavg = LookupEavg(g.alpha);
     if (1.0 - eavg > 1e-10)
         f += Fms(g.spec * g.favg, eavg) * (1.0 - LookupEss(nr, g.alpha)) * (1.0 - LookupEss(nv, g.alpha)) / (kPi * (1.0 - eavg));
@@ -898,11 +903,11 @@ double GgxPdf(const Ggx& g, V n, V gn, V r, V v)
     return (wms * MsPdf(cv, g.alpha, MsZ(g.alpha)) + ws * VndfPdf(r, v, n, g.alpha)) / total;
 }
 
-void EvalBsdf(const Scene& S, int mat, double lam, V ns, V gn, V r, V v, double& f, double& pdf)
+void EvalBsdf(const Scene& S, int mat, double lam, double amb, V ns, V gn, V r, V v, double& f, double& pdf)
 {
     if (S.mi[5 * mat] == 1) {
         const V n = Dot(r, ns) < 0 ? -ns : ns;
-        const Ggx g = GgxAt(S, mat, lam);
+        const Ggx g = GgxAt(S, mat, lam, amb);
         f = GgxValue(g, n, gn, r, v);
         pdf = GgxPdf(g, n, gn, r, v);
     } else {
@@ -1002,6 +1007,14 @@ void Sample(const Scene& S, uint32_t pixel, uint32_t sample, double xyz[3])
     double thr[4] = {1, 1, 1, 1}, L[4] = {0, 0, 0, 0};
     double bsdfPdf = 0.0;
     int bounces[3] = {0, 0, 0};
+    // The index-of-refraction stack (Utilities/IORStack.h): the meshes the
+    // path is inside, innermost last, over air; each entry's index is its
+    // material's at the hero wavelength.
+    std::vector<int> inside;
+    auto iorOf = [&](int m) {
+        const int mm = (int)S.meshes[4 * m + 2], sp = S.mi[5 * mm + 3];
+        return sp >= 0 ? Spec(S, sp, lam[0]) : (double)S.mf[2 * mm + 1];
+    };
     for (int depth = 0; depth < S.maxDepth; ++depth) {
         VertexRng rng{key, sample, depth, S.sampler, 0u};
         double mx = 0.0;
@@ -1036,6 +1049,8 @@ void Sample(const Scene& S, uint32_t pixel, uint32_t sample, double xyz[3])
         const int mat = (int)S.meshes[4 * mesh + 2];
         const bool ds = S.meshes[4 * mesh + 3] != 0;
         const int light = S.meshLight[mesh];
+        const double amb = inside.empty() ? 1.0 : iorOf(inside.back());
+        int stackOp = 0;   // 1: push this mesh; -1 - i: remove entry i
         // Shading normal: vertex normals interpolated at the hit, normalised
         // (TriangleMeshGeometryIndexedSpecializations.h:194-199, Object.cpp:543);
         // geometric normal: the face normal on the shading normal's side.
@@ -1085,16 +1100,36 @@ void Sample(const Scene& S, uint32_t pixel, uint32_t sample, double xyz[3])
                         term |= 0xeu;
                         break;
                     }
-            const bool entering = Dot(d, ns0) < 0;
-            const V nn = entering ? ns0 : -ns0;
-            const double n1 = entering ? 1.0 : ior, n2 = entering ? ior : 1.0;
-            const double cosI = -Dot(d, nn), eta = n1 / n2;
+            // Inside or outside from the path's index stack, not the facing
+            // (DielectricSPF.cpp:406-418): inside, the ray leaves for the
+            // medium under this mesh's entry (:177-183); outside, it comes
+            // from the stack's top (:198-207).  w is ri.onb.w(), the shading
+            // normal, turned towards the ray on a double-sided mesh.
+            int pos = -1;
+            for (int i = (int)inside.size() - 1; i >= 0; --i)
+                if (inside[i] == mesh) { pos = i; break; }
+            const bool fromInside = pos >= 0;
+            double exitIor = 1.0;
+            if (fromInside) {
+                const int nIn = (int)inside.size();
+                if (pos == nIn - 1) exitIor = nIn > 1 ? iorOf(inside[nIn - 2]) : 1.0;
+                else exitIor = iorOf(inside[nIn - 1]);
+            }
+            const double n1 = fromInside ? ior : amb, n2 = fromInside ? exitIor : ior;
+            const V w = nsv;
+            const V nEff = fromInside ? -w : w;
+            V geomN = Dot(ng, nEff) >= 0 ? ng : -ng;
+            // Snell's law with the normal turned against the ray
+            // (Optics.cpp:84-98); Fresnel on absolute cosines (:101-159).
+            const V nf = Dot(w, d) > 0 ? -w : w;
+            const double cosI = -Dot(d, nf), eta = n1 / n2;
             const double s2t = eta * eta * std::max(0.0, 1.0 - cosI * cosI);
             double R = 1.0;
             V tdir = {0, 0, 0};
-            if (s2t < 1.0) {
+            const bool snell = 1.0 - s2t >= kNearZero;
+            if (snell) {
                 const double cosT = std::sqrt(1.0 - s2t);
-                tdir = Norm(d * eta + nn * (eta * cosI - cosT));
+                tdir = Norm(d * eta + nf * (eta * cosI - cosT));
                 R = DielectricR(cosI, cosT, n1, n2);
             }
             // ScatterNM's two numbers tilt the transmitted direction by the
@@ -1102,7 +1137,7 @@ void Sample(const Scene& S, uint32_t pixel, uint32_t sample, double xyz[3])
             // exponent of 0 or >= 1e6, mf[0] holding it for a dielectric).
             const double u1 = rng.next(16), u2 = rng.next(17);
             const double expo = S.mf[2 * mat];
-            bool refr = s2t < 1.0;
+            bool refr = snell;
             if (refr && expo > 0 && expo < 1e6) {
                 const double al = std::acos(std::pow(u1, 1.0 / (expo + 1.0)));
                 if (al > 0 && al < 0.5 * kPi) {
@@ -1112,21 +1147,25 @@ void Sample(const Scene& S, uint32_t pixel, uint32_t sample, double xyz[3])
                     tdir = Norm(tdir * std::cos(al) + (tx * std::cos(ph) + ty * std::sin(ph)) * std::sin(al));
                 }
             }
-            // Transmission must cross the surface; reflection must stay above
-            // the geometric surface, mirrored about it under total internal
-            // reflection (:221-243, :274-279).
-            if (refr && !(Dot(tdir, nn) < -kNearZero)) refr = false;
-            V rdir = Norm(d + nn * (2.0 * cosI));
+            // Transmission must cross to the far side of w's crossing;
+            // reflection must stay above the geometric normal on that side,
+            // mirrored about it under total internal reflection
+            // (:221-243, :274-279).
+            if (refr && !(Dot(tdir, nEff) < -kNearZero)) refr = false;
+            V rdir = Norm(d - w * (2.0 * Dot(d, w)));
             bool refl = true;
-            if (!(Dot(rdir, gnv) > 0)) {
-                if (R >= 1.0) rdir = Norm(d - gnv * (2.0 * Dot(d, gnv)));
+            if (!(Dot(rdir, geomN) > 0)) {
+                if (R >= 1.0) rdir = Norm(d - geomN * (2.0 * Dot(d, geomN)));
                 else refl = false;
             }
-            // RandomlySelect over (transmitted 1 - R, reflected R).
+            // RandomlySelect over (transmitted 1 - R, reflected R); the
+            // transmitted ray carries the stack with this mesh pushed or
+            // removed (PathTracingIntegrator.cpp:4814-4816).
             if (rng.next(18) < 1.0 - R) {
                 if (!refr) break;
                 nd = tdir;
                 btype = 2;
+                stackOp = fromInside ? -1 - pos : 1;
             } else {
                 if (!refl) break;
                 nd = rdir;
@@ -1166,7 +1205,7 @@ void Sample(const Scene& S, uint32_t pixel, uint32_t sample, double xyz[3])
                             for (int j = 0; j < 4; ++j) {
                                 if ((S.neePerLambda && j != k) || !live(j)) continue;
                                 double f, pb;
-                                EvalBsdf(S, mat, lam[j], ns, gnv, r, toL, f, pb);
+                                EvalBsdf(S, mat, lam[j], amb, ns, gnv, r, toL, f, pb);
                                 L[j] += thr[j] * lg.le * f * cosS / (dist * dist) / psel;
                             }
                         }
@@ -1195,7 +1234,7 @@ void Sample(const Scene& S, uint32_t pixel, uint32_t sample, double xyz[3])
                             for (int j = 0; j < 4; ++j) {
                                 if ((S.neePerLambda && j != k) || !live(j)) continue;
                                 double f, pb;
-                                EvalBsdf(S, mat, lam[j], ns, gnv, r, toL, f, pb);
+                                EvalBsdf(S, mat, lam[j], amb, ns, gnv, r, toL, f, pb);
                                 const double w = (pb > 0 ? PowerHeuristic(plight, pb) : 1.0) / psel;
                                 L[j] += thr[j] * Spec(S, lg.emit, lam[j]) * cosS * geom * f * w;
                             }
@@ -1227,7 +1266,7 @@ void Sample(const Scene& S, uint32_t pixel, uint32_t sample, double xyz[3])
                         for (int j = 0; j < 4; ++j) {
                             if ((S.neePerLambda && j != k) || !live(j)) continue;
                             double f, pb;
-                            EvalBsdf(S, mat, lam[j], ns, gnv, r, dir, f, pb);
+                            EvalBsdf(S, mat, lam[j], amb, ns, gnv, r, dir, f, pb);
                             const double w = pb > 0 ? PowerHeuristic(epdf, pb) : 1.0;
                             const double le = S.envImg.rgb ? EnvImage::Spectrum(ec, esc, lam[j]) : Spec(S, S.env, lam[j]);
                             L[j] += thr[j] * le * f * cosE / epdf * w;
@@ -1242,7 +1281,7 @@ void Sample(const Scene& S, uint32_t pixel, uint32_t sample, double xyz[3])
             const double ulobe = type == 1 ? rng.next(18) : 0.0;   // GGXSPF draws the lobe first
             const double u1 = rng.next(16), u2 = rng.next(17);
             if (type == 1) {
-                const Ggx g0 = GgxAt(S, mat, lam[0]);
+                const Ggx g0 = GgxAt(S, mat, lam[0], amb);
                 const double cosR = Dot(r, w);
                 const double ws = g0.spec, wms = ws * (1.0 - LookupEss(cosR, g0.alpha)), total = ws + wms;
                 if (!(total > 1e-10)) break;
@@ -1264,7 +1303,7 @@ void Sample(const Scene& S, uint32_t pixel, uint32_t sample, double xyz[3])
                     npdf = (wms * MsPdf(cosO, g0.alpha, msz) + ws * vpdf) / total;
                     const double G2 = 1.0 / (1.0 + Lambda(g0.alpha, cosR) + Lambda(g0.alpha, cosO));
                     const double G1 = 1.0 / (1.0 + Lambda(g0.alpha, cosR));
-                    khero = g0.spec * ConductorF(rm, 1.0, g0.eta, g0.k) * G2 / (G1 * pSpec);
+                    khero = g0.spec * ConductorF(rm, amb, g0.eta, g0.k) * G2 / (G1 * pSpec);
                 } else {
                     // Multiple-scattering lobe: mu from (1 - E_ss(mu)) mu, uniform azimuth.
                     const double eavg = LookupEavg(g0.alpha);
@@ -1285,7 +1324,7 @@ void Sample(const Scene& S, uint32_t pixel, uint32_t sample, double xyz[3])
                 kray[0] = live(0) ? khero : 0.0;
                 const double cosV = std::fabs(Dot(nd, ns));
                 for (int k = 1; k < 4; ++k)
-                    kray[k] = live(k) ? GgxValue(GgxAt(S, mat, lam[k]), w, gnv, r, nd) * cosV / npdf : 0.0;
+                    kray[k] = live(k) ? GgxValue(GgxAt(S, mat, lam[k], amb), w, gnv, r, nd) * cosV / npdf : 0.0;
             } else {
                 const double phi = 2.0 * kPi * u1, sint = std::sqrt(u2), cost = std::sqrt(1.0 - u2);
                 nd = Norm(tx * (std::cos(phi) * sint) + ty * (std::sin(phi) * sint) + w * cost);
@@ -1314,6 +1353,8 @@ void Sample(const Scene& S, uint32_t pixel, uint32_t sample, double xyz[3])
         if (++bounces[btype] > S.maxBounce[btype]) break;
         if (depth + 1 >= S.maxDepth) break;
         for (int k = 0; k < 4; ++k) thr[k] *= kray[k];
+        if (stackOp > 0) inside.push_back(mesh);
+        else if (stackOp < 0) inside.erase(inside.begin() + (-1 - stackOp));
         bsdfPdf = npdf;
         o = p + nd * 1e-8;   // Ray::Advance(1e-8), PathTracingIntegrator.cpp:4812
         d = nd;

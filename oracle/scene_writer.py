@@ -14,7 +14,8 @@ is black) and smooth dielectric (dielectric_material, tau 1, scattering 1e6)
 materials; one RAW triangle file per mesh (rawmesh_geometry); the uniform
 sky as the rasterizer's radiance_map of its spectrum; a pinhole camera and
 the path-tracing spectral rasterizer with hero-wavelength bundles, the box
-filter of width 1 and max depth - 1 bounces of each type.
+filter of width 1 and the settings' per-type bounce limits (else max depth - 1 of
+each type).
 """
 import math
 import os
@@ -34,14 +35,17 @@ def write_risescene(desc, folder, name, spp=16, settings=None):
     returns the scene file's path."""
     st = settings or desc.settings
     os.makedirs(folder, exist_ok=True)
-    bounces = max(1, st.max_depth - 1)
+    # Per-type bounce limits: the settings' own, else max depth - 1 of each
+    # (the reference caps the path itself at 128 vertices).
+    bounces = [getattr(st, k, None) for k in ("max_diffuse_bounce", "max_glossy_bounce", "max_transmission_bounce")]
+    bounces = [max(1, st.max_depth - 1) if b is None else b for b in bounces]
     out = ["RISE ASCII SCENE 7", "", "pathtracing_shaderop", "{", "\tname\t\tpt", "}", "",
            "standard_shader", "{", "\tname\t\tglobal", "\tshaderop\tpt", "}", ""]
     raster = ["pathtracing_spectral_rasterizer", "{", f"\tsamples\t\t\t\t{spp}",
               f"\tnmbegin\t\t\t\t{st.lambda_min:g}", f"\tnmend\t\t\t\t{st.lambda_max:g}", "\thwss\t\t\t\ttrue",
               "\tspectral_samples\t1", "\tpixel_filter\t\tbox", "\tpixel_filter_width\t1", "\tpixel_filter_height\t1",
-              f"\trr_min_depth\t\t{st.rr_min_depth}", f"\tmax_diffuse_bounce\t{bounces}",
-              f"\tmax_glossy_bounce\t{bounces}", f"\tmax_transmission_bounce\t{bounces}", "\toidn_denoise\t\tfalse"]
+              f"\trr_min_depth\t\t{st.rr_min_depth}", f"\tmax_diffuse_bounce\t{bounces[0]}",
+              f"\tmax_glossy_bounce\t{bounces[1]}", f"\tmax_transmission_bounce\t{bounces[2]}", "\toidn_denoise\t\tfalse"]
     if desc.env >= 0:
         raster += ["\tradiance_map\t\tpnt_%d" % desc.env, f"\tradiance_background\t{'true' if desc.env_visible else 'false'}"]
     out += ["film", "{", f"\twidth\t\t{st.width}", f"\theight\t\t{st.height}", "}", ""]

@@ -47,7 +47,8 @@ def signature(descs, spp):
     h = hashlib.sha1()
     for d, s in zip(descs, spp):
         st = d.settings
-        h.update(f"{st.width}x{st.height}:{d.n_tri}:{st.max_depth}:{st.nee_per_lambda}:{s};".encode())
+        lim = (st.max_diffuse_bounce, st.max_glossy_bounce, st.max_transmission_bounce)
+        h.update(f"{st.width}x{st.height}:{d.n_tri}:{st.max_depth}:{lim}:{st.nee_per_lambda}:{s};".encode())
     return h.hexdigest()[:16]
 
 

@@ -30,6 +30,9 @@ __device__ float g_ess[kLut * kLut];          // E_ss[alpha row][mu cell]
 __device__ float g_eavg[kLut];
 __device__ float g_msz[kLut];                 // per row: 2 * integral of (1 - E_ss(mu)) mu dmu
 __device__ float g_mscum[kLut * (kLut + 2)];  // per row: integral of the lobe shape up to each segment
+constexpr int kFavgNodes = 21;
+__device__ float g_favg_x[kFavgNodes];        // Gauss-Legendre nodes on [0, 1] and weights 2 mu w
+__device__ float g_favg_w[kFavgNodes];
 
 // MicrofacetEnergyLUT::LookupEss / LookupEavg (MicrofacetEnergyLUT.h:90-120):
 // bilinear in (alpha, mu) with mu at cell centres.
@@ -223,16 +226,34 @@ struct GgxParams {
     float spec;    // specular colour at this wavelength
     float eta, k;  // conductor optical constants
     float favg;    // hemispherical average of the conductor Fresnel
+    float amb;     // index of the medium around the surface (1: air)
 };
 
-__device__ __forceinline__ GgxParams GgxAt(const PtMaterial& M, const float* spectra, float lam)
+// Hemispherical average 2 * integral of F(mu) mu dmu of the conductor
+// Fresnel from a medium of index ni (MicrofacetEnergyLUT::ComputeFresnelAvg,
+// 21-point Gauss-Legendre); only paths inside a dielectric need it, air's is
+// a spectrum of the material.
+__device__ __noinline__ float ConductorFavg(float ni, float nt, float kt)
+{
+    float s = 0.0f;
+    #pragma unroll 1
+    for (int i = 0; i < kFavgNodes; ++i) s += ConductorF(__ldg(g_favg_x + i), ni, nt, kt) * __ldg(g_favg_w + i);
+    return s;
+}
+
+// amb: the index of the medium around the hit, the top of the path's
+// index-of-refraction stack, which the conductor Fresnel and its average
+// take as the incident index (GGXBRDF.cpp:430-434,476-481).
+__device__ __forceinline__ GgxParams GgxAt(const PtMaterial& M, const float* spectra, float lam, float amb)
 {
     GgxParams g;
     g.alpha = fmaxf(M.alpha, 1e-4f);
     g.spec = M.refl >= 0 ? Spec(spectra, M.refl, lam) : 1.0f;
     g.eta = M.eta >= 0 ? Spec(spectra, M.eta, lam) : M.ior;
     g.k = M.kappa >= 0 ? Spec(spectra, M.kappa, lam) : 0.0f;
-    g.favg = M.pad >= 0 ? Spec(spectra, M.pad, lam) : 0.0f;
+    g.amb = amb;
+    if (amb == 1.0f) g.favg = M.pad >= 0 ? Spec(spectra, M.pad, lam) : 0.0f;
+    else g.favg = ConductorFavg(amb, g.eta, g.k);
     return g;
 }
 
@@ -302,7 +323,7 @@ __device__ __noinline__ float GgxValueAt(const GgxPair& q, const GgxParams& p, f
 {
     if (!q.ok) return 0.0f;
     float f = 0.0f;
-    if (q.sf > 0.0f) f = p.spec * ConductorF(q.rh, 1.0f, p.eta, p.k) * q.sf;
+    if (q.sf > 0.0f) f = p.spec * ConductorF(q.rh, p.amb, p.eta, p.k) * q.sf;
     return f + Fms(p.spec * p.favg, eavg) * q.ms;
 }
 

@@ -91,6 +91,8 @@ struct rtb200_scene {
     std::vector<rtb200::PtLightTri> light_tris;
     // device copies (path tracer)
     rtb200::PtTriAttr* d_attr = nullptr;
+    std::vector<int> mesh_mat;       // material per mesh, built at commit
+    int* d_mesh_mat = nullptr;
     rtb200::PtMaterial* d_mats = nullptr;
     float* d_spectra = nullptr;
     rtb200::PtLight* d_lights = nullptr;

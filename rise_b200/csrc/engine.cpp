@@ -180,7 +180,7 @@ int EngineCreate(rtb200_ctx* ctx, int capacity, rtb200_engine** out)
     size_t off = 0;
     auto take = [&](size_t bytes) { const size_t at = off; off += Align(bytes); return at; };
     const size_t oRo = take(16 * c), oRd = take(16 * c), oHit = take(16 * c), oThr = take(16 * c), oL = take(16 * c),
-                 oAux = take(16 * c), oMeta = take(16 * c);
+                 oAux = take(16 * c), oMeta = take(16 * c), oMed = take(16 * c);
     const size_t oQa = take(4 * c), oQan = take(4 * c), oQf = take(4 * c), oQfn = take(4 * c), oIota = take(4 * c);
     const size_t oSh = take(sizeof(ShadowEntry) * 8 * c);   // up to 4 light + 4 sky samples per path
     const size_t oTab = take(sizeof(PtJobDev) * kMaxJobs), oIds = take(4 * kMaxJobs),
@@ -193,7 +193,7 @@ int EngineCreate(rtb200_ctx* ctx, int capacity, rtb200_engine** out)
     char* b = (char*)e->buf;
     cudaMemset(b, 0, off);
     e->paths = PtPaths{(float4*)(b + oRo), (float4*)(b + oRd), (float4*)(b + oHit), (float4*)(b + oThr),
-                       (float4*)(b + oL), (float4*)(b + oAux), (uint4*)(b + oMeta)};
+                       (float4*)(b + oL), (float4*)(b + oAux), (uint4*)(b + oMeta), (int4*)(b + oMed)};
     e->queues = PtQueues{(int*)(b + oQa), (int*)(b + oQan), (int*)(b + oQf), (int*)(b + oQfn),
                          (ShadowEntry*)(b + oSh), (int*)(b + oCnt), (unsigned long long*)(b + oSmp),
                          (unsigned long long*)(b + oTr), (unsigned*)(b + oErr), (PtAssign*)(b + oAsg),
@@ -261,7 +261,7 @@ int EngineSubmit(rtb200_engine* e, rtb200_job* j, int spp)
     PtJobDev& d = e->h_table[entry];
     d.scene = PtScene{s->d_nodes, s->layout, (int)s->n_nodes, s->d_tris, (int)s->tri_material.size(), s->d_attr, s->d_mats,
                       s->d_spectra, s->d_lights, s->d_light_tris, s->d_light_nodes, s->d_light_alias,
-                      s->d_tri_normals, (const PtEnvMap*)s->d_env};
+                      s->d_tri_normals, (const PtEnvMap*)s->d_env, s->d_mesh_mat};
     d.cam = j->cam;
     d.set = j->set;
     int npx = j->npix;

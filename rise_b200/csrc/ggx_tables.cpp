@@ -196,6 +196,12 @@ const GgxTables& GetGgxTables()
             t.mscum[a * (kGgxLut + 2) + kGgxLut + 1] = (float)I;
             t.msz[a] = (float)(2.0 * I);
         }
+        double x[kGgxFavgNodes], w[kGgxFavgNodes];
+        LegendreNodes(kGgxFavgNodes, x, w);
+        for (int i = 0; i < kGgxFavgNodes; ++i) {
+            t.favg_x[i] = (float)x[i];
+            t.favg_w[i] = (float)(2.0 * x[i] * w[i]);
+        }
     });
     return t;
 }

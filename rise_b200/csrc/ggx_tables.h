@@ -4,6 +4,7 @@
 namespace rtb200 {
 
 constexpr int kGgxLut = 32;
+constexpr int kGgxFavgNodes = 21;   // Gauss-Legendre nodes of the Fresnel average
 
 struct GgxTables {
     float ess[kGgxLut * kGgxLut];  // [alpha][mu]
@@ -12,6 +13,9 @@ struct GgxTables {
     // per alpha row: integral of (1 - E_ss(mu)) mu over the segments before
     // segment k, k = 0 .. kGgxLut + 1 (the last entry is the whole integral)
     float mscum[kGgxLut * (kGgxLut + 2)];
+    // Hemispherical Fresnel average as a sum over [0, 1]: nodes mu_i and
+    // weights 2 mu_i w_i, for an incident index other than air's.
+    float favg_x[kGgxFavgNodes], favg_w[kGgxFavgNodes];
 };
 
 // Computed once per process (thread-safe).

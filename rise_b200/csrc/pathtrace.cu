@@ -506,12 +506,27 @@ __device__ __forceinline__ GgxPair NeePair(int mtype, const GgxPoint& gp, V3 ns,
     return q;
 }
 
+// Top of a path's index-of-refraction stack (entries from x upward, -1 past
+// the top); the stack is read only when it holds a mesh.
+__device__ __forceinline__ int MediaTop(int4 m)
+{
+    return m.w >= 0 ? m.w : (m.z >= 0 ? m.z : (m.y >= 0 ? m.y : m.x));
+}
+
+// The index a stack entry stands for: its dielectric's at the hero
+// wavelength, as IORStack::push records it (DielectricSPF.cpp:198-207).
+__device__ __noinline__ float MeshIor(const PtScene& S, int mesh, float lam)
+{
+    const PtMaterial M = S.mats[__ldg(S.mesh_mat + mesh)];
+    return M.eta >= 0 ? Spec(S.spectra, M.eta, lam) : M.ior;
+}
+
 // The BSDF value at one wavelength for a next-event pair.
 __device__ __forceinline__ float NeeValue(int mtype, const PtMaterial& M, const float* spectra, float lam,
-                                          const GgxPair& q, float eavg)
+                                          const GgxPair& q, float eavg, float amb)
 {
     if (!q.ok) return 0.0f;
-    if (mtype == kMatGGX) return GgxValueAt(q, GgxAt(M, spectra, lam), eavg);
+    if (mtype == kMatGGX) return GgxValueAt(q, GgxAt(M, spectra, lam, amb), eavg);
     return Spec(spectra, M.refl, lam) * kInvPi;
 }
 
@@ -640,6 +655,17 @@ KShade(const PtJobDev* __restrict__ jobs, PtPaths P, PtQueues Q, int from_class)
             const V3 gnv = dot(ng, d) < 0.0f ? ng : -ng;   // geometric normal facing the ray
             const PtMaterial M = S.mats[mi];
             const int mtype = CLS < 0 ? M.type : CLS;
+            // The path's index-of-refraction stack (IORStack.h); its top is
+            // the medium around the hit, the ambient index of a conductor
+            // (PathTracingIntegrator.cpp:4315-4322).  Lambertian shading
+            // needs neither.
+            int4 med = make_int4(-1, -1, -1, -1);
+            float amb = 1.0f;
+            if (CLS != 0 && (m.z & kFlagInMedium)) {
+                med = P.media[slot];
+                amb = MeshIor(S, MediaTop(med), lam[0]);
+            }
+            bool media_changed = false;
 
             // PART 1: emission with MIS against light sampling (:4424-4518).
             if (M.emit >= 0 && (m.z & kFlagConsiderEmission) && dot(-d, ng) > 0.0f) {
@@ -682,17 +708,41 @@ KShade(const PtJobDev* __restrict__ jobs, PtPaths P, PtQueues Q, int from_class)
                         }
                     }
                 }
-                const bool entering = dot(d, ns0) < 0.0f;
-                const V3 nn = entering ? ns0 : -ns0;
-                const float n1 = entering ? 1.0f : ior, n2 = entering ? ior : 1.0f;
-                const float cosI = -dot(d, nn);
+                // Inside or outside from the stack, not the facing
+                // (DielectricSPF.cpp:406-418): inside, the ray leaves for the
+                // medium under this mesh's entry (:177-183); outside, it comes
+                // from the stack's top (:198-207).  w is ri.onb.w(), the
+                // shading normal turned towards the ray on a double-sided mesh.
+                const int mesh = at.light >= 0 ? S.lights[at.light].mesh : ~at.light;
+                int e[kPtMediaDepth] = {med.x, med.y, med.z, med.w};
+                int depthIn = 0, pos = -1;
+                #pragma unroll
+                for (int i = 0; i < kPtMediaDepth; ++i) {
+                    if (e[i] >= 0) depthIn = i + 1;
+                    if (e[i] == mesh) pos = i;
+                }
+                const bool fromInside = pos >= 0;
+                float exitIor = 1.0f;
+                if (fromInside) {
+                    const int below = pos == depthIn - 1 ? (depthIn >= 2 ? e[depthIn - 2] : -1) : e[depthIn - 1];
+                    if (below >= 0) exitIor = MeshIor(S, below, lam[0]);
+                }
+                const float n1 = fromInside ? ior : amb, n2 = fromInside ? exitIor : ior;
+                const V3 w = ns;
+                const V3 nEff = fromInside ? -w : w;
+                const V3 geomN = dot(ng, nEff) >= 0.0f ? ng : -ng;
+                // Snell's law with the normal turned against the ray
+                // (Optics.cpp:84-98); Fresnel on absolute cosines (:101-159).
+                const V3 nf = dot(w, d) > 0.0f ? -w : w;
+                const float cosI = -dot(d, nf);
                 const float eta = n1 / n2;
                 const float s2t = eta * eta * fmaxf(0.0f, 1.0f - cosI * cosI);
+                const bool snell = 1.0f - s2t >= kNearZero;
                 float R = 1.0f;
                 V3 tdir = mk(0.0f, 0.0f, 0.0f);
-                if (s2t < 1.0f) {
+                if (snell) {
                     const float cosT = sqrtf(1.0f - s2t);
-                    tdir = normalize(d * eta + nn * (eta * cosI - cosT));
+                    tdir = normalize(d * eta + nf * (eta * cosI - cosT));
                     R = DielectricR(cosI, cosT, n1, n2);
                 }
                 // ScatterNM's two numbers (DielectricSPF.cpp:421) tilt the
@@ -700,7 +750,7 @@ KShade(const PtJobDev* __restrict__ jobs, PtPaths P, PtQueues Q, int from_class)
                 // exponent: acos(u^(1/(n+1))) off it, uniform in azimuth
                 // (GenerateScatteredRay, :248-272; none at 0 or >= 1e6).
                 const float u1 = rng.next(16), u2 = rng.next(17);
-                bool refr = s2t < 1.0f;
+                bool refr = snell;
                 if (refr && M.alpha > 0.0f && M.alpha < 1e6f) {
                     const float a = acosf(powf(u1, 1.0f / (M.alpha + 1.0f)));
                     if (a > 0.0f && a < 0.5f * kPi) {
@@ -712,24 +762,39 @@ KShade(const PtJobDev* __restrict__ jobs, PtPaths P, PtQueues Q, int from_class)
                         tdir = normalize(tdir * ca + (tx * cp + ty * sp) * sa);
                     }
                 }
-                // The transmitted ray must cross the surface (:274-279); the
-                // reflected one must stay above the geometric surface, and
-                // under total internal reflection mirrors about the geometric
-                // normal instead (:221-243).
-                if (refr && !(dot(tdir, nn) < -kNearZero)) refr = false;
-                V3 rdir = normalize(d + nn * (2.0f * cosI));
+                // The transmitted ray must cross to the far side of w's
+                // crossing (:274-279); the reflected one must stay above the
+                // geometric normal on that side, and under total internal
+                // reflection mirrors about it instead (:221-243).
+                if (refr && !(dot(tdir, nEff) < -kNearZero)) refr = false;
+                V3 rdir = normalize(d - w * (2.0f * dot(d, w)));
                 bool refl = true;
-                if (!(dot(rdir, gnv) > 0.0f)) {
-                    if (R >= 1.0f) rdir = normalize(d - gnv * (2.0f * dot(d, gnv)));
+                if (!(dot(rdir, geomN) > 0.0f)) {
+                    if (R >= 1.0f) rdir = normalize(d - geomN * (2.0f * dot(d, geomN)));
                     else refl = false;
                 }
                 // RandomlySelect over (transmitted 1 - R, reflected R)
                 // (ScatteredRayContainer.cpp:43-70); a lobe the reference
-                // drops ends the path here with the same expectation.
+                // drops ends the path here with the same expectation.  The
+                // transmitted ray carries the stack with this mesh pushed or
+                // removed (PathTracingIntegrator.cpp:4814-4816).
                 if (rng.next(18) < 1.0f - R) {
                     if (!refr) break;
                     nd = tdir;
                     btype = kBounceTransmission;
+                    if (fromInside) {
+                        #pragma unroll
+                        for (int i = 0; i < kPtMediaDepth - 1; ++i)
+                            if (i >= pos) e[i] = e[i + 1];
+                        e[kPtMediaDepth - 1] = -1;
+                    } else {
+                        if (depthIn == kPtMediaDepth) break;   // deeper than the stack kept per path
+                        #pragma unroll
+                        for (int i = 0; i < kPtMediaDepth; ++i)
+                            if (i == depthIn) e[i] = mesh;
+                    }
+                    med = make_int4(e[0], e[1], e[2], e[3]);
+                    media_changed = true;
                 } else {
                     if (!refl) break;
                     nd = rdir;
@@ -780,7 +845,7 @@ KShade(const PtJobDev* __restrict__ jobs, PtPaths P, PtQueues Q, int from_class)
                                 for (int j = 0; j < 4; ++j) {
                                     if (term & (1u << j)) continue;
                                     if (set.nee_per_lambda && j != k) continue;
-                                    const float f = NeeValue(mtype, M, S.spectra, lam[j], bq, gp.eavg);
+                                    const float f = NeeValue(mtype, M, S.spectra, lam[j], bq, gp.eavg, amb);
                                     const float v = Get(thr, j) * lg.le * f * cosS / (dist * dist) / psel;
                                     Set(c, j, v);
                                     any |= v != 0.0f;
@@ -824,7 +889,7 @@ KShade(const PtJobDev* __restrict__ jobs, PtPaths P, PtQueues Q, int from_class)
                                 for (int j = 0; j < 4; ++j) {
                                     if (term & (1u << j)) continue;
                                     if (set.nee_per_lambda && j != k) continue;
-                                    const float f = NeeValue(mtype, M, S.spectra, lam[j], bq, gp.eavg);
+                                    const float f = NeeValue(mtype, M, S.spectra, lam[j], bq, gp.eavg, amb);
                                     const float w = (pb > 0.0f ? PowerHeuristic(plight, pb) : 1.0f) / psel;
                                     const float v = Get(thr, j) * Spec(S.spectra, lg.emit, lam[j]) * cosS * geom * f * w;
                                     Set(c, j, v);
@@ -870,7 +935,7 @@ KShade(const PtJobDev* __restrict__ jobs, PtPaths P, PtQueues Q, int from_class)
                             for (int j = 0; j < 4; ++j) {
                                 if (term & (1u << j)) continue;
                                 if (set.nee_per_lambda && j != k) continue;
-                                const float f = NeeValue(mtype, M, S.spectra, lam[j], bq, gp.eavg);
+                                const float f = NeeValue(mtype, M, S.spectra, lam[j], bq, gp.eavg, amb);
                                 const float w = pb > 0.0f ? PowerHeuristic(epdf, pb) : 1.0f;
                                 const float le = (ENV && S.env_map) ? EnvSpectrum(es, lam[j])
                                                                     : Spec(S.spectra, set.env, lam[j]);
@@ -893,7 +958,7 @@ KShade(const PtJobDev* __restrict__ jobs, PtPaths P, PtQueues Q, int from_class)
                 const float ulobe = mtype == kMatGGX ? rng.next(18) : 0.0f;
                 const float u1 = rng.next(16), u2 = rng.next(17);
                 if (mtype == kMatGGX) {
-                    const GgxParams g0 = GgxAt(M, S.spectra, lam[0]);
+                    const GgxParams g0 = GgxAt(M, S.spectra, lam[0], amb);
                     const float cosR = dot(r, w);
                     const float ws = g0.spec;
                     const float wms = ws * (1.0f - gp.essR);
@@ -915,7 +980,7 @@ KShade(const PtJobDev* __restrict__ jobs, PtPaths P, PtQueues Q, int from_class)
                         npdf = (wms * MsPdf(cosO, g0.alpha, msz) + ws * vpdf) / total;
                         const float G2 = 1.0f / (1.0f + GgxLambda(g0.alpha, cosR) + GgxLambda(g0.alpha, cosO));
                         const float G1 = 1.0f / (1.0f + GgxLambda(g0.alpha, cosR));
-                        khero = g0.spec * ConductorF(rm, 1.0f, g0.eta, g0.k) * G2 / (G1 * pSpec);
+                        khero = g0.spec * ConductorF(rm, amb, g0.eta, g0.k) * G2 / (G1 * pSpec);
                     } else {
                         // Multiple-scattering lobe: mu_o from (1 - E(mu_o)) mu_o,
                         // uniform azimuth (GGXSPF.cpp:604-675).
@@ -944,7 +1009,7 @@ KShade(const PtJobDev* __restrict__ jobs, PtPaths P, PtQueues Q, int from_class)
                     #pragma unroll 1
                     for (int k = 1; k < 4; ++k) {
                         if (term & (1u << k)) continue;
-                        Set(kray, k, GgxValueAt(cq, GgxAt(M, S.spectra, lam[k]), gp.eavg) * cosV / npdf);
+                        Set(kray, k, GgxValueAt(cq, GgxAt(M, S.spectra, lam[k], amb), gp.eavg) * cosV / npdf);
                     }
                 } else {
                     // Lambertian: cosine-weighted direction, kray = rho(lambda),
@@ -997,6 +1062,10 @@ KShade(const PtJobDev* __restrict__ jobs, PtPaths P, PtQueues Q, int from_class)
             P.thr[slot] = thr;
             P.aux[slot] = make_float4(aux.x, npdf, aux.z, __uint_as_float(bounces));
             m.z = (m.z & ~(kFlagDepthMask | kFlagSpecular)) | (unsigned)(depth + 1) | nflags;
+            if (media_changed) {
+                P.media[slot] = med;
+                m.z = med.x >= 0 ? (m.z | kFlagInMedium) : (m.z & ~kFlagInMedium);
+            }
             P.meta[slot].z = m.z;
             cont = true;
         } while (false);
@@ -1153,12 +1222,15 @@ void LaunchTrace(const PtLaunch& L, cudaStream_t st, bool extend)
     }
 }
 
-cudaError_t PtSetGgxTables(const float* ess, const float* eavg, const float* msz, const float* mscum)
+cudaError_t PtSetGgxTables(const float* ess, const float* eavg, const float* msz, const float* mscum,
+                           const float* favg_x, const float* favg_w)
 {
     cudaError_t e = cudaMemcpyToSymbol(g_ess, ess, sizeof(float) * kLut * kLut);
     if (e == cudaSuccess) e = cudaMemcpyToSymbol(g_eavg, eavg, sizeof(float) * kLut);
     if (e == cudaSuccess) e = cudaMemcpyToSymbol(g_msz, msz, sizeof(float) * kLut);
     if (e == cudaSuccess) e = cudaMemcpyToSymbol(g_mscum, mscum, sizeof(float) * kLut * (kLut + 2));
+    if (e == cudaSuccess) e = cudaMemcpyToSymbol(g_favg_x, favg_x, sizeof(float) * kFavgNodes);
+    if (e == cudaSuccess) e = cudaMemcpyToSymbol(g_favg_w, favg_w, sizeof(float) * kFavgNodes);
     return e;
 }
 

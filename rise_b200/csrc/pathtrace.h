@@ -33,7 +33,8 @@ cudaError_t PtIteration(const PtLaunch& L, int iter, cudaStream_t st);
 cudaError_t PtDrain(const PtLaunch& L, cudaStream_t st);
 // Upload the GGX E_ss (32 x 32), E_avg (32), multiple-scattering lobe
 // normalisation (32) and cumulative segment integral (32 x 34) tables.
-cudaError_t PtSetGgxTables(const float* ess, const float* eavg, const float* msz, const float* mscum);
+cudaError_t PtSetGgxTables(const float* ess, const float* eavg, const float* msz, const float* mscum,
+                           const float* favg_x, const float* favg_w);
 // Fold a film of this request (n floats) into the compensated running sums
 // and clear it.
 cudaError_t PtFold(float* pass, float* sum, float* comp, int n, int sms, cudaStream_t st);

@@ -197,7 +197,7 @@ int UploadShading(rtb200_scene* s)
     }
     {
         const GgxTables& gt = GetGgxTables();
-        const cudaError_t e = PtSetGgxTables(gt.ess, gt.eavg, gt.msz, gt.mscum);
+        const cudaError_t e = PtSetGgxTables(gt.ess, gt.eavg, gt.msz, gt.mscum, gt.favg_x, gt.favg_w);
         if (e != cudaSuccess) return CudaCheck(ctx, e, "GGX tables");
     }
     for (const auto& mesh : s->meshes)
@@ -247,6 +247,7 @@ int UploadShading(rtb200_scene* s)
         weight.push_back(area * std::max(mean, 1e-12));
         boxes.push_back(box);
         meshLight[mi] = (int)s->lights.size();
+        L.mesh = (int)mi;
         s->lights.push_back(L);
     }
     // Point lights (PointLight.h:49-57, LightSampler.cpp:655-668): the
@@ -262,6 +263,7 @@ int UploadShading(rtb200_scene* s)
         PtLight L{};
         L.kind = 1;
         L.emit = -1;
+        L.mesh = -1;
         L.first = L.count = 0;
         L.le = (float)(0.2126 * pl.color[0] * pl.power + 0.7152 * pl.color[1] * pl.power +
                        0.0722 * pl.color[2] * pl.power);
@@ -303,7 +305,7 @@ int UploadShading(rtb200_scene* s)
         const int mi = triMesh[s->leaf_prims[slot]];
         const auto& mesh = s->meshes[mi];
         attr[slot].mat = (mesh.material & kAttrMatMask) | (mesh.double_sided ? kAttrDoubleSided : 0);
-        attr[slot].light = meshLight[mi];
+        attr[slot].light = meshLight[mi] >= 0 ? meshLight[mi] : ~mi;
     }
     // Vertex normals in leaf order, unit length, octahedron-encoded; the
     // triangles of meshes without normals keep their face normal.
@@ -373,6 +375,11 @@ int UploadShading(rtb200_scene* s)
     if (!rc && !s->light_nodes.empty()) rc = Upload(ctx, &s->d_light_nodes, s->light_nodes, total);
     if (!rc && !s->light_alias.empty()) rc = Upload(ctx, &s->d_light_alias, s->light_alias, total);
     if (!rc && !s->tri_normals.empty()) rc = Upload(ctx, &s->d_tri_normals, s->tri_normals, total);
+    if (!rc) {
+        s->mesh_mat.resize(s->meshes.size());
+        for (size_t mi = 0; mi < s->meshes.size(); ++mi) s->mesh_mat[mi] = (int)s->meshes[mi].material;
+        rc = Upload(ctx, &s->d_mesh_mat, s->mesh_mat, total);
+    }
     if (!rc && s->env_w > 0) rc = UploadEnv(s, total);
     s->shade_bytes = total;
     if (rc) FreeShading(s);
@@ -390,6 +397,8 @@ void FreeShading(rtb200_scene* s)
     DevFree(ctx, s->d_light_nodes, s->light_nodes.size() * sizeof(PtLightNode));
     DevFree(ctx, s->d_light_alias, s->light_alias.size() * sizeof(PtLightAlias));
     DevFree(ctx, s->d_tri_normals, s->tri_normals.size() * sizeof(uint4));
+    DevFree(ctx, s->d_mesh_mat, s->mesh_mat.size() * sizeof(int));
+    s->d_mesh_mat = nullptr;
     DevFree(ctx, s->d_env, s->env_bytes);
     s->d_env = nullptr;
     s->env_bytes = 0;

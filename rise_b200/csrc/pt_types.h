@@ -42,7 +42,7 @@ struct PtLight {
     int kind;        // 0: a mesh luminary; 1: a point light at pos, radiance-like `le`
     float le;        // point light: luminance of colour x power (flat over wavelength)
     float pos[3];
-    int pad;
+    int mesh;        // the luminary's mesh (-1 for a point light)
 };
 
 // Light BVH node (LightBVHNode, Lights/LightBVH.h:100-115), preorder: the
@@ -130,11 +130,18 @@ constexpr int kFilterSplat = 1;   // Gaussian splat, 4 channels (XYZ and weight)
 constexpr int kFilterWarp = 2;    // Gaussian-warped position, 3-channel mean
 
 // Per-triangle shading attributes in leaf order: material | double-sided
-// bit (bit 30), and luminary index (-1 = none).
+// bit (bit 30), and the luminary index, or ~mesh for a triangle of a mesh
+// that is no luminary (the index-of-refraction stack keys on meshes, the
+// reference's objects; a luminary's mesh is PtLight::mesh).
 struct PtTriAttr {
     int mat;
     int light;
 };
+
+// Index-of-refraction stack depth kept per path (PtPaths::media): dielectric
+// meshes a path can be inside at once.  The reference's stack is unbounded;
+// a path that would enter a fifth nested dielectric ends there.
+constexpr int kPtMediaDepth = 4;
 
 constexpr int kAttrDoubleSided = 1 << 30;
 constexpr int kAttrSmooth = 1 << 29;   // interpolated vertex normals (PtScene::tri_normals)
@@ -145,6 +152,7 @@ constexpr unsigned kFlagDepthMask = 0xffu;
 constexpr unsigned kFlagConsiderEmission = 1u << 8;
 constexpr unsigned kFlagFinishing = 1u << 9;
 constexpr unsigned kFlagSpecular = 1u << 10;
+constexpr unsigned kFlagInMedium = 1u << 11;   // PtPaths::media holds at least one mesh
 constexpr unsigned kTermShift = 12;        // 4 bits: terminated wavelengths
 
 // Shadow-ray queue entry, 48 bytes.
@@ -192,6 +200,9 @@ struct PtScene {
     // Image environment (env_map.h), or null: then PtSettings::env names a
     // uniform sky's spectrum, or none.
     const PtEnvMap* env_map;
+    // Material of each mesh, for the indices of the meshes on a path's
+    // index-of-refraction stack.
+    const int* mesh_mat;
 };
 
 // Octahedral encoding of a unit vector (Cigolle et al., "A Survey of
@@ -222,6 +233,10 @@ struct PtPaths {
     float4* L;       // radiance per wavelength
     float4* aux;     // x hero wavelength, y bsdf pdf
     uint4* meta;     // x pixel, y sample, z flags, w rng key
+    // Index-of-refraction stack (Utilities/IORStack.h): the dielectric
+    // meshes the path is inside, innermost last, -1 past the top; read only
+    // when meta.z has kFlagInMedium (an empty stack otherwise).
+    int4* media;
 };
 
 constexpr int kPtMaxJobs = 1024;   // jobs per engine (one KAssign thread each)

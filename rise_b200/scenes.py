@@ -453,6 +453,12 @@ def spheres_scene(grid=1024, n_spheres=64, sphere_tris=20000, width=1024, height
     radiance 0.3 (both on 400-700 nm).  With the defaults this is the
     large-scene configuration: 2,093,058 + 64 x 20,000 triangles, 1024 x 1024
     pixels, max depth 16.
+
+    Max depth N is set as the reference's path-tracing rasterizer takes it
+    from a scene file: per-type bounce limits of N - 1 diffuse, glossy and
+    transmission scatters (max_diffuse_bounce etc., StabilityConfig) under
+    its fixed cap of 128 path vertices (PathTracingIntegrator.h:187), so
+    that a path through glass may have more than N vertices.
     """
     rng = np.random.default_rng(seed)
     d = SceneDesc()
@@ -481,8 +487,9 @@ def spheres_scene(grid=1024, n_spheres=64, sphere_tris=20000, width=1024, height
     d.env = sky
     d.env_visible = 1
     d.settings = RenderSettings(width=width, height=height, cam_pos=(0.5, 0.55, -0.45), cam_look=(0.5, 0.0, 0.55),
-                                cam_up=(0.0, 1.0, 0.0), fov_deg=45.0, max_depth=max_depth,
-                                nee_per_lambda=nee_per_lambda, seed=1)
+                                cam_up=(0.0, 1.0, 0.0), fov_deg=45.0, max_depth=128,
+                                max_diffuse_bounce=max_depth - 1, max_glossy_bounce=max_depth - 1,
+                                max_transmission_bounce=max_depth - 1, nee_per_lambda=nee_per_lambda, seed=1)
     return d
 
 

@@ -33,11 +33,16 @@ oracle/rise_ref.mk), on tests/golden/cornell_c1.RISEscene:
   wavelength bundles; the prism with one wavelength per path in 30 bins and
   two spectral samples per pixel sample (the prism scenes at 16 batches of 64
   samples per pixel).
+* cornell_overlap_ref_k16_independent.npz -- 16 x 64 spp with independent
+  numbers of tests/golden/cornell_overlap.RISEscene (make_cornell_scene.py
+  overlap): overlapping glass spheres of indices 1.5 and 1.33 and a GGX
+  conductor cutting into one of them, the z-test of the index-of-refraction
+  stack.
 * cornell_env_ref_k16_independent.npz -- the same for
   tests/golden/cornell_env.RISEscene (tests/golden/make_env_scene.py): a
   scene lit only by an HDR light probe, rotated and scaled, 128 x 128.
 
-    make -C oracle && python tests/golden/make_cornell_reference.py [k16|k16i|smooth|variants|env|fp64]
+    make -C oracle && python tests/golden/make_cornell_reference.py [k16|k16i|smooth|variants|overlap|env|fp64]
     (k16, k16i: ~40 s each, fp64: ~45 min on 8 cores; rows are checkpointed under
     oracle/_ref/ so an interrupted run resumes)
 """
@@ -82,7 +87,7 @@ def make_fp64(r):
 
 
 def main():
-    which = sys.argv[1:] or ["k16", "k16i", "smooth", "variants", "env", "fp64"]
+    which = sys.argv[1:] or ["k16", "k16i", "smooth", "variants", "overlap", "env", "fp64"]
     r = oracle.RefRenderer(SCENE)
     if "k16" in which:
         make_k16(r)
@@ -102,6 +107,9 @@ def main():
         for v, spp in (("cornell_nm", K_SPP), ("cornell_prism", 64), ("cornell_prism_nm", 64)):
             make_k16(oracle.RefRenderer(os.path.join(HERE, v + ".RISEscene")), independent=True,
                      name=v + "_ref_k16_independent.npz", spp=spp)
+    if "overlap" in which:
+        make_k16(oracle.RefRenderer(os.path.join(HERE, "cornell_overlap.RISEscene")), independent=True,
+                 name="cornell_overlap_ref_k16_independent.npz", spp=64)
 
 
 if __name__ == "__main__":

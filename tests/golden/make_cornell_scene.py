@@ -22,6 +22,7 @@ depth 8), 256 x 256, 16 samples per pixel.
     python tests/golden/make_cornell_scene.py           (the C1 scene)
     python tests/golden/make_cornell_scene.py smooth    (the smooth-shaded variant)
     python tests/golden/make_cornell_scene.py variants  (single-wavelength and dispersive variants)
+    python tests/golden/make_cornell_scene.py overlap   (overlapping glass and metal spheres)
 """
 import math
 import os
@@ -231,3 +232,54 @@ def main_variants():
 
 if __name__ == "__main__" and sys.argv[1:] == ["variants"]:
     main_variants()
+
+
+# ---- overlapping media ---------------------------------------------------------
+# cornell_overlap: the C1 walls and light around two overlapping glass spheres
+# of different indices (1.5 and 1.33; single-sided, outward winding) and a
+# GGX conductor sphere (double-sided) that cuts into the first.  The
+# reference's index-of-refraction stack (Utilities/IORStack.h) gives the
+# indices on either side of each crossing (1.5 -> 1.33 from the first sphere
+# into the second, not air -> 1.33) and the conductor's Fresnel seen from
+# inside the glass (incident index 1.5).  Hero-wavelength bundles.
+#     python tests/golden/make_cornell_scene.py overlap
+OVERLAP = [("glass_a", (0.42, 0.25, 0.45), 0.2, "glass_a", False),
+           ("glass_b", (0.62, 0.22, 0.38), 0.16, "glass_b", False),
+           ("metal", (0.30, 0.14, 0.30), 0.12, "metal", True)]
+
+
+def overlap_scene_text():
+    text, _ = scene_text()
+    text = text.replace("# The C1 spectral Cornell box (written by tests/golden/make_cornell_scene.py).",
+                        "# The C1 box around overlapping glass and metal spheres "
+                        "(written by tests/golden/make_cornell_scene.py).")
+    text = text.replace(f"\tfile\t\t{NAME}_", "\tfile\t\tcornell_c1_")
+    cut = text.index("rawmesh_geometry\n{\n\tname\t\tg_boxes")
+    end = text.index("rawmesh_geometry\n{\n\tname\t\tg_light")
+    text = text[:cut] + text[end:]
+    text = text.replace("max_diffuse_bounce\t7", "max_diffuse_bounce\t7\n\tmax_glossy_bounce\t8\n"
+                        "\tmax_transmission_bounce\t8")
+    extra = ["dielectric_material", "{", "\tname\t\tglass_a", "\ttau\t\t\t1.0", "\tior\t\t\t1.5",
+             "\tscattering\t1000000", "}", "",
+             "dielectric_material", "{", "\tname\t\tglass_b", "\ttau\t\t\t1.0", "\tior\t\t\t1.33",
+             "\tscattering\t1000000", "}", "",
+             "ggx_material", "{", "\tname\t\tmetal", "\trs\t\t\tpnt_white", "\tior\t\t\t0.4",
+             "\textinction\t2.5", "\talphax\t\t0.2", "\talphay\t\t0.2", "}", ""]
+    for name, c, r, mat, ds in OVERLAP:
+        extra += ["rawmesh_geometry", "{", f"\tname\t\tg_{name}", f"\tfile\t\tcornell_overlap_{name}.raw",
+                  f"\tdouble_sided\t{'true' if ds else 'false'}", "}", ""]
+        extra += ["standard_object", "{", f"\tname\t\to_{name}", f"\tgeometry\tg_{name}", f"\tmaterial\t{mat}",
+                  "}", ""]
+    return text + "\n".join(extra)
+
+
+def main_overlap():
+    with open(os.path.join(HERE, "cornell_overlap.RISEscene"), "w") as f:
+        f.write(overlap_scene_text())
+    for name, c, r, _, _ in OVERLAP:
+        with open(os.path.join(HERE, f"cornell_overlap_{name}.raw"), "w") as f:
+            f.write(raw_text(scenes.uv_sphere(c, r, 960)))
+
+
+if __name__ == "__main__" and sys.argv[1:] == ["overlap"]:
+    main_overlap()

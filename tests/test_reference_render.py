@@ -171,6 +171,26 @@ def test_dispersive_glass_matches_the_reference(name):
     assert _z_rate(const, st, mr, vr, k, spp, rows, 1100)[0] > 2 * Z_ALLOWED_RATE
 
 
+def test_overlapping_media_match_the_reference():
+    """Two overlapping glass spheres (indices 1.5 and 1.33) and a GGX
+    conductor cutting into the first: the reference keeps an index-of-
+    refraction stack per path (IORStack.h), so a ray crossing from the first
+    sphere into the second refracts from 1.5 to 1.33, leaves the first for
+    the second's 1.33, and the conductor's Fresnel inside the glass takes 1.5
+    as its incident index.  The restatement's 16 batches against the
+    reference's 16 on the rows through the overlaps."""
+    ls, mr, vr, k, spp = _variant("cornell_overlap")
+    st = ls.desc.settings
+    assert sorted(m.ior for m in ls.desc.materials if m.type == 2) == [1.33, 1.5]
+    rows = (160, 192)
+    rate, g = _z_rate(ls.desc, st, mr, vr, k, spp, rows, 1500)
+    assert rate <= Z_ALLOWED_RATE, rate
+    y0, y1 = rows
+    for c in range(3):
+        se = np.sqrt(g[..., c].mean(axis=(1, 2)).var(ddof=1) / k + vr[y0:y1, :, c].mean() / k / g[0, ..., c].size)
+        assert abs(g[..., c].mean() - mr[y0:y1, :, c].mean()) < 4 * se, c
+
+
 def test_image_environment_matches_the_reference():
     """A scene lit only by an HDR light probe: the angular mapping after a
     30-degree turn about y, bilinear texels, the unbounded spectral uplift per
