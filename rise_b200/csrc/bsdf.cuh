@@ -241,20 +241,31 @@ __device__ __noinline__ float ConductorFavg(float ni, float nt, float kt)
     return s;
 }
 
-// amb: the index of the medium around the hit, the top of the path's
-// index-of-refraction stack, which the conductor Fresnel and its average
-// take as the incident index (GGXBRDF.cpp:430-434,476-481).
-__device__ __forceinline__ GgxParams GgxAt(const PtMaterial& M, const float* spectra, float lam, float amb)
+// One wavelength's parameters from the values a shading point looked up once
+// for each of its wavelengths (specular colour, optical constants, and the
+// Fresnel average for the incident index amb: GgxFavg).  amb is the index of
+// the medium around the hit, the top of the path's index-of-refraction stack,
+// which the conductor Fresnel takes as the incident index (GGXBRDF.cpp:430-434).
+__device__ __forceinline__ GgxParams GgxFrom(const PtMaterial& M, float spec, float eta, float k, float favg, float amb)
 {
     GgxParams g;
     g.alpha = fmaxf(M.alpha, 1e-4f);
-    g.spec = M.refl >= 0 ? Spec(spectra, M.refl, lam) : 1.0f;
-    g.eta = M.eta >= 0 ? Spec(spectra, M.eta, lam) : M.ior;
-    g.k = M.kappa >= 0 ? Spec(spectra, M.kappa, lam) : 0.0f;
+    g.spec = spec;
+    g.eta = eta;
+    g.k = k;
+    g.favg = favg;
     g.amb = amb;
-    if (amb == 1.0f) g.favg = M.pad >= 0 ? Spec(spectra, M.pad, lam) : 0.0f;
-    else g.favg = ConductorFavg(amb, g.eta, g.k);
     return g;
+}
+
+// The conductor's hemispherical Fresnel average at one wavelength for the
+// incident index amb (GGXBRDF.cpp:476-481): air's is a spectrum of the
+// material, any other is integrated here.
+__device__ __forceinline__ float GgxFavg(const PtMaterial& M, const float* spectra, float lam, float amb, float eta,
+                                         float k)
+{
+    if (amb == 1.0f) return M.pad >= 0 ? Spec(spectra, M.pad, lam) : 0.0f;
+    return ConductorFavg(amb, eta, k);
 }
 
 // ---- evaluation split by what depends on the wavelength ----------------------

@@ -522,12 +522,25 @@ __device__ __noinline__ float MeshIor(const PtScene& S, int mesh, float lam)
 }
 
 // The BSDF value at one wavelength for a next-event pair.
-__device__ __forceinline__ float NeeValue(int mtype, const PtMaterial& M, const float* spectra, float lam,
+// The shading point's spectra at its four wavelengths, looked up once: the
+// Lambertian reflectance or the GGX specular colour, the conductor's optical
+// constants and its Fresnel average for the medium around the hit.
+struct PointSpectra {
+    float4 refl, eta, k, favg;
+};
+
+__device__ __forceinline__ GgxParams GgxOf(const PtMaterial& M, const PointSpectra& ps, int j, float amb)
+{
+    return GgxFrom(M, Get(ps.refl, j), Get(ps.eta, j), Get(ps.k, j), Get(ps.favg, j), amb);
+}
+
+// The BSDF value at wavelength j for a next-event pair.
+__device__ __forceinline__ float NeeValue(int mtype, const PtMaterial& M, const PointSpectra& ps, int j,
                                           const GgxPair& q, float eavg, float amb)
 {
     if (!q.ok) return 0.0f;
-    if (mtype == kMatGGX) return GgxValueAt(q, GgxAt(M, spectra, lam, amb), eavg);
-    return Spec(spectra, M.refl, lam) * kInvPi;
+    if (mtype == kMatGGX) return GgxValueAt(q, GgxOf(M, ps, j, amb), eavg);
+    return Get(ps.refl, j) * kInvPi;
 }
 
 // Sort the active paths into shading classes (escaped or Lambertian, GGX,
@@ -805,7 +818,23 @@ KShade(const PtJobDev* __restrict__ jobs, PtPaths P, PtQueues Q, int from_class)
             } else {
                 const V3 r = -d;
                 GgxPoint gp{1.0f, 0.0f, 0.0f, 0.0f};
-                if (mtype == kMatGGX) gp = GgxPointAt(M.alpha, fabsf(dot(r, ns)));
+                PointSpectra ps;
+                ps.refl = ps.eta = ps.k = ps.favg = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+                if (mtype == kMatGGX) {
+                    gp = GgxPointAt(M.alpha, fabsf(dot(r, ns)));
+                    #pragma unroll 1
+                    for (int k = 0; k < 4; ++k) {
+                        const float e = M.eta >= 0 ? Spec(S.spectra, M.eta, lam[k]) : M.ior;
+                        const float kk = M.kappa >= 0 ? Spec(S.spectra, M.kappa, lam[k]) : 0.0f;
+                        Set(ps.refl, k, M.refl >= 0 ? Spec(S.spectra, M.refl, lam[k]) : 1.0f);
+                        Set(ps.eta, k, e);
+                        Set(ps.k, k, kk);
+                        Set(ps.favg, k, GgxFavg(M, S.spectra, lam[k], amb, e, kk));
+                    }
+                } else {
+                    #pragma unroll 1
+                    for (int k = 0; k < 4; ++k) Set(ps.refl, k, Spec(S.spectra, M.refl, lam[k]));
+                }
                 // PART 2: next-event estimation (LightSampler::EvaluateDirectLightingNM,
                 // LightSampler.cpp:1942-2361): one area-light sample and one sky
                 // sample per wavelength (reference) or one shared sample.
@@ -845,7 +874,7 @@ KShade(const PtJobDev* __restrict__ jobs, PtPaths P, PtQueues Q, int from_class)
                                 for (int j = 0; j < 4; ++j) {
                                     if (term & (1u << j)) continue;
                                     if (set.nee_per_lambda && j != k) continue;
-                                    const float f = NeeValue(mtype, M, S.spectra, lam[j], bq, gp.eavg, amb);
+                                    const float f = NeeValue(mtype, M, ps, j, bq, gp.eavg, amb);
                                     const float v = Get(thr, j) * lg.le * f * cosS / (dist * dist) / psel;
                                     Set(c, j, v);
                                     any |= v != 0.0f;
@@ -889,7 +918,7 @@ KShade(const PtJobDev* __restrict__ jobs, PtPaths P, PtQueues Q, int from_class)
                                 for (int j = 0; j < 4; ++j) {
                                     if (term & (1u << j)) continue;
                                     if (set.nee_per_lambda && j != k) continue;
-                                    const float f = NeeValue(mtype, M, S.spectra, lam[j], bq, gp.eavg, amb);
+                                    const float f = NeeValue(mtype, M, ps, j, bq, gp.eavg, amb);
                                     const float w = (pb > 0.0f ? PowerHeuristic(plight, pb) : 1.0f) / psel;
                                     const float v = Get(thr, j) * Spec(S.spectra, lg.emit, lam[j]) * cosS * geom * f * w;
                                     Set(c, j, v);
@@ -935,7 +964,7 @@ KShade(const PtJobDev* __restrict__ jobs, PtPaths P, PtQueues Q, int from_class)
                             for (int j = 0; j < 4; ++j) {
                                 if (term & (1u << j)) continue;
                                 if (set.nee_per_lambda && j != k) continue;
-                                const float f = NeeValue(mtype, M, S.spectra, lam[j], bq, gp.eavg, amb);
+                                const float f = NeeValue(mtype, M, ps, j, bq, gp.eavg, amb);
                                 const float w = pb > 0.0f ? PowerHeuristic(epdf, pb) : 1.0f;
                                 const float le = (ENV && S.env_map) ? EnvSpectrum(es, lam[j])
                                                                     : Spec(S.spectra, set.env, lam[j]);
@@ -958,7 +987,7 @@ KShade(const PtJobDev* __restrict__ jobs, PtPaths P, PtQueues Q, int from_class)
                 const float ulobe = mtype == kMatGGX ? rng.next(18) : 0.0f;
                 const float u1 = rng.next(16), u2 = rng.next(17);
                 if (mtype == kMatGGX) {
-                    const GgxParams g0 = GgxAt(M, S.spectra, lam[0], amb);
+                    const GgxParams g0 = GgxOf(M, ps, 0, amb);
                     const float cosR = dot(r, w);
                     const float ws = g0.spec;
                     const float wms = ws * (1.0f - gp.essR);
@@ -1009,7 +1038,7 @@ KShade(const PtJobDev* __restrict__ jobs, PtPaths P, PtQueues Q, int from_class)
                     #pragma unroll 1
                     for (int k = 1; k < 4; ++k) {
                         if (term & (1u << k)) continue;
-                        Set(kray, k, GgxValueAt(cq, GgxAt(M, S.spectra, lam[k], amb), gp.eavg) * cosV / npdf);
+                        Set(kray, k, GgxValueAt(cq, GgxOf(M, ps, k, amb), gp.eavg) * cosV / npdf);
                     }
                 } else {
                     // Lambertian: cosine-weighted direction, kray = rho(lambda),
@@ -1022,7 +1051,7 @@ KShade(const PtJobDev* __restrict__ jobs, PtPaths P, PtQueues Q, int from_class)
                     npdf = fabsf(dot(nd, w)) * kInvPi;
                     // Geometric-horizon gate (LambertianSPF.cpp:141-151).
                     if (!(dot(nd, gn) > 0.0f)) break;
-                    for (int k = 0; k < 4; ++k) Set(kray, k, (term & (1u << k)) ? 0.0f : Spec(S.spectra, M.refl, lam[k]));
+                    for (int k = 0; k < 4; ++k) Set(kray, k, (term & (1u << k)) ? 0.0f : Get(ps.refl, k));
                 }
                 // The integrator's choice among the scattered rays
                 // (ScatteredRayContainer::RandomlySelect; one ray here).
