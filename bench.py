@@ -308,16 +308,18 @@ def bench_large_scene(ctx, layout="f32"):
                                            "sampler": "sobol_shuffled", **rel}
     scene.close()
     if layout == "f32":
-        # The same render over 8-bit quantised child boxes (64-byte nodes).
-        q = pathtracer.upload_scene(ctx, desc, "q8")
-        r = pathtracer.SpectralRasterizer(ctx, desc, scene=q)
-        r.rasterize_scene(4)
-        s0 = r.stats()
-        r.rasterize_scene(64)
-        s1 = r.stats()
-        out["q8_nodes_msamples_s"] = (s1["samples"] - s0["samples"]) / (s1["seconds"] - s0["seconds"]) / 1e6
-        r.close()
-        q.close()
+        # The same render over 8-bit quantised child boxes (64-byte nodes) and
+        # over binary16 child boxes (the same hits as FP32 boxes).
+        for lay in ("q8", "f16"):
+            q = pathtracer.upload_scene(ctx, desc, lay)
+            r = pathtracer.SpectralRasterizer(ctx, desc, scene=q)
+            r.rasterize_scene(4)
+            s0 = r.stats()
+            r.rasterize_scene(64)
+            s1 = r.stats()
+            out[lay + "_nodes_msamples_s"] = (s1["samples"] - s0["samples"]) / (s1["seconds"] - s0["seconds"]) / 1e6
+            r.close()
+            q.close()
     return out
 
 
