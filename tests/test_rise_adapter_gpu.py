@@ -20,7 +20,7 @@ GOLDEN = os.path.join(ROOT, "tests", "golden")
 EXE = os.path.join(ROOT, "oracle", "_ref", "rise_adapter_check")
 
 
-@pytest.mark.parametrize("name", ["cornell_c1", "cornell_smooth", "cornell_env"])
+@pytest.mark.parametrize("name", ["cornell_c1", "cornell_smooth", "cornell_env", "cornell_overlap"])
 def test_adapter_renders_the_reference_scene_as_the_ingest_does(name, tmp_path):
     if not os.path.exists(EXE):
         pytest.skip("the RISE adapter test driver is not built (needs the reference tree)")

@@ -310,3 +310,23 @@ def test_reference_pointlight_cornell_loads():
     p = os.path.join(REF, "scenes", "Tests", "Spectral", "cornellbox_pointlight_spectral.RISEscene")
     s = scenefile.load_scene(p, search=[REF])
     assert len(s.desc.point_lights) == 1 and s.desc.n_tri > 0
+
+
+def test_written_scene_keeps_the_depth_semantics(tmp_path):
+    """A scene description written in the reference's scene language
+    (oracle/scene_writer.py, the input of the reference-renderer fixtures)
+    reads back with the same depth settings: the reference's file format has
+    no total path cap (its rasterizer caps paths at 128 vertices) and takes
+    max depth N as per-type bounce limits of N - 1, which is how
+    scenes.spheres_scene() sets its own; materials and the sky read back
+    too."""
+    from oracle.scene_writer import write_risescene
+    d = scenes.spheres_scene(grid=8, n_spheres=2, sphere_tris=80, width=16, height=12, max_depth=10)
+    st = d.settings
+    assert (st.max_depth, st.max_diffuse_bounce, st.max_glossy_bounce, st.max_transmission_bounce) == (128, 9, 9, 9)
+    back = scenefile.load_scene(write_risescene(d, str(tmp_path), "s"))
+    bs = back.desc.settings
+    assert (bs.max_depth, bs.max_diffuse_bounce, bs.max_glossy_bounce, bs.max_transmission_bounce) == (128, 9, 9, 9)
+    assert (bs.width, bs.height) == (16, 12)
+    assert [m.type for m in back.desc.materials if m.emission < 0] == [m.type for m in d.materials if m.emission < 0]
+    assert back.desc.n_tri == d.n_tri and back.desc.env >= 0
