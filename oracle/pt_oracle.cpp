@@ -17,7 +17,10 @@
 //                                                GeometricUtilities.cpp:85-98
 //   * GGX conductor                             GGXSPF.cpp:424-688, GGXBRDF.cpp:339-498,
 //                                                MicrofacetUtils.h, MicrofacetEnergyLUT.h, Optics.hpp
-//   * smooth dielectric                         DielectricSPF.cpp:120-300, Optics.cpp:101-160
+//   * smooth dielectric                         DielectricSPF.cpp:120-300, :395-432, Optics.cpp:39-160
+//   * index-of-refraction stack per path         IORStack.h, PathTracingIntegrator.cpp:4315-4328,
+//                                                :4684, :4814-4816; conductor incident index
+//                                                GGXBRDF.cpp:430-434, :476-481
 //   * point on a mesh luminary                  TriangleMeshGeometryIndexed.cpp:207-218,
 //                                                GeometricUtilities.cpp:543-569
 //   * power heuristic, Russian roulette         PathTransportUtilities.h:86-110, :251
