@@ -24,8 +24,10 @@
 //   * point on a mesh luminary                  TriangleMeshGeometryIndexed.cpp:207-218,
 //                                                GeometricUtilities.cpp:543-569
 //   * power heuristic, Russian roulette         PathTransportUtilities.h:86-110, :251
-// Random numbers are the same counter-based hash the device uses, so a pixel
-// sample follows the same decisions here and on the GPU up to rounding.
+// Random numbers come from the same samplers the device has (the counter-
+// based hash, the reference's Owen-scrambled Sobol and its shuffled variant),
+// so a pixel sample follows the same decisions here and on the GPU up to
+// rounding.
 // Loaded only by tests and bench.py's CPU-baseline leg.
 
 #include <algorithm>
