@@ -38,11 +38,15 @@ oracle/rise_ref.mk), on tests/golden/cornell_c1.RISEscene:
   overlap): overlapping glass spheres of indices 1.5 and 1.33 and a GGX
   conductor cutting into one of them, the z-test of the index-of-refraction
   stack.
+* cornell_dsglass_ref_k16_independent.npz -- 16 x 64 spp with independent
+  numbers of tests/golden/cornell_dsglass.RISEscene (make_cornell_scene.py
+  dsglass): a double-sided glass sphere, whose normals turn towards the ray
+  while its dielectric reads inside / outside from the stack.
 * cornell_env_ref_k16_independent.npz -- the same for
   tests/golden/cornell_env.RISEscene (tests/golden/make_env_scene.py): a
   scene lit only by an HDR light probe, rotated and scaled, 128 x 128.
 
-    make -C oracle && python tests/golden/make_cornell_reference.py [k16|k16i|smooth|variants|overlap|env|fp64]
+    make -C oracle && python tests/golden/make_cornell_reference.py [k16|k16i|smooth|variants|overlap|dsglass|env|fp64]
     (k16, k16i: ~40 s each, fp64: ~45 min on 8 cores; rows are checkpointed under
     oracle/_ref/ so an interrupted run resumes)
 """
@@ -87,7 +91,7 @@ def make_fp64(r):
 
 
 def main():
-    which = sys.argv[1:] or ["k16", "k16i", "smooth", "variants", "overlap", "env", "fp64"]
+    which = sys.argv[1:] or ["k16", "k16i", "smooth", "variants", "overlap", "dsglass", "env", "fp64"]
     r = oracle.RefRenderer(SCENE)
     if "k16" in which:
         make_k16(r)
@@ -110,6 +114,9 @@ def main():
     if "overlap" in which:
         make_k16(oracle.RefRenderer(os.path.join(HERE, "cornell_overlap.RISEscene")), independent=True,
                  name="cornell_overlap_ref_k16_independent.npz", spp=64)
+    if "dsglass" in which:
+        make_k16(oracle.RefRenderer(os.path.join(HERE, "cornell_dsglass.RISEscene")), independent=True,
+                 name="cornell_dsglass_ref_k16_independent.npz", spp=64)
 
 
 if __name__ == "__main__":

@@ -23,6 +23,7 @@ depth 8), 256 x 256, 16 samples per pixel.
     python tests/golden/make_cornell_scene.py smooth    (the smooth-shaded variant)
     python tests/golden/make_cornell_scene.py variants  (single-wavelength and dispersive variants)
     python tests/golden/make_cornell_scene.py overlap   (overlapping glass and metal spheres)
+    python tests/golden/make_cornell_scene.py dsglass   (a double-sided glass sphere)
 """
 import math
 import os
@@ -283,3 +284,40 @@ def main_overlap():
 
 if __name__ == "__main__" and sys.argv[1:] == ["overlap"]:
     main_overlap()
+
+
+# ---- double-sided glass ----------------------------------------------------------
+# cornell_dsglass: the C1 walls and light around one glass sphere (IOR 1.5,
+# flat-shaded RAW mesh) marked double-sided.  The reference turns a double-
+# sided mesh's normals towards the ray (TriangleMeshGeometry.cpp:94-120) while
+# its dielectric takes inside / outside from the index-of-refraction stack, so
+# a ray leaving the sphere sees the normal on its own side and the refracted
+# ray fails the crossing test (DielectricSPF.cpp:274-279): only total internal
+# reflection leaves the inside.
+#     python tests/golden/make_cornell_scene.py dsglass
+DSGLASS = ("glass_ds", (0.5, 0.25, 0.45), 0.22)
+
+
+def dsglass_scene_text():
+    text = overlap_scene_text()
+    text = text.replace("# The C1 box around overlapping glass and metal spheres",
+                        "# The C1 box around a double-sided glass sphere")
+    cut = text.index("dielectric_material\n{\n\tname\t\tglass_b")
+    text = text[:cut]
+    name, c, r = DSGLASS
+    extra = ["rawmesh_geometry", "{", f"\tname\t\tg_{name}", f"\tfile\t\tcornell_dsglass_{name}.raw",
+             "\tdouble_sided\ttrue", "}", "",
+             "standard_object", "{", f"\tname\t\to_{name}", f"\tgeometry\tg_{name}", "\tmaterial\tglass_a", "}", ""]
+    return text + "\n".join(extra)
+
+
+def main_dsglass():
+    with open(os.path.join(HERE, "cornell_dsglass.RISEscene"), "w") as f:
+        f.write(dsglass_scene_text())
+    name, c, r = DSGLASS
+    with open(os.path.join(HERE, f"cornell_dsglass_{name}.raw"), "w") as f:
+        f.write(raw_text(scenes.uv_sphere(c, r, 960)))
+
+
+if __name__ == "__main__" and sys.argv[1:] == ["dsglass"]:
+    main_dsglass()

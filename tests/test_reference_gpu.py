@@ -133,7 +133,7 @@ def test_smooth_shading_same_random_numbers_as_the_oracle(ctx, sampler):
     assert abs(g[..., 1].mean() / o[..., 1].mean() - 1) < 2e-3
 
 
-VARIANTS = ["cornell_nm", "cornell_prism", "cornell_prism_nm", "cornell_env", "cornell_overlap"]
+VARIANTS = ["cornell_nm", "cornell_prism", "cornell_prism_nm", "cornell_env", "cornell_overlap", "cornell_dsglass"]
 
 
 def _variant(name):
@@ -150,7 +150,8 @@ def test_wavelength_sampling_z_test_against_the_reference(ctx, name, sampler):
     with two spectral samples; a scene lit only by an HDR light probe
     (rotated, scaled; bilinear lookups uplifted per lookup, importance-
     sampled next events); overlapping glass spheres of different indices and
-    a conductor inside glass (the index-of-refraction stack): 16 GPU batches
+    a conductor inside glass (the index-of-refraction stack); a double-sided
+    glass sphere: 16 GPU batches
     against the reference's 16
     (independent numbers), every pixel; image means per channel within 4
     standard errors."""

@@ -191,6 +191,26 @@ def test_overlapping_media_match_the_reference():
         assert abs(g[..., c].mean() - mr[y0:y1, :, c].mean()) < 4 * se, c
 
 
+def test_double_sided_glass_matches_the_reference():
+    """A glass sphere on a double-sided mesh: the reference turns both of its
+    normals towards the ray (TriangleMeshGeometry.cpp:94-120) while the
+    dielectric reads inside / outside from the index-of-refraction stack, so
+    from inside the refracted ray fails the crossing test and only total
+    internal reflection goes on (DielectricSPF.cpp:177-279).  The
+    restatement's 16 batches against the reference's 16 on the rows through
+    the sphere; the same sphere read as single-sided fails the test."""
+    ls, mr, vr, k, spp = _variant("cornell_dsglass")
+    st = ls.desc.settings
+    glass = [i for i, (_, _, mat, ds) in enumerate(ls.desc.meshes) if ls.desc.materials[mat].type == 2]
+    assert len(glass) == 1 and ls.desc.meshes[glass[0]][3] == 1
+    rows = (176, 208)
+    rate, _ = _z_rate(ls.desc, st, mr, vr, k, spp, rows, 1700)
+    assert rate <= Z_ALLOWED_RATE, rate
+    single = dataclasses.replace(ls.desc)
+    single.meshes = [(f, c, m, 0 if i == glass[0] else ds) for i, (f, c, m, ds) in enumerate(ls.desc.meshes)]
+    assert _z_rate(single, st, mr, vr, k, spp, rows, 1700)[0] > 2 * Z_ALLOWED_RATE
+
+
 def test_image_environment_matches_the_reference():
     """A scene lit only by an HDR light probe: the angular mapping after a
     30-degree turn about y, bilinear texels, the unbounded spectral uplift per
