@@ -25,7 +25,7 @@ from rise_b200 import scenes, scenefile
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 GOLDEN = os.path.join(ROOT, "tests", "golden")
 EXE = os.path.join(ROOT, "oracle", "_ref", "rise_adapter_check")
-SCENES = ["cornell_c1", "cornell_smooth", "cornell_prism", "cornell_env", "cornell_overlap"]
+SCENES = ["cornell_c1", "cornell_smooth", "cornell_prism", "cornell_env", "cornell_overlap", "cornell_dsglass"]
 NM = np.arange(380.0, 781.0, 1.0) + 0.25
 
 
